@@ -1,0 +1,1040 @@
+// ORACLE TEST INFRASTRUCTURE -- not part of the product. Only the tests, smoke() and the
+// CPU-baseline leg of bench.py load this library, and only as the checker.
+//
+// Single-threaded CPU restatement of the reference's per-timestep RT path (plain C2Ray mode:
+// subgrid = FALSE, ifront = FALSE, c2ray_iter = TRUE, multi_freq = TRUE, case-B recombination),
+// configured at run time instead of through user_inputs.h. Every routine follows the reference
+// expression by expression -- including which sub-expressions are float and which double,
+// and which float overloads of the <cmath> functions get picked -- so that with the reference
+// compiled for one thread (oracle/build_ref.py) the two agree bit for bit. The ray buffer is a
+// list kept in creation order, which is the reference's slot order for one thread while the
+// allocation ring has not wrapped (mem_funcs.cc:79-97).
+//
+// Reference map: rates rates.cc:41-238; spectrum gas_funcs.cc:11-70; init init_funcs.cc:10-142;
+// cast ray_tracing.cc:230-321 + rt_funcs.cc:240-261; advance ray_tracing.cc:1222-1512 +
+// rt_funcs.cc:159-208; C2Ray iteration ray_tracing.cc:623-1216; merge machinery
+// ray_tracing.cc:35-227, 324-477; split ray_tracing.cc:482-619 + rt_funcs.cc:211-237; thermal
+// gas_funcs.cc:104-242, 353-457; rotations healpix_funcs.cc:21-39, 102-143; dt rt_funcs.cc:9-12.
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <cmath>
+#include <vector>
+
+#include "frtd.h"
+#include "../flexrt_imaging_reion_b200/csrc/hp_nest.h"
+
+using namespace std;
+
+namespace orc {
+
+// ---- constants (global_constants.h, global_variables.cc) --------------------------------
+#define O_PI 3.14159
+#define O_H 6.626068e-27
+#define O_H_EV 4.135667e-15
+#define O_KB 1.38065e-16
+#define O_KPC_TO_CM 3.086e21
+#define O_CL 2.998e10
+#define O_MH 1.672622e-24
+#define O_Y 0.246
+#define O_HH 0.68
+#define O_OMEGA_M 0.305147
+#define O_OMEGA_L 0.6948
+#define O_MPC_TO_KM 3.086e19
+#define O_EV_CGS 1.60218e-12
+static const double kPhotNorm = 1e60;
+static const float kNheToNh = (O_Y / 4.) / (1. - O_Y);
+static const float kTempMin = 1e2;
+static const float kMinDist = 1e-4;
+static const int kNalpha = 35;
+static const int kNtheta = 42875;
+static const int kMaxF = 8;
+static const int kMaxPL = 16;
+
+static inline float mind(float a, float b) { return (a >= b) ? b : a; }
+static inline float maxd(float a, float b) { return (b >= a) ? b : a; }
+static inline double mindd(double a, double b) { return (a >= b) ? b : a; }
+static inline float absd(float x) { return (x >= 0.) ? x : -1. * x; }
+static inline int mins(short a, short b) { return (a >= b) ? b : a; }
+static inline int maxs(short a, short b) { return (b >= a) ? b : a; }
+static inline int imin(int a, int b) { return (a >= b) ? b : a; }
+static inline int imod(int a, int b) {
+  while (a < 0) a += b;
+  return a % b;
+}
+
+// ---- atomic data: Verner et al. 1996 cross sections, Hui & Gnedin 1997 rates -------------
+static double lambda_x(double T, double Eth) {
+  double K2eV = O_KB / O_EV_CGS;
+  double eV2K = 1.0 / K2eV;
+  return 2 * Eth * eV2K / T;
+}
+static double verner(double nu, double Eth, double Emax, double E0, double y0, double y1, double yw, double ya,
+                     double P) {
+  double E = O_H_EV * nu;
+  double x = E / E0 - y0;
+  double y = pow(pow(x, 2) + pow(y1, 2), 0.5);
+  double F = (pow(x - 1, 2) + pow(yw, 2)) * pow(y, 0.5 * P - 5.5) * pow(1 + pow(y / ya, 0.5), -P);
+  if (O_H_EV * nu >= Eth && O_H_EV * nu <= Emax) return F;
+  return 0;
+}
+static double sig_H1(double nu) { return 5.475e-14 * verner(nu, 13.6, 5e4, 4.298e-1, 0, 0, 0, 3.288e+1, 2.963); }
+static double sig_He1(double nu) {
+  return 9.492e-16 * verner(nu, 2.459e+1, 5e4, 1.361e+1, 4.434e-1, 2.136, 2.039, 1.469, 3.188);
+}
+static double alphaB_H2(double T) {
+  double x = lambda_x(T, 13.6);
+  return 2.753e-14 * pow(x, 1.500) / pow((1.0 + pow((x / 2.740), 0.407)), 2.2420);
+}
+static double alphaB_He2(double T) {
+  double x = lambda_x(T, 2.459e+1);
+  return 1.26e-14 * pow(x, 0.750);
+}
+static double alphaB_He3(double T) {
+  double x = lambda_x(T, 5.442e+1);
+  return 2 * 2.753e-14 * pow(x, 1.500) / pow((1.0 + pow((x / 2.740), 0.407)), 2.2420);
+}
+static double Dalpha_He2(double T) {
+  double x = lambda_x(T, 5.442e+1);
+  return 1.90e-3 * pow(T, -1.5) * exp(-0.75 * x / 2) * (1 + 0.3 * exp(-0.15 * x / 2));
+}
+static double rcrB_H2(double T) {
+  double x = lambda_x(T, 13.6);
+  return 3.435e-30 * T * pow(x, 1.970) / (pow(1. + pow(x / 2.250, 0.376), 3.720));
+}
+static double rcrB_He2(double T) { return O_KB * T * alphaB_He2(T); }
+static double free_free_rate(double T) { return 1.42e-27 * pow(T, 0.5) * 1.30; }
+static double compton_rate(double z) { return 5.6072e-36 * pow(1 + z, 4.); }
+static float hubble(float a) { return O_HH * 100. / O_MPC_TO_KM * pow(O_OMEGA_M / pow(a, 3.) + O_OMEGA_L, 0.5); }
+
+// ---- state -----------------------------------------------------------------------------
+struct Ray {
+  bool alive, active;
+  short order;
+  int pixel;
+  unsigned short itheta;
+  float xhat, yhat, zhat;
+  float nphot[kMaxF];
+  float r, dr, x, y, z, time;
+  int pind[kMaxPL];
+  float pdist[kMaxPL];
+  short ray_end;
+};
+
+struct Src {
+  int i, j, k;
+  double lum;
+};
+
+struct Ctx {
+  // configuration
+  int N, F, PL, itercount, ray_per_cell_max, hpx_lvl, l_max;
+  double nu[kMaxF];
+  float cl_factor, tstep_factor, nl_const, safety_factor, const_clump, zz, fH1_0, fHe1_0, fHe2_0, temp_0, Lx0;
+  double rkill;
+  // scalars
+  float dx0, Lx, dxc, dt, t, clight, nc;
+  float spectrum[kMaxF];
+  double nphot_min, nphot_max, nphot_base_avg;
+  float nphot_merge;
+  long num_thresh, total_rays;
+  float random_angles[kNtheta][3];
+  double sigH1[kMaxF], sigHe1[kMaxF];
+  // fields
+  std::vector<float> rho, nH, nHe, nH1, nHe1, nH2, nHe2, nHe3, ne, n_tot, f_H1, f_He1, f_H2, f_He2, f_He3, temp,
+      clump, clump_in, avg_nh1, avg_nhe1, avg_gamma, avg_gamma_he1, recomb_H2, recomb_He2, recomb_He3, recrate_H2,
+      recrate_He2, dne_dt, mfp, mfp_912, treion, treion_out, heat_rate, cool_rate, gamma_H1_tot, gamma_He1_tot,
+      nH1_prev, IF_speed, Inc_Flux, ray_dt;
+  std::vector<float> gamma_H1_nu, gamma_He1_nu, ngam_nu, u_nu, avg_gamma_nu, avg_gamma_nu_he1;
+  std::vector<unsigned char> treion_flag;
+  bool have_clump;
+  std::vector<Src> src;
+  std::vector<Ray> rays;
+  long last_crossings, last_moved;
+  int step;
+};
+
+static inline long cidx(const Ctx& c, int i, int j, int k) { return ((long)i * c.N + j) * c.N + k; }
+static inline void split_ind(const Ctx& c, int ind, int* i, int* j, int* k) {
+  const int nyz = c.N * c.N;
+  *i = (ind - imod(ind, nyz)) / nyz;
+  int jj = ind - *i * nyz;
+  *j = (jj - imod(jj, c.N)) / c.N;
+  *k = ind - *i * nyz - *j * c.N;
+}
+
+static float sum_nphot(const Ctx& c, const Ray& R) {
+  float s = 0.;
+  for (int nu = 0; nu < c.F; nu++) s += R.nphot[nu];
+  return s;
+}
+
+static float rmin_from_l(const Ctx& c, short l) {
+  float r = c.dx0 * pow(2, l - 1) * pow(3. / O_PI / c.safety_factor, 0.5);
+  if (l == 0) r = 0.;
+  return r;
+}
+static float rmax_from_l(const Ctx& c, short l) { return c.dx0 * pow(2, l) * pow(3. / O_PI / c.safety_factor, 0.5); }
+static short l_from_r(const Ctx& c, float r) {
+  short l = (short)imin((int)ceil(log(O_PI * c.safety_factor / 3. * pow(r / c.dx0, 2.)) / log(4.)), (int)c.l_max);
+  l = mins(c.l_max, maxs(c.hpx_lvl, l));
+  if (r / c.dx0 < 1.) l = c.hpx_lvl;
+  return l;
+}
+
+// forward (direction 0) and inverse (direction 6) ZYX rotation, healpix_funcs.cc:102-143
+static void rotate(float a0, float b0, float g0, int direction, double vx, double vy, double vz, double* ox,
+                   double* oy, double* oz) {
+  float xhat = (float)vx, yhat = (float)vy, zhat = (float)vz, xp, yp, zp;
+  if (direction == 0) {
+    xp = (cos(b0) * cos(g0)) * xhat + (-cos(b0) * sin(g0)) * yhat + (sin(b0)) * zhat;
+    yp = (sin(a0) * sin(b0) * cos(g0) + cos(a0) * sin(g0)) * xhat +
+         (-sin(a0) * sin(b0) * sin(g0) + cos(a0) * cos(g0)) * yhat + (-sin(a0) * cos(b0)) * zhat;
+    zp = (-cos(a0) * sin(b0) * cos(g0) + sin(a0) * sin(g0)) * xhat +
+         (cos(a0) * sin(b0) * sin(g0) + sin(a0) * cos(g0)) * yhat + (cos(a0) * cos(b0)) * zhat;
+  } else {
+    xp = (cos(g0) * cos(b0)) * xhat + (sin(g0) * cos(a0) + cos(g0) * sin(b0) * sin(a0)) * yhat +
+         (sin(g0) * sin(a0) - cos(g0) * sin(b0) * cos(a0)) * zhat;
+    yp = (-sin(g0) * cos(b0)) * xhat + (cos(g0) * cos(a0) - sin(g0) * sin(b0) * sin(a0)) * yhat +
+         (cos(g0) * sin(a0) + sin(g0) * sin(b0) * cos(a0)) * zhat;
+    zp = (sin(b0)) * xhat + (-cos(b0) * sin(a0)) * yhat + (cos(b0) * cos(a0)) * zhat;
+  }
+  *ox = xp;
+  *oy = yp;
+  *oz = zp;
+}
+
+// ---- set-up -----------------------------------------------------------------------------
+struct Params {
+  int N, F, path_length, itercount, ray_per_cell_max, hpx_lvl;
+  double nu_eV[kMaxF];
+  double spectrum_alpha[15];
+  double spectrum_table[15][kMaxF];
+  float cl_factor, box_hmpc, z, const_clump;
+  double rkill_cm;
+  unsigned int seed;
+};
+
+static void set_spectrum(Ctx& c, const Params& p) {
+  // read_spectrum_table + set_spectrum (gas_funcs.cc:11-70) with the table passed in
+  const int Nalph = 15;
+  double alpha_spec = 1.5;
+  int m = floor((alpha_spec - p.spectrum_alpha[0]) / (p.spectrum_alpha[Nalph - 1] - p.spectrum_alpha[0]) * (Nalph - 1));
+  m = imin(m, Nalph - 2);
+  int q = m + 1;
+  float spec_sum = 0.;
+  for (int nu = 0; nu < c.F; nu++) {
+    c.spectrum[nu] = (float)(p.spectrum_table[m][nu] + (p.spectrum_table[q][nu] - p.spectrum_table[m][nu]) /
+                                                           (p.spectrum_alpha[q] - p.spectrum_alpha[m]) *
+                                                           (alpha_spec - p.spectrum_alpha[m]));
+    spec_sum += c.spectrum[nu];
+  }
+  for (int nu = 0; nu < c.F; nu++) c.spectrum[nu] /= spec_sum;
+}
+
+static void alloc(Ctx& c) {
+  const size_t n3 = (size_t)c.N * c.N * c.N;
+  std::vector<float>* f[] = {&c.rho, &c.nH, &c.nHe, &c.nH1, &c.nHe1, &c.nH2, &c.nHe2, &c.nHe3, &c.ne, &c.n_tot,
+                             &c.f_H1, &c.f_He1, &c.f_H2, &c.f_He2, &c.f_He3, &c.temp, &c.clump, &c.avg_nh1,
+                             &c.avg_nhe1, &c.avg_gamma, &c.avg_gamma_he1, &c.recomb_H2, &c.recomb_He2,
+                             &c.recomb_He3, &c.recrate_H2, &c.recrate_He2, &c.dne_dt, &c.mfp, &c.mfp_912, &c.treion,
+                             &c.treion_out, &c.heat_rate, &c.cool_rate, &c.gamma_H1_tot, &c.gamma_He1_tot,
+                             &c.nH1_prev, &c.IF_speed, &c.Inc_Flux, &c.ray_dt};
+  for (auto* v : f) v->assign(n3, 0.f);
+  std::vector<float>* g[] = {&c.gamma_H1_nu, &c.gamma_He1_nu, &c.ngam_nu, &c.u_nu, &c.avg_gamma_nu,
+                             &c.avg_gamma_nu_he1};
+  for (auto* v : g) v->assign(n3 * c.F, 0.f);
+  c.treion_flag.assign(n3, 0);
+}
+
+static void init_rays(Ctx& c, int i, int j, int k, double lum);
+
+static void new_rays(Ctx& c) {
+  long created = 0;
+  for (size_t s = 0; s < c.src.size(); ++s) {
+    const Src& S = c.src[s];
+    init_rays(c, S.i, S.j, S.k, S.lum);
+    created += 12 * pow(2, 2 * c.hpx_lvl);
+    c.ray_dt[cidx(c, S.i, S.j, S.k)] = 0.;
+  }
+  c.total_rays += created;
+}
+
+static void init_rays(Ctx& c, int i, int j, int k, double lum) {
+  const long ci = cidx(c, i, j, k);
+  unsigned short itheta = (unsigned short)(rand() % kNtheta);
+  float a0 = c.random_angles[itheta][0], b0 = c.random_angles[itheta][1], g0 = c.random_angles[itheta][2];
+  int Nside;
+  short lpix;
+  if (c.nH1[ci] / c.nH[ci] > 0.1) {
+    Nside = 1;
+    lpix = 0;
+  } else {
+    Nside = (int)pow(2, c.hpx_lvl);
+    lpix = c.hpx_lvl;
+  }
+  for (int f = 0; f < 12; f++) {
+    for (int pnp = 0; pnp < pow(Nside, 2); pnp++) {
+      int pix = f * pow(Nside, 2) + pnp;
+      double vx, vy, vz;
+      hpn::pix2vec(lpix, pix, &vx, &vy, &vz);
+      rotate(a0, b0, g0, 0, vx, vy, vz, &vx, &vy, &vz);
+      Ray R;
+      memset(&R, 0, sizeof R);
+      R.alive = true;
+      R.active = true;
+      R.order = lpix;
+      R.pixel = pix;
+      R.itheta = itheta;
+      R.xhat = vx;
+      R.yhat = vy;
+      R.zhat = vz;
+      for (int nu = 0; nu < c.F; nu++)
+        R.nphot[nu] = (float)(c.spectrum[nu] * lum * c.ray_dt[ci] / 12. / pow(Nside, 2.) / kPhotNorm);
+      R.r = 0.;
+      R.dr = rmax_from_l(c, lpix) - R.r;
+      R.x = c.dxc / 2.;
+      R.y = c.dxc / 2.;
+      R.z = c.dxc / 2.;
+      R.time = 0.;
+      R.pind[0] = i * c.N * c.N + j * c.N + k;
+      c.rays.push_back(R);
+    }
+  }
+}
+
+// ---- advance (ray_tracing.cc:1222-1512), plain mode: fion = 1 everywhere ---------------------
+static void advance_ray(Ctx& c, Ray& R) {
+  float tx, ty, tz, tmin = 0;
+  int tag;
+  const float dxc = c.dxc;
+  int i, j, k;
+  split_ind(c, R.pind[0], &i, &j, &k);
+  float xhat = R.xhat, yhat = R.yhat, zhat = R.zhat;
+  float x0 = R.x, y0 = R.y, z0 = R.z;
+  R.time += c.dt;
+  float deltat = R.time;
+  float dist = c.clight * deltat;
+  const float nc = c.nc;
+  if ((x0 + dist * xhat > nc * dxc) || (y0 + dist * yhat > nc * dxc) || (z0 + dist * zhat > nc * dxc) ||
+      (x0 + dist * xhat < (1. - nc) * dxc) || (y0 + dist * yhat < (1. - nc) * dxc) ||
+      (z0 + dist * zhat < (1. - nc) * dxc)) {
+    float r0 = R.r, dr = R.dr;
+    int p = 0;
+    R.time = 0.;
+    float scale_factor = dxc / c.dx0;
+    r0 += dist / scale_factor;
+    dr -= dist / scale_factor;
+    int in = i, jn = j, kn = k;
+    float tlast = 0.;
+    while (tlast < deltat) {
+      float clgt = c.clight;
+      if (xhat > 0.) tx = (dxc - x0) / xhat / clgt;
+      else if (xhat < 0.) tx = -1. * x0 / xhat / clgt;
+      else tx = 9e99;
+      if (yhat > 0.) ty = (dxc - y0) / yhat / clgt;
+      else if (yhat < 0.) ty = -1. * y0 / yhat / clgt;
+      else ty = 9e99;
+      if (zhat > 0.) tz = (dxc - z0) / zhat / clgt;
+      else if (zhat < 0.) tz = -1. * z0 / zhat / clgt;
+      else tz = 9e99;
+      if ((tx <= ty) && (tx <= tz)) { tmin = tx; tag = 0; }
+      else if ((ty <= tx) && (ty <= tz)) { tmin = ty; tag = 1; }
+      else { tmin = tz; tag = 2; }
+      if ((tlast + tmin) < deltat) {
+        dist = tmin * clgt;
+        if (p >= c.PL) { fprintf(stderr, "oracle: path overflow\n"); abort(); }
+        R.pind[p] = in * c.N * c.N + jn * c.N + kn;
+        R.pdist[p] = dist;
+        p += 1;
+        x0 += dist * xhat;
+        y0 += dist * yhat;
+        z0 += dist * zhat;
+        if (tag == 0) {
+          if (xhat > 0.) { in = imod(in + 1, c.N); x0 = kMinDist * dxc; }
+          else { in = imod(in - 1, c.N); x0 = dxc * (1. - kMinDist); }
+        } else if (tag == 1) {
+          if (yhat > 0.) { jn = imod(jn + 1, c.N); y0 = kMinDist * dxc; }
+          else { jn = imod(jn - 1, c.N); y0 = dxc * (1. - kMinDist); }
+        } else {
+          if (zhat > 0.) { kn = imod(kn + 1, c.N); z0 = kMinDist * dxc; }
+          else { kn = imod(kn - 1, c.N); z0 = dxc * (1. - kMinDist); }
+        }
+        if (x0 <= 0.) x0 = kMinDist * dxc;
+        if (x0 >= dxc * (1. - kMinDist / 2.)) x0 = dxc * (1. - kMinDist);
+        if (y0 <= 0.) y0 = kMinDist * dxc;
+        if (y0 >= dxc * (1. - kMinDist / 2.)) y0 = dxc * (1. - kMinDist);
+        if (z0 <= 0.) z0 = kMinDist * dxc;
+        if (z0 >= dxc * (1. - kMinDist / 2.)) z0 = dxc * (1. - kMinDist);
+      }
+      tlast += tmin;
+    }
+    dist = (deltat - tlast + tmin) * c.clight;
+    dist = maxd(dist, kMinDist * dxc);
+    if (p >= c.PL) { fprintf(stderr, "oracle: path overflow\n"); abort(); }
+    R.pind[p] = in * c.N * c.N + jn * c.N + kn;
+    R.pdist[p] = dist;
+    R.ray_end = p + 1;
+    x0 += dist * xhat;
+    y0 += dist * yhat;
+    z0 += dist * zhat;
+    if (x0 <= 0.) x0 = kMinDist * dxc;
+    if (x0 >= dxc * (1. - kMinDist / 2.)) x0 = dxc * (1. - kMinDist);
+    if (y0 <= 0.) y0 = kMinDist * dxc;
+    if (y0 >= dxc * (1. - kMinDist / 2.)) y0 = dxc * (1. - kMinDist);
+    if (z0 <= 0.) z0 = kMinDist * dxc;
+    if (z0 >= dxc * (1. - kMinDist / 2.)) z0 = dxc * (1. - kMinDist);
+    R.active = false;
+    R.r = r0;
+    R.dr = dr;
+    R.x = x0;
+    R.y = y0;
+    R.z = z0;
+  }
+}
+
+static void update_rays(Ctx& c) {
+  for (const Src& S : c.src) c.ray_dt[cidx(c, S.i, S.j, S.k)] += c.dt;
+  for (Ray& R : c.rays)
+    if (R.alive) advance_ray(c, R);
+}
+
+// ---- C2Ray iteration (ray_tracing.cc:623-1216), plain mode -------------------------------
+static void find_avg_unu(Ctx& c) {
+  const long n3 = (long)c.N * c.N * c.N;
+  const int F = c.F;
+  const double vol = ((double)c.dxc) * ((double)c.dxc) * ((double)c.dxc);
+  for (int iter = 0; iter < c.itercount; iter++) {
+    for (long q = 0; q < n3; q++) {
+      c.avg_gamma[q] = 0.;
+      c.avg_gamma_he1[q] = 0.;
+      c.IF_speed[q] = 0.;
+      c.Inc_Flux[q] = 0.;
+      for (int nu = 0; nu < F; nu++) {
+        c.ngam_nu[q * F + nu] = 0.;
+        c.avg_gamma_nu[q * F + nu] = 0.;
+        c.avg_gamma_nu_he1[q * F + nu] = 0.;
+        c.u_nu[q * F + nu] = 0.;
+      }
+      if (iter == 0) {
+        c.avg_nh1[q] = c.nH1[q];
+        c.avg_nhe1[q] = c.nHe1[q];
+        c.recomb_H2[q] = (float)alphaB_H2(maxd(kTempMin, c.temp[q]));
+        c.recomb_He2[q] = (float)alphaB_He2(maxd(kTempMin, c.temp[q]));
+        c.recomb_He3[q] = (float)alphaB_He3(maxd(kTempMin, c.temp[q]));
+        if ((c.temp[q] >= 3e4) && (c.temp[q] <= 1e6)) c.recomb_He2[q] += (float)Dalpha_He2(maxd(kTempMin, c.temp[q]));
+        c.dne_dt[q] = -c.ne[q];
+        c.mfp[q] = 1. / c.nH1[q] / c.sigH1[0];
+      }
+    }
+    // ray pass
+    for (Ray& R : c.rays) {
+      if (!(R.alive && !R.active)) continue;
+      double nphot[kMaxF], tau_h1[kMaxF], dtau_h1[kMaxF], tau_he1[kMaxF], dtau_he1[kMaxF];
+      for (int nu = 0; nu < F; nu++) {
+        nphot[nu] = R.nphot[nu] * kPhotNorm;
+        tau_h1[nu] = 0.;
+        dtau_h1[nu] = 0.;
+        tau_he1[nu] = 0.;
+        dtau_he1[nu] = 0.;
+      }
+      short p = 0;
+      while (p < R.ray_end) {
+        const int ind = R.pind[p];
+        const long q = ind;
+        for (int nu = 0; nu < F; nu++) {
+          dtau_h1[nu] = c.avg_nh1[q] * c.sigH1[nu] * R.pdist[p];
+          dtau_he1[nu] = c.avg_nhe1[q] * c.sigHe1[nu] * R.pdist[p];
+        }
+        double nphot_in[kMaxF];
+        double nphot_in_total = 0.;
+        for (int nu = 0; nu < F; nu++) {
+          nphot_in[nu] = nphot[nu] * exp(-tau_h1[nu] - tau_he1[nu]);
+          nphot_in_total += nphot_in[nu] / kPhotNorm;
+        }
+        double frac_h1[kMaxF], frac_he1[kMaxF];
+        for (int nu = 0; nu < F; nu++) {
+          if ((dtau_h1[nu] > 0.) || (dtau_he1[nu] > 0.)) {
+            frac_h1[nu] = (1. - exp(-dtau_h1[nu])) * exp(-dtau_he1[nu]) /
+                          ((1. - exp(-dtau_h1[nu])) * exp(-dtau_he1[nu]) + (1. - exp(-dtau_he1[nu])) * exp(-dtau_h1[nu]));
+            frac_he1[nu] = (1. - exp(-dtau_he1[nu])) * exp(-dtau_h1[nu]) /
+                           ((1. - exp(-dtau_h1[nu])) * exp(-dtau_he1[nu]) + (1. - exp(-dtau_he1[nu])) * exp(-dtau_h1[nu]));
+          } else {
+            frac_h1[nu] = 0.;
+            frac_he1[nu] = 0.;
+          }
+        }
+        if (nphot_in_total < c.nphot_min) {
+          for (int nu = 0; nu < F; nu++) {
+            c.ngam_nu[q * F + nu] += (float)(nphot_in[nu] / kPhotNorm);
+            c.avg_gamma_nu[q * F + nu] += (float)(frac_h1[nu] * nphot_in[nu] / c.dt / vol / c.avg_nh1[q]);
+            c.avg_gamma[q] += (float)(frac_h1[nu] * nphot_in[nu] / c.dt / vol / c.avg_nh1[q]);
+            c.avg_gamma_nu_he1[q * F + nu] += (float)(frac_he1[nu] * nphot_in[nu] / c.dt / vol / c.avg_nhe1[q]);
+            c.avg_gamma_he1[q] += (float)(frac_he1[nu] * nphot_in[nu] / c.dt / vol / c.avg_nhe1[q]);
+          }
+          p = 99;
+        } else {
+          for (int nu = 0; nu < F; nu++) {
+            c.ngam_nu[q * F + nu] += (float)(nphot_in[nu] / kPhotNorm);
+            c.avg_gamma_nu[q * F + nu] +=
+                (float)(frac_h1[nu] * nphot_in[nu] * (1. - exp(-dtau_h1[nu] - dtau_he1[nu])) / c.dt / vol / c.avg_nh1[q]);
+            c.avg_gamma[q] +=
+                (float)(frac_h1[nu] * nphot_in[nu] * (1. - exp(-dtau_h1[nu] - dtau_he1[nu])) / c.dt / vol / c.avg_nh1[q]);
+            c.avg_gamma_nu_he1[q * F + nu] += (float)(frac_he1[nu] * nphot_in[nu] *
+                                                      (1. - exp(-dtau_h1[nu] - dtau_he1[nu])) / c.dt / vol / c.avg_nhe1[q]);
+            c.avg_gamma_he1[q] += (float)(frac_he1[nu] * nphot_in[nu] * (1. - exp(-dtau_h1[nu] - dtau_he1[nu])) /
+                                          c.dt / vol / c.avg_nhe1[q]);
+          }
+          p += 1;
+        }
+        for (int nu = 0; nu < F; nu++) {
+          tau_h1[nu] += dtau_h1[nu];
+          tau_he1[nu] += dtau_he1[nu];
+        }
+      }
+      if (iter == c.itercount - 1) {
+        for (int nu = 0; nu < F; nu++) R.nphot[nu] = (float)(nphot[nu] * exp(-tau_h1[nu] - tau_he1[nu]) / kPhotNorm);
+        if (sum_nphot(c, R) > c.nphot_min) {
+          R.active = true;
+          R.pind[0] = R.pind[R.ray_end - 1];
+        } else {
+          R.alive = false;
+          R.active = false;
+        }
+      }
+    }
+    // cell pass B
+    for (long q = 0; q < n3; q++) {
+      double nelec = (double)(c.nH[q] - c.avg_nh1[q] + c.nHe[q] - c.avg_nhe1[q]);
+      c.mfp[q] = 1. / c.sigH1[0] / c.avg_nh1[q];
+      c.mfp_912[q] = 1. / sig_H1(13.6 / O_H_EV) / c.avg_nh1[q];
+      double col = 0.;
+      double x0 = (double)(1. - c.f_H1[q]);
+      double pr = (double)c.avg_gamma[q] + col + c.clump[q] * c.recomb_H2[q] * nelec;
+      double xeq = (c.avg_gamma[q] + col) / pr;
+      double ti = 1. / pr;
+      c.avg_nh1[q] = (float)(c.nH[q] * (1. - (xeq + ti / c.dt * (x0 - xeq) * (1. - exp(-c.dt / ti)))));
+      double x0_he = (double)(1. - c.f_He1[q]);
+      double pr_he = (double)c.avg_gamma_he1[q] + c.clump[q] * c.recomb_He2[q] * nelec;
+      double xeq_he = c.avg_gamma_he1[q] / pr_he;
+      double ti_he = 1. / pr_he;
+      c.avg_nhe1[q] = (float)(c.nHe[q] * (1. - (xeq_he + ti_he / c.dt * (x0_he - xeq_he) * (1. - exp(-c.dt / ti_he)))));
+      if (iter == c.itercount - 1) {
+        c.nH1[q] = (float)c.nH[q] * (1. - (xeq + (x0 - xeq) * exp(-c.dt / ti)));
+        c.nH2[q] = (float)c.nH[q] - c.nH1[q];
+        c.nHe1[q] = (float)c.nHe[q] * (1. - (xeq_he + (x0_he - xeq_he) * exp(-c.dt / ti_he)));
+        c.nHe2[q] = (float)c.nHe[q] - c.nHe1[q];
+        c.nHe3[q] = 0.;
+        if ((c.avg_nh1[q] / c.nH[q] < 0.5) && (c.treion_flag[q] == 0)) {
+          c.treion[q] = c.t;
+          c.treion_out[q] = c.t;
+          c.treion_flag[q] = 1;
+        }
+        for (int nu = 0; nu < F; nu++)
+          c.u_nu[q * F + nu] = (float)(c.spectrum[nu] * c.avg_gamma[q] / c.sigH1[nu]) * O_H * (c.nu[nu]) / c.clight;
+        for (int nu = 0; nu < F; nu++) {
+          c.gamma_H1_nu[q * F + nu] = c.avg_gamma_nu[q * F + nu];
+          c.gamma_He1_nu[q * F + nu] = c.avg_gamma_nu_he1[q * F + nu];
+        }
+        c.gamma_H1_tot[q] = c.avg_gamma[q];
+        c.gamma_He1_tot[q] = c.avg_gamma_he1[q];
+        c.recrate_H2[q] = c.clump[q] * c.recomb_H2[q] * nelec * c.nH2[q];
+        c.recrate_He2[q] = c.clump[q] * c.recomb_He2[q] * nelec * c.nHe2[q];
+        c.ne[q] = c.nH2[q] + c.nHe2[q] + 2. * c.nHe3[q];
+        c.dne_dt[q] += c.ne[q];
+        c.n_tot[q] = c.nH[q] + c.nHe[q] + c.ne[q];
+        c.dne_dt[q] /= c.dt;
+        c.f_H2[q] = c.nH2[q] / c.nH[q];
+        c.f_He2[q] = c.nHe2[q] / c.nHe[q];
+        c.f_He3[q] = c.nHe3[q] / c.nHe[q];
+        c.f_H1[q] = c.nH1[q] / c.nH[q];
+        c.f_He1[q] = c.nHe1[q] / c.nHe[q];
+      }
+    }
+  }
+}
+
+// ---- merge machinery (ray_tracing.cc:35-227, 324-477) -------------------------------------
+static long count_rays(const Ctx& c) {
+  long n = 0;
+  for (const Ray& R : c.rays) n += R.alive ? 1 : 0;
+  return n;
+}
+
+static void calc_nphot_merge(Ctx& c) {
+  double lg_max = log10(c.nphot_max);
+  double lg_min = log10(c.nphot_min);
+  double del = (lg_max - lg_min) / (10000 - 1);
+  static int pdf[10000];
+  memset(pdf, 0, sizeof pdf);
+  long ray_cum = 0;
+  c.nphot_merge = 0.;
+  for (const Ray& R : c.rays) {
+    if (!R.alive) continue;
+    int pdf_ind = (int)maxd((log10(sum_nphot(c, R)) - lg_min) / del, 0.);
+    pdf_ind = imin(pdf_ind, 9999);
+    pdf[pdf_ind] += 1;
+  }
+  int pi_ = 9999;
+  while (pi_ >= 0) {
+    ray_cum += pdf[pi_];
+    if (ray_cum >= c.num_thresh) {
+      c.nphot_merge = pow(10., pi_ * del + lg_min);
+      pi_ = -1;
+    } else {
+      pi_ -= 1;
+    }
+  }
+}
+
+static void merge(Ctx& c) {
+  unsigned short itheta = (unsigned short)(rand() % kNtheta);
+  float a0 = c.random_angles[itheta][0], b0 = c.random_angles[itheta][1], g0 = c.random_angles[itheta][2];
+  const int lm = c.hpx_lvl;
+  const int npix = 12 * (1 << (2 * lm));
+  const long n3 = (long)c.N * c.N * c.N;
+  std::vector<long> base((size_t)n3 * npix, -1);
+  std::vector<unsigned char> flag((size_t)n3 * npix, 0);
+  for (size_t xi = 0; xi < c.rays.size(); ++xi) {
+    Ray& R = c.rays[xi];
+    if (!(R.alive && R.active)) continue;
+    if (!(sum_nphot(c, R) < c.nphot_merge)) continue;
+    const long q = R.pind[0];
+    double vx = R.xhat, vy = R.yhat, vz = R.zhat;
+    rotate(a0, b0, g0, 6, vx, vy, vz, &vx, &vy, &vz);
+    const int pixel = hpn::vec2pix(lm, vx, vy, vz);
+    const size_t b = (size_t)q * npix + pixel;
+    if (base[b] == -1) {
+      base[b] = (long)xi;
+      flag[b] = 0;
+      float nt = sum_nphot(c, R);
+      R.r /= c.dx0;
+      R.r = pow(R.r, 2.) * nt;
+      R.dr *= nt;
+      R.x *= nt;
+      R.y *= nt;
+      R.z *= nt;
+      R.time *= nt;
+    } else {
+      Ray& M = c.rays[base[b]];
+      float nt = sum_nphot(c, R);
+      for (int nu = 0; nu < c.F; nu++) M.nphot[nu] += R.nphot[nu];
+      R.r /= c.dx0;
+      M.r += pow(R.r, 2.) * nt;
+      M.dr += R.dr * nt;
+      M.x += R.x * nt;
+      M.y += R.y * nt;
+      M.z += R.z * nt;
+      M.time += R.time * nt;
+      flag[b] = 1;
+      R.alive = false;
+      R.active = false;
+    }
+  }
+  for (long q = 0; q < n3; q++) {
+    for (int pix = 0; pix < npix; pix++) {
+      const size_t b = (size_t)q * npix + pix;
+      if (base[b] == -1) continue;
+      Ray& R = c.rays[base[b]];
+      float nt = sum_nphot(c, R);
+      R.r /= nt;
+      R.r = pow(R.r, 0.5);
+      R.r *= c.dx0;
+      R.dr /= nt;
+      R.x /= nt;
+      R.y /= nt;
+      R.z /= nt;
+      R.time /= nt;
+      if (flag[b]) {
+        double vx, vy, vz;
+        hpn::pix2vec(lm, pix, &vx, &vy, &vz);
+        R.itheta = itheta;
+        R.order = mins(c.l_max, l_from_r(c, R.r));
+        float rmin = rmin_from_l(c, R.order);
+        float rmax = rmax_from_l(c, R.order);
+        R.r = maxd(rmax - R.dr, rmin);
+        R.dr = rmax - R.r;
+        R.pixel = hpn::vec2pix(R.order, vx, vy, vz);
+        hpn::pix2vec(R.order, R.pixel, &vx, &vy, &vz);
+        rotate(a0, b0, g0, 0, vx, vy, vz, &vx, &vy, &vz);
+        R.xhat = vx;
+        R.yhat = vy;
+        R.zhat = vz;
+      }
+    }
+  }
+}
+
+// ---- split (rt_funcs.cc:211-237, ray_tracing.cc:482-619) -----------------------------------
+static void split_rays(Ctx& c) {
+  const size_t n0 = c.rays.size();
+  for (size_t xi = 0; xi < n0; ++xi) {
+    if (!(c.rays[xi].alive && c.rays[xi].active)) continue;
+    const Ray P = c.rays[xi];
+    short l = P.order;
+    float r = P.r;
+    if (!((r > rmax_from_l(c, l)) && (l < c.l_max) && (sum_nphot(c, P) > maxd(4. * c.nphot_merge, 4. * c.nphot_min))))
+      continue;
+    int ic, jc, kc;
+    split_ind(c, P.pind[0], &ic, &jc, &kc);
+    float r0 = P.r, x0_old = P.x, y0_old = P.y, z0_old = P.z, time = P.time;
+    unsigned short itheta = P.itheta;
+    float a0 = c.random_angles[itheta][0], b0 = c.random_angles[itheta][1], g0 = c.random_angles[itheta][2];
+    float nph[kMaxF];
+    for (int nu = 0; nu < c.F; nu++) nph[nu] = P.nphot[nu] / 4.;
+    const double vox = P.xhat, voy = P.yhat, voz = P.zhat;
+    c.rays[xi].alive = false;
+    c.rays[xi].active = false;
+    for (int n = 0; n < 4; n++) {
+      int icn = ic, jcn = jc, kcn = kc;
+      int pix = 4 * P.pixel + n;
+      double vx, vy, vz;
+      hpn::pix2vec(l + 1, pix, &vx, &vy, &vz);
+      rotate(a0, b0, g0, 0, vx, vy, vz, &vx, &vy, &vz);
+      double dxv = vx - vox, dyv = vy - voy, dzv = vz - voz;
+      float scale_factor = c.dxc / c.dx0;
+      float x0 = x0_old + dxv * (r0 * scale_factor);
+      float y0 = y0_old + dyv * (r0 * scale_factor);
+      float z0 = z0_old + dzv * (r0 * scale_factor);
+      while (x0 > c.dxc) { x0 -= c.dxc; icn = imod(icn + 1, c.N); }
+      while (x0 < 0.) { x0 += c.dxc; icn = imod(icn - 1, c.N); }
+      while (y0 > c.dxc) { y0 -= c.dxc; jcn = imod(jcn + 1, c.N); }
+      while (y0 < 0.) { y0 += c.dxc; jcn = imod(jcn - 1, c.N); }
+      while (z0 > c.dxc) { z0 -= c.dxc; kcn = imod(kcn + 1, c.N); }
+      while (z0 < 0.) { z0 += c.dxc; kcn = imod(kcn - 1, c.N); }
+      Ray Ch;
+      memset(&Ch, 0, sizeof Ch);
+      Ch.alive = true;
+      Ch.active = false;
+      float rmax = rmax_from_l(c, l + 1);
+      Ch.order = l + 1;
+      Ch.pixel = pix;
+      Ch.itheta = itheta;
+      Ch.xhat = vx;
+      Ch.yhat = vy;
+      Ch.zhat = vz;
+      for (int nu = 0; nu < c.F; nu++) Ch.nphot[nu] = nph[nu];
+      Ch.r = r0;
+      Ch.dr = rmax - r0;
+      Ch.x = x0;
+      Ch.y = y0;
+      Ch.z = z0;
+      Ch.time = time;
+      Ch.pind[0] = icn * c.N * c.N + jcn * c.N + kcn;
+      c.rays.push_back(Ch);
+    }
+  }
+  for (Ray& R : c.rays)
+    if (R.alive && !R.active) R.active = true;
+}
+
+// ---- thermal (gas_funcs.cc:104-242, 353-457), plain mode ------------------------------------
+static void set_Treion_default(Ctx& c, long q) {
+  float fion_new = (c.nH[q] - c.nH1[q]) / c.nH[q];
+  float fion_old = (c.nH[q] - c.nH1_prev[q]) / c.nH[q];
+  float deltax = c.dxc * (fion_new - fion_old);
+  float vIF = deltax / c.dt;
+  float Cn[5] = {9.5432, -1.6441e-2, -9.8010e-3, 4.1664e-3, -2.2710e-4};
+  float lnTreion = 0.;
+  for (int t = 0; t < 5; t++) lnTreion += Cn[t] * pow(log(vIF / 1e5), t);
+  if ((fion_new > fion_old) && (fion_new < 0.98)) {
+    c.temp[q] = (fion_old * c.temp[q] + (fion_new - fion_old) * exp(lnTreion)) / fion_new;
+  }
+  c.IF_speed[q] = maxd(0., vIF);
+  c.Inc_Flux[q] = (1. + kNheToNh) * c.nH[q] * maxd(0., vIF);
+}
+
+static void update_heat_cool(Ctx& c, long q) {
+  const int F = c.F;
+  c.heat_rate[q] = 0;
+  c.cool_rate[q] = 0;
+  if (c.f_H2[q] > 0.98) {
+    for (int nu = 0; nu < F; nu++) {
+      c.heat_rate[q] += c.avg_nh1[q] * c.gamma_H1_nu[q * F + nu] * O_H * (O_H_EV * c.nu[nu] - 13.6) / O_H_EV;
+      c.heat_rate[q] += c.avg_nhe1[q] * c.gamma_He1_nu[q * F + nu] * O_H * (O_H_EV * c.nu[nu] - 2.459e+1) / O_H_EV;
+    }
+  } else {
+    c.heat_rate[q] = 0.;
+  }
+  c.cool_rate[q] += rcrB_H2(maxd(kTempMin, c.temp[q])) * c.ne[q] * c.nH2[q];
+  c.cool_rate[q] += rcrB_He2(maxd(kTempMin, c.temp[q])) * c.ne[q] * c.nHe2[q];
+  float nff = c.nH2[q] + c.nHe2[q] + 4. * c.nHe3[q];
+  c.cool_rate[q] += free_free_rate(maxd(kTempMin, c.temp[q])) * c.ne[q] * nff;
+  c.cool_rate[q] -= compton_rate(c.zz) * c.ne[q] * (2.726 * (1 + c.zz) - maxd(kTempMin, c.temp[q]));
+}
+
+static float get_thermal_tstep(Ctx& c, long q) {
+  float dT_dt = 2. / 3. / O_KB / c.n_tot[q] * (c.heat_rate[q] - c.cool_rate[q]) -
+                (2. * hubble(1. / (1. + c.zz)) + c.dne_dt[q] / c.n_tot[q]) * c.temp[q];
+  float min_dt = 0.1 * c.dt;
+  return maxd(min_dt, mind(0.1 * c.temp[q] / absd(dT_dt), c.dt));
+}
+
+static void update_thermal(Ctx& c) {
+  const long n3 = (long)c.N * c.N * c.N;
+  for (long q = 0; q < n3; q++) {
+    float t_temp = 0.;
+    set_Treion_default(c, q);
+    while (t_temp < c.dt) {
+      float dt_temp = mind(get_thermal_tstep(c, q), c.dt - t_temp);
+      update_heat_cool(c, q);
+      c.temp[q] = (c.temp[q] + 2. / 3. / O_KB / c.n_tot[q] * (c.heat_rate[q] - c.cool_rate[q]) * dt_temp) /
+                  (1. + 2. * hubble(1. / (1. + c.zz)) * dt_temp + 1. / c.n_tot[q] * c.dne_dt[q] * dt_temp);
+      t_temp += dt_temp;
+    }
+    c.temp[q] = maxd(c.temp[q], kTempMin);
+    c.nH1_prev[q] = c.nH1[q];
+  }
+}
+
+static void compact(Ctx& c) {
+  size_t w = 0;
+  for (size_t r = 0; r < c.rays.size(); ++r)
+    if (c.rays[r].alive) c.rays[w++] = c.rays[r];
+  c.rays.resize(w);
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+extern "C" {
+
+// Create a box from proper-density-free inputs: delta1 is 1+delta on N^3 (float32, C order),
+// sources are pre-gridded (i,j,k,lum) in (i,j,k) order, clump may be NULL (C = const_clump).
+void* orc_create(const Params* p, const float* delta1, int nsrc, const int32_t* src_ijk, const double* src_lum,
+                 const float* clump) {
+  Ctx* c = new Ctx();
+  c->N = p->N;
+  c->F = p->F;
+  c->PL = p->path_length;
+  c->itercount = p->itercount;
+  c->ray_per_cell_max = p->ray_per_cell_max;
+  c->hpx_lvl = p->hpx_lvl;
+  c->l_max = 12;
+  for (int nu = 0; nu < c->F; nu++) c->nu[nu] = p->nu_eV[nu] / O_H_EV;
+  c->cl_factor = p->cl_factor;
+  c->tstep_factor = 1.0f;
+  c->nl_const = 0.5f;
+  c->safety_factor = 3.f;
+  c->const_clump = p->const_clump;
+  c->zz = p->z;
+  c->fH1_0 = 1. - 1.2e-3;
+  c->fHe1_0 = 1. - 1.2e-3;
+  c->fHe2_0 = 1.2e-3;
+  c->temp_0 = 1e4;
+  c->rkill = p->rkill_cm;
+  c->Lx0 = p->box_hmpc * 1e3 / O_HH;
+  c->dx0 = c->Lx0 / c->N * O_KPC_TO_CM;
+  for (int nu = 0; nu < c->F; nu++) {
+    c->sigH1[nu] = sig_H1(c->nu[nu]);
+    c->sigHe1[nu] = sig_He1(c->nu[nu]);
+  }
+  srand(p->seed);
+  alloc(*c);
+  const long n3 = (long)c->N * c->N * c->N;
+  // first-snapshot set-up at a = 1/(1+z) (gas_funcs.cc:595-613, io_funcs.cc:33-62)
+  const float a_snap = (float)(1. / (1. + c->zz));
+  c->Lx = c->Lx0 * a_snap;
+  {
+    float rho_c_cgs = 1.87890e-29, ob = 0.0482266, h0 = 0.68;
+    double rho_unit = rho_c_cgs * ob * pow(h0, 2.);
+    for (long q = 0; q < n3; q++) {
+      c->rho[q] = delta1[q];
+      c->rho[q] *= (float)rho_unit;
+    }
+    for (long q = 0; q < n3; q++) c->rho[q] *= pow(a_snap, -3.);
+  }
+  for (int s = 0; s < nsrc; s++) c->src.push_back({src_ijk[3 * s], src_ijk[3 * s + 1], src_ijk[3 * s + 2], src_lum[s]});
+  for (int i = 0; i < kNalpha; i++)
+    for (int j = 0; j < kNalpha; j++)
+      for (int k = 0; k < kNalpha; k++) {
+        int ind = i * pow(kNalpha, 2) + j * kNalpha + k;
+        c->random_angles[ind][0] = 2. * O_PI / kNalpha * i;
+        c->random_angles[ind][1] = 2. * O_PI / kNalpha * j;
+        c->random_angles[ind][2] = 2. * O_PI / kNalpha * k;
+      }
+  // init() (init_funcs.cc:10-142), input_grid = FALSE; fion is still 0 here
+  c->dxc = c->Lx / c->N * O_KPC_TO_CM;
+  for (long q = 0; q < n3; q++) {
+    c->f_H1[q] = c->fH1_0;
+    c->f_H2[q] = 1. - c->f_H1[q];
+    c->f_He1[q] = c->fHe1_0;
+    c->f_He2[q] = c->fHe2_0;
+    c->f_He3[q] = 1. - c->f_He1[q] - c->f_He2[q];
+    c->temp[q] = c->temp_0;
+    c->nH[q] = (1. - O_Y) * c->rho[q] / O_MH;
+    c->nHe[q] = O_Y * c->rho[q] / (4. * O_MH);
+    c->nH2[q] = c->nH[q] * (1. - c->fH1_0);
+    c->nHe2[q] = c->nHe[q] * (1. - c->fHe1_0);
+    c->nHe3[q] = 0.;
+    c->nH1[q] = c->nH[q] - c->nH2[q];
+    c->avg_nh1[q] = c->nH1[q];
+    c->nHe1[q] = c->nHe[q] - c->nHe2[q] - c->nHe3[q];
+    c->avg_nhe1[q] = c->nHe1[q];
+    c->ne[q] = c->nH2[q] + c->nHe2[q] + 2. * c->nHe3[q];
+    c->n_tot[q] = c->nH[q] + c->nHe[q] + c->ne[q];
+    c->nH1_prev[q] = c->nH1[q];
+    c->recomb_H2[q] = alphaB_H2(c->temp[q]);
+    c->recomb_He2[q] = alphaB_He2(c->temp[q]);
+    c->recomb_He3[q] = alphaB_He3(c->temp[q]);
+    c->treion[q] = 0.;
+    c->treion_out[q] = 0.;
+    c->mfp[q] = 1. / c->sigH1[0] / c->avg_nh1[q];
+    c->mfp_912[q] = 1. / sig_H1(13.6 / O_H_EV) / c->avg_nh1[q];
+    float dnH2_dt = c->gamma_H1_tot[q] * c->nH1[q] - c->recomb_H2[q] * c->ne[q] * c->nH2[q];
+    float dnHe2_dt = c->nHe1[q] * c->gamma_He1_tot[q] - c->recomb_He2[q] * c->ne[q] * c->nHe2[q] +
+                     c->recomb_He3[q] * c->ne[q] * c->nHe3[q] - c->nHe2[q] * 0.f;
+    float dnHe3_dt = c->nHe2[q] * 0.f - c->recomb_He3[q] * c->ne[q] * c->nHe3[q];
+    c->dne_dt[q] = dnH2_dt + dnHe2_dt + 2 * dnHe3_dt;
+  }
+  // update_dt (rt_funcs.cc:9-12)
+  c->dt = c->tstep_factor * c->dxc / c->cl_factor / O_CL;
+  set_spectrum(*c, *p);
+  // init_rt (rt_funcs.cc:36-126): fion = 1 (ifront FALSE); ray_dt of source cells = dt
+  for (const Src& S : c->src)
+    if (S.lum != 0) c->ray_dt[cidx(*c, S.i, S.j, S.k)] = c->dt;
+  c->have_clump = clump != nullptr;
+  if (clump) {
+    c->clump_in.assign(clump, clump + n3);
+    c->clump = c->clump_in;  // the driver's set-up hook writes the field once before the loop
+  }
+  c->total_rays = 0;
+  c->t = 0.;
+  c->nphot_merge = 0.;
+  c->step = 0;
+  new_rays(*c);
+  // get_nphot_min_max (ray_tracing.cc:129-154)
+  {
+    int counter = 0;
+    c->nphot_base_avg = 0.;
+    for (const Src& S : c->src) {
+      if (S.lum > 0.) {
+        double tmp = 0.;
+        for (int nu = 0; nu < c->F; nu++)
+          tmp += c->spectrum[nu] * S.lum * c->dt / 12. / pow(2., 2. * c->hpx_lvl) / kPhotNorm;
+        c->nphot_base_avg += (double)log10(tmp);
+        counter += 1;
+      }
+    }
+    c->nphot_base_avg /= counter;
+    c->nphot_base_avg = pow(10., c->nphot_base_avg);
+    c->nphot_max = 1e3 * c->nphot_base_avg;
+    c->nphot_min = 1e-10 * c->nphot_base_avg;
+  }
+  c->last_crossings = 0;
+  c->last_moved = 0;
+  return c;
+}
+
+// One RT step in the order of main.cc:108-264 (plain mode, fixed redshift).
+void orc_step(void* h) {
+  Ctx& c = *(Ctx*)h;
+  c.step += 1;
+  const long n3 = (long)c.N * c.N * c.N;
+  for (long q = 0; q < n3; q++) c.clump[q] = c.const_clump;
+  if (c.have_clump) c.clump = c.clump_in;
+  c.clight = c.cl_factor * O_CL;
+  c.nc = c.nl_const;
+  c.t += c.dt;
+  update_rays(c);
+  c.last_crossings = 0;
+  c.last_moved = 0;
+  for (const Ray& R : c.rays)
+    if (R.alive && !R.active) {
+      c.last_crossings += R.ray_end;
+      c.last_moved += 1;
+    }
+  if (c.rkill > 0.0)
+    for (Ray& R : c.rays)
+      if (R.alive && (double)R.r > c.rkill) { R.alive = false; R.active = false; }
+  find_avg_unu(c);
+  c.num_thresh = 0;
+  for (long q = 0; q < n3; q++) c.num_thresh += (long)(c.ray_per_cell_max - 12 * pow(2, 2 * c.hpx_lvl));
+  long count = count_rays(c);
+  if (count > c.num_thresh) calc_nphot_merge(c);
+  merge(c);
+  compact(c);
+  split_rays(c);
+  compact(c);
+  update_thermal(c);
+  new_rays(c);
+  c.dt = c.tstep_factor * c.dxc / c.cl_factor / O_CL;
+}
+
+long orc_num_rays(void* h) { return count_rays(*(Ctx*)h); }
+long orc_last_crossings(void* h) { return ((Ctx*)h)->last_crossings; }
+
+void orc_scalars(void* h, double* out16) {
+  Ctx& c = *(Ctx*)h;
+  double sc[16] = {(double)c.t, (double)c.dt, c.nphot_min, c.nphot_max, (double)c.nphot_merge, (double)c.num_thresh,
+                   (double)c.total_rays, (double)c.dx0, (double)c.dxc, (double)c.step, (double)c.last_crossings,
+                   (double)c.last_moved, c.nphot_base_avg, 0.0, (double)c.src.size(), 1.0};
+  memcpy(out16, sc, sizeof sc);
+}
+
+int orc_dump(void* h, const char* path) {
+  Ctx& c = *(Ctx*)h;
+  struct frtd_writer w;
+  if (frtd_open(&w, path) != 0) return -1;
+  const int64_t n3 = (int64_t)c.N * c.N * c.N;
+  const int64_t nf[2] = {n3, c.F};
+#define DF(name) frtd_add1(&w, #name, FRTD_F32, n3, c.name.data())
+#define DFN(name) frtd_add(&w, #name, FRTD_F32, 2, nf, c.name.data())
+  DF(rho); DF(nH); DF(nHe); DF(nH1); DF(nHe1); DF(nH2); DF(nHe2); DF(nHe3); DF(ne); DF(n_tot);
+  DF(f_H1); DF(f_He1); DF(f_H2); DF(f_He2); DF(f_He3); DF(temp); DF(clump); DF(avg_nh1); DF(avg_nhe1);
+  DF(gamma_H1_tot); DF(gamma_He1_tot); DF(heat_rate); DF(cool_rate); DF(recomb_H2); DF(recomb_He2);
+  DF(recomb_He3); DF(recrate_H2); DF(recrate_He2); DF(dne_dt); DF(mfp); DF(mfp_912); DF(treion);
+  DF(treion_out); DF(IF_speed); DF(Inc_Flux); DF(avg_gamma); DF(avg_gamma_he1); DF(nH1_prev);
+  DFN(gamma_H1_nu); DFN(gamma_He1_nu); DFN(ngam_nu); DFN(u_nu); DFN(avg_gamma_nu); DFN(avg_gamma_nu_he1);
+#undef DF
+#undef DFN
+  frtd_add1(&w, "treion_flag", FRTD_U8, n3, c.treion_flag.data());
+  double sc[16];
+  orc_scalars(h, sc);
+  frtd_add1(&w, "scalars", FRTD_F64, 16, sc);
+  frtd_add1(&w, "spectrum", FRTD_F32, c.F, c.spectrum);
+  std::vector<const Ray*> live;
+  for (const Ray& R : c.rays)
+    if (R.alive) live.push_back(&R);
+  const int64_t nr = (int64_t)live.size();
+  std::vector<int64_t> slot(nr);
+  std::vector<uint8_t> act(nr);
+  std::vector<int16_t> ord(nr), rend(nr);
+  std::vector<int32_t> pix(nr), cell(nr);
+  std::vector<uint16_t> ith(nr);
+  std::vector<float> g9(nr * 9), np(nr * c.F);
+  for (int64_t q = 0; q < nr; ++q) {
+    const Ray& R = *live[q];
+    slot[q] = q;
+    act[q] = R.active;
+    ord[q] = R.order;
+    pix[q] = R.pixel;
+    ith[q] = R.itheta;
+    cell[q] = R.pind[0];
+    rend[q] = R.ray_end;
+    const float v[9] = {R.xhat, R.yhat, R.zhat, R.r, R.dr, R.x, R.y, R.z, R.time};
+    for (int k = 0; k < 9; ++k) g9[q * 9 + k] = v[k];
+    for (int nu = 0; nu < c.F; ++nu) np[q * c.F + nu] = R.nphot[nu];
+  }
+  frtd_add1(&w, "ray_slot", FRTD_I64, nr, slot.data());
+  frtd_add1(&w, "ray_active", FRTD_U8, nr, act.data());
+  frtd_add1(&w, "ray_order", FRTD_I16, nr, ord.data());
+  frtd_add1(&w, "ray_pixel", FRTD_I32, nr, pix.data());
+  frtd_add1(&w, "ray_itheta", FRTD_U16, nr, ith.data());
+  frtd_add1(&w, "ray_cell", FRTD_I32, nr, cell.data());
+  frtd_add1(&w, "ray_end", FRTD_I16, nr, rend.data());
+  const int64_t d9[2] = {nr, 9};
+  frtd_add(&w, "ray_geom", FRTD_F32, 2, d9, g9.data());
+  const int64_t dnf[2] = {nr, c.F};
+  frtd_add(&w, "ray_nphot", FRTD_F32, 2, dnf, np.data());
+  frtd_close(&w);
+  return 0;
+}
+
+void orc_destroy(void* h) { delete (Ctx*)h; }
+
+}  // extern "C"

@@ -1,0 +1,140 @@
+"""ORACLE TEST INFRASTRUCTURE -- not part of the product.
+
+ctypes front end of the CPU restatement in oracle/frt_oracle.cc, plus the build recipe for it.
+Only the tests, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module, and only
+as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import sys
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(BUILD, "liboracle.so")
+
+sys.path.insert(0, REPO)
+from flexrt_imaging_reion_b200 import workloads as W  # noqa: E402
+
+# The alpha = 1.5 interpolation of the reference's 5-bin spectrum table (set_spectrum,
+# gas_funcs.cc:44-70) lands on index floor(2/3.5*14) = 8, i.e. it interpolates between the rows
+# alpha = 1.5 and 1.75 at weight 0 (input_files/spectrum_tables_5bins.txt lines 10-11). Only the
+# alpha column and those two rows enter the arithmetic.
+SPEC_ALPHA = [-0.5 + 0.25 * i for i in range(15)]
+SPEC_ROWS = {8: [0.2, 0.2, 0.2, 0.2, 0.2], 9: [0.221, 0.213, 0.203, 0.191, 0.172]}
+
+
+class Params(C.Structure):
+    _fields_ = [("N", C.c_int), ("F", C.c_int), ("path_length", C.c_int), ("itercount", C.c_int),
+                ("ray_per_cell_max", C.c_int), ("hpx_lvl", C.c_int), ("nu_eV", C.c_double * 8),
+                ("spectrum_alpha", C.c_double * 15), ("spectrum_table", (C.c_double * 8) * 15),
+                ("cl_factor", C.c_float), ("box_hmpc", C.c_float), ("z", C.c_float), ("const_clump", C.c_float),
+                ("rkill_cm", C.c_double), ("seed", C.c_uint)]
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(HERE, "frt_oracle.cc")
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(
+            os.path.getmtime(src), os.path.getmtime(os.path.join(REPO, "flexrt_imaging_reion_b200", "csrc",
+                                                                 "hp_nest.h"))):
+        return LIB
+    os.makedirs(BUILD, exist_ok=True)
+    subprocess.run(["g++", "-O2", "-std=gnu++17", "-ffp-contract=off", "-fPIC", "-shared", "-w", "-I", HERE,
+                    src, "-o", LIB], check=True)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(build())
+        _lib.orc_create.restype = C.c_void_p
+        _lib.orc_create.argtypes = [C.POINTER(Params), C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_step.argtypes = [C.c_void_p]
+        _lib.orc_num_rays.restype = C.c_long
+        _lib.orc_num_rays.argtypes = [C.c_void_p]
+        _lib.orc_last_crossings.restype = C.c_long
+        _lib.orc_last_crossings.argtypes = [C.c_void_p]
+        _lib.orc_dump.argtypes = [C.c_void_p, C.c_char_p]
+        _lib.orc_scalars.argtypes = [C.c_void_p, C.c_void_p]
+        _lib.orc_destroy.argtypes = [C.c_void_p]
+    return _lib
+
+
+def make_params(spec: W.BoxSpec, seed: int, path_length: int = 8) -> Params:
+    p = Params()
+    p.N = spec.n
+    p.F = 5
+    p.path_length = path_length
+    p.itercount = 5
+    p.ray_per_cell_max = spec.ray_per_cell_max
+    p.hpx_lvl = 0
+    for i, e in enumerate(W.NU_EV_5BIN):
+        p.nu_eV[i] = e
+    for i, a in enumerate(SPEC_ALPHA):
+        p.spectrum_alpha[i] = a
+    for r, vals in SPEC_ROWS.items():
+        for nu, v in enumerate(vals):
+            p.spectrum_table[r][nu] = v
+    p.cl_factor = spec.cl_factor()
+    p.box_hmpc = spec.box_hmpc
+    p.z = spec.z
+    p.const_clump = 1.0
+    p.rkill_cm = spec.rkill_cm()
+    p.seed = seed
+    return p
+
+
+class Oracle:
+    """One box of the CPU restatement."""
+
+    def __init__(self, inp: W.BoxInputs, seed: int):
+        self._lib = lib()
+        self.spec = inp.spec
+        ijk, lum = W.grid_sources(inp)
+        self._keep = [np.ascontiguousarray(inp.delta1, dtype=np.float32), np.ascontiguousarray(ijk, np.int32),
+                      np.ascontiguousarray(lum, np.float64)]
+        clump = None if inp.clump is None else np.ascontiguousarray(inp.clump, np.float32)
+        self._keep.append(clump)
+        self._p = make_params(inp.spec, seed)
+        self.h = self._lib.orc_create(C.byref(self._p), self._keep[0].ctypes.data, len(lum),
+                                      self._keep[1].ctypes.data, self._keep[2].ctypes.data,
+                                      None if clump is None else clump.ctypes.data)
+
+    def step(self) -> None:
+        self._lib.orc_step(self.h)
+
+    def num_rays(self) -> int:
+        return int(self._lib.orc_num_rays(self.h))
+
+    def last_crossings(self) -> int:
+        return int(self._lib.orc_last_crossings(self.h))
+
+    def scalars(self) -> np.ndarray:
+        out = np.zeros(16, np.float64)
+        self._lib.orc_scalars(self.h, out.ctypes.data)
+        return out
+
+    def dump(self, path: str) -> None:
+        if self._lib.orc_dump(self.h, path.encode()) != 0:
+            raise IOError(path)
+
+    def close(self) -> None:
+        if self.h:
+            self._lib.orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
