@@ -1,0 +1,111 @@
+"""ctypes declarations of the C ABI in include/flexrt.h (libflexrt_b200.so).
+
+The library is loaded from the package's lib/ directory; importing this module fails loudly when
+it is missing -- there is no CPU fallback for the RT path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libflexrt_b200.so")
+
+FRT_MAX_FREQ = 8
+FRT_NTHETA = 42875
+
+FRT_OK, FRT_ERR_INVALID, FRT_ERR_CAPACITY, FRT_ERR_TIMEOUT, FRT_ERR_CUDA, FRT_ERR_STATE = range(6)
+FRT_PREC_MIXED, FRT_PREC_STRICT = 0, 1
+FRT_OUT_CORE, FRT_OUT_DIAG = 0, 1
+
+FIELDS = ["RHO", "NH", "NHE", "NH1", "NHE1", "NH2", "NHE2", "NE", "N_TOT", "F_H1", "F_HE1", "F_H2", "F_HE2", "TEMP",
+          "CLUMP", "AVG_NH1", "AVG_NHE1", "GAMMA_H1_TOT", "GAMMA_HE1_TOT", "HEAT_RATE", "COOL_RATE", "TREION",
+          "TREION_FLAG", "DNE_DT", "RECOMB_H2", "RECOMB_HE2", "RECRATE_H2", "RECRATE_HE2", "MFP", "MFP_912",
+          "IF_SPEED", "INC_FLUX", "GAMMA_H1_NU", "GAMMA_HE1_NU", "NGAM_NU", "U_NU"]
+FIELD_ID = {name: i for i, name in enumerate(FIELDS)}
+PER_BIN_FIELDS = {"GAMMA_H1_NU", "GAMMA_HE1_NU", "NGAM_NU", "U_NU"}
+
+EXPORTS = ["frt_create", "frt_destroy", "frt_last_error", "frt_rotation_table", "frt_build_rotation_table", "frt_init_gas", "frt_set_sources",
+           "frt_set_clump_field", "frt_set_field", "frt_get_field", "frt_init_rt", "frt_update_dt",
+           "frt_get_nphot_min_max", "frt_set_clump", "frt_set_clight", "frt_update_rays", "frt_find_avg_unu",
+           "frt_count_rays", "frt_merge", "frt_split_rays", "frt_update_thermal", "frt_new_rays", "frt_step",
+           "frt_step_plain", "frt_last_stats", "frt_num_rays", "frt_download_rays", "frt_box_scalars",
+           "frt_last_timing"]
+
+
+class BoxDesc(C.Structure):
+    _fields_ = [("n", C.c_int), ("box_hmpc", C.c_double), ("zz", C.c_float), ("cl_factor", C.c_float),
+                ("ray_per_cell_max", C.c_int), ("rkill_cm", C.c_double)]
+
+
+class Config(C.Structure):
+    _fields_ = [("nfreq", C.c_int), ("nu_phot", C.c_double * FRT_MAX_FREQ), ("spectrum", C.c_float * FRT_MAX_FREQ),
+                ("itercount", C.c_int), ("path_length", C.c_int), ("hpx_lvl", C.c_int),
+                ("safety_factor", C.c_float), ("tstep_factor", C.c_float), ("nl_const", C.c_float),
+                ("const_clump", C.c_float), ("fH1_0", C.c_float), ("fHe1_0", C.c_float), ("fHe2_0", C.c_float),
+                ("temp_0", C.c_float), ("nbox", C.c_int), ("boxes", C.POINTER(BoxDesc)),
+                ("ray_capacity", C.c_longlong), ("lit_capacity", C.c_longlong), ("src_capacity", C.c_longlong),
+                ("precision", C.c_int), ("outputs", C.c_int), ("device", C.c_int)]
+
+
+class StepStats(C.Structure):
+    _fields_ = [("rays_alive", C.c_longlong), ("rays_moved", C.c_longlong), ("crossings", C.c_longlong),
+                ("lit_cells", C.c_longlong), ("rays_split", C.c_longlong), ("rays_merged", C.c_longlong),
+                ("rays_killed", C.c_longlong), ("rays_cast", C.c_longlong), ("photons_emitted", C.c_double),
+                ("photons_deposited", C.c_double), ("photons_killed", C.c_double), ("photons_overlap", C.c_double),
+                ("photons_in_flight", C.c_double), ("t", C.c_double), ("dt", C.c_double),
+                ("error_flags", C.c_uint), ("pad", C.c_uint)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with flexrt_imaging_reion_b200.build.build() "
+                           "(the RT step has no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    P, I, LL, U16P = C.c_void_p, C.c_int, C.c_longlong, C.c_void_p
+    sig = {
+        "frt_create": ([C.POINTER(Config), C.POINTER(C.c_void_p)], I),
+        "frt_destroy": ([P], I),
+        "frt_last_error": ([P], C.c_char_p),
+        "frt_rotation_table": ([P, P], I),
+        "frt_build_rotation_table": ([P], I),
+        "frt_init_gas": ([P, I, P], I),
+        "frt_set_sources": ([P, I, I, P, P], I),
+        "frt_set_clump_field": ([P, I, P], I),
+        "frt_set_field": ([P, I, I, P], I),
+        "frt_get_field": ([P, I, I, P], I),
+        "frt_init_rt": ([P], I),
+        "frt_update_dt": ([P, P], I),
+        "frt_get_nphot_min_max": ([P, P, P], I),
+        "frt_set_clump": ([P], I),
+        "frt_set_clight": ([P], I),
+        "frt_update_rays": ([P], I),
+        "frt_find_avg_unu": ([P], I),
+        "frt_count_rays": ([P, P], I),
+        "frt_merge": ([P, U16P], I),
+        "frt_split_rays": ([P], I),
+        "frt_update_thermal": ([P], I),
+        "frt_new_rays": ([P, U16P], I),
+        "frt_step": ([P, U16P, U16P, C.POINTER(StepStats)], I),
+        "frt_step_plain": ([P, U16P, U16P, C.POINTER(StepStats)], I),
+        "frt_last_stats": ([P, C.POINTER(StepStats)], I),
+        "frt_num_rays": ([P, I, C.POINTER(LL)], I),
+        "frt_download_rays": ([P, I, P, P, P, P, P, P], I),
+        "frt_box_scalars": ([P, I, P], I),
+        "frt_last_timing": ([P, P, P], I),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L

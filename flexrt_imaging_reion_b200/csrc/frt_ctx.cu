@@ -1,0 +1,879 @@
+// RT context: device memory, the step sequences (fused CUDA-graph step and the reference's
+// individual step functions) and the C-ABI entry points declared in include/flexrt.h.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "frt_hostmath.h"
+#include "frt_internal.cuh"
+
+using namespace frt;
+
+struct frt_ctx {
+  frt_config cfg;
+  std::vector<frt_box_desc> boxes;
+  Dev d;
+  std::vector<BoxP> hbox;
+  std::vector<void*> allocs;
+  cudaStream_t s_main = nullptr, s_dark = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_t0 = nullptr, ev_t1 = nullptr, ev_d0 = nullptr, ev_d1 = nullptr;
+  // sources per box (host copy)
+  std::vector<std::vector<int>> src_cell;
+  std::vector<std::vector<double>> src_lum;
+  std::vector<char> gas_ready;
+  std::vector<std::vector<float>> rho;  // host copy of the proper density (set-up output)
+  std::vector<float> rot;
+  // pinned staging
+  uint16_t* h_ith_box = nullptr;
+  uint16_t* h_ith_src = nullptr;
+  Ctl* h_ctl = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  bool graph_valid = false;
+  bool strict = false;
+  int grid_rays = 0, grid_cells = 0, grid_lit = 0;
+  float last_step_ms = 0.f, last_dark_ms = 0.f;
+  frt_step_stats last{};
+  std::string err;
+};
+
+namespace {
+
+#define CK(x)                                                                          \
+  do {                                                                                 \
+    cudaError_t e_ = (x);                                                              \
+    if (e_ != cudaSuccess) {                                                           \
+      ctx->err = std::string(#x) + ": " + cudaGetErrorString(e_);                      \
+      return FRT_ERR_CUDA;                                                             \
+    }                                                                                  \
+  } while (0)
+
+template <typename T>
+frt_status dalloc(frt_ctx* ctx, T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) return FRT_OK;
+  void* q = nullptr;
+  CK(cudaMalloc(&q, n * sizeof(T)));
+  CK(cudaMemset(q, 0, n * sizeof(T)));
+  ctx->allocs.push_back(q);
+  *p = (T*)q;
+  return FRT_OK;
+}
+
+#define AL(ptr, n)                                   \
+  do {                                               \
+    frt_status st_ = dalloc(ctx, &(ptr), (size_t)(n)); \
+    if (st_ != FRT_OK) return st_;                   \
+  } while (0)
+
+frt_status upload_boxes(frt_ctx* ctx) {
+  CK(cudaMemcpy(ctx->d.box, ctx->hbox.data(), sizeof(BoxP) * ctx->hbox.size(), cudaMemcpyHostToDevice));
+  return FRT_OK;
+}
+frt_status download_boxes(frt_ctx* ctx) {
+  CK(cudaMemcpy(ctx->hbox.data(), ctx->d.box, sizeof(BoxP) * ctx->hbox.size(), cudaMemcpyDeviceToHost));
+  return FRT_OK;
+}
+
+frt_status check_box(frt_ctx* ctx, int box) {
+  if (!ctx || box < 0 || box >= (int)ctx->boxes.size()) {
+    if (ctx) ctx->err = "box index out of range";
+    return FRT_ERR_INVALID;
+  }
+  return FRT_OK;
+}
+
+frt_status sync_and_check(frt_ctx* ctx) {
+  CK(cudaStreamSynchronize(ctx->s_main));
+  CK(cudaStreamSynchronize(ctx->s_dark));
+  CK(cudaGetLastError());
+  Ctl c;
+  CK(cudaMemcpy(&c, ctx->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+  if (c.err) {
+    ctx->err = "device error flags " + std::to_string(c.err) +
+               " (1 ray pool full, 2 path_length exceeded, 4 lit-cell list full)";
+    return FRT_ERR_CAPACITY;
+  }
+  return FRT_OK;
+}
+
+// Rebuild the concatenated source arrays of all boxes (box order, then (i,j,k) order).
+frt_status upload_sources(frt_ctx* ctx) {
+  std::vector<int> cell;
+  std::vector<uint16_t> box;
+  std::vector<double> lum;
+  std::vector<float> rdt;
+  for (size_t b = 0; b < ctx->boxes.size(); b++)
+    for (size_t s = 0; s < ctx->src_cell[b].size(); s++) {
+      cell.push_back(ctx->src_cell[b][s]);
+      box.push_back((uint16_t)b);
+      lum.push_back(ctx->src_lum[b][s]);
+      rdt.push_back(0.f);
+    }
+  const int n = (int)cell.size();
+  if (n > ctx->d.src_cap) {
+    ctx->err = "more sources than src_capacity";
+    return FRT_ERR_CAPACITY;
+  }
+  ctx->d.nsrc = n;
+  if (n) {
+    CK(cudaMemcpy(ctx->d.src_cell, cell.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d.src_box, box.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d.src_lum, lum.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d.src_ray_dt, rdt.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  }
+  ctx->graph_valid = false;
+  return FRT_OK;
+}
+
+// ---- step sequences ---------------------------------------------------------------------------
+void enqueue_begin_advance(frt_ctx* ctx) {
+  const Dev& d = ctx->d;
+  launch_clear_lit(d, ctx->grid_lit, ctx->s_main);
+  launch_step_begin(d, ctx->s_main);
+  launch_advance(d, ctx->grid_rays, ctx->s_main);
+}
+
+void enqueue_iterations(frt_ctx* ctx, bool fused_thermal) {
+  const Dev& d = ctx->d;
+  launch_lit_init(d, ctx->strict, ctx->grid_lit, ctx->s_main);
+  for (int it = 0; it < d.itercount; it++) {
+    launch_raypass(d, it, ctx->strict, ctx->grid_rays, ctx->s_main);
+    launch_litpass(d, it, ctx->strict, fused_thermal, ctx->grid_lit, ctx->s_main);
+  }
+}
+
+// The whole step of main.cc:108-264 (fixed redshift): the dark-cell pass runs on a second
+// stream concurrently with the lit-cell iteration and the ray life-cycle kernels.
+void enqueue_step(frt_ctx* ctx, bool in_graph) {
+  const Dev& d = ctx->d;
+  cudaStream_t s = ctx->s_main;
+  cudaMemcpyAsync(d.itheta_merge, ctx->h_ith_box, sizeof(uint16_t) * d.nbox, cudaMemcpyHostToDevice, s);
+  if (d.nsrc) cudaMemcpyAsync(d.src_itheta, ctx->h_ith_src, sizeof(uint16_t) * d.nsrc, cudaMemcpyHostToDevice, s);
+  enqueue_begin_advance(ctx);
+  cudaEventRecord(ctx->ev_fork, s);
+  cudaStreamWaitEvent(ctx->s_dark, ctx->ev_fork, 0);
+  if (in_graph) cudaEventRecordWithFlags(ctx->ev_d0, ctx->s_dark, cudaEventRecordExternal);
+  else cudaEventRecord(ctx->ev_d0, ctx->s_dark);
+  launch_dark(d, ctx->strict, true, ctx->grid_cells, ctx->s_dark);
+  if (in_graph) cudaEventRecordWithFlags(ctx->ev_d1, ctx->s_dark, cudaEventRecordExternal);
+  else cudaEventRecord(ctx->ev_d1, ctx->s_dark);
+  cudaEventRecord(ctx->ev_join, ctx->s_dark);
+  enqueue_iterations(ctx, true);
+  launch_count(d, ctx->grid_rays, s);
+  launch_merge(d, ctx->grid_rays, s);
+  launch_split_compact(d, ctx->grid_rays, s);
+  cudaStreamWaitEvent(s, ctx->ev_join, 0);
+  launch_cast(d, s);
+  cudaMemcpyAsync(ctx->h_ctl, d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+}
+
+void fill_stats(frt_ctx* ctx, const Ctl& c, frt_step_stats* st) {
+  frt_step_stats o{};
+  o.rays_alive = c.nray[c.cur];
+  o.rays_moved = c.rays_moved;
+  o.crossings = c.crossings;
+  o.lit_cells = c.n_lit;
+  o.rays_split = c.split;
+  o.rays_merged = c.merged;
+  o.rays_killed = c.killed;
+  o.rays_cast = c.cast;
+  o.photons_emitted = c.emitted;
+  o.photons_deposited = c.deposited;
+  o.photons_killed = c.killed_ph;
+  o.photons_overlap = c.overlap;
+  o.photons_in_flight = c.in_flight;
+  o.t = ctx->hbox.empty() ? 0.0 : 0.0;
+  o.dt = ctx->hbox.empty() ? 0.0 : (double)ctx->hbox[0].dt;
+  o.error_flags = c.err;
+  ctx->last = o;
+  if (st) *st = o;
+}
+
+frt_status stage_itheta(frt_ctx* ctx, const uint16_t* ith_box, const uint16_t* ith_src) {
+  for (int b = 0; b < ctx->d.nbox; b++) {
+    const uint16_t v = ith_box ? ith_box[b] : 0;
+    if (v >= kNtheta) {
+      ctx->err = "itheta out of range";
+      return FRT_ERR_INVALID;
+    }
+    ctx->h_ith_box[b] = v;
+  }
+  for (int s = 0; s < ctx->d.nsrc; s++) {
+    const uint16_t v = ith_src ? ith_src[s] : 0;
+    if (v >= kNtheta) {
+      ctx->err = "itheta out of range";
+      return FRT_ERR_INVALID;
+    }
+    ctx->h_ith_src[s] = v;
+  }
+  return FRT_OK;
+}
+
+frt_status finish_step(frt_ctx* ctx, frt_step_stats* stats) {
+  CK(cudaEventSynchronize(ctx->ev_t1));
+  CK(cudaStreamSynchronize(ctx->s_dark));
+  CK(cudaGetLastError());
+  float ms = 0.f, dms = 0.f;
+  CK(cudaEventElapsedTime(&ms, ctx->ev_t0, ctx->ev_t1));
+  if (cudaEventElapsedTime(&dms, ctx->ev_d0, ctx->ev_d1) != cudaSuccess) {
+    cudaGetLastError();
+    dms = -1.f;
+  }
+  ctx->last_step_ms = ms;
+  ctx->last_dark_ms = dms;
+  fill_stats(ctx, *ctx->h_ctl, stats);
+  if (ctx->h_ctl->err) {
+    ctx->err = "device error flags " + std::to_string(ctx->h_ctl->err) +
+               " (1 ray pool full, 2 path_length exceeded, 4 lit-cell list full)";
+    return FRT_ERR_CAPACITY;
+  }
+  return FRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* frt_last_error(const frt_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
+  if (!cfg || !out || cfg->nbox < 1 || !cfg->boxes || cfg->nfreq < 1 || cfg->nfreq > FRT_MAX_FREQ ||
+      cfg->path_length < 2 || cfg->path_length > FRT_MAX_PATH || cfg->itercount < 1 || cfg->ray_capacity < 1 ||
+      cfg->hpx_lvl < 0 || cfg->hpx_lvl > 6 || cfg->nbox > 65535)
+    return FRT_ERR_INVALID;
+  frt_ctx* ctx = new frt_ctx();
+  *out = ctx;
+  ctx->cfg = *cfg;
+  ctx->boxes.assign(cfg->boxes, cfg->boxes + cfg->nbox);
+  ctx->cfg.boxes = ctx->boxes.data();
+  ctx->strict = cfg->precision == FRT_PREC_STRICT;
+  CK(cudaSetDevice(cfg->device));
+  int nsm = 148;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cfg->device));
+  ctx->grid_rays = nsm * 8;
+  ctx->grid_cells = nsm * 8;
+  ctx->grid_lit = nsm * 8;
+  CK(cudaStreamCreateWithFlags(&ctx->s_main, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&ctx->s_dark, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+  CK(cudaEventCreate(&ctx->ev_t0));
+  CK(cudaEventCreate(&ctx->ev_t1));
+  CK(cudaEventCreate(&ctx->ev_d0));
+  CK(cudaEventCreate(&ctx->ev_d1));
+
+  Dev& d = ctx->d;
+  memset(&d, 0, sizeof(d));
+  d.nbox = cfg->nbox;
+  d.F = cfg->nfreq;
+  d.PL = cfg->path_length;
+  d.itercount = cfg->itercount;
+  d.hpx_lvl = cfg->hpx_lvl;
+  d.outputs = cfg->outputs;
+  d.nhe_to_nh = (0.246 / 4.) / (1. - 0.246);
+  d.const_clump = cfg->const_clump;
+  // boxes: tile-aligned concatenation
+  ctx->hbox.resize(cfg->nbox);
+  long long off = 0;
+  for (int b = 0; b < cfg->nbox; b++) {
+    const frt_box_desc& bd = cfg->boxes[b];
+    if (bd.n < 2 || bd.n > 1024 || !(bd.cl_factor > 0.f)) {
+      ctx->err = "bad box description";
+      return FRT_ERR_INVALID;
+    }
+    host::box_params(&ctx->hbox[b], &ctx->cfg, &bd, off);
+    off += ((ctx->hbox[b].ncell + kTile - 1) / kTile) * kTile;
+  }
+  d.ncell_total = off;
+  d.ntile = off / kTile;
+  if (off >= (1LL << 31)) {
+    ctx->err = "too many cells for 32-bit cell indices";
+    return FRT_ERR_INVALID;
+  }
+  d.ray_cap = (int)std::min<long long>(cfg->ray_capacity, (1LL << 31) - 64);
+  long long lc = cfg->lit_capacity > 0 ? cfg->lit_capacity : off;
+  lc = std::min<long long>(lc, std::min<long long>(off, (long long)d.ray_cap * d.PL));
+  d.lit_cap = (int)std::max<long long>(lc, 1024);
+  d.src_cap = (int)std::max<long long>(cfg->src_capacity, 1);
+  // spectrum / cross sections
+  for (int nu = 0; nu < FRT_MAX_FREQ; nu++) d.spectrum[nu] = nu < d.F ? cfg->spectrum[nu] : 0.f;
+  host::derived_constants(&ctx->cfg, d.sigH1_d, d.sigHe1_d, &d.sigH1_0, &d.sigH1_912, &d.pi_sf_3, &d.log4);
+  for (int nu = 0; nu < d.F; nu++) {
+    d.sigH1_f[nu] = (float)d.sigH1_d[nu];
+    d.sigHe1_f[nu] = (float)d.sigHe1_d[nu];
+  }
+  // device memory
+  AL(d.box, cfg->nbox);
+  AL(d.count, cfg->nbox);
+  AL(d.need_hist, cfg->nbox);
+  AL(d.hist, (size_t)cfg->nbox * kPdfBins);
+  AL(d.itheta_merge, cfg->nbox);
+  AL(d.lg, 2 * cfg->nbox);
+  {
+    ctx->rot.resize((size_t)kNtheta * 18);
+    host::rotation_table(ctx->rot.data());
+    float* r = nullptr;
+    AL(r, ctx->rot.size());
+    CK(cudaMemcpy(r, ctx->rot.data(), sizeof(float) * ctx->rot.size(), cudaMemcpyHostToDevice));
+    d.rot = r;
+  }
+  {
+    std::vector<int16_t> tb(d.ntile, (int16_t)-1);
+    for (int b = 0; b < cfg->nbox; b++) {
+      const long long t0 = ctx->hbox[b].cell0 >> kTileShift;
+      const long long nt = (ctx->hbox[b].ncell + kTile - 1) / kTile;
+      for (long long t = t0; t < t0 + nt; t++) tb[t] = (int16_t)b;
+    }
+    AL(d.tile_box, d.ntile);
+    CK(cudaMemcpy(d.tile_box, tb.data(), sizeof(int16_t) * d.ntile, cudaMemcpyHostToDevice));
+  }
+  const size_t NC = (size_t)off;
+  AL(d.nH, NC); AL(d.nHe, NC); AL(d.nH1, NC); AL(d.nHe1, NC); AL(d.f_H1, NC); AL(d.f_He1, NC);
+  AL(d.temp, NC); AL(d.ne, NC); AL(d.heat, NC); AL(d.cool, NC); AL(d.avg_nh1, NC); AL(d.avg_nhe1, NC);
+  AL(d.treion, NC); AL(d.treion_flag, NC); AL(d.lit_flag, NC); AL(d.lit_slot, NC);
+  AL(d.nH1_prev, NC); AL(d.n_tot, NC); AL(d.dne_dt, NC);
+  d.clump = nullptr;
+  if (cfg->outputs == FRT_OUT_DIAG) {
+    AL(d.rec_h2, NC); AL(d.rec_he2, NC); AL(d.recrate_h2, NC); AL(d.recrate_he2, NC);
+    AL(d.mfp, NC); AL(d.mfp912, NC); AL(d.if_speed, NC); AL(d.inc_flux, NC);
+  }
+  launch_fill_i32(d.lit_slot, -1, (long long)NC, ctx->s_main);
+  const size_t L = (size_t)d.lit_cap;
+  AL(d.l_cell, L); AL(d.l_nh, L); AL(d.l_nhe, L); AL(d.l_y0h, L); AL(d.l_y0he, L); AL(d.l_crec_h, L);
+  AL(d.l_crec_he, L); AL(d.l_rec_h2, L); AL(d.l_rec_he2, L); AL(d.l_avg_h, L); AL(d.l_avg_he, L);
+  AL(d.l_nh1_old, L); AL(d.l_acc_g, L); AL(d.l_acc_ghe, L);
+  AL(d.l_acc_nu_h, L * d.F); AL(d.l_acc_nu_he, L * d.F); AL(d.l_ngam, L * d.F);
+  const size_t R = (size_t)d.ray_cap;
+  for (int p = 0; p < 2; p++) {
+    RayPool& P = d.pool[p];
+    AL(P.cell, R); AL(P.box, R); AL(P.order, R); AL(P.pixel, R); AL(P.itheta, R);
+    AL(P.xh, R); AL(P.yh, R); AL(P.zh, R); AL(P.nphot, R * d.F);
+    AL(P.r, R); AL(P.dr, R); AL(P.x, R); AL(P.y, R); AL(P.z, R); AL(P.time, R);
+  }
+  AL(d.seg, R * d.PL); AL(d.seg_dist, R * d.PL); AL(d.nseg, R); AL(d.dead, R);
+  // merge bins only when some box can reach its merge threshold with this pool size
+  bool merge_reachable = false;
+  for (int b = 0; b < cfg->nbox; b++) merge_reachable |= ctx->hbox[b].num_thresh < (long long)d.ray_cap;
+  if (merge_reachable) {
+    const long long npix = 12LL << (2 * cfg->hpx_lvl);
+    if ((long long)NC * npix >= (1LL << 31)) {
+      ctx->err = "merge bin table exceeds 32-bit indices";
+      return FRT_ERR_INVALID;
+    }
+    AL(d.bin_base, NC * npix);
+    launch_fill_i32(d.bin_base, 0x7fffffff, (long long)NC * npix, ctx->s_main);
+    AL(d.ray_bin, R);
+    launch_fill_i32(d.ray_bin, -1, (long long)R, ctx->s_main);
+    AL(d.merged_flag, R);
+  }
+  AL(d.src_cell, d.src_cap); AL(d.src_box, d.src_cap); AL(d.src_lum, d.src_cap); AL(d.src_ray_dt, d.src_cap);
+  AL(d.src_itheta, d.src_cap);
+  AL(d.ctl, 1);
+  CK(cudaMallocHost(&ctx->h_ith_box, sizeof(uint16_t) * cfg->nbox));
+  CK(cudaMallocHost(&ctx->h_ith_src, sizeof(uint16_t) * d.src_cap));
+  CK(cudaMallocHost(&ctx->h_ctl, sizeof(Ctl)));
+  memset(ctx->h_ctl, 0, sizeof(Ctl));
+  ctx->src_cell.resize(cfg->nbox);
+  ctx->src_lum.resize(cfg->nbox);
+  ctx->gas_ready.assign(cfg->nbox, 0);
+  ctx->rho.resize(cfg->nbox);
+  {
+    frt_status st = upload_boxes(ctx);
+    if (st) return st;
+  }
+  CK(cudaStreamSynchronize(ctx->s_main));
+  return FRT_OK;
+}
+
+frt_status frt_destroy(frt_ctx* ctx) {
+  if (!ctx) return FRT_OK;
+  if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+  for (void* p : ctx->allocs) cudaFree(p);
+  if (ctx->h_ith_box) cudaFreeHost(ctx->h_ith_box);
+  if (ctx->h_ith_src) cudaFreeHost(ctx->h_ith_src);
+  if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
+  cudaEvent_t evs[] = {ctx->ev_fork, ctx->ev_join, ctx->ev_t0, ctx->ev_t1, ctx->ev_d0, ctx->ev_d1};
+  for (cudaEvent_t e : evs)
+    if (e) cudaEventDestroy(e);
+  if (ctx->s_main) cudaStreamDestroy(ctx->s_main);
+  if (ctx->s_dark) cudaStreamDestroy(ctx->s_dark);
+  delete ctx;
+  return FRT_OK;
+}
+
+frt_status frt_build_rotation_table(float* out) {
+  if (!out) return FRT_ERR_INVALID;
+  host::rotation_table(out);
+  return FRT_OK;
+}
+
+frt_status frt_rotation_table(const frt_ctx* ctx, float* out) {
+  if (!ctx || !out) return FRT_ERR_INVALID;
+  memcpy(out, ctx->rot.data(), sizeof(float) * ctx->rot.size());
+  return FRT_OK;
+}
+
+frt_status frt_init_gas(frt_ctx* ctx, int box, const float* delta1) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  if (!delta1) return FRT_ERR_INVALID;
+  const BoxP& B = ctx->hbox[box];
+  const size_t n = (size_t)B.ncell;
+  std::vector<float> rho(n), nH(n), nHe(n), nH1(n), nHe1(n), fH1(n), fHe1(n), temp(n), ne(n), ntot(n), rh(n), rhe(n),
+      dne(n);
+  host::GasInit g{rho.data(), nH.data(), nHe.data(), nH1.data(), nHe1.data(), fH1.data(), fHe1.data(), temp.data(),
+                  ne.data(), ntot.data(), rh.data(), rhe.data(), dne.data()};
+  host::init_gas(&ctx->cfg, &ctx->boxes[box], delta1, &g);
+  Dev& d = ctx->d;
+  const size_t o = (size_t)B.cell0;
+  auto up = [&](float* dst, const std::vector<float>& src) {
+    return cudaMemcpy(dst + o, src.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+  };
+  CK(up(d.nH, nH)); CK(up(d.nHe, nHe)); CK(up(d.nH1, nH1)); CK(up(d.nHe1, nHe1)); CK(up(d.f_H1, fH1));
+  CK(up(d.f_He1, fHe1)); CK(up(d.temp, temp)); CK(up(d.ne, ne)); CK(up(d.avg_nh1, nH1)); CK(up(d.avg_nhe1, nHe1));
+  CK(up(d.n_tot, ntot)); CK(up(d.dne_dt, dne)); CK(up(d.nH1_prev, nH1));
+  CK(cudaMemset(d.heat + o, 0, sizeof(float) * n));
+  CK(cudaMemset(d.cool + o, 0, sizeof(float) * n));
+  CK(cudaMemset(d.treion + o, 0, sizeof(float) * n));
+  CK(cudaMemset(d.treion_flag + o, 0, n));
+  if (d.rec_h2) {
+    CK(up(d.rec_h2, rh));
+    CK(up(d.rec_he2, rhe));
+  }
+  ctx->rho[box] = rho;
+  ctx->gas_ready[box] = 1;
+  return FRT_OK;
+}
+
+frt_status frt_set_sources(frt_ctx* ctx, int box, int nsrc, const int32_t* ijk, const double* lum) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  if (nsrc < 0 || (nsrc > 0 && (!ijk || !lum))) return FRT_ERR_INVALID;
+  const int n = ctx->hbox[box].n;
+  ctx->src_cell[box].clear();
+  ctx->src_lum[box].clear();
+  for (int s = 0; s < nsrc; s++) {
+    const int i = ijk[3 * s], j = ijk[3 * s + 1], k = ijk[3 * s + 2];
+    if (i < 0 || j < 0 || k < 0 || i >= n || j >= n || k >= n) {
+      ctx->err = "source cell out of range";
+      return FRT_ERR_INVALID;
+    }
+    ctx->src_cell[box].push_back((i * n + j) * n + k);
+    ctx->src_lum[box].push_back(lum[s]);
+  }
+  return upload_sources(ctx);
+}
+
+frt_status frt_set_clump_field(frt_ctx* ctx, int box, const float* clump) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  Dev& d = ctx->d;
+  if (!d.clump) {
+    if (!clump) return FRT_OK;
+    AL(d.clump, (size_t)d.ncell_total);
+    // cells of other boxes keep the constant
+    std::vector<float> c(d.ncell_total, ctx->cfg.const_clump);
+    CK(cudaMemcpy(d.clump, c.data(), sizeof(float) * c.size(), cudaMemcpyHostToDevice));
+    ctx->graph_valid = false;
+  }
+  const BoxP& B = ctx->hbox[box];
+  if (clump) {
+    CK(cudaMemcpy(d.clump + B.cell0, clump, sizeof(float) * B.ncell, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> c(B.ncell, ctx->cfg.const_clump);
+    CK(cudaMemcpy(d.clump + B.cell0, c.data(), sizeof(float) * B.ncell, cudaMemcpyHostToDevice));
+  }
+  return FRT_OK;
+}
+
+static float* field_ptr(frt_ctx* ctx, frt_field f) {
+  Dev& d = ctx->d;
+  switch (f) {
+    case FRT_F_NH: return d.nH;
+    case FRT_F_NHE: return d.nHe;
+    case FRT_F_NH1: return d.nH1;
+    case FRT_F_NHE1: return d.nHe1;
+    case FRT_F_NE: return d.ne;
+    case FRT_F_F_H1: return d.f_H1;
+    case FRT_F_F_HE1: return d.f_He1;
+    case FRT_F_TEMP: return d.temp;
+    case FRT_F_CLUMP: return d.clump;
+    case FRT_F_AVG_NH1: return d.avg_nh1;
+    case FRT_F_AVG_NHE1: return d.avg_nhe1;
+    case FRT_F_HEAT_RATE: return d.heat;
+    case FRT_F_COOL_RATE: return d.cool;
+    case FRT_F_TREION: return d.treion;
+    case FRT_F_DNE_DT: return d.dne_dt;
+    case FRT_F_N_TOT: return d.n_tot;
+    case FRT_F_RECOMB_H2: return d.rec_h2;
+    case FRT_F_RECOMB_HE2: return d.rec_he2;
+    case FRT_F_RECRATE_H2: return d.recrate_h2;
+    case FRT_F_RECRATE_HE2: return d.recrate_he2;
+    case FRT_F_MFP: return d.mfp;
+    case FRT_F_MFP_912: return d.mfp912;
+    case FRT_F_IF_SPEED: return d.if_speed;
+    case FRT_F_INC_FLUX: return d.inc_flux;
+    default: return nullptr;
+  }
+}
+
+frt_status frt_set_field(frt_ctx* ctx, int box, frt_field f, const float* host) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  if (!host) return FRT_ERR_INVALID;
+  if (f == FRT_F_CLUMP) return frt_set_clump_field(ctx, box, host);
+  float* p = field_ptr(ctx, f);
+  if (!p) {
+    ctx->err = "field is not settable";
+    return FRT_ERR_INVALID;
+  }
+  const BoxP& B = ctx->hbox[box];
+  CK(cudaMemcpy(p + B.cell0, host, sizeof(float) * B.ncell, cudaMemcpyHostToDevice));
+  return FRT_OK;
+}
+
+frt_status frt_get_field(frt_ctx* ctx, int box, frt_field f, float* host) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  if (!host) return FRT_ERR_INVALID;
+  Dev& d = ctx->d;
+  const BoxP& B = ctx->hbox[box];
+  const size_t n = (size_t)B.ncell;
+  const int F = d.F;
+  auto get = [&](const float* src, float* dst) {
+    return cudaMemcpy(dst, src + B.cell0, sizeof(float) * n, cudaMemcpyDeviceToHost);
+  };
+  auto sparse = [&](int which, float* dst) -> frt_status {
+    float* tmp = nullptr;
+    CK(cudaMalloc(&tmp, sizeof(float) * n));
+    launch_gather_sparse(d, B.cell0, (long long)n, which, tmp, ctx->s_main);
+    CK(cudaStreamSynchronize(ctx->s_main));
+    CK(cudaMemcpy(dst, tmp, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    CK(cudaFree(tmp));
+    return FRT_OK;
+  };
+  CK(cudaStreamSynchronize(ctx->s_main));
+  CK(cudaStreamSynchronize(ctx->s_dark));
+  switch (f) {
+    case FRT_F_RHO:
+      if (ctx->rho[box].size() != n) return FRT_ERR_STATE;
+      memcpy(host, ctx->rho[box].data(), sizeof(float) * n);
+      return FRT_OK;
+    case FRT_F_CLUMP:
+      if (!d.clump) {
+        for (size_t i = 0; i < n; i++) host[i] = ctx->cfg.const_clump;
+        return FRT_OK;
+      }
+      CK(get(d.clump, host));
+      return FRT_OK;
+    case FRT_F_NH2:
+    case FRT_F_NHE2:
+    case FRT_F_F_H2:
+    case FRT_F_F_HE2: {
+      const bool h = (f == FRT_F_NH2 || f == FRT_F_F_H2);
+      std::vector<float> a(n), b(n);
+      CK(get(h ? d.nH : d.nHe, a.data()));
+      CK(get(h ? d.nH1 : d.nHe1, b.data()));
+      const bool frac = (f == FRT_F_F_H2 || f == FRT_F_F_HE2);
+      for (size_t i = 0; i < n; i++) {
+        const float x2 = a[i] - b[i];          // nH2 = (float) nH - nH1 (ray_tracing.cc:1119)
+        host[i] = frac ? x2 / a[i] : x2;       // f_H2 = nH2/nH (ray_tracing.cc:1192)
+      }
+      return FRT_OK;
+    }
+    case FRT_F_TREION_FLAG: {
+      std::vector<uint8_t> a(n);
+      CK(cudaMemcpy(a.data(), d.treion_flag + B.cell0, n, cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < n; i++) host[i] = a[i] ? 1.f : 0.f;
+      return FRT_OK;
+    }
+    case FRT_F_GAMMA_H1_TOT: return sparse(0, host);
+    case FRT_F_GAMMA_HE1_TOT: return sparse(1, host);
+    case FRT_F_GAMMA_H1_NU:
+    case FRT_F_GAMMA_HE1_NU:
+    case FRT_F_NGAM_NU: {
+      const int base = (f == FRT_F_GAMMA_H1_NU) ? 2 : (f == FRT_F_GAMMA_HE1_NU ? 2 + F : 2 + 2 * F);
+      std::vector<float> tmp(n);
+      for (int nu = 0; nu < F; nu++) {
+        st = sparse(base + nu, tmp.data());
+        if (st) return st;
+        for (size_t i = 0; i < n; i++) host[i * F + nu] = tmp[i];
+      }
+      return FRT_OK;
+    }
+    case FRT_F_U_NU: {
+      // u_nu = (float)(spectrum*Gamma/sigma) * h * nu / clight (ray_tracing.cc:1142-1144)
+      std::vector<float> g(n);
+      st = sparse(0, g.data());
+      if (st) return st;
+      for (size_t i = 0; i < n; i++)
+        for (int nu = 0; nu < F; nu++)
+          host[i * F + nu] = (float)(d.spectrum[nu] * g[i] / d.sigH1_d[nu]) * 6.626068e-27 * ctx->cfg.nu_phot[nu] /
+                             B.clight;
+      return FRT_OK;
+    }
+    default: {
+      const float* p = field_ptr(ctx, f);
+      if (!p) {
+        ctx->err = "field not kept in this output mode";
+        return FRT_ERR_STATE;
+      }
+      CK(get(p, host));
+      return FRT_OK;
+    }
+  }
+}
+
+frt_status frt_init_rt(frt_ctx* ctx) {
+  if (!ctx) return FRT_ERR_INVALID;
+  Dev& d = ctx->d;
+  for (size_t b = 0; b < ctx->boxes.size(); b++)
+    if (!ctx->gas_ready[b]) {
+      ctx->err = "frt_init_gas not called for every box";
+      return FRT_ERR_STATE;
+    }
+  // ray_dt of the source cells = dt (rt_funcs.cc:85-101, input_grid = FALSE)
+  std::vector<float> rdt;
+  for (size_t b = 0; b < ctx->boxes.size(); b++)
+    for (size_t s = 0; s < ctx->src_cell[b].size(); s++) rdt.push_back(ctx->src_lum[b][s] != 0 ? ctx->hbox[b].dt : 0.f);
+  if (!rdt.empty()) CK(cudaMemcpy(d.src_ray_dt, rdt.data(), sizeof(float) * rdt.size(), cudaMemcpyHostToDevice));
+  Ctl c;
+  memset(&c, 0, sizeof(c));
+  CK(cudaMemcpy(d.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice));
+  CK(cudaMemset(d.lit_flag, 0, (size_t)d.ncell_total));
+  launch_fill_i32(d.lit_slot, -1, d.ncell_total, ctx->s_main);
+  CK(cudaStreamSynchronize(ctx->s_main));
+  for (auto& B : ctx->hbox) {
+    B.t = 0.f;
+    B.nphot_merge = 0.f;
+  }
+  return upload_boxes(ctx);
+}
+
+frt_status frt_update_dt(frt_ctx* ctx, float* dt_out) {
+  if (!ctx) return FRT_ERR_INVALID;
+  if (dt_out)
+    for (size_t b = 0; b < ctx->hbox.size(); b++) dt_out[b] = ctx->hbox[b].dt;
+  return FRT_OK;
+}
+
+frt_status frt_get_nphot_min_max(frt_ctx* ctx, double* nmin_out, double* nmax_out) {
+  if (!ctx) return FRT_ERR_INVALID;
+  frt_status st = download_boxes(ctx);
+  if (st) return st;
+  std::vector<double> lg(2 * ctx->hbox.size());
+  for (size_t b = 0; b < ctx->hbox.size(); b++) {
+    BoxP& B = ctx->hbox[b];
+    double mn = 0, mx = 0;
+    if (!ctx->src_lum[b].empty())
+      host::nphot_min_max(&ctx->cfg, &B, (int)ctx->src_lum[b].size(), ctx->src_lum[b].data(), &mn, &mx);
+    B.nphot_min = mn;
+    B.nphot_max = mx;
+    const double lg_max = log10(mx), lg_min = log10(mn);
+    lg[2 * b] = lg_min;
+    lg[2 * b + 1] = (lg_max - lg_min) / (10000 - 1);
+    const float a = (float)(4. * (double)B.nphot_merge), c = (float)(4. * B.nphot_min);
+    B.split_thr = (c >= a) ? c : a;
+    if (nmin_out) nmin_out[b] = mn;
+    if (nmax_out) nmax_out[b] = mx;
+  }
+  CK(cudaMemcpy(ctx->d.lg, lg.data(), sizeof(double) * lg.size(), cudaMemcpyHostToDevice));
+  return upload_boxes(ctx);
+}
+
+frt_status frt_set_clump(frt_ctx* ctx) { return ctx ? FRT_OK : FRT_ERR_INVALID; }
+frt_status frt_set_clight(frt_ctx* ctx) { return ctx ? FRT_OK : FRT_ERR_INVALID; }
+
+frt_status frt_update_rays(frt_ctx* ctx) {
+  if (!ctx) return FRT_ERR_INVALID;
+  enqueue_begin_advance(ctx);
+  return sync_and_check(ctx);
+}
+
+frt_status frt_find_avg_unu(frt_ctx* ctx) {
+  if (!ctx) return FRT_ERR_INVALID;
+  enqueue_iterations(ctx, false);
+  launch_dark(ctx->d, ctx->strict, false, ctx->grid_cells, ctx->s_main);
+  return sync_and_check(ctx);
+}
+
+frt_status frt_count_rays(frt_ctx* ctx, long long* count_per_box) {
+  if (!ctx) return FRT_ERR_INVALID;
+  launch_count(ctx->d, ctx->grid_rays, ctx->s_main);
+  frt_status st = sync_and_check(ctx);
+  if (st) return st;
+  if (count_per_box) CK(cudaMemcpy(count_per_box, ctx->d.count, sizeof(long long) * ctx->d.nbox, cudaMemcpyDeviceToHost));
+  return FRT_OK;
+}
+
+frt_status frt_merge(frt_ctx* ctx, const uint16_t* itheta_per_box) {
+  if (!ctx) return FRT_ERR_INVALID;
+  frt_status st = stage_itheta(ctx, itheta_per_box, nullptr);
+  if (st) return st;
+  CK(cudaMemcpyAsync(ctx->d.itheta_merge, ctx->h_ith_box, sizeof(uint16_t) * ctx->d.nbox, cudaMemcpyHostToDevice,
+                     ctx->s_main));
+  launch_count(ctx->d, ctx->grid_rays, ctx->s_main);
+  launch_merge(ctx->d, ctx->grid_rays, ctx->s_main);
+  return sync_and_check(ctx);
+}
+
+frt_status frt_split_rays(frt_ctx* ctx) {
+  if (!ctx) return FRT_ERR_INVALID;
+  launch_split_compact(ctx->d, ctx->grid_rays, ctx->s_main);
+  return sync_and_check(ctx);
+}
+
+frt_status frt_update_thermal(frt_ctx* ctx) {
+  if (!ctx) return FRT_ERR_INVALID;
+  launch_thermal_all(ctx->d, ctx->strict, ctx->grid_cells, ctx->s_main);
+  return sync_and_check(ctx);
+}
+
+frt_status frt_new_rays(frt_ctx* ctx, const uint16_t* itheta_per_source) {
+  if (!ctx) return FRT_ERR_INVALID;
+  frt_status st = stage_itheta(ctx, nullptr, itheta_per_source);
+  if (st) return st;
+  if (ctx->d.nsrc)
+    CK(cudaMemcpyAsync(ctx->d.src_itheta, ctx->h_ith_src, sizeof(uint16_t) * ctx->d.nsrc, cudaMemcpyHostToDevice,
+                       ctx->s_main));
+  launch_cast(ctx->d, ctx->s_main);
+  return sync_and_check(ctx);
+}
+
+frt_status frt_step_plain(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t* itheta_per_source,
+                          frt_step_stats* stats) {
+  if (!ctx) return FRT_ERR_INVALID;
+  frt_status st = stage_itheta(ctx, itheta_per_box, itheta_per_source);
+  if (st) return st;
+  CK(cudaEventRecord(ctx->ev_t0, ctx->s_main));
+  enqueue_step(ctx, false);
+  CK(cudaEventRecord(ctx->ev_t1, ctx->s_main));
+  return finish_step(ctx, stats);
+}
+
+frt_status frt_step(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t* itheta_per_source,
+                    frt_step_stats* stats) {
+  if (!ctx) return FRT_ERR_INVALID;
+  frt_status st = stage_itheta(ctx, itheta_per_box, itheta_per_source);
+  if (st) return st;
+  if (!ctx->graph_valid) {
+    if (ctx->graph) {
+      cudaGraphExecDestroy(ctx->graph);
+      ctx->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamSynchronize(ctx->s_main));
+    CK(cudaStreamBeginCapture(ctx->s_main, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(ctx, true);
+    CK(cudaStreamEndCapture(ctx->s_main, &g));
+    CK(cudaGraphInstantiate(&ctx->graph, g, 0));
+    CK(cudaGraphDestroy(g));
+    ctx->graph_valid = true;
+  }
+  CK(cudaEventRecord(ctx->ev_t0, ctx->s_main));
+  CK(cudaGraphLaunch(ctx->graph, ctx->s_main));
+  CK(cudaEventRecord(ctx->ev_t1, ctx->s_main));
+  return finish_step(ctx, stats);
+}
+
+frt_status frt_last_stats(frt_ctx* ctx, frt_step_stats* stats) {
+  if (!ctx || !stats) return FRT_ERR_INVALID;
+  Ctl c;
+  CK(cudaStreamSynchronize(ctx->s_main));
+  CK(cudaMemcpy(&c, ctx->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+  fill_stats(ctx, c, stats);
+  return FRT_OK;
+}
+
+frt_status frt_num_rays(frt_ctx* ctx, int box, long long* n) {
+  if (!ctx || !n) return FRT_ERR_INVALID;
+  Ctl c;
+  CK(cudaStreamSynchronize(ctx->s_main));
+  CK(cudaMemcpy(&c, ctx->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+  const int nr = std::min(c.nray[c.cur], ctx->d.ray_cap);
+  if (box < 0) {
+    *n = nr;
+    return FRT_OK;
+  }
+  std::vector<uint16_t> bx(nr);
+  std::vector<uint8_t> dead(nr);
+  if (nr) {
+    CK(cudaMemcpy(bx.data(), ctx->d.pool[c.cur].box, sizeof(uint16_t) * nr, cudaMemcpyDeviceToHost));
+  }
+  long long k = 0;
+  for (int i = 0; i < nr; i++) k += (bx[i] == box);
+  *n = k;
+  return FRT_OK;
+}
+
+frt_status frt_download_rays(frt_ctx* ctx, int box, int16_t* order, int32_t* pixel, uint16_t* itheta, int32_t* cell,
+                             float* geom9, float* nphot) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  Ctl c;
+  CK(cudaStreamSynchronize(ctx->s_main));
+  CK(cudaMemcpy(&c, ctx->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+  const int nr = std::min(c.nray[c.cur], ctx->d.ray_cap);
+  const RayPool& P = ctx->d.pool[c.cur];
+  const int F = ctx->d.F;
+  const size_t cap = (size_t)ctx->d.ray_cap;
+  std::vector<uint16_t> bx(nr), ith(nr);
+  std::vector<int16_t> ord(nr);
+  std::vector<int32_t> pix(nr), cl(nr);
+  std::vector<float> g[9], np((size_t)F * nr);
+  float* gp[9] = {P.xh, P.yh, P.zh, P.r, P.dr, P.x, P.y, P.z, P.time};
+  if (nr) {
+    CK(cudaMemcpy(bx.data(), P.box, sizeof(uint16_t) * nr, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ith.data(), P.itheta, sizeof(uint16_t) * nr, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ord.data(), P.order, sizeof(int16_t) * nr, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(pix.data(), P.pixel, sizeof(int32_t) * nr, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(cl.data(), P.cell, sizeof(int32_t) * nr, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 9; k++) {
+      g[k].resize(nr);
+      CK(cudaMemcpy(g[k].data(), gp[k], sizeof(float) * nr, cudaMemcpyDeviceToHost));
+    }
+    for (int nu = 0; nu < F; nu++)
+      CK(cudaMemcpy(np.data() + (size_t)nu * nr, P.nphot + nu * cap, sizeof(float) * nr, cudaMemcpyDeviceToHost));
+  }
+  size_t w = 0;
+  for (int i = 0; i < nr; i++) {
+    if (bx[i] != box) continue;
+    if (order) order[w] = ord[i];
+    if (pixel) pixel[w] = pix[i];
+    if (itheta) itheta[w] = ith[i];
+    if (cell) cell[w] = cl[i];
+    if (geom9)
+      for (int k = 0; k < 9; k++) geom9[w * 9 + k] = g[k][i];
+    if (nphot)
+      for (int nu = 0; nu < F; nu++) nphot[w * F + nu] = np[(size_t)nu * nr + i];
+    w++;
+  }
+  return FRT_OK;
+}
+
+frt_status frt_box_scalars(frt_ctx* ctx, int box, double* out8) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  if (!out8) return FRT_ERR_INVALID;
+  CK(cudaStreamSynchronize(ctx->s_main));
+  st = download_boxes(ctx);
+  if (st) return st;
+  const BoxP& B = ctx->hbox[box];
+  const double v[8] = {(double)B.t, (double)B.dt, B.nphot_min, B.nphot_max, (double)B.nphot_merge,
+                       (double)B.num_thresh, (double)B.dx, (double)B.dx0};
+  memcpy(out8, v, sizeof v);
+  return FRT_OK;
+}
+
+frt_status frt_last_timing(frt_ctx* ctx, float* step_ms, float* cell_kernel_ms) {
+  if (!ctx) return FRT_ERR_INVALID;
+  if (step_ms) *step_ms = ctx->last_step_ms;
+  if (cell_kernel_ms) *cell_kernel_ms = ctx->last_dark_ms;
+  return FRT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,679 @@
+// Ray geometry kernels: advance through the grid, split, merge, cast, compaction.
+//
+// This translation unit is compiled with -fmad=false: the reference's geometry is float
+// arithmetic (with a few double sub-expressions) whose results decide cell indices, split and
+// merge trees and HEALPix pixels, so every product and sum here is rounded exactly as the
+// reference's g++ build rounds it (no a*b+c contraction). Each kernel cites the reference code
+// whose arithmetic it reproduces.
+#include <math.h>
+
+#include "frt_internal.cuh"
+#include "hp_nest.h"
+
+namespace frt {
+
+namespace {
+
+__device__ __forceinline__ int imod(int a, int b) {
+  while (a < 0) a += b;
+  return a % b;
+}
+
+// Rotation of a unit vector by the precomputed coefficient table: the reference evaluates
+// (c00)*xhat + (c01)*yhat + (c02)*zhat with each coefficient a float product of cosf/sinf
+// values (healpix_funcs.cc:102-143); the host builds those coefficients with the same
+// expressions, the device does the remaining products and sums.
+__device__ __forceinline__ void rot_apply(const float* m, float x, float y, float z, float* ox, float* oy, float* oz) {
+  *ox = (m[0] * x + m[1] * y) + m[2] * z;
+  *oy = (m[3] * x + m[4] * y) + m[5] * z;
+  *oz = (m[6] * x + m[7] * y) + m[8] * z;
+}
+
+__device__ __forceinline__ float sum_nphot(const RayPool& P, int i, int F, int cap) {
+  float s = 0.f;
+  for (int nu = 0; nu < F; nu++) s += P.nphot[(size_t)nu * cap + i];
+  return s;
+}
+
+template <typename T>
+__device__ __forceinline__ T block_sum(T v) {
+  __shared__ T red[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  T r = 0;
+  if (w == 0) {
+    r = (lane < (int)(blockDim.x >> 5)) ? red[lane] : (T)0;
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  }
+  return r;  // valid in thread 0
+}
+
+// Warp-aggregated slot reservation in a counter: every active lane asks for `want` slots.
+__device__ __forceinline__ int reserve(int* counter, int want) {
+  const unsigned mask = __activemask();
+  const int lane = threadIdx.x & 31;
+  int incl = want;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(mask, incl, o);
+    // lanes outside the mask return their own value; only add real predecessors
+    if (lane >= o && ((mask >> (lane - o)) & 1u)) incl += v;
+  }
+  // the shuffle-up above assumes contiguous active lanes; fall back to per-lane atomics otherwise
+  if (mask != 0xffffffffu) return atomicAdd(counter, want);
+  const int total = __shfl_sync(mask, incl, 31);
+  int base = 0;
+  if (lane == 31) base = atomicAdd(counter, total);
+  base = __shfl_sync(mask, base, 31);
+  return base + incl - want;
+}
+
+__device__ __forceinline__ void copy_ray(const RayPool& A, int i, const RayPool& B, int j, int F, int cap) {
+  B.cell[j] = A.cell[i];
+  B.box[j] = A.box[i];
+  B.order[j] = A.order[i];
+  B.pixel[j] = A.pixel[i];
+  B.itheta[j] = A.itheta[i];
+  B.xh[j] = A.xh[i];
+  B.yh[j] = A.yh[i];
+  B.zh[j] = A.zh[i];
+  for (int nu = 0; nu < F; nu++) B.nphot[(size_t)nu * cap + j] = A.nphot[(size_t)nu * cap + i];
+  B.r[j] = A.r[i];
+  B.dr[j] = A.dr[i];
+  B.x[j] = A.x[i];
+  B.y[j] = A.y[i];
+  B.z[j] = A.z[i];
+  B.time[j] = A.time[i];
+}
+
+// ---------------------------------------------------------------------------------------
+// Start of a step: t += dt (main.cc:127), ray_dt of the sources += dt (rt_funcs.cc:163-172),
+// per-step counters to zero, the next pool emptied.
+__global__ void k_step_begin(Dev d) {
+  Ctl* c = d.ctl;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    c->n_lit_prev = c->n_lit;
+    c->n_lit = 0;
+    c->nray[c->cur ^ 1] = 0;
+    // after a capacity error the pools may hold unwritten slots: drop every ray so that no
+    // kernel ever reads an uninitialised record (the error stays latched for the host)
+    if (c->err) c->nray[c->cur] = 0;
+    c->rays_moved = c->crossings = c->split = c->merged = c->killed = c->cast = 0;
+    c->emitted = c->deposited = c->killed_ph = c->overlap = c->in_flight = 0.0;
+  }
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < d.nbox; b += gridDim.x * blockDim.x) d.box[b].t += d.box[b].dt;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < d.nsrc; s += gridDim.x * blockDim.x)
+    d.src_ray_dt[s] += d.box[d.src_box[s]].dt;
+}
+
+// Claim a lit slot for a cell touched by a segment (first toucher wins).
+__device__ __forceinline__ void claim_lit(const Dev& d, long long gc) {
+  if (d.lit_slot[gc] != -1) return;
+  if (atomicCAS(&d.lit_slot[gc], -1, -2) != -1) return;
+  const int s = atomicAdd(&d.ctl->n_lit, 1);
+  if (s < d.lit_cap) {
+    d.l_cell[s] = (int)gc;
+    d.lit_flag[gc] = 1;
+    d.lit_slot[gc] = s;
+  } else {
+    atomicOr(&d.ctl->err, ERR_LIT_CAP);
+  }
+}
+
+// advance_ray (ray_tracing.cc:1222-1512) with c2ray_iter = TRUE and fion = 1 (plain mode):
+// cell-boundary walk over c_sim * time, path segments {cell, dist}, periodic wrap, corner nudge.
+__global__ void __launch_bounds__(256) k_advance(Dev d) {
+  const int cur = d.ctl->cur;
+  const int n = d.ctl->nray[cur];
+  const RayPool A = d.pool[cur];
+  const int cap = d.ray_cap, PL = d.PL;
+  long long cross = 0, moved = 0, killed = 0;
+  double killed_ph = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    d.dead[i] = 0;
+    const BoxP& B = d.box[A.box[i]];
+    const int N = B.n;
+    const int ind = A.cell[i];
+    const int ii = ind / B.nn;
+    const int jj = (ind - ii * B.nn) / N;
+    const int kk = ind - ii * B.nn - jj * N;
+    const float xhat = A.xh[i], yhat = A.yh[i], zhat = A.zh[i];
+    float x0 = A.x[i], y0 = A.y[i], z0 = A.z[i];
+    const float deltat = A.time[i] + B.dt;
+    float dist = B.clight * deltat;
+    const float px = x0 + dist * xhat, py = y0 + dist * yhat, pz = z0 + dist * zhat;
+    const bool mv = (px > B.mv_hi) || (py > B.mv_hi) || (pz > B.mv_hi) || ((double)px < B.mv_lo) ||
+                    ((double)py < B.mv_lo) || ((double)pz < B.mv_lo);
+    if (!mv) {
+      A.time[i] = deltat;
+      d.nseg[i] = 0;
+      continue;
+    }
+    float r0 = A.r[i], dr = A.dr[i];
+    r0 += dist / B.scale;
+    dr -= dist / B.scale;
+    int in = ii, jn = jj, kn = kk, p = 0;
+    float tlast = 0.f, tmin = 0.f;
+    const float clgt = B.clight;
+    const float dxc = B.dx;
+    bool overflow = false;
+    while (tlast < deltat) {
+      float tx, ty, tz;
+      if (xhat > 0.f) tx = (dxc - x0) / xhat / clgt;
+      else if (xhat < 0.f) tx = (float)(-1. * (double)x0 / (double)xhat / (double)clgt);
+      else tx = INFINITY;
+      if (yhat > 0.f) ty = (dxc - y0) / yhat / clgt;
+      else if (yhat < 0.f) ty = (float)(-1. * (double)y0 / (double)yhat / (double)clgt);
+      else ty = INFINITY;
+      if (zhat > 0.f) tz = (dxc - z0) / zhat / clgt;
+      else if (zhat < 0.f) tz = (float)(-1. * (double)z0 / (double)zhat / (double)clgt);
+      else tz = INFINITY;
+      int tag;
+      if ((tx <= ty) && (tx <= tz)) { tmin = tx; tag = 0; }
+      else if ((ty <= tx) && (ty <= tz)) { tmin = ty; tag = 1; }
+      else { tmin = tz; tag = 2; }
+      if ((tlast + tmin) < deltat) {
+        dist = tmin * clgt;
+        if (p >= PL - 1) { overflow = true; break; }
+        const long long gc = B.cell0 + (long long)in * B.nn + jn * N + kn;
+        d.seg[(size_t)p * cap + i] = (int)gc;
+        d.seg_dist[(size_t)p * cap + i] = dist;
+        claim_lit(d, gc);
+        p += 1;
+        x0 += dist * xhat;
+        y0 += dist * yhat;
+        z0 += dist * zhat;
+        if (tag == 0) {
+          if (xhat > 0.f) { in = imod(in + 1, N); x0 = B.lo_edge; }
+          else { in = imod(in - 1, N); x0 = B.hi_edge; }
+        } else if (tag == 1) {
+          if (yhat > 0.f) { jn = imod(jn + 1, N); y0 = B.lo_edge; }
+          else { jn = imod(jn - 1, N); y0 = B.hi_edge; }
+        } else {
+          if (zhat > 0.f) { kn = imod(kn + 1, N); z0 = B.lo_edge; }
+          else { kn = imod(kn - 1, N); z0 = B.hi_edge; }
+        }
+        if (x0 <= 0.f) x0 = B.lo_edge;
+        if ((double)x0 >= B.hi_thr) x0 = B.hi_edge;
+        if (y0 <= 0.f) y0 = B.lo_edge;
+        if ((double)y0 >= B.hi_thr) y0 = B.hi_edge;
+        if (z0 <= 0.f) z0 = B.lo_edge;
+        if ((double)z0 >= B.hi_thr) z0 = B.hi_edge;
+      }
+      tlast += tmin;
+    }
+    if (overflow) {
+      atomicOr(&d.ctl->err, ERR_PATH);
+      d.nseg[i] = 0;
+      d.dead[i] = 1;
+      continue;
+    }
+    dist = (deltat - tlast + tmin) * clgt;
+    dist = (B.lo_edge >= dist) ? B.lo_edge : dist;   // maxd(dist, min_dist*dx)
+    const long long gc = B.cell0 + (long long)in * B.nn + jn * N + kn;
+    d.seg[(size_t)p * cap + i] = (int)gc;
+    d.seg_dist[(size_t)p * cap + i] = dist;
+    claim_lit(d, gc);
+    d.nseg[i] = (uint8_t)(p + 1);
+    x0 += dist * xhat;
+    y0 += dist * yhat;
+    z0 += dist * zhat;
+    if (x0 <= 0.f) x0 = B.lo_edge;
+    if ((double)x0 >= B.hi_thr) x0 = B.hi_edge;
+    if (y0 <= 0.f) y0 = B.lo_edge;
+    if ((double)y0 >= B.hi_thr) y0 = B.hi_edge;
+    if (z0 <= 0.f) z0 = B.lo_edge;
+    if ((double)z0 >= B.hi_thr) z0 = B.hi_edge;
+    A.time[i] = 0.f;
+    A.r[i] = r0;
+    A.dr[i] = dr;
+    A.x[i] = x0;
+    A.y[i] = y0;
+    A.z[i] = z0;
+    A.cell[i] = in * B.nn + jn * N + kn;
+    cross += p + 1;
+    moved += 1;
+    // optional removal beyond rkill (comoving), applied after update_rays
+    if (B.rkill > 0.0 && (double)r0 > B.rkill) {
+      d.dead[i] = 1;
+      killed += 1;
+      killed_ph += (double)sum_nphot(A, i, d.F, cap) * kPhotNorm;
+    }
+  }
+  cross = block_sum(cross);
+  moved = block_sum(moved);
+  killed = block_sum(killed);
+  killed_ph = block_sum(killed_ph);
+  if (threadIdx.x == 0) {
+    if (cross) atomicAdd((unsigned long long*)&d.ctl->crossings, (unsigned long long)cross);
+    if (moved) atomicAdd((unsigned long long*)&d.ctl->rays_moved, (unsigned long long)moved);
+    if (killed) atomicAdd((unsigned long long*)&d.ctl->killed, (unsigned long long)killed);
+    if (killed_ph != 0.0) atomicAdd(&d.ctl->killed_ph, killed_ph);
+  }
+}
+
+// count_rays per box (ray_tracing.cc:35-47) after the C2Ray pass removed rays; then the merge
+// set-up: num_thresh test and histogram reset (main.cc:153-163).
+__global__ void k_count(Dev d) {
+  const int cur = d.ctl->cur;
+  const int n = d.ctl->nray[cur];
+  const RayPool A = d.pool[cur];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (d.dead[i]) continue;
+    const int b = A.box[i];
+    const unsigned m = __match_any_sync(__activemask(), b);
+    if ((int)(threadIdx.x & 31) == __ffs(m) - 1)
+      atomicAdd((unsigned long long*)&d.count[b], (unsigned long long)__popc(m));
+  }
+}
+
+__global__ void k_merge_setup(Dev d) {
+  const int b = blockIdx.x;
+  const bool need = d.count[b] > d.box[b].num_thresh;
+  if (threadIdx.x == 0) d.need_hist[b] = need ? 1 : 0;
+  if (need)
+    for (int k = threadIdx.x; k < kPdfBins; k += blockDim.x) d.hist[(size_t)b * kPdfBins + k] = 0;
+}
+
+// calc_nphot_merge histogram (ray_tracing.cc:193-209)
+__global__ void k_hist(Dev d, const double* lg) {
+  const int cur = d.ctl->cur;
+  const int n = d.ctl->nray[cur];
+  const RayPool A = d.pool[cur];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (d.dead[i]) continue;
+    const int b = A.box[i];
+    if (!d.need_hist[b]) continue;
+    const double lg_min = lg[2 * b], del = lg[2 * b + 1];
+    const float v = (float)((log10f(sum_nphot(A, i, d.F, d.ray_cap)) - lg_min) / del);
+    int pdf_ind = (int)((v >= 0.f) ? v : 0.f);   // maxd(..., 0.)
+    pdf_ind = (pdf_ind >= 9999) ? 9999 : pdf_ind;
+    atomicAdd(&d.hist[(size_t)b * kPdfBins + pdf_ind], 1);
+  }
+}
+
+// threshold scan from the top of the PDF (ray_tracing.cc:211-224), one thread per box
+__global__ void k_merge_thresh(Dev d, const double* lg) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nbox) return;
+  BoxP& B = d.box[b];
+  if (d.need_hist[b]) {
+    const double lg_min = lg[2 * b], del = lg[2 * b + 1];
+    long long cum = 0;
+    float nm = 0.f;
+    for (int k = kPdfBins - 1; k >= 0; --k) {
+      cum += d.hist[(size_t)b * kPdfBins + k];
+      if (cum >= B.num_thresh) {
+        nm = (float)pow(10., k * del + lg_min);
+        break;
+      }
+    }
+    B.nphot_merge = nm;
+  }
+  const float a = (float)(4. * (double)B.nphot_merge), c = (float)(4. * B.nphot_min);
+  B.split_thr = (c >= a) ? c : a;   // maxd(4.*nphot_merge, 4.*nphot_min)
+  if (B.nphot_merge > 0.f) atomicOr(&d.ctl->any_merge, 1);
+}
+
+// l_from_r (ray_tracing.cc:87-95)
+__device__ __forceinline__ int l_from_r(const BoxP& B, float r, double pi_sf_3, double log4) {
+  const double q = (double)(r / B.dx0);
+  int l = (int)ceil(log(pi_sf_3 * (q * q)) / log4);
+  l = (l >= kLmax) ? kLmax : l;
+  const int lmin = B.lm;
+  l = (l >= lmin) ? l : lmin;
+  l = (kLmax >= l) ? l : kLmax;
+  if (r / B.dx0 < 1.) l = lmin;
+  return l;
+}
+
+// merge pass 1 (ray_tracing.cc:336-357): bin candidates by (cell, pixel at l_merge in the frame
+// of this step's random rotation); the smallest pool index in a bin becomes its base ray.
+__global__ void k_merge_bin(Dev d) {
+  if (!d.ctl->any_merge) return;
+  const int cur = d.ctl->cur;
+  const int n = d.ctl->nray[cur];
+  const RayPool A = d.pool[cur];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    d.ray_bin[i] = -1;
+    if (d.dead[i]) continue;
+    const BoxP& B = d.box[A.box[i]];
+    if (!(B.nphot_merge > 0.f)) continue;
+    if (!(sum_nphot(A, i, d.F, d.ray_cap) < B.nphot_merge)) continue;
+    const float* m = d.rot + (size_t)d.itheta_merge[A.box[i]] * 18 + 9;   // inverse rotation
+    float vx, vy, vz;
+    rot_apply(m, A.xh[i], A.yh[i], A.zh[i], &vx, &vy, &vz);
+    const int pix = hpn::vec2pix(B.lm, (double)vx, (double)vy, (double)vz);
+    const int npix = 12 << (2 * B.lm);
+    const long long bin = (B.cell0 + A.cell[i]) * npix + pix;
+    d.ray_bin[i] = (int)bin;
+    atomicMin(&d.bin_base[bin], i);
+  }
+}
+
+// base rays start their photon-weighted sums (ray_tracing.cc:362-377)
+__global__ void k_merge_base(Dev d) {
+  if (!d.ctl->any_merge) return;
+  const int cur = d.ctl->cur;
+  const int n = d.ctl->nray[cur];
+  const RayPool A = d.pool[cur];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int bin = d.ray_bin[i];
+    if (bin < 0 || d.bin_base[bin] != i) continue;
+    const BoxP& B = d.box[A.box[i]];
+    const float nt = sum_nphot(A, i, d.F, d.ray_cap);
+    const float rr = A.r[i] / B.dx0;
+    A.r[i] = (float)((double)rr * (double)rr * (double)nt);
+    A.dr[i] *= nt;
+    A.x[i] *= nt;
+    A.y[i] *= nt;
+    A.z[i] *= nt;
+    A.time[i] *= nt;
+    d.merged_flag[i] = 0;
+  }
+}
+
+// other rays of a bin add their photon-weighted quantities to the base and are removed
+// (ray_tracing.cc:379-402)
+__global__ void k_merge_accum(Dev d) {
+  if (!d.ctl->any_merge) return;
+  const int cur = d.ctl->cur;
+  const int n = d.ctl->nray[cur];
+  const RayPool A = d.pool[cur];
+  const int cap = d.ray_cap;
+  long long merged = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int bin = d.ray_bin[i];
+    if (bin < 0) continue;
+    const int base = d.bin_base[bin];
+    if (base == i) continue;
+    const BoxP& B = d.box[A.box[i]];
+    const float nt = sum_nphot(A, i, d.F, cap);
+    for (int nu = 0; nu < d.F; nu++) atomicAdd(&A.nphot[(size_t)nu * cap + base], A.nphot[(size_t)nu * cap + i]);
+    const float rr = A.r[i] / B.dx0;
+    atomicAdd(&A.r[base], (float)((double)rr * (double)rr * (double)nt));
+    atomicAdd(&A.dr[base], A.dr[i] * nt);
+    atomicAdd(&A.x[base], A.x[i] * nt);
+    atomicAdd(&A.y[base], A.y[i] * nt);
+    atomicAdd(&A.z[base], A.z[i] * nt);
+    atomicAdd(&A.time[base], A.time[i] * nt);
+    d.merged_flag[base] = 1;
+    d.dead[i] = 1;
+    d.ray_bin[i] = -1;
+    merged += 1;
+  }
+  merged = block_sum(merged);
+  if (threadIdx.x == 0 && merged) atomicAdd((unsigned long long*)&d.ctl->merged, (unsigned long long)merged);
+}
+
+// merge pass 2 (ray_tracing.cc:409-476): normalise; bins that merged > 1 ray get the bin's
+// direction, an order from the merged radius, and a pixel at that order.
+__global__ void k_merge_final(Dev d, double pi_sf_3, double log4) {
+  if (!d.ctl->any_merge) return;
+  const int cur = d.ctl->cur;
+  const int n = d.ctl->nray[cur];
+  const RayPool A = d.pool[cur];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int bin = d.ray_bin[i];
+    if (bin < 0) continue;
+    d.ray_bin[i] = -1;
+    const int b = A.box[i];
+    const BoxP& B = d.box[b];
+    const float nt = sum_nphot(A, i, d.F, d.ray_cap);
+    float r = A.r[i] / nt;
+    r = (float)sqrt((double)r);
+    r *= B.dx0;
+    float dr = A.dr[i] / nt;
+    A.x[i] /= nt;
+    A.y[i] /= nt;
+    A.z[i] /= nt;
+    A.time[i] /= nt;
+    if (d.merged_flag[i]) {
+      const int npix = 12 << (2 * B.lm);
+      const int pix = bin % npix;
+      double vx, vy, vz;
+      hpn::pix2vec(B.lm, pix, &vx, &vy, &vz);
+      const uint16_t ith = d.itheta_merge[b];
+      A.itheta[i] = ith;
+      const int order = l_from_r(B, r, pi_sf_3, log4);
+      const float rmin = B.rmin[order], rmax = B.rmax[order];
+      const float cand = rmax - dr;
+      r = (rmin >= cand) ? rmin : cand;    // maxd(rmax - dr, rmin)
+      dr = rmax - r;
+      A.order[i] = (int16_t)order;
+      const int pixel = hpn::vec2pix(order, vx, vy, vz);
+      A.pixel[i] = pixel;
+      hpn::pix2vec(order, pixel, &vx, &vy, &vz);
+      float ox, oy, oz;
+      rot_apply(d.rot + (size_t)ith * 18, (float)vx, (float)vy, (float)vz, &ox, &oy, &oz);
+      A.xh[i] = ox;
+      A.yh[i] = oy;
+      A.zh[i] = oz;
+      d.merged_flag[i] = 0;
+    }
+    A.r[i] = r;
+    A.dr[i] = dr;
+    d.bin_base[bin] = 0x7fffffff;
+  }
+}
+
+// split_rays + split_ray (rt_funcs.cc:211-237, ray_tracing.cc:482-619) fused with the
+// compaction into the next pool: live rays are copied, rays past rmax(l) become 4 children
+// at pixels 4*pn + n of order l+1, displaced by (v_child - v_parent) r0 dx/dx0.
+__global__ void __launch_bounds__(256) k_split_compact(Dev d) {
+  const int cur = d.ctl->cur;
+  const int nxt = cur ^ 1;
+  const int n = d.ctl->nray[cur];
+  const RayPool A = d.pool[cur];
+  const RayPool Bp = d.pool[nxt];
+  const int cap = d.ray_cap, F = d.F;
+  long long nsplit = 0;
+  double inflight = 0.0;
+  for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+    const int i = i0 + threadIdx.x;
+    bool live = (i < n) && !d.dead[i];
+    bool split = false;
+    const BoxP* Bx = nullptr;
+    if (live) {
+      Bx = &d.box[A.box[i]];
+      const int l = A.order[i];
+      split = (A.r[i] > Bx->rmax[l]) && (l < kLmax) && (sum_nphot(A, i, F, cap) > Bx->split_thr);
+    }
+    const int want = live ? (split ? 4 : 1) : 0;
+    const int pos = reserve(&d.ctl->nray[nxt], want);
+    if (!live) continue;
+    if (pos + want > cap) {
+      atomicOr(&d.ctl->err, ERR_RAY_CAP);
+      continue;
+    }
+    if (!split) {
+      copy_ray(A, i, Bp, pos, F, cap);
+      inflight += (double)sum_nphot(A, i, F, cap);
+      continue;
+    }
+    const BoxP& B = *Bx;
+    nsplit += 1;
+    const int N = B.n;
+    const int l = A.order[i];
+    const int pn = A.pixel[i];
+    const float r0 = A.r[i], x0o = A.x[i], y0o = A.y[i], z0o = A.z[i], time = A.time[i];
+    const uint16_t ith = A.itheta[i];
+    const float* m = d.rot + (size_t)ith * 18;
+    const double vox = A.xh[i], voy = A.yh[i], voz = A.zh[i];
+    const int ind = A.cell[i];
+    const int ic = ind / B.nn, jc = (ind - ic * B.nn) / N, kc = ind - ic * B.nn - jc * N;
+    const float rmax = B.rmax[l + 1];
+    const float rs = r0 * B.scale;
+    for (int c = 0; c < 4; c++) {
+      const int j = pos + c;
+      const int pix = 4 * pn + c;
+      double vx, vy, vz;
+      hpn::pix2vec(l + 1, pix, &vx, &vy, &vz);
+      float nx, ny, nz;
+      rot_apply(m, (float)vx, (float)vy, (float)vz, &nx, &ny, &nz);
+      float x0 = (float)((double)x0o + ((double)nx - vox) * (double)rs);
+      float y0 = (float)((double)y0o + ((double)ny - voy) * (double)rs);
+      float z0 = (float)((double)z0o + ((double)nz - voz) * (double)rs);
+      int icn = ic, jcn = jc, kcn = kc;
+      for (int g = 0; g < 64 && x0 > B.dx; g++) { x0 -= B.dx; icn = imod(icn + 1, N); }
+      for (int g = 0; g < 64 && x0 < 0.f; g++) { x0 += B.dx; icn = imod(icn - 1, N); }
+      for (int g = 0; g < 64 && y0 > B.dx; g++) { y0 -= B.dx; jcn = imod(jcn + 1, N); }
+      for (int g = 0; g < 64 && y0 < 0.f; g++) { y0 += B.dx; jcn = imod(jcn - 1, N); }
+      for (int g = 0; g < 64 && z0 > B.dx; g++) { z0 -= B.dx; kcn = imod(kcn + 1, N); }
+      for (int g = 0; g < 64 && z0 < 0.f; g++) { z0 += B.dx; kcn = imod(kcn - 1, N); }
+      Bp.cell[j] = icn * B.nn + jcn * N + kcn;
+      Bp.box[j] = A.box[i];
+      Bp.order[j] = (int16_t)(l + 1);
+      Bp.pixel[j] = pix;
+      Bp.itheta[j] = ith;
+      Bp.xh[j] = nx;
+      Bp.yh[j] = ny;
+      Bp.zh[j] = nz;
+      float s = 0.f;
+      for (int nu = 0; nu < F; nu++) {
+        const float q = (float)((double)A.nphot[(size_t)nu * cap + i] / 4.);
+        Bp.nphot[(size_t)nu * cap + j] = q;
+        s += q;
+      }
+      inflight += (double)s;
+      Bp.r[j] = r0;
+      Bp.dr[j] = rmax - r0;
+      Bp.x[j] = x0;
+      Bp.y[j] = y0;
+      Bp.z[j] = z0;
+      Bp.time[j] = time;
+    }
+  }
+  nsplit = block_sum(nsplit);
+  inflight = block_sum(inflight);
+  if (threadIdx.x == 0) {
+    if (nsplit) atomicAdd((unsigned long long*)&d.ctl->split, (unsigned long long)nsplit);
+    if (inflight != 0.0) atomicAdd(&d.ctl->in_flight, inflight * kPhotNorm);
+  }
+}
+
+__global__ void k_swap(Dev d) {
+  Ctl* c = d.ctl;
+  const int nxt = c->cur ^ 1;
+  const int n = c->nray[nxt];
+  c->nray[nxt] = c->err ? 0 : ((n > d.ray_cap) ? d.ray_cap : n);
+  c->nray[c->cur] = 0;
+  c->cur = nxt;
+}
+
+// new_rays -> init_rays (rt_funcs.cc:240-261, ray_tracing.cc:230-321): 12 Nside^2 rays per source
+// at the cell centre, directions of the NEST pixels rotated by the source's random angles.
+__global__ void k_cast(Dev d) {
+  const int cur = d.ctl->cur;
+  const RayPool A = d.pool[cur];
+  const int cap = d.ray_cap, F = d.F;
+  long long ncast = 0;
+  double emitted = 0.0;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < d.nsrc; s += gridDim.x * blockDim.x) {
+    const int b = d.src_box[s];
+    const BoxP& B = d.box[b];
+    const int c = d.src_cell[s];
+    const long long gc = B.cell0 + c;
+    int nside = 1, lpix = 0;
+    if (!(d.nH1[gc] / d.nH[gc] > 0.1)) {
+      nside = 1 << B.lsource;
+      lpix = B.lsource;
+    }
+    const int count = 12 * nside * nside;
+    const int pos = atomicAdd(&d.ctl->nray[cur], count);
+    if (pos + count > cap) {
+      atomicOr(&d.ctl->err, ERR_RAY_CAP);
+      continue;
+    }
+    const uint16_t ith = d.src_itheta[s];
+    const float* m = d.rot + (size_t)ith * 18;
+    const double lum = d.src_lum[s];
+    const float rdt = d.src_ray_dt[s];
+    float np[FRT_MAX_FREQ];
+    double tot = 0.0;
+    for (int nu = 0; nu < F; nu++) {
+      np[nu] = (float)((double)d.spectrum[nu] * lum * (double)rdt / 12. / (double)(nside * nside) / kPhotNorm);
+      tot += (double)np[nu];
+    }
+    for (int p = 0; p < count; p++) {
+      const int j = pos + p;
+      double vx, vy, vz;
+      hpn::pix2vec(lpix, p, &vx, &vy, &vz);
+      float ox, oy, oz;
+      rot_apply(m, (float)vx, (float)vy, (float)vz, &ox, &oy, &oz);
+      A.cell[j] = c;
+      A.box[j] = (uint16_t)b;
+      A.order[j] = (int16_t)lpix;
+      A.pixel[j] = p;
+      A.itheta[j] = ith;
+      A.xh[j] = ox;
+      A.yh[j] = oy;
+      A.zh[j] = oz;
+      for (int nu = 0; nu < F; nu++) A.nphot[(size_t)nu * cap + j] = np[nu];
+      A.r[j] = 0.f;
+      A.dr[j] = B.rmax[lpix] - 0.f;
+      A.x[j] = B.dx_half;
+      A.y[j] = B.dx_half;
+      A.z[j] = B.dx_half;
+      A.time[j] = 0.f;
+    }
+    d.src_ray_dt[s] = 0.f;
+    ncast += count;
+    emitted += tot * count;
+  }
+  ncast = block_sum(ncast);
+  emitted = block_sum(emitted);
+  if (threadIdx.x == 0) {
+    if (ncast) atomicAdd((unsigned long long*)&d.ctl->cast, (unsigned long long)ncast);
+    if (emitted != 0.0) {
+      atomicAdd(&d.ctl->emitted, emitted * kPhotNorm);
+      atomicAdd(&d.ctl->in_flight, emitted * kPhotNorm);
+    }
+  }
+}
+
+__global__ void k_fill_i32(int* p, int v, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+}  // namespace
+
+// ---- launchers ------------------------------------------------------------------------------
+void launch_step_begin(const Dev& d, cudaStream_t s) { k_step_begin<<<grid_for(d.nsrc + 1, 256, 1184), 256, 0, s>>>(d); }
+
+void launch_advance(const Dev& d, int grid, cudaStream_t s) { k_advance<<<grid, 256, 0, s>>>(d); }
+
+void launch_count(const Dev& d, int grid, cudaStream_t s) {
+  cudaMemsetAsync(d.count, 0, sizeof(long long) * d.nbox, s);
+  k_count<<<grid, 256, 0, s>>>(d);
+}
+
+void launch_merge(const Dev& d, int grid, cudaStream_t s) {
+  k_merge_setup<<<d.nbox, 256, 0, s>>>(d);
+  k_hist<<<grid, 256, 0, s>>>(d, d.lg);
+  k_merge_thresh<<<grid_for(d.nbox, 128, 1024), 128, 0, s>>>(d, d.lg);
+  if (d.bin_base) {
+    k_merge_bin<<<grid, 256, 0, s>>>(d);
+    k_merge_base<<<grid, 256, 0, s>>>(d);
+    k_merge_accum<<<grid, 256, 0, s>>>(d);
+    k_merge_final<<<grid, 256, 0, s>>>(d, d.pi_sf_3, d.log4);
+  }
+}
+
+void launch_split_compact(const Dev& d, int grid, cudaStream_t s) {
+  k_split_compact<<<grid, 256, 0, s>>>(d);
+  k_swap<<<1, 1, 0, s>>>(d);
+}
+
+void launch_cast(const Dev& d, cudaStream_t s) {
+  if (d.nsrc > 0) k_cast<<<grid_for(d.nsrc, 128, 4096), 128, 0, s>>>(d);
+}
+
+void launch_fill_i32(int* p, int v, long long n, cudaStream_t s) {
+  k_fill_i32<<<grid_for(n, 256, 4096), 256, 0, s>>>(p, v, n);
+}
+
+}  // namespace frt

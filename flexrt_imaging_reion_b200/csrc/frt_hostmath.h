@@ -1,0 +1,21 @@
+// Host-side set-up arithmetic (frt_hostmath.cc, compiled by g++ with -ffp-contract=off).
+#pragma once
+#include "../../include/flexrt.h"
+#include "frt_params.h"
+
+namespace frt {
+namespace host {
+
+struct GasInit {  // caller-owned arrays of n^3 floats
+  float *rho, *nH, *nHe, *nH1, *nHe1, *f_H1, *f_He1, *temp, *ne, *n_tot, *rec_h2, *rec_he2, *dne_dt;
+};
+
+void rotation_table(float* out);  // kNtheta x 18 floats (forward, inverse)
+void box_params(BoxP* B, const frt_config* cfg, const frt_box_desc* bd, long long cell0);
+void init_gas(const frt_config* cfg, const frt_box_desc* bd, const float* delta1, GasInit* g);
+void nphot_min_max(const frt_config* cfg, const BoxP* B, int nsrc, const double* lum, double* nmin, double* nmax);
+void derived_constants(const frt_config* cfg, double* sigH1, double* sigHe1, double* sig0, double* sig912,
+                       double* pi_sf_3, double* log4);
+
+}  // namespace host
+}  // namespace frt

@@ -1,0 +1,126 @@
+// Device-side data layout of an RT context and the kernel launchers shared by the .cu files.
+//
+// HBM layout (all structure-of-arrays, 4-byte fields unless noted):
+//  * dense cell state, one entry per cell of every box; boxes are concatenated, each starting
+//    on a 1024-cell tile boundary (tile -> box table), cells in C order (i, j, k) with k fastest
+//    like the reference's [Nx][Ny][Nz] arrays;
+//  * a compact list of the cells touched by a ray segment in the current step ("lit" cells)
+//    with the per-iteration C2Ray state of just those cells, so that the 5 C2Ray iterations
+//    only revisit lit cells while all other cells do their whole step in one streaming pass;
+//  * two ray pools (the current one and the one the next step compacts into) indexed by ray,
+//    plus the per-step path segments [path_length][capacity];
+//  * a control block with the pool counts, lit count, error word and per-step totals.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/flexrt.h"
+#include "frt_physics.cuh"
+
+namespace frt {
+
+
+enum : unsigned { ERR_RAY_CAP = 1u, ERR_PATH = 2u, ERR_LIT_CAP = 4u, ERR_BIN = 8u };
+
+struct RayPool {
+  int* cell;          // local cell index (path[0].ind)
+  uint16_t* box;
+  int16_t* order;
+  int* pixel;
+  uint16_t* itheta;
+  float *xh, *yh, *zh;
+  float* nphot;       // [F][cap]
+  float *r, *dr, *x, *y, *z, *time;
+};
+
+struct Ctl {
+  int nray[2];             // live rays in pool 0 / 1
+  int cur;                 // current pool
+  int n_lit;               // lit cells this step
+  int n_lit_prev;
+  unsigned err;
+  int any_merge;           // some box has nphot_merge > 0
+  int pad;
+  long long rays_moved, crossings, split, merged, killed, cast;
+  double emitted, deposited, killed_ph, overlap, in_flight;
+};
+
+struct Dev {
+  // sizes
+  int nbox, F, PL, itercount, hpx_lvl;
+  int ray_cap, lit_cap, src_cap, nsrc;
+  long long ncell_total, ntile;
+  int outputs;             // FRT_OUT_*
+  float nhe_to_nh;
+  float const_clump;
+  // per-box
+  BoxP* box;
+  long long* count;        // live rays per box (count_rays)
+  int* need_hist;          // per box
+  int* hist;               // [nbox][kPdfBins]
+  uint16_t* itheta_merge;  // per box
+  double* lg;              // per box (log10 nphot_min, PDF bin width) for calc_nphot_merge
+  double pi_sf_3, log4;    // pi*safety_factor/3. and log(4.) (l_from_r, ray_tracing.cc:89)
+  // spectrum constants
+  float spectrum[FRT_MAX_FREQ];
+  double sigH1_d[FRT_MAX_FREQ], sigHe1_d[FRT_MAX_FREQ];
+  float sigH1_f[FRT_MAX_FREQ], sigHe1_f[FRT_MAX_FREQ];
+  double sigH1_0, sigH1_912;
+  // tables
+  const float* rot;        // [kNtheta][2][9] forward, inverse
+  // dense cells
+  int16_t* tile_box;
+  float *nH, *nHe, *nH1, *nHe1, *f_H1, *f_He1, *temp, *clump, *ne, *heat, *cool, *avg_nh1, *avg_nhe1, *treion;
+  uint8_t *treion_flag, *lit_flag;
+  int* lit_slot;
+  float *nH1_prev, *n_tot, *dne_dt;                              // unfused path
+  float *rec_h2, *rec_he2, *recrate_h2, *recrate_he2, *mfp, *mfp912, *if_speed, *inc_flux;  // diag
+  // lit cells
+  int* l_cell;
+  float *l_nh, *l_nhe, *l_y0h, *l_y0he, *l_crec_h, *l_crec_he, *l_rec_h2, *l_rec_he2;
+  float *l_avg_h, *l_avg_he, *l_nh1_old, *l_acc_g, *l_acc_ghe;
+  float *l_acc_nu_h, *l_acc_nu_he, *l_ngam;   // [F][lit_cap]
+  // rays
+  RayPool pool[2];
+  int* seg;                // [PL][ray_cap]
+  float* seg_dist;         // [PL][ray_cap]
+  uint8_t* nseg;
+  uint8_t* dead;
+  int* ray_bin;            // merge bin of a candidate or -1
+  uint8_t* merged_flag;
+  int* bin_base;           // [ncell_total * 12*4^lm] or NULL when merging is unreachable
+  // sources
+  int* src_cell;           // local cell
+  uint16_t* src_box;
+  double* src_lum;
+  float* src_ray_dt;
+  uint16_t* src_itheta;
+  // control
+  Ctl* ctl;
+};
+
+inline __host__ __device__ int grid_for(long long n, int block, int maxblocks) {
+  long long g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > maxblocks) g = maxblocks;
+  return (int)g;
+}
+
+// ---- launchers (frt_geom.cu) ----------------------------------------------------------
+void launch_step_begin(const Dev& d, cudaStream_t s);
+void launch_advance(const Dev& d, int grid, cudaStream_t s);
+void launch_count(const Dev& d, int grid, cudaStream_t s);
+void launch_merge(const Dev& d, int grid, cudaStream_t s);
+void launch_split_compact(const Dev& d, int grid, cudaStream_t s);
+void launch_cast(const Dev& d, cudaStream_t s);
+void launch_fill_i32(int* p, int v, long long n, cudaStream_t s);
+// ---- launchers (frt_phys.cu) ----------------------------------------------------------
+void launch_lit_init(const Dev& d, bool strict, int grid, cudaStream_t s);
+void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t s);
+void launch_litpass(const Dev& d, int iter, bool strict, bool fused_thermal, int grid, cudaStream_t s);
+void launch_dark(const Dev& d, bool strict, bool fused_thermal, int grid, cudaStream_t s);
+void launch_thermal_all(const Dev& d, bool strict, int grid, cudaStream_t s);
+void launch_clear_lit(const Dev& d, int grid, cudaStream_t s);
+void launch_gather_sparse(const Dev& d, long long cell0, long long ncell, int which, float* out, cudaStream_t s);
+
+}  // namespace frt

@@ -1,0 +1,586 @@
+// Physics kernels of the RT step: the C2Ray iteration (ray pass with Gamma deposition and the
+// cell update, ray_tracing.cc:623-1216) and the thermal update (gas_funcs.cc:362-457).
+//
+// Work split. A cell that no ray segment touches in a step receives Gamma = 0 in all C2Ray
+// iterations, so its whole step -- 5 C2Ray updates, the last-iteration bookkeeping and the
+// sub-cycled thermal update -- depends only on its own state. k_dark does that whole step for
+// every such cell in one streaming pass over HBM (read the state once, write it once). Cells
+// touched by at least one segment ("lit") are gathered into a compact list; only they go
+// through the iteration with the ray passes in between (k_lit_init, k_raypass, k_litpass).
+// Both paths call the same per-cell device functions (frt_physics.cuh), so a cell gets the same
+// arithmetic whichever path handles it.
+#include <math.h>
+
+#include "frt_internal.cuh"
+
+namespace frt {
+
+namespace {
+
+template <typename T>
+__device__ __forceinline__ T block_sum(T v) {
+  __shared__ T red[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  T r = 0;
+  if (w == 0) {
+    r = (lane < (int)(blockDim.x >> 5)) ? red[lane] : (T)0;
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  }
+  return r;
+}
+
+__device__ __forceinline__ int box_of_cell(const Dev& d, long long gc) { return d.tile_box[gc >> kTileShift]; }
+
+// ---- clear the previous step's lit marks ------------------------------------------------
+__global__ void k_clear_lit(Dev d) {
+  const int n = min(d.ctl->n_lit, d.lit_cap);
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const int gc = d.l_cell[s];
+    d.lit_flag[gc] = 0;
+    d.lit_slot[gc] = -1;
+  }
+}
+
+// ---- iteration-0 set-up of the lit cells (ray_tracing.cc:630-697, iter == 0) --------------
+template <bool STRICT>
+__global__ void k_lit_init(Dev d) {
+  const int n = min(d.ctl->n_lit, d.lit_cap);
+  const int F = d.F, L = d.lit_cap;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const int gc = d.l_cell[s];
+    const float temp = d.temp[gc];
+    float rh, rhe;
+    recomb_coeffs<STRICT>(temp, &rh, &rhe);
+    const float cl = d.clump ? d.clump[gc] : d.const_clump;
+    d.l_nh[s] = d.nH[gc];
+    d.l_nhe[s] = d.nHe[gc];
+    d.l_y0h[s] = d.f_H1[gc];
+    d.l_y0he[s] = d.f_He1[gc];
+    d.l_rec_h2[s] = rh;
+    d.l_rec_he2[s] = rhe;
+    d.l_crec_h[s] = cl * rh;
+    d.l_crec_he[s] = cl * rhe;
+    const float nh1 = d.nH1[gc];
+    d.l_avg_h[s] = nh1;
+    d.l_nh1_old[s] = nh1;
+    d.l_avg_he[s] = d.nHe1[gc];
+    d.l_acc_g[s] = 0.f;
+    d.l_acc_ghe[s] = 0.f;
+    for (int nu = 0; nu < F; nu++) {
+      d.l_acc_nu_h[(size_t)nu * L + s] = 0.f;
+      d.l_acc_nu_he[(size_t)nu * L + s] = 0.f;
+      d.l_ngam[(size_t)nu * L + s] = 0.f;
+    }
+  }
+}
+
+// ---- ray pass of one C2Ray iteration (ray_tracing.cc:701-938), plain mode ------------------
+// One thread per moved ray walks its stored segments, attenuates the photon count per bin with
+// the current time-averaged neutral densities of the lit cells, and deposits Gamma_HI / HeI.
+// FIRST converts the segment cell indices to lit slots; LAST also writes per-bin rates, the new
+// photon counts and removes rays below nphot_min.
+template <bool STRICT, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(256) k_raypass(Dev d) {
+  const int cur = d.ctl->cur;
+  const int n = d.ctl->nray[cur];
+  const RayPool A = d.pool[cur];
+  const int cap = d.ray_cap, F = d.F, L = d.lit_cap;
+  double dep = 0.0, kil = 0.0, ovl = 0.0;
+  long long nkill = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int ns = d.nseg[i];
+    if (ns == 0 || d.dead[i]) continue;
+    const BoxP& B = d.box[A.box[i]];
+    const double nmin = B.nphot_min;
+    float nph[FRT_MAX_FREQ];
+#pragma unroll
+    for (int nu = 0; nu < FRT_MAX_FREQ; nu++) nph[nu] = (nu < F) ? A.nphot[(size_t)nu * cap + i] : 0.f;
+    bool dumped = false;
+    unsigned dump_mask = 0;
+    if (STRICT) {
+      double tau_h1[FRT_MAX_FREQ], tau_he1[FRT_MAX_FREQ];
+#pragma unroll
+      for (int nu = 0; nu < FRT_MAX_FREQ; nu++) { tau_h1[nu] = 0.; tau_he1[nu] = 0.; }
+      const double dt = B.dt, vol = B.vol;
+      for (int p = 0; p < ns; p++) {
+        int slot = d.seg[(size_t)p * cap + i];
+        if (FIRST) {
+          slot = d.lit_slot[slot];
+          d.seg[(size_t)p * cap + i] = slot;
+        }
+        if (slot < 0) continue;
+        const float dist = d.seg_dist[(size_t)p * cap + i];
+        const float a = d.l_avg_h[slot], b = d.l_avg_he[slot];
+        double dth[FRT_MAX_FREQ], dthe[FRT_MAX_FREQ], nin[FRT_MAX_FREQ];
+        double total = 0.;
+#pragma unroll
+        for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
+          if (nu >= F) continue;
+          dth[nu] = a * d.sigH1_d[nu] * dist;
+          dthe[nu] = b * d.sigHe1_d[nu] * dist;
+          nin[nu] = (nph[nu] * kPhotNorm) * exp(-tau_h1[nu] - tau_he1[nu]);
+          total += nin[nu] / kPhotNorm;
+        }
+        const bool dump = total < nmin;
+#pragma unroll
+        for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
+          if (nu >= F) continue;
+          double fh = 0., fhe = 0.;
+          if ((dth[nu] > 0.) || (dthe[nu] > 0.)) {
+            const double den = (1. - exp(-dth[nu])) * exp(-dthe[nu]) + (1. - exp(-dthe[nu])) * exp(-dth[nu]);
+            fh = (1. - exp(-dth[nu])) * exp(-dthe[nu]) / den;
+            fhe = (1. - exp(-dthe[nu])) * exp(-dth[nu]) / den;
+          }
+          const double absb = dump ? 1.0 : (1. - exp(-dth[nu] - dthe[nu]));
+          const float gh = (float)(fh * nin[nu] * absb / dt / vol / a);
+          const float ghe = (float)(fhe * nin[nu] * absb / dt / vol / b);
+          atomicAdd(&d.l_acc_g[slot], gh);
+          atomicAdd(&d.l_acc_ghe[slot], ghe);
+          if (LAST) {
+            atomicAdd(&d.l_ngam[(size_t)nu * L + slot], (float)(nin[nu] / kPhotNorm));
+            atomicAdd(&d.l_acc_nu_h[(size_t)nu * L + slot], gh);
+            atomicAdd(&d.l_acc_nu_he[(size_t)nu * L + slot], ghe);
+            dep += (fh + fhe) * nin[nu] * absb / kPhotNorm;
+            if (dump && (fh + fhe) > 0.) dump_mask |= 1u << nu;
+          }
+          tau_h1[nu] += dth[nu];
+          tau_he1[nu] += dthe[nu];
+        }
+        if (dump) { dumped = true; break; }
+      }
+      if (LAST) {
+        float s = 0.f;
+        for (int nu = 0; nu < F; nu++) {
+          nph[nu] = (float)((nph[nu] * kPhotNorm) * exp(-tau_h1[nu] - tau_he1[nu]) / kPhotNorm);
+          A.nphot[(size_t)nu * cap + i] = nph[nu];
+          s += nph[nu];
+        }
+        if (!(s > nmin)) {
+          d.dead[i] = 1;
+          nkill += 1;
+          kil += (double)s;
+          if (dumped)
+            for (int nu = 0; nu < F; nu++)
+              if (dump_mask & (1u << nu)) ovl += (double)nph[nu];
+        }
+      }
+    } else {
+      float tau[FRT_MAX_FREQ];
+#pragma unroll
+      for (int nu = 0; nu < FRT_MAX_FREQ; nu++) tau[nu] = 0.f;
+      const double kdep = B.kdep;
+      for (int p = 0; p < ns; p++) {
+        int slot = d.seg[(size_t)p * cap + i];
+        if (FIRST) {
+          slot = d.lit_slot[slot];
+          d.seg[(size_t)p * cap + i] = slot;
+        }
+        if (slot < 0) continue;
+        const float dist = d.seg_dist[(size_t)p * cap + i];
+        const float a = d.l_avg_h[slot], b = d.l_avg_he[slot];
+        float nin[FRT_MAX_FREQ], dtt[FRT_MAX_FREQ];
+        float total = 0.f;
+#pragma unroll
+        for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
+          nin[nu] = (nu < F) ? nph[nu] * expf(-tau[nu]) : 0.f;
+          total += nin[nu];
+        }
+        const bool dump = (double)total < nmin;
+        float gsum_h = 0.f, gsum_he = 0.f;
+        float gh_nu[FRT_MAX_FREQ], ghe_nu[FRT_MAX_FREQ];
+#pragma unroll
+        for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
+          gh_nu[nu] = 0.f;
+          ghe_nu[nu] = 0.f;
+          dtt[nu] = 0.f;
+          if (nu >= F) continue;
+          const float dth = (a * d.sigH1_f[nu]) * dist;
+          const float dthe = (b * d.sigHe1_f[nu]) * dist;
+          dtt[nu] = dth + dthe;
+          if ((dth > 0.f) || (dthe > 0.f)) {
+            const float ah = -expm1f(-dth), ahe = -expm1f(-dthe);
+            const float eh = expf(-dth), ehe = expf(-dthe);
+            const float x1 = ah * ehe, x2 = ahe * eh;
+            const float inv = 1.0f / (x1 + x2);
+            const float absb = dump ? 1.0f : -expm1f(-dtt[nu]);
+            const float q = nin[nu] * absb;
+            gh_nu[nu] = (x1 * inv) * q;
+            ghe_nu[nu] = (x2 * inv) * q;
+            gsum_h += gh_nu[nu];
+            gsum_he += ghe_nu[nu];
+            if (LAST && dump) dump_mask |= 1u << nu;
+          }
+        }
+        const double wh = kdep / (double)a, whe = kdep / (double)b;
+        if (gsum_h != 0.f) atomicAdd(&d.l_acc_g[slot], (float)((double)gsum_h * wh));
+        if (gsum_he != 0.f) atomicAdd(&d.l_acc_ghe[slot], (float)((double)gsum_he * whe));
+        if (LAST) {
+#pragma unroll
+          for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
+            if (nu >= F) continue;
+            atomicAdd(&d.l_ngam[(size_t)nu * L + slot], nin[nu]);
+            if (gh_nu[nu] != 0.f) atomicAdd(&d.l_acc_nu_h[(size_t)nu * L + slot], (float)((double)gh_nu[nu] * wh));
+            if (ghe_nu[nu] != 0.f) atomicAdd(&d.l_acc_nu_he[(size_t)nu * L + slot], (float)((double)ghe_nu[nu] * whe));
+          }
+          dep += (double)gsum_h + (double)gsum_he;
+        }
+#pragma unroll
+        for (int nu = 0; nu < FRT_MAX_FREQ; nu++) tau[nu] += dtt[nu];
+        if (dump) { dumped = true; break; }
+      }
+      if (LAST) {
+        float s = 0.f;
+        for (int nu = 0; nu < F; nu++) {
+          nph[nu] = nph[nu] * expf(-tau[nu]);
+          A.nphot[(size_t)nu * cap + i] = nph[nu];
+          s += nph[nu];
+        }
+        if (!((double)s > nmin)) {
+          d.dead[i] = 1;
+          nkill += 1;
+          kil += (double)s;
+          if (dumped)
+            for (int nu = 0; nu < F; nu++)
+              if (dump_mask & (1u << nu)) ovl += (double)nph[nu];
+        }
+      }
+    }
+  }
+  if (LAST) {
+    dep = block_sum(dep);
+    kil = block_sum(kil);
+    ovl = block_sum(ovl);
+    nkill = block_sum(nkill);
+    if (threadIdx.x == 0) {
+      if (dep != 0.0) atomicAdd(&d.ctl->deposited, dep * kPhotNorm);
+      if (kil != 0.0) atomicAdd(&d.ctl->killed_ph, kil * kPhotNorm);
+      if (ovl != 0.0) atomicAdd(&d.ctl->overlap, ovl * kPhotNorm);
+      if (nkill) atomicAdd((unsigned long long*)&d.ctl->killed, (unsigned long long)nkill);
+    }
+  }
+}
+
+// ---- the last-iteration bookkeeping of one cell (ray_tracing.cc:1116-1209) -----------------
+struct Final {
+  float nH1, nHe1, nH2, nHe2, ne, n_tot, dne_dt, f_H1, f_He1, f_H2;
+  bool set_treion;
+};
+
+__device__ __forceinline__ Final finalize(float nH, float nHe, float nh1_end, float nhe1_end, float avg_h, float ne_old,
+                                          float dt, bool flag) {
+  Final f;
+  f.nH1 = nh1_end;
+  f.nH2 = nH - f.nH1;
+  f.nHe1 = nhe1_end;
+  f.nHe2 = nHe - f.nHe1;
+  f.set_treion = (avg_h / nH < 0.5) && !flag;
+  f.ne = (float)((double)(f.nH2 + f.nHe2) + 2. * 0.0);
+  f.dne_dt = (-ne_old + f.ne) / dt;
+  f.n_tot = nH + nHe + f.ne;
+  f.f_H2 = f.nH2 / nH;
+  f.f_H1 = f.nH1 / nH;
+  f.f_He1 = f.nHe1 / nHe;
+  return f;
+}
+
+// ---- cell pass of one C2Ray iteration over the lit cells ----------------------------------
+template <bool STRICT, bool LAST, bool THERMAL>
+__global__ void __launch_bounds__(256) k_litpass(Dev d) {
+  const int n = min(d.ctl->n_lit, d.lit_cap);
+  const int L = d.lit_cap;
+  const bool diag = d.outputs == FRT_OUT_DIAG;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const int gc = d.l_cell[s];
+    const BoxP& B = d.box[box_of_cell(d, gc)];
+    const float dt = B.dt;
+    const float g = d.l_acc_g[s], ghe = d.l_acc_ghe[s];
+    const float a_prev = d.l_avg_h[s], b_prev = d.l_avg_he[s];
+    const float nH = d.l_nh[s], nHe = d.l_nhe[s];
+    const float nelec_f = nH - a_prev + nHe - b_prev;
+    const double nelec_d = (double)nelec_f;
+    const C2Species H{nH, d.l_y0h[s], d.l_crec_h[s]};
+    const C2Species He{nHe, d.l_y0he[s], d.l_crec_he[s]};
+    float nh1_end = 0.f, nhe1_end = 0.f;
+    const float a_new = c2ray_species<STRICT>(H, g, nelec_d, nelec_f, a_prev, dt, LAST, &nh1_end);
+    const float b_new = c2ray_species<STRICT>(He, ghe, nelec_d, nelec_f, b_prev, dt, LAST, &nhe1_end);
+    if (!LAST) {
+      d.l_avg_h[s] = a_new;
+      d.l_avg_he[s] = b_new;
+      d.l_acc_g[s] = 0.f;
+      d.l_acc_ghe[s] = 0.f;
+      continue;
+    }
+    const bool flag = d.treion_flag[gc] != 0;
+    const float ne_old = d.ne[gc];
+    const Final f = finalize(nH, nHe, nh1_end, nhe1_end, a_new, ne_old, dt, flag);
+    if (f.set_treion) {
+      d.treion[gc] = B.t;
+      d.treion_flag[gc] = 1;
+    }
+    d.nH1[gc] = f.nH1;
+    d.nHe1[gc] = f.nHe1;
+    d.f_H1[gc] = f.f_H1;
+    d.f_He1[gc] = f.f_He1;
+    d.ne[gc] = f.ne;
+    d.avg_nh1[gc] = a_new;
+    d.avg_nhe1[gc] = b_new;
+    if (diag) {
+      d.mfp[gc] = (float)(1. / d.sigH1_0 / (double)a_prev);
+      d.mfp912[gc] = (float)(1. / d.sigH1_912 / (double)a_prev);
+      d.rec_h2[gc] = d.l_rec_h2[s];
+      d.rec_he2[gc] = d.l_rec_he2[s];
+      d.recrate_h2[gc] = (float)((double)d.l_crec_h[s] * nelec_d * (double)f.nH2);
+      d.recrate_he2[gc] = (float)((double)d.l_crec_he[s] * nelec_d * (double)f.nHe2);
+      d.n_tot[gc] = f.n_tot;
+      d.dne_dt[gc] = f.dne_dt;
+    }
+    if (THERMAL) {
+      ThermCell c;
+      c.temp = d.temp[gc];
+      c.heat = d.heat[gc];
+      c.cool = d.cool[gc];
+      c.nH = nH;
+      c.nH1 = f.nH1;
+      c.nH1_prev = d.l_nh1_old[s];
+      c.nH2 = f.nH2;
+      c.nHe2 = f.nHe2;
+      c.ne = f.ne;
+      c.n_tot = f.n_tot;
+      c.dne_dt = f.dne_dt;
+      c.f_H2 = f.f_H2;
+      c.avg_nh1 = a_new;
+      c.avg_nhe1 = b_new;
+      thermal_update<STRICT>(c, B.th, d.l_acc_nu_h + s, d.l_acc_nu_he + s, L, d.F, d.nhe_to_nh);
+      d.temp[gc] = c.temp;
+      d.heat[gc] = c.heat;
+      d.cool[gc] = c.cool;
+      if (diag) {
+        d.if_speed[gc] = c.if_speed;
+        d.inc_flux[gc] = c.inc_flux;
+      }
+    } else {
+      d.nH1_prev[gc] = d.l_nh1_old[s];
+      d.n_tot[gc] = f.n_tot;
+      d.dne_dt[gc] = f.dne_dt;
+    }
+  }
+}
+
+// ---- whole step of the cells no ray touched -----------------------------------------------
+// 5 C2Ray updates with Gamma = 0 (ray_tracing.cc:941-1136), the last-iteration bookkeeping
+// (1138-1209) and, when THERMAL, update_thermal (gas_funcs.cc:362-411), all in registers.
+template <bool STRICT, bool THERMAL>
+__global__ void __launch_bounds__(256) k_dark(Dev d) {
+  const long long ncell = d.ncell_total;
+  const bool diag = d.outputs == FRT_OUT_DIAG;
+  const int I = d.itercount;
+  for (long long gc = blockIdx.x * (long long)blockDim.x + threadIdx.x; gc < ncell;
+       gc += (long long)gridDim.x * blockDim.x) {
+    const int b = box_of_cell(d, gc);
+    if (b < 0) continue;   // padding between boxes
+    if (d.lit_flag[gc]) continue;
+    const BoxP& B = d.box[b];
+    if (gc - B.cell0 >= B.ncell) continue;
+    const float dt = B.dt;
+    const float nH = d.nH[gc], nHe = d.nHe[gc];
+    const float nh1 = d.nH1[gc], nhe1 = d.nHe1[gc];
+    const float temp0 = d.temp[gc];
+    const float cl = d.clump ? d.clump[gc] : d.const_clump;
+    float rh, rhe;
+    recomb_coeffs<STRICT>(temp0, &rh, &rhe);
+    const C2Species H{nH, d.f_H1[gc], cl * rh};
+    const C2Species He{nHe, d.f_He1[gc], cl * rhe};
+    float a = nh1, bb = nhe1, a_prev = nh1;
+    float nh1_end = 0.f, nhe1_end = 0.f;
+    double nelec_last = 0.0;
+    for (int it = 0; it < I; it++) {
+      const bool last = (it == I - 1);
+      const float nelec_f = nH - a + nHe - bb;
+      const double nelec_d = (double)nelec_f;
+      a_prev = a;
+      const float an = c2ray_species<STRICT>(H, 0.f, nelec_d, nelec_f, a, dt, last, &nh1_end);
+      const float bn = c2ray_species<STRICT>(He, 0.f, nelec_d, nelec_f, bb, dt, last, &nhe1_end);
+      a = an;
+      bb = bn;
+      nelec_last = nelec_d;
+    }
+    const bool flag = d.treion_flag[gc] != 0;
+    const float ne_old = d.ne[gc];
+    const Final f = finalize(nH, nHe, nh1_end, nhe1_end, a, ne_old, dt, flag);
+    if (f.set_treion) {
+      d.treion[gc] = B.t;
+      d.treion_flag[gc] = 1;
+    }
+    d.nH1[gc] = f.nH1;
+    d.nHe1[gc] = f.nHe1;
+    d.f_H1[gc] = f.f_H1;
+    d.f_He1[gc] = f.f_He1;
+    d.ne[gc] = f.ne;
+    d.avg_nh1[gc] = a;
+    d.avg_nhe1[gc] = bb;
+    if (diag) {
+      d.mfp[gc] = (float)(1. / d.sigH1_0 / (double)a_prev);
+      d.mfp912[gc] = (float)(1. / d.sigH1_912 / (double)a_prev);
+      d.rec_h2[gc] = rh;
+      d.rec_he2[gc] = rhe;
+      d.recrate_h2[gc] = (float)((double)(cl * rh) * nelec_last * (double)f.nH2);
+      d.recrate_he2[gc] = (float)((double)(cl * rhe) * nelec_last * (double)f.nHe2);
+      d.n_tot[gc] = f.n_tot;
+      d.dne_dt[gc] = f.dne_dt;
+    }
+    if (THERMAL) {
+      ThermCell c;
+      c.temp = temp0;
+      c.heat = d.heat[gc];
+      c.cool = d.cool[gc];
+      c.nH = nH;
+      c.nH1 = f.nH1;
+      c.nH1_prev = nh1;
+      c.nH2 = f.nH2;
+      c.nHe2 = f.nHe2;
+      c.ne = f.ne;
+      c.n_tot = f.n_tot;
+      c.dne_dt = f.dne_dt;
+      c.f_H2 = f.f_H2;
+      c.avg_nh1 = a;
+      c.avg_nhe1 = bb;
+      thermal_update<STRICT>(c, B.th, nullptr, nullptr, 0, d.F, d.nhe_to_nh);
+      d.temp[gc] = c.temp;
+      d.heat[gc] = c.heat;
+      d.cool[gc] = c.cool;
+      if (diag) {
+        d.if_speed[gc] = c.if_speed;
+        d.inc_flux[gc] = c.inc_flux;
+      }
+    } else {
+      d.nH1_prev[gc] = nh1;
+      d.n_tot[gc] = f.n_tot;
+      d.dne_dt[gc] = f.dne_dt;
+    }
+  }
+}
+
+// ---- update_thermal over all cells (the unfused call sequence) ----------------------------
+template <bool STRICT>
+__global__ void __launch_bounds__(256) k_thermal_all(Dev d) {
+  const long long ncell = d.ncell_total;
+  const bool diag = d.outputs == FRT_OUT_DIAG;
+  const int L = d.lit_cap;
+  for (long long gc = blockIdx.x * (long long)blockDim.x + threadIdx.x; gc < ncell;
+       gc += (long long)gridDim.x * blockDim.x) {
+    const int b = box_of_cell(d, gc);
+    if (b < 0) continue;
+    const BoxP& B = d.box[b];
+    if (gc - B.cell0 >= B.ncell) continue;
+    ThermCell c;
+    c.temp = d.temp[gc];
+    c.heat = d.heat[gc];
+    c.cool = d.cool[gc];
+    c.nH = d.nH[gc];
+    c.nH1 = d.nH1[gc];
+    c.nH1_prev = d.nH1_prev[gc];
+    c.nH2 = c.nH - c.nH1;
+    c.nHe2 = d.nHe[gc] - d.nHe1[gc];
+    c.ne = d.ne[gc];
+    c.n_tot = d.n_tot[gc];
+    c.dne_dt = d.dne_dt[gc];
+    c.f_H2 = c.nH2 / c.nH;
+    c.avg_nh1 = d.avg_nh1[gc];
+    c.avg_nhe1 = d.avg_nhe1[gc];
+    const int slot = d.lit_slot[gc];
+    if (slot >= 0)
+      thermal_update<STRICT>(c, B.th, d.l_acc_nu_h + slot, d.l_acc_nu_he + slot, L, d.F, d.nhe_to_nh);
+    else
+      thermal_update<STRICT>(c, B.th, nullptr, nullptr, 0, d.F, d.nhe_to_nh);
+    d.temp[gc] = c.temp;
+    d.heat[gc] = c.heat;
+    d.cool[gc] = c.cool;
+    if (diag) {
+      d.if_speed[gc] = c.if_speed;
+      d.inc_flux[gc] = c.inc_flux;
+    }
+  }
+}
+
+// ---- dense view of a per-step sparse output (zero where no ray deposited) ------------------
+// field: 0 gamma_H1_tot, 1 gamma_He1_tot, 2+nu gamma_H1_nu, 2+F+nu gamma_He1_nu, 2+2F+nu ngam_nu
+__global__ void k_gather_sparse(Dev d, long long cell0, long long ncell, int which, float* out) {
+  const int L = d.lit_cap, F = d.F;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+    const int slot = d.lit_slot[cell0 + c];
+    float v = 0.f;
+    if (slot >= 0) {
+      if (which == 0) v = d.l_acc_g[slot];
+      else if (which == 1) v = d.l_acc_ghe[slot];
+      else if (which < 2 + F) v = d.l_acc_nu_h[(size_t)(which - 2) * L + slot];
+      else if (which < 2 + 2 * F) v = d.l_acc_nu_he[(size_t)(which - 2 - F) * L + slot];
+      else v = d.l_ngam[(size_t)(which - 2 - 2 * F) * L + slot];
+    }
+    out[c] = v;
+  }
+}
+
+}  // namespace
+
+// ---- launchers -------------------------------------------------------------------------------
+void launch_clear_lit(const Dev& d, int grid, cudaStream_t s) { k_clear_lit<<<grid, 256, 0, s>>>(d); }
+
+void launch_lit_init(const Dev& d, bool strict, int grid, cudaStream_t s) {
+  if (strict) k_lit_init<true><<<grid, 256, 0, s>>>(d);
+  else k_lit_init<false><<<grid, 256, 0, s>>>(d);
+}
+
+void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t s) {
+  const bool first = iter == 0, last = iter == d.itercount - 1;
+#define RP(ST, FI, LA) k_raypass<ST, FI, LA><<<grid, 256, 0, s>>>(d)
+  if (strict) {
+    if (first && last) RP(true, true, true);
+    else if (first) RP(true, true, false);
+    else if (last) RP(true, false, true);
+    else RP(true, false, false);
+  } else {
+    if (first && last) RP(false, true, true);
+    else if (first) RP(false, true, false);
+    else if (last) RP(false, false, true);
+    else RP(false, false, false);
+  }
+#undef RP
+}
+
+void launch_litpass(const Dev& d, int iter, bool strict, bool fused_thermal, int grid, cudaStream_t s) {
+  const bool last = iter == d.itercount - 1;
+  if (strict) {
+    if (!last) k_litpass<true, false, false><<<grid, 256, 0, s>>>(d);
+    else if (fused_thermal) k_litpass<true, true, true><<<grid, 256, 0, s>>>(d);
+    else k_litpass<true, true, false><<<grid, 256, 0, s>>>(d);
+  } else {
+    if (!last) k_litpass<false, false, false><<<grid, 256, 0, s>>>(d);
+    else if (fused_thermal) k_litpass<false, true, true><<<grid, 256, 0, s>>>(d);
+    else k_litpass<false, true, false><<<grid, 256, 0, s>>>(d);
+  }
+}
+
+void launch_dark(const Dev& d, bool strict, bool fused_thermal, int grid, cudaStream_t s) {
+  if (strict) {
+    if (fused_thermal) k_dark<true, true><<<grid, 256, 0, s>>>(d);
+    else k_dark<true, false><<<grid, 256, 0, s>>>(d);
+  } else {
+    if (fused_thermal) k_dark<false, true><<<grid, 256, 0, s>>>(d);
+    else k_dark<false, false><<<grid, 256, 0, s>>>(d);
+  }
+}
+
+void launch_thermal_all(const Dev& d, bool strict, int grid, cudaStream_t s) {
+  if (strict) k_thermal_all<true><<<grid, 256, 0, s>>>(d);
+  else k_thermal_all<false><<<grid, 256, 0, s>>>(d);
+}
+
+void launch_gather_sparse(const Dev& d, long long cell0, long long ncell, int which, float* out, cudaStream_t s) {
+  k_gather_sparse<<<grid_for(ncell, 256, 4096), 256, 0, s>>>(d, cell0, ncell, which, out);
+}
+
+}  // namespace frt

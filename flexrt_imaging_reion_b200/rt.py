@@ -1,0 +1,306 @@
+"""Host-side mirror of the reference's RT call surface over the C ABI.
+
+The reference driver (main.cc) calls, per step, set_clump, set_clight, update_rays, find_avg_unu,
+set_lmerge/set_merge_domain/get_num_thresh/count_rays/calc_nphot_merge, merge, split_rays,
+update_thermal, new_rays, update_dt (main.cc:108-264), after a set-up of init, update_dt,
+set_spectrum, init_rt, new_rays and get_nphot_min_max (main.cc:10-106). RTContext exposes the same
+calls by the same names; `step()` runs the fused CUDA-graph form of one whole step.
+
+Random rotations: the reference draws siRand(Ntheta) = rand() % 42875 from glibc's rand() once per
+step in merge() (ray_tracing.cc:327) and once per source in init_rays (ray_tracing.cc:233), in that
+order. Each box here keeps its own glibc random stream (srand(seed) + rand() semantics, through
+glibc's reentrant initstate_r/random_r), so a box reproduces the draws of a one-box reference run.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import _abi
+from . import workloads as W
+
+# set_spectrum (gas_funcs.cc:44-70) at alpha = 1.5 interpolates between the table rows alpha = 1.5
+# and 1.75 of the reference's 5-bin spectrum table (input_files/spectrum_tables_5bins.txt) with
+# weight 0; only those rows and the alpha column enter the arithmetic.
+_SPEC_ALPHA = [-0.5 + 0.25 * i for i in range(15)]
+_SPEC_ROWS = {8: [0.2, 0.2, 0.2, 0.2, 0.2], 9: [0.221, 0.213, 0.203, 0.191, 0.172]}
+
+
+def spectrum_alpha15() -> np.ndarray:
+    """set_spectrum() for the 5-bin table at alpha = 1.5, with the reference's float arithmetic."""
+    a0, a1 = _SPEC_ALPHA[0], _SPEC_ALPHA[-1]
+    m = int(np.floor((1.5 - a0) / (a1 - a0) * 14))
+    m = min(m, 13)
+    p = m + 1
+    rows = _SPEC_ROWS
+    spec = np.zeros(5, np.float32)
+    ssum = np.float32(0.0)
+    for nu in range(5):
+        v = rows[m][nu] + (rows[p][nu] - rows[m][nu]) / (_SPEC_ALPHA[p] - _SPEC_ALPHA[m]) * (1.5 - _SPEC_ALPHA[m])
+        spec[nu] = np.float32(v)
+        ssum = np.float32(ssum + spec[nu])
+    return (spec / ssum).astype(np.float32)
+
+
+class RandStream:
+    """glibc rand() sequence after srand(seed), kept per box with initstate_r / random_r."""
+
+    _libc = None
+
+    def __init__(self, seed: int):
+        if RandStream._libc is None:
+            RandStream._libc = C.CDLL("libc.so.6")
+            RandStream._libc.initstate_r.argtypes = [C.c_uint, C.c_void_p, C.c_size_t, C.c_void_p]
+            RandStream._libc.random_r.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
+        self._state = C.create_string_buffer(128)
+        self._data = C.create_string_buffer(64)
+        if RandStream._libc.initstate_r(C.c_uint(seed), self._state, 128, self._data) != 0:
+            raise RuntimeError("initstate_r failed")
+        self._out = C.c_int32(0)
+
+    def rand(self) -> int:
+        RandStream._libc.random_r(self._data, C.byref(self._out))
+        return int(self._out.value)
+
+    def si_rand(self, a: int = _abi.FRT_NTHETA) -> int:
+        return self.rand() % a
+
+
+class FrtError(RuntimeError):
+    pass
+
+
+class RTContext:
+    """One or more independent boxes of the RT step on one GPU."""
+
+    def __init__(self, inputs: Sequence[W.BoxInputs], seeds: Sequence[int], precision: str = "mixed",
+                 outputs: str = "core", ray_capacity: Optional[int] = None, lit_capacity: int = 0,
+                 device: int = 0, path_length: int = 8):
+        self.L = _abi.lib()
+        self.inputs = list(inputs)
+        self.specs = [i.spec for i in self.inputs]
+        self.nbox = len(self.inputs)
+        self.rng = [RandStream(s) for s in seeds]
+        self.F = 5
+        self.spectrum = spectrum_alpha15()
+        self._boxes = (_abi.BoxDesc * self.nbox)()
+        for b, s in enumerate(self.specs):
+            bd = self._boxes[b]
+            bd.n = s.n
+            bd.box_hmpc = s.box_hmpc
+            bd.zz = s.z
+            bd.cl_factor = s.cl_factor()
+            bd.ray_per_cell_max = s.ray_per_cell_max
+            bd.rkill_cm = s.rkill_cm()
+        cfg = _abi.Config()
+        cfg.nfreq = self.F
+        for nu, e in enumerate(W.NU_EV_5BIN):
+            cfg.nu_phot[nu] = e / W.H_EV
+            cfg.spectrum[nu] = float(self.spectrum[nu])
+        cfg.itercount = 5
+        cfg.path_length = path_length
+        cfg.hpx_lvl = 0
+        cfg.safety_factor = 3.0
+        cfg.tstep_factor = 1.0
+        cfg.nl_const = 0.5
+        cfg.const_clump = 1.0
+        cfg.fH1_0 = 1.0 - 1.2e-3
+        cfg.fHe1_0 = 1.0 - 1.2e-3
+        cfg.fHe2_0 = 1.2e-3
+        cfg.temp_0 = 1e4
+        cfg.nbox = self.nbox
+        cfg.boxes = C.cast(self._boxes, C.POINTER(_abi.BoxDesc))
+        ncell = sum(s.n ** 3 for s in self.specs)
+        cfg.ray_capacity = int(ray_capacity or max(1 << 20, 4 * ncell))
+        cfg.lit_capacity = int(lit_capacity)
+        self.src = [W.grid_sources(i) for i in self.inputs]
+        cfg.src_capacity = max(1, sum(len(l) for _, l in self.src))
+        cfg.precision = _abi.FRT_PREC_STRICT if precision == "strict" else _abi.FRT_PREC_MIXED
+        cfg.outputs = _abi.FRT_OUT_DIAG if outputs == "diag" else _abi.FRT_OUT_CORE
+        cfg.device = device
+        self._cfg = cfg
+        h = C.c_void_p()
+        st = self.L.frt_create(C.byref(cfg), C.byref(h))
+        self.h = h
+        self._check(st, "frt_create")
+        self.nsrc_box = [len(l) for _, l in self.src]
+        self.nsrc = sum(self.nsrc_box)
+        self._ith_box = np.zeros(self.nbox, np.uint16)
+        self._ith_src = np.zeros(max(1, self.nsrc), np.uint16)
+        self.stats = _abi.StepStats()
+
+    # ---- plumbing ---------------------------------------------------------------------------
+    def _check(self, st: int, what: str) -> None:
+        if st != _abi.FRT_OK:
+            msg = self.L.frt_last_error(self.h).decode() if self.h else ""
+            raise FrtError(f"{what} failed with status {st}: {msg}")
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.L.frt_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- set-up, as main.cc:10-106 -------------------------------------------------------------
+    def setup(self) -> None:
+        for b, inp in enumerate(self.inputs):
+            d1 = np.ascontiguousarray(inp.delta1, np.float32)
+            self._check(self.L.frt_init_gas(self.h, b, d1.ctypes.data), "frt_init_gas")
+            ijk, lum = self.src[b]
+            ijk = np.ascontiguousarray(ijk, np.int32)
+            lum = np.ascontiguousarray(lum, np.float64)
+            self._check(self.L.frt_set_sources(self.h, b, len(lum), ijk.ctypes.data, lum.ctypes.data),
+                        "frt_set_sources")
+            if inp.clump is not None:
+                cl = np.ascontiguousarray(inp.clump, np.float32)
+                self._check(self.L.frt_set_clump_field(self.h, b, cl.ctypes.data), "frt_set_clump_field")
+        self.update_dt()
+        self.init_rt()
+        self.new_rays(self.draw_cast())
+        self.get_nphot_min_max()
+
+    def draw_cast(self) -> np.ndarray:
+        out = np.zeros(max(1, self.nsrc), np.uint16)
+        k = 0
+        for b in range(self.nbox):
+            for _ in range(self.nsrc_box[b]):
+                out[k] = self.rng[b].si_rand()
+                k += 1
+        return out
+
+    def draw_merge(self) -> np.ndarray:
+        return np.array([self.rng[b].si_rand() for b in range(self.nbox)], np.uint16)
+
+    def draw_step(self):
+        """Draws of one step in reference order: merge() first, then init_rays per source."""
+        m = self.draw_merge()
+        c = self.draw_cast()
+        return m, c
+
+    # ---- the reference's step functions ---------------------------------------------------------
+    def update_dt(self) -> np.ndarray:
+        dt = np.zeros(self.nbox, np.float32)
+        self._check(self.L.frt_update_dt(self.h, dt.ctypes.data), "frt_update_dt")
+        return dt
+
+    def init_rt(self) -> None:
+        self._check(self.L.frt_init_rt(self.h), "frt_init_rt")
+
+    def get_nphot_min_max(self):
+        mn = np.zeros(self.nbox)
+        mx = np.zeros(self.nbox)
+        self._check(self.L.frt_get_nphot_min_max(self.h, mn.ctypes.data, mx.ctypes.data), "frt_get_nphot_min_max")
+        return mn, mx
+
+    def set_clump(self) -> None:
+        self._check(self.L.frt_set_clump(self.h), "frt_set_clump")
+
+    def set_clight(self) -> None:
+        self._check(self.L.frt_set_clight(self.h), "frt_set_clight")
+
+    def update_rays(self) -> None:
+        self._check(self.L.frt_update_rays(self.h), "frt_update_rays")
+
+    def find_avg_unu(self) -> None:
+        self._check(self.L.frt_find_avg_unu(self.h), "frt_find_avg_unu")
+
+    def count_rays(self) -> np.ndarray:
+        out = np.zeros(self.nbox, np.int64)
+        self._check(self.L.frt_count_rays(self.h, out.ctypes.data), "frt_count_rays")
+        return out
+
+    def merge(self, itheta_per_box: np.ndarray) -> None:
+        a = np.ascontiguousarray(itheta_per_box, np.uint16)
+        self._check(self.L.frt_merge(self.h, a.ctypes.data), "frt_merge")
+
+    def split_rays(self) -> None:
+        self._check(self.L.frt_split_rays(self.h), "frt_split_rays")
+
+    def update_thermal(self) -> None:
+        self._check(self.L.frt_update_thermal(self.h), "frt_update_thermal")
+
+    def new_rays(self, itheta_per_source: np.ndarray) -> None:
+        a = np.ascontiguousarray(itheta_per_source, np.uint16)
+        self._check(self.L.frt_new_rays(self.h, a.ctypes.data), "frt_new_rays")
+
+    # ---- whole steps ------------------------------------------------------------------------------
+    def step_unfused(self) -> None:
+        """One step through the individual step functions, in main.cc's order."""
+        self.set_clump()
+        self.set_clight()
+        self.update_rays()
+        self.find_avg_unu()
+        m, c = self.draw_step()
+        self.merge(m)
+        self.split_rays()
+        self.update_thermal()
+        self.new_rays(c)
+        self.update_dt()
+
+    def step(self, graph: bool = True, draws=None) -> Dict[str, float]:
+        """One whole step, fused (CUDA graph when graph=True)."""
+        m, c = self.draw_step() if draws is None else draws
+        self._ith_box[:] = m
+        self._ith_src[: len(c)] = c[: len(self._ith_src)]
+        fn = self.L.frt_step if graph else self.L.frt_step_plain
+        st = fn(self.h, self._ith_box.ctypes.data, self._ith_src.ctypes.data, C.byref(self.stats))
+        self._check(st, "frt_step")
+        return self.stats.as_dict()
+
+    def last_timing(self):
+        a = C.c_float(0.0)
+        b = C.c_float(0.0)
+        self._check(self.L.frt_last_timing(self.h, C.byref(a), C.byref(b)), "frt_last_timing")
+        return a.value, b.value
+
+    # ---- state access --------------------------------------------------------------------------------
+    def get_field(self, box: int, name: str) -> np.ndarray:
+        n = self.specs[box].n
+        shape = (n ** 3, self.F) if name in _abi.PER_BIN_FIELDS else (n ** 3,)
+        out = np.zeros(shape, np.float32)
+        self._check(self.L.frt_get_field(self.h, box, _abi.FIELD_ID[name], out.ctypes.data), f"get_field {name}")
+        return out
+
+    def set_field(self, box: int, name: str, values: np.ndarray) -> None:
+        a = np.ascontiguousarray(values, np.float32)
+        self._check(self.L.frt_set_field(self.h, box, _abi.FIELD_ID[name], a.ctypes.data), f"set_field {name}")
+
+    def num_rays(self, box: int = -1) -> int:
+        n = C.c_longlong(0)
+        self._check(self.L.frt_num_rays(self.h, box, C.byref(n)), "frt_num_rays")
+        return int(n.value)
+
+    def rays(self, box: int = 0) -> Dict[str, np.ndarray]:
+        n = self.num_rays(box)
+        out = {"ray_order": np.zeros(n, np.int16), "ray_pixel": np.zeros(n, np.int32),
+               "ray_itheta": np.zeros(n, np.uint16), "ray_cell": np.zeros(n, np.int32),
+               "ray_geom": np.zeros((n, 9), np.float32), "ray_nphot": np.zeros((n, self.F), np.float32)}
+        self._check(self.L.frt_download_rays(self.h, box, out["ray_order"].ctypes.data, out["ray_pixel"].ctypes.data,
+                                             out["ray_itheta"].ctypes.data, out["ray_cell"].ctypes.data,
+                                             out["ray_geom"].ctypes.data, out["ray_nphot"].ctypes.data),
+                    "frt_download_rays")
+        return out
+
+    def box_scalars(self, box: int = 0) -> Dict[str, float]:
+        v = np.zeros(8)
+        self._check(self.L.frt_box_scalars(self.h, box, v.ctypes.data), "frt_box_scalars")
+        keys = ["t", "dt", "nphot_min", "nphot_max", "nphot_merge", "num_thresh", "dx", "dx0"]
+        return dict(zip(keys, v.tolist()))
+
+    def rotation_table(self) -> np.ndarray:
+        out = np.zeros((_abi.FRT_NTHETA, 18), np.float32)
+        self._check(self.L.frt_rotation_table(self.h, out.ctypes.data), "frt_rotation_table")
+        return out

@@ -1,0 +1,188 @@
+/* flexrt.h -- C ABI of the B200 (sm_100a) radiative-transfer step.
+ *
+ * Drop-in boundary for the per-timestep RT path of FlexRT. The reference is one C++/OpenMP
+ * program whose driver (main.cc:108-264) calls void(void) step functions on process-global
+ * arrays. Each entry point below replaces one of those functions (cited per declaration); the
+ * state they share lives on the GPU inside an frt_ctx instead of in globals. Host arrays are
+ * borrowed only for the duration of a call. Every entry point returns an frt_status; none
+ * aborts, and device-side failures (ray-pool or path overflow) come back as FRT_ERR_CAPACITY.
+ *
+ * Plain C2Ray mode of the reference: c2ray_iter = TRUE, subgrid = FALSE, ifront = FALSE,
+ * multi_freq = TRUE, case-B recombination, temperature evolution on (user_inputs.h:6-25).
+ * A context may hold several independent periodic boxes (batched ensemble); single-box use
+ * is nbox = 1.
+ */
+#ifndef FLEXRT_H
+#define FLEXRT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FRT_MAX_FREQ 8
+#define FRT_MAX_PATH 16
+#define FRT_NTHETA 42875 /* 35^3 random Euler-angle triples (healpix_funcs.cc:8-9) */
+
+typedef int frt_status;
+enum {
+  FRT_OK = 0,
+  FRT_ERR_INVALID = 1,  /* bad argument / configuration */
+  FRT_ERR_CAPACITY = 2, /* ray pool, lit-cell list or per-ray path capacity exceeded */
+  FRT_ERR_TIMEOUT = 3,  /* a bounded device wait ran out */
+  FRT_ERR_CUDA = 4,     /* CUDA runtime error (message via frt_last_error) */
+  FRT_ERR_STATE = 5     /* call out of order (e.g. step before sources/gas are set) */
+};
+
+enum { FRT_PREC_MIXED = 0, FRT_PREC_STRICT = 1 };
+enum { FRT_OUT_CORE = 0, FRT_OUT_DIAG = 1 };
+
+typedef struct frt_ctx frt_ctx;
+
+/* One periodic box. All boxes of a context share the spectrum and the solver constants. */
+typedef struct {
+  int n;                /* cells per side: Nx = Ny = Nz (user_inputs.h:75-77) */
+  double box_hmpc;      /* comoving side in h^-1 Mpc; Lx0 = box*1e3/hh kpc (user_inputs.h:92) */
+  float zz;             /* snapshot redshift; a = 1/(1+zz) (gas_funcs.cc:563-595) */
+  float cl_factor;      /* simulated / true speed of light (user_inputs.h:84) */
+  int ray_per_cell_max; /* merge threshold parameter (global_variables.cc:40), 22 */
+  double rkill_cm;      /* rays with comoving r above this are removed after the advance; 0 = never */
+} frt_box_desc;
+
+typedef struct {
+  int nfreq;                        /* Nfreq (user_inputs.h:78) */
+  double nu_phot[FRT_MAX_FREQ];     /* bin frequencies in Hz (user_inputs.h:95) */
+  float spectrum[FRT_MAX_FREQ];     /* photon fraction per bin (set_spectrum, gas_funcs.cc:44-70) */
+  int itercount;                    /* C2Ray iterations (user_inputs.h:85), 5 */
+  int path_length;                  /* segments stored per ray per step (user_inputs.h:107) */
+  int hpx_lvl;                      /* casting / merging HEALPix order (user_inputs.h:81) */
+  float safety_factor;              /* split when beam area > dx^2/safety_factor (user_inputs.h:86) */
+  float tstep_factor;               /* user_inputs.h:82 */
+  float nl_const;                   /* user_inputs.h:83 */
+  float const_clump;                /* user_inputs.h:87 */
+  float fH1_0, fHe1_0, fHe2_0;      /* initial ionisation state (user_inputs.h:98-100) */
+  float temp_0;                     /* initial temperature (user_inputs.h:96) */
+  int nbox;
+  const frt_box_desc* boxes;
+  long long ray_capacity;           /* device ray-pool slots (all boxes) */
+  long long lit_capacity;           /* cells touched by rays in one step (all boxes); 0 = all cells */
+  long long src_capacity;           /* sources (all boxes) */
+  int precision;                    /* FRT_PREC_MIXED (FP32 + FP64 where x_HI < 1e-3) or FRT_PREC_STRICT */
+  int outputs;                      /* FRT_OUT_CORE or FRT_OUT_DIAG (also keep mfp, recrate, u_nu, vIF...) */
+  int device;                       /* CUDA device ordinal */
+} frt_config;
+
+/* Per-cell fields addressable by frt_get_field / frt_set_field, C order [i][j][k] with k
+ * fastest; the *_NU fields carry nfreq values per cell, [cell][nu]. Names follow the reference's
+ * globals (global_variables.cc:78-260). */
+typedef enum {
+  FRT_F_RHO = 0, FRT_F_NH, FRT_F_NHE, FRT_F_NH1, FRT_F_NHE1, FRT_F_NH2, FRT_F_NHE2, FRT_F_NE, FRT_F_N_TOT,
+  FRT_F_F_H1, FRT_F_F_HE1, FRT_F_F_H2, FRT_F_F_HE2, FRT_F_TEMP, FRT_F_CLUMP, FRT_F_AVG_NH1, FRT_F_AVG_NHE1,
+  FRT_F_GAMMA_H1_TOT, FRT_F_GAMMA_HE1_TOT, FRT_F_HEAT_RATE, FRT_F_COOL_RATE, FRT_F_TREION,
+  FRT_F_TREION_FLAG /* as float 0/1 */, FRT_F_DNE_DT, FRT_F_RECOMB_H2, FRT_F_RECOMB_HE2, FRT_F_RECRATE_H2,
+  FRT_F_RECRATE_HE2, FRT_F_MFP, FRT_F_MFP_912, FRT_F_IF_SPEED, FRT_F_INC_FLUX,
+  FRT_F_GAMMA_H1_NU, FRT_F_GAMMA_HE1_NU, FRT_F_NGAM_NU, FRT_F_U_NU,
+  FRT_F_COUNT
+} frt_field;
+
+/* Per-step totals (device-computed). Photon counts are physical photons (not 1e60-normalised). */
+typedef struct {
+  long long rays_alive;      /* after the step (after cast) */
+  long long rays_moved;      /* rays advanced this step */
+  long long crossings;       /* ray-cell crossings = stored path segments (sum of ray_end) */
+  long long lit_cells;       /* cells touched by at least one segment */
+  long long rays_split;      /* parents split */
+  long long rays_merged;     /* rays merged away */
+  long long rays_killed;     /* removed below nphot_min */
+  long long rays_cast;       /* new rays */
+  double photons_emitted;    /* sum of nphot of the new rays */
+  double photons_deposited;  /* photons entering Gamma_HI + Gamma_HeI on the last C2Ray iteration */
+  double photons_killed;     /* photons left in rays removed below nphot_min */
+  double photons_overlap;    /* photons both dumped into a cell and left in the killed ray */
+  double photons_in_flight;  /* sum of nphot over live rays after the step */
+  double t;                  /* simulation time after the step [s] */
+  double dt;                 /* time step [s] */
+  unsigned int error_flags;  /* device error word (0 = ok) */
+  unsigned int pad;
+} frt_step_stats;
+
+/* ---- life cycle ----------------------------------------------------------------------- */
+frt_status frt_create(const frt_config* cfg, frt_ctx** out);
+frt_status frt_destroy(frt_ctx* ctx);
+const char* frt_last_error(const frt_ctx* ctx);
+/* Copy of the rotation coefficient table (FRT_NTHETA x 2 x 9 floats: forward, inverse) that the
+ * context built from the reference's float expressions (healpix_funcs.cc:21-39, 102-143). */
+frt_status frt_rotation_table(const frt_ctx* ctx, float* out);
+/* The same table without a context (host only; no GPU needed). */
+frt_status frt_build_rotation_table(float* out);
+
+/* ---- set-up (one call per box) ------------------------------------------------------------ */
+/* Gas set-up of the first snapshot: rho from the density cube (1+delta, as read by get_ugas,
+ * io_funcs.cc:33-62, times a^-3, gas_funcs.cc:601-610), then init() (init_funcs.cc:10-142). */
+frt_status frt_init_gas(frt_ctx* ctx, int box, const float* delta1);
+/* Sources gridded per cell in (i,j,k) order as read_source_catalog produces them
+ * (io_funcs.cc:157-233): ijk[3*s..3*s+2], lum[s] in photons/s. */
+frt_status frt_set_sources(frt_ctx* ctx, int box, int nsrc, const int32_t* ijk, const double* lum);
+/* Per-cell clumping factor written over set_clump()'s constant every step (NULL = constant). */
+frt_status frt_set_clump_field(frt_ctx* ctx, int box, const float* clump);
+frt_status frt_set_field(frt_ctx* ctx, int box, frt_field f, const float* host);
+frt_status frt_get_field(frt_ctx* ctx, int box, frt_field f, float* host);
+
+/* ---- the reference's step functions ------------------------------------------------------- */
+/* init_rt (rt_funcs.cc:36-126, input_grid = FALSE) */
+frt_status frt_init_rt(frt_ctx* ctx);
+/* update_dt (rt_funcs.cc:9-12); dt_out[box] may be NULL */
+frt_status frt_update_dt(frt_ctx* ctx, float* dt_out);
+/* get_nphot_min_max (ray_tracing.cc:129-154) */
+frt_status frt_get_nphot_min_max(frt_ctx* ctx, double* nmin_out, double* nmax_out);
+/* set_clump + set_clight (subgrid.cc:799-811, rt_funcs.cc:129-143) */
+frt_status frt_set_clump(frt_ctx* ctx);
+frt_status frt_set_clight(frt_ctx* ctx);
+/* t += dt, then update_rays (rt_funcs.cc:159-208 -> advance_ray, ray_tracing.cc:1222-1512) */
+frt_status frt_update_rays(frt_ctx* ctx);
+/* find_avg_unu (ray_tracing.cc:623-1216): C2Ray iteration, Gamma deposition, cell update */
+frt_status frt_find_avg_unu(frt_ctx* ctx);
+/* count_rays (ray_tracing.cc:35-47) per box */
+frt_status frt_count_rays(frt_ctx* ctx, long long* count_per_box);
+/* set_lmerge/set_merge_domain/get_num_thresh/count_rays/calc_nphot_merge, then merge
+ * (main.cc:153-165; ray_tracing.cc:157-227, 324-477). itheta_per_box: one random-angle index per
+ * box, drawn by the caller (siRand(Ntheta), ray_tracing.cc:327). */
+frt_status frt_merge(frt_ctx* ctx, const uint16_t* itheta_per_box);
+/* split_rays (rt_funcs.cc:211-237 -> split_ray, ray_tracing.cc:482-619) */
+frt_status frt_split_rays(frt_ctx* ctx);
+/* update_thermal (gas_funcs.cc:362-457) */
+frt_status frt_update_thermal(frt_ctx* ctx);
+/* new_rays (rt_funcs.cc:240-261 -> init_rays, ray_tracing.cc:230-321). itheta_per_source: one
+ * index per source of all boxes in order, drawn by the caller (ray_tracing.cc:233). */
+frt_status frt_new_rays(frt_ctx* ctx, const uint16_t* itheta_per_source);
+
+/* One whole RT step in the order of main.cc:108-264 (fixed redshift), captured once as a CUDA
+ * graph and replayed: the fused form of the calls above. Host inputs are the random-angle
+ * indices; stats (may be NULL) receives the per-step totals of box -1 = all boxes. */
+frt_status frt_step(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t* itheta_per_source,
+                    frt_step_stats* stats);
+/* Same as frt_step but launching every kernel directly (no graph) */
+frt_status frt_step_plain(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t* itheta_per_source,
+                          frt_step_stats* stats);
+frt_status frt_last_stats(frt_ctx* ctx, frt_step_stats* stats);
+
+/* ---- rays ----------------------------------------------------------------------------------- */
+frt_status frt_num_rays(frt_ctx* ctx, int box, long long* n);
+/* Live rays of a box in pool order, unpacked like write_rays_binary (io_funcs.cc:274-303):
+ * order, pixel, itheta, cell (= path[0].ind, local to the box), geom[9] = xhat, yhat, zhat, r, dr,
+ * x, y, z, time; nphot[nfreq]. Arrays must hold frt_num_rays() entries. */
+frt_status frt_download_rays(frt_ctx* ctx, int box, int16_t* order, int32_t* pixel, uint16_t* itheta,
+                             int32_t* cell, float* geom9, float* nphot);
+
+/* Scalars of one box: t, dt, nphot_min, nphot_max, nphot_merge, num_thresh, dx, dx0 */
+frt_status frt_box_scalars(frt_ctx* ctx, int box, double* out8);
+/* Kernel time of the last frt_step / frt_step_plain in ms (device events on the step stream),
+ * and the time of its dominant cell kernel. */
+frt_status frt_last_timing(frt_ctx* ctx, float* step_ms, float* cell_kernel_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLEXRT_H */

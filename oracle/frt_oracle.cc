@@ -1037,4 +1037,13 @@ int orc_dump(void* h, const char* path) {
 
 void orc_destroy(void* h) { delete (Ctx*)h; }
 
+// rotation of healpix_funcs.cc:102-143 with the angles of get_random_angles (healpix_funcs.cc:21-39)
+void orc_rotate(int itheta, int direction, const double* v, double* out) {
+  const int i = itheta / (kNalpha * kNalpha), j = (itheta / kNalpha) % kNalpha, k = itheta % kNalpha;
+  float a0 = 2. * O_PI / kNalpha * i, b0 = 2. * O_PI / kNalpha * j, g0 = 2. * O_PI / kNalpha * k;
+  rotate(a0, b0, g0, direction, v[0], v[1], v[2], &out[0], &out[1], &out[2]);
+}
+void orc_pix2vec(int order, int pix, double* v) { hpn::pix2vec(order, pix, &v[0], &v[1], &v[2]); }
+int orc_vec2pix(int order, const double* v) { return hpn::vec2pix(order, v[0], v[1], v[2]); }
+
 }  // extern "C"

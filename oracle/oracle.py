@@ -67,6 +67,10 @@ def lib():
         _lib.orc_dump.argtypes = [C.c_void_p, C.c_char_p]
         _lib.orc_scalars.argtypes = [C.c_void_p, C.c_void_p]
         _lib.orc_destroy.argtypes = [C.c_void_p]
+        _lib.orc_rotate.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        _lib.orc_pix2vec.argtypes = [C.c_int, C.c_int, C.c_void_p]
+        _lib.orc_vec2pix.argtypes = [C.c_int, C.c_void_p]
+        _lib.orc_vec2pix.restype = C.c_int
     return _lib
 
 
