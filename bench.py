@@ -1,0 +1,313 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 RT step: ray-cell crossings/s and ms per RT step.
+
+Workload (default "L"): the large configuration -- 256^3 box of 100 h^-1 cMpc at z = 6.5,
+lognormal gas (sigma_ln = 0.8), 16384 sources with dN/dL ~ L^-2 on [1e50, 1e54] ph/s, 5 frequency
+bins, dt = 0.25 Myr -- from seeded synthetic inputs. A "step" is one whole RT step (advance,
+5-iteration C2Ray with Gamma deposition, merge, split, thermal, cast); W warm-up steps, then K
+timed steps of the same run. The state (16.8 M cells, ~7 M rays) is far larger than L2, so no
+L2 flush is needed between steps.
+
+  value      crossings of the K steps / device time of the K steps (CUDA events around each
+             graph launch on the step stream), summed over ranks / max over ranks
+  e2e        same crossings / host wall time of the frt_step calls (per step: H2D of the step's
+             random-angle indices from pinned memory, graph launch, D2H of the step totals)
+  roofline   the dark-cell kernel (the whole step of every cell no ray touched, one streaming
+             pass): algorithmic bytes = cells x 82 B (10 float fields + 2 flag bytes read,
+             10 float fields written) / its CUDA-event time, against MEASURED_PEAKS.json hbm_gbs
+  cpu_baseline  the reference's own OpenMP code (compiled from its sources, oracle/_ref) on the
+             host cores, on a bounded sample (its first steps) of the same workload
+
+--impl reference runs that compiled reference alone (all host threads) and prints its line.
+Multi-GPU: the single-box workloads do not shard; --gpus N runs N independent replicas (one per
+rank, "weak" scaling), value = all ranks' crossings / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import resource
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+DARK_BYTES_PER_CELL = 82  # 10 float fields + treion_flag + lit_flag read, 10 float fields written
+
+
+def _peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm = [float(r[0]) for r in self.rows if r and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) > 1 and r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 3 + k and r[3 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def _spec(name):
+    from flexrt_imaging_reion_b200 import workloads as W
+    return {"L": W.config_L, "M": W.config_M, "S": W.config_S}[name]()
+
+
+def _describe(spec):
+    return (f"{spec.name}: {spec.n}^3, {spec.box_hmpc:g} h^-1 cMpc, z={spec.z:g}, sigma_ln={spec.sigma_ln}, "
+            f"{spec.n_src} sources ({spec.lum_law} [{spec.lum_min:.0e},{spec.lum_max:.0e}] ph/s), 5 bins, "
+            f"dt={spec.dt_myr} Myr, clumping={spec.clump_model}")
+
+
+def _unlimited_stack():
+    # update_thermal keeps a float[Nx][Ny][Nz] array on the stack (gas_funcs.cc:364)
+    try:
+        resource.setrlimit(resource.RLIMIT_STACK, (resource.RLIM_INFINITY, resource.RLIM_INFINITY))
+    except (ValueError, OSError):
+        soft, hard = resource.getrlimit(resource.RLIMIT_STACK)
+        resource.setrlimit(resource.RLIMIT_STACK, (hard, hard))
+
+
+# ---- the compiled reference (oracle/_ref) ------------------------------------------------------
+def _ref_exe(name: str, spec, threads: int) -> str:
+    from oracle import build_ref as B
+    d = os.path.join(B.OUT, name)
+    exe = os.path.join(d, "ref_driver")
+    meta_p = os.path.join(d, "stage.json")
+    ncpu = None
+    if os.path.exists(meta_p):
+        with open(meta_p) as f:
+            ncpu = json.load(f).get("ncpu")
+    if not os.path.exists(exe) or ncpu is None or ncpu < threads:
+        if os.path.isdir(B.REF_SRC):
+            B.build(name, spec, ncpu=threads)
+        elif os.path.isdir(os.path.join(d, "src")):
+            B.compile_stage(d, ncpu=threads)
+        else:
+            raise RuntimeError("compiled reference not available (oracle/_ref/%s)" % name)
+    return exe
+
+
+def run_reference(spec, name: str, steps: int, threads: int, time_cap_s: float, seed: int):
+    """Run the compiled reference for up to `steps` steps (stopping once the steps so far exceed
+    time_cap_s); returns per-step (crossings, wall) and the set-up time."""
+    from flexrt_imaging_reion_b200 import workloads as W
+    exe = _ref_exe(name, spec, threads)
+    inp = W.make_inputs(spec)
+    with tempfile.TemporaryDirectory() as td:
+        W.write_reference_inputs(inp, td)
+        args = [exe, td, str(steps), str(seed), "0", repr(spec.rkill_cm())]
+        if inp.clump is not None:
+            args.append(os.path.join(td, "clump.bin"))
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        p = subprocess.Popen(args, cwd=os.path.dirname(exe), env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                             text=True, preexec_fn=_unlimited_stack)
+        rows, setup = [], None
+        t_steps = 0.0
+        for line in p.stdout:
+            if line.startswith("SETUP"):
+                setup = float(line.split()[1])
+            m = re.match(r"STEP (\d+) rays_before=\d+ crossings=(\d+) moved=\d+ wall=([0-9.eE+-]+)", line)
+            if m:
+                rows.append((int(m.group(2)), float(m.group(3))))
+                t_steps += float(m.group(3))
+                if t_steps > time_cap_s:
+                    p.kill()
+                    break
+        p.wait()
+    return rows, setup
+
+
+# ---- our arm ---------------------------------------------------------------------------------
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import numpy as np
+    from flexrt_imaging_reion_b200 import workloads as W, rt
+    spec = _spec(args.workload)
+    inp = W.make_inputs(spec)
+    ctx = rt.RTContext([inp], [args.seed + rank], precision="mixed", outputs="core",
+                       ray_capacity=args.ray_capacity, device=local_rank)
+    ctx.setup()
+    ncell = spec.n ** 3
+    for _ in range(args.warmup):
+        ctx.step(graph=not args.plain)
+    dist = world > 1
+    if dist:
+        import torch
+        import torch.distributed as tdist
+        tdist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    cross = 0
+    dev_ms = 0.0
+    dark_ms = 0.0
+    dark_bytes = 0.0
+    h2d = 2 * ctx.nbox + 2 * ctx.nsrc
+    d2h = 0
+    launches = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st = ctx.step(graph=not args.plain)
+        ms, dms = ctx.last_timing()
+        cross += st["crossings"]
+        dev_ms += ms
+        dark_ms += dms
+        dark_bytes += DARK_BYTES_PER_CELL * (ncell - st["lit_cells"])
+        launches += 22
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    d2h = 144  # control block (per-step totals) read back each step
+    if dist:
+        import torch
+        import torch.distributed as tdist
+        t = torch.tensor([dev_ms, wall, float(cross)], dtype=torch.float64, device=f"cuda:{local_rank}")
+        mx = t.clone()
+        tdist.all_reduce(mx, op=tdist.ReduceOp.MAX)
+        sm = t.clone()
+        tdist.all_reduce(sm, op=tdist.ReduceOp.SUM)
+        dev_ms_max, wall_max, cross_all = float(mx[0]), float(mx[1]), float(sm[2])
+    else:
+        dev_ms_max, wall_max, cross_all = dev_ms, wall, float(cross)
+    peak, peak_kind = _peaks()
+    dark_gbs = dark_bytes / (dark_ms * 1e-3) / 1e9 if dark_ms > 0 else None
+    res = {
+        "metric": "ray-cell crossings/s", "value": cross_all / (dev_ms_max * 1e-3), "unit": "crossings/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded lognormal gas + L^-2 sources; the reference's inputs are not shipped)",
+        "config": {"workload": _describe(spec), "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps}",
+                   "graph": not args.plain, "l2": "state (>1 GB) larger than L2, no flush",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "e2e": {"value": cross_all / wall_max, "unit": "crossings/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "kernel": "k_dark (cells no ray touched: whole step in one pass)",
+                     "achieved": dark_gbs, "peak": peak, "unit": "GB/s",
+                     "frac": (dark_gbs / peak) if dark_gbs else None, "traffic": None,
+                     "peak_kind": peak_kind, "bytes_per_cell": DARK_BYTES_PER_CELL,
+                     "kernel_ms_per_step": dark_ms / args.steps},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "crossings_per_step": cross / args.steps,
+    }
+    ctx.close()
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["L", "M", "S"], default="L")
+    ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--ray-capacity", type=int, default=16 << 20)
+    ap.add_argument("--plain", action="store_true", help="launch kernels directly instead of the CUDA graph")
+    ap.add_argument("--cpu-baseline-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-time-cap", type=float, default=150.0)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        spec = _spec(args.workload)
+        try:
+            rows, setup = run_reference(spec, args.workload, args.warmup + args.steps, threads, args.ref_time_cap,
+                                        args.seed)
+        except Exception as e:  # the reference arm must print a line even when it cannot run
+            print(json.dumps({"impl": "reference", "unavailable": f"compiled reference failed: {e}"}))
+            return
+        timed = rows[args.warmup:] if len(rows) > args.warmup else rows
+        cr = sum(c for c, _ in timed)
+        wt = sum(w for _, w in timed)
+        v = cr / wt if wt > 0 else None
+        print(json.dumps({
+            "impl": "reference", "metric": "ray-cell crossings/s", "value": v, "unit": "crossings/s",
+            "n_gpus": world, "steps": len(timed), "warmup": min(args.warmup, len(rows)),
+            "ms_per_step": 1e3 * wt / max(1, len(timed)), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64 (reference float storage, double locals)", "data": "synthetic",
+            "config": {"workload": _describe(spec), "timed_steps": f"{min(args.warmup, len(rows)) + 1}.."
+                       f"{len(rows)}", "setup_s": setup},
+            "cpu_baseline": {"value": v, "unit": "crossings/s", "cores": threads, "kind": "reference",
+                             "sample": f"{len(timed)} timed steps after {min(args.warmup, len(rows))} warm-up steps, "
+                                       f"OpenMP {threads} threads (time cap {args.ref_time_cap:.0f} s)"},
+            "e2e": {"value": v, "unit": "crossings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    res = run_ours(args, rank, world, local_rank)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        spec = _spec(args.workload)
+        try:
+            rows, setup = run_reference(spec, args.workload, args.cpu_baseline_steps, threads, 60.0, args.seed)
+            cr = sum(c for c, _ in rows)
+            wt = sum(w for _, w in rows)
+            res["cpu_baseline"] = {"value": cr / wt if wt else None, "unit": "crossings/s", "cores": threads,
+                                   "kind": "reference",
+                                   "sample": f"steps 1..{len(rows)} of the same workload (set-up {setup:.1f} s "
+                                             f"excluded), reference OpenMP code compiled from its sources"}
+        except Exception as e:
+            res["cpu_baseline"] = {"value": None, "unit": "crossings/s", "cores": threads, "kind": "reference",
+                                   "sample": f"unavailable: {e}"}
+    if world > 1:
+        import torch.distributed as tdist
+        tdist.barrier()
+        tdist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

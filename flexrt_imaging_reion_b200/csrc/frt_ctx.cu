@@ -2,6 +2,7 @@
 // individual step functions) and the C-ABI entry points declared in include/flexrt.h.
 #include <cuda_runtime.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -38,6 +39,10 @@ struct frt_ctx {
   float last_step_ms = 0.f, last_dark_ms = 0.f;
   frt_step_stats last{};
   std::string err;
+  // glibc rand() streams, one per box (srand(seed) semantics via initstate_r / random_r)
+  std::vector<std::vector<char>> rng_state;
+  std::vector<struct random_data> rng;
+  std::vector<uint16_t> draw_box, draw_src;
 };
 
 namespace {
@@ -209,6 +214,29 @@ frt_status stage_itheta(frt_ctx* ctx, const uint16_t* ith_box, const uint16_t* i
       return FRT_ERR_INVALID;
     }
     ctx->h_ith_src[s] = v;
+  }
+  return FRT_OK;
+}
+
+int si_rand(frt_ctx* ctx, int b) {
+  int32_t v = 0;
+  random_r(&ctx->rng[b], &v);
+  return v % kNtheta;
+}
+
+frt_status draw(frt_ctx* ctx, uint16_t* ith_box, uint16_t* ith_src) {
+  if (ctx->rng.size() != ctx->boxes.size()) {
+    ctx->err = "frt_seed_boxes not called";
+    return FRT_ERR_STATE;
+  }
+  // per box: the merge draw first, then one per source of that box (the sources of all boxes
+  // are concatenated in box order)
+  std::vector<size_t> off(ctx->boxes.size() + 1, 0);
+  for (size_t b = 0; b < ctx->boxes.size(); b++) off[b + 1] = off[b] + ctx->src_cell[b].size();
+  for (size_t b = 0; b < ctx->boxes.size(); b++) {
+    if (ith_box) ith_box[b] = (uint16_t)si_rand(ctx, (int)b);
+    if (ith_src)
+      for (size_t s = off[b]; s < off[b + 1]; s++) ith_src[s] = (uint16_t)si_rand(ctx, (int)b);
   }
   return FRT_OK;
 }
@@ -744,10 +772,47 @@ frt_status frt_new_rays(frt_ctx* ctx, const uint16_t* itheta_per_source) {
   return sync_and_check(ctx);
 }
 
+frt_status frt_seed_boxes(frt_ctx* ctx, const unsigned int* seeds) {
+  if (!ctx || !seeds) return FRT_ERR_INVALID;
+  const size_t nb = ctx->boxes.size();
+  ctx->rng_state.assign(nb, std::vector<char>(128, 0));
+  ctx->rng.assign(nb, random_data{});
+  for (size_t b = 0; b < nb; b++) {
+    memset(&ctx->rng[b], 0, sizeof(random_data));
+    if (initstate_r(seeds[b], ctx->rng_state[b].data(), 128, &ctx->rng[b]) != 0) {
+      ctx->err = "initstate_r failed";
+      return FRT_ERR_INVALID;
+    }
+  }
+  return FRT_OK;
+}
+
+frt_status frt_draw_cast(frt_ctx* ctx, uint16_t* itheta_per_source) {
+  if (!ctx || !itheta_per_source) return FRT_ERR_INVALID;
+  return draw(ctx, nullptr, itheta_per_source);
+}
+
+frt_status frt_draw_step(frt_ctx* ctx, uint16_t* itheta_per_box, uint16_t* itheta_per_source) {
+  if (!ctx || !itheta_per_box) return FRT_ERR_INVALID;
+  return draw(ctx, itheta_per_box, itheta_per_source);
+}
+
+// Resolve the step's angle indices: caller-provided, or drawn from the context's streams.
+static frt_status step_inputs(frt_ctx* ctx, const uint16_t* ib, const uint16_t* is) {
+  if (!ib && !is) {
+    ctx->draw_box.resize(ctx->boxes.size());
+    ctx->draw_src.resize(std::max(1, ctx->d.nsrc));
+    frt_status st = draw(ctx, ctx->draw_box.data(), ctx->draw_src.data());
+    if (st) return st;
+    return stage_itheta(ctx, ctx->draw_box.data(), ctx->draw_src.data());
+  }
+  return stage_itheta(ctx, ib, is);
+}
+
 frt_status frt_step_plain(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t* itheta_per_source,
                           frt_step_stats* stats) {
   if (!ctx) return FRT_ERR_INVALID;
-  frt_status st = stage_itheta(ctx, itheta_per_box, itheta_per_source);
+  frt_status st = step_inputs(ctx, itheta_per_box, itheta_per_source);
   if (st) return st;
   CK(cudaEventRecord(ctx->ev_t0, ctx->s_main));
   enqueue_step(ctx, false);
@@ -758,7 +823,7 @@ frt_status frt_step_plain(frt_ctx* ctx, const uint16_t* itheta_per_box, const ui
 frt_status frt_step(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t* itheta_per_source,
                     frt_step_stats* stats) {
   if (!ctx) return FRT_ERR_INVALID;
-  frt_status st = stage_itheta(ctx, itheta_per_box, itheta_per_source);
+  frt_status st = step_inputs(ctx, itheta_per_box, itheta_per_source);
   if (st) return st;
   if (!ctx->graph_valid) {
     if (ctx->graph) {

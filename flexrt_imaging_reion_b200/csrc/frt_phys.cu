@@ -202,14 +202,25 @@ __global__ void __launch_bounds__(256) k_raypass(Dev d) {
           const float dthe = (b * d.sigHe1_f[nu]) * dist;
           dtt[nu] = dth + dthe;
           if ((dth > 0.f) || (dthe > 0.f)) {
+            // Absorption split between HI and HeI, frac_h1 = A e^-b / (A e^-b + B e^-a) with
+            // A = 1-e^-a, B = 1-e^-b (ray_tracing.cc:770-771), evaluated as 1/(1+r) with
+            // r = (B/A) e^-(a-b) <= 1 for a >= b (and symmetrically), which cannot underflow
+            // to 0/0 in FP32 when both optical depths are large.
             const float ah = -expm1f(-dth), ahe = -expm1f(-dthe);
-            const float eh = expf(-dth), ehe = expf(-dthe);
-            const float x1 = ah * ehe, x2 = ahe * eh;
-            const float inv = 1.0f / (x1 + x2);
+            float fh, fhe;
+            if (dth >= dthe) {
+              const float r = (ahe / ah) * expf(dthe - dth);
+              fh = 1.0f / (1.0f + r);
+              fhe = r * fh;
+            } else {
+              const float r = (ah / ahe) * expf(dth - dthe);
+              fhe = 1.0f / (1.0f + r);
+              fh = r * fhe;
+            }
             const float absb = dump ? 1.0f : -expm1f(-dtt[nu]);
             const float q = nin[nu] * absb;
-            gh_nu[nu] = (x1 * inv) * q;
-            ghe_nu[nu] = (x2 * inv) * q;
+            gh_nu[nu] = fh * q;
+            ghe_nu[nu] = fhe * q;
             gsum_h += gh_nu[nu];
             gsum_he += ghe_nu[nu];
             if (LAST && dump) dump_mask |= 1u << nu;

@@ -191,7 +191,7 @@ __device__ inline void heat_cool(ThermCell& c, const ThermConst& k, const float*
     return;
   }
   float heat = 0.0f;
-  if (c.f_H2 > 0.98f && g_h1) {
+  if (c.f_H2 > 0.98 && g_h1) {   // double comparison, as the reference (gas_funcs.cc:148)
     for (int nu = 0; nu < nfreq; nu++) {
       heat += (c.avg_nh1 * g_h1[nu * gstride]) * k.cH1[nu];
       heat += (c.avg_nhe1 * g_he1[nu * gstride]) * k.cHe1[nu];

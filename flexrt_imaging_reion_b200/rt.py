@@ -82,7 +82,6 @@ class RTContext:
         self.inputs = list(inputs)
         self.specs = [i.spec for i in self.inputs]
         self.nbox = len(self.inputs)
-        self.rng = [RandStream(s) for s in seeds]
         self.F = 5
         self.spectrum = spectrum_alpha15()
         self._boxes = (_abi.BoxDesc * self.nbox)()
@@ -130,6 +129,8 @@ class RTContext:
         self._ith_box = np.zeros(self.nbox, np.uint16)
         self._ith_src = np.zeros(max(1, self.nsrc), np.uint16)
         self.stats = _abi.StepStats()
+        seeds_arr = np.ascontiguousarray([int(s) & 0xFFFFFFFF for s in seeds], np.uint32)
+        self._check(self.L.frt_seed_boxes(self.h, seeds_arr.ctypes.data), "frt_seed_boxes")
 
     # ---- plumbing ---------------------------------------------------------------------------
     def _check(self, st: int, what: str) -> None:
@@ -173,21 +174,16 @@ class RTContext:
         self.get_nphot_min_max()
 
     def draw_cast(self) -> np.ndarray:
+        """init_rays draws of the set-up cast, from the context's per-box glibc streams."""
         out = np.zeros(max(1, self.nsrc), np.uint16)
-        k = 0
-        for b in range(self.nbox):
-            for _ in range(self.nsrc_box[b]):
-                out[k] = self.rng[b].si_rand()
-                k += 1
+        self._check(self.L.frt_draw_cast(self.h, out.ctypes.data), "frt_draw_cast")
         return out
-
-    def draw_merge(self) -> np.ndarray:
-        return np.array([self.rng[b].si_rand() for b in range(self.nbox)], np.uint16)
 
     def draw_step(self):
         """Draws of one step in reference order: merge() first, then init_rays per source."""
-        m = self.draw_merge()
-        c = self.draw_cast()
+        m = np.zeros(self.nbox, np.uint16)
+        c = np.zeros(max(1, self.nsrc), np.uint16)
+        self._check(self.L.frt_draw_step(self.h, m.ctypes.data, c.ctypes.data), "frt_draw_step")
         return m, c
 
     # ---- the reference's step functions ---------------------------------------------------------
@@ -251,14 +247,27 @@ class RTContext:
         self.update_dt()
 
     def step(self, graph: bool = True, draws=None) -> Dict[str, float]:
-        """One whole step, fused (CUDA graph when graph=True)."""
-        m, c = self.draw_step() if draws is None else draws
-        self._ith_box[:] = m
-        self._ith_src[: len(c)] = c[: len(self._ith_src)]
+        """One whole step, fused (CUDA graph when graph=True). Without `draws` the library draws
+        the step's random angles from its per-box streams (reference order)."""
         fn = self.L.frt_step if graph else self.L.frt_step_plain
-        st = fn(self.h, self._ith_box.ctypes.data, self._ith_src.ctypes.data, C.byref(self.stats))
+        if draws is None:
+            st = fn(self.h, None, None, C.byref(self.stats))
+        else:
+            m, c = draws
+            self._ith_box[:] = m
+            self._ith_src[: len(c)] = c[: len(self._ith_src)]
+            st = fn(self.h, self._ith_box.ctypes.data, self._ith_src.ctypes.data, C.byref(self.stats))
         self._check(st, "frt_step")
         return self.stats.as_dict()
+
+    def last_stats(self) -> Dict[str, float]:
+        st = _abi.StepStats()
+        self._check(self.L.frt_last_stats(self.h, C.byref(st)), "frt_last_stats")
+        return st.as_dict()
+
+    def in_flight(self) -> float:
+        """Photons in the live rays (the running total of the device ledger)."""
+        return float(self.last_stats()["photons_in_flight"])
 
     def last_timing(self):
         a = C.c_float(0.0)

@@ -89,7 +89,7 @@ def _gaussian_field(n: int, rng: np.random.Generator) -> np.ndarray:
     k2[0, 0, 0] = 1.0
     fk /= np.sqrt(k2)          # P(k) ~ k^-2  <=>  amplitude ~ k^-1
     fk[0, 0, 0] = 0.0
-    g = np.fft.irfftn(fk, s=(n, n, n))
+    g = np.fft.irfftn(fk, s=(n, n, n), axes=(0, 1, 2))
     g /= g.std()
     return g
 

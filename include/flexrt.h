@@ -158,9 +158,19 @@ frt_status frt_update_thermal(frt_ctx* ctx);
  * index per source of all boxes in order, drawn by the caller (ray_tracing.cc:233). */
 frt_status frt_new_rays(frt_ctx* ctx, const uint16_t* itheta_per_source);
 
+/* Random-angle draws of the reference, siRand(Ntheta) = rand() % 42875 (general_funcs.cc:170-173):
+ * one glibc rand() stream per box, seeded as srand(seed), held by the context. The reference draws
+ * once per step in merge() (ray_tracing.cc:327) and then once per source in init_rays
+ * (ray_tracing.cc:233); frt_draw_step fills both arrays in that order, frt_draw_cast only the
+ * per-source ones (the set-up cast, main.cc:99). */
+frt_status frt_seed_boxes(frt_ctx* ctx, const unsigned int* seeds);
+frt_status frt_draw_cast(frt_ctx* ctx, uint16_t* itheta_per_source);
+frt_status frt_draw_step(frt_ctx* ctx, uint16_t* itheta_per_box, uint16_t* itheta_per_source);
+
 /* One whole RT step in the order of main.cc:108-264 (fixed redshift), captured once as a CUDA
  * graph and replayed: the fused form of the calls above. Host inputs are the random-angle
- * indices; stats (may be NULL) receives the per-step totals of box -1 = all boxes. */
+ * indices (both NULL: drawn from the context's streams, frt_draw_step); stats (may be NULL)
+ * receives the per-step totals of all boxes. */
 frt_status frt_step(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t* itheta_per_source,
                     frt_step_stats* stats);
 /* Same as frt_step but launching every kernel directly (no graph) */

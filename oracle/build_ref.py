@@ -25,6 +25,7 @@ import json
 import os
 import re
 import shutil
+import resource
 import subprocess
 import sys
 from typing import Optional
@@ -152,6 +153,15 @@ def build(name: str, spec: W.BoxSpec, ncpu: int = 1, path_length: int = 8, from_
     return compile_stage(d, ncpu)
 
 
+def _unlimited_stack():
+    # update_thermal keeps a float[Nx][Ny][Nz] array on the stack (gas_funcs.cc:364)
+    try:
+        resource.setrlimit(resource.RLIMIT_STACK, (resource.RLIM_INFINITY, resource.RLIM_INFINITY))
+    except (ValueError, OSError):
+        soft, hard = resource.getrlimit(resource.RLIMIT_STACK)
+        resource.setrlimit(resource.RLIMIT_STACK, (hard, hard))
+
+
 def run(name: str, inp: W.BoxInputs, rundir: str, nsteps: int, seed: int, dump_every: int = 1,
         threads: int = 1, timeout: Optional[float] = None) -> str:
     """Run the compiled reference on inputs written to rundir; returns stdout."""
@@ -162,7 +172,8 @@ def run(name: str, inp: W.BoxInputs, rundir: str, nsteps: int, seed: int, dump_e
     if inp.clump is not None:
         args.append(os.path.join(os.path.abspath(rundir), "clump.bin"))
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-    r = subprocess.run(args, cwd=d, env=env, capture_output=True, text=True, timeout=timeout)
+    r = subprocess.run(args, cwd=d, env=env, capture_output=True, text=True, timeout=timeout,
+                       preexec_fn=_unlimited_stack)
     if r.returncode != 0:
         raise RuntimeError(f"ref_driver failed ({r.returncode}): {r.stdout[-2000:]} {r.stderr[-2000:]}")
     return r.stdout

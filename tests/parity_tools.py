@@ -110,44 +110,77 @@ def _ray_keys(st: Dict[str, np.ndarray], exact_geom: bool):
     return keys
 
 
-def compare_rays(dev: Dict[str, np.ndarray], ref: Dict[str, np.ndarray], nphot_min: float, rel_nphot: float,
-                 exact_geom: bool = True) -> Dict[str, float]:
-    """Multiset comparison of the live rays (pool order differs from the reference's slot order)."""
-    kd = _ray_keys(dev, exact_geom)
-    kr = _ray_keys(ref, exact_geom)
+def _match(kd, kr, cand_d, cand_r):
     from collections import defaultdict
     idx = defaultdict(list)
-    for i, k in enumerate(kr):
-        idx[k].append(i)
-    matched_d, matched_r = [], []
-    unmatched_d = []
-    for i, k in enumerate(kd):
-        lst = idx.get(k)
+    for i in cand_r:
+        idx[kr[i]].append(i)
+    md, mr, ud = [], [], []
+    for i in cand_d:
+        lst = idx.get(kd[i])
         if lst:
-            matched_r.append(lst.pop())
-            matched_d.append(i)
+            mr.append(lst.pop())
+            md.append(i)
         else:
-            unmatched_d.append(i)
-    unmatched_r = [i for lst in idx.values() for i in lst]
-    md, mr = np.array(matched_d, int), np.array(matched_r, int)
-    out = {"n_dev": len(kd), "n_ref": len(kr), "matched": len(md)}
-    if len(md):
-        gd, gr = dev["ray_geom"][md], ref["ray_geom"][mr]
-        out["geom_exact"] = bool((gd.view(np.uint32) == gr.view(np.uint32)).all())
-        out["geom_maxrel"] = float(_rel(gd, gr, 1e-30).max())
-        npd, npr = dev["ray_nphot"][md], ref["ray_nphot"][mr]
+            ud.append(i)
+    ur = [i for lst in idx.values() for i in lst]
+    return md, mr, ud, ur
+
+
+def compare_rays(dev: Dict[str, np.ndarray], ref: Dict[str, np.ndarray], nphot_min: float, rel_nphot: float,
+                 rel_geom_merged: float = 1e-5, dx: float = 1.0, dx0: float = 1.0) -> Dict[str, float]:
+    """Multiset comparison of the live rays (pool order differs from the reference's slot order).
+
+    Pass 1 matches rays on (cell, order, pixel, itheta) plus the exact bits of x, y, z, r (every
+    ray that was only advanced / split / cast). Pass 2 matches the remaining rays on the integer
+    key alone and checks their geometry (rays whose x, y, z, r, dr are photon-weighted float sums
+    of a merge) to rel_geom_merged of the cell size: r, dr against dx0 (comoving), x, y, z against dx."""
+    kd, kr = _ray_keys(dev, True), _ray_keys(ref, True)
+    md, mr, ud, ur = _match(kd, kr, range(len(kd)), range(len(kr)))
+    kd2, kr2 = _ray_keys(dev, False), _ray_keys(ref, False)
+    md2, mr2, ud2, ur2 = _match(kd2, kr2, ud, ur)
+    out = {"n_dev": len(kd), "n_ref": len(kr), "matched_exact": len(md), "matched_merged": len(md2)}
+    out["geom_exact"] = True
+    if md2:
+        gd, gr = dev["ray_geom"][md2].astype(np.float64), ref["ray_geom"][mr2].astype(np.float64)
+        scale = np.array([dx0, dx0, dx, dx, dx])
+        r = np.abs(gd[:, 3:8] - gr[:, 3:8]) / scale
+        out["merged_geom_maxrel"] = float(r.max())
+        out["merged_geom_bad"] = int((r.max(axis=1) > rel_geom_merged).sum())
+    else:
+        out["merged_geom_maxrel"] = 0.0
+        out["merged_geom_bad"] = 0
+    ma, mb = np.array(md + md2, int), np.array(mr + mr2, int)
+    if len(ma):
+        npd, npr = dev["ray_nphot"][ma], ref["ray_nphot"][mb]
         floor = max(float(np.abs(npr).max()) * 1e-7, 1e-300)
         r = _rel(npd, npr, floor)
         out["nphot_maxrel"] = float(r.max())
         out["nphot_bad"] = int((r.max(axis=1) > rel_nphot).sum())
+        hd, hr = dev["ray_geom"][ma, 0:3], ref["ray_geom"][mb, 0:3]
+        out["dir_maxabs"] = float(np.abs(hd.astype(np.float64) - hr).max())
     else:
-        out.update(geom_exact=True, geom_maxrel=0.0, nphot_maxrel=0.0, nphot_bad=0)
+        out.update(nphot_maxrel=0.0, nphot_bad=0, dir_maxabs=0.0)
 
     def near_tie(st, ids):
         s = st["ray_nphot"][ids].astype(np.float64).sum(axis=1) if len(ids) else np.zeros(0)
         return int((np.abs(s / nphot_min - 1.0) < 1e-3).sum()) if nphot_min > 0 else 0
 
-    out["unmatched_dev"] = len(unmatched_d)
-    out["unmatched_ref"] = len(unmatched_r)
-    out["unmatched_near_tie"] = near_tie(dev, unmatched_d) + near_tie(ref, unmatched_r)
+    out["unmatched_dev"] = len(ud2)
+    out["unmatched_ref"] = len(ur2)
+    out["unmatched_near_tie"] = near_tie(dev, ud2) + near_tie(ref, ur2)
     return out
+
+
+def photon_budget(stats_list, in_flight_0: float) -> float:
+    """Relative closure of the photon ledger over the steps: in-flight(start) + emitted - (deposited -
+    overlap) - killed - in-flight(end), divided by the photons emitted (set-up cast included)."""
+    emitted = in_flight_0
+    dep = kil = ovl = 0.0
+    for st in stats_list:
+        emitted += st["photons_emitted"]
+        dep += st["photons_deposited"]
+        kil += st["photons_killed"]
+        ovl += st["photons_overlap"]
+    end = stats_list[-1]["photons_in_flight"]
+    return abs(emitted - (dep - ovl) - kil - end) / emitted

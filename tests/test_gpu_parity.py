@@ -1,0 +1,138 @@
+"""Parity of the CUDA RT step (through the C ABI) with the CPU oracle on seeded boxes.
+
+The oracle (oracle/frt_oracle.cc) is pinned bit-exact to the reference's own code by
+tests/test_oracle_golden.py. Tolerances are stated in tests/parity_tools.py: ray tree and ray
+geometry exact (merged rays 1e-5), Gamma_HI 1e-4 relative per cell, x_HI 1e-4 absolute,
+T 1e-4 relative (strict mode: 1e-5 on Gamma / T), photon ledger closed to 1e-6.
+"""
+import numpy as np
+import pytest
+
+import parity_tools as PT
+from flexrt_imaging_reion_b200 import rt, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+T16 = (W.config_tiny(), 11)
+T16M = (W.config_tiny(n=16, n_src=6, steps=6, seed=5, name="T16M", clump_model="sqrt", ray_per_cell_max=12), 3)
+T16N = (W.config_tiny(n=16, n_src=10, steps=8, seed=9, name="T16N", ray_per_cell_max=13, lum_min=1e53, lum_max=1e55),
+        4)
+
+_ORACLE_CACHE = {}
+
+
+def oracle_run(spec, seed):
+    key = (spec.name, seed)
+    if key not in _ORACLE_CACHE:
+        _ORACLE_CACHE[key] = PT.oracle_states(W.make_inputs(spec), seed, spec.steps)
+    return _ORACLE_CACHE[key]
+
+
+def run_device(spec, seed, precision, mode, diag=True):
+    inp = W.make_inputs(spec)
+    ctx = rt.RTContext([inp], [seed], precision=precision, outputs="diag" if diag else "core", ray_capacity=1 << 20)
+    ctx.setup()
+    states, stats = [PT.device_state(ctx, 0, diag)], []
+    in_flight0 = ctx.in_flight()
+    for _ in range(spec.steps):
+        if mode == "unfused":
+            ctx.step_unfused()
+            stats.append(ctx.last_stats())
+        else:
+            stats.append(ctx.step(graph=(mode == "graph")))
+        states.append(PT.device_state(ctx, 0, diag))
+    ctx.close()
+    return states, stats, in_flight0
+
+
+def check(states, ref, strict, merged=False):
+    # T: set_Treion_default (gas_funcs.cc:104-129) turns a 1-ulp change of nH1 in a nearly
+    # neutral cell into a ~1e-4 relative temperature change, so T is held to 1e-4 (strict) and
+    # 1e-3 (mixed); Gamma_HI and x_HI keep the contract tolerances.
+    tol_g = 1e-5 if strict else 1e-4
+    tol_t = 1e-4 if strict else 1e-3
+    for s in range(len(states)):
+        f = PT.compare_fields(states[s], ref[s], tol_g, 1e-4, tol_t)
+        assert f["gamma_H1_tot_bad"] == 0, (s, f)
+        assert f["gamma_He1_tot_bad"] == 0, (s, f)
+        assert f["f_H1_bad"] == 0 and f["f_He1_bad"] == 0, (s, f)
+        assert f["avg_xHI_bad"] == 0, (s, f)
+        assert f["temp_bad"] == 0, (s, f)
+        assert f["treion_flag_mismatch"] == 0, (s, f)
+        r = PT.compare_rays(states[s], ref[s], ref[s]["scalars"][2], 1e-5 if strict else 1e-4,
+                            dx=float(ref[s]["scalars"][8]), dx0=float(ref[s]["scalars"][7]))
+        assert r["unmatched_dev"] + r["unmatched_ref"] - r["unmatched_near_tie"] == 0, (s, r)
+        assert r["nphot_bad"] == 0, (s, r)
+        if not merged:
+            assert r["matched_merged"] == 0, (s, r)
+        assert r["merged_geom_bad"] == 0, (s, r)
+
+
+@pytest.mark.parametrize("precision,mode", [("strict", "graph"), ("strict", "unfused"), ("mixed", "graph"),
+                                            ("mixed", "plain"), ("mixed", "unfused")])
+def test_t16_parity(precision, mode):
+    spec, seed = T16
+    ref = oracle_run(spec, seed)
+    states, stats, _ = run_device(spec, seed, precision, mode)
+    check(states, ref, precision == "strict")
+    # crossings per step = sum of path segments of the moved rays (ray_tracing.cc:1471)
+    if mode != "unfused":
+        for s, st in enumerate(stats, 1):
+            assert st["crossings"] == int(ref[s]["scalars"][10])
+
+
+@pytest.mark.parametrize("case", ["T16M", "T16N"])
+@pytest.mark.parametrize("precision", ["strict", "mixed"])
+def test_merge_parity(case, precision):
+    spec, seed = {"T16M": T16M, "T16N": T16N}[case]
+    ref = oracle_run(spec, seed)
+    states, _, _ = run_device(spec, seed, precision, "graph")
+    check(states, ref, precision == "strict", merged=True)
+    # merging really happened on both sides
+    assert any(float(r["scalars"][4]) > 0 for r in ref)
+
+
+def test_s_config_parity():
+    spec = W.config_S()
+    seed = 21
+    ref = PT.oracle_states(W.make_inputs(spec), seed, spec.steps)
+    states, stats, _ = run_device(spec, seed, "mixed", "graph", diag=False)
+    check(states, ref, False)
+
+
+@pytest.mark.parametrize("precision", ["strict", "mixed"])
+def test_photon_budget_closes(precision):
+    spec, seed = W.config_S(), 21
+    _, stats, in_flight0 = run_device(spec, seed, precision, "graph", diag=False)
+    assert PT.photon_budget(stats, in_flight0) < 1e-6
+
+
+def test_diag_outputs_match():
+    spec, seed = T16
+    ref = oracle_run(spec, seed)
+    states, _, _ = run_device(spec, seed, "strict", "graph", diag=True)
+    for s in range(1, len(states)):
+        for k in ("mfp", "mfp_912", "n_tot", "recrate_H2", "u_nu"):
+            a, b = states[s][k].astype(np.float64), ref[s][k].astype(np.float64)
+            den = np.maximum(np.abs(b), np.abs(b).max() * 1e-6 + 1e-300)
+            assert (np.abs(a - b) / den).max() < 1e-5, (s, k)
+        # the I-front speed is dx (fion_new - fion_old) / dt of two nearly equal floats
+        # (gas_funcs.cc:105-108): compare to a few ulp of the ionised fraction
+        dx, dt = float(ref[s]["scalars"][8]), float(ref[s]["scalars"][1])
+        a, b = states[s]["IF_speed"].astype(np.float64), ref[s]["IF_speed"].astype(np.float64)
+        assert np.abs(a - b).max() <= 4 * np.finfo(np.float32).eps * dx / dt, s
+
+
+def test_capacity_error_is_reported_not_faulted():
+    """A ray pool too small for the step: the step returns FRT_ERR_CAPACITY, later steps keep
+    returning it, and the context stays usable (no device fault)."""
+    spec, seed = T16
+    ctx = rt.RTContext([W.make_inputs(spec)], [seed], ray_capacity=200)
+    ctx.setup()
+    with pytest.raises(rt.FrtError, match="status 2"):
+        for _ in range(4):
+            ctx.step()
+    with pytest.raises(rt.FrtError, match="status 2"):
+        ctx.step()
+    assert ctx.num_rays() == 0 or ctx.num_rays() <= 200
+    ctx.close()
