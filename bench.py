@@ -167,7 +167,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     spec = _spec(args.workload)
     inp = W.make_inputs(spec)
     ctx = rt.RTContext([inp], [args.seed + rank], precision="mixed", outputs="core",
-                       ray_capacity=args.ray_capacity, device=local_rank)
+                       ray_capacity=args.ray_capacity, lit_capacity=args.lit_capacity, device=local_rank)
     ctx.setup()
     ncell = spec.n ** 3
     for _ in range(args.warmup):
@@ -243,6 +243,7 @@ def main():
     ap.add_argument("--workload", choices=["L", "M", "S"], default="L")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--ray-capacity", type=int, default=16 << 20)
+    ap.add_argument("--lit-capacity", type=int, default=0, help="0 = all cells")
     ap.add_argument("--plain", action="store_true", help="launch kernels directly instead of the CUDA graph")
     ap.add_argument("--cpu-baseline-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")

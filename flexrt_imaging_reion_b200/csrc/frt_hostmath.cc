@@ -108,6 +108,7 @@ void box_params(BoxP* B, const frt_config* cfg, const frt_box_desc* bd, long lon
   B->t = 0.f;
   B->vol = ((double)dx) * ((double)dx) * ((double)dx);               // ray_tracing.cc:747
   B->kdep = 1e60 / (double)B->dt / B->vol;
+  B->kdep_f = (float)B->kdep;
   B->rkill = bd->rkill_cm;
   B->nphot_min = 0.;
   B->nphot_max = 0.;

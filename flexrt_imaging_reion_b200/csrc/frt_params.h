@@ -40,6 +40,7 @@ struct BoxP {
   float dt, t;
   double vol;                // dx*dy*dz in double
   double kdep;               // phot_norm / dt / vol
+  float kdep_f;              // the same in float (mixed-precision deposits)
   double rkill;              // comoving cm; 0 = off
   double nphot_min, nphot_max;
   float nphot_merge, split_thr;

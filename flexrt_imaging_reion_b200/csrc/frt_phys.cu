@@ -35,6 +35,19 @@ __device__ __forceinline__ T block_sum(T v) {
 
 __device__ __forceinline__ int box_of_cell(const Dev& d, long long gc) { return d.tile_box[gc >> kTileShift]; }
 
+// 1 - e^-x and e^-x, both to full relative precision, for one transcendental: for x > 0.5 the
+// transmission is formed directly and the absorbed part as 1 - e (>= 0.39, no cancellation);
+// below, the absorbed part comes from expm1 and the transmission as 1 - a (>= 0.61).
+__device__ __forceinline__ void absorb_transmit(float x, float* a, float* e) {
+  if (x > 0.5f) {
+    *e = expf(-x);
+    *a = 1.0f - *e;
+  } else {
+    *a = -expm1f(-x);
+    *e = 1.0f - *a;
+  }
+}
+
 // ---- clear the previous step's lit marks ------------------------------------------------
 __global__ void k_clear_lit(Dev d) {
   const int n = min(d.ctl->n_lit, d.lit_cap);
@@ -94,6 +107,13 @@ __global__ void __launch_bounds__(256) k_raypass(Dev d) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int ns = d.nseg[i];
     if (ns == 0 || d.dead[i]) continue;
+    // The first pass turns every stored segment's cell index into its lit slot, before the walk:
+    // a walk may stop early (a dumped ray), but later iterations still read all segments.
+    if (FIRST)
+      for (int p = 0; p < ns; p++) {
+        int* sp = d.seg + (size_t)p * cap + i;
+        *sp = d.lit_slot[*sp];
+      }
     const BoxP& B = d.box[A.box[i]];
     const double nmin = B.nphot_min;
     float nph[FRT_MAX_FREQ];
@@ -107,11 +127,7 @@ __global__ void __launch_bounds__(256) k_raypass(Dev d) {
       for (int nu = 0; nu < FRT_MAX_FREQ; nu++) { tau_h1[nu] = 0.; tau_he1[nu] = 0.; }
       const double dt = B.dt, vol = B.vol;
       for (int p = 0; p < ns; p++) {
-        int slot = d.seg[(size_t)p * cap + i];
-        if (FIRST) {
-          slot = d.lit_slot[slot];
-          d.seg[(size_t)p * cap + i] = slot;
-        }
+        const int slot = d.seg[(size_t)p * cap + i];
         if (slot < 0) continue;
         const float dist = d.seg_dist[(size_t)p * cap + i];
         const float a = d.l_avg_h[slot], b = d.l_avg_he[slot];
@@ -169,84 +185,90 @@ __global__ void __launch_bounds__(256) k_raypass(Dev d) {
         }
       }
     } else {
-      float tau[FRT_MAX_FREQ];
+      // Mixed precision: per bin the photon count is carried from segment to segment by its
+      // transmission e^-dtau instead of recomputing e^-tau, and each bin costs one transcendental
+      // when HeI does not absorb there (sigma_HeI = 0 below 24.59 eV) and two when it does.
+      float nin[FRT_MAX_FREQ];
 #pragma unroll
-      for (int nu = 0; nu < FRT_MAX_FREQ; nu++) tau[nu] = 0.f;
-      const double kdep = B.kdep;
+      for (int nu = 0; nu < FRT_MAX_FREQ; nu++) nin[nu] = nph[nu];
+      const float kdep = B.kdep_f;
       for (int p = 0; p < ns; p++) {
-        int slot = d.seg[(size_t)p * cap + i];
-        if (FIRST) {
-          slot = d.lit_slot[slot];
-          d.seg[(size_t)p * cap + i] = slot;
-        }
+        const int slot = d.seg[(size_t)p * cap + i];
         if (slot < 0) continue;
         const float dist = d.seg_dist[(size_t)p * cap + i];
         const float a = d.l_avg_h[slot], b = d.l_avg_he[slot];
-        float nin[FRT_MAX_FREQ], dtt[FRT_MAX_FREQ];
         float total = 0.f;
 #pragma unroll
-        for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
-          nin[nu] = (nu < F) ? nph[nu] * expf(-tau[nu]) : 0.f;
-          total += nin[nu];
-        }
+        for (int nu = 0; nu < FRT_MAX_FREQ; nu++) total += (nu < F) ? nin[nu] : 0.f;
         const bool dump = (double)total < nmin;
         float gsum_h = 0.f, gsum_he = 0.f;
-        float gh_nu[FRT_MAX_FREQ], ghe_nu[FRT_MAX_FREQ];
+        float gh_nu[FRT_MAX_FREQ], ghe_nu[FRT_MAX_FREQ], tr[FRT_MAX_FREQ];
 #pragma unroll
         for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
           gh_nu[nu] = 0.f;
           ghe_nu[nu] = 0.f;
-          dtt[nu] = 0.f;
+          tr[nu] = 1.f;
           if (nu >= F) continue;
           const float dth = (a * d.sigH1_f[nu]) * dist;
           const float dthe = (b * d.sigHe1_f[nu]) * dist;
-          dtt[nu] = dth + dthe;
-          if ((dth > 0.f) || (dthe > 0.f)) {
-            // Absorption split between HI and HeI, frac_h1 = A e^-b / (A e^-b + B e^-a) with
-            // A = 1-e^-a, B = 1-e^-b (ray_tracing.cc:770-771), evaluated as 1/(1+r) with
-            // r = (B/A) e^-(a-b) <= 1 for a >= b (and symmetrically), which cannot underflow
-            // to 0/0 in FP32 when both optical depths are large.
-            const float ah = -expm1f(-dth), ahe = -expm1f(-dthe);
-            float fh, fhe;
-            if (dth >= dthe) {
-              const float r = (ahe / ah) * expf(dthe - dth);
-              fh = 1.0f / (1.0f + r);
+          float ah, eh;
+          absorb_transmit(dth, &ah, &eh);
+          float fh, fhe, absb, e;
+          if (dthe > 0.f) {
+            float ahe, ehe;
+            absorb_transmit(dthe, &ahe, &ehe);
+            e = eh * ehe;
+            absb = ah + eh * ahe;                   // 1 - e^-(dth+dthe) without cancellation
+            // frac_h1 = A e^-b / (A e^-b + B e^-a) (ray_tracing.cc:770-771)
+            const float x1 = ah * ehe, x2 = ahe * eh;
+            if (x1 + x2 > 1e-30f) {
+              const float inv = __fdividef(1.0f, x1 + x2);
+              fh = x1 * inv;
+              fhe = x2 * inv;
+            } else if (dth >= dthe) {                // both optical depths huge: ratio form
+              const float r = __fdividef(ahe, ah) * expf(dthe - dth);
+              fh = __fdividef(1.0f, 1.0f + r);
               fhe = r * fh;
             } else {
-              const float r = (ah / ahe) * expf(dth - dthe);
-              fhe = 1.0f / (1.0f + r);
+              const float r = __fdividef(ah, ahe) * expf(dth - dthe);
+              fhe = __fdividef(1.0f, 1.0f + r);
               fh = r * fhe;
             }
-            const float absb = dump ? 1.0f : -expm1f(-dtt[nu]);
-            const float q = nin[nu] * absb;
-            gh_nu[nu] = fh * q;
-            ghe_nu[nu] = fhe * q;
-            gsum_h += gh_nu[nu];
-            gsum_he += ghe_nu[nu];
-            if (LAST && dump) dump_mask |= 1u << nu;
+          } else {
+            e = eh;
+            absb = ah;
+            fh = (dth > 0.f) ? 1.0f : 0.0f;           // frac_h1 = 1, frac_he1 = 0 when dtau_he1 = 0
+            fhe = 0.f;
           }
+          const float q = nin[nu] * (dump ? 1.0f : absb);
+          gh_nu[nu] = fh * q;
+          ghe_nu[nu] = fhe * q;
+          gsum_h += gh_nu[nu];
+          gsum_he += ghe_nu[nu];
+          tr[nu] = e;
+          if (LAST && dump && (fh + fhe) > 0.f) dump_mask |= 1u << nu;
         }
-        const double wh = kdep / (double)a, whe = kdep / (double)b;
-        if (gsum_h != 0.f) atomicAdd(&d.l_acc_g[slot], (float)((double)gsum_h * wh));
-        if (gsum_he != 0.f) atomicAdd(&d.l_acc_ghe[slot], (float)((double)gsum_he * whe));
+        const float wh = __fdividef(kdep, a), whe = __fdividef(kdep, b);
+        if (gsum_h != 0.f) atomicAdd(&d.l_acc_g[slot], gsum_h * wh);
+        if (gsum_he != 0.f) atomicAdd(&d.l_acc_ghe[slot], gsum_he * whe);
         if (LAST) {
 #pragma unroll
           for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
             if (nu >= F) continue;
             atomicAdd(&d.l_ngam[(size_t)nu * L + slot], nin[nu]);
-            if (gh_nu[nu] != 0.f) atomicAdd(&d.l_acc_nu_h[(size_t)nu * L + slot], (float)((double)gh_nu[nu] * wh));
-            if (ghe_nu[nu] != 0.f) atomicAdd(&d.l_acc_nu_he[(size_t)nu * L + slot], (float)((double)ghe_nu[nu] * whe));
+            if (gh_nu[nu] != 0.f) atomicAdd(&d.l_acc_nu_h[(size_t)nu * L + slot], gh_nu[nu] * wh);
+            if (ghe_nu[nu] != 0.f) atomicAdd(&d.l_acc_nu_he[(size_t)nu * L + slot], ghe_nu[nu] * whe);
           }
           dep += (double)gsum_h + (double)gsum_he;
         }
 #pragma unroll
-        for (int nu = 0; nu < FRT_MAX_FREQ; nu++) tau[nu] += dtt[nu];
+        for (int nu = 0; nu < FRT_MAX_FREQ; nu++) nin[nu] *= tr[nu];
         if (dump) { dumped = true; break; }
       }
       if (LAST) {
         float s = 0.f;
         for (int nu = 0; nu < F; nu++) {
-          nph[nu] = nph[nu] * expf(-tau[nu]);
+          nph[nu] = nin[nu];
           A.nphot[(size_t)nu * cap + i] = nph[nu];
           s += nph[nu];
         }
@@ -385,7 +407,7 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d) {
 // 5 C2Ray updates with Gamma = 0 (ray_tracing.cc:941-1136), the last-iteration bookkeeping
 // (1138-1209) and, when THERMAL, update_thermal (gas_funcs.cc:362-411), all in registers.
 template <bool STRICT, bool THERMAL>
-__global__ void __launch_bounds__(256) k_dark(Dev d) {
+__global__ void __launch_bounds__(256, 4) k_dark(Dev d) {
   const long long ncell = d.ncell_total;
   const bool diag = d.outputs == FRT_OUT_DIAG;
   const int I = d.itercount;
@@ -413,8 +435,8 @@ __global__ void __launch_bounds__(256) k_dark(Dev d) {
       const float nelec_f = nH - a + nHe - bb;
       const double nelec_d = (double)nelec_f;
       a_prev = a;
-      const float an = c2ray_species<STRICT>(H, 0.f, nelec_d, nelec_f, a, dt, last, &nh1_end);
-      const float bn = c2ray_species<STRICT>(He, 0.f, nelec_d, nelec_f, bb, dt, last, &nhe1_end);
+      const float an = c2ray_species<STRICT, true>(H, 0.f, nelec_d, nelec_f, a, dt, last, &nh1_end);
+      const float bn = c2ray_species<STRICT, true>(He, 0.f, nelec_d, nelec_f, bb, dt, last, &nhe1_end);
       a = an;
       bb = bn;
       nelec_last = nelec_d;

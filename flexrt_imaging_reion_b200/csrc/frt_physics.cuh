@@ -67,24 +67,32 @@ __device__ inline double rcrB_He2_d(double T) { return kKB * T * alphaB_He2_d(T)
 __device__ inline double free_free_d(double T) { return 1.42e-27 * pow(T, 0.5) * 1.30; }
 
 // ---- the same rates in FP32 -------------------------------------------------------------
-__device__ inline float alphaB_H2_f(float T) {
-  const float x = kLamH1 / T;
-  return 2.753e-14f * (x * sqrtf(x)) / powf(1.0f + powf(x * (1.0f / 2.740f), 0.407f), 2.2420f);
+// x = lambda(T) = 2 Eth eV2K / T enters every rate as a power law, so each rate is evaluated
+// from lT = log2(T) as exp2 of a linear combination of log2 x = log2(2 Eth eV2K) - lT.
+// log2(2 Eth eV2K) for Eth = 13.6 / 24.59 / 54.42 eV, and log2 of the break points 2.74, 2.25:
+constexpr float kLog2LamH1 = 18.26793572782709f;
+constexpr float kLog2LamHe1 = 19.122400811285473f;
+constexpr float kLog2_274 = 1.4541758931858022f;
+constexpr float kLog2_225 = 1.1699250014423124f;
+
+__device__ __forceinline__ float alphaB_H2_lt(float lT) {     // rates.cc:135-138
+  const float L = kLog2LamH1 - lT;
+  const float q = exp2f(0.407f * (L - kLog2_274));
+  return 2.753e-14f * exp2f(1.5f * L - 2.2420f * log2f(1.0f + q));
 }
-__device__ inline float alphaB_He2_f(float T) {
-  const float x = kLamHe1 / T;
-  return 1.26e-14f * powf(x, 0.750f);
+__device__ __forceinline__ float alphaB_He2_lt(float lT) {    // rates.cc:147-151
+  return 1.26e-14f * exp2f(0.750f * (kLog2LamHe1 - lT));
 }
-__device__ inline float Dalpha_He2_f(float T) {
+__device__ __forceinline__ float rcrB_H2_lt(float T, float lT) {   // rates.cc:183-187
+  const float L = kLog2LamH1 - lT;
+  const float q = exp2f(0.376f * (L - kLog2_225));
+  return 3.435e-30f * T * exp2f(1.970f * L - 3.720f * log2f(1.0f + q));
+}
+__device__ inline float Dalpha_He2_f(float T) {               // rates.cc:168-171
   const float x = kLamHe2 / T;
-  return 1.90e-3f * (1.0f / (T * sqrtf(T))) * expf(-0.375f * x) * (1.0f + 0.3f * expf(-0.075f * x));
+  return 1.90e-3f * __fdividef(1.0f, T * sqrtf(T)) * expf(-0.375f * x) * (1.0f + 0.3f * expf(-0.075f * x));
 }
-__device__ inline float rcrB_H2_f(float T) {
-  const float x = kLamH1 / T;
-  return 3.435e-30f * T * powf(x, 1.970f) / powf(1.0f + powf(x * (1.0f / 2.250f), 0.376f), 3.720f);
-}
-__device__ inline float rcrB_He2_f(float T) { return (float)kKB * T * alphaB_He2_f(T); }
-__device__ inline float free_free_f(float T) { return (float)(1.42e-27 * 1.30) * sqrtf(T); }
+__device__ __forceinline__ float free_free_f(float T) { return (float)(1.42e-27 * 1.30) * sqrtf(T); }
 
 // Recombination coefficients of one cell at the start of a step (ray_tracing.cc:655-674).
 template <bool STRICT>
@@ -96,8 +104,9 @@ __device__ inline void recomb_coeffs(float temp, float* rec_h2, float* rec_he2) 
     if ((temp >= 3e4) && (temp <= 1e6)) he2 += (float)Dalpha_He2_d(tm);
     *rec_he2 = he2;
   } else {
-    *rec_h2 = alphaB_H2_f(tm);
-    float he2 = alphaB_He2_f(tm);
+    const float lT = log2f(tm);
+    *rec_h2 = alphaB_H2_lt(lT);
+    float he2 = alphaB_He2_lt(lT);
     if ((temp >= 3e4f) && (temp <= 1e6f)) he2 += Dalpha_He2_f(tm);
     *rec_he2 = he2;
   }
@@ -113,7 +122,9 @@ struct C2Species {
 // One C2Ray update of one species (ray_tracing.cc:1084-1113 and, on the last iteration,
 // 1116-1127). Returns the time-averaged neutral density; *n_end receives the end-of-step
 // neutral density when last is true.
-template <bool STRICT>
+// ZERO_GAMMA: the caller knows gamma = 0 (a cell no ray touched); x_eq = 0 and y_eq = rec/rec = 1
+// exactly, which the general form also yields, so both paths give the same bits.
+template <bool STRICT, bool ZERO_GAMMA = false>
 __device__ inline float c2ray_species(const C2Species& s, float gamma, double nelec_d, float nelec_f, float avg_prev,
                                       float dt, bool last, float* n_end) {
   if (STRICT) {
@@ -134,17 +145,17 @@ __device__ inline float c2ray_species(const C2Species& s, float gamma, double ne
   const bool fp64 = (s.y0 < 1e-3f) || (avg_prev < 1e-3f * s.n);
   if (fp64) {
     const double prd = (double)gamma + (double)s.crec * nelec_d;
-    const double yeq = ((double)s.crec * nelec_d) / prd;
+    const double yeq = ZERO_GAMMA ? 1.0 : ((double)s.crec * nelec_d) / prd;
     const double r = (double)dt * prd;
     const double em = -expm1(-r);  // 1 - e^-r
     const double yavg = yeq + ((double)s.y0 - yeq) * (em / r);
     if (last) *n_end = (float)((double)s.n * (yeq + ((double)s.y0 - yeq) * (1.0 - em)));
     return (float)((double)s.n * yavg);
   }
-  const float yeq = rec / pr;
+  const float yeq = ZERO_GAMMA ? 1.0f : rec / pr;   // exact division: 1 when gamma = 0
   const float r = dt * pr;
   const float em = -expm1f(-r);
-  const float yavg = yeq + (s.y0 - yeq) * (em / r);
+  const float yavg = yeq + (s.y0 - yeq) * __fdividef(em, r);
   if (last) *n_end = s.n * (yeq + (s.y0 - yeq) * (1.0f - em));
   return s.n * yavg;
 }
@@ -197,10 +208,11 @@ __device__ inline void heat_cool(ThermCell& c, const ThermConst& k, const float*
       heat += (c.avg_nhe1 * g_he1[nu * gstride]) * k.cHe1[nu];
     }
   }
+  const float lT = log2f(tm);
   const float nenh2 = c.ne * c.nH2;
   const float nenhe2 = c.ne * c.nHe2;
-  float cool = rcrB_H2_f(tm) * nenh2;
-  cool += rcrB_He2_f(tm) * nenhe2;
+  float cool = rcrB_H2_lt(tm, lT) * nenh2;
+  cool += ((float)kKB * tm * alphaB_He2_lt(lT)) * nenhe2;
   cool += free_free_f(tm) * (c.ne * (c.nH2 + c.nHe2));
   cool -= (k.compton_f * (2.726f * (1.0f + k.zz) - tm)) * c.ne;
   c.heat = heat;
@@ -218,9 +230,10 @@ __device__ inline float thermal_tstep(const ThermCell& c, const ThermConst& k) {
     return (m1 >= min_dt) ? m1 : min_dt;
   }
   const float c23 = (float)(2. / 3. / kKB);
-  const float dT_dt = c23 / c.n_tot * (c.heat - c.cool) - (k.hub2f + c.dne_dt / c.n_tot) * c.temp;
+  const float inv_n = __fdividef(1.0f, c.n_tot);
+  const float dT_dt = (c23 * inv_n) * (c.heat - c.cool) - (k.hub2f + c.dne_dt * inv_n) * c.temp;
   const float min_dt = 0.1f * k.dt;
-  const float cand = 0.1f * c.temp / fabsf(dT_dt);
+  const float cand = __fdividef(0.1f * c.temp, fabsf(dT_dt));
   const float m1 = (cand >= k.dt) ? k.dt : cand;
   return (m1 >= min_dt) ? m1 : min_dt;
 }
@@ -270,8 +283,9 @@ __device__ inline void thermal_update(ThermCell& c, const ThermConst& k, const f
                (1. + 2. * (double)(k.hub2f * 0.5f) * dt_temp + 1. / c.n_tot * c.dne_dt * dt_temp);
     } else {
       const float c23 = (float)(2. / 3. / kKB);
-      c.temp = (c.temp + (c23 / c.n_tot) * (c.heat - c.cool) * dt_temp) /
-               (1.0f + k.hub2f * dt_temp + (c.dne_dt / c.n_tot) * dt_temp);
+      const float inv_n = __fdividef(1.0f, c.n_tot);
+      c.temp = __fdividef(c.temp + (c23 * inv_n) * (c.heat - c.cool) * dt_temp,
+                          1.0f + k.hub2f * dt_temp + (c.dne_dt * inv_n) * dt_temp);
     }
     t_temp += dt_temp;
     ++guard;

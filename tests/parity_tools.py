@@ -128,7 +128,8 @@ def _match(kd, kr, cand_d, cand_r):
 
 
 def compare_rays(dev: Dict[str, np.ndarray], ref: Dict[str, np.ndarray], nphot_min: float, rel_nphot: float,
-                 rel_geom_merged: float = 1e-5, dx: float = 1.0, dx0: float = 1.0) -> Dict[str, float]:
+                 rel_geom_merged: float = 1e-5, dx: float = 1.0, dx0: float = 1.0,
+                 rel_nphot_merged: float = 1e-3) -> Dict[str, float]:
     """Multiset comparison of the live rays (pool order differs from the reference's slot order).
 
     Pass 1 matches rays on (cell, order, pixel, itheta) plus the exact bits of x, y, z, r (every
@@ -150,17 +151,21 @@ def compare_rays(dev: Dict[str, np.ndarray], ref: Dict[str, np.ndarray], nphot_m
     else:
         out["merged_geom_maxrel"] = 0.0
         out["merged_geom_bad"] = 0
+    # photon counts: rays matched exactly to rel_nphot; merged rays (float sums over the rays of a
+    # bin, accumulated in another order) to rel_nphot_merged
+    out.update(nphot_maxrel=0.0, nphot_bad=0, nphot_merged_maxrel=0.0, nphot_merged_bad=0, dir_maxabs=0.0)
+    allref = ref["ray_nphot"]
+    floor = max(float(np.abs(allref).max()) * 1e-7, 1e-300) if allref.size else 1e-300
+    for lab, ids_d, ids_r, tol in (("", md, mr, rel_nphot), ("_merged", md2, mr2, rel_nphot_merged)):
+        if not ids_d:
+            continue
+        r = _rel(dev["ray_nphot"][ids_d], ref["ray_nphot"][ids_r], floor)
+        out[f"nphot{lab}_maxrel"] = float(r.max())
+        out[f"nphot{lab}_bad"] = int((r.max(axis=1) > tol).sum())
     ma, mb = np.array(md + md2, int), np.array(mr + mr2, int)
     if len(ma):
-        npd, npr = dev["ray_nphot"][ma], ref["ray_nphot"][mb]
-        floor = max(float(np.abs(npr).max()) * 1e-7, 1e-300)
-        r = _rel(npd, npr, floor)
-        out["nphot_maxrel"] = float(r.max())
-        out["nphot_bad"] = int((r.max(axis=1) > rel_nphot).sum())
         hd, hr = dev["ray_geom"][ma, 0:3], ref["ray_geom"][mb, 0:3]
         out["dir_maxabs"] = float(np.abs(hd.astype(np.float64) - hr).max())
-    else:
-        out.update(nphot_maxrel=0.0, nphot_bad=0, dir_maxabs=0.0)
 
     def near_tie(st, ids):
         s = st["ray_nphot"][ids].astype(np.float64).sum(axis=1) if len(ids) else np.zeros(0)
