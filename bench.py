@@ -161,6 +161,17 @@ def run_reference(spec, name: str, steps: int, threads: int, time_cap_s: float, 
 
 
 # ---- our arm ---------------------------------------------------------------------------------
+def launches_per_step(spec, ray_capacity, itercount=5, hpx_lvl=0):
+    """Kernels one fused step launches: clear_lit, step_begin, advance, dark, lit_init,
+    itercount x (ray pass + lit pass), count, 3 merge set-up kernels (+4 binning kernels when the
+    pool can reach the merge threshold), compact, split, swap, cast."""
+    n = 1 + 1 + 1 + 1 + 1 + 2 * itercount + 1 + 3 + 3 + 1
+    num_thresh = (spec.ray_per_cell_max - 12 * 4 ** hpx_lvl) * spec.n ** 3
+    if num_thresh < ray_capacity:
+        n += 4
+    return n
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import numpy as np
     from flexrt_imaging_reion_b200 import workloads as W, rt
@@ -186,6 +197,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     h2d = 2 * ctx.nbox + 2 * ctx.nsrc
     d2h = 0
     launches = 0
+    lit = 0
+    per_step = launches_per_step(spec, args.ray_capacity)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         st = ctx.step(graph=not args.plain)
@@ -194,7 +207,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dev_ms += ms
         dark_ms += dms
         dark_bytes += DARK_BYTES_PER_CELL * (ncell - st["lit_cells"])
-        launches += 22
+        launches += per_step
+        lit += st["lit_cells"]
     wall = time.perf_counter() - t0
     clk = clocks.stop()
     d2h = 144  # control block (per-step totals) read back each step
@@ -229,6 +243,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "gpu_launches": launches,
         "clocks": clk,
         "crossings_per_step": cross / args.steps,
+        "lit_cells_per_step": lit / args.steps,
     }
     ctx.close()
     return res

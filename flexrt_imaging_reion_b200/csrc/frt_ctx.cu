@@ -374,7 +374,16 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
   AL(d.l_cell, L); AL(d.l_nh, L); AL(d.l_nhe, L); AL(d.l_y0h, L); AL(d.l_y0he, L); AL(d.l_crec_h, L);
   AL(d.l_crec_he, L); AL(d.l_rec_h2, L); AL(d.l_rec_he2, L); AL(d.l_avg_h, L); AL(d.l_avg_he, L);
   AL(d.l_nh1_old, L); AL(d.l_acc_g, L); AL(d.l_acc_ghe, L);
-  AL(d.l_acc_nu_h, L * d.F); AL(d.l_acc_nu_he, L * d.F); AL(d.l_ngam, L * d.F);
+  d.per_bin = (ctx->strict || cfg->outputs == FRT_OUT_DIAG) ? 1 : 0;
+  AL(d.l_ngam, L * d.F); AL(d.l_heat_h, L); AL(d.l_heat_he, L);
+  if (d.per_bin) {
+    AL(d.l_acc_nu_h, L * d.F);
+    AL(d.l_acc_nu_he, L * d.F);
+  }
+  for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
+    d.cH1_f[nu] = ctx->hbox[0].th.cH1[nu];
+    d.cHe1_f[nu] = ctx->hbox[0].th.cHe1[nu];
+  }
   const size_t R = (size_t)d.ray_cap;
   for (int p = 0; p < 2; p++) {
     RayPool& P = d.pool[p];
@@ -383,6 +392,7 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
     AL(P.r, R); AL(P.dr, R); AL(P.x, R); AL(P.y, R); AL(P.z, R); AL(P.time, R);
   }
   AL(d.seg, R * d.PL); AL(d.seg_dist, R * d.PL); AL(d.nseg, R); AL(d.dead, R);
+  AL(d.split_list, R / 4 + 1);
   // merge bins only when some box can reach its merge threshold with this pool size
   bool merge_reachable = false;
   for (int b = 0; b < cfg->nbox; b++) merge_reachable |= ctx->hbox[b].num_thresh < (long long)d.ray_cap;
@@ -625,6 +635,10 @@ frt_status frt_get_field(frt_ctx* ctx, int box, frt_field f, float* host) {
     case FRT_F_GAMMA_HE1_NU:
     case FRT_F_NGAM_NU: {
       const int base = (f == FRT_F_GAMMA_H1_NU) ? 2 : (f == FRT_F_GAMMA_HE1_NU ? 2 + F : 2 + 2 * F);
+      if (f != FRT_F_NGAM_NU && !d.per_bin) {
+        ctx->err = "per-bin rates are kept only with diag outputs or strict precision";
+        return FRT_ERR_STATE;
+      }
       std::vector<float> tmp(n);
       for (int nu = 0; nu < F; nu++) {
         st = sparse(base + nu, tmp.data());
@@ -942,3 +956,4 @@ frt_status frt_last_timing(frt_ctx* ctx, float* step_ms, float* cell_kernel_ms) 
 }
 
 }  // extern "C"
+

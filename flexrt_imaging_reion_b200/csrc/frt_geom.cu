@@ -459,10 +459,13 @@ __global__ void k_merge_final(Dev d, double pi_sf_3, double log4) {
   }
 }
 
-// split_rays + split_ray (rt_funcs.cc:211-237, ray_tracing.cc:482-619) fused with the
-// compaction into the next pool: live rays are copied, rays past rmax(l) become 4 children
-// at pixels 4*pn + n of order l+1, displaced by (v_child - v_parent) r0 dx/dx0.
-__global__ void __launch_bounds__(256) k_split_compact(Dev d) {
+// split_rays (rt_funcs.cc:211-237) fused with the compaction into the next pool, in two
+// kernels. k_compact decides per ray: a live ray is copied; a ray past rmax(l) with enough
+// photons reserves 4 slots and is put on the split list. k_split then builds the children one
+// thread per child (split_ray, ray_tracing.cc:482-619): pixels 4*pn + c of order l+1, displaced
+// by (v_child - v_parent) r0 dx/dx0. Keeping the child arithmetic (pix2vec, rotation, wrap) out
+// of the copy loop keeps the copy kernel light and spreads the children over 4x the threads.
+__global__ void __launch_bounds__(256) k_compact(Dev d) {
   const int cur = d.ctl->cur;
   const int nxt = cur ^ 1;
   const int n = d.ctl->nray[cur];
@@ -475,11 +478,12 @@ __global__ void __launch_bounds__(256) k_split_compact(Dev d) {
     const int i = i0 + threadIdx.x;
     bool live = (i < n) && !d.dead[i];
     bool split = false;
-    const BoxP* Bx = nullptr;
+    float s = 0.f;
     if (live) {
-      Bx = &d.box[A.box[i]];
+      const BoxP& B = d.box[A.box[i]];
       const int l = A.order[i];
-      split = (A.r[i] > Bx->rmax[l]) && (l < kLmax) && (sum_nphot(A, i, F, cap) > Bx->split_thr);
+      s = sum_nphot(A, i, F, cap);
+      split = (A.r[i] > B.rmax[l]) && (l < kLmax) && (s > B.split_thr);
     }
     const int want = live ? (split ? 4 : 1) : 0;
     const int pos = reserve(&d.ctl->nray[nxt], want);
@@ -490,61 +494,12 @@ __global__ void __launch_bounds__(256) k_split_compact(Dev d) {
     }
     if (!split) {
       copy_ray(A, i, Bp, pos, F, cap);
-      inflight += (double)sum_nphot(A, i, F, cap);
+      inflight += (double)s;
       continue;
     }
-    const BoxP& B = *Bx;
     nsplit += 1;
-    const int N = B.n;
-    const int l = A.order[i];
-    const int pn = A.pixel[i];
-    const float r0 = A.r[i], x0o = A.x[i], y0o = A.y[i], z0o = A.z[i], time = A.time[i];
-    const uint16_t ith = A.itheta[i];
-    const float* m = d.rot + (size_t)ith * 18;
-    const double vox = A.xh[i], voy = A.yh[i], voz = A.zh[i];
-    const int ind = A.cell[i];
-    const int ic = ind / B.nn, jc = (ind - ic * B.nn) / N, kc = ind - ic * B.nn - jc * N;
-    const float rmax = B.rmax[l + 1];
-    const float rs = r0 * B.scale;
-    for (int c = 0; c < 4; c++) {
-      const int j = pos + c;
-      const int pix = 4 * pn + c;
-      double vx, vy, vz;
-      hpn::pix2vec(l + 1, pix, &vx, &vy, &vz);
-      float nx, ny, nz;
-      rot_apply(m, (float)vx, (float)vy, (float)vz, &nx, &ny, &nz);
-      float x0 = (float)((double)x0o + ((double)nx - vox) * (double)rs);
-      float y0 = (float)((double)y0o + ((double)ny - voy) * (double)rs);
-      float z0 = (float)((double)z0o + ((double)nz - voz) * (double)rs);
-      int icn = ic, jcn = jc, kcn = kc;
-      for (int g = 0; g < 64 && x0 > B.dx; g++) { x0 -= B.dx; icn = imod(icn + 1, N); }
-      for (int g = 0; g < 64 && x0 < 0.f; g++) { x0 += B.dx; icn = imod(icn - 1, N); }
-      for (int g = 0; g < 64 && y0 > B.dx; g++) { y0 -= B.dx; jcn = imod(jcn + 1, N); }
-      for (int g = 0; g < 64 && y0 < 0.f; g++) { y0 += B.dx; jcn = imod(jcn - 1, N); }
-      for (int g = 0; g < 64 && z0 > B.dx; g++) { z0 -= B.dx; kcn = imod(kcn + 1, N); }
-      for (int g = 0; g < 64 && z0 < 0.f; g++) { z0 += B.dx; kcn = imod(kcn - 1, N); }
-      Bp.cell[j] = icn * B.nn + jcn * N + kcn;
-      Bp.box[j] = A.box[i];
-      Bp.order[j] = (int16_t)(l + 1);
-      Bp.pixel[j] = pix;
-      Bp.itheta[j] = ith;
-      Bp.xh[j] = nx;
-      Bp.yh[j] = ny;
-      Bp.zh[j] = nz;
-      float s = 0.f;
-      for (int nu = 0; nu < F; nu++) {
-        const float q = (float)((double)A.nphot[(size_t)nu * cap + i] / 4.);
-        Bp.nphot[(size_t)nu * cap + j] = q;
-        s += q;
-      }
-      inflight += (double)s;
-      Bp.r[j] = r0;
-      Bp.dr[j] = rmax - r0;
-      Bp.x[j] = x0;
-      Bp.y[j] = y0;
-      Bp.z[j] = z0;
-      Bp.time[j] = time;
-    }
+    const int k = atomicAdd(&d.ctl->n_split, 1);
+    d.split_list[k] = make_int2(i, pos);
   }
   nsplit = block_sum(nsplit);
   inflight = block_sum(inflight);
@@ -552,6 +507,66 @@ __global__ void __launch_bounds__(256) k_split_compact(Dev d) {
     if (nsplit) atomicAdd((unsigned long long*)&d.ctl->split, (unsigned long long)nsplit);
     if (inflight != 0.0) atomicAdd(&d.ctl->in_flight, inflight * kPhotNorm);
   }
+}
+
+__global__ void __launch_bounds__(256) k_split(Dev d) {
+  const int cur = d.ctl->cur;
+  const RayPool A = d.pool[cur];
+  const RayPool Bp = d.pool[cur ^ 1];
+  const int cap = d.ray_cap, F = d.F;
+  const int nchild = 4 * d.ctl->n_split;
+  double inflight = 0.0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nchild; t += gridDim.x * blockDim.x) {
+    const int2 e = d.split_list[t >> 2];
+    const int c = t & 3;
+    const int i = e.x, j = e.y + c;
+    const BoxP& B = d.box[A.box[i]];
+    const int N = B.n;
+    const int l = A.order[i];
+    const int pix = 4 * A.pixel[i] + c;
+    const uint16_t ith = A.itheta[i];
+    const float r0 = A.r[i];
+    const float rs = r0 * B.scale;
+    double vx, vy, vz;
+    hpn::pix2vec(l + 1, pix, &vx, &vy, &vz);
+    float nx, ny, nz;
+    rot_apply(d.rot + (size_t)ith * 18, (float)vx, (float)vy, (float)vz, &nx, &ny, &nz);
+    float x0 = (float)((double)A.x[i] + ((double)nx - (double)A.xh[i]) * (double)rs);
+    float y0 = (float)((double)A.y[i] + ((double)ny - (double)A.yh[i]) * (double)rs);
+    float z0 = (float)((double)A.z[i] + ((double)nz - (double)A.zh[i]) * (double)rs);
+    const int ind = A.cell[i];
+    const int ic = ind / B.nn, jc = (ind - ic * B.nn) / N, kc = ind - ic * B.nn - jc * N;
+    int icn = ic, jcn = jc, kcn = kc;
+    for (int g = 0; g < 64 && x0 > B.dx; g++) { x0 -= B.dx; icn = imod(icn + 1, N); }
+    for (int g = 0; g < 64 && x0 < 0.f; g++) { x0 += B.dx; icn = imod(icn - 1, N); }
+    for (int g = 0; g < 64 && y0 > B.dx; g++) { y0 -= B.dx; jcn = imod(jcn + 1, N); }
+    for (int g = 0; g < 64 && y0 < 0.f; g++) { y0 += B.dx; jcn = imod(jcn - 1, N); }
+    for (int g = 0; g < 64 && z0 > B.dx; g++) { z0 -= B.dx; kcn = imod(kcn + 1, N); }
+    for (int g = 0; g < 64 && z0 < 0.f; g++) { z0 += B.dx; kcn = imod(kcn - 1, N); }
+    Bp.cell[j] = icn * B.nn + jcn * N + kcn;
+    Bp.box[j] = A.box[i];
+    Bp.order[j] = (int16_t)(l + 1);
+    Bp.pixel[j] = pix;
+    Bp.itheta[j] = ith;
+    Bp.xh[j] = nx;
+    Bp.yh[j] = ny;
+    Bp.zh[j] = nz;
+    float s = 0.f;
+    for (int nu = 0; nu < F; nu++) {
+      const float q = (float)((double)A.nphot[(size_t)nu * cap + i] / 4.);
+      Bp.nphot[(size_t)nu * cap + j] = q;
+      s += q;
+    }
+    inflight += (double)s;
+    Bp.r[j] = r0;
+    Bp.dr[j] = B.rmax[l + 1] - r0;
+    Bp.x[j] = x0;
+    Bp.y[j] = y0;
+    Bp.z[j] = z0;
+    Bp.time[j] = A.time[i];
+  }
+  inflight = block_sum(inflight);
+  if (threadIdx.x == 0 && inflight != 0.0) atomicAdd(&d.ctl->in_flight, inflight * kPhotNorm);
 }
 
 __global__ void k_swap(Dev d) {
@@ -664,7 +679,9 @@ void launch_merge(const Dev& d, int grid, cudaStream_t s) {
 }
 
 void launch_split_compact(const Dev& d, int grid, cudaStream_t s) {
-  k_split_compact<<<grid, 256, 0, s>>>(d);
+  cudaMemsetAsync(&d.ctl->n_split, 0, sizeof(int), s);
+  k_compact<<<grid, 256, 0, s>>>(d);
+  k_split<<<grid, 256, 0, s>>>(d);
   k_swap<<<1, 1, 0, s>>>(d);
 }
 

@@ -40,7 +40,7 @@ struct Ctl {
   int n_lit_prev;
   unsigned err;
   int any_merge;           // some box has nphot_merge > 0
-  int pad;
+  int n_split;             // entries of the split list this step
   long long rays_moved, crossings, split, merged, killed, cast;
   double emitted, deposited, killed_ph, overlap, in_flight;
 };
@@ -80,6 +80,9 @@ struct Dev {
   float *l_nh, *l_nhe, *l_y0h, *l_y0he, *l_crec_h, *l_crec_he, *l_rec_h2, *l_rec_he2;
   float *l_avg_h, *l_avg_he, *l_nh1_old, *l_acc_g, *l_acc_ghe;
   float *l_acc_nu_h, *l_acc_nu_he, *l_ngam;   // [F][lit_cap]
+  float *l_heat_h, *l_heat_he;              // bin-weighted photo-heating sums (mixed, core outputs)
+  int per_bin;                               // keep per-bin rates (diag outputs or strict)
+  float cH1_f[FRT_MAX_FREQ], cHe1_f[FRT_MAX_FREQ];  // h (h_eV nu - Eth)/h_eV
   // rays
   RayPool pool[2];
   int* seg;                // [PL][ray_cap]
@@ -88,6 +91,7 @@ struct Dev {
   uint8_t* dead;
   int* ray_bin;            // merge bin of a candidate or -1
   uint8_t* merged_flag;
+  int2* split_list;         // (parent ray, first child slot) of the rays split this step
   int* bin_base;           // [ncell_total * 12*4^lm] or NULL when merging is unreachable
   // sources
   int* src_cell;           // local cell

@@ -83,10 +83,14 @@ __global__ void k_lit_init(Dev d) {
     d.l_avg_he[s] = d.nHe1[gc];
     d.l_acc_g[s] = 0.f;
     d.l_acc_ghe[s] = 0.f;
+    d.l_heat_h[s] = 0.f;
+    d.l_heat_he[s] = 0.f;
     for (int nu = 0; nu < F; nu++) {
-      d.l_acc_nu_h[(size_t)nu * L + s] = 0.f;
-      d.l_acc_nu_he[(size_t)nu * L + s] = 0.f;
       d.l_ngam[(size_t)nu * L + s] = 0.f;
+      if (STRICT || d.per_bin) {
+        d.l_acc_nu_h[(size_t)nu * L + s] = 0.f;
+        d.l_acc_nu_he[(size_t)nu * L + s] = 0.f;
+      }
     }
   }
 }
@@ -252,13 +256,21 @@ __global__ void __launch_bounds__(256) k_raypass(Dev d) {
         if (gsum_h != 0.f) atomicAdd(&d.l_acc_g[slot], gsum_h * wh);
         if (gsum_he != 0.f) atomicAdd(&d.l_acc_ghe[slot], gsum_he * whe);
         if (LAST) {
+          float hh = 0.f, hhe = 0.f;
 #pragma unroll
           for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
             if (nu >= F) continue;
             atomicAdd(&d.l_ngam[(size_t)nu * L + slot], nin[nu]);
-            if (gh_nu[nu] != 0.f) atomicAdd(&d.l_acc_nu_h[(size_t)nu * L + slot], gh_nu[nu] * wh);
-            if (ghe_nu[nu] != 0.f) atomicAdd(&d.l_acc_nu_he[(size_t)nu * L + slot], ghe_nu[nu] * whe);
+            if (d.per_bin) {
+              if (gh_nu[nu] != 0.f) atomicAdd(&d.l_acc_nu_h[(size_t)nu * L + slot], gh_nu[nu] * wh);
+              if (ghe_nu[nu] != 0.f) atomicAdd(&d.l_acc_nu_he[(size_t)nu * L + slot], ghe_nu[nu] * whe);
+            }
+            hh += gh_nu[nu] * d.cH1_f[nu];
+            hhe += ghe_nu[nu] * d.cHe1_f[nu];
           }
+          // photo-heating weights sum_nu Gamma_nu h (h_eV nu - Eth)/h_eV (gas_funcs.cc:155-158)
+          if (hh != 0.f) atomicAdd(&d.l_heat_h[slot], hh * wh);
+          if (hhe != 0.f) atomicAdd(&d.l_heat_he[slot], hhe * whe);
           dep += (double)gsum_h + (double)gsum_he;
         }
 #pragma unroll
@@ -387,7 +399,13 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d) {
       c.f_H2 = f.f_H2;
       c.avg_nh1 = a_new;
       c.avg_nhe1 = b_new;
-      thermal_update<STRICT>(c, B.th, d.l_acc_nu_h + s, d.l_acc_nu_he + s, L, d.F, d.nhe_to_nh);
+      HeatSrc hs{d.l_acc_nu_h + s, d.l_acc_nu_he + s, L, 0.f, 0.f, 1};
+      if (!STRICT && !d.per_bin) {
+        hs.mode = 2;
+        hs.hh = d.l_heat_h[s];
+        hs.hhe = d.l_heat_he[s];
+      }
+      thermal_update<STRICT>(c, B.th, hs, d.F, d.nhe_to_nh);
       d.temp[gc] = c.temp;
       d.heat[gc] = c.heat;
       d.cool[gc] = c.cool;
@@ -481,7 +499,8 @@ __global__ void __launch_bounds__(256, 4) k_dark(Dev d) {
       c.f_H2 = f.f_H2;
       c.avg_nh1 = a;
       c.avg_nhe1 = bb;
-      thermal_update<STRICT>(c, B.th, nullptr, nullptr, 0, d.F, d.nhe_to_nh);
+      const HeatSrc hs{nullptr, nullptr, 0, 0.f, 0.f, 0};
+      thermal_update<STRICT>(c, B.th, hs, d.F, d.nhe_to_nh);
       d.temp[gc] = c.temp;
       d.heat[gc] = c.heat;
       d.cool[gc] = c.cool;
@@ -525,10 +544,12 @@ __global__ void __launch_bounds__(256) k_thermal_all(Dev d) {
     c.avg_nh1 = d.avg_nh1[gc];
     c.avg_nhe1 = d.avg_nhe1[gc];
     const int slot = d.lit_slot[gc];
-    if (slot >= 0)
-      thermal_update<STRICT>(c, B.th, d.l_acc_nu_h + slot, d.l_acc_nu_he + slot, L, d.F, d.nhe_to_nh);
-    else
-      thermal_update<STRICT>(c, B.th, nullptr, nullptr, 0, d.F, d.nhe_to_nh);
+    HeatSrc hs{nullptr, nullptr, 0, 0.f, 0.f, 0};
+    if (slot >= 0) {
+      if (!STRICT && !d.per_bin) hs = HeatSrc{nullptr, nullptr, 0, d.l_heat_h[slot], d.l_heat_he[slot], 2};
+      else hs = HeatSrc{d.l_acc_nu_h + slot, d.l_acc_nu_he + slot, L, 0.f, 0.f, 1};
+    }
+    thermal_update<STRICT>(c, B.th, hs, d.F, d.nhe_to_nh);
     d.temp[gc] = c.temp;
     d.heat[gc] = c.heat;
     d.cool[gc] = c.cool;

@@ -154,9 +154,19 @@ __device__ inline float c2ray_species(const C2Species& s, float gamma, double ne
   }
   const float yeq = ZERO_GAMMA ? 1.0f : rec / pr;   // exact division: 1 when gamma = 0
   const float r = dt * pr;
-  const float em = -expm1f(-r);
-  const float yavg = yeq + (s.y0 - yeq) * __fdividef(em, r);
-  if (last) *n_end = s.n * (yeq + (s.y0 - yeq) * (1.0f - em));
+  float em_r, ex;   // (1 - e^-r)/r and e^-r
+  if (r < 1e-2f) {
+    // Taylor series, truncation error below r^4/120 < 1e-10: the usual case of a cell that is
+    // only recombining (r = dt C alpha n_e is ~1e-6 .. 1e-3)
+    em_r = 1.0f - r * (0.5f - r * ((1.0f / 6.0f) - r * (1.0f / 24.0f)));
+    ex = 1.0f - r * (1.0f - r * (0.5f - r * ((1.0f / 6.0f) - r * (1.0f / 24.0f))));
+  } else {
+    const float em = -expm1f(-r);
+    em_r = __fdividef(em, r);
+    ex = 1.0f - em;
+  }
+  const float yavg = yeq + (s.y0 - yeq) * em_r;
+  if (last) *n_end = s.n * (yeq + (s.y0 - yeq) * ex);
   return s.n * yavg;
 }
 
@@ -167,12 +177,25 @@ struct ThermCell {
   float if_speed, inc_flux;
 };
 
+// Photo-ionisation input of the heating term. The reference sums over bins
+// avg_nh1 gamma_H1_nu h (h_eV nu - Eth)/h_eV (gas_funcs.cc:155-158); that needs either the
+// per-bin rates of the cell (mode 1) or, equivalently, their bin-weighted sums
+// sum_nu gamma_nu c_nu accumulated by the last ray pass (mode 2). Mode 0: no deposit.
+struct HeatSrc {
+  const float* g_h1;
+  const float* g_he1;
+  int stride;
+  float hh, hhe;
+  int mode;
+};
+
 // update_heat_cool (gas_funcs.cc:134-242) for subgrid = FALSE, case B, recombination /
-// free-free / Compton cooling on, collisional terms off. g_h1 / g_he1 point at the per-bin
-// photo-ionisation rates of the cell (NULL = all zero, a cell no ray touched).
+// free-free / Compton cooling on, collisional terms off.
 template <bool STRICT>
-__device__ inline void heat_cool(ThermCell& c, const ThermConst& k, const float* g_h1, const float* g_he1, int gstride,
-                                 int nfreq) {
+__device__ inline void heat_cool(ThermCell& c, const ThermConst& k, const HeatSrc& hs, int nfreq) {
+  const float* g_h1 = hs.mode == 1 ? hs.g_h1 : nullptr;
+  const float* g_he1 = hs.g_he1;
+  const int gstride = hs.stride;
   const float tm = (c.temp >= kTempMin) ? c.temp : kTempMin;   // maxd(temp_min, temp)
   if (STRICT) {
     float heat = 0;
@@ -202,10 +225,14 @@ __device__ inline void heat_cool(ThermCell& c, const ThermConst& k, const float*
     return;
   }
   float heat = 0.0f;
-  if (c.f_H2 > 0.98 && g_h1) {   // double comparison, as the reference (gas_funcs.cc:148)
-    for (int nu = 0; nu < nfreq; nu++) {
-      heat += (c.avg_nh1 * g_h1[nu * gstride]) * k.cH1[nu];
-      heat += (c.avg_nhe1 * g_he1[nu * gstride]) * k.cHe1[nu];
+  if (c.f_H2 > 0.98) {   // double comparison, as the reference (gas_funcs.cc:148)
+    if (g_h1) {
+      for (int nu = 0; nu < nfreq; nu++) {
+        heat += (c.avg_nh1 * g_h1[nu * gstride]) * k.cH1[nu];
+        heat += (c.avg_nhe1 * g_he1[nu * gstride]) * k.cHe1[nu];
+      }
+    } else if (hs.mode == 2) {
+      heat = c.avg_nh1 * hs.hh + c.avg_nhe1 * hs.hhe;
     }
   }
   const float lT = log2f(tm);
@@ -268,8 +295,8 @@ __device__ inline void treion_default(ThermCell& c, const ThermConst& k, float n
 
 // update_thermal for one cell (gas_funcs.cc:362-411, temp_ev = TRUE, subgrid = FALSE).
 template <bool STRICT>
-__device__ inline void thermal_update(ThermCell& c, const ThermConst& k, const float* g_h1, const float* g_he1,
-                                      int gstride, int nfreq, float nhe_to_nh) {
+__device__ inline void thermal_update(ThermCell& c, const ThermConst& k, const HeatSrc& hs, int nfreq,
+                                      float nhe_to_nh) {
   float t_temp = 0.f;
   treion_default<STRICT>(c, k, nhe_to_nh);
   int guard = 0;
@@ -277,7 +304,7 @@ __device__ inline void thermal_update(ThermCell& c, const ThermConst& k, const f
     const float ts = thermal_tstep<STRICT>(c, k);
     const float rem = k.dt - t_temp;
     const float dt_temp = (ts >= rem) ? rem : ts;
-    heat_cool<STRICT>(c, k, g_h1, g_he1, gstride, nfreq);
+    heat_cool<STRICT>(c, k, hs, nfreq);
     if (STRICT) {
       c.temp = (c.temp + 2. / 3. / kKB / c.n_tot * (c.heat - c.cool) * dt_temp) /
                (1. + 2. * (double)(k.hub2f * 0.5f) * dt_temp + 1. / c.n_tot * c.dne_dt * dt_temp);

@@ -48,9 +48,10 @@ DEVICE_FIELDS = {
     "nH": "NH", "nHe": "NHE", "nH1": "NH1", "nHe1": "NHE1", "ne": "NE", "f_H1": "F_H1", "f_He1": "F_HE1",
     "f_H2": "F_H2", "temp": "TEMP", "avg_nh1": "AVG_NH1", "avg_nhe1": "AVG_NHE1", "gamma_H1_tot": "GAMMA_H1_TOT",
     "gamma_He1_tot": "GAMMA_HE1_TOT", "heat_rate": "HEAT_RATE", "cool_rate": "COOL_RATE", "treion": "TREION",
-    "gamma_H1_nu": "GAMMA_H1_NU", "gamma_He1_nu": "GAMMA_HE1_NU", "ngam_nu": "NGAM_NU", "rho": "RHO",
+    "ngam_nu": "NGAM_NU", "rho": "RHO",
 }
-DIAG_FIELDS = {"mfp": "MFP", "mfp_912": "MFP_912", "recrate_H2": "RECRATE_H2", "n_tot": "N_TOT",
+# per-bin rates are kept by the device only with diag outputs (or strict precision)
+DIAG_FIELDS = {"gamma_H1_nu": "GAMMA_H1_NU", "gamma_He1_nu": "GAMMA_HE1_NU", "mfp": "MFP", "mfp_912": "MFP_912", "recrate_H2": "RECRATE_H2", "n_tot": "N_TOT",
                "dne_dt": "DNE_DT", "IF_speed": "IF_SPEED", "u_nu": "U_NU"}
 
 
@@ -110,20 +111,29 @@ def _ray_keys(st: Dict[str, np.ndarray], exact_geom: bool):
     return keys
 
 
-def _match(kd, kr, cand_d, cand_r):
+def _match(kd, kr, cand_d, cand_r, sd=None, sr=None):
+    """Pair rays with equal keys. Several rays can share a key (same cell, order, pixel and
+    angle index but different radius, e.g. after a merge); with sort values sd / sr they are
+    paired in sorted order inside each key group."""
     from collections import defaultdict
-    idx = defaultdict(list)
+    idx_r, idx_d = defaultdict(list), defaultdict(list)
     for i in cand_r:
-        idx[kr[i]].append(i)
-    md, mr, ud = [], [], []
+        idx_r[kr[i]].append(i)
     for i in cand_d:
-        lst = idx.get(kd[i])
-        if lst:
-            mr.append(lst.pop())
-            md.append(i)
-        else:
-            ud.append(i)
-    ur = [i for lst in idx.values() for i in lst]
+        idx_d[kd[i]].append(i)
+    md, mr, ud, ur = [], [], [], []
+    for k, ld in idx_d.items():
+        lr = idx_r.pop(k, [])
+        if sd is not None and len(ld) > 1:
+            ld = sorted(ld, key=lambda i: sd[i])
+            lr = sorted(lr, key=lambda i: sr[i])
+        n = min(len(ld), len(lr))
+        md += ld[:n]
+        mr += lr[:n]
+        ud += ld[n:]
+        ur += lr[n:]
+    for lr in idx_r.values():
+        ur += lr
     return md, mr, ud, ur
 
 
@@ -139,7 +149,8 @@ def compare_rays(dev: Dict[str, np.ndarray], ref: Dict[str, np.ndarray], nphot_m
     kd, kr = _ray_keys(dev, True), _ray_keys(ref, True)
     md, mr, ud, ur = _match(kd, kr, range(len(kd)), range(len(kr)))
     kd2, kr2 = _ray_keys(dev, False), _ray_keys(ref, False)
-    md2, mr2, ud2, ur2 = _match(kd2, kr2, ud, ur)
+    md2, mr2, ud2, ur2 = _match(kd2, kr2, ud, ur, dev["ray_geom"][:, 3].astype(np.float64),
+                                ref["ray_geom"][:, 3].astype(np.float64))
     out = {"n_dev": len(kd), "n_ref": len(kr), "matched_exact": len(md), "matched_merged": len(md2)}
     out["geom_exact"] = True
     if md2:
@@ -161,7 +172,12 @@ def compare_rays(dev: Dict[str, np.ndarray], ref: Dict[str, np.ndarray], nphot_m
             continue
         r = _rel(dev["ray_nphot"][ids_d], ref["ray_nphot"][ids_r], floor)
         out[f"nphot{lab}_maxrel"] = float(r.max())
-        out[f"nphot{lab}_bad"] = int((r.max(axis=1) > tol).sum())
+        bad = np.nonzero(r.max(axis=1) > tol)[0]
+        out[f"nphot{lab}_bad"] = int(len(bad))
+        # the first few offenders: key, photon sums and radii on both sides
+        out[f"nphot{lab}_worst"] = [
+            (kd2[ids_d[j]], float(dev["ray_nphot"][ids_d[j]].sum()), float(ref["ray_nphot"][ids_r[j]].sum()),
+             float(dev["ray_geom"][ids_d[j], 3]), float(ref["ray_geom"][ids_r[j], 3])) for j in bad[:3]]
     ma, mb = np.array(md + md2, int), np.array(mr + mr2, int)
     if len(ma):
         hd, hr = dev["ray_geom"][ma, 0:3], ref["ray_geom"][mb, 0:3]

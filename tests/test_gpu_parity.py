@@ -83,6 +83,22 @@ def test_t16_parity(precision, mode):
             assert st["crossings"] == int(ref[s]["scalars"][10])
 
 
+def test_t16_core_outputs():
+    """Core outputs, mixed precision: the last ray pass keeps only the bin-weighted photo-heating
+    sums, so the temperature path differs from the diag run; per-bin rates are refused."""
+    spec, seed = T16
+    ref = oracle_run(spec, seed)
+    states, stats, _ = run_device(spec, seed, "mixed", "graph", diag=False)
+    check(states, ref, False)
+    ctx = rt.RTContext([W.make_inputs(spec)], [seed], outputs="core", ray_capacity=1 << 20)
+    ctx.setup()
+    ctx.step()
+    with pytest.raises(rt.FrtError, match="status 5"):
+        ctx.get_field(0, "GAMMA_H1_NU")
+    assert ctx.get_field(0, "NGAM_NU").shape[-1] == 5
+    ctx.close()
+
+
 @pytest.mark.parametrize("case", ["T16M", "T16N"])
 @pytest.mark.parametrize("precision", ["strict", "mixed"])
 def test_merge_parity(case, precision):
