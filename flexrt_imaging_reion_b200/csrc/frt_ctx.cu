@@ -957,3 +957,101 @@ frt_status frt_last_timing(frt_ctx* ctx, float* step_ms, float* cell_kernel_ms) 
 
 }  // extern "C"
 
+// ---- field read-back without device allocation ---------------------------------------------
+// frt_get_field gathers a lit-cell field (Gamma, photon counts) through a temporary device
+// buffer of one box's size, taken with cudaMalloc and released with cudaFree. Some callers must
+// not allocate there: an output hook that runs between steps while the ray pool was sized to
+// fill the GPU (the allocation fails exactly when the run is largest), and drivers that keep
+// the dark-cell stream running across the read (cudaFree waits for the whole device). The entry
+// point below gathers into a fixed scratch array in the module's global memory instead and hands
+// out at most FRT_NOALLOC_MAX_CELLS cells per call; a caller reads a larger box in windows.
+#include <mutex>
+
+namespace {
+
+constexpr long long kNoAllocMaxCells = FRT_NOALLOC_MAX_CELLS;
+// The scratch array: 4 MiB of static device memory, one per device the module is loaded on.
+// The gather writes every element it later copies out, so nothing in it has to start at zero.
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocMaxCells];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+float* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Address of the scratch array on `device`, looked up once per device with that device current.
+cudaError_t noalloc_scratch(int device, float** out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (device < 0 || device >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+  if (!g_noalloc_ptr[device]) {
+    int prev = -1;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) return e;
+    if (prev != device && (e = cudaSetDevice(device)) != cudaSuccess) return e;
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (prev != device) {
+      const cudaError_t e2 = cudaSetDevice(prev);
+      if (e == cudaSuccess) e = e2;
+    }
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[device] = static_cast<float*>(p);
+  }
+  *out = g_noalloc_ptr[device];
+  return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+frt_status frt_get_sparse_field_noalloc(frt_ctx* ctx, int box, frt_field f, int bin, long long first_cell,
+                                        long long count, float* host) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  Dev& d = ctx->d;
+  const BoxP& B = ctx->hbox[box];
+  const int F = d.F;
+  int which = -1;
+  switch (f) {
+    case FRT_F_GAMMA_H1_TOT: which = 0; break;
+    case FRT_F_GAMMA_HE1_TOT: which = 1; break;
+    case FRT_F_GAMMA_H1_NU: which = 2 + bin; break;
+    case FRT_F_GAMMA_HE1_NU: which = 2 + F + bin; break;
+    case FRT_F_NGAM_NU: which = 2 + 2 * F + bin; break;
+    default:
+      ctx->err = "frt_get_sparse_field_noalloc: not a lit-cell field (GAMMA_*_TOT, GAMMA_*_NU, NGAM_NU)";
+      return FRT_ERR_INVALID;
+  }
+  const bool per_bin = (f == FRT_F_GAMMA_H1_NU || f == FRT_F_GAMMA_HE1_NU || f == FRT_F_NGAM_NU);
+  if (per_bin && (bin < 0 || bin >= F)) {
+    ctx->err = "frt_get_sparse_field_noalloc: bin out of range";
+    return FRT_ERR_INVALID;
+  }
+  if ((f == FRT_F_GAMMA_H1_NU || f == FRT_F_GAMMA_HE1_NU) && !d.per_bin) {
+    ctx->err = "per-bin rates are kept only with diag outputs or strict precision";
+    return FRT_ERR_STATE;
+  }
+  if (count < 0 || first_cell < 0 || first_cell > B.ncell || count > B.ncell - first_cell) {
+    ctx->err = "frt_get_sparse_field_noalloc: cell window outside the box";
+    return FRT_ERR_INVALID;
+  }
+  if (count > kNoAllocMaxCells) {
+    ctx->err = "frt_get_sparse_field_noalloc: count " + std::to_string(count) +
+               " exceeds FRT_NOALLOC_MAX_CELLS (" + std::to_string(kNoAllocMaxCells) +
+               "); read the box in windows";
+    return FRT_ERR_INVALID;
+  }
+  if (count == 0) return FRT_OK;
+  if (!host) return FRT_ERR_INVALID;
+  float* scratch = nullptr;
+  CK(noalloc_scratch(ctx->cfg.device, &scratch));
+  CK(cudaStreamSynchronize(ctx->s_main));
+  CK(cudaStreamSynchronize(ctx->s_dark));
+  launch_gather_sparse(d, B.cell0 + first_cell, count, which, scratch, ctx->s_main);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, scratch, sizeof(float) * (size_t)count, cudaMemcpyDeviceToHost, ctx->s_main));
+  CK(cudaStreamSynchronize(ctx->s_main));
+  return FRT_OK;
+}
+
+}  // extern "C"

@@ -192,6 +192,21 @@ frt_status frt_box_scalars(frt_ctx* ctx, int box, double* out8);
  * and the time of its dominant cell kernel. */
 frt_status frt_last_timing(frt_ctx* ctx, float* step_ms, float* cell_kernel_ms);
 
+/* ---- field read-back without device allocation ---------------------------------------------
+ * No counterpart in the reference (its fields live in host arrays). Gathers cells
+ * [first_cell, first_cell + count) of one lit-cell field -- GAMMA_H1_TOT, GAMMA_HE1_TOT, or bin
+ * `bin` of GAMMA_H1_NU, GAMMA_HE1_NU, NGAM_NU -- into `host`, the same values frt_get_field
+ * returns, without allocating device memory: the gather goes through a fixed 4 MiB scratch array
+ * in the library's static device memory, so count is limited to FRT_NOALLOC_MAX_CELLS (larger
+ * requests return FRT_ERR_INVALID; read a box in windows). The first call on a device looks up
+ * the scratch address (cudaGetSymbolAddress, with the context's device made current); make that
+ * first call before any stream capture. The scratch array is shared by every context on the
+ * device: calls that overlap in time (two host threads, two contexts) race on it and must be
+ * serialised by the caller. Blocks until the values are in `host`. */
+#define FRT_NOALLOC_MAX_CELLS (1 << 20)
+frt_status frt_get_sparse_field_noalloc(frt_ctx* ctx, int box, frt_field f, int bin, long long first_cell,
+                                        long long count, float* host);
+
 #ifdef __cplusplus
 }
 #endif
