@@ -40,6 +40,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 DARK_BYTES_PER_CELL = 82  # 10 float fields + treion_flag + lit_flag read, 10 float fields written
+# DRAM bytes per dark cell of one k_dark launch, from ncu (dram__bytes_read.sum + write.sum) at
+# step 24 of the L workload: 1342.3 MB for 13 264 000 dark cells (profiles/k_dark_L.md). The
+# bench scales it by the dark cells of its own steps (traffic grows with the cells processed).
+DARK_TRAFFIC_BYTES_PER_CELL = 1342312448 / 13264000
 
 
 def _peaks():
@@ -93,6 +97,14 @@ class ClockSampler:
 def _spec(name):
     from flexrt_imaging_reion_b200 import workloads as W
     return {"L": W.config_L, "M": W.config_M, "S": W.config_S}[name]()
+
+
+def _describe_ensemble(specs):
+    sizes = sorted({s.n for s in specs})
+    return (f"E: {len(specs)} independent boxes, N in {sizes} (same comoving cell), z={specs[0].z:g}, "
+            f"sigma_ln U[0.3,0.9], {sum(s.n_src for s in specs)} sources (log-uniform 8..4096 per box, "
+            f"L^-2 [1e50,1e54] ph/s), 5 bins, dt={specs[0].dt_myr} Myr, "
+            f"{sum(s.n ** 3 for s in specs) / 1e6:.1f} M cells")
 
 
 def _describe(spec):
@@ -160,12 +172,101 @@ def run_reference(spec, name: str, steps: int, threads: int, time_cap_s: float, 
     return rows, setup
 
 
+# ---- uneven ensemble (E) --------------------------------------------------------------------
+def run_reference_ensemble(steps: int, threads: int, time_cap_s: float, seed: int):
+    """The compiled reference over the ensemble's boxes in order (one build per grid size), each
+    box for `steps` steps, until the summed step time passes time_cap_s. Returns (crossings,
+    step seconds, boxes run)."""
+    from flexrt_imaging_reion_b200 import workloads as W
+    specs = W.config_E()
+    cross, wall, nb = 0, 0.0, 0
+    for b, spec in enumerate(specs):
+        rows, _ = run_reference(spec, f"E{spec.n}", steps, threads, max(1.0, time_cap_s - wall), seed + b)
+        cross += sum(c for c, _ in rows)
+        wall += sum(w for _, w in rows)
+        nb += 1
+        if wall > time_cap_s:
+            break
+    return cross, wall, nb
+
+
+def run_ensemble(args, rank: int, world: int, local_rank: int):
+    """Batched + graph form of the ensemble (every box of this rank in one context), and on one GPU
+    also the per-box launch loop over the same boxes and seeds for the comparison. Across ranks the
+    boxes are sharded by the longest-processing-time plan (no exchange inside the step)."""
+    from flexrt_imaging_reion_b200 import ensemble as EN, workloads as W
+    specs = W.config_E()
+    plan = EN.lpt_shards([EN.box_cost(s) for s in specs], world)
+    mine = plan[rank]
+    inputs = [W.make_inputs(specs[b]) for b in mine]
+    seeds = [args.seed + b for b in mine]
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+        tdist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    bat = EN.run_batched(inputs, seeds, args.warmup, args.steps, device=local_rank, box_ids=mine)
+    clk = clocks.stop()
+    per_box = EN.gather_box_results(bat["per_box"], world)
+    ncell = sum(s.n ** 3 for s in (specs[b] for b in mine))
+    if dist:
+        import torch
+        import torch.distributed as tdist
+        t = torch.tensor([bat["device_ms"], bat["wall_s"], float(bat["crossings"])], dtype=torch.float64,
+                         device=f"cuda:{local_rank}")
+        mx, sm = t.clone(), t.clone()
+        tdist.all_reduce(mx, op=tdist.ReduceOp.MAX)
+        tdist.all_reduce(sm, op=tdist.ReduceOp.SUM)
+        dev_ms, wall, cross = float(mx[0]), float(mx[1]), float(sm[2])
+    else:
+        dev_ms, wall, cross = bat["device_ms"], bat["wall_s"], float(bat["crossings"])
+    cap = EN.ray_capacity([specs[b] for b in mine])
+    per_step = max(launches_per_step(specs[b], cap) for b in mine) if mine else 0
+    dark_bytes = DARK_BYTES_PER_CELL * (ncell * args.steps - bat["lit_cells"])
+    dark_gbs = dark_bytes / (bat["dark_ms"] * 1e-3) / 1e9 if bat["dark_ms"] > 0 else None
+    peak, peak_kind = _peaks()
+    res = {
+        "metric": "ray-cell crossings/s", "value": cross / (dev_ms * 1e-3), "unit": "crossings/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded lognormal gas + L^-2 sources per box)",
+        "config": {"workload": _describe_ensemble(specs), "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps}",
+                   "graph": True, "l2": "state larger than L2, no flush",
+                   "parallelism": f"boxes sharded over {world} ranks (LPT)" if dist else "single"},
+        "e2e": {"value": cross / wall, "unit": "crossings/s", "h2d_bytes_per_step": 2 * len(mine) + 2 * sum(
+            len(W.grid_sources(i)[1]) for i in inputs), "d2h_bytes_per_step": 144},
+        "roofline": {"bound": "hbm", "kernel": "k_dark (cells no ray touched: whole step in one pass)",
+                     "achieved": dark_gbs, "peak": peak, "unit": "GB/s",
+                     "frac": (dark_gbs / peak) if dark_gbs else None,
+                     "traffic": DARK_TRAFFIC_BYTES_PER_CELL * (ncell - bat["lit_cells"] / args.steps),
+                     "traffic_note": "bytes per launch: ncu DRAM bytes per dark cell (L) x dark cells per step",
+                     "peak_kind": peak_kind,
+                     "bytes_per_cell": DARK_BYTES_PER_CELL},
+        "gpu_launches": per_step * args.steps,
+        "clocks": clk,
+        "crossings_per_step": cross / args.steps,
+        "rays_end": sum(v[2] for v in per_box.values()),
+    }
+    if not dist and not args.no_loop:
+        loop = EN.run_per_box_loop(inputs, seeds, args.warmup, args.steps, device=local_rank)
+        res["per_box_plain_loop"] = {
+            "value": loop["crossings"] / loop["wall_s"], "unit": "crossings/s", "ms_per_step": 1e3 * loop["wall_s"] / args.steps,
+            "crossings": loop["crossings"],
+            "gpu_launches": args.steps * sum(launches_per_step(specs[b], EN.ray_capacity([specs[b]])) for b in mine),
+            "what": "one context per box, every kernel launched directly (no graph), boxes one after another; "
+                    "host wall clock"}
+        res["batched_vs_loop_wall"] = (cross / wall) / (loop["crossings"] / loop["wall_s"])
+        res["same_crossings"] = int(loop["crossings"]) == int(bat["crossings"])
+    return res
+
+
 # ---- our arm ---------------------------------------------------------------------------------
 def launches_per_step(spec, ray_capacity, itercount=5, hpx_lvl=0):
-    """Kernels one fused step launches: clear_lit, step_begin, advance, dark, lit_init,
+    """Kernels one fused step launches: clear_lit, step_begin, advance, lit_compact, dark, lit_init,
     itercount x (ray pass + lit pass), count, 3 merge set-up kernels (+4 binning kernels when the
     pool can reach the merge threshold), compact, split, swap, cast."""
-    n = 1 + 1 + 1 + 1 + 1 + 2 * itercount + 1 + 3 + 3 + 1
+    n = 1 + 1 + 1 + 1 + 1 + 1 + 2 * itercount + 1 + 3 + 3 + 1
     num_thresh = (spec.ray_per_cell_max - 12 * 4 ** hpx_lvl) * spec.n ** 3
     if num_thresh < ray_capacity:
         n += 4
@@ -237,7 +338,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "kernel": "k_dark (cells no ray touched: whole step in one pass)",
                      "achieved": dark_gbs, "peak": peak, "unit": "GB/s",
-                     "frac": (dark_gbs / peak) if dark_gbs else None, "traffic": None,
+                     "frac": (dark_gbs / peak) if dark_gbs else None,
+                     "traffic": DARK_TRAFFIC_BYTES_PER_CELL * (ncell - lit / args.steps),
+                     "traffic_note": "bytes per launch: ncu DRAM bytes per dark cell x dark cells per step",
+                     "algorithmic_bytes_per_launch": DARK_BYTES_PER_CELL * (ncell - lit / args.steps),
                      "peak_kind": peak_kind, "bytes_per_cell": DARK_BYTES_PER_CELL,
                      "kernel_ms_per_step": dark_ms / args.steps},
         "gpu_launches": launches,
@@ -255,7 +359,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["L", "M", "S"], default="L")
+    ap.add_argument("--workload", choices=["L", "M", "S", "E"], default="L")
+    ap.add_argument("--no-loop", action="store_true", help="E: skip the per-box launch-loop comparison")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--ray-capacity", type=int, default=16 << 20)
     ap.add_argument("--lit-capacity", type=int, default=0, help="0 = all cells")
@@ -271,6 +376,26 @@ def main():
 
     if args.impl == "reference":
         if rank != 0:
+            return
+        if args.workload == "E":
+            try:
+                cr, wt, nb = run_reference_ensemble(args.warmup + args.steps, threads, args.ref_time_cap, args.seed)
+            except Exception as e:
+                print(json.dumps({"impl": "reference", "unavailable": f"compiled reference failed: {e}"}))
+                return
+            v = cr / wt if wt > 0 else None
+            from flexrt_imaging_reion_b200 import workloads as W
+            print(json.dumps({
+                "impl": "reference", "metric": "ray-cell crossings/s", "value": v, "unit": "crossings/s",
+                "n_gpus": world, "steps": args.warmup + args.steps, "warmup": 0,
+                "ms_per_step": None, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "f32+f64 (reference float storage, double locals)", "data": "synthetic",
+                "config": {"workload": _describe_ensemble(W.config_E())},
+                "cpu_baseline": {"value": v, "unit": "crossings/s", "cores": threads, "kind": "reference",
+                                 "sample": f"first {nb} boxes of the ensemble, {args.warmup + args.steps} steps each, "
+                                           f"OpenMP {threads} threads (time cap {args.ref_time_cap:.0f} s)"},
+                "e2e": {"value": v, "unit": "crossings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            }))
             return
         spec = _spec(args.workload)
         try:
@@ -303,8 +428,21 @@ def main():
         from datetime import timedelta
         torch.cuda.set_device(local_rank)
         tdist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    res = run_ours(args, rank, world, local_rank)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if args.workload == "E":
+        res = run_ensemble(args, rank, world, local_rank)
+    else:
+        res = run_ours(args, rank, world, local_rank)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "E":
+        try:
+            cr, wt, nb = run_reference_ensemble(args.cpu_baseline_steps, threads, 30.0, args.seed)
+            res["cpu_baseline"] = {"value": cr / wt if wt else None, "unit": "crossings/s", "cores": threads,
+                                   "kind": "reference",
+                                   "sample": f"steps 1..{args.cpu_baseline_steps} of the first {nb} boxes, reference "
+                                             f"OpenMP code compiled from its sources (one build per grid size)"}
+        except Exception as e:
+            res["cpu_baseline"] = {"value": None, "unit": "crossings/s", "cores": threads, "kind": "reference",
+                                   "sample": f"unavailable: {e}"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != "E":
         spec = _spec(args.workload)
         try:
             rows, setup = run_reference(spec, args.workload, args.cpu_baseline_steps, threads, 60.0, args.seed)

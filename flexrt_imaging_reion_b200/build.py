@@ -1,7 +1,8 @@
 """Build libflexrt_b200.so in-tree (sm_100a).
 
 nvcc compiles the CUDA sources for compute_100a / sm_100a; the geometry translation unit uses
--fmad=false (its float arithmetic must round exactly like the reference's g++ build), the host
+-fmad=false (its float arithmetic must round exactly like the reference's g++ build; the adjoint
+recomputes the same ray walk and is compiled the same way), the host
 set-up arithmetic is compiled by g++ with -ffp-contract=off for the same reason.
 """
 from __future__ import annotations
@@ -24,9 +25,10 @@ SOURCES = [
     # (file, extra flags)
     ("frt_geom.cu", ["-fmad=false"]),
     ("frt_phys.cu", []),
+    ("frt_adjoint.cu", ["-fmad=false"]),
     ("frt_ctx.cu", []),
 ]
-HEADERS = ["frt_internal.cuh", "frt_physics.cuh", "frt_params.h", "hp_nest.h", "frt_hostmath.h",
+HEADERS = ["frt_internal.cuh", "frt_physics.cuh", "frt_params.h", "hp_nest.h", "frt_hostmath.h", "frt_dda.cuh",
            os.path.join("..", "..", "include", "flexrt.h")]
 
 

@@ -37,6 +37,10 @@ struct frt_ctx {
   bool strict = false;
   int grid_rays = 0, grid_cells = 0, grid_lit = 0;
   float last_step_ms = 0.f, last_dark_ms = 0.f;
+  bool rays_moved = false;   // an advance, merge or split ran (rays no longer one source's cast)
+  AdjDev adj{};
+  bool adj_ready = false;
+  float* adj_out = nullptr;   // gather buffer of the adjoint's per-cell output (largest box)
   frt_step_stats last{};
   std::string err;
   // glibc rand() streams, one per box (srand(seed) semantics via initstate_r / random_r)
@@ -136,6 +140,7 @@ frt_status upload_sources(frt_ctx* ctx) {
 
 // ---- step sequences ---------------------------------------------------------------------------
 void enqueue_begin_advance(frt_ctx* ctx) {
+  ctx->rays_moved = true;
   const Dev& d = ctx->d;
   launch_clear_lit(d, ctx->grid_lit, ctx->s_main);
   launch_step_begin(d, ctx->s_main);
@@ -375,8 +380,9 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
   AL(d.l_crec_he, L); AL(d.l_rec_h2, L); AL(d.l_rec_he2, L); AL(d.l_avg_h, L); AL(d.l_avg_he, L);
   AL(d.l_nh1_old, L); AL(d.l_acc_g, L); AL(d.l_acc_ghe, L);
   d.per_bin = (ctx->strict || cfg->outputs == FRT_OUT_DIAG) ? 1 : 0;
-  AL(d.l_ngam, L * d.F); AL(d.l_heat_h, L); AL(d.l_heat_he, L);
+  AL(d.l_heat_h, L); AL(d.l_heat_he, L);
   if (d.per_bin) {
+    AL(d.l_ngam, L * d.F);
     AL(d.l_acc_nu_h, L * d.F);
     AL(d.l_acc_nu_he, L * d.F);
   }
@@ -635,8 +641,8 @@ frt_status frt_get_field(frt_ctx* ctx, int box, frt_field f, float* host) {
     case FRT_F_GAMMA_HE1_NU:
     case FRT_F_NGAM_NU: {
       const int base = (f == FRT_F_GAMMA_H1_NU) ? 2 : (f == FRT_F_GAMMA_HE1_NU ? 2 + F : 2 + 2 * F);
-      if (f != FRT_F_NGAM_NU && !d.per_bin) {
-        ctx->err = "per-bin rates are kept only with diag outputs or strict precision";
+      if (!d.per_bin) {
+        ctx->err = "per-bin rates and photon counts are kept only with diag outputs or strict precision";
         return FRT_ERR_STATE;
       }
       std::vector<float> tmp(n);
@@ -754,6 +760,7 @@ frt_status frt_count_rays(frt_ctx* ctx, long long* count_per_box) {
 
 frt_status frt_merge(frt_ctx* ctx, const uint16_t* itheta_per_box) {
   if (!ctx) return FRT_ERR_INVALID;
+  ctx->rays_moved = true;
   frt_status st = stage_itheta(ctx, itheta_per_box, nullptr);
   if (st) return st;
   CK(cudaMemcpyAsync(ctx->d.itheta_merge, ctx->h_ith_box, sizeof(uint16_t) * ctx->d.nbox, cudaMemcpyHostToDevice,
@@ -765,6 +772,7 @@ frt_status frt_merge(frt_ctx* ctx, const uint16_t* itheta_per_box) {
 
 frt_status frt_split_rays(frt_ctx* ctx) {
   if (!ctx) return FRT_ERR_INVALID;
+  ctx->rays_moved = true;
   launch_split_compact(ctx->d, ctx->grid_rays, ctx->s_main);
   return sync_and_check(ctx);
 }
@@ -957,6 +965,102 @@ frt_status frt_last_timing(frt_ctx* ctx, float* step_ms, float* cell_kernel_ms) 
 
 }  // extern "C"
 
+// ---- adjoint of the next step's Gamma field ----------------------------------------------------
+namespace {
+
+frt_status adj_alloc(frt_ctx* ctx) {
+  if (ctx->adj_ready) return FRT_OK;
+  Dev& d = ctx->d;
+  AdjDev& a = ctx->adj;
+  a.cap = d.lit_cap;
+  a.I = d.itercount;
+  const size_t NC = (size_t)d.ncell_total, L = (size_t)a.cap, LI = L * (size_t)a.I;
+  AL(a.flag, NC); AL(a.slot, NC); AL(a.src_of_cell, NC); AL(a.cell, L); AL(a.in_obj, L);
+  AL(a.nH, L); AL(a.nHe, L); AL(a.y0h, L); AL(a.y0he, L); AL(a.crh, L); AL(a.crhe, L);
+  AL(a.a, LI); AL(a.b, LI); AL(a.gh, LI); AL(a.ghe, LI);
+  AL(a.abar, L); AL(a.bbar, L); AL(a.gbh, L); AL(a.gbhe, L); AL(a.nhbar, L);
+  AL(a.dlbar, std::max<size_t>(1, (size_t)d.src_cap)); AL(a.count, 1); AL(a.err, 1); AL(a.J, 1);
+  long long maxcell = 1;
+  for (const BoxP& B : ctx->hbox) maxcell = std::max(maxcell, B.ncell);
+  AL(ctx->adj_out, (size_t)maxcell);
+  // source cell -> context-wide source index
+  std::vector<int> soc(NC, -1);
+  int s = 0;
+  for (size_t b = 0; b < ctx->src_cell.size(); b++)
+    for (size_t q = 0; q < ctx->src_cell[b].size(); q++, s++) soc[(size_t)ctx->hbox[b].cell0 + ctx->src_cell[b][q]] = s;
+  CK(cudaMemcpy(a.src_of_cell, soc.data(), sizeof(int) * NC, cudaMemcpyHostToDevice));
+  ctx->adj_ready = true;
+  return FRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+frt_status frt_adjoint(frt_ctx* ctx, const frt_adj_objective* obj, double* J, double* dL, float* dnH) {
+  if (!ctx || !obj) return FRT_ERR_INVALID;
+  frt_status st = check_box(ctx, obj->box);
+  if (st) return st;
+  const BoxP& B = ctx->hbox[obj->box];
+  for (int k = 0; k < 3; k++)
+    if (obj->lo[k] < 0 || obj->hi[k] > B.n || obj->lo[k] > obj->hi[k]) {
+      ctx->err = "frt_adjoint: objective sub-box outside the box";
+      return FRT_ERR_INVALID;
+    }
+  if (ctx->rays_moved) {
+    ctx->err = "frt_adjoint needs the state right after set-up (no advance, merge or split yet)";
+    return FRT_ERR_STATE;
+  }
+  st = adj_alloc(ctx);
+  if (st) return st;
+  Dev& d = ctx->d;
+  AdjDev& a = ctx->adj;
+  a.box = obj->box;
+  for (int k = 0; k < 3; k++) {
+    a.lo[k] = obj->lo[k];
+    a.hi[k] = obj->hi[k];
+  }
+  cudaStream_t s = ctx->s_main;
+  CK(cudaStreamSynchronize(ctx->s_dark));
+  CK(cudaMemsetAsync(a.flag, 0, (size_t)d.ncell_total, s));
+  launch_fill_i32(a.slot, -1, d.ncell_total, s);
+  CK(cudaMemsetAsync(a.count, 0, sizeof(int), s));
+  CK(cudaMemsetAsync(a.err, 0, sizeof(unsigned), s));
+  CK(cudaMemsetAsync(a.J, 0, sizeof(double), s));
+  CK(cudaMemsetAsync(a.dlbar, 0, sizeof(double) * std::max(1, d.src_cap), s));
+  launch_adjoint(d, a, ctx->grid_rays, s);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));
+  unsigned err = 0;
+  double Jv = 0.0;
+  CK(cudaMemcpy(&err, a.err, sizeof err, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&Jv, a.J, sizeof Jv, cudaMemcpyDeviceToHost));
+  if (err) {
+    ctx->err = "frt_adjoint: " + std::string((err & 1u) ? "path_length exceeded " : "") +
+               std::string((err & 2u) ? "path cells above the lit-cell capacity" : "");
+    return FRT_ERR_CAPACITY;
+  }
+  if (J) *J = Jv;
+  if (dL) {
+    int s0 = 0;
+    for (int b = 0; b < obj->box; b++) s0 += (int)ctx->src_cell[b].size();
+    const size_t ns = ctx->src_cell[obj->box].size();
+    std::vector<double> v(ns);
+    if (ns) CK(cudaMemcpy(v.data(), a.dlbar + s0, sizeof(double) * ns, cudaMemcpyDeviceToHost));
+    for (size_t q = 0; q < ns; q++) {
+      const double lum = ctx->src_lum[obj->box][q];
+      dL[q] = lum != 0.0 ? v[q] / lum : 0.0;
+    }
+  }
+  if (dnH) {
+    launch_adjoint_gather(d, a, B.cell0, B.ncell, ctx->adj_out, s);
+    CK(cudaMemcpy(dnH, ctx->adj_out, sizeof(float) * (size_t)B.ncell, cudaMemcpyDeviceToHost));
+  }
+  return FRT_OK;
+}
+
+}  // extern "C"
+
 // ---- field read-back without device allocation ---------------------------------------------
 // frt_get_field gathers a lit-cell field (Gamma, photon counts) through a temporary device
 // buffer of one box's size, taken with cudaMalloc and released with cudaFree. Some callers must
@@ -1027,8 +1131,8 @@ frt_status frt_get_sparse_field_noalloc(frt_ctx* ctx, int box, frt_field f, int 
     ctx->err = "frt_get_sparse_field_noalloc: bin out of range";
     return FRT_ERR_INVALID;
   }
-  if ((f == FRT_F_GAMMA_H1_NU || f == FRT_F_GAMMA_HE1_NU) && !d.per_bin) {
-    ctx->err = "per-bin rates are kept only with diag outputs or strict precision";
+  if (per_bin && !d.per_bin) {
+    ctx->err = "per-bin rates and photon counts are kept only with diag outputs or strict precision";
     return FRT_ERR_STATE;
   }
   if (count < 0 || first_cell < 0 || first_cell > B.ncell || count > B.ncell - first_cell) {

@@ -8,6 +8,7 @@
 #include <math.h>
 
 #include "frt_internal.cuh"
+#include "frt_dda.cuh"
 #include "hp_nest.h"
 
 namespace frt {
@@ -108,23 +109,20 @@ __global__ void k_step_begin(Dev d) {
     d.src_ray_dt[s] += d.box[d.src_box[s]].dt;
 }
 
-// Claim a lit slot for a cell touched by a segment (first toucher wins).
-__device__ __forceinline__ void claim_lit(const Dev& d, long long gc) {
-  if (d.lit_slot[gc] != -1) return;
-  if (atomicCAS(&d.lit_slot[gc], -1, -2) != -1) return;
-  const int s = atomicAdd(&d.ctl->n_lit, 1);
-  if (s < d.lit_cap) {
-    d.l_cell[s] = (int)gc;
-    d.lit_flag[gc] = 1;
-    d.lit_slot[gc] = s;
-  } else {
-    atomicOr(&d.ctl->err, ERR_LIT_CAP);
-  }
+// Mark a cell touched by a segment. The lit list is numbered afterwards in cell order
+// (k_lit_compact), so that the lit-cell kernels read the dense fields in address order.
+__device__ __forceinline__ void mark_lit(const Dev& d, long long gc) {
+  if (!d.lit_flag[gc]) d.lit_flag[gc] = 1;
+}
+
+// Number the marked cells in cell order (compact_marked, frt_dda.cuh).
+__global__ void __launch_bounds__(256) k_lit_compact(Dev d) {
+  compact_marked(d.lit_flag, d.ncell_total, d.lit_slot, d.l_cell, &d.ctl->n_lit, d.lit_cap, &d.ctl->err, ERR_LIT_CAP);
 }
 
 // advance_ray (ray_tracing.cc:1222-1512) with c2ray_iter = TRUE and fion = 1 (plain mode):
 // cell-boundary walk over c_sim * time, path segments {cell, dist}, periodic wrap, corner nudge.
-__global__ void __launch_bounds__(256) k_advance(Dev d) {
+__global__ void __launch_bounds__(256, 4) k_advance(Dev d) {
   const int cur = d.ctl->cur;
   const int n = d.ctl->nray[cur];
   const RayPool A = d.pool[cur];
@@ -142,11 +140,8 @@ __global__ void __launch_bounds__(256) k_advance(Dev d) {
     const float xhat = A.xh[i], yhat = A.yh[i], zhat = A.zh[i];
     float x0 = A.x[i], y0 = A.y[i], z0 = A.z[i];
     const float deltat = A.time[i] + B.dt;
-    float dist = B.clight * deltat;
-    const float px = x0 + dist * xhat, py = y0 + dist * yhat, pz = z0 + dist * zhat;
-    const bool mv = (px > B.mv_hi) || (py > B.mv_hi) || (pz > B.mv_hi) || ((double)px < B.mv_lo) ||
-                    ((double)py < B.mv_lo) || ((double)pz < B.mv_lo);
-    if (!mv) {
+    const float dist = B.clight * deltat;
+    if (!ray_moves(B, x0, y0, z0, xhat, yhat, zhat, dist)) {
       A.time[i] = deltat;
       d.nseg[i] = 0;
       continue;
@@ -154,78 +149,20 @@ __global__ void __launch_bounds__(256) k_advance(Dev d) {
     float r0 = A.r[i], dr = A.dr[i];
     r0 += dist / B.scale;
     dr -= dist / B.scale;
-    int in = ii, jn = jj, kn = kk, p = 0;
-    float tlast = 0.f, tmin = 0.f;
-    const float clgt = B.clight;
-    const float dxc = B.dx;
-    bool overflow = false;
-    while (tlast < deltat) {
-      float tx, ty, tz;
-      if (xhat > 0.f) tx = (dxc - x0) / xhat / clgt;
-      else if (xhat < 0.f) tx = (float)(-1. * (double)x0 / (double)xhat / (double)clgt);
-      else tx = INFINITY;
-      if (yhat > 0.f) ty = (dxc - y0) / yhat / clgt;
-      else if (yhat < 0.f) ty = (float)(-1. * (double)y0 / (double)yhat / (double)clgt);
-      else ty = INFINITY;
-      if (zhat > 0.f) tz = (dxc - z0) / zhat / clgt;
-      else if (zhat < 0.f) tz = (float)(-1. * (double)z0 / (double)zhat / (double)clgt);
-      else tz = INFINITY;
-      int tag;
-      if ((tx <= ty) && (tx <= tz)) { tmin = tx; tag = 0; }
-      else if ((ty <= tx) && (ty <= tz)) { tmin = ty; tag = 1; }
-      else { tmin = tz; tag = 2; }
-      if ((tlast + tmin) < deltat) {
-        dist = tmin * clgt;
-        if (p >= PL - 1) { overflow = true; break; }
-        const long long gc = B.cell0 + (long long)in * B.nn + jn * N + kn;
-        d.seg[(size_t)p * cap + i] = (int)gc;
-        d.seg_dist[(size_t)p * cap + i] = dist;
-        claim_lit(d, gc);
-        p += 1;
-        x0 += dist * xhat;
-        y0 += dist * yhat;
-        z0 += dist * zhat;
-        if (tag == 0) {
-          if (xhat > 0.f) { in = imod(in + 1, N); x0 = B.lo_edge; }
-          else { in = imod(in - 1, N); x0 = B.hi_edge; }
-        } else if (tag == 1) {
-          if (yhat > 0.f) { jn = imod(jn + 1, N); y0 = B.lo_edge; }
-          else { jn = imod(jn - 1, N); y0 = B.hi_edge; }
-        } else {
-          if (zhat > 0.f) { kn = imod(kn + 1, N); z0 = B.lo_edge; }
-          else { kn = imod(kn - 1, N); z0 = B.hi_edge; }
-        }
-        if (x0 <= 0.f) x0 = B.lo_edge;
-        if ((double)x0 >= B.hi_thr) x0 = B.hi_edge;
-        if (y0 <= 0.f) y0 = B.lo_edge;
-        if ((double)y0 >= B.hi_thr) y0 = B.hi_edge;
-        if (z0 <= 0.f) z0 = B.lo_edge;
-        if ((double)z0 >= B.hi_thr) z0 = B.hi_edge;
-      }
-      tlast += tmin;
-    }
-    if (overflow) {
+    int in = ii, jn = jj, kn = kk;
+    const int ns = dda_walk(B, PL, xhat, yhat, zhat, deltat, x0, y0, z0, in, jn, kn,
+                            [&](int p, long long gc, float ds) {
+                              d.seg[(size_t)p * cap + i] = (int)gc;
+                              d.seg_dist[(size_t)p * cap + i] = ds;
+                              mark_lit(d, gc);
+                            });
+    if (ns < 0) {
       atomicOr(&d.ctl->err, ERR_PATH);
       d.nseg[i] = 0;
       d.dead[i] = 1;
       continue;
     }
-    dist = (deltat - tlast + tmin) * clgt;
-    dist = (B.lo_edge >= dist) ? B.lo_edge : dist;   // maxd(dist, min_dist*dx)
-    const long long gc = B.cell0 + (long long)in * B.nn + jn * N + kn;
-    d.seg[(size_t)p * cap + i] = (int)gc;
-    d.seg_dist[(size_t)p * cap + i] = dist;
-    claim_lit(d, gc);
-    d.nseg[i] = (uint8_t)(p + 1);
-    x0 += dist * xhat;
-    y0 += dist * yhat;
-    z0 += dist * zhat;
-    if (x0 <= 0.f) x0 = B.lo_edge;
-    if ((double)x0 >= B.hi_thr) x0 = B.hi_edge;
-    if (y0 <= 0.f) y0 = B.lo_edge;
-    if ((double)y0 >= B.hi_thr) y0 = B.hi_edge;
-    if (z0 <= 0.f) z0 = B.lo_edge;
-    if ((double)z0 >= B.hi_thr) z0 = B.hi_edge;
+    d.nseg[i] = (uint8_t)ns;
     A.time[i] = 0.f;
     A.r[i] = r0;
     A.dr[i] = dr;
@@ -233,7 +170,7 @@ __global__ void __launch_bounds__(256) k_advance(Dev d) {
     A.y[i] = y0;
     A.z[i] = z0;
     A.cell[i] = in * B.nn + jn * N + kn;
-    cross += p + 1;
+    cross += ns;
     moved += 1;
     // optional removal beyond rkill (comoving), applied after update_rays
     if (B.rkill > 0.0 && (double)r0 > B.rkill) {
@@ -257,16 +194,43 @@ __global__ void __launch_bounds__(256) k_advance(Dev d) {
 // count_rays per box (ray_tracing.cc:35-47) after the C2Ray pass removed rays; then the merge
 // set-up: num_thresh test and histogram reset (main.cc:153-163).
 __global__ void k_count(Dev d) {
+  // per-block counts in shared memory (one global atomic per box and block at the end); a warp
+  // whose live rays all belong to one box adds its ballot count in one step
+  constexpr int kSh = 256;
+  __shared__ unsigned long long sh[kSh];
+  const int nb = d.nbox;
+  const bool use_sh = nb <= kSh;
+  for (int k = threadIdx.x; k < kSh; k += blockDim.x) sh[k] = 0ull;
+  __syncthreads();
   const int cur = d.ctl->cur;
   const int n = d.ctl->nray[cur];
   const RayPool A = d.pool[cur];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    if (d.dead[i]) continue;
-    const int b = A.box[i];
-    const unsigned m = __match_any_sync(__activemask(), b);
-    if ((int)(threadIdx.x & 31) == __ffs(m) - 1)
-      atomicAdd((unsigned long long*)&d.count[b], (unsigned long long)__popc(m));
+  const int lane = threadIdx.x & 31;
+  for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+    const int i = i0 + threadIdx.x;
+    const bool alive = (i < n) && !d.dead[i];
+    const int b = alive ? (int)A.box[i] : -1;
+    const unsigned live = __ballot_sync(0xffffffffu, alive);
+    if (!live) continue;
+    const int b0 = __shfl_sync(0xffffffffu, b, __ffs(live) - 1);
+    const bool same = __all_sync(0xffffffffu, !alive || b == b0);
+    int add_box = -1;
+    unsigned long long add_n = 0;
+    if (same) {
+      if (lane == __ffs(live) - 1) { add_box = b0; add_n = __popc(live); }
+    } else if (alive) {
+      const unsigned m = __match_any_sync(live, b);
+      if (lane == __ffs(m) - 1) { add_box = b; add_n = __popc(m); }
+    }
+    if (add_box >= 0) {
+      if (use_sh) atomicAdd(&sh[add_box], add_n);
+      else atomicAdd((unsigned long long*)&d.count[add_box], add_n);
+    }
   }
+  __syncthreads();
+  if (use_sh)
+    for (int k = threadIdx.x; k < nb; k += blockDim.x)
+      if (sh[k]) atomicAdd((unsigned long long*)&d.count[k], sh[k]);
 }
 
 __global__ void k_merge_setup(Dev d) {
@@ -659,7 +623,10 @@ __global__ void k_fill_i32(int* p, int v, long long n) {
 // ---- launchers ------------------------------------------------------------------------------
 void launch_step_begin(const Dev& d, cudaStream_t s) { k_step_begin<<<grid_for(d.nsrc + 1, 256, 1184), 256, 0, s>>>(d); }
 
-void launch_advance(const Dev& d, int grid, cudaStream_t s) { k_advance<<<grid, 256, 0, s>>>(d); }
+void launch_advance(const Dev& d, int grid, cudaStream_t s) {
+  k_advance<<<grid, 256, 0, s>>>(d);
+  k_lit_compact<<<grid_for(d.ncell_total >> 4, 256, 148 * 8), 256, 0, s>>>(d);
+}
 
 void launch_count(const Dev& d, int grid, cudaStream_t s) {
   cudaMemsetAsync(d.count, 0, sizeof(long long) * d.nbox, s);

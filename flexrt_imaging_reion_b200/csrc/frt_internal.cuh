@@ -103,6 +103,26 @@ struct Dev {
   Ctl* ctl;
 };
 
+// Buffers of the adjoint of one step's Gamma field (frt_adjoint.cu). Cells on the paths of the
+// step's rays get a slot (in cell order); per slot the constants of the cell, the C2Ray iterates
+// a^k, b^k and the ray-pass rates of every iteration k, and the adjoint accumulators.
+struct AdjDev {
+  int cap, I, box;
+  int lo[3], hi[3];
+  uint8_t* flag;           // [ncell_total] cell on a path
+  int* slot;               // [ncell_total] slot or -1
+  int* cell;               // [cap]
+  uint8_t* in_obj;         // [cap] inside the objective sub-box
+  double *nH, *nHe, *y0h, *y0he, *crh, *crhe;   // [cap]
+  double *a, *b, *gh, *ghe;                    // [I][cap]
+  double *abar, *bbar, *gbh, *gbhe, *nhbar;    // [cap]
+  int* src_of_cell;        // [ncell_total] source index (context-wide) of a source cell, else -1
+  double* dlbar;           // [nsrc] sum over the source's rays of n0 * dJ/dn0
+  int* count;              // slots in use
+  unsigned* err;           // path overflow / slot capacity
+  double* J;               // objective
+};
+
 inline __host__ __device__ int grid_for(long long n, int block, int maxblocks) {
   long long g = (n + block - 1) / block;
   if (g < 1) g = 1;
@@ -126,5 +146,9 @@ void launch_dark(const Dev& d, bool strict, bool fused_thermal, int grid, cudaSt
 void launch_thermal_all(const Dev& d, bool strict, int grid, cudaStream_t s);
 void launch_clear_lit(const Dev& d, int grid, cudaStream_t s);
 void launch_gather_sparse(const Dev& d, long long cell0, long long ncell, int which, float* out, cudaStream_t s);
+// ---- adjoint (frt_adjoint.cu) --------------------------------------------------------
+void launch_adjoint(const Dev& d, const AdjDev& a, int grid, cudaStream_t s);
+void launch_adjoint_gather(const Dev& d, const AdjDev& a, long long cell0, long long ncell, float* out,
+                           cudaStream_t s);
 
 }  // namespace frt

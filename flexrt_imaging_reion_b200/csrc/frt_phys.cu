@@ -37,13 +37,23 @@ __device__ __forceinline__ int box_of_cell(const Dev& d, long long gc) { return 
 
 // 1 - e^-x and e^-x, both to full relative precision, for one transcendental: for x > 0.5 the
 // transmission is formed directly and the absorbed part as 1 - e (>= 0.39, no cancellation);
-// below, the absorbed part comes from expm1 and the transmission as 1 - a (>= 0.61).
+// below, the absorbed part is the Taylor series of 1 - e^-x = x - x^2/2! + x^3/3! - ... to the
+// x^8 term (alternating with decreasing terms for x <= 0.5: truncation below 0.5^8/9! ~ 1e-11
+// relative) and the transmission is 1 - a (>= 0.61).
 __device__ __forceinline__ void absorb_transmit(float x, float* a, float* e) {
   if (x > 0.5f) {
     *e = expf(-x);
     *a = 1.0f - *e;
   } else {
-    *a = -expm1f(-x);
+    float p = -1.0f / 40320.0f;
+    p = fmaf(p, x, 1.0f / 5040.0f);
+    p = fmaf(p, x, -1.0f / 720.0f);
+    p = fmaf(p, x, 1.0f / 120.0f);
+    p = fmaf(p, x, -1.0f / 24.0f);
+    p = fmaf(p, x, 1.0f / 6.0f);
+    p = fmaf(p, x, -0.5f);
+    p = fmaf(p, x, 1.0f);
+    *a = x * p;
     *e = 1.0f - *a;
   }
 }
@@ -85,13 +95,12 @@ __global__ void k_lit_init(Dev d) {
     d.l_acc_ghe[s] = 0.f;
     d.l_heat_h[s] = 0.f;
     d.l_heat_he[s] = 0.f;
-    for (int nu = 0; nu < F; nu++) {
-      d.l_ngam[(size_t)nu * L + s] = 0.f;
-      if (STRICT || d.per_bin) {
+    if (STRICT || d.per_bin)
+      for (int nu = 0; nu < F; nu++) {
+        d.l_ngam[(size_t)nu * L + s] = 0.f;
         d.l_acc_nu_h[(size_t)nu * L + s] = 0.f;
         d.l_acc_nu_he[(size_t)nu * L + s] = 0.f;
       }
-    }
   }
 }
 
@@ -100,12 +109,16 @@ __global__ void k_lit_init(Dev d) {
 // the current time-averaged neutral densities of the lit cells, and deposits Gamma_HI / HeI.
 // FIRST converts the segment cell indices to lit slots; LAST also writes per-bin rates, the new
 // photon counts and removes rays below nphot_min.
-template <bool STRICT, bool FIRST, bool LAST>
+// NF > 0 fixes the number of frequency bins at compile time (the 5-bin spectrum of every
+// configuration here), so the per-bin loops unroll exactly; NF = 0 takes d.F at run time.
+template <bool STRICT, bool FIRST, bool LAST, int NF>
 __global__ void __launch_bounds__(256) k_raypass(Dev d) {
   const int cur = d.ctl->cur;
   const int n = d.ctl->nray[cur];
   const RayPool A = d.pool[cur];
   const int cap = d.ray_cap, F = d.F, L = d.lit_cap;
+  constexpr int MAXF = NF > 0 ? NF : FRT_MAX_FREQ;
+  const int Fr = NF > 0 ? NF : F;
   double dep = 0.0, kil = 0.0, ovl = 0.0;
   long long nkill = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -122,7 +135,7 @@ __global__ void __launch_bounds__(256) k_raypass(Dev d) {
     const double nmin = B.nphot_min;
     float nph[FRT_MAX_FREQ];
 #pragma unroll
-    for (int nu = 0; nu < FRT_MAX_FREQ; nu++) nph[nu] = (nu < F) ? A.nphot[(size_t)nu * cap + i] : 0.f;
+    for (int nu = 0; nu < FRT_MAX_FREQ; nu++) nph[nu] = (nu < Fr) ? A.nphot[(size_t)nu * cap + i] : 0.f;
     bool dumped = false;
     unsigned dump_mask = 0;
     if (STRICT) {
@@ -192,9 +205,9 @@ __global__ void __launch_bounds__(256) k_raypass(Dev d) {
       // Mixed precision: per bin the photon count is carried from segment to segment by its
       // transmission e^-dtau instead of recomputing e^-tau, and each bin costs one transcendental
       // when HeI does not absorb there (sigma_HeI = 0 below 24.59 eV) and two when it does.
-      float nin[FRT_MAX_FREQ];
+      float nin[MAXF];
 #pragma unroll
-      for (int nu = 0; nu < FRT_MAX_FREQ; nu++) nin[nu] = nph[nu];
+      for (int nu = 0; nu < MAXF; nu++) nin[nu] = nph[nu];
       const float kdep = B.kdep_f;
       for (int p = 0; p < ns; p++) {
         const int slot = d.seg[(size_t)p * cap + i];
@@ -203,16 +216,16 @@ __global__ void __launch_bounds__(256) k_raypass(Dev d) {
         const float a = d.l_avg_h[slot], b = d.l_avg_he[slot];
         float total = 0.f;
 #pragma unroll
-        for (int nu = 0; nu < FRT_MAX_FREQ; nu++) total += (nu < F) ? nin[nu] : 0.f;
+        for (int nu = 0; nu < MAXF; nu++) total += (nu < Fr) ? nin[nu] : 0.f;
         const bool dump = (double)total < nmin;
         float gsum_h = 0.f, gsum_he = 0.f;
-        float gh_nu[FRT_MAX_FREQ], ghe_nu[FRT_MAX_FREQ], tr[FRT_MAX_FREQ];
+        float gh_nu[MAXF], ghe_nu[MAXF], tr[MAXF];
 #pragma unroll
-        for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
+        for (int nu = 0; nu < MAXF; nu++) {
           gh_nu[nu] = 0.f;
           ghe_nu[nu] = 0.f;
           tr[nu] = 1.f;
-          if (nu >= F) continue;
+          if (nu >= Fr) continue;
           const float dth = (a * d.sigH1_f[nu]) * dist;
           const float dthe = (b * d.sigHe1_f[nu]) * dist;
           float ah, eh;
@@ -258,10 +271,10 @@ __global__ void __launch_bounds__(256) k_raypass(Dev d) {
         if (LAST) {
           float hh = 0.f, hhe = 0.f;
 #pragma unroll
-          for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
-            if (nu >= F) continue;
-            atomicAdd(&d.l_ngam[(size_t)nu * L + slot], nin[nu]);
-            if (d.per_bin) {
+          for (int nu = 0; nu < MAXF; nu++) {
+            if (nu >= Fr) continue;
+            if (d.per_bin) {   // per-bin rates and photon counts: output fields (diag outputs)
+              atomicAdd(&d.l_ngam[(size_t)nu * L + slot], nin[nu]);
               if (gh_nu[nu] != 0.f) atomicAdd(&d.l_acc_nu_h[(size_t)nu * L + slot], gh_nu[nu] * wh);
               if (ghe_nu[nu] != 0.f) atomicAdd(&d.l_acc_nu_he[(size_t)nu * L + slot], ghe_nu[nu] * whe);
             }
@@ -274,12 +287,12 @@ __global__ void __launch_bounds__(256) k_raypass(Dev d) {
           dep += (double)gsum_h + (double)gsum_he;
         }
 #pragma unroll
-        for (int nu = 0; nu < FRT_MAX_FREQ; nu++) nin[nu] *= tr[nu];
+        for (int nu = 0; nu < MAXF; nu++) nin[nu] *= tr[nu];
         if (dump) { dumped = true; break; }
       }
       if (LAST) {
         float s = 0.f;
-        for (int nu = 0; nu < F; nu++) {
+        for (int nu = 0; nu < Fr; nu++) {
           nph[nu] = nin[nu];
           A.nphot[(size_t)nu * cap + i] = nph[nu];
           s += nph[nu];
@@ -289,7 +302,7 @@ __global__ void __launch_bounds__(256) k_raypass(Dev d) {
           nkill += 1;
           kil += (double)s;
           if (dumped)
-            for (int nu = 0; nu < F; nu++)
+            for (int nu = 0; nu < Fr; nu++)
               if (dump_mask & (1u << nu)) ovl += (double)nph[nu];
         }
       }
@@ -315,6 +328,9 @@ struct Final {
   bool set_treion;
 };
 
+// Mixed precision takes the fractions and dn_e/dt with the fast division (2 ulp); the ratio
+// that decides the reionisation flag keeps the correctly rounded one.
+template <bool STRICT>
 __device__ __forceinline__ Final finalize(float nH, float nHe, float nh1_end, float nhe1_end, float avg_h, float ne_old,
                                           float dt, bool flag) {
   Final f;
@@ -324,11 +340,19 @@ __device__ __forceinline__ Final finalize(float nH, float nHe, float nh1_end, fl
   f.nHe2 = nHe - f.nHe1;
   f.set_treion = (avg_h / nH < 0.5) && !flag;
   f.ne = (float)((double)(f.nH2 + f.nHe2) + 2. * 0.0);
-  f.dne_dt = (-ne_old + f.ne) / dt;
   f.n_tot = nH + nHe + f.ne;
-  f.f_H2 = f.nH2 / nH;
-  f.f_H1 = f.nH1 / nH;
-  f.f_He1 = f.nHe1 / nHe;
+  if (STRICT) {
+    f.dne_dt = (-ne_old + f.ne) / dt;
+    f.f_H2 = f.nH2 / nH;
+    f.f_H1 = f.nH1 / nH;
+    f.f_He1 = f.nHe1 / nHe;
+  } else {
+    f.dne_dt = __fdividef(-ne_old + f.ne, dt);
+    const float inv_nh = __fdividef(1.0f, nH);
+    f.f_H2 = f.nH2 * inv_nh;
+    f.f_H1 = f.nH1 * inv_nh;
+    f.f_He1 = __fdividef(f.nHe1, nHe);
+  }
   return f;
 }
 
@@ -361,7 +385,7 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d) {
     }
     const bool flag = d.treion_flag[gc] != 0;
     const float ne_old = d.ne[gc];
-    const Final f = finalize(nH, nHe, nh1_end, nhe1_end, a_new, ne_old, dt, flag);
+    const Final f = finalize<STRICT>(nH, nHe, nh1_end, nhe1_end, a_new, ne_old, dt, flag);
     if (f.set_treion) {
       d.treion[gc] = B.t;
       d.treion_flag[gc] = 1;
@@ -461,7 +485,7 @@ __global__ void __launch_bounds__(256, 4) k_dark(Dev d) {
     }
     const bool flag = d.treion_flag[gc] != 0;
     const float ne_old = d.ne[gc];
-    const Final f = finalize(nH, nHe, nh1_end, nhe1_end, a, ne_old, dt, flag);
+    const Final f = finalize<STRICT>(nH, nHe, nh1_end, nhe1_end, a, ne_old, dt, flag);
     if (f.set_treion) {
       d.treion[gc] = B.t;
       d.treion_flag[gc] = 1;
@@ -590,7 +614,11 @@ void launch_lit_init(const Dev& d, bool strict, int grid, cudaStream_t s) {
 
 void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t s) {
   const bool first = iter == 0, last = iter == d.itercount - 1;
-#define RP(ST, FI, LA) k_raypass<ST, FI, LA><<<grid, 256, 0, s>>>(d)
+#define RP(ST, FI, LA)                                                   \
+  do {                                                                   \
+    if (d.F == 5) k_raypass<ST, FI, LA, 5><<<grid, 256, 0, s>>>(d);      \
+    else k_raypass<ST, FI, LA, 0><<<grid, 256, 0, s>>>(d);               \
+  } while (0)
   if (strict) {
     if (first && last) RP(true, true, true);
     else if (first) RP(true, true, false);

@@ -268,10 +268,17 @@ __device__ inline float thermal_tstep(const ThermCell& c, const ThermConst& k) {
 // set_Treion_default (gas_funcs.cc:104-129): post-I-front temperature, I-front speed and flux.
 template <bool STRICT>
 __device__ inline void treion_default(ThermCell& c, const ThermConst& k, float nhe_to_nh) {
-  const float fion_new = (c.nH - c.nH1) / c.nH;
-  const float fion_old = (c.nH - c.nH1_prev) / c.nH;
-  const float deltax = k.dx * (fion_new - fion_old);
-  const float vIF = deltax / k.dt;
+  float fion_new, fion_old, vIF;
+  if (STRICT) {
+    fion_new = (c.nH - c.nH1) / c.nH;
+    fion_old = (c.nH - c.nH1_prev) / c.nH;
+    vIF = k.dx * (fion_new - fion_old) / k.dt;
+  } else {
+    const float inv_nh = __fdividef(1.0f, c.nH);
+    fion_new = (c.nH - c.nH1) * inv_nh;
+    fion_old = (c.nH - c.nH1_prev) * inv_nh;
+    vIF = __fdividef(k.dx * (fion_new - fion_old), k.dt);
+  }
   if ((fion_new > fion_old) && (fion_new < 0.98)) {
     const float Cn[5] = {9.5432f, -1.6441e-2f, -9.8010e-3f, 4.1664e-3f, -2.2710e-4f};
     float lnT = 0.f;

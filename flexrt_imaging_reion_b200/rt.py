@@ -303,6 +303,24 @@ class RTContext:
                     "frt_download_rays")
         return out
 
+    def adjoint(self, lo, hi, box: int = 0, want_dl: bool = True, want_dnh: bool = True):
+        """frt_adjoint: J = sum of Gamma_HI over cells [lo, hi) of `box` after the next step's
+        C2Ray iteration, with dJ/dL per source (photons/s) and dJ/dn_H per cell (cm^-3, N^3).
+        Needs the state right after setup()."""
+        obj = _abi.AdjObjective()
+        obj.box = box
+        for k in range(3):
+            obj.lo[k] = int(lo[k])
+            obj.hi[k] = int(hi[k])
+        J = C.c_double(0.0)
+        dl = np.zeros(max(1, self.nsrc_box[box]), np.float64) if want_dl else None
+        dnh = np.zeros(self.specs[box].n ** 3, np.float32) if want_dnh else None
+        self._check(self.L.frt_adjoint(self.h, C.byref(obj), C.byref(J), None if dl is None else dl.ctypes.data,
+                                       None if dnh is None else dnh.ctypes.data), "frt_adjoint")
+        if dl is not None:
+            dl = dl[:self.nsrc_box[box]]
+        return float(J.value), dl, dnh
+
     def box_scalars(self, box: int = 0) -> Dict[str, float]:
         v = np.zeros(8)
         self._check(self.L.frt_box_scalars(self.h, box, v.ctypes.data), "frt_box_scalars")

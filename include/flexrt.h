@@ -70,7 +70,10 @@ typedef struct {
   long long lit_capacity;           /* cells touched by rays in one step (all boxes); 0 = all cells */
   long long src_capacity;           /* sources (all boxes) */
   int precision;                    /* FRT_PREC_MIXED (FP32 + FP64 where x_HI < 1e-3) or FRT_PREC_STRICT */
-  int outputs;                      /* FRT_OUT_CORE or FRT_OUT_DIAG (also keep mfp, recrate, u_nu, vIF...) */
+  int outputs;                      /* FRT_OUT_CORE: the state, Gamma totals and heating rates;
+                                       FRT_OUT_DIAG also keeps the output-only fields: per-bin Gamma and
+                                       photon counts (ngam_nu, io_funcs.cc:387), mfp, recrate, u_nu, vIF.
+                                       Strict precision keeps the per-bin fields in either mode. */
   int device;                       /* CUDA device ordinal */
 } frt_config;
 
@@ -191,6 +194,22 @@ frt_status frt_box_scalars(frt_ctx* ctx, int box, double* out8);
 /* Kernel time of the last frt_step / frt_step_plain in ms (device events on the step stream),
  * and the time of its dominant cell kernel. */
 frt_status frt_last_timing(frt_ctx* ctx, float* step_ms, float* cell_kernel_ms);
+
+/* ---- adjoint of the next step's Gamma field --------------------------------------------------
+ * Objective: J = sum of Gamma_HI (gamma_H1_tot, ray_tracing.cc:1152) over the cells
+ * [lo, hi) (i, j, k) of one box after the C2Ray iteration of the next step. frt_adjoint returns J
+ * and its gradient with respect to every source luminosity of that box (photons/s, in
+ * frt_set_sources order) and every cell's hydrogen density n_H (cm^-3; the cell's n_He, n_HI and
+ * n_HeI scale with it as one density; ionised fractions, temperature, clumping and nphot_min are
+ * held fixed). The segments of the step's rays are recomputed from the ray state, nothing is
+ * stored between passes, and the context's state is not modified. Needs the state right after
+ * set-up (no step taken: every ray still belongs to one source's cast); FRT_ERR_STATE otherwise.
+ * dL (nsrc of the box) and dnH (N^3) may be NULL. No counterpart in the reference. */
+typedef struct {
+  int box;
+  int lo[3], hi[3];
+} frt_adj_objective;
+frt_status frt_adjoint(frt_ctx* ctx, const frt_adj_objective* obj, double* J, double* dL, float* dnH);
 
 /* ---- field read-back without device allocation ---------------------------------------------
  * No counterpart in the reference (its fields live in host arrays). Gathers cells

@@ -22,6 +22,7 @@
 #include <string.h>
 
 #include <cmath>
+#include <unordered_map>
 #include <vector>
 
 #include "frtd.h"
@@ -1036,6 +1037,195 @@ int orc_dump(void* h, const char* path) {
 }
 
 void orc_destroy(void* h) { delete (Ctx*)h; }
+
+}  // extern "C"
+
+// ---- FP64 objective of one step and its tangent-linear form (checks of the adjoint) -------------
+// The objective J = sum of Gamma_HI over a sub-box after the C2Ray iteration of the next step
+// (ray pass ray_tracing.cc:701-938, cell update 1077-1113, Gamma total 1152), as a function of
+// per-source luminosity factors lam_s and per-cell density factors s_c. A factor s_c scales the
+// cell's n_H together with everything init() derives from the same density (n_He, n_HI, n_HeI;
+// init_funcs.cc:34-62); ionised fractions, temperatures and recombination coefficients stay
+// fixed. Rays take the photon counts of their set-up cast scaled by lam of their source, and the
+// segments of the next advance (advance_ray above). The kill threshold nphot_min stays at its
+// set-up value. Evaluated in double throughout (no float storage of the iterates), generic over
+// the scalar type so that the same code gives the value (double) and the directional derivative
+// (Dual: value and tangent, forward-mode differentiation).
+namespace {
+
+struct Dual {
+  double v, d;
+};
+inline Dual mk(double v, double d = 0.) { return Dual{v, d}; }
+inline Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+inline Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+inline Dual operator-(Dual a) { return {-a.v, -a.d}; }
+inline Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+inline Dual operator/(Dual a, Dual b) { return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)}; }
+inline Dual exp(Dual a) {
+  const double e = std::exp(a.v);
+  return {e, e * a.d};
+}
+inline double val(Dual a) { return a.v; }
+inline double val(double a) { return a; }
+template <typename S> S cst(double v) { return S(v); }
+template <> Dual cst<Dual>(double v) { return mk(v); }
+inline double expx(double a) { return std::exp(a); }
+inline Dual expx(Dual a) { return exp(a); }
+
+struct AdjRay {
+  int src;
+  int nseg;
+  long cell[kMaxPL];
+  double dist[kMaxPL];
+  double n0[kMaxF];
+};
+
+struct AdjProblem {
+  std::vector<AdjRay> rays;
+  std::vector<long> lit;                         // lit cells (global index)
+  std::unordered_map<long, int> slot;            // cell -> lit slot
+  std::vector<char> in_obj;                      // per lit slot: inside the objective sub-box
+};
+
+AdjProblem adj_setup(Ctx& c, const int* lo, const int* hi) {
+  AdjProblem P;
+  std::unordered_map<long, int> src_of;
+  for (size_t s = 0; s < c.src.size(); ++s) src_of[cidx(c, c.src[s].i, c.src[s].j, c.src[s].k)] = (int)s;
+  c.clight = c.cl_factor * O_CL;
+  c.nc = c.nl_const;
+  for (const Ray& R0 : c.rays) {
+    if (!R0.alive) continue;
+    Ray R = R0;
+    const long cell0 = R.pind[0];
+    advance_ray(c, R);
+    if (R.active) continue;   // did not leave its cell: no segments this step
+    if (c.rkill > 0.0 && (double)R.r > c.rkill) continue;
+    AdjRay A;
+    auto it = src_of.find(cell0);
+    A.src = it == src_of.end() ? -1 : it->second;
+    A.nseg = R.ray_end;
+    for (int p = 0; p < R.ray_end; ++p) {
+      A.cell[p] = R.pind[p];
+      A.dist[p] = R.pdist[p];
+      if (!P.slot.count(R.pind[p])) {
+        P.slot[R.pind[p]] = (int)P.lit.size();
+        P.lit.push_back(R.pind[p]);
+      }
+    }
+    for (int nu = 0; nu < c.F; ++nu) A.n0[nu] = (double)R0.nphot[nu] * kPhotNorm;
+    P.rays.push_back(A);
+  }
+  P.in_obj.resize(P.lit.size());
+  for (size_t j = 0; j < P.lit.size(); ++j) {
+    int i, jj, k;
+    split_ind(c, (int)P.lit[j], &i, &jj, &k);
+    P.in_obj[j] = i >= lo[0] && i < hi[0] && jj >= lo[1] && jj < hi[1] && k >= lo[2] && k < hi[2];
+  }
+  return P;
+}
+
+template <typename S>
+S adj_objective(const Ctx& c, const AdjProblem& P, const std::vector<S>& lam, const std::vector<S>& sc) {
+  const int F = c.F, I = c.itercount;
+  const size_t L = P.lit.size();
+  const double dt = c.dt, vol = (double)c.dxc * (double)c.dxc * (double)c.dxc;
+  std::vector<S> nH(L), nHe(L), a(L), b(L), gh(L), ghe(L);
+  std::vector<double> y0h(L), y0he(L), crh(L), crhe(L);
+  for (size_t j = 0; j < L; ++j) {
+    const long q = P.lit[j];
+    nH[j] = cst<S>((double)c.nH[q]) * sc[j];
+    nHe[j] = cst<S>((double)c.nHe[q]) * sc[j];
+    a[j] = cst<S>((double)c.nH1[q]) * sc[j];
+    b[j] = cst<S>((double)c.nHe1[q]) * sc[j];
+    y0h[j] = c.f_H1[q];
+    y0he[j] = c.f_He1[q];
+    const float cl = c.have_clump ? c.clump_in[q] : c.const_clump;
+    crh[j] = (double)(cl * (float)alphaB_H2(maxd(kTempMin, c.temp[q])));
+    float rhe = (float)alphaB_He2(maxd(kTempMin, c.temp[q]));
+    if ((c.temp[q] >= 3e4) && (c.temp[q] <= 1e6)) rhe += (float)Dalpha_He2(maxd(kTempMin, c.temp[q]));
+    crhe[j] = (double)(cl * rhe);
+  }
+  S J = cst<S>(0.);
+  for (int it = 0; it < I; ++it) {
+    for (size_t j = 0; j < L; ++j) { gh[j] = cst<S>(0.); ghe[j] = cst<S>(0.); }
+    for (const AdjRay& R : P.rays) {
+      S nin[kMaxF];
+      for (int nu = 0; nu < F; ++nu) nin[nu] = cst<S>(R.n0[nu]) * (R.src >= 0 ? lam[R.src] : cst<S>(1.));
+      for (int p = 0; p < R.nseg; ++p) {
+        const int j = P.slot.at(R.cell[p]);
+        double tot = 0.;
+        for (int nu = 0; nu < F; ++nu) tot += val(nin[nu]) / kPhotNorm;
+        const bool dump = tot < c.nphot_min;
+        S tr[kMaxF];
+        for (int nu = 0; nu < F; ++nu) {
+          const S x = a[j] * cst<S>(c.sigH1[nu] * R.dist[p]);
+          const S y = b[j] * cst<S>(c.sigHe1[nu] * R.dist[p]);
+          const S ex = expx(-x), ey = expx(-y);
+          S fh = cst<S>(0.), fhe = cst<S>(0.);
+          if (val(x) > 0. || val(y) > 0.) {
+            const S x1 = (cst<S>(1.) - ex) * ey, x2 = (cst<S>(1.) - ey) * ex;
+            fh = x1 / (x1 + x2);
+            fhe = x2 / (x1 + x2);
+          }
+          const S absb = dump ? cst<S>(1.) : cst<S>(1.) - ex * ey;
+          gh[j] = gh[j] + fh * nin[nu] * absb / cst<S>(dt * vol) / a[j];
+          ghe[j] = ghe[j] + fhe * nin[nu] * absb / cst<S>(dt * vol) / b[j];
+          tr[nu] = ex * ey;
+        }
+        if (dump) break;
+        for (int nu = 0; nu < F; ++nu) nin[nu] = nin[nu] * tr[nu];
+      }
+    }
+    if (it == I - 1) {
+      for (size_t j = 0; j < L; ++j)
+        if (P.in_obj[j]) J = J + gh[j];
+      break;
+    }
+    for (size_t j = 0; j < L; ++j) {   // C2Ray update of the lit cells (dark cells never enter J)
+      const S ne = nH[j] - a[j] + nHe[j] - b[j];
+      const S prh = gh[j] + cst<S>(crh[j]) * ne;
+      const S xeq = gh[j] / prh;
+      const S a_new = nH[j] * (cst<S>(1.) - (xeq + (cst<S>(1. - y0h[j]) - xeq) * (cst<S>(1.) - expx(-cst<S>(dt) * prh)) /
+                                                     (cst<S>(dt) * prh)));
+      const S prhe = ghe[j] + cst<S>(crhe[j]) * ne;
+      const S xeqhe = ghe[j] / prhe;
+      const S b_new = nHe[j] * (cst<S>(1.) - (xeqhe + (cst<S>(1. - y0he[j]) - xeqhe) *
+                                                           (cst<S>(1.) - expx(-cst<S>(dt) * prhe)) / (cst<S>(dt) * prhe)));
+      a[j] = a_new;
+      b[j] = b_new;
+    }
+  }
+  return J;
+}
+
+}  // namespace
+
+extern "C" {
+
+// J and, with tangent directions (dlam per source, dsc per cell; NULL = 0), its directional
+// derivative. lam / sc are the factors (NULL = all 1); sc and dsc are dense per cell (N^3).
+double orc_adj_objective(void* h, const int* lo, const int* hi, const double* lam, const double* sc,
+                         const double* dlam, const double* dsc, double* jvp, long* nlit) {
+  Ctx& c = *(Ctx*)h;
+  AdjProblem P = adj_setup(c, lo, hi);
+  if (nlit) *nlit = (long)P.lit.size();
+  const size_t ns = c.src.size(), L = P.lit.size();
+  if (!dlam && !dsc) {
+    std::vector<double> l(ns, 1.), s(L, 1.);
+    if (lam) for (size_t i = 0; i < ns; ++i) l[i] = lam[i];
+    if (sc) for (size_t j = 0; j < L; ++j) s[j] = sc[P.lit[j]];
+    if (jvp) *jvp = 0.;
+    return adj_objective<double>(c, P, l, s);
+  }
+  std::vector<Dual> l(ns), s(L);
+  for (size_t i = 0; i < ns; ++i) l[i] = mk(lam ? lam[i] : 1., dlam ? dlam[i] : 0.);
+  for (size_t j = 0; j < L; ++j) s[j] = mk(sc ? sc[P.lit[j]] : 1., dsc ? dsc[P.lit[j]] : 0.);
+  const Dual J = adj_objective<Dual>(c, P, l, s);
+  if (jvp) *jvp = J.d;
+  return J.v;
+}
+
 
 // rotation of healpix_funcs.cc:102-143 with the angles of get_random_angles (healpix_funcs.cc:21-39)
 void orc_rotate(int itheta, int direction, const double* v, double* out) {

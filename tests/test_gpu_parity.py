@@ -2,8 +2,8 @@
 
 The oracle (oracle/frt_oracle.cc) is pinned bit-exact to the reference's own code by
 tests/test_oracle_golden.py. Tolerances are stated in tests/parity_tools.py: ray tree and ray
-geometry exact (merged rays 1e-5 of the cell size), ray photon counts 1e-4 relative (strict 1e-5;
-merged rays 1e-3), Gamma_HI 1e-4 relative per cell (strict 1e-5), x_HI 1e-4 absolute, T 1e-3
+geometry exact (merged rays 1e-5 of the cell size), ray photon counts per bin 1e-4 of the ray's
+photon total (strict 1e-5; merged rays 1e-3), Gamma_HI 1e-4 relative per cell (strict 1e-5), x_HI 1e-4 absolute, T 1e-3
 relative (strict 1e-4), photon ledger closed to 1e-6.
 """
 import numpy as np
@@ -63,8 +63,8 @@ def check(states, ref, strict, merged=False):
         r = PT.compare_rays(states[s], ref[s], ref[s]["scalars"][2], 1e-5 if strict else 1e-4,
                             dx=float(ref[s]["scalars"][8]), dx0=float(ref[s]["scalars"][7]))
         assert r["unmatched_dev"] + r["unmatched_ref"] - r["unmatched_near_tie"] == 0, (s, r)
-        assert r["nphot_bad"] == 0, (s, r)
-        assert r["nphot_merged_bad"] == 0, (s, r)
+        assert r["nphot_bad"] == 0, f"step {s}: {r}"
+        assert r["nphot_merged_bad"] == 0, f"step {s}: {r}"
         if not merged:
             assert r["matched_merged"] == 0, (s, r)
         assert r["merged_geom_bad"] == 0, (s, r)
@@ -84,8 +84,9 @@ def test_t16_parity(precision, mode):
 
 
 def test_t16_core_outputs():
-    """Core outputs, mixed precision: the last ray pass keeps only the bin-weighted photo-heating
-    sums, so the temperature path differs from the diag run; per-bin rates are refused."""
+    """Core outputs, mixed precision: the last ray pass keeps only the Gamma totals and the
+    bin-weighted photo-heating sums, so the temperature path differs from the diag run; the
+    per-bin output fields (rates, photon counts) are refused."""
     spec, seed = T16
     ref = oracle_run(spec, seed)
     states, stats, _ = run_device(spec, seed, "mixed", "graph", diag=False)
@@ -93,9 +94,10 @@ def test_t16_core_outputs():
     ctx = rt.RTContext([W.make_inputs(spec)], [seed], outputs="core", ray_capacity=1 << 20)
     ctx.setup()
     ctx.step()
-    with pytest.raises(rt.FrtError, match="status 5"):
-        ctx.get_field(0, "GAMMA_H1_NU")
-    assert ctx.get_field(0, "NGAM_NU").shape[-1] == 5
+    for f in ("GAMMA_H1_NU", "GAMMA_HE1_NU", "NGAM_NU"):
+        with pytest.raises(rt.FrtError, match="status 5"):
+            ctx.get_field(0, f)
+    assert ctx.get_field(0, "GAMMA_H1_TOT").max() > 0
     ctx.close()
 
 

@@ -37,9 +37,9 @@ def test_noalloc_matches_get_field_twice(outputs):
     ctx = rt.RTContext([W.make_inputs(spec)], [3], outputs=outputs, ray_capacity=1 << 20)
     ctx.setup()
     ncell = spec.n ** 3
-    fields = [("GAMMA_H1_TOT", 0), ("GAMMA_HE1_TOT", 0), ("NGAM_NU", 2)]
+    fields = [("GAMMA_H1_TOT", 0), ("GAMMA_HE1_TOT", 0)]
     if outputs == "diag":
-        fields += [("GAMMA_H1_NU", 1), ("GAMMA_HE1_NU", 4)]
+        fields += [("NGAM_NU", 2), ("GAMMA_H1_NU", 1), ("GAMMA_HE1_NU", 4)]
     for _ in range(2):   # two calls in a row, each after a step
         ctx.step()
         for field, b in fields:
@@ -71,8 +71,9 @@ def test_noalloc_rejects_bad_requests():
     assert st == _abi.FRT_ERR_INVALID
     st, _ = _noalloc(ctx, 0, "NGAM_NU", 9, 0, 10)                     # bin out of range
     assert st == _abi.FRT_ERR_INVALID
-    st, _ = _noalloc(ctx, 0, "GAMMA_H1_NU", 0, 0, 10)                 # per-bin rates not kept
-    assert st == _abi.FRT_ERR_STATE
+    for f in ("GAMMA_H1_NU", "NGAM_NU"):                               # per-bin fields not kept
+        st, _ = _noalloc(ctx, 0, f, 0, 0, 10)
+        assert st == _abi.FRT_ERR_STATE
     st, got = _noalloc(ctx, 0, "GAMMA_H1_TOT", 0, 0, ncell)
     assert st == _abi.FRT_OK
     np.testing.assert_array_equal(got, ctx.get_field(0, "GAMMA_H1_TOT"))
