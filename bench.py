@@ -261,6 +261,43 @@ def run_ensemble(args, rank: int, world: int, local_rank: int):
     return res
 
 
+# ---- adjoint (A) ------------------------------------------------------------------------------
+def run_adjoint(args):
+    """One forward step of the adjoint box (graph, CUDA-event device time) against frt_adjoint of
+    the same set-up state (CUDA-event device time of its kernels; the host wall time of the whole
+    call, gradient read-back included, is reported beside it)."""
+    import numpy as np
+    from flexrt_imaging_reion_b200 import workloads as W, rt
+    spec = W.config_A()
+    inp = W.make_inputs(spec)
+    lo, hi = [56, 56, 56], [72, 72, 72]
+    fwd = []
+    for _ in range(max(3, args.steps)):
+        with rt.RTContext([inp], [args.seed], ray_capacity=1 << 20) as c:
+            c.setup()
+            c.step()
+            fwd.append(c.last_timing()[0])
+    with rt.RTContext([inp], [args.seed], ray_capacity=1 << 20) as c:
+        c.setup()
+        for _ in range(args.warmup):
+            c.adjoint(lo, hi)
+        ts, dev = [], []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            J, dl, dnh = c.adjoint(lo, hi)
+            ts.append(1e3 * (time.perf_counter() - t0))
+            dev.append(c.last_adjoint_ms())
+    step_ms = float(np.median(fwd))
+    adj_ms = float(np.median(dev))
+    return {"metric": "adjoint cost / forward step (device time)", "value": adj_ms / step_ms, "unit": "ratio",
+            "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "step_ms": step_ms, "adjoint_ms": adj_ms, "adjoint_call_ms_wall": float(np.median(ts)),
+            "J": J, "nonzero_dnH": int(np.count_nonzero(dnh)),
+            "config": {"workload": "A: 128^3, 50 h^-1 cMpc, z=7, 256 sources log-uniform [1e51,1e53] in the centred "
+                                   "32^3 cells, 1 step of 1 Myr; J = sum Gamma_HI over the centred 16^3 cells"},
+            "dtype": "f64 (adjoint), f32 (forward step)", "data": "synthetic"}
+
+
 # ---- our arm ---------------------------------------------------------------------------------
 def launches_per_step(spec, ray_capacity, itercount=5, hpx_lvl=0):
     """Kernels one fused step launches: clear_lit, step_begin, advance, lit_compact, dark, lit_init,
@@ -359,7 +396,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["L", "M", "S", "E"], default="L")
+    ap.add_argument("--workload", choices=["L", "M", "S", "E", "A"], default="L")
     ap.add_argument("--no-loop", action="store_true", help="E: skip the per-box launch-loop comparison")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--ray-capacity", type=int, default=16 << 20)
@@ -428,6 +465,10 @@ def main():
         from datetime import timedelta
         torch.cuda.set_device(local_rank)
         tdist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    if args.workload == "A":
+        if rank == 0:
+            print(json.dumps(run_adjoint(args)))
+        return
     if args.workload == "E":
         res = run_ensemble(args, rank, world, local_rank)
     else:

@@ -30,7 +30,8 @@ EXPORTS = ["frt_create", "frt_destroy", "frt_last_error", "frt_rotation_table", 
            "frt_get_nphot_min_max", "frt_set_clump", "frt_set_clight", "frt_update_rays", "frt_find_avg_unu",
            "frt_count_rays", "frt_merge", "frt_split_rays", "frt_update_thermal", "frt_new_rays", "frt_step",
            "frt_step_plain", "frt_last_stats", "frt_num_rays", "frt_download_rays", "frt_box_scalars",
-           "frt_last_timing", "frt_seed_boxes", "frt_draw_cast", "frt_draw_step", "frt_get_sparse_field_noalloc", "frt_adjoint"]
+           "frt_last_timing", "frt_seed_boxes", "frt_draw_cast", "frt_draw_step", "frt_get_sparse_field_noalloc", "frt_adjoint",
+           "frt_last_adjoint_timing"]
 NOALLOC_MAX_CELLS = 1 << 20
 
 
@@ -112,6 +113,7 @@ def lib() -> C.CDLL:
         "frt_draw_step": ([P, P, P], I),
         "frt_get_sparse_field_noalloc": ([P, I, I, I, LL, LL, P], I),
         "frt_adjoint": ([P, C.POINTER(AdjObjective), P, P, P], I),
+        "frt_last_adjoint_timing": ([P, P], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

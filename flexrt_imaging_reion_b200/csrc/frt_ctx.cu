@@ -41,6 +41,7 @@ struct frt_ctx {
   AdjDev adj{};
   bool adj_ready = false;
   float* adj_out = nullptr;   // gather buffer of the adjoint's per-cell output (largest box)
+  float last_adjoint_ms = 0.f;
   frt_step_stats last{};
   std::string err;
   // glibc rand() streams, one per box (srand(seed) semantics via initstate_r / random_r)
@@ -956,6 +957,12 @@ frt_status frt_box_scalars(frt_ctx* ctx, int box, double* out8) {
   return FRT_OK;
 }
 
+frt_status frt_last_adjoint_timing(frt_ctx* ctx, float* ms) {
+  if (!ctx || !ms) return FRT_ERR_INVALID;
+  *ms = ctx->last_adjoint_ms;
+  return FRT_OK;
+}
+
 frt_status frt_last_timing(frt_ctx* ctx, float* step_ms, float* cell_kernel_ms) {
   if (!ctx) return FRT_ERR_INVALID;
   if (step_ms) *step_ms = ctx->last_step_ms;
@@ -1028,9 +1035,12 @@ frt_status frt_adjoint(frt_ctx* ctx, const frt_adj_objective* obj, double* J, do
   CK(cudaMemsetAsync(a.err, 0, sizeof(unsigned), s));
   CK(cudaMemsetAsync(a.J, 0, sizeof(double), s));
   CK(cudaMemsetAsync(a.dlbar, 0, sizeof(double) * std::max(1, d.src_cap), s));
+  CK(cudaEventRecord(ctx->ev_t0, s));
   launch_adjoint(d, a, ctx->grid_rays, s);
+  CK(cudaEventRecord(ctx->ev_t1, s));
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(s));
+  CK(cudaEventElapsedTime(&ctx->last_adjoint_ms, ctx->ev_t0, ctx->ev_t1));
   unsigned err = 0;
   double Jv = 0.0;
   CK(cudaMemcpy(&err, a.err, sizeof err, cudaMemcpyDeviceToHost));

@@ -479,6 +479,10 @@ __global__ void __launch_bounds__(256, 4) k_dark(Dev d) {
       a_prev = a;
       const float an = c2ray_species<STRICT, true>(H, 0.f, nelec_d, nelec_f, a, dt, last, &nh1_end);
       const float bn = c2ray_species<STRICT, true>(He, 0.f, nelec_d, nelec_f, bb, dt, last, &nhe1_end);
+      // An update is a function of (a, bb) alone (Gamma = 0). When it returns its own input, every
+      // later iteration repeats it bit for bit, so go straight to the last one (which also forms
+      // the end-of-step densities) -- the usual case of a neutral cell after one or two updates.
+      if (!last && an == a && bn == bb) it = I - 2;
       a = an;
       bb = bn;
       nelec_last = nelec_d;

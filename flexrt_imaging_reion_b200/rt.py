@@ -321,6 +321,11 @@ class RTContext:
             dl = dl[:self.nsrc_box[box]]
         return float(J.value), dl, dnh
 
+    def last_adjoint_ms(self) -> float:
+        v = C.c_float(0.0)
+        self._check(self.L.frt_last_adjoint_timing(self.h, C.byref(v)), "frt_last_adjoint_timing")
+        return float(v.value)
+
     def box_scalars(self, box: int = 0) -> Dict[str, float]:
         v = np.zeros(8)
         self._check(self.L.frt_box_scalars(self.h, box, v.ctypes.data), "frt_box_scalars")

@@ -210,6 +210,8 @@ typedef struct {
   int lo[3], hi[3];
 } frt_adj_objective;
 frt_status frt_adjoint(frt_ctx* ctx, const frt_adj_objective* obj, double* J, double* dL, float* dnH);
+/* Device time of the last frt_adjoint's kernels in ms (CUDA events on the context's stream). */
+frt_status frt_last_adjoint_timing(frt_ctx* ctx, float* ms);
 
 /* ---- field read-back without device allocation ---------------------------------------------
  * No counterpart in the reference (its fields live in host arrays). Gathers cells

@@ -3,8 +3,6 @@ objective, tangent-linear directional derivatives, and central finite difference
 (h = 1e-4 relative) of the oracle's FP64 objective on 64 random inputs (32 source luminosities,
 32 cell densities on the ray paths), to 1e-3 relative. Also: the context state is left as it was,
 the call is refused after a step, the torch.autograd harness, and the cost against one step."""
-import time
-
 import numpy as np
 import pytest
 import torch
@@ -90,14 +88,20 @@ def test_state_untouched_and_refused_after_step(setup):
     inp = setup["inp"]
     with rt.RTContext([inp], [SEED], ray_capacity=1 << 20) as ref:
         ref.setup()
-        ref.step()
+        st_ref = ref.step()
         g_ref = ref.get_field(0, "GAMMA_H1_TOT")
+        rays_ref = ref.rays(0)
     with rt.RTContext([inp], [SEED], ray_capacity=1 << 20) as c:
         c.setup()
         c.adjoint(LO, HI)
         c.adjoint(LO, HI)
-        c.step()
-        np.testing.assert_array_equal(c.get_field(0, "GAMMA_H1_TOT"), g_ref)
+        st = c.step()
+        # the ray tree is deterministic; Gamma sums are float atomics in any order (1e-6)
+        assert st["crossings"] == st_ref["crossings"] and st["rays_alive"] == st_ref["rays_alive"]
+        r = c.rays(0)
+        assert sorted(zip(r["ray_cell"].tolist(), r["ray_pixel"].tolist())) == \
+            sorted(zip(rays_ref["ray_cell"].tolist(), rays_ref["ray_pixel"].tolist()))
+        np.testing.assert_allclose(c.get_field(0, "GAMMA_H1_TOT"), g_ref, rtol=1e-5, atol=0)
         with pytest.raises(rt.FrtError, match="status 5"):
             c.adjoint(LO, HI)
 
@@ -126,13 +130,13 @@ def test_adjoint_cost_against_one_step(setup):
     with rt.RTContext([inp], [SEED], ray_capacity=1 << 20) as c:
         c.setup()
         c.adjoint(LO, HI, want_dl=False, want_dnh=False)   # buffers allocated on the first call
-        t0 = time.perf_counter()
+        t_adj = []
         for _ in range(5):
             c.adjoint(LO, HI, want_dl=False, want_dnh=False)
-        t_adj = (time.perf_counter() - t0) / 5
+            t_adj.append(c.last_adjoint_ms())
     with rt.RTContext([inp], [SEED], ray_capacity=1 << 20) as c:
         c.setup()
         c.step()
-        t_step = c.last_timing()[0] * 1e-3
-    # the target is <= 3x; the host-timed call carries launch and copy overheads on top
-    assert t_adj <= 6 * t_step, (t_adj, t_step)
+        t_step = c.last_timing()[0]
+    # device time of the adjoint's kernels against one forward step of the same box (target 3x)
+    assert np.median(t_adj) <= 3 * t_step, (t_adj, t_step)
