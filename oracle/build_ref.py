@@ -58,8 +58,9 @@ def user_inputs_values(spec: W.BoxSpec, ncpu: int, path_length: int = 8) -> dict
     }
 
 
-def stage(name: str, spec: W.BoxSpec, ncpu: int, path_length: int = 8) -> str:
-    """Copy + configure the reference sources into oracle/_ref/<name>."""
+def stage(name: str, spec: W.BoxSpec, ncpu: int, path_length: int = 8, restart: bool = False) -> str:
+    """Copy + configure the reference sources into oracle/_ref/<name>. A restart stage is built
+    with input_grid = TRUE and reads input_files/restart_{gas,rays,tre}.bin."""
     d = os.path.join(OUT, name)
     src = os.path.join(d, "src")
     os.makedirs(src, exist_ok=True)
@@ -68,11 +69,11 @@ def stage(name: str, spec: W.BoxSpec, ncpu: int, path_length: int = 8) -> str:
         shutil.copyfile(os.path.join(REF_SRC, f), os.path.join(src, f))
     for f in REF_DATA:
         shutil.copyfile(os.path.join(REF_SRC, f), os.path.join(d, f))
-    _configure(d, spec, ncpu, path_length)
+    _configure(d, spec, ncpu, path_length, restart)
     return d
 
 
-def _configure(d: str, spec: W.BoxSpec, ncpu: int, path_length: int) -> None:
+def _configure(d: str, spec: W.BoxSpec, ncpu: int, path_length: int, restart: bool = False) -> None:
     src = os.path.join(d, "src")
     # HEALPix includes -> project shim
     for f in ("ray_tracing.cc", "mem_funcs.cc"):
@@ -84,7 +85,10 @@ def _configure(d: str, spec: W.BoxSpec, ncpu: int, path_length: int) -> None:
     t = open(p).read()
     nu = ", ".join(f"{e}/h_eV" for e in W.NU_EV_5BIN)
     reps = [
-        (r"^int const input_grid\s*=.*$", "int const input_grid    = FALSE;"),
+        (r"^int const input_grid\s*=.*$", f"int const input_grid    = {'TRUE' if restart else 'FALSE'};"),
+        (r"^const char start_file_init\[\]\s*=.*$", 'const char start_file_init[]   = "./input_files/restart_gas.bin";'),
+        (r"^const char ray_file_init\[\]\s*=.*$", 'const char ray_file_init[]     = "./input_files/restart_rays.bin";'),
+        (r"^const char treion_file_init\[\]\s*=.*$", 'const char treion_file_init[]  = "./input_files/restart_tre.bin";'),
         (r"^bool const c2ray_iter\s*=.*$", "bool const c2ray_iter    = TRUE;"),
         (r"^bool const ifront\s*=.*$", "bool const ifront        = FALSE;"),
         (r"^bool const he2_tr_h2\s*=.*$", "bool const he2_tr_h2     = FALSE;"),
@@ -143,12 +147,13 @@ def compile_stage(d: str, ncpu: Optional[int] = None) -> str:
     return exe
 
 
-def build(name: str, spec: W.BoxSpec, ncpu: int = 1, path_length: int = 8, from_stage: bool = False) -> str:
+def build(name: str, spec: W.BoxSpec, ncpu: int = 1, path_length: int = 8, from_stage: bool = False,
+          restart: bool = False) -> str:
     d = os.path.join(OUT, name)
     if not from_stage:
         if not os.path.isdir(REF_SRC):
             raise RuntimeError("reference checkout not available; use from_stage=True")
-        stage(name, spec, ncpu, path_length)
+        stage(name, spec, ncpu, path_length, restart)
         return compile_stage(d)
     return compile_stage(d, ncpu)
 
@@ -163,8 +168,9 @@ def _unlimited_stack():
 
 
 def run(name: str, inp: W.BoxInputs, rundir: str, nsteps: int, seed: int, dump_every: int = 1,
-        threads: int = 1, timeout: Optional[float] = None) -> str:
-    """Run the compiled reference on inputs written to rundir; returns stdout."""
+        threads: int = 1, timeout: Optional[float] = None, restart_out: Optional[str] = None) -> str:
+    """Run the compiled reference on inputs written to rundir; returns stdout. With restart_out,
+    the reference's restart writers store gas.bin / rays.bin / tre.bin there after the last step."""
     d = os.path.join(OUT, name)
     W.write_reference_inputs(inp, rundir)
     args = [os.path.join(d, "ref_driver"), os.path.abspath(rundir), str(nsteps), str(seed), str(dump_every),
@@ -172,6 +178,8 @@ def run(name: str, inp: W.BoxInputs, rundir: str, nsteps: int, seed: int, dump_e
     if inp.clump is not None:
         args.append(os.path.join(os.path.abspath(rundir), "clump.bin"))
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    if restart_out:
+        env["FRT_RESTART_OUT"] = os.path.abspath(restart_out)
     r = subprocess.run(args, cwd=d, env=env, capture_output=True, text=True, timeout=timeout,
                        preexec_fn=_unlimited_stack)
     if r.returncode != 0:

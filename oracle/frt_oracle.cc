@@ -156,6 +156,7 @@ struct Ctx {
   std::vector<Ray> rays;
   long last_crossings, last_moved;
   int step;
+  unsigned seed;
 };
 
 static inline long cidx(const Ctx& c, int i, int j, int k) { return ((long)i * c.N + j) * c.N + k; }
@@ -835,6 +836,7 @@ void* orc_create(const Params* p, const float* delta1, int nsrc, const int32_t* 
     c->sigHe1[nu] = sig_He1(c->nu[nu]);
   }
   srand(p->seed);
+  c->seed = p->seed;
   alloc(*c);
   const long n3 = (long)c->N * c->N * c->N;
   // first-snapshot set-up at a = 1/(1+z) (gas_funcs.cc:595-613, io_funcs.cc:33-62)
@@ -1037,6 +1039,188 @@ int orc_dump(void* h, const char* path) {
 }
 
 void orc_destroy(void* h) { delete (Ctx*)h; }
+
+}  // extern "C"
+
+// ---- restart files in the reference's formats -------------------------------------------------
+// write_gas_binary (io_funcs.cc:358-393), write_rays_binary (274-303), write_treion (338-355):
+// fields written one after another with ofstream::write, so the records are packed. In plain mode
+// fion = 1 and tcross = 0 everywhere (rt_funcs.cc:49-58) and neutral_flag keeps its initial TRUE
+// (it only changes in the sub-grid branch, ray_tracing.cc:1010).
+namespace {
+
+struct ByteOut {
+  unsigned char* p;
+  size_t n, cap;
+  template <typename T> void put(const T& v) {
+    if (p && n + sizeof(T) <= cap) memcpy(p + n, &v, sizeof(T));
+    n += sizeof(T);
+  }
+};
+
+struct ByteIn {
+  const unsigned char* p;
+  size_t n, size;
+  bool ok = true;
+  template <typename T> T get() {
+    T v{};
+    if (n + sizeof(T) <= size) memcpy(&v, p + n, sizeof(T));
+    else ok = false;
+    n += sizeof(T);
+    return v;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+size_t orc_write_gas(void* h, void* buf, size_t cap) {
+  Ctx& c = *(Ctx*)h;
+  ByteOut o{(unsigned char*)buf, 0, cap};
+  const long n3 = (long)c.N * c.N * c.N;
+  o.put<float>(c.t);
+  for (long q = 0; q < n3; q++) {
+    o.put<float>(c.rho[q]); o.put<float>(c.temp[q]); o.put<float>(c.nH1[q]); o.put<float>(c.f_H1[q]);
+    o.put<float>(c.f_He1[q]); o.put<float>(c.f_H2[q]); o.put<float>(c.f_He2[q]); o.put<float>(c.f_He3[q]);
+    o.put<float>(c.gamma_H1_tot[q]); o.put<float>(c.gamma_He1_tot[q]); o.put<float>(c.mfp[q]);
+    o.put<float>(c.mfp_912[q]); o.put<float>(c.heat_rate[q]); o.put<float>(c.cool_rate[q]); o.put<float>(c.avg_nh1[q]);
+    o.put<float>(1.f);              // fion
+    o.put<float>(0.f);              // tcross
+    o.put<float>(c.treion_out[q]);
+    for (int nu = 0; nu < c.F; nu++) o.put<float>(c.ngam_nu[q * c.F + nu]);
+  }
+  return o.n;
+}
+
+size_t orc_write_rays(void* h, void* buf, size_t cap) {
+  Ctx& c = *(Ctx*)h;
+  ByteOut o{(unsigned char*)buf, 0, cap};
+  long x = 0;
+  for (const Ray& R : c.rays) {
+    if (!R.alive) continue;
+    o.put<long>(x++);
+    o.put<bool>(R.active);
+    o.put<short>(R.order);
+    o.put<int>(R.pixel);
+    o.put<unsigned short>(R.itheta);
+    o.put<float>(R.xhat); o.put<float>(R.yhat); o.put<float>(R.zhat);
+    for (int nu = 0; nu < c.F; nu++) o.put<float>(R.nphot[nu]);
+    o.put<float>(R.r); o.put<float>(R.dr); o.put<float>(R.x); o.put<float>(R.y); o.put<float>(R.z); o.put<float>(R.time);
+    o.put<int>(R.pind[0]);
+  }
+  o.put<long>(-1);
+  return o.n;
+}
+
+size_t orc_write_treion(void* h, void* buf, size_t cap) {
+  Ctx& c = *(Ctx*)h;
+  ByteOut o{(unsigned char*)buf, 0, cap};
+  const long n3 = (long)c.N * c.N * c.N;
+  for (long q = 0; q < n3; q++) {
+    o.put<float>(c.treion[q]);
+    o.put<bool>(c.treion_flag[q] != 0);
+    o.put<bool>(false);   // tcross_flag
+    o.put<bool>(true);    // neutral_flag
+  }
+  return o.n;
+}
+
+// Restart from the three files: read_grid_binary + read_treion (io_funcs.cc:65-116) and init()
+// with input_grid = TRUE (init_funcs.cc:10-19, 62-138), then init_rt's restart branch: ray_dt = 0
+// at the sources, read_rays_binary (rt_funcs.cc:95-107, io_funcs.cc:119-146), and the free-slot
+// probe of rt_funcs.cc:117-124: select_index(0) hands out slot 0 and a ray there whose first-bin
+// photon count is 0 is removed (for one processor: the record with slot number 0). The restarted
+// run draws from a fresh srand(seed) (no set-up cast precedes it). Replaces the set-up state of a
+// box made by orc_create (same grid, sources and seed). Returns 0 on success.
+int orc_read_restart(void* h, const void* gas, size_t gas_size, const void* tre, size_t tre_size, const void* rays,
+                     size_t ray_size) {
+  Ctx& c = *(Ctx*)h;
+  const long n3 = (long)c.N * c.N * c.N;
+  std::vector<float> fion(n3);
+  {
+    ByteIn in{(const unsigned char*)gas, 0, gas_size};
+    c.t = in.get<float>();
+    for (long q = 0; q < n3; q++) {
+      c.rho[q] = in.get<float>(); c.temp[q] = in.get<float>(); c.nH1[q] = in.get<float>(); c.f_H1[q] = in.get<float>();
+      c.f_He1[q] = in.get<float>(); c.f_H2[q] = in.get<float>(); c.f_He2[q] = in.get<float>();
+      c.f_He3[q] = in.get<float>(); c.gamma_H1_tot[q] = in.get<float>(); c.gamma_He1_tot[q] = in.get<float>();
+      c.mfp[q] = in.get<float>(); c.mfp_912[q] = in.get<float>(); c.heat_rate[q] = in.get<float>();
+      c.cool_rate[q] = in.get<float>(); c.avg_nh1[q] = in.get<float>(); fion[q] = in.get<float>();
+      (void)in.get<float>();   // tcross
+      c.treion_out[q] = in.get<float>();
+      for (int nu = 0; nu < c.F; nu++) c.ngam_nu[q * c.F + nu] = in.get<float>();
+    }
+    if (!in.ok || in.n != gas_size) return 1;
+  }
+  {
+    ByteIn in{(const unsigned char*)tre, 0, tre_size};
+    for (long q = 0; q < n3; q++) {
+      c.treion[q] = in.get<float>();
+      c.treion_flag[q] = in.get<bool>() ? 1 : 0;
+      (void)in.get<bool>();
+      (void)in.get<bool>();
+    }
+    if (!in.ok || in.n != tre_size) return 2;
+  }
+  for (long q = 0; q < n3; q++) {
+    c.nH[q] = (1. - O_Y) * c.rho[q] / O_MH;
+    c.nHe[q] = O_Y * c.rho[q] / (4. * O_MH);
+    if (fion[q] > 0.) {
+      c.nH2[q] = c.f_H2[q] * c.nH[q] / fion[q];
+      c.nHe2[q] = c.f_He2[q] * c.nHe[q] / fion[q];
+      c.nHe3[q] = c.f_He3[q] * c.nHe[q] / fion[q];
+    } else {
+      c.nH2[q] = c.nH[q] * (1. - c.fH1_0);
+      c.nHe2[q] = c.nHe[q] * (1. - c.fHe1_0);
+      c.nHe3[q] = 0.;
+    }
+    c.nH1[q] = c.nH[q] - c.nH2[q];
+    c.avg_nh1[q] = c.nH1[q];
+    c.nHe1[q] = c.nHe[q] - c.nHe2[q] - c.nHe3[q];
+    c.avg_nhe1[q] = c.nHe1[q];
+    c.ne[q] = c.nH2[q] + c.nHe2[q] + 2. * c.nHe3[q];
+    c.n_tot[q] = c.nH[q] + c.nHe[q] + c.ne[q];
+    c.IF_speed[q] = 0.;
+    c.Inc_Flux[q] = 0.;
+    c.nH1_prev[q] = c.nH1[q];
+    c.recomb_H2[q] = alphaB_H2(c.temp[q]);
+    c.recomb_He2[q] = alphaB_He2(c.temp[q]);
+    c.recomb_He3[q] = alphaB_He3(c.temp[q]);
+    c.avg_gamma[q] = c.gamma_H1_tot[q];
+    c.avg_gamma_he1[q] = c.gamma_He1_tot[q];
+    float dnH2_dt = c.gamma_H1_tot[q] * c.nH1[q] - c.recomb_H2[q] * c.ne[q] * c.nH2[q];
+    float dnHe2_dt = c.nHe1[q] * c.gamma_He1_tot[q] - c.recomb_He2[q] * c.ne[q] * c.nHe2[q] +
+                     c.recomb_He3[q] * c.ne[q] * c.nHe3[q] - c.nHe2[q] * 0.f;
+    float dnHe3_dt = c.nHe2[q] * 0.f - c.recomb_He3[q] * c.ne[q] * c.nHe3[q];
+    c.dne_dt[q] = dnH2_dt + dnHe2_dt + 2 * dnHe3_dt;
+  }
+  for (const Src& S : c.src) c.ray_dt[cidx(c, S.i, S.j, S.k)] = 0.f;
+  srand(c.seed);
+  c.rays.clear();
+  {
+    ByteIn in{(const unsigned char*)rays, 0, ray_size};
+    long x = in.get<long>();
+    while (in.ok && x != -1) {
+      Ray R;
+      memset(&R, 0, sizeof R);
+      R.alive = true;
+      R.active = in.get<bool>();
+      R.order = in.get<short>();
+      R.pixel = in.get<int>();
+      R.itheta = in.get<unsigned short>();
+      R.xhat = in.get<float>(); R.yhat = in.get<float>(); R.zhat = in.get<float>();
+      for (int nu = 0; nu < c.F; nu++) R.nphot[nu] = in.get<float>();
+      R.r = in.get<float>(); R.dr = in.get<float>(); R.x = in.get<float>(); R.y = in.get<float>();
+      R.z = in.get<float>(); R.time = in.get<float>();
+      R.pind[0] = in.get<int>();
+      if (in.ok && !(x == 0 && R.nphot[0] == 0.)) c.rays.push_back(R);
+      x = in.get<long>();
+    }
+    if (!in.ok) return 3;
+  }
+  return 0;
+}
 
 }  // extern "C"
 

@@ -71,6 +71,11 @@ def lib():
         _lib.orc_pix2vec.argtypes = [C.c_int, C.c_int, C.c_void_p]
         _lib.orc_vec2pix.argtypes = [C.c_int, C.c_void_p]
         _lib.orc_vec2pix.restype = C.c_int
+        for fn in ("orc_write_gas", "orc_write_rays", "orc_write_treion"):
+            getattr(_lib, fn).restype = C.c_size_t
+            getattr(_lib, fn).argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+        _lib.orc_read_restart.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
+                                          C.c_size_t]
         _lib.orc_adj_objective.restype = C.c_double
         _lib.orc_adj_objective.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_long)]
@@ -144,6 +149,22 @@ class Oracle:
         J = self._lib.orc_adj_objective(self.h, lo.ctypes.data, hi.ctypes.data, ptr[0], ptr[1], ptr[2], ptr[3],
                                         C.byref(jvp), C.byref(nlit))
         return float(J), float(jvp.value), int(nlit.value)
+
+    def _write(self, fn) -> bytes:
+        f = getattr(self._lib, fn)
+        n = f(self.h, None, 0)
+        buf = (C.c_ubyte * n)()
+        f(self.h, buf, n)
+        return bytes(buf)
+
+    def write_restart(self):
+        """(gas, rays, treion) restart records in the reference's formats (frt_oracle.cc)."""
+        return self._write("orc_write_gas"), self._write("orc_write_rays"), self._write("orc_write_treion")
+
+    def read_restart(self, gas: bytes, treion: bytes, rays: bytes) -> None:
+        st = self._lib.orc_read_restart(self.h, gas, len(gas), treion, len(treion), rays, len(rays))
+        if st != 0:
+            raise ValueError(f"orc_read_restart: malformed record set ({st})")
 
     def dump(self, path: str) -> None:
         if self._lib.orc_dump(self.h, path.encode()) != 0:

@@ -10,7 +10,12 @@
 //   * optional per-cell clumping field written over clump[] after set_clump() each step;
 //   * optional removal of rays with comoving r > rkill after update_rays;
 //   * update_cosmo_expansion / update_hydro_step / write_otf are not called (fixed redshift);
-//   * state dumps (FRTD files) and per-step timings.
+//   * state dumps (FRTD files) and per-step timings;
+//   * with FRT_RESTART_OUT=<dir> in the environment, the reference's own restart writers
+//     (write_gas_binary, write_rays_binary, write_treion) run after the last step;
+//   * in a stage built with input_grid = TRUE the set-up is the reference's restart path: the
+//     grid is sized as init() would (init_funcs.cc:22-30), the catalogue is read, init() reads the
+//     gas and treion restart files, init_rt() reads the ray file, and no rays are cast.
 // Usage: ref_driver <input_dir> <nsteps> <seed> <dump_every> <rkill_cm> [clump.bin]
 //   input_dir holds density.bin (float32 N^3, 1+delta), catalog.bin (5 doubles per source),
 //   numhalos.bin (int64) and receives dump_XXXX.frtd files. cwd must contain input_files/.
@@ -114,11 +119,17 @@ int main(int argc, char** argv) {
   Lx = Lx0 * a_snap;
   Ly = Ly0 * a_snap;
   Lz = Lz0 * a_snap;
-  get_ugas((dir + "/density.bin").c_str());
-  for (int i = 0; i < Nx; i++)
-    for (int j = 0; j < Ny; j++)
-      for (int k = 0; k < Nz; k++) rho[i][j][k] *= pow(a_snap, -3.);
-  avg_rho *= pow(a_snap, -3.);
+  if (input_grid == TRUE) {
+    for (int i = 0; i < Nx; i++) dx[i] = Lx / Nx * kpc_to_cm;
+    for (int j = 0; j < Ny; j++) dy[j] = Ly / Ny * kpc_to_cm;
+    for (int k = 0; k < Nz; k++) dz[k] = Lz / Nz * kpc_to_cm;
+  } else {
+    get_ugas((dir + "/density.bin").c_str());
+    for (int i = 0; i < Nx; i++)
+      for (int j = 0; j < Ny; j++)
+        for (int k = 0; k < Nz; k++) rho[i][j][k] *= pow(a_snap, -3.);
+    avg_rho *= pow(a_snap, -3.);
+  }
   read_source_catalog((dir + "/catalog.bin").c_str(), (dir + "/numhalos.bin").c_str());
   get_random_angles();
   init();
@@ -128,7 +139,7 @@ int main(int argc, char** argv) {
   init_rt();
   set_ray_per_cell();
   set_lsource();
-  new_rays();
+  if (input_grid == FALSE) new_rays();
   if (have_clump) memcpy(&clump[0][0][0], &clump_in[0][0][0], sizeof(clump));
   get_nphot_min_max();
   const double t_setup = omp_get_wtime() - t_setup0;
@@ -190,5 +201,11 @@ int main(int argc, char** argv) {
     }
   }
   printf("TOTAL %.6f s for %d steps\n", tot, nsteps);
+  if (const char* rdir = getenv("FRT_RESTART_OUT")) {
+    const std::string r = rdir;
+    write_gas_binary((r + "/gas.bin").c_str());
+    write_rays_binary((r + "/rays.bin").c_str());
+    write_treion((r + "/tre.bin").c_str());
+  }
   return 0;
 }

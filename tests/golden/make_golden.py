@@ -5,7 +5,10 @@ by the reference's C++ RT code compiled for one thread (oracle/build_ref.py; nee
 checkout, so this runs in the development container, not on the GPU box). The committed .npz
 files pin the CPU restatement in oracle/frt_oracle.cc and, through it, the CUDA path.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [names]
+
+T16R holds the reference's restart files (write_gas_binary / write_rays_binary / write_treion
+after 3 steps of T16) and the states of the reference's own restart path run from them.
 """
 from __future__ import annotations
 
@@ -53,7 +56,58 @@ def make(name, spec, seed, keep):
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), seed=seed, steps=np.array(keep), **out)
 
 
+def compact_ray_slots(raw: bytes, nfreq: int = 5) -> bytes:
+    """The same ray records with slot numbers 0..n-1 (the reference's reader takes any slot; with
+    no holes, rays cast after the restart take the slots after the loaded ones, so the slot order
+    stays the creation order the oracle keeps)."""
+    rec = 8 + 1 + 2 + 4 + 2 + 12 + 4 * nfreq + 24 + 4
+    out = bytearray()
+    pos, x = 0, 0
+    while True:
+        slot = int(np.frombuffer(raw[pos:pos + 8], np.int64)[0])
+        if slot == -1:
+            break
+        out += np.int64(x).tobytes() + raw[pos + 8:pos + rec]
+        pos += rec
+        x += 1
+    out += np.int64(-1).tobytes()
+    return bytes(out)
+
+
+def make_restart(name="T16R", base=("T16", W.config_tiny(), 11), steps_before=3, steps_after=2, seed=21):
+    """The reference's restart files after `steps_before` steps of a fresh run (its own writers),
+    and the states of a run of the reference's restart path (input_grid = TRUE) from them."""
+    bname, spec, bseed = base
+    B.build(bname, spec, ncpu=1)
+    B.build(name, spec, ncpu=1, restart=True)
+    inp = W.make_inputs(spec)
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        rs = os.path.join(td, "rs")
+        os.makedirs(rs)
+        B.run(bname, inp, os.path.join(td, "a"), steps_before, bseed, dump_every=0, restart_out=rs)
+        raw = {k: open(os.path.join(rs, f"{k}.bin"), "rb").read() for k in ("gas", "rays", "tre")}
+        comp = compact_ray_slots(raw["rays"])
+        d = os.path.join(B.OUT, name, "input_files")
+        for k, v in (("gas", raw["gas"]), ("rays", comp), ("tre", raw["tre"])):
+            open(os.path.join(d, f"restart_{k}.bin"), "wb").write(v)
+        B.run(name, inp, os.path.join(td, "b"), steps_after, seed, dump_every=1)
+        for s in range(1, steps_after + 1):
+            dd = frtd.read(os.path.join(td, "b", f"dump_{s:04d}.frtd"))
+            for k in FIELDS + RAYS + ["scalars"]:
+                out[f"s{s}_{k}"] = dd[k]
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), seed=seed, base_seed=bseed, steps_before=steps_before,
+                        steps=np.arange(1, steps_after + 1),
+                        gas=np.frombuffer(raw["gas"], np.uint8), rays=np.frombuffer(raw["rays"], np.uint8),
+                        rays_compact=np.frombuffer(comp, np.uint8), tre=np.frombuffer(raw["tre"], np.uint8), **out)
+
+
 if __name__ == "__main__":
+    only = sys.argv[1:]
     for case in CASES:
-        make(*case)
-        print("wrote", case[0])
+        if not only or case[0] in only:
+            make(*case)
+            print("wrote", case[0])
+    if not only or "T16R" in only:
+        make_restart()
+        print("wrote T16R")
