@@ -168,9 +168,12 @@ def _unlimited_stack():
 
 
 def run(name: str, inp: W.BoxInputs, rundir: str, nsteps: int, seed: int, dump_every: int = 1,
-        threads: int = 1, timeout: Optional[float] = None, restart_out: Optional[str] = None) -> str:
+        threads: int = 1, timeout: Optional[float] = None, restart_out: Optional[str] = None,
+        cosmo: bool = False) -> str:
     """Run the compiled reference on inputs written to rundir; returns stdout. With restart_out,
-    the reference's restart writers store gas.bin / rays.bin / tre.bin there after the last step."""
+    the reference's restart writers store gas.bin / rays.bin / tre.bin there after the last step;
+    with cosmo, the cosmological expansion runs after every step (its scale factors are logged as
+    'COSMO step a_current a_prev' lines)."""
     d = os.path.join(OUT, name)
     W.write_reference_inputs(inp, rundir)
     args = [os.path.join(d, "ref_driver"), os.path.abspath(rundir), str(nsteps), str(seed), str(dump_every),
@@ -180,6 +183,8 @@ def run(name: str, inp: W.BoxInputs, rundir: str, nsteps: int, seed: int, dump_e
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
     if restart_out:
         env["FRT_RESTART_OUT"] = os.path.abspath(restart_out)
+    if cosmo:
+        env["FRT_COSMO"] = "1"
     r = subprocess.run(args, cwd=d, env=env, capture_output=True, text=True, timeout=timeout,
                        preexec_fn=_unlimited_stack)
     if r.returncode != 0:

@@ -1042,6 +1042,44 @@ void orc_destroy(void* h) { delete (Ctx*)h; }
 
 }  // extern "C"
 
+// ---- cosmological expansion between steps (gas_funcs.cc:460-548) ------------------------------
+extern "C" void orc_cosmo_expansion(void* h, float a_current, float a_prev) {
+  Ctx& c = *(Ctx*)h;
+  const long n3 = (long)c.N * c.N * c.N;
+  c.Lx *= a_current / a_prev;
+  c.dxc *= a_current / a_prev;
+  const float fion = 1.f;   // plain mode (rt_funcs.cc:55)
+  for (long q = 0; q < n3; q++) {
+    c.rho[q] *= pow(a_prev / a_current, 3.);
+    c.nH[q] = (1. - O_Y) * c.rho[q] / O_MH;
+    c.nHe[q] = O_Y * c.rho[q] / (4. * O_MH);
+    c.nH2[q] = c.f_H2[q] * c.nH[q] / fion;
+    c.nHe2[q] = c.f_He2[q] * c.nHe[q] / fion;
+    c.nHe3[q] = c.f_He3[q] * c.nHe[q] / fion;
+    c.nH1[q] = c.nH[q] - c.nH2[q];
+    c.avg_nh1[q] = c.nH1[q];
+    c.nHe1[q] = c.nHe[q] - c.nHe2[q] - c.nHe3[q];
+    c.avg_nhe1[q] = c.nHe1[q];
+    c.ne[q] = c.nH2[q] + c.nHe2[q] + 2. * c.nHe3[q];
+    c.n_tot[q] = c.nH[q] + c.nHe[q] + c.ne[q];
+    c.nH1_prev[q] = c.nH1[q];
+  }
+  const float dxc = c.dxc;
+  for (Ray& R : c.rays) {
+    if (!R.alive) continue;
+    R.x *= a_current / a_prev;
+    R.y *= a_current / a_prev;
+    R.z *= a_current / a_prev;
+    if (R.x <= 0.) R.x = kMinDist * dxc;
+    if (R.x >= dxc * (1. - kMinDist / 2.)) R.x = dxc * (1. - kMinDist);
+    if (R.y <= 0.) R.y = kMinDist * dxc;
+    if (R.y >= dxc * (1. - kMinDist / 2.)) R.y = dxc * (1. - kMinDist);
+    if (R.z <= 0.) R.z = kMinDist * dxc;
+    if (R.z >= dxc * (1. - kMinDist / 2.)) R.z = dxc * (1. - kMinDist);
+  }
+  c.dt = c.tstep_factor * c.dxc / c.cl_factor / O_CL;   // update_dt (main.cc:237)
+}
+
 // ---- restart files in the reference's formats -------------------------------------------------
 // write_gas_binary (io_funcs.cc:358-393), write_rays_binary (274-303), write_treion (338-355):
 // fields written one after another with ofstream::write, so the records are packed. In plain mode

@@ -76,6 +76,7 @@ def lib():
             getattr(_lib, fn).argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
         _lib.orc_read_restart.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                                           C.c_size_t]
+        _lib.orc_cosmo_expansion.argtypes = [C.c_void_p, C.c_float, C.c_float]
         _lib.orc_adj_objective.restype = C.c_double
         _lib.orc_adj_objective.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_long)]
@@ -149,6 +150,10 @@ class Oracle:
         J = self._lib.orc_adj_objective(self.h, lo.ctypes.data, hi.ctypes.data, ptr[0], ptr[1], ptr[2], ptr[3],
                                         C.byref(jvp), C.byref(nlit))
         return float(J), float(jvp.value), int(nlit.value)
+
+    def cosmo_expansion(self, a_current: float, a_prev: float) -> None:
+        """update_cosmo_expansion with the given scale factors, then update_dt."""
+        self._lib.orc_cosmo_expansion(self.h, C.c_float(a_current), C.c_float(a_prev))
 
     def _write(self, fn) -> bytes:
         f = getattr(self._lib, fn)

@@ -13,6 +13,8 @@
 //   * state dumps (FRTD files) and per-step timings;
 //   * with FRT_RESTART_OUT=<dir> in the environment, the reference's own restart writers
 //     (write_gas_binary, write_rays_binary, write_treion) run after the last step;
+//   * with FRT_COSMO in the environment, update_cosmo_expansion (gas_funcs.cc:460-548) runs after
+//     new_rays as in main.cc:219-220, and the two scale factors it uses are logged (hex floats);
 //   * in a stage built with input_grid = TRUE the set-up is the reference's restart path: the
 //     grid is sized as init() would (init_funcs.cc:22-30), the catalogue is read, init() reads the
 //     gas and treion restart files, init_rt() reads the ray file, and no rays are cast.
@@ -112,6 +114,8 @@ int main(int argc, char** argv) {
   double t_setup0 = omp_get_wtime();
   init_lock();
   import_cosmic_time();
+  const bool cosmo = getenv("FRT_COSMO") != nullptr;
+  if (cosmo) make_scale_factor_table();
 
   // first-snapshot set-up (gas_funcs.cc:595-613) at a = 1/(1+zinit)
   zz = zinit;
@@ -186,6 +190,15 @@ int main(int argc, char** argv) {
     update_thermal();
     const double w5 = omp_get_wtime();
     new_rays();
+    if (cosmo) {
+      // the scale factors update_cosmo_expansion takes (gas_funcs.cc:461-465), for the record
+      float cosmic_time_current = t + cosmic_time(1. / (1. + zinit));
+      float cosmic_time_previous = t + cosmic_time(1. / (1. + zinit)) - dt;
+      float a_current = scale_factor(cosmic_time_current);
+      float a_prev = scale_factor(cosmic_time_previous);
+      printf("COSMO %d %a %a\n", s, a_current, a_prev);
+      update_cosmo_expansion();
+    }
     update_dt();
     balance_cpus();
     const double w6 = omp_get_wtime();

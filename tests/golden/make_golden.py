@@ -7,7 +7,8 @@ files pin the CPU restatement in oracle/frt_oracle.cc and, through it, the CUDA 
 
     python tests/golden/make_golden.py [names]
 
-T16R holds the reference's restart files (write_gas_binary / write_rays_binary / write_treion
+T16C holds a run with the reference's cosmological expansion after every step and the scale
+factors it used. T16R holds the reference's restart files (write_gas_binary / write_rays_binary / write_treion
 after 3 steps of T16) and the states of the reference's own restart path run from them.
 """
 from __future__ import annotations
@@ -102,6 +103,30 @@ def make_restart(name="T16R", base=("T16", W.config_tiny(), 11), steps_before=3,
                         rays_compact=np.frombuffer(comp, np.uint8), tre=np.frombuffer(raw["tre"], np.uint8), **out)
 
 
+def make_cosmo(name="T16C", base=("T16", W.config_tiny(), 11), steps=4):
+    """A fresh run with the cosmological expansion after every step (the reference's own
+    update_cosmo_expansion), its states and the scale factors each expansion used."""
+    bname, spec, seed = base
+    B.build(bname, spec, ncpu=1)
+    inp = W.make_inputs(spec)
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        log = B.run(bname, inp, td, steps, seed, dump_every=1, cosmo=True)
+        ac, ap = [], []
+        for line in log.splitlines():
+            if line.startswith("COSMO"):
+                _, s, a, b = line.split()
+                ac.append(float.fromhex(a))
+                ap.append(float.fromhex(b))
+        assert len(ac) == steps
+        for s in range(1, steps + 1):
+            dd = frtd.read(os.path.join(td, f"dump_{s:04d}.frtd"))
+            for k in FIELDS + RAYS + ["scalars"]:
+                out[f"s{s}_{k}"] = dd[k]
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), seed=seed, steps=np.arange(1, steps + 1),
+                        a_current=np.array(ac, np.float32), a_prev=np.array(ap, np.float32), **out)
+
+
 if __name__ == "__main__":
     only = sys.argv[1:]
     for case in CASES:
@@ -111,3 +136,6 @@ if __name__ == "__main__":
     if not only or "T16R" in only:
         make_restart()
         print("wrote T16R")
+    if not only or "T16C" in only:
+        make_cosmo()
+        print("wrote T16C")
