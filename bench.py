@@ -301,9 +301,9 @@ def run_adjoint(args):
 # ---- our arm ---------------------------------------------------------------------------------
 def launches_per_step(spec, ray_capacity, itercount=5, hpx_lvl=0):
     """Kernels one fused step launches: clear_lit, step_begin, advance, lit_compact, dark, lit_init,
-    itercount x (ray pass + lit pass), count, 3 merge set-up kernels (+4 binning kernels when the
-    pool can reach the merge threshold), compact, split, swap, cast."""
-    n = 1 + 1 + 1 + 1 + 1 + 1 + 2 * itercount + 1 + 3 + 3 + 1
+    seg_slots, itercount x (ray pass + lit pass), count, 3 merge set-up kernels (+4 binning kernels
+    when the pool can reach the merge threshold), compact, split, swap, cast."""
+    n = 1 + 1 + 1 + 1 + 1 + 1 + 1 + 2 * itercount + 1 + 3 + 3 + 1
     num_thresh = (spec.ray_per_cell_max - 12 * 4 ** hpx_lvl) * spec.n ** 3
     if num_thresh < ray_capacity:
         n += 4

@@ -31,7 +31,8 @@ EXPORTS = ["frt_create", "frt_destroy", "frt_last_error", "frt_rotation_table", 
            "frt_count_rays", "frt_merge", "frt_split_rays", "frt_update_thermal", "frt_new_rays", "frt_step",
            "frt_step_plain", "frt_last_stats", "frt_num_rays", "frt_download_rays", "frt_box_scalars",
            "frt_last_timing", "frt_seed_boxes", "frt_draw_cast", "frt_draw_step", "frt_get_sparse_field_noalloc", "frt_adjoint",
-           "frt_last_adjoint_timing"]
+           "frt_last_adjoint_timing", "frt_write_gas", "frt_write_rays", "frt_write_treion", "frt_read_gas",
+           "frt_read_treion", "frt_read_rays", "frt_update_cosmo_expansion"]
 NOALLOC_MAX_CELLS = 1 << 20
 
 
@@ -114,6 +115,13 @@ def lib() -> C.CDLL:
         "frt_get_sparse_field_noalloc": ([P, I, I, I, LL, LL, P], I),
         "frt_adjoint": ([P, C.POINTER(AdjObjective), P, P, P], I),
         "frt_last_adjoint_timing": ([P, P], I),
+        "frt_write_gas": ([P, I, P, C.c_size_t, C.POINTER(C.c_size_t)], I),
+        "frt_write_rays": ([P, I, P, C.c_size_t, C.POINTER(C.c_size_t)], I),
+        "frt_write_treion": ([P, I, P, C.c_size_t, C.POINTER(C.c_size_t)], I),
+        "frt_read_gas": ([P, I, P, C.c_size_t], I),
+        "frt_read_treion": ([P, I, P, C.c_size_t], I),
+        "frt_read_rays": ([P, I, P, C.c_size_t], I),
+        "frt_update_cosmo_expansion": ([P, P, P], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -26,6 +26,8 @@ struct frt_ctx {
   std::vector<std::vector<int>> src_cell;
   std::vector<std::vector<double>> src_lum;
   std::vector<char> gas_ready;
+  std::vector<char> restarted;           // gas read from a restart file (init_rt's restart branch)
+  std::vector<float> restart_t;          // its time
   std::vector<std::vector<float>> rho;  // host copy of the proper density (set-up output)
   std::vector<float> rot;
   // pinned staging
@@ -398,7 +400,7 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
     AL(P.xh, R); AL(P.yh, R); AL(P.zh, R); AL(P.nphot, R * d.F);
     AL(P.r, R); AL(P.dr, R); AL(P.x, R); AL(P.y, R); AL(P.z, R); AL(P.time, R);
   }
-  AL(d.seg, R * d.PL); AL(d.seg_dist, R * d.PL); AL(d.nseg, R); AL(d.dead, R);
+  AL(d.segs, R * d.PL); AL(d.nseg, R); AL(d.dead, R); AL(d.moved, R);
   AL(d.split_list, R / 4 + 1);
   // merge bins only when some box can reach its merge threshold with this pool size
   bool merge_reachable = false;
@@ -425,6 +427,8 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
   ctx->src_cell.resize(cfg->nbox);
   ctx->src_lum.resize(cfg->nbox);
   ctx->gas_ready.assign(cfg->nbox, 0);
+  ctx->restarted.assign(cfg->nbox, 0);
+  ctx->restart_t.assign(cfg->nbox, 0.f);
   ctx->rho.resize(cfg->nbox);
   {
     frt_status st = upload_boxes(ctx);
@@ -489,8 +493,10 @@ frt_status frt_init_gas(frt_ctx* ctx, int box, const float* delta1) {
     CK(up(d.rec_h2, rh));
     CK(up(d.rec_he2, rhe));
   }
+  if (d.rho) CK(up(d.rho, rho));
   ctx->rho[box] = rho;
   ctx->gas_ready[box] = 1;
+  ctx->restarted[box] = 0;
   return FRT_OK;
 }
 
@@ -605,6 +611,10 @@ frt_status frt_get_field(frt_ctx* ctx, int box, frt_field f, float* host) {
   CK(cudaStreamSynchronize(ctx->s_dark));
   switch (f) {
     case FRT_F_RHO:
+      if (d.rho) {   // moved to the device by a cosmological expansion
+        CK(get(d.rho, host));
+        return FRT_OK;
+      }
       if (ctx->rho[box].size() != n) return FRT_ERR_STATE;
       memcpy(host, ctx->rho[box].data(), sizeof(float) * n);
       return FRT_OK;
@@ -685,10 +695,12 @@ frt_status frt_init_rt(frt_ctx* ctx) {
       ctx->err = "frt_init_gas not called for every box";
       return FRT_ERR_STATE;
     }
-  // ray_dt of the source cells = dt (rt_funcs.cc:85-101, input_grid = FALSE)
+  // ray_dt of the source cells = dt (rt_funcs.cc:85-101, input_grid = FALSE); 0 for a box
+  // restarted from files (input_grid = TRUE)
   std::vector<float> rdt;
   for (size_t b = 0; b < ctx->boxes.size(); b++)
-    for (size_t s = 0; s < ctx->src_cell[b].size(); s++) rdt.push_back(ctx->src_lum[b][s] != 0 ? ctx->hbox[b].dt : 0.f);
+    for (size_t s = 0; s < ctx->src_cell[b].size(); s++)
+      rdt.push_back(ctx->src_lum[b][s] != 0 && !ctx->restarted[b] ? ctx->hbox[b].dt : 0.f);
   if (!rdt.empty()) CK(cudaMemcpy(d.src_ray_dt, rdt.data(), sizeof(float) * rdt.size(), cudaMemcpyHostToDevice));
   Ctl c;
   memset(&c, 0, sizeof(c));
@@ -696,11 +708,48 @@ frt_status frt_init_rt(frt_ctx* ctx) {
   CK(cudaMemset(d.lit_flag, 0, (size_t)d.ncell_total));
   launch_fill_i32(d.lit_slot, -1, d.ncell_total, ctx->s_main);
   CK(cudaStreamSynchronize(ctx->s_main));
-  for (auto& B : ctx->hbox) {
-    B.t = 0.f;
-    B.nphot_merge = 0.f;
+  for (size_t b = 0; b < ctx->hbox.size(); b++) {
+    ctx->hbox[b].t = ctx->restarted[b] ? ctx->restart_t[b] : 0.f;
+    ctx->hbox[b].nphot_merge = 0.f;
   }
+  ctx->rays_moved = false;
   return upload_boxes(ctx);
+}
+
+frt_status frt_update_cosmo_expansion(frt_ctx* ctx, const float* a_current, const float* a_prev) {
+  if (!ctx || !a_current || !a_prev) return FRT_ERR_INVALID;
+  Dev& d = ctx->d;
+  for (size_t b = 0; b < ctx->hbox.size(); b++)
+    if (!(a_current[b] > 0.f) || !(a_prev[b] > 0.f) || !ctx->gas_ready[b]) {
+      ctx->err = "frt_update_cosmo_expansion: scale factors must be positive and the gas set up";
+      return FRT_ERR_INVALID;
+    }
+  CK(cudaStreamSynchronize(ctx->s_main));
+  CK(cudaStreamSynchronize(ctx->s_dark));
+  if (!d.rho) {
+    frt_status st = dalloc(ctx, &d.rho, (size_t)d.ncell_total);
+    if (st) return st;
+    for (size_t b = 0; b < ctx->hbox.size(); b++)
+      CK(cudaMemcpy(d.rho + ctx->hbox[b].cell0, ctx->rho[b].data(), sizeof(float) * ctx->rho[b].size(),
+                    cudaMemcpyHostToDevice));
+    ctx->graph_valid = false;   // the graph keeps a copy of the device pointers
+  }
+  frt_status st = download_boxes(ctx);
+  if (st) return st;
+  std::vector<float> ratio(ctx->hbox.size());
+  std::vector<double> rf(ctx->hbox.size());
+  for (size_t b = 0; b < ctx->hbox.size(); b++) {
+    // gas_funcs.cc:472-485: dx[i] *= a_current/a_prev; rho *= pow(a_prev/a_current, 3.)
+    ratio[b] = a_current[b] / a_prev[b];
+    rf[b] = pow(a_prev[b] / a_current[b], 3.);
+    float dx = ctx->hbox[b].dx;
+    dx *= ratio[b];
+    host::set_cell_size(&ctx->hbox[b], &ctx->cfg, &ctx->boxes[b], dx);
+  }
+  if ((st = upload_boxes(ctx))) return st;
+  for (size_t b = 0; b < ctx->hbox.size(); b++)
+    launch_cosmo_expansion(d, (int)b, ratio[b], rf[b], ctx->grid_cells, ctx->s_main);
+  return sync_and_check(ctx);
 }
 
 frt_status frt_update_dt(frt_ctx* ctx, float* dt_out) {
@@ -967,6 +1016,284 @@ frt_status frt_last_timing(frt_ctx* ctx, float* step_ms, float* cell_kernel_ms) 
   if (!ctx) return FRT_ERR_INVALID;
   if (step_ms) *step_ms = ctx->last_step_ms;
   if (cell_kernel_ms) *cell_kernel_ms = ctx->last_dark_ms;
+  return FRT_OK;
+}
+
+}  // extern "C"
+
+// ---- restart files in the reference's formats ------------------------------------------------
+// write_gas_binary (io_funcs.cc:358-393): float t, then per cell 18 floats + nfreq floats;
+// write_rays_binary (274-303): packed records {int64 slot, bool active, int16 order, int32 pixel,
+// uint16 itheta, 3 floats direction, nfreq floats photons, r, dr, x, y, z, time, int32 cell}
+// ended by slot -1; write_treion (338-355): per cell float + 3 bools. In plain mode fion = 1,
+// tcross = 0, f_He3 = 0 and neutral_flag stays TRUE; every ray is active at a step boundary.
+namespace {
+
+struct Bytes {
+  unsigned char* p;
+  size_t n, cap;
+  template <typename T> void put(const T& v) {
+    if (p && n + sizeof(T) <= cap) memcpy(p + n, &v, sizeof(T));
+    n += sizeof(T);
+  }
+};
+
+size_t ray_record_size(int F) { return 8 + 1 + 2 + 4 + 2 + 12 + 4 * (size_t)F + 24 + 4; }
+
+}  // namespace
+
+extern "C" {
+
+frt_status frt_write_gas(frt_ctx* ctx, int box, void* buf, size_t cap, size_t* len) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  const size_t n = (size_t)ctx->hbox[box].ncell;
+  const int F = ctx->d.F;
+  const size_t need = 4 + n * (18 + (size_t)F) * 4;
+  if (len) *len = need;
+  if (!buf) return FRT_OK;
+  if (cap < need) {
+    ctx->err = "frt_write_gas: buffer too small";
+    return FRT_ERR_INVALID;
+  }
+  const frt_field ids[] = {FRT_F_RHO, FRT_F_TEMP, FRT_F_NH1, FRT_F_F_H1, FRT_F_F_HE1, FRT_F_F_H2, FRT_F_F_HE2,
+                           FRT_F_GAMMA_H1_TOT, FRT_F_GAMMA_HE1_TOT, FRT_F_HEAT_RATE, FRT_F_COOL_RATE, FRT_F_AVG_NH1,
+                           FRT_F_TREION};
+  std::vector<std::vector<float>> f(13, std::vector<float>(n));
+  for (int k = 0; k < 13; k++) {
+    st = frt_get_field(ctx, box, ids[k], f[k].data());
+    if (st) return st;
+  }
+  std::vector<float> mfp(n), mfp912(n), ngam((size_t)n * F, 0.f);
+  if (ctx->d.mfp) {
+    if ((st = frt_get_field(ctx, box, FRT_F_MFP, mfp.data()))) return st;
+    if ((st = frt_get_field(ctx, box, FRT_F_MFP_912, mfp912.data()))) return st;
+  } else {
+    // core outputs keep no mean free paths: from the final <n_HI> (the reference takes the
+    // iterate before the last C2Ray update, ray_tracing.cc:945)
+    for (size_t q = 0; q < n; q++) {
+      mfp[q] = (float)(1. / ctx->d.sigH1_0 / (double)f[11][q]);
+      mfp912[q] = (float)(1. / ctx->d.sigH1_912 / (double)f[11][q]);
+    }
+  }
+  if (ctx->d.per_bin && (st = frt_get_field(ctx, box, FRT_F_NGAM_NU, ngam.data()))) return st;
+  if ((st = download_boxes(ctx))) return st;
+  Bytes o{(unsigned char*)buf, 0, cap};
+  o.put<float>(ctx->hbox[box].t);
+  for (size_t q = 0; q < n; q++) {
+    for (int k = 0; k < 7; k++) o.put<float>(f[k][q]);      // rho temp nH1 f_H1 f_He1 f_H2 f_He2
+    o.put<float>(0.f);                                        // f_He3
+    o.put<float>(f[7][q]);
+    o.put<float>(f[8][q]);
+    o.put<float>(mfp[q]);
+    o.put<float>(mfp912[q]);
+    o.put<float>(f[9][q]);
+    o.put<float>(f[10][q]);
+    o.put<float>(f[11][q]);
+    o.put<float>(1.f);                                        // fion
+    o.put<float>(0.f);                                        // tcross
+    o.put<float>(f[12][q]);                                   // treion_out
+    for (int nu = 0; nu < F; nu++) o.put<float>(ngam[q * F + nu]);
+  }
+  return FRT_OK;
+}
+
+frt_status frt_write_treion(frt_ctx* ctx, int box, void* buf, size_t cap, size_t* len) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  const size_t n = (size_t)ctx->hbox[box].ncell;
+  const size_t need = n * 7;
+  if (len) *len = need;
+  if (!buf) return FRT_OK;
+  if (cap < need) {
+    ctx->err = "frt_write_treion: buffer too small";
+    return FRT_ERR_INVALID;
+  }
+  std::vector<float> tre(n), fl(n);
+  if ((st = frt_get_field(ctx, box, FRT_F_TREION, tre.data()))) return st;
+  if ((st = frt_get_field(ctx, box, FRT_F_TREION_FLAG, fl.data()))) return st;
+  Bytes o{(unsigned char*)buf, 0, cap};
+  for (size_t q = 0; q < n; q++) {
+    o.put<float>(tre[q]);
+    o.put<bool>(fl[q] != 0.f);
+    o.put<bool>(false);   // tcross_flag
+    o.put<bool>(true);    // neutral_flag
+  }
+  return FRT_OK;
+}
+
+frt_status frt_write_rays(frt_ctx* ctx, int box, void* buf, size_t cap, size_t* len) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  long long nr = 0;
+  if ((st = frt_num_rays(ctx, box, &nr))) return st;
+  const int F = ctx->d.F;
+  const size_t need = (size_t)nr * ray_record_size(F) + 8;
+  if (len) *len = need;
+  if (!buf) return FRT_OK;
+  if (cap < need) {
+    ctx->err = "frt_write_rays: buffer too small";
+    return FRT_ERR_INVALID;
+  }
+  std::vector<int16_t> ord(nr);
+  std::vector<int32_t> pix(nr), cell(nr);
+  std::vector<uint16_t> ith(nr);
+  std::vector<float> g((size_t)nr * 9), np((size_t)nr * F);
+  if ((st = frt_download_rays(ctx, box, ord.data(), pix.data(), ith.data(), cell.data(), g.data(), np.data())))
+    return st;
+  Bytes o{(unsigned char*)buf, 0, cap};
+  for (long long x = 0; x < nr; x++) {
+    const float* v = &g[(size_t)x * 9];
+    o.put<int64_t>(x);
+    o.put<bool>(true);
+    o.put<int16_t>(ord[x]);
+    o.put<int32_t>(pix[x]);
+    o.put<uint16_t>(ith[x]);
+    o.put<float>(v[0]); o.put<float>(v[1]); o.put<float>(v[2]);
+    for (int nu = 0; nu < F; nu++) o.put<float>(np[(size_t)x * F + nu]);
+    for (int k = 3; k < 9; k++) o.put<float>(v[k]);   // r dr x y z time
+    o.put<int32_t>(cell[x]);
+  }
+  o.put<int64_t>(-1);
+  return FRT_OK;
+}
+
+frt_status frt_read_gas(frt_ctx* ctx, int box, const void* buf, size_t len) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  const BoxP& B = ctx->hbox[box];
+  const size_t n = (size_t)B.ncell;
+  const int F = ctx->d.F;
+  if (!buf || len != 4 + n * (18 + (size_t)F) * 4) {
+    ctx->err = "frt_read_gas: record size does not match the box";
+    return FRT_ERR_INVALID;
+  }
+  float t0;
+  memcpy(&t0, buf, 4);
+  std::vector<float> rec(n * (18 + F));
+  memcpy(rec.data(), (const char*)buf + 4, rec.size() * 4);
+  std::vector<float> rho(n), nH(n), nHe(n), nH1(n), nHe1(n), fH1(n), fHe1(n), temp(n), ne(n), ntot(n), rh(n), rhe(n),
+      dne(n), heat(n), cool(n);
+  host::GasInit g{rho.data(), nH.data(), nHe.data(), nH1.data(), nHe1.data(), fH1.data(), fHe1.data(), temp.data(),
+                  ne.data(), ntot.data(), rh.data(), rhe.data(), dne.data()};
+  host::init_gas_restart(&ctx->cfg, &ctx->boxes[box], host::GasRestart{rec.data(), 18 + F}, &g, heat.data(),
+                         cool.data());
+  Dev& d = ctx->d;
+  const size_t o = (size_t)B.cell0;
+  auto up = [&](float* dst, const std::vector<float>& src) {
+    return cudaMemcpy(dst + o, src.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+  };
+  CK(up(d.nH, nH)); CK(up(d.nHe, nHe)); CK(up(d.nH1, nH1)); CK(up(d.nHe1, nHe1)); CK(up(d.f_H1, fH1));
+  CK(up(d.f_He1, fHe1)); CK(up(d.temp, temp)); CK(up(d.ne, ne)); CK(up(d.avg_nh1, nH1)); CK(up(d.avg_nhe1, nHe1));
+  CK(up(d.n_tot, ntot)); CK(up(d.dne_dt, dne)); CK(up(d.nH1_prev, nH1)); CK(up(d.heat, heat)); CK(up(d.cool, cool));
+  if (d.rec_h2) {
+    CK(up(d.rec_h2, rh));
+    CK(up(d.rec_he2, rhe));
+  }
+  if (d.rho) CK(up(d.rho, rho));
+  ctx->rho[box] = rho;
+  ctx->gas_ready[box] = 1;
+  ctx->restarted[box] = 1;
+  ctx->restart_t[box] = t0;
+  return FRT_OK;
+}
+
+frt_status frt_read_treion(frt_ctx* ctx, int box, const void* buf, size_t len) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  const BoxP& B = ctx->hbox[box];
+  const size_t n = (size_t)B.ncell;
+  if (!buf || len != n * 7) {
+    ctx->err = "frt_read_treion: record size does not match the box";
+    return FRT_ERR_INVALID;
+  }
+  std::vector<float> tre(n);
+  std::vector<uint8_t> fl(n);
+  const unsigned char* p = (const unsigned char*)buf;
+  for (size_t q = 0; q < n; q++) {
+    memcpy(&tre[q], p + q * 7, 4);
+    fl[q] = p[q * 7 + 4] ? 1 : 0;
+  }
+  Dev& d = ctx->d;
+  CK(cudaMemcpy(d.treion + B.cell0, tre.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d.treion_flag + B.cell0, fl.data(), n, cudaMemcpyHostToDevice));
+  return FRT_OK;
+}
+
+frt_status frt_read_rays(frt_ctx* ctx, int box, const void* buf, size_t len) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  if (!buf) return FRT_ERR_INVALID;
+  Dev& d = ctx->d;
+  const int F = d.F;
+  const size_t rs = ray_record_size(F);
+  const unsigned char* p = (const unsigned char*)buf;
+  std::vector<int32_t> cell, pix;
+  std::vector<int16_t> ord;
+  std::vector<uint16_t> ith, bx;
+  std::vector<float> g[9], np[FRT_MAX_FREQ];
+  size_t pos = 0;
+  while (true) {
+    if (pos + 8 > len) {
+      ctx->err = "frt_read_rays: record set not ended by slot -1";
+      return FRT_ERR_INVALID;
+    }
+    int64_t slot;
+    memcpy(&slot, p + pos, 8);
+    if (slot == -1) break;
+    if (pos + rs > len) {
+      ctx->err = "frt_read_rays: truncated record";
+      return FRT_ERR_INVALID;
+    }
+    const unsigned char* r = p + pos + 8;
+    int16_t o;
+    int32_t px, c;
+    uint16_t it;
+    float v[3 + FRT_MAX_FREQ + 6];
+    memcpy(&o, r + 1, 2);
+    memcpy(&px, r + 3, 4);
+    memcpy(&it, r + 7, 2);
+    memcpy(v, r + 9, sizeof(float) * (3 + F + 6));
+    memcpy(&c, r + 9 + 4 * (3 + F + 6), 4);
+    pos += rs;
+    // init_rt's free-slot probe (rt_funcs.cc:117-124): select_index(0) hands out slot 0, and a ray
+    // there whose first-bin photon count is 0 is removed
+    if (slot == 0 && v[3] == 0.f) continue;
+    if (c < 0 || c >= ctx->hbox[box].ncell || px < 0 || o < 0 || o > kLmax || it >= kNtheta) {
+      ctx->err = "frt_read_rays: ray outside the box or with an invalid order / pixel / angle index";
+      return FRT_ERR_INVALID;
+    }
+    cell.push_back(c); pix.push_back(px); ord.push_back(o); ith.push_back(it); bx.push_back((uint16_t)box);
+    for (int k = 0; k < 3; k++) g[k].push_back(v[k]);
+    for (int nu = 0; nu < F; nu++) np[nu].push_back(v[3 + nu]);
+    for (int k = 0; k < 6; k++) g[3 + k].push_back(v[3 + F + k]);
+  }
+  Ctl c;
+  CK(cudaStreamSynchronize(ctx->s_main));
+  CK(cudaMemcpy(&c, d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+  const size_t base = (size_t)c.nray[c.cur], m = cell.size();
+  if (base + m > (size_t)d.ray_cap) {
+    ctx->err = "frt_read_rays: ray pool capacity exceeded";
+    return FRT_ERR_CAPACITY;
+  }
+  double inflight = 0.0;
+  if (m) {
+    const RayPool& P = d.pool[c.cur];
+    CK(cudaMemcpy(P.cell + base, cell.data(), 4 * m, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P.pixel + base, pix.data(), 4 * m, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P.order + base, ord.data(), 2 * m, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P.itheta + base, ith.data(), 2 * m, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P.box + base, bx.data(), 2 * m, cudaMemcpyHostToDevice));
+    float* gp[9] = {P.xh, P.yh, P.zh, P.r, P.dr, P.x, P.y, P.z, P.time};
+    for (int k = 0; k < 9; k++) CK(cudaMemcpy(gp[k] + base, g[k].data(), 4 * m, cudaMemcpyHostToDevice));
+    for (int nu = 0; nu < F; nu++) {
+      CK(cudaMemcpy(P.nphot + (size_t)nu * d.ray_cap + base, np[nu].data(), 4 * m, cudaMemcpyHostToDevice));
+      for (float x : np[nu]) inflight += (double)x;
+    }
+  }
+  c.nray[c.cur] = (int)(base + m);
+  c.in_flight += inflight * 1e60;   // photon ledger: physical photons of the loaded rays
+  CK(cudaMemcpy(d.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice));
   return FRT_OK;
 }
 

@@ -102,6 +102,7 @@ __global__ void k_step_begin(Dev d) {
     // kernel ever reads an uninitialised record (the error stays latched for the host)
     if (c->err) c->nray[c->cur] = 0;
     c->rays_moved = c->crossings = c->split = c->merged = c->killed = c->cast = 0;
+    c->n_moved = 0;
     c->emitted = c->deposited = c->killed_ph = c->overlap = c->in_flight = 0.0;
   }
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < d.nbox; b += gridDim.x * blockDim.x) d.box[b].t += d.box[b].dt;
@@ -129,54 +130,70 @@ __global__ void __launch_bounds__(256, 4) k_advance(Dev d) {
   const int cap = d.ray_cap, PL = d.PL;
   long long cross = 0, moved = 0, killed = 0;
   double killed_ph = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    d.dead[i] = 0;
-    const BoxP& B = d.box[A.box[i]];
-    const int N = B.n;
-    const int ind = A.cell[i];
-    const int ii = ind / B.nn;
-    const int jj = (ind - ii * B.nn) / N;
-    const int kk = ind - ii * B.nn - jj * N;
-    const float xhat = A.xh[i], yhat = A.yh[i], zhat = A.zh[i];
-    float x0 = A.x[i], y0 = A.y[i], z0 = A.z[i];
-    const float deltat = A.time[i] + B.dt;
-    const float dist = B.clight * deltat;
-    if (!ray_moves(B, x0, y0, z0, xhat, yhat, zhat, dist)) {
-      A.time[i] = deltat;
-      d.nseg[i] = 0;
-      continue;
-    }
-    float r0 = A.r[i], dr = A.dr[i];
-    r0 += dist / B.scale;
-    dr -= dist / B.scale;
-    int in = ii, jn = jj, kn = kk;
-    const int ns = dda_walk(B, PL, xhat, yhat, zhat, deltat, x0, y0, z0, in, jn, kn,
-                            [&](int p, long long gc, float ds) {
-                              d.seg[(size_t)p * cap + i] = (int)gc;
-                              d.seg_dist[(size_t)p * cap + i] = ds;
-                              mark_lit(d, gc);
-                            });
-    if (ns < 0) {
-      atomicOr(&d.ctl->err, ERR_PATH);
-      d.nseg[i] = 0;
-      d.dead[i] = 1;
-      continue;
-    }
-    d.nseg[i] = (uint8_t)ns;
-    A.time[i] = 0.f;
-    A.r[i] = r0;
-    A.dr[i] = dr;
-    A.x[i] = x0;
-    A.y[i] = y0;
-    A.z[i] = z0;
-    A.cell[i] = in * B.nn + jn * N + kn;
-    cross += ns;
-    moved += 1;
-    // optional removal beyond rkill (comoving), applied after update_rays
-    if (B.rkill > 0.0 && (double)r0 > B.rkill) {
-      d.dead[i] = 1;
-      killed += 1;
-      killed_ph += (double)sum_nphot(A, i, d.F, cap) * kPhotNorm;
+  const int lane = threadIdx.x & 31;
+  for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+    const int i = i0 + threadIdx.x;
+    bool listed = false;
+    if (i < n) do {
+      d.dead[i] = 0;
+      const BoxP& B = d.box[A.box[i]];
+      const int N = B.n;
+      const int ind = A.cell[i];
+      const int ii = ind / B.nn;
+      const int jj = (ind - ii * B.nn) / N;
+      const int kk = ind - ii * B.nn - jj * N;
+      const float xhat = A.xh[i], yhat = A.yh[i], zhat = A.zh[i];
+      float x0 = A.x[i], y0 = A.y[i], z0 = A.z[i];
+      const float deltat = A.time[i] + B.dt;
+      const float dist = B.clight * deltat;
+      if (!ray_moves(B, x0, y0, z0, xhat, yhat, zhat, dist)) {
+        A.time[i] = deltat;
+        d.nseg[i] = 0;
+        break;
+      }
+      float r0 = A.r[i], dr = A.dr[i];
+      r0 += dist / B.scale;
+      dr -= dist / B.scale;
+      int in = ii, jn = jj, kn = kk;
+      int2* sp = d.segs + (size_t)i * PL;
+      const int ns = dda_walk(B, PL, xhat, yhat, zhat, deltat, x0, y0, z0, in, jn, kn,
+                              [&](int p, long long gc, float ds) {
+                                sp[p] = make_int2((int)gc, __float_as_int(ds));
+                                mark_lit(d, gc);
+                              });
+      if (ns < 0) {
+        atomicOr(&d.ctl->err, ERR_PATH);
+        d.nseg[i] = 0;
+        d.dead[i] = 1;
+        break;
+      }
+      d.nseg[i] = (uint8_t)ns;
+      A.time[i] = 0.f;
+      A.r[i] = r0;
+      A.dr[i] = dr;
+      A.x[i] = x0;
+      A.y[i] = y0;
+      A.z[i] = z0;
+      A.cell[i] = in * B.nn + jn * N + kn;
+      cross += ns;
+      moved += 1;
+      // optional removal beyond rkill (comoving), applied after update_rays
+      if (B.rkill > 0.0 && (double)r0 > B.rkill) {
+        d.dead[i] = 1;
+        killed += 1;
+        killed_ph += (double)sum_nphot(A, i, d.F, cap) * kPhotNorm;
+        break;
+      }
+      listed = true;
+    } while (0);
+    // warp-aggregated append of the moved rays to the list the ray passes work through
+    const unsigned m = __ballot_sync(0xffffffffu, listed);
+    if (m) {
+      const int leader = __ffs(m) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(&d.ctl->n_moved, __popc(m));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (listed) d.moved[base + __popc(m & ((1u << lane) - 1u))] = i;
     }
   }
   cross = block_sum(cross);
@@ -613,6 +630,64 @@ __global__ void k_cast(Dev d) {
   }
 }
 
+// update_cosmo_expansion (gas_funcs.cc:460-548) for one box, plain mode (fion = 1): the proper
+// density scales by (a_prev/a)^3 (rho_factor, computed on the host in double as the reference
+// does), the number densities follow from it and the stored ionised fractions (f_H2 = nH2/nH and
+// f_He2 = nHe2/nHe as the last C2Ray update left them, f_He3 = 0), and the rays' positions in their
+// cells scale by a/a_prev (ratio) with the corner nudges of the new cell size (already in the box).
+__global__ void k_cosmo_cells(Dev d, int box, double rho_factor) {
+  const BoxP& B = d.box[box];
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < B.ncell;
+       c += (long long)gridDim.x * blockDim.x) {
+    const long long q = B.cell0 + c;
+    const float nH0 = d.nH[q], nHe0 = d.nHe[q];
+    const float f_H2 = (nH0 - d.nH1[q]) / nH0;
+    const float f_He2 = (nHe0 - d.nHe1[q]) / nHe0;
+    float rho = d.rho[q];
+    rho *= rho_factor;
+    d.rho[q] = rho;
+    const float nH = (1. - kY) * rho / kMH;
+    const float nHe = kY * rho / (4. * kMH);
+    const float nH2 = f_H2 * nH / 1.0f;
+    const float nHe2 = f_He2 * nHe / 1.0f;
+    const float nH1 = nH - nH2;
+    const float nHe1 = nHe - nHe2;
+    const float ne = nH2 + nHe2;
+    d.nH[q] = nH;
+    d.nHe[q] = nHe;
+    d.nH1[q] = nH1;
+    d.nHe1[q] = nHe1;
+    d.avg_nh1[q] = nH1;
+    d.avg_nhe1[q] = nHe1;
+    d.ne[q] = ne;
+    d.n_tot[q] = nH + nHe + ne;
+    d.nH1_prev[q] = nH1;
+  }
+}
+
+__global__ void k_cosmo_rays(Dev d, int box, float ratio) {
+  const int cur = d.ctl->cur;
+  const int n = d.ctl->nray[cur];
+  const RayPool A = d.pool[cur];
+  const BoxP& B = d.box[box];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (A.box[i] != box) continue;
+    float x = A.x[i], y = A.y[i], z = A.z[i];
+    x *= ratio;
+    y *= ratio;
+    z *= ratio;
+    if (x <= 0.f) x = B.lo_edge;
+    if ((double)x >= B.hi_thr) x = B.hi_edge;
+    if (y <= 0.f) y = B.lo_edge;
+    if ((double)y >= B.hi_thr) y = B.hi_edge;
+    if (z <= 0.f) z = B.lo_edge;
+    if ((double)z >= B.hi_thr) z = B.hi_edge;
+    A.x[i] = x;
+    A.y[i] = y;
+    A.z[i] = z;
+  }
+}
+
 __global__ void k_fill_i32(int* p, int v, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     p[i] = v;
@@ -654,6 +729,11 @@ void launch_split_compact(const Dev& d, int grid, cudaStream_t s) {
 
 void launch_cast(const Dev& d, cudaStream_t s) {
   if (d.nsrc > 0) k_cast<<<grid_for(d.nsrc, 128, 4096), 128, 0, s>>>(d);
+}
+
+void launch_cosmo_expansion(const Dev& d, int box, float ratio, double rho_factor, int grid, cudaStream_t s) {
+  k_cosmo_cells<<<grid, 256, 0, s>>>(d, box, rho_factor);
+  k_cosmo_rays<<<grid, 256, 0, s>>>(d, box, ratio);
 }
 
 void launch_fill_i32(int* p, int v, long long n, cudaStream_t s) {

@@ -46,6 +46,10 @@ double alphaB_He2(double T) {
   double x = lam(T, 2.459e+1);
   return 1.26e-14 * pow(x, 0.750);
 }
+double alphaB_He3(double T) {   // rates.cc:161-165
+  double x = lam(T, 5.442e+1);
+  return 2 * 2.753e-14 * pow(x, 1.500) / pow((1.0 + pow((x / 2.740), 0.407)), 2.2420);
+}
 float hubble(float a) { return kHh * 100. / kMpcToKm * pow(kOmegaM / pow(a, 3.) + kOmegaL, 0.5); }
 }  // namespace
 
@@ -81,6 +85,24 @@ void rotation_table(float* out) {
       }
 }
 
+void set_cell_size(BoxP* B, const frt_config* cfg, const frt_box_desc* bd, float dx) {
+  B->dx = dx;
+  B->scale = dx / B->dx0;                                            // ray_tracing.cc:1262
+  B->dx_half = dx / 2.;                                              // ray_tracing.cc:308
+  B->lo_edge = kMinDist * dx;                                        // ray_tracing.cc:1366
+  B->hi_edge = dx * (1. - kMinDist);                                 // ray_tracing.cc:1370
+  B->hi_thr = dx * (1. - kMinDist / 2.);                             // ray_tracing.cc:1403
+  const float nc = B->nc;
+  B->mv_hi = nc * dx;                                                // ray_tracing.cc:1252
+  B->mv_lo = (1. - nc) * dx;                                         // ray_tracing.cc:1253
+  B->dt = cfg->tstep_factor * dx / bd->cl_factor / kCl;              // rt_funcs.cc:11
+  B->vol = ((double)dx) * ((double)dx) * ((double)dx);               // ray_tracing.cc:747
+  B->kdep = 1e60 / (double)B->dt / B->vol;
+  B->kdep_f = (float)B->kdep;
+  B->th.dt = B->dt;
+  B->th.dx = dx;
+}
+
 void box_params(BoxP* B, const frt_config* cfg, const frt_box_desc* bd, long long cell0) {
   const int n = bd->n;
   B->n = n;
@@ -92,23 +114,11 @@ void box_params(BoxP* B, const frt_config* cfg, const frt_box_desc* bd, long lon
   const float a_snap = (float)(1. / (1. + bd->zz));
   const float Lx = Lx0 * a_snap;                                     // gas_funcs.cc:595
   const float dx = Lx / n * kKpcToCm;                                // init_funcs.cc:23
-  B->dx = dx;
   B->dx0 = dx0;
-  B->scale = dx / dx0;                                               // ray_tracing.cc:1262
-  B->dx_half = dx / 2.;                                              // ray_tracing.cc:308
-  B->lo_edge = kMinDist * dx;                                        // ray_tracing.cc:1366
-  B->hi_edge = dx * (1. - kMinDist);                                 // ray_tracing.cc:1370
-  B->hi_thr = dx * (1. - kMinDist / 2.);                             // ray_tracing.cc:1403
-  const float nc = cfg->nl_const;                                    // rt_funcs.cc:138
-  B->nc = nc;
-  B->mv_hi = nc * dx;                                                // ray_tracing.cc:1252
-  B->mv_lo = (1. - nc) * dx;                                         // ray_tracing.cc:1253
+  B->nc = cfg->nl_const;                                             // rt_funcs.cc:138
   B->clight = bd->cl_factor * kCl;                                   // rt_funcs.cc:137
-  B->dt = cfg->tstep_factor * dx / bd->cl_factor / kCl;              // rt_funcs.cc:11
+  set_cell_size(B, cfg, bd, dx);
   B->t = 0.f;
-  B->vol = ((double)dx) * ((double)dx) * ((double)dx);               // ray_tracing.cc:747
-  B->kdep = 1e60 / (double)B->dt / B->vol;
-  B->kdep_f = (float)B->kdep;
   B->rkill = bd->rkill_cm;
   B->nphot_min = 0.;
   B->nphot_max = 0.;
@@ -186,6 +196,56 @@ void init_gas(const frt_config* cfg, const frt_box_desc* bd, const float* delta1
     const float dnHe3_dt = nHe2 * 0.f - 0.f * ne * nHe3;
     (void)fHe2_0;
     g->dne_dt[q] = dnH2_dt + dnHe2_dt + 2 * dnHe3_dt;
+  }
+}
+
+void init_gas_restart(const frt_config* cfg, const frt_box_desc* bd, const GasRestart& r, GasInit* g, float* heat,
+                      float* cool) {
+  const long long n3 = (long long)bd->n * bd->n * bd->n;
+  const float fH1_0 = cfg->fH1_0, fHe1_0 = cfg->fHe1_0;
+  for (long long q = 0; q < n3; q++) {
+    // read_grid_binary order (io_funcs.cc:87-108): rho temp nH1 f_H1 f_He1 f_H2 f_He2 f_He3
+    // gamma_H1_tot gamma_He1_tot mfp mfp_912 heat cool avg_nh1 fion tcross treion_out ngam_nu[]
+    const float* v = r.rec + (size_t)q * r.stride;
+    const float rho = v[0], temp = v[1], f_H1 = v[3], f_He1 = v[4], f_H2 = v[5], f_He2 = v[6], f_He3 = v[7];
+    const float g_h1 = v[8], g_he1 = v[9], fion = v[15];
+    g->rho[q] = rho;
+    // init() with input_grid = TRUE (init_funcs.cc:62-137)
+    const float nH = (1. - kY) * rho / kMH;
+    const float nHe = kY * rho / (4. * kMH);
+    float nH2, nHe2, nHe3;
+    if (fion > 0.) {
+      nH2 = f_H2 * nH / fion;
+      nHe2 = f_He2 * nHe / fion;
+      nHe3 = f_He3 * nHe / fion;
+    } else {
+      nH2 = nH * (1. - fH1_0);
+      nHe2 = nHe * (1. - fHe1_0);
+      nHe3 = 0.;
+    }
+    const float nH1 = nH - nH2;
+    const float nHe1 = nHe - nHe2 - nHe3;
+    const float ne = nH2 + nHe2 + 2. * nHe3;
+    g->nH[q] = nH;
+    g->nHe[q] = nHe;
+    g->nH1[q] = nH1;
+    g->nHe1[q] = nHe1;
+    g->f_H1[q] = f_H1;
+    g->f_He1[q] = f_He1;
+    g->temp[q] = temp;
+    g->ne[q] = ne;
+    g->n_tot[q] = nH + nHe + ne;
+    const float rec_h2 = alphaB_H2(temp);
+    const float rec_he2 = alphaB_He2(temp);
+    const float rec_he3 = alphaB_He3(temp);
+    g->rec_h2[q] = rec_h2;
+    g->rec_he2[q] = rec_he2;
+    const float dnH2_dt = g_h1 * nH1 - rec_h2 * ne * nH2;
+    const float dnHe2_dt = nHe1 * g_he1 - rec_he2 * ne * nHe2 + rec_he3 * ne * nHe3 - nHe2 * 0.f;
+    const float dnHe3_dt = nHe2 * 0.f - rec_he3 * ne * nHe3;
+    g->dne_dt[q] = dnH2_dt + dnHe2_dt + 2 * dnHe3_dt;
+    heat[q] = v[12];
+    cool[q] = v[13];
   }
 }
 

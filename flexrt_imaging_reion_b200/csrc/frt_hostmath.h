@@ -12,7 +12,18 @@ struct GasInit {  // caller-owned arrays of n^3 floats
 
 void rotation_table(float* out);  // kNtheta x 18 floats (forward, inverse)
 void box_params(BoxP* B, const frt_config* cfg, const frt_box_desc* bd, long long cell0);
+// The cell-size dependent members of a box (dx, the cell-edge thresholds, dt of update_dt, the
+// deposit normalisation): set up by box_params, and again after a cosmological expansion.
+void set_cell_size(BoxP* B, const frt_config* cfg, const frt_box_desc* bd, float dx);
 void init_gas(const frt_config* cfg, const frt_box_desc* bd, const float* delta1, GasInit* g);
+// The state init() derives on a restart (input_grid = TRUE) from a gas file's per-cell records of
+// 18 + nfreq floats (write_gas_binary order); heat and cool rates are taken from the records.
+struct GasRestart {
+  const float* rec;   // n^3 records
+  int stride;         // 18 + nfreq
+};
+void init_gas_restart(const frt_config* cfg, const frt_box_desc* bd, const GasRestart& r, GasInit* g, float* heat,
+                      float* cool);
 void nphot_min_max(const frt_config* cfg, const BoxP* B, int nsrc, const double* lum, double* nmin, double* nmax);
 void derived_constants(const frt_config* cfg, double* sigH1, double* sigHe1, double* sig0, double* sig912,
                        double* pi_sf_3, double* log4);

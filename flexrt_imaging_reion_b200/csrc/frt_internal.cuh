@@ -41,6 +41,8 @@ struct Ctl {
   unsigned err;
   int any_merge;           // some box has nphot_merge > 0
   int n_split;             // entries of the split list this step
+  int n_moved;             // entries of the moved-ray list this step
+  int pad2;
   long long rays_moved, crossings, split, merged, killed, cast;
   double emitted, deposited, killed_ph, overlap, in_flight;
 };
@@ -74,6 +76,7 @@ struct Dev {
   uint8_t *treion_flag, *lit_flag;
   int* lit_slot;
   float *nH1_prev, *n_tot, *dne_dt;                              // unfused path
+  float* rho;              // proper density, on the device once a cosmological expansion ran
   float *rec_h2, *rec_he2, *recrate_h2, *recrate_he2, *mfp, *mfp912, *if_speed, *inc_flux;  // diag
   // lit cells
   int* l_cell;
@@ -85,9 +88,9 @@ struct Dev {
   float cH1_f[FRT_MAX_FREQ], cHe1_f[FRT_MAX_FREQ];  // h (h_eV nu - Eth)/h_eV
   // rays
   RayPool pool[2];
-  int* seg;                // [PL][ray_cap]
-  float* seg_dist;         // [PL][ray_cap]
+  int2* segs;              // [ray_cap][PL] {cell (then lit slot), dist bits}: a ray's segments contiguous
   uint8_t* nseg;
+  int* moved;              // rays with segments this step (appended by k_advance)
   uint8_t* dead;
   int* ray_bin;            // merge bin of a candidate or -1
   uint8_t* merged_flag;
@@ -138,6 +141,7 @@ void launch_merge(const Dev& d, int grid, cudaStream_t s);
 void launch_split_compact(const Dev& d, int grid, cudaStream_t s);
 void launch_cast(const Dev& d, cudaStream_t s);
 void launch_fill_i32(int* p, int v, long long n, cudaStream_t s);
+void launch_cosmo_expansion(const Dev& d, int box, float ratio, double rho_factor, int grid, cudaStream_t s);
 // ---- launchers (frt_phys.cu) ----------------------------------------------------------
 void launch_lit_init(const Dev& d, bool strict, int grid, cudaStream_t s);
 void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t s);

@@ -105,207 +105,280 @@ __global__ void k_lit_init(Dev d) {
 }
 
 // ---- ray pass of one C2Ray iteration (ray_tracing.cc:701-938), plain mode ------------------
-// One thread per moved ray walks its stored segments, attenuates the photon count per bin with
-// the current time-averaged neutral densities of the lit cells, and deposits Gamma_HI / HeI.
-// FIRST converts the segment cell indices to lit slots; LAST also writes per-bin rates, the new
-// photon counts and removes rays below nphot_min.
-// NF > 0 fixes the number of frequency bins at compile time (the 5-bin spectrum of every
-// configuration here), so the per-bin loops unroll exactly; NF = 0 takes d.F at run time.
-template <bool STRICT, bool FIRST, bool LAST, int NF>
-__global__ void __launch_bounds__(256) k_raypass(Dev d) {
-  const int cur = d.ctl->cur;
-  const int n = d.ctl->nray[cur];
-  const RayPool A = d.pool[cur];
-  const int cap = d.ray_cap, F = d.F, L = d.lit_cap;
-  constexpr int MAXF = NF > 0 ? NF : FRT_MAX_FREQ;
-  const int Fr = NF > 0 ? NF : F;
+// The moved rays (the list k_advance builds) walk their stored segments, attenuate the photon
+// count per bin with the current time-averaged neutral densities of the lit cells, and deposit
+// Gamma_HI / HeI (the segments hold lit slots, k_seg_slots); LAST also writes the per-bin output
+// fields (diag), the new photon counts, and removes rays below nphot_min.
+
+// The segments' cell indices become lit slots once per step, before the first ray pass: one
+// thread per (moved ray, segment), a ray's segments being contiguous.
+__global__ void k_seg_slots(Dev d) {
+  const int nmv = min(d.ctl->n_moved, d.ray_cap);
+  const int PL = d.PL;
+  const long long total = (long long)nmv * PL;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(t / PL), p = (int)(t - (long long)q * PL);
+    const int i = d.moved[q];
+    if (p < d.nseg[i]) {
+      int2* sp = d.segs + (size_t)i * PL + p;
+      sp->x = d.lit_slot[sp->x];
+    }
+  }
+}
+
+// Strict precision: the reference's double expressions, one thread per moved ray.
+template <bool LAST>
+__global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
+  const int nmv = min(d.ctl->n_moved, d.ray_cap);
+  const RayPool A = d.pool[d.ctl->cur];
+  const int cap = d.ray_cap, F = d.F, L = d.lit_cap, PL = d.PL;
   double dep = 0.0, kil = 0.0, ovl = 0.0;
   long long nkill = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nmv; q += gridDim.x * blockDim.x) {
+    const int i = d.moved[q];
     const int ns = d.nseg[i];
-    if (ns == 0 || d.dead[i]) continue;
-    // The first pass turns every stored segment's cell index into its lit slot, before the walk:
-    // a walk may stop early (a dumped ray), but later iterations still read all segments.
-    if (FIRST)
-      for (int p = 0; p < ns; p++) {
-        int* sp = d.seg + (size_t)p * cap + i;
-        *sp = d.lit_slot[*sp];
-      }
+    const int2* sp = d.segs + (size_t)i * PL;
     const BoxP& B = d.box[A.box[i]];
     const double nmin = B.nphot_min;
     float nph[FRT_MAX_FREQ];
-#pragma unroll
-    for (int nu = 0; nu < FRT_MAX_FREQ; nu++) nph[nu] = (nu < Fr) ? A.nphot[(size_t)nu * cap + i] : 0.f;
+    for (int nu = 0; nu < F; nu++) nph[nu] = A.nphot[(size_t)nu * cap + i];
     bool dumped = false;
     unsigned dump_mask = 0;
-    if (STRICT) {
-      double tau_h1[FRT_MAX_FREQ], tau_he1[FRT_MAX_FREQ];
-#pragma unroll
-      for (int nu = 0; nu < FRT_MAX_FREQ; nu++) { tau_h1[nu] = 0.; tau_he1[nu] = 0.; }
-      const double dt = B.dt, vol = B.vol;
-      for (int p = 0; p < ns; p++) {
-        const int slot = d.seg[(size_t)p * cap + i];
-        if (slot < 0) continue;
-        const float dist = d.seg_dist[(size_t)p * cap + i];
-        const float a = d.l_avg_h[slot], b = d.l_avg_he[slot];
-        double dth[FRT_MAX_FREQ], dthe[FRT_MAX_FREQ], nin[FRT_MAX_FREQ];
-        double total = 0.;
-#pragma unroll
-        for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
-          if (nu >= F) continue;
-          dth[nu] = a * d.sigH1_d[nu] * dist;
-          dthe[nu] = b * d.sigHe1_d[nu] * dist;
-          nin[nu] = (nph[nu] * kPhotNorm) * exp(-tau_h1[nu] - tau_he1[nu]);
-          total += nin[nu] / kPhotNorm;
-        }
-        const bool dump = total < nmin;
-#pragma unroll
-        for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
-          if (nu >= F) continue;
-          double fh = 0., fhe = 0.;
-          if ((dth[nu] > 0.) || (dthe[nu] > 0.)) {
-            const double den = (1. - exp(-dth[nu])) * exp(-dthe[nu]) + (1. - exp(-dthe[nu])) * exp(-dth[nu]);
-            fh = (1. - exp(-dth[nu])) * exp(-dthe[nu]) / den;
-            fhe = (1. - exp(-dthe[nu])) * exp(-dth[nu]) / den;
-          }
-          const double absb = dump ? 1.0 : (1. - exp(-dth[nu] - dthe[nu]));
-          const float gh = (float)(fh * nin[nu] * absb / dt / vol / a);
-          const float ghe = (float)(fhe * nin[nu] * absb / dt / vol / b);
-          atomicAdd(&d.l_acc_g[slot], gh);
-          atomicAdd(&d.l_acc_ghe[slot], ghe);
-          if (LAST) {
-            atomicAdd(&d.l_ngam[(size_t)nu * L + slot], (float)(nin[nu] / kPhotNorm));
-            atomicAdd(&d.l_acc_nu_h[(size_t)nu * L + slot], gh);
-            atomicAdd(&d.l_acc_nu_he[(size_t)nu * L + slot], ghe);
-            dep += (fh + fhe) * nin[nu] * absb / kPhotNorm;
-            if (dump && (fh + fhe) > 0.) dump_mask |= 1u << nu;
-          }
-          tau_h1[nu] += dth[nu];
-          tau_he1[nu] += dthe[nu];
-        }
-        if (dump) { dumped = true; break; }
+    double tau_h1[FRT_MAX_FREQ], tau_he1[FRT_MAX_FREQ];
+    for (int nu = 0; nu < F; nu++) { tau_h1[nu] = 0.; tau_he1[nu] = 0.; }
+    const double dt = B.dt, vol = B.vol;
+    for (int p = 0; p < ns; p++) {
+      const int2 sg = sp[p];
+      const int slot = sg.x;
+      if (slot < 0) continue;
+      const float dist = __int_as_float(sg.y);
+      const float a = d.l_avg_h[slot], b = d.l_avg_he[slot];
+      double dth[FRT_MAX_FREQ], dthe[FRT_MAX_FREQ], nin[FRT_MAX_FREQ];
+      double total = 0.;
+      for (int nu = 0; nu < F; nu++) {
+        dth[nu] = a * d.sigH1_d[nu] * dist;
+        dthe[nu] = b * d.sigHe1_d[nu] * dist;
+        nin[nu] = (nph[nu] * kPhotNorm) * exp(-tau_h1[nu] - tau_he1[nu]);
+        total += nin[nu] / kPhotNorm;
       }
+      const bool dump = total < nmin;
+      for (int nu = 0; nu < F; nu++) {
+        double fh = 0., fhe = 0.;
+        if ((dth[nu] > 0.) || (dthe[nu] > 0.)) {
+          const double den = (1. - exp(-dth[nu])) * exp(-dthe[nu]) + (1. - exp(-dthe[nu])) * exp(-dth[nu]);
+          fh = (1. - exp(-dth[nu])) * exp(-dthe[nu]) / den;
+          fhe = (1. - exp(-dthe[nu])) * exp(-dth[nu]) / den;
+        }
+        const double absb = dump ? 1.0 : (1. - exp(-dth[nu] - dthe[nu]));
+        const float gh = (float)(fh * nin[nu] * absb / dt / vol / a);
+        const float ghe = (float)(fhe * nin[nu] * absb / dt / vol / b);
+        atomicAdd(&d.l_acc_g[slot], gh);
+        atomicAdd(&d.l_acc_ghe[slot], ghe);
+        if (LAST) {
+          atomicAdd(&d.l_ngam[(size_t)nu * L + slot], (float)(nin[nu] / kPhotNorm));
+          atomicAdd(&d.l_acc_nu_h[(size_t)nu * L + slot], gh);
+          atomicAdd(&d.l_acc_nu_he[(size_t)nu * L + slot], ghe);
+          dep += (fh + fhe) * nin[nu] * absb / kPhotNorm;
+          if (dump && (fh + fhe) > 0.) dump_mask |= 1u << nu;
+        }
+        tau_h1[nu] += dth[nu];
+        tau_he1[nu] += dthe[nu];
+      }
+      if (dump) { dumped = true; break; }
+    }
+    if (LAST) {
+      float s = 0.f;
+      for (int nu = 0; nu < F; nu++) {
+        nph[nu] = (float)((nph[nu] * kPhotNorm) * exp(-tau_h1[nu] - tau_he1[nu]) / kPhotNorm);
+        A.nphot[(size_t)nu * cap + i] = nph[nu];
+        s += nph[nu];
+      }
+      if (!(s > nmin)) {
+        d.dead[i] = 1;
+        nkill += 1;
+        kil += (double)s;
+        if (dumped)
+          for (int nu = 0; nu < F; nu++)
+            if (dump_mask & (1u << nu)) ovl += (double)nph[nu];
+      }
+    }
+  }
+  if (LAST) {
+    dep = block_sum(dep);
+    kil = block_sum(kil);
+    ovl = block_sum(ovl);
+    nkill = block_sum(nkill);
+    if (threadIdx.x == 0) {
+      if (dep != 0.0) atomicAdd(&d.ctl->deposited, dep * kPhotNorm);
+      if (kil != 0.0) atomicAdd(&d.ctl->killed_ph, kil * kPhotNorm);
+      if (ovl != 0.0) atomicAdd(&d.ctl->overlap, ovl * kPhotNorm);
+      if (nkill) atomicAdd((unsigned long long*)&d.ctl->killed, (unsigned long long)nkill);
+    }
+  }
+}
+
+// Mixed precision, persistent lanes. Rays have 1..path_length segments, so one ray per thread
+// leaves most lanes of a warp idle behind its longest ray. Here every warp owns a contiguous slice
+// of the moved list and a lane takes the slice's next ray as soon as its own ray ends (a ballot
+// and a warp-uniform cursor, no atomics), so every lane walks a segment in every loop trip; a
+// ray's segments are contiguous, so a lane's walk stays in one or two cache lines. Per bin the
+// photon count is carried from segment to segment by its transmission e^-dtau instead of
+// recomputing e^-tau, and each bin costs one transcendental when HeI does not absorb there
+// (sigma_HeI = 0 below 24.59 eV) and two when it does.
+// NF > 0 fixes the number of frequency bins at compile time (the 5-bin spectrum of every
+// configuration here), so the per-bin loops unroll exactly; NF = 0 takes d.F at run time.
+template <bool LAST, int NF>
+__global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
+  constexpr int MAXF = NF > 0 ? NF : FRT_MAX_FREQ;
+  const int Fr = NF > 0 ? NF : d.F;
+  const int nmv = min(d.ctl->n_moved, d.ray_cap);
+  const RayPool A = d.pool[d.ctl->cur];
+  const int cap = d.ray_cap, L = d.lit_cap, PL = d.PL;
+  const int lane = threadIdx.x & 31;
+  const unsigned lanes_below = (1u << lane) - 1u;
+  // this warp's slice [cursor, slice_end) of the moved list
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const long long per = (nmv + nwarps - 1) / nwarps;
+  long long cursor = wid * per;
+  const long long slice_end = min((long long)nmv, cursor + per);
+  double dep = 0.0, kil = 0.0, ovl = 0.0;
+  long long nkill = 0;
+  int i = -1, p = 0, ns = 0;
+  bool exhausted = false, dumped = false;
+  unsigned dump_mask = 0;
+  float nin[MAXF];
+  float kdep = 0.f;
+  double nmin = 0.0;
+  const int2* sp = nullptr;
+  while (true) {
+    // refill the lanes whose ray ended
+    const bool need = (i < 0) && !exhausted;
+    const unsigned m = __ballot_sync(0xffffffffu, need);
+    if (m) {
+      const long long q = cursor + __popc(m & lanes_below);
+      cursor += __popc(m);
+      if (need) {
+        if (q < slice_end) {
+          i = d.moved[q];
+          ns = d.nseg[i];
+          p = 0;
+          dumped = false;
+          dump_mask = 0;
+          sp = d.segs + (size_t)i * PL;
+          const BoxP& B = d.box[A.box[i]];
+          kdep = B.kdep_f;
+          nmin = B.nphot_min;
+#pragma unroll
+          for (int nu = 0; nu < MAXF; nu++) nin[nu] = (nu < Fr) ? A.nphot[(size_t)nu * cap + i] : 0.f;
+        } else {
+          exhausted = true;
+        }
+      }
+    }
+    if (__all_sync(0xffffffffu, i < 0)) break;
+    if (i < 0) continue;
+    // one segment of ray i
+    const int2 sg = sp[p];
+    const int slot = sg.x;
+    bool done = (p + 1 >= ns);
+    if (slot >= 0) {
+      const float dist = __int_as_float(sg.y);
+      const float a = d.l_avg_h[slot], b = d.l_avg_he[slot];
+      float total = 0.f;
+#pragma unroll
+      for (int nu = 0; nu < MAXF; nu++) total += (nu < Fr) ? nin[nu] : 0.f;
+      const bool dump = (double)total < nmin;
+      float gsum_h = 0.f, gsum_he = 0.f, hh = 0.f, hhe = 0.f;
+#pragma unroll
+      for (int nu = 0; nu < MAXF; nu++) {
+        if (nu >= Fr) continue;
+        const float dth = (a * d.sigH1_f[nu]) * dist;
+        const float dthe = (b * d.sigHe1_f[nu]) * dist;
+        float ah, eh;
+        absorb_transmit(dth, &ah, &eh);
+        float fh, fhe, absb, e;
+        if (dthe > 0.f) {
+          float ahe, ehe;
+          absorb_transmit(dthe, &ahe, &ehe);
+          e = eh * ehe;
+          absb = ah + eh * ahe;                   // 1 - e^-(dth+dthe) without cancellation
+          // frac_h1 = A e^-b / (A e^-b + B e^-a) (ray_tracing.cc:770-771)
+          const float x1 = ah * ehe, x2 = ahe * eh;
+          if (x1 + x2 > 1e-30f) {
+            const float inv = __fdividef(1.0f, x1 + x2);
+            fh = x1 * inv;
+            fhe = x2 * inv;
+          } else if (dth >= dthe) {                // both optical depths huge: ratio form
+            const float r = __fdividef(ahe, ah) * expf(dthe - dth);
+            fh = __fdividef(1.0f, 1.0f + r);
+            fhe = r * fh;
+          } else {
+            const float r = __fdividef(ah, ahe) * expf(dth - dthe);
+            fhe = __fdividef(1.0f, 1.0f + r);
+            fh = r * fhe;
+          }
+        } else {
+          e = eh;
+          absb = ah;
+          fh = (dth > 0.f) ? 1.0f : 0.0f;           // frac_h1 = 1, frac_he1 = 0 when dtau_he1 = 0
+          fhe = 0.f;
+        }
+        const float q = nin[nu] * (dump ? 1.0f : absb);
+        const float gh = fh * q, ghe = fhe * q;
+        gsum_h += gh;
+        gsum_he += ghe;
+        if (LAST) {
+          hh += gh * d.cH1_f[nu];
+          hhe += ghe * d.cHe1_f[nu];
+          if (d.per_bin) {   // per-bin rates and photon counts: output fields (diag outputs)
+            const float wh_ = __fdividef(kdep, a), whe_ = __fdividef(kdep, b);
+            atomicAdd(&d.l_ngam[(size_t)nu * L + slot], nin[nu]);
+            if (gh != 0.f) atomicAdd(&d.l_acc_nu_h[(size_t)nu * L + slot], gh * wh_);
+            if (ghe != 0.f) atomicAdd(&d.l_acc_nu_he[(size_t)nu * L + slot], ghe * whe_);
+          }
+          if (dump && (fh + fhe) > 0.f) dump_mask |= 1u << nu;
+        }
+        nin[nu] *= e;
+      }
+      const float wh = __fdividef(kdep, a), whe = __fdividef(kdep, b);
+      if (gsum_h != 0.f) atomicAdd(&d.l_acc_g[slot], gsum_h * wh);
+      if (gsum_he != 0.f) atomicAdd(&d.l_acc_ghe[slot], gsum_he * whe);
       if (LAST) {
-        float s = 0.f;
-        for (int nu = 0; nu < F; nu++) {
-          nph[nu] = (float)((nph[nu] * kPhotNorm) * exp(-tau_h1[nu] - tau_he1[nu]) / kPhotNorm);
-          A.nphot[(size_t)nu * cap + i] = nph[nu];
-          s += nph[nu];
-        }
-        if (!(s > nmin)) {
-          d.dead[i] = 1;
-          nkill += 1;
-          kil += (double)s;
-          if (dumped)
-            for (int nu = 0; nu < F; nu++)
-              if (dump_mask & (1u << nu)) ovl += (double)nph[nu];
-        }
+        // photo-heating weights sum_nu Gamma_nu h (h_eV nu - Eth)/h_eV (gas_funcs.cc:155-158)
+        if (hh != 0.f) atomicAdd(&d.l_heat_h[slot], hh * wh);
+        if (hhe != 0.f) atomicAdd(&d.l_heat_he[slot], hhe * whe);
+        dep += (double)gsum_h + (double)gsum_he;
       }
-    } else {
-      // Mixed precision: per bin the photon count is carried from segment to segment by its
-      // transmission e^-dtau instead of recomputing e^-tau, and each bin costs one transcendental
-      // when HeI does not absorb there (sigma_HeI = 0 below 24.59 eV) and two when it does.
-      float nin[MAXF];
-#pragma unroll
-      for (int nu = 0; nu < MAXF; nu++) nin[nu] = nph[nu];
-      const float kdep = B.kdep_f;
-      for (int p = 0; p < ns; p++) {
-        const int slot = d.seg[(size_t)p * cap + i];
-        if (slot < 0) continue;
-        const float dist = d.seg_dist[(size_t)p * cap + i];
-        const float a = d.l_avg_h[slot], b = d.l_avg_he[slot];
-        float total = 0.f;
-#pragma unroll
-        for (int nu = 0; nu < MAXF; nu++) total += (nu < Fr) ? nin[nu] : 0.f;
-        const bool dump = (double)total < nmin;
-        float gsum_h = 0.f, gsum_he = 0.f;
-        float gh_nu[MAXF], ghe_nu[MAXF], tr[MAXF];
+      if (dump) {
+        dumped = true;
+        done = true;
+      }
+    }
+    ++p;
+    if (done) {
+      if (LAST) {
+        // the photons leaving the last walked segment become the ray's count
+        // (ray_tracing.cc:923-935); below nphot_min the ray is removed
+        float s = 0.f;
 #pragma unroll
         for (int nu = 0; nu < MAXF; nu++) {
-          gh_nu[nu] = 0.f;
-          ghe_nu[nu] = 0.f;
-          tr[nu] = 1.f;
           if (nu >= Fr) continue;
-          const float dth = (a * d.sigH1_f[nu]) * dist;
-          const float dthe = (b * d.sigHe1_f[nu]) * dist;
-          float ah, eh;
-          absorb_transmit(dth, &ah, &eh);
-          float fh, fhe, absb, e;
-          if (dthe > 0.f) {
-            float ahe, ehe;
-            absorb_transmit(dthe, &ahe, &ehe);
-            e = eh * ehe;
-            absb = ah + eh * ahe;                   // 1 - e^-(dth+dthe) without cancellation
-            // frac_h1 = A e^-b / (A e^-b + B e^-a) (ray_tracing.cc:770-771)
-            const float x1 = ah * ehe, x2 = ahe * eh;
-            if (x1 + x2 > 1e-30f) {
-              const float inv = __fdividef(1.0f, x1 + x2);
-              fh = x1 * inv;
-              fhe = x2 * inv;
-            } else if (dth >= dthe) {                // both optical depths huge: ratio form
-              const float r = __fdividef(ahe, ah) * expf(dthe - dth);
-              fh = __fdividef(1.0f, 1.0f + r);
-              fhe = r * fh;
-            } else {
-              const float r = __fdividef(ah, ahe) * expf(dth - dthe);
-              fhe = __fdividef(1.0f, 1.0f + r);
-              fh = r * fhe;
-            }
-          } else {
-            e = eh;
-            absb = ah;
-            fh = (dth > 0.f) ? 1.0f : 0.0f;           // frac_h1 = 1, frac_he1 = 0 when dtau_he1 = 0
-            fhe = 0.f;
-          }
-          const float q = nin[nu] * (dump ? 1.0f : absb);
-          gh_nu[nu] = fh * q;
-          ghe_nu[nu] = fhe * q;
-          gsum_h += gh_nu[nu];
-          gsum_he += ghe_nu[nu];
-          tr[nu] = e;
-          if (LAST && dump && (fh + fhe) > 0.f) dump_mask |= 1u << nu;
-        }
-        const float wh = __fdividef(kdep, a), whe = __fdividef(kdep, b);
-        if (gsum_h != 0.f) atomicAdd(&d.l_acc_g[slot], gsum_h * wh);
-        if (gsum_he != 0.f) atomicAdd(&d.l_acc_ghe[slot], gsum_he * whe);
-        if (LAST) {
-          float hh = 0.f, hhe = 0.f;
-#pragma unroll
-          for (int nu = 0; nu < MAXF; nu++) {
-            if (nu >= Fr) continue;
-            if (d.per_bin) {   // per-bin rates and photon counts: output fields (diag outputs)
-              atomicAdd(&d.l_ngam[(size_t)nu * L + slot], nin[nu]);
-              if (gh_nu[nu] != 0.f) atomicAdd(&d.l_acc_nu_h[(size_t)nu * L + slot], gh_nu[nu] * wh);
-              if (ghe_nu[nu] != 0.f) atomicAdd(&d.l_acc_nu_he[(size_t)nu * L + slot], ghe_nu[nu] * whe);
-            }
-            hh += gh_nu[nu] * d.cH1_f[nu];
-            hhe += ghe_nu[nu] * d.cHe1_f[nu];
-          }
-          // photo-heating weights sum_nu Gamma_nu h (h_eV nu - Eth)/h_eV (gas_funcs.cc:155-158)
-          if (hh != 0.f) atomicAdd(&d.l_heat_h[slot], hh * wh);
-          if (hhe != 0.f) atomicAdd(&d.l_heat_he[slot], hhe * whe);
-          dep += (double)gsum_h + (double)gsum_he;
-        }
-#pragma unroll
-        for (int nu = 0; nu < MAXF; nu++) nin[nu] *= tr[nu];
-        if (dump) { dumped = true; break; }
-      }
-      if (LAST) {
-        float s = 0.f;
-        for (int nu = 0; nu < Fr; nu++) {
-          nph[nu] = nin[nu];
-          A.nphot[(size_t)nu * cap + i] = nph[nu];
-          s += nph[nu];
+          A.nphot[(size_t)nu * cap + i] = nin[nu];
+          s += nin[nu];
         }
         if (!((double)s > nmin)) {
           d.dead[i] = 1;
           nkill += 1;
           kil += (double)s;
           if (dumped)
-            for (int nu = 0; nu < Fr; nu++)
-              if (dump_mask & (1u << nu)) ovl += (double)nph[nu];
+#pragma unroll
+            for (int nu = 0; nu < MAXF; nu++)
+              if (nu < Fr && (dump_mask & (1u << nu))) ovl += (double)nin[nu];
         }
       }
+      i = -1;
     }
   }
   if (LAST) {
@@ -617,24 +690,20 @@ void launch_lit_init(const Dev& d, bool strict, int grid, cudaStream_t s) {
 }
 
 void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t s) {
-  const bool first = iter == 0, last = iter == d.itercount - 1;
-#define RP(ST, FI, LA)                                                   \
-  do {                                                                   \
-    if (d.F == 5) k_raypass<ST, FI, LA, 5><<<grid, 256, 0, s>>>(d);      \
-    else k_raypass<ST, FI, LA, 0><<<grid, 256, 0, s>>>(d);               \
-  } while (0)
+  const bool last = iter == d.itercount - 1;
+  if (iter == 0) k_seg_slots<<<grid, 256, 0, s>>>(d);
   if (strict) {
-    if (first && last) RP(true, true, true);
-    else if (first) RP(true, true, false);
-    else if (last) RP(true, false, true);
-    else RP(true, false, false);
-  } else {
-    if (first && last) RP(false, true, true);
-    else if (first) RP(false, true, false);
-    else if (last) RP(false, false, true);
-    else RP(false, false, false);
+    if (last) k_raypass_strict<true><<<grid, 256, 0, s>>>(d);
+    else k_raypass_strict<false><<<grid, 256, 0, s>>>(d);
+    return;
   }
-#undef RP
+  if (d.F == 5) {
+    if (last) k_raypass_mixed<true, 5><<<grid, 256, 0, s>>>(d);
+    else k_raypass_mixed<false, 5><<<grid, 256, 0, s>>>(d);
+  } else {
+    if (last) k_raypass_mixed<true, 0><<<grid, 256, 0, s>>>(d);
+    else k_raypass_mixed<false, 0><<<grid, 256, 0, s>>>(d);
+  }
 }
 
 void launch_litpass(const Dev& d, int iter, bool strict, bool fused_thermal, int grid, cudaStream_t s) {

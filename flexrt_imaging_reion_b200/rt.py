@@ -173,6 +173,47 @@ class RTContext:
         self.new_rays(self.draw_cast())
         self.get_nphot_min_max()
 
+    def setup_restart(self, files) -> None:
+        """Set-up from restart records in the reference's formats, one (gas, treion, rays) bytes
+        triple per box (the reference's restart path: init() and init_rt() with input_grid = TRUE,
+        no set-up cast)."""
+        for b, (gas, tre, _) in enumerate(files):
+            self._check(self.L.frt_read_gas(self.h, b, gas, len(gas)), "frt_read_gas")
+            self._check(self.L.frt_read_treion(self.h, b, tre, len(tre)), "frt_read_treion")
+            ijk, lum = self.src[b]
+            ijk = np.ascontiguousarray(ijk, np.int32)
+            lum = np.ascontiguousarray(lum, np.float64)
+            self._check(self.L.frt_set_sources(self.h, b, len(lum), ijk.ctypes.data, lum.ctypes.data),
+                        "frt_set_sources")
+            inp = self.inputs[b]
+            if inp.clump is not None:
+                cl = np.ascontiguousarray(inp.clump, np.float32)
+                self._check(self.L.frt_set_clump_field(self.h, b, cl.ctypes.data), "frt_set_clump_field")
+        self.update_dt()
+        self.init_rt()
+        for b, (_, _, rays) in enumerate(files):
+            self._check(self.L.frt_read_rays(self.h, b, rays, len(rays)), "frt_read_rays")
+        self.get_nphot_min_max()
+
+    def cosmo_expansion(self, a_current, a_prev) -> None:
+        """update_cosmo_expansion + update_dt with per-box scale factors (end and start of the
+        step just taken)."""
+        ac = np.ascontiguousarray(np.broadcast_to(np.asarray(a_current, np.float32), (self.nbox,)))
+        ap = np.ascontiguousarray(np.broadcast_to(np.asarray(a_prev, np.float32), (self.nbox,)))
+        self._check(self.L.frt_update_cosmo_expansion(self.h, ac.ctypes.data, ap.ctypes.data),
+                    "frt_update_cosmo_expansion")
+
+    def write_restart(self, box: int = 0):
+        """(gas, rays, treion) records of a box in the reference's restart formats."""
+        out = []
+        for fn in ("frt_write_gas", "frt_write_rays", "frt_write_treion"):
+            n = C.c_size_t(0)
+            self._check(getattr(self.L, fn)(self.h, box, None, 0, C.byref(n)), fn)
+            buf = (C.c_ubyte * n.value)()
+            self._check(getattr(self.L, fn)(self.h, box, buf, n.value, C.byref(n)), fn)
+            out.append(bytes(buf))
+        return tuple(out)
+
     def draw_cast(self) -> np.ndarray:
         """init_rays draws of the set-up cast, from the context's per-box glibc streams."""
         out = np.zeros(max(1, self.nsrc), np.uint16)

@@ -138,6 +138,12 @@ frt_status frt_get_field(frt_ctx* ctx, int box, frt_field f, float* host);
 frt_status frt_init_rt(frt_ctx* ctx);
 /* update_dt (rt_funcs.cc:9-12); dt_out[box] may be NULL */
 frt_status frt_update_dt(frt_ctx* ctx, float* dt_out);
+/* update_cosmo_expansion (gas_funcs.cc:460-548) followed by update_dt, as main.cc:219-237 calls
+ * them after new_rays: per box, the scale factors of this step's end and start (a_current[box],
+ * a_prev[box], as the caller's cosmic-time table gives them, gas_funcs.cc:461-465). The cell size
+ * and ray positions scale by a_current/a_prev, the proper density by (a_prev/a_current)^3, and the
+ * number densities follow from it with the ionised fractions kept. */
+frt_status frt_update_cosmo_expansion(frt_ctx* ctx, const float* a_current, const float* a_prev);
 /* get_nphot_min_max (ray_tracing.cc:129-154) */
 frt_status frt_get_nphot_min_max(frt_ctx* ctx, double* nmin_out, double* nmax_out);
 /* set_clump + set_clight (subgrid.cc:799-811, rt_funcs.cc:129-143) */
@@ -194,6 +200,27 @@ frt_status frt_box_scalars(frt_ctx* ctx, int box, double* out8);
 /* Kernel time of the last frt_step / frt_step_plain in ms (device events on the step stream),
  * and the time of its dominant cell kernel. */
 frt_status frt_last_timing(frt_ctx* ctx, float* step_ms, float* cell_kernel_ms);
+
+/* ---- restart files (the reference's own formats) ------------------------------------------------
+ * Writers: the records of write_gas_binary (io_funcs.cc:358-393: float t, then per cell rho, temp,
+ * nH1, f_H1, f_He1, f_H2, f_He2, f_He3, gamma_H1_tot, gamma_He1_tot, mfp, mfp_912, heat_rate,
+ * cool_rate, avg_nh1, fion, tcross, treion_out, ngam_nu[nfreq]), write_rays_binary (274-303:
+ * packed {int64 slot, bool active, int16 order, int32 pixel, uint16 itheta, float xhat, yhat,
+ * zhat, nphot[nfreq], r, dr, x, y, z, time, int32 cell} ended by slot -1) and write_treion
+ * (338-355: per cell float treion, bool treion_flag, tcross_flag, neutral_flag). With buf NULL
+ * only *len (the byte count) is returned. With core outputs mfp comes from the final <n_HI> and
+ * ngam_nu is 0 (both are output fields; diag outputs write the reference's values).
+ * Readers (a restart, input_grid = TRUE): frt_read_gas replaces frt_init_gas (init_funcs.cc:10-19,
+ * 62-138), frt_read_treion sets treion and its flag, and after frt_init_rt (which then keeps the
+ * file's time and sets ray_dt = 0 at the sources, rt_funcs.cc:95-101) frt_read_rays appends the
+ * file's rays (read_rays_binary, io_funcs.cc:119-146, with init_rt's removal of an empty ray in
+ * slot 0, rt_funcs.cc:117-124). No set-up cast follows a restart. */
+frt_status frt_write_gas(frt_ctx* ctx, int box, void* buf, size_t cap, size_t* len);
+frt_status frt_write_rays(frt_ctx* ctx, int box, void* buf, size_t cap, size_t* len);
+frt_status frt_write_treion(frt_ctx* ctx, int box, void* buf, size_t cap, size_t* len);
+frt_status frt_read_gas(frt_ctx* ctx, int box, const void* buf, size_t len);
+frt_status frt_read_treion(frt_ctx* ctx, int box, const void* buf, size_t len);
+frt_status frt_read_rays(frt_ctx* ctx, int box, const void* buf, size_t len);
 
 /* ---- adjoint of the next step's Gamma field --------------------------------------------------
  * Objective: J = sum of Gamma_HI (gamma_H1_tot, ray_tracing.cc:1152) over the cells

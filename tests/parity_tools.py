@@ -241,3 +241,20 @@ def photon_budget(stats_list, in_flight_0: float) -> float:
         ovl += st["photons_overlap"]
     end = stats_list[-1]["photons_in_flight"]
     return abs(emitted - (dep - ovl) - kil - end) / emitted
+
+
+def oracle_restart_states(inp: W.BoxInputs, seed: int, files, steps: int) -> List[Dict[str, np.ndarray]]:
+    """States of the oracle restarted from (gas, treion, rays) records, after the read (index 0)
+    and after each step."""
+    o = O.Oracle(inp, seed)
+    o.read_restart(*files)
+    out = []
+    with tempfile.TemporaryDirectory() as td:
+        for s in range(steps + 1):
+            if s > 0:
+                o.step()
+            p = os.path.join(td, f"s{s}.frtd")
+            o.dump(p)
+            out.append(frtd.read(p))
+    o.close()
+    return out
