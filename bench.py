@@ -44,6 +44,13 @@ DARK_BYTES_PER_CELL = 82  # 10 float fields + treion_flag + lit_flag read, 10 fl
 # step 24 of the L workload: 1342.3 MB for 13 264 000 dark cells (profiles/k_dark_L.md). The
 # bench scales it by the dark cells of its own steps (traffic grows with the cells processed).
 DARK_TRAFFIC_BYTES_PER_CELL = 1342312448 / 13264000
+# Ray pass (the dominant kernel): the algorithmic bytes of one crossing in one C2Ray iteration as
+# the hot-path analysis counts them -- 8 B segment read, 8 B of gathered <n_HI>, <n_HeI>, 68 B of
+# deposits (2 + 3 x 5 floats) -- and the ncu DRAM bytes per crossing of one launch at step 24 of L
+# (profiles/k_raypass_L.md).
+ITERCOUNT = 5
+RAYPASS_BYTES_PER_CROSSING = 8 + 8 + 68
+RAYPASS_TRAFFIC_BYTES_PER_CROSSING = None
 
 
 def _peaks():
@@ -257,7 +264,17 @@ def run_ensemble(args, rank: int, world: int, local_rank: int):
             "what": "one context per box, every kernel launched directly (no graph), boxes one after another; "
                     "host wall clock"}
         res["batched_vs_loop_wall"] = (cross / wall) / (loop["crossings"] / loop["wall_s"])
-        res["same_crossings"] = int(loop["crossings"]) == int(bat["crossings"])
+        # the ray trees agree up to rays whose photon count ties with a threshold (float sums in
+        # another order)
+        res["crossings_rel_diff"] = abs(loop["crossings"] - bat["crossings"]) / max(1, bat["crossings"])
+        ps = EN.run_per_box_loop(inputs, seeds, args.warmup, args.steps, device=local_rank, per_source=True)
+        res["per_box_per_source_loop"] = {
+            "value": ps["crossings"] / ps["wall_s"], "unit": "crossings/s", "ms_per_step": 1e3 * ps["wall_s"] / args.steps,
+            "crossings": ps["crossings"],
+            "gpu_launches": args.steps * sum(launches_per_step(specs[b], EN.ray_capacity([specs[b]])) - 1 +
+                                             len(W.grid_sources(inp)[1]) for b, inp in zip(mine, inputs)),
+            "what": "as per_box_plain_loop, and the cast launched once per source; host wall clock"}
+        res["batched_vs_per_source_loop_wall"] = (cross / wall) / (ps["crossings"] / ps["wall_s"])
     return res
 
 
@@ -332,6 +349,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     dev_ms = 0.0
     dark_ms = 0.0
     dark_bytes = 0.0
+    rp_ms = 0.0
     h2d = 2 * ctx.nbox + 2 * ctx.nsrc
     d2h = 0
     launches = 0
@@ -344,6 +362,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         cross += st["crossings"]
         dev_ms += ms
         dark_ms += dms
+        rp_ms += ctx.last_raypass_ms()
         dark_bytes += DARK_BYTES_PER_CELL * (ncell - st["lit_cells"])
         launches += per_step
         lit += st["lit_cells"]
@@ -363,6 +382,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dev_ms_max, wall_max, cross_all = dev_ms, wall, float(cross)
     peak, peak_kind = _peaks()
     dark_gbs = dark_bytes / (dark_ms * 1e-3) / 1e9 if dark_ms > 0 else None
+    rp_gbs = RAYPASS_BYTES_PER_CROSSING * cross * ITERCOUNT / (rp_ms * 1e-3) / 1e9 if rp_ms > 0 else None
     res = {
         "metric": "ray-cell crossings/s", "value": cross_all / (dev_ms_max * 1e-3), "unit": "crossings/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps,
@@ -373,14 +393,24 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                    "parallelism": "replicas" if world > 1 else "single"},
         "e2e": {"value": cross_all / wall_max, "unit": "crossings/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "hbm", "kernel": "k_dark (cells no ray touched: whole step in one pass)",
-                     "achieved": dark_gbs, "peak": peak, "unit": "GB/s",
-                     "frac": (dark_gbs / peak) if dark_gbs else None,
-                     "traffic": DARK_TRAFFIC_BYTES_PER_CELL * (ncell - lit / args.steps),
-                     "traffic_note": "bytes per launch: ncu DRAM bytes per dark cell x dark cells per step",
-                     "algorithmic_bytes_per_launch": DARK_BYTES_PER_CELL * (ncell - lit / args.steps),
-                     "peak_kind": peak_kind, "bytes_per_cell": DARK_BYTES_PER_CELL,
-                     "kernel_ms_per_step": dark_ms / args.steps},
+        # the dominant kernel: the ray pass (five launches per step, one per C2Ray iteration)
+        "roofline": {"bound": "hbm", "kernel": "k_raypass_mixed (ray pass of one C2Ray iteration)",
+                     "achieved": rp_gbs, "peak": peak, "unit": "GB/s",
+                     "frac": (rp_gbs / peak) if rp_gbs else None,
+                     "traffic": (RAYPASS_TRAFFIC_BYTES_PER_CROSSING * cross / args.steps
+                                 if RAYPASS_TRAFFIC_BYTES_PER_CROSSING else None),
+                     "traffic_note": "bytes per launch: ncu DRAM bytes per crossing of a ray pass x crossings per step",
+                     "algorithmic_bytes_per_launch": RAYPASS_BYTES_PER_CROSSING * cross / args.steps,
+                     "bytes_per_crossing": RAYPASS_BYTES_PER_CROSSING,
+                     "peak_kind": peak_kind, "launch_ms": rp_ms / args.steps / ITERCOUNT,
+                     "launches_per_step": ITERCOUNT},
+        "roofline_dark": {"bound": "hbm", "kernel": "k_dark (cells no ray touched: whole step in one pass)",
+                          "achieved": dark_gbs, "peak": peak, "unit": "GB/s",
+                          "frac": (dark_gbs / peak) if dark_gbs else None,
+                          "traffic": DARK_TRAFFIC_BYTES_PER_CELL * (ncell - lit / args.steps),
+                          "algorithmic_bytes_per_launch": DARK_BYTES_PER_CELL * (ncell - lit / args.steps),
+                          "peak_kind": peak_kind, "bytes_per_cell": DARK_BYTES_PER_CELL,
+                          "kernel_ms_per_step": dark_ms / args.steps},
         "gpu_launches": launches,
         "clocks": clk,
         "crossings_per_step": cross / args.steps,

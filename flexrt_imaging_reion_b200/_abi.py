@@ -32,7 +32,8 @@ EXPORTS = ["frt_create", "frt_destroy", "frt_last_error", "frt_rotation_table", 
            "frt_step_plain", "frt_last_stats", "frt_num_rays", "frt_download_rays", "frt_box_scalars",
            "frt_last_timing", "frt_seed_boxes", "frt_draw_cast", "frt_draw_step", "frt_get_sparse_field_noalloc", "frt_adjoint",
            "frt_last_adjoint_timing", "frt_write_gas", "frt_write_rays", "frt_write_treion", "frt_read_gas",
-           "frt_read_treion", "frt_read_rays", "frt_update_cosmo_expansion"]
+           "frt_read_treion", "frt_read_rays", "frt_update_cosmo_expansion",
+           "frt_set_cast_per_source", "frt_last_kernel_timing"]
 NOALLOC_MAX_CELLS = 1 << 20
 
 
@@ -122,6 +123,8 @@ def lib() -> C.CDLL:
         "frt_read_treion": ([P, I, P, C.c_size_t], I),
         "frt_read_rays": ([P, I, P, C.c_size_t], I),
         "frt_update_cosmo_expansion": ([P, P, P], I),
+        "frt_set_cast_per_source": ([P, I], I),
+        "frt_last_kernel_timing": ([P, I, P], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -22,6 +22,9 @@ struct frt_ctx {
   std::vector<void*> allocs;
   cudaStream_t s_main = nullptr, s_dark = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_t0 = nullptr, ev_t1 = nullptr, ev_d0 = nullptr, ev_d1 = nullptr;
+  static constexpr int kMaxTimedIter = 16;
+  cudaEvent_t ev_r[2 * kMaxTimedIter] = {};   // around each ray pass of the step
+  float last_raypass_ms = 0.f;
   // sources per box (host copy)
   std::vector<std::vector<int>> src_cell;
   std::vector<std::vector<double>> src_lum;
@@ -40,6 +43,7 @@ struct frt_ctx {
   int grid_rays = 0, grid_cells = 0, grid_lit = 0;
   float last_step_ms = 0.f, last_dark_ms = 0.f;
   bool rays_moved = false;   // an advance, merge or split ran (rays no longer one source's cast)
+  bool cast_per_source = false;   // unbatched cast in the direct-launch step (comparison baseline)
   AdjDev adj{};
   bool adj_ready = false;
   float* adj_out = nullptr;   // gather buffer of the adjoint's per-cell output (largest box)
@@ -150,11 +154,19 @@ void enqueue_begin_advance(frt_ctx* ctx) {
   launch_advance(d, ctx->grid_rays, ctx->s_main);
 }
 
-void enqueue_iterations(frt_ctx* ctx, bool fused_thermal) {
+void record(cudaEvent_t e, cudaStream_t s, bool in_graph) {
+  if (in_graph) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+  else cudaEventRecord(e, s);
+}
+
+void enqueue_iterations(frt_ctx* ctx, bool fused_thermal, bool in_graph = false) {
   const Dev& d = ctx->d;
   launch_lit_init(d, ctx->strict, ctx->grid_lit, ctx->s_main);
   for (int it = 0; it < d.itercount; it++) {
+    const bool timed = it < frt_ctx::kMaxTimedIter;
+    if (timed) record(ctx->ev_r[2 * it], ctx->s_main, in_graph);
     launch_raypass(d, it, ctx->strict, ctx->grid_rays, ctx->s_main);
+    if (timed) record(ctx->ev_r[2 * it + 1], ctx->s_main, in_graph);
     launch_litpass(d, it, ctx->strict, fused_thermal, ctx->grid_lit, ctx->s_main);
   }
 }
@@ -175,12 +187,13 @@ void enqueue_step(frt_ctx* ctx, bool in_graph) {
   if (in_graph) cudaEventRecordWithFlags(ctx->ev_d1, ctx->s_dark, cudaEventRecordExternal);
   else cudaEventRecord(ctx->ev_d1, ctx->s_dark);
   cudaEventRecord(ctx->ev_join, ctx->s_dark);
-  enqueue_iterations(ctx, true);
+  enqueue_iterations(ctx, true, in_graph);
   launch_count(d, ctx->grid_rays, s);
   launch_merge(d, ctx->grid_rays, s);
   launch_split_compact(d, ctx->grid_rays, s);
   cudaStreamWaitEvent(s, ctx->ev_join, 0);
-  launch_cast(d, s);
+  if (!in_graph && ctx->cast_per_source) launch_cast_per_source(d, s);
+  else launch_cast(d, s);
   cudaMemcpyAsync(ctx->h_ctl, d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
 }
 
@@ -261,6 +274,17 @@ frt_status finish_step(frt_ctx* ctx, frt_step_stats* stats) {
   }
   ctx->last_step_ms = ms;
   ctx->last_dark_ms = dms;
+  float rms = 0.f;
+  for (int it = 0; it < std::min(ctx->d.itercount, (int)frt_ctx::kMaxTimedIter); it++) {
+    float x = 0.f;
+    if (cudaEventElapsedTime(&x, ctx->ev_r[2 * it], ctx->ev_r[2 * it + 1]) != cudaSuccess) {
+      cudaGetLastError();
+      rms = -1.f;
+      break;
+    }
+    rms += x;
+  }
+  ctx->last_raypass_ms = rms;
   fill_stats(ctx, *ctx->h_ctl, stats);
   if (ctx->h_ctl->err) {
     ctx->err = "device error flags " + std::to_string(ctx->h_ctl->err) +
@@ -301,6 +325,7 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
   CK(cudaEventCreate(&ctx->ev_t1));
   CK(cudaEventCreate(&ctx->ev_d0));
   CK(cudaEventCreate(&ctx->ev_d1));
+  for (cudaEvent_t& e : ctx->ev_r) CK(cudaEventCreate(&e));
 
   Dev& d = ctx->d;
   memset(&d, 0, sizeof(d));
@@ -356,6 +381,10 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
     AL(r, ctx->rot.size());
     CK(cudaMemcpy(r, ctx->rot.data(), sizeof(float) * ctx->rot.size(), cudaMemcpyHostToDevice));
     d.rot = r;
+    float4* pt = nullptr;
+    AL(pt, (size_t)pix_tab_offset(kPixTabMax + 1));
+    launch_pix_table(pt, ctx->s_main);
+    d.pix_tab = pt;
   }
   {
     std::vector<int16_t> tb(d.ntile, (int16_t)-1);
@@ -445,6 +474,8 @@ frt_status frt_destroy(frt_ctx* ctx) {
   if (ctx->h_ith_box) cudaFreeHost(ctx->h_ith_box);
   if (ctx->h_ith_src) cudaFreeHost(ctx->h_ith_src);
   if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
+  for (cudaEvent_t e : ctx->ev_r)
+    if (e) cudaEventDestroy(e);
   cudaEvent_t evs[] = {ctx->ev_fork, ctx->ev_join, ctx->ev_t0, ctx->ev_t1, ctx->ev_d0, ctx->ev_d1};
   for (cudaEvent_t e : evs)
     if (e) cudaEventDestroy(e);
@@ -1006,9 +1037,21 @@ frt_status frt_box_scalars(frt_ctx* ctx, int box, double* out8) {
   return FRT_OK;
 }
 
+frt_status frt_set_cast_per_source(frt_ctx* ctx, int per_source) {
+  if (!ctx) return FRT_ERR_INVALID;
+  ctx->cast_per_source = per_source != 0;
+  return FRT_OK;
+}
+
 frt_status frt_last_adjoint_timing(frt_ctx* ctx, float* ms) {
   if (!ctx || !ms) return FRT_ERR_INVALID;
   *ms = ctx->last_adjoint_ms;
+  return FRT_OK;
+}
+
+frt_status frt_last_kernel_timing(frt_ctx* ctx, int which, float* ms) {
+  if (!ctx || !ms || which < 0 || which > 1) return FRT_ERR_INVALID;
+  *ms = which == 0 ? ctx->last_dark_ms : ctx->last_raypass_ms;
   return FRT_OK;
 }
 

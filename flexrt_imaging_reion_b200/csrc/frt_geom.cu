@@ -30,6 +30,40 @@ __device__ __forceinline__ void rot_apply(const float* m, float x, float y, floa
   *oz = (m[6] * x + m[7] * y) + m[8] * z;
 }
 
+// Direction of NEST pixel `pix` at HEALPix `order` as the float triple the rotation takes: from
+// the table for orders up to kPixTabMax (built by the same pix2vec), else computed (out of line,
+// so that the common table path keeps few registers).
+__device__ __noinline__ void pix_dir_computed(int order, int pix, float* fx, float* fy, float* fz) {
+  double vx, vy, vz;
+  hpn::pix2vec(order, pix, &vx, &vy, &vz);
+  *fx = (float)vx;
+  *fy = (float)vy;
+  *fz = (float)vz;
+}
+
+__device__ __forceinline__ void pix_dir(const Dev& d, int order, int pix, float* fx, float* fy, float* fz) {
+  if (order <= kPixTabMax) {
+    const float4 v = d.pix_tab[4ll * ((1ll << (2 * order)) - 1) + pix];
+    *fx = v.x;
+    *fy = v.y;
+    *fz = v.z;
+  } else {
+    pix_dir_computed(order, pix, fx, fy, fz);
+  }
+}
+
+__global__ void k_pix_table(float4* tab) {
+  const long long n = 4ll * ((1ll << (2 * (kPixTabMax + 1))) - 1);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    int order = 0;
+    while (e >= 4ll * ((1ll << (2 * (order + 1))) - 1)) order++;
+    const int pix = (int)(e - 4ll * ((1ll << (2 * order)) - 1));
+    double vx, vy, vz;
+    hpn::pix2vec(order, pix, &vx, &vy, &vz);
+    tab[e] = make_float4((float)vx, (float)vy, (float)vz, 0.f);
+  }
+}
+
 __device__ __forceinline__ float sum_nphot(const RayPool& P, int i, int F, int cap) {
   float s = 0.f;
   for (int nu = 0; nu < F; nu++) s += P.nphot[(size_t)nu * cap + i];
@@ -426,9 +460,10 @@ __global__ void k_merge_final(Dev d, double pi_sf_3, double log4) {
       A.order[i] = (int16_t)order;
       const int pixel = hpn::vec2pix(order, vx, vy, vz);
       A.pixel[i] = pixel;
-      hpn::pix2vec(order, pixel, &vx, &vy, &vz);
+      float fx, fy, fz;
+      pix_dir(d, order, pixel, &fx, &fy, &fz);
       float ox, oy, oz;
-      rot_apply(d.rot + (size_t)ith * 18, (float)vx, (float)vy, (float)vz, &ox, &oy, &oz);
+      rot_apply(d.rot + (size_t)ith * 18, fx, fy, fz, &ox, &oy, &oz);
       A.xh[i] = ox;
       A.yh[i] = oy;
       A.zh[i] = oz;
@@ -508,10 +543,10 @@ __global__ void __launch_bounds__(256) k_split(Dev d) {
     const uint16_t ith = A.itheta[i];
     const float r0 = A.r[i];
     const float rs = r0 * B.scale;
-    double vx, vy, vz;
-    hpn::pix2vec(l + 1, pix, &vx, &vy, &vz);
+    float fx, fy, fz;
+    pix_dir(d, l + 1, pix, &fx, &fy, &fz);
     float nx, ny, nz;
-    rot_apply(d.rot + (size_t)ith * 18, (float)vx, (float)vy, (float)vz, &nx, &ny, &nz);
+    rot_apply(d.rot + (size_t)ith * 18, fx, fy, fz, &nx, &ny, &nz);
     float x0 = (float)((double)A.x[i] + ((double)nx - (double)A.xh[i]) * (double)rs);
     float y0 = (float)((double)A.y[i] + ((double)ny - (double)A.yh[i]) * (double)rs);
     float z0 = (float)((double)A.z[i] + ((double)nz - (double)A.zh[i]) * (double)rs);
@@ -561,13 +596,13 @@ __global__ void k_swap(Dev d) {
 
 // new_rays -> init_rays (rt_funcs.cc:240-261, ray_tracing.cc:230-321): 12 Nside^2 rays per source
 // at the cell centre, directions of the NEST pixels rotated by the source's random angles.
-__global__ void k_cast(Dev d) {
+__global__ void k_cast(Dev d, int s_begin, int s_end) {
   const int cur = d.ctl->cur;
   const RayPool A = d.pool[cur];
   const int cap = d.ray_cap, F = d.F;
   long long ncast = 0;
   double emitted = 0.0;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < d.nsrc; s += gridDim.x * blockDim.x) {
+  for (int s = s_begin + blockIdx.x * blockDim.x + threadIdx.x; s < s_end; s += gridDim.x * blockDim.x) {
     const int b = d.src_box[s];
     const BoxP& B = d.box[b];
     const int c = d.src_cell[s];
@@ -595,10 +630,10 @@ __global__ void k_cast(Dev d) {
     }
     for (int p = 0; p < count; p++) {
       const int j = pos + p;
-      double vx, vy, vz;
-      hpn::pix2vec(lpix, p, &vx, &vy, &vz);
+      float fx, fy, fz;
+      pix_dir(d, lpix, p, &fx, &fy, &fz);
       float ox, oy, oz;
-      rot_apply(m, (float)vx, (float)vy, (float)vz, &ox, &oy, &oz);
+      rot_apply(m, fx, fy, fz, &ox, &oy, &oz);
       A.cell[j] = c;
       A.box[j] = (uint16_t)b;
       A.order[j] = (int16_t)lpix;
@@ -728,13 +763,19 @@ void launch_split_compact(const Dev& d, int grid, cudaStream_t s) {
 }
 
 void launch_cast(const Dev& d, cudaStream_t s) {
-  if (d.nsrc > 0) k_cast<<<grid_for(d.nsrc, 128, 4096), 128, 0, s>>>(d);
+  if (d.nsrc > 0) k_cast<<<grid_for(d.nsrc, 128, 4096), 128, 0, s>>>(d, 0, d.nsrc);
+}
+
+void launch_cast_per_source(const Dev& d, cudaStream_t s) {
+  for (int src = 0; src < d.nsrc; src++) k_cast<<<1, 32, 0, s>>>(d, src, src + 1);
 }
 
 void launch_cosmo_expansion(const Dev& d, int box, float ratio, double rho_factor, int grid, cudaStream_t s) {
   k_cosmo_cells<<<grid, 256, 0, s>>>(d, box, rho_factor);
   k_cosmo_rays<<<grid, 256, 0, s>>>(d, box, ratio);
 }
+
+void launch_pix_table(float4* tab, cudaStream_t s) { k_pix_table<<<148 * 8, 256, 0, s>>>(tab); }
 
 void launch_fill_i32(int* p, int v, long long n, cudaStream_t s) {
   k_fill_i32<<<grid_for(n, 256, 4096), 256, 0, s>>>(p, v, n);

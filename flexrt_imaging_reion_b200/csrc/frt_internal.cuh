@@ -70,6 +70,7 @@ struct Dev {
   double sigH1_0, sigH1_912;
   // tables
   const float* rot;        // [kNtheta][2][9] forward, inverse
+  const float4* pix_tab;   // HEALPix NEST pixel centres of orders 0..kPixTabMax, (float) of pix2vec
   // dense cells
   int16_t* tile_box;
   float *nH, *nHe, *nH1, *nHe1, *f_H1, *f_He1, *temp, *clump, *ne, *heat, *cool, *avg_nh1, *avg_nhe1, *treion;
@@ -140,7 +141,11 @@ void launch_count(const Dev& d, int grid, cudaStream_t s);
 void launch_merge(const Dev& d, int grid, cudaStream_t s);
 void launch_split_compact(const Dev& d, int grid, cudaStream_t s);
 void launch_cast(const Dev& d, cudaStream_t s);
+void launch_cast_per_source(const Dev& d, cudaStream_t s);   // one launch per source
 void launch_fill_i32(int* p, int v, long long n, cudaStream_t s);
+constexpr int kPixTabMax = 9;
+inline long long pix_tab_offset(int order) { return 4ll * ((1ll << (2 * order)) - 1); }   // sum of 12*4^k, k < order
+void launch_pix_table(float4* tab, cudaStream_t s);
 void launch_cosmo_expansion(const Dev& d, int box, float ratio, double rho_factor, int grid, cudaStream_t s);
 // ---- launchers (frt_phys.cu) ----------------------------------------------------------
 void launch_lit_init(const Dev& d, bool strict, int grid, cudaStream_t s);

@@ -111,19 +111,15 @@ __global__ void k_lit_init(Dev d) {
 // fields (diag), the new photon counts, and removes rays below nphot_min.
 
 // The segments' cell indices become lit slots once per step, before the first ray pass: one
-// thread per (moved ray, segment), a ray's segments being contiguous.
-__global__ void k_seg_slots(Dev d) {
+// thread per moved ray, whose segments are contiguous.
+__global__ void __launch_bounds__(256) k_seg_slots(Dev d) {
   const int nmv = min(d.ctl->n_moved, d.ray_cap);
   const int PL = d.PL;
-  const long long total = (long long)nmv * PL;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int q = (int)(t / PL), p = (int)(t - (long long)q * PL);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nmv; q += gridDim.x * blockDim.x) {
     const int i = d.moved[q];
-    if (p < d.nseg[i]) {
-      int2* sp = d.segs + (size_t)i * PL + p;
-      sp->x = d.lit_slot[sp->x];
-    }
+    const int ns = d.nseg[i];
+    int2* sp = d.segs + (size_t)i * PL;
+    for (int p = 0; p < ns; p++) sp[p].x = d.lit_slot[sp[p].x];
   }
 }
 

@@ -86,14 +86,17 @@ def run_batched(inputs: Sequence[W.BoxInputs], seeds: Sequence[int], warmup: int
 
 
 def run_per_box_loop(inputs: Sequence[W.BoxInputs], seeds: Sequence[int], warmup: int, steps: int,
-                     device: int = 0) -> Dict[str, float]:
+                     device: int = 0, per_source: bool = False) -> Dict[str, float]:
     """The unbatched form: one context per box, every kernel launched directly (no graph), the
-    boxes stepped one after another. Timed by host wall clock around each step of all boxes (each
-    plain step ends with a synchronising read of its totals)."""
+    boxes stepped one after another; with per_source, the cast is also one launch per source.
+    Timed by host wall clock around each step of all boxes (each plain step ends with a
+    synchronising read of its totals)."""
     ctxs = []
     for inp, seed in zip(inputs, seeds):
         c = _ctx([inp], [seed], device)
         c.setup()
+        if per_source:
+            c.set_cast_per_source(True)
         ctxs.append(c)
     for _ in range(warmup):
         for c in ctxs:

@@ -195,6 +195,10 @@ class RTContext:
             self._check(self.L.frt_read_rays(self.h, b, rays, len(rays)), "frt_read_rays")
         self.get_nphot_min_max()
 
+    def set_cast_per_source(self, on: bool) -> None:
+        """One cast launch per source in step(graph=False) (the unbatched comparison form)."""
+        self._check(self.L.frt_set_cast_per_source(self.h, int(bool(on))), "frt_set_cast_per_source")
+
     def cosmo_expansion(self, a_current, a_prev) -> None:
         """update_cosmo_expansion + update_dt with per-box scale factors (end and start of the
         step just taken)."""
@@ -361,6 +365,12 @@ class RTContext:
         if dl is not None:
             dl = dl[:self.nsrc_box[box]]
         return float(J.value), dl, dnh
+
+    def last_raypass_ms(self) -> float:
+        """Device time of the ray passes of the last step (sum over the C2Ray iterations)."""
+        v = C.c_float(0.0)
+        self._check(self.L.frt_last_kernel_timing(self.h, 1, C.byref(v)), "frt_last_kernel_timing")
+        return float(v.value)
 
     def last_adjoint_ms(self) -> float:
         v = C.c_float(0.0)

@@ -182,6 +182,10 @@ frt_status frt_draw_step(frt_ctx* ctx, uint16_t* itheta_per_box, uint16_t* ithet
  * receives the per-step totals of all boxes. */
 frt_status frt_step(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t* itheta_per_source,
                     frt_step_stats* stats);
+/* The unbatched cast for comparisons: with per_source != 0, frt_step_plain casts the new rays
+ * with one kernel launch per source (the way a per-source loop would), not one for all sources.
+ * Results are the same; frt_step (the graph) is not affected. */
+frt_status frt_set_cast_per_source(frt_ctx* ctx, int per_source);
 /* Same as frt_step but launching every kernel directly (no graph) */
 frt_status frt_step_plain(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t* itheta_per_source,
                           frt_step_stats* stats);
@@ -200,6 +204,9 @@ frt_status frt_box_scalars(frt_ctx* ctx, int box, double* out8);
 /* Kernel time of the last frt_step / frt_step_plain in ms (device events on the step stream),
  * and the time of its dominant cell kernel. */
 frt_status frt_last_timing(frt_ctx* ctx, float* step_ms, float* cell_kernel_ms);
+/* Device time in ms of one kernel family in the last frt_step / frt_step_plain (CUDA events on its
+ * stream): which = 0 the dark-cell kernel, 1 the ray passes of the C2Ray iteration (summed). */
+frt_status frt_last_kernel_timing(frt_ctx* ctx, int which, float* ms);
 
 /* ---- restart files (the reference's own formats) ------------------------------------------------
  * Writers: the records of write_gas_binary (io_funcs.cc:358-393: float t, then per cell rho, temp,

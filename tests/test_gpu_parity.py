@@ -35,6 +35,8 @@ def run_device(spec, seed, precision, mode, diag=True):
     ctx.setup()
     states, stats = [PT.device_state(ctx, 0, diag)], []
     in_flight0 = ctx.in_flight()
+    if mode == "plain_per_source":
+        ctx.set_cast_per_source(True)
     for _ in range(spec.steps):
         if mode == "unfused":
             ctx.step_unfused()
@@ -71,7 +73,7 @@ def check(states, ref, strict, merged=False):
 
 
 @pytest.mark.parametrize("precision,mode", [("strict", "graph"), ("strict", "unfused"), ("mixed", "graph"),
-                                            ("mixed", "plain"), ("mixed", "unfused")])
+                                            ("mixed", "plain"), ("mixed", "unfused"), ("mixed", "plain_per_source")])
 def test_t16_parity(precision, mode):
     spec, seed = T16
     ref = oracle_run(spec, seed)
