@@ -41,16 +41,16 @@ sys.path.insert(0, HERE)
 
 DARK_BYTES_PER_CELL = 82  # 10 float fields + treion_flag + lit_flag read, 10 float fields written
 # DRAM bytes per dark cell of one k_dark launch, from ncu (dram__bytes_read.sum + write.sum) at
-# step 24 of the L workload: 1342.3 MB for 13 264 000 dark cells (profiles/k_dark_L.md). The
+# step 24 of the L workload: 1342.3 MB for 13 264 000 dark cells. The
 # bench scales it by the dark cells of its own steps (traffic grows with the cells processed).
 DARK_TRAFFIC_BYTES_PER_CELL = 1342312448 / 13264000
 # Ray pass (the dominant kernel): the algorithmic bytes of one crossing in one C2Ray iteration as
 # the hot-path analysis counts them -- 8 B segment read, 8 B of gathered <n_HI>, <n_HeI>, 68 B of
-# deposits (2 + 3 x 5 floats) -- and the ncu DRAM bytes per crossing of one launch at step 24 of L
-# (profiles/k_raypass_L.md).
+# deposits (2 + 3 x 5 floats) -- and the ncu DRAM bytes (read + write) per crossing of one launch,
+# the mean over the 5 passes of step 24 of L (17 465 926 crossings per pass; 1160.4 MB per launch).
 ITERCOUNT = 5
 RAYPASS_BYTES_PER_CROSSING = 8 + 8 + 68
-RAYPASS_TRAFFIC_BYTES_PER_CROSSING = None
+RAYPASS_TRAFFIC_BYTES_PER_CROSSING = 66.4
 
 
 def _peaks():
@@ -317,10 +317,10 @@ def run_adjoint(args):
 
 # ---- our arm ---------------------------------------------------------------------------------
 def launches_per_step(spec, ray_capacity, itercount=5, hpx_lvl=0):
-    """Kernels one fused step launches: clear_lit, step_begin, advance, lit_compact, dark, lit_init,
-    seg_slots, itercount x (ray pass + lit pass), count, 3 merge set-up kernels (+4 binning kernels
-    when the pool can reach the merge threshold), compact, split, swap, cast."""
-    n = 1 + 1 + 1 + 1 + 1 + 1 + 1 + 2 * itercount + 1 + 3 + 3 + 1
+    """Kernels one fused step launches: clear_lit, step_begin, advance, lit_compact, moved_pack,
+    dark, lit_init, itercount x (ray pass + lit pass), count, 3 merge set-up kernels (+4 binning
+    kernels when the pool can reach the merge threshold), compact_split, swap, cast."""
+    n = 1 + 1 + 1 + 1 + 1 + 1 + 1 + 2 * itercount + 1 + 3 + 2 + 1
     num_thresh = (spec.ray_per_cell_max - 12 * 4 ** hpx_lvl) * spec.n ** 3
     if num_thresh < ray_capacity:
         n += 4

@@ -355,7 +355,8 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
     ctx->err = "too many cells for 32-bit cell indices";
     return FRT_ERR_INVALID;
   }
-  d.ray_cap = (int)std::min<long long>(cfg->ray_capacity, (1LL << 31) - 64);
+  // packed segment offsets are 32-bit: ray_cap * path_length stays below 2^31
+  d.ray_cap = (int)std::min<long long>(cfg->ray_capacity, ((1LL << 31) - 64) / d.PL);
   long long lc = cfg->lit_capacity > 0 ? cfg->lit_capacity : off;
   lc = std::min<long long>(lc, std::min<long long>(off, (long long)d.ray_cap * d.PL));
   d.lit_cap = (int)std::max<long long>(lc, 1024);
@@ -366,6 +367,8 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
   for (int nu = 0; nu < d.F; nu++) {
     d.sigH1_f[nu] = (float)d.sigH1_d[nu];
     d.sigHe1_f[nu] = (float)d.sigHe1_d[nu];
+    d.sigH1_l2[nu] = (float)(d.sigH1_d[nu] * 1.4426950408889634);
+    d.sigHe1_l2[nu] = (float)(d.sigHe1_d[nu] * 1.4426950408889634);
   }
   // device memory
   AL(d.box, cfg->nbox);
@@ -409,10 +412,10 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
   launch_fill_i32(d.lit_slot, -1, (long long)NC, ctx->s_main);
   const size_t L = (size_t)d.lit_cap;
   AL(d.l_cell, L); AL(d.l_nh, L); AL(d.l_nhe, L); AL(d.l_y0h, L); AL(d.l_y0he, L); AL(d.l_crec_h, L);
-  AL(d.l_crec_he, L); AL(d.l_rec_h2, L); AL(d.l_rec_he2, L); AL(d.l_avg_h, L); AL(d.l_avg_he, L);
-  AL(d.l_nh1_old, L); AL(d.l_acc_g, L); AL(d.l_acc_ghe, L);
+  AL(d.l_crec_he, L); AL(d.l_rec_h2, L); AL(d.l_rec_he2, L); AL(d.l_avg, L);
+  AL(d.l_nh1_old, L); AL(d.l_acc, L);
   d.per_bin = (ctx->strict || cfg->outputs == FRT_OUT_DIAG) ? 1 : 0;
-  AL(d.l_heat_h, L); AL(d.l_heat_he, L);
+  AL(d.l_heat, L);
   if (d.per_bin) {
     AL(d.l_ngam, L * d.F);
     AL(d.l_acc_nu_h, L * d.F);
@@ -429,8 +432,8 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
     AL(P.xh, R); AL(P.yh, R); AL(P.zh, R); AL(P.nphot, R * d.F);
     AL(P.r, R); AL(P.dr, R); AL(P.x, R); AL(P.y, R); AL(P.z, R); AL(P.time, R);
   }
-  AL(d.segs, R * d.PL); AL(d.nseg, R); AL(d.dead, R); AL(d.moved, R);
-  AL(d.split_list, R / 4 + 1);
+  AL(d.segs, R * d.PL); AL(d.nseg, R); AL(d.dead, R);
+  AL(d.pk, R * d.PL); AL(d.mv_hdr, R);
   // merge bins only when some box can reach its merge threshold with this pool size
   bool merge_reachable = false;
   for (int b = 0; b < cfg->nbox; b++) merge_reachable |= ctx->hbox[b].num_thresh < (long long)d.ray_cap;

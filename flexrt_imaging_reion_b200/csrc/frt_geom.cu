@@ -86,43 +86,6 @@ __device__ __forceinline__ T block_sum(T v) {
   return r;  // valid in thread 0
 }
 
-// Warp-aggregated slot reservation in a counter: every active lane asks for `want` slots.
-__device__ __forceinline__ int reserve(int* counter, int want) {
-  const unsigned mask = __activemask();
-  const int lane = threadIdx.x & 31;
-  int incl = want;
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(mask, incl, o);
-    // lanes outside the mask return their own value; only add real predecessors
-    if (lane >= o && ((mask >> (lane - o)) & 1u)) incl += v;
-  }
-  // the shuffle-up above assumes contiguous active lanes; fall back to per-lane atomics otherwise
-  if (mask != 0xffffffffu) return atomicAdd(counter, want);
-  const int total = __shfl_sync(mask, incl, 31);
-  int base = 0;
-  if (lane == 31) base = atomicAdd(counter, total);
-  base = __shfl_sync(mask, base, 31);
-  return base + incl - want;
-}
-
-__device__ __forceinline__ void copy_ray(const RayPool& A, int i, const RayPool& B, int j, int F, int cap) {
-  B.cell[j] = A.cell[i];
-  B.box[j] = A.box[i];
-  B.order[j] = A.order[i];
-  B.pixel[j] = A.pixel[i];
-  B.itheta[j] = A.itheta[i];
-  B.xh[j] = A.xh[i];
-  B.yh[j] = A.yh[i];
-  B.zh[j] = A.zh[i];
-  for (int nu = 0; nu < F; nu++) B.nphot[(size_t)nu * cap + j] = A.nphot[(size_t)nu * cap + i];
-  B.r[j] = A.r[i];
-  B.dr[j] = A.dr[i];
-  B.x[j] = A.x[i];
-  B.y[j] = A.y[i];
-  B.z[j] = A.z[i];
-  B.time[j] = A.time[i];
-}
-
 // ---------------------------------------------------------------------------------------
 // Start of a step: t += dt (main.cc:127), ray_dt of the sources += dt (rt_funcs.cc:163-172),
 // per-step counters to zero, the next pool emptied.
@@ -136,7 +99,7 @@ __global__ void k_step_begin(Dev d) {
     // kernel ever reads an uninitialised record (the error stays latched for the host)
     if (c->err) c->nray[c->cur] = 0;
     c->rays_moved = c->crossings = c->split = c->merged = c->killed = c->cast = 0;
-    c->n_moved = 0;
+    c->mv_seg = 0ull;
     c->emitted = c->deposited = c->killed_ph = c->overlap = c->in_flight = 0.0;
   }
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < d.nbox; b += gridDim.x * blockDim.x) d.box[b].t += d.box[b].dt;
@@ -164,10 +127,8 @@ __global__ void __launch_bounds__(256, 4) k_advance(Dev d) {
   const int cap = d.ray_cap, PL = d.PL;
   long long cross = 0, moved = 0, killed = 0;
   double killed_ph = 0.0;
-  const int lane = threadIdx.x & 31;
   for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
     const int i = i0 + threadIdx.x;
-    bool listed = false;
     if (i < n) do {
       d.dead[i] = 0;
       const BoxP& B = d.box[A.box[i]];
@@ -218,17 +179,7 @@ __global__ void __launch_bounds__(256, 4) k_advance(Dev d) {
         killed_ph += (double)sum_nphot(A, i, d.F, cap) * kPhotNorm;
         break;
       }
-      listed = true;
     } while (0);
-    // warp-aggregated append of the moved rays to the list the ray passes work through
-    const unsigned m = __ballot_sync(0xffffffffu, listed);
-    if (m) {
-      const int leader = __ffs(m) - 1;
-      int base = 0;
-      if (lane == leader) base = atomicAdd(&d.ctl->n_moved, __popc(m));
-      base = __shfl_sync(0xffffffffu, base, leader);
-      if (listed) d.moved[base + __popc(m & ((1u << lane) - 1u))] = i;
-    }
   }
   cross = block_sum(cross);
   moved = block_sum(moved);
@@ -239,6 +190,71 @@ __global__ void __launch_bounds__(256, 4) k_advance(Dev d) {
     if (moved) atomicAdd((unsigned long long*)&d.ctl->rays_moved, (unsigned long long)moved);
     if (killed) atomicAdd((unsigned long long*)&d.ctl->killed, (unsigned long long)killed);
     if (killed_ph != 0.0) atomicAdd(&d.ctl->killed_ph, killed_ph);
+  }
+}
+
+// The rays with segments this step (moved and not removed) and their segments, packed in
+// moved-list order for the ray passes: thread per pool ray, block-wide scans of the predicate and
+// of the segment counts, one 64-bit atomicAdd per block for both bases (so that the moved list
+// and the packed segments are allocated in the same block order). Moved ray q gets a 16-byte
+// header {pool index, first packed segment, segment count, box} that a ray pass reads at once. The
+// segment cells become lit slots here (after k_lit_compact); the first segment of each ray
+// carries the head bit (the sign of its dist, which is positive).
+__global__ void __launch_bounds__(256) k_moved_pack(Dev d) {
+  __shared__ int wt[8], ws[8];
+  __shared__ unsigned long long base_s;
+  const int n = d.ctl->nray[d.ctl->cur];
+  const uint16_t* rbox = d.pool[d.ctl->cur].box;
+  const int PL = d.PL;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned below = (1u << lane) - 1u;
+  for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+    const int i = i0 + threadIdx.x;
+    const bool take = (i < n) && d.nseg[i] > 0 && !d.dead[i];
+    const int ns = take ? (int)d.nseg[i] : 0;
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    int x = ns;   // inclusive scan of the segment counts over the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) {
+      wt[w] = __popc(m);
+      ws[w] = x;
+    }
+    __syncthreads();
+    if (w == 0) {
+      int a = (lane < 8) ? wt[lane] : 0, b = (lane < 8) ? ws[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) {
+        const int ya = __shfl_up_sync(0xffffffffu, a, o), yb = __shfl_up_sync(0xffffffffu, b, o);
+        if (lane >= o) {
+          a += ya;
+          b += yb;
+        }
+      }
+      if (lane < 8) {   // inclusive prefixes over the warps
+        wt[lane] = a;
+        ws[lane] = b;
+      }
+      if (lane == 7)
+        base_s = (a > 0) ? atomicAdd(&d.ctl->mv_seg, ((unsigned long long)a << 32) | (unsigned long long)b) : 0ull;
+    }
+    __syncthreads();
+    if (take) {
+      const int q = (int)(base_s >> 32) + (w > 0 ? wt[w - 1] : 0) + __popc(m & below);
+      const int off = (int)(base_s & 0xffffffffull) + (w > 0 ? ws[w - 1] : 0) + (x - ns);
+      d.mv_hdr[q] = make_int4(i, off, ns, (int)rbox[i]);
+      const int2* sp = d.segs + (size_t)i * PL;
+      int2* dp = d.pk + off;
+      for (int p = 0; p < ns; p++) {
+        const int2 c = sp[p];
+        // dist > 0: its sign bit is free for the head mark
+        dp[p] = make_int2(d.lit_slot[c.x], (int)(((unsigned)c.y & 0x7fffffffu) | (p == 0 ? 0x80000000u : 0u)));
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -475,47 +491,192 @@ __global__ void k_merge_final(Dev d, double pi_sf_3, double log4) {
   }
 }
 
-// split_rays (rt_funcs.cc:211-237) fused with the compaction into the next pool, in two
-// kernels. k_compact decides per ray: a live ray is copied; a ray past rmax(l) with enough
-// photons reserves 4 slots and is put on the split list. k_split then builds the children one
-// thread per child (split_ray, ray_tracing.cc:482-619): pixels 4*pn + c of order l+1, displaced
-// by (v_child - v_parent) r0 dx/dx0. Keeping the child arithmetic (pix2vec, rotation, wrap) out
-// of the copy loop keeps the copy kernel light and spreads the children over 4x the threads.
-__global__ void __launch_bounds__(256) k_compact(Dev d) {
+// split_rays (rt_funcs.cc:211-237) fused with the compaction into the next pool, one kernel.
+// A block takes 256 rays of the pool at a time; every thread loads its ray's record (all loads
+// issued back to back) and decides how many slots of the next pool it needs: a dead ray none, a
+// live ray one, a ray past rmax(l) with enough photons four (its children, split_ray,
+// ray_tracing.cc:482-619: pixels 4*pn + c of order l+1, displaced by (v_child - v_parent)
+// r0 dx/dx0). One block-wide scan gives each ray its offset and each split ray its rank among
+// the block's split rays, and one atomicAdd per block places the block's outputs contiguously. A
+// live ray is written by its own thread from registers; a split ray parks its record in shared
+// memory and the block's threads then build the children, four per split ray, spread over all
+// threads so that the child arithmetic (pixel table, rotation, wrap) runs at full width.
+__global__ void __launch_bounds__(256) k_compact_split(Dev d) {
+  __shared__ int s_cell[256], s_pixel[256], s_dst[256];
+  __shared__ float s_xh[256], s_yh[256], s_zh[256], s_r[256], s_x[256], s_y[256], s_z[256], s_time[256];
+  __shared__ float s_nph[FRT_MAX_FREQ][256];
+  __shared__ uint16_t s_box[256], s_ith[256];
+  __shared__ int16_t s_order[256];
+  __shared__ int s_wt[8];
+  __shared__ int s_tot, s_base;
   const int cur = d.ctl->cur;
   const int nxt = cur ^ 1;
   const int n = d.ctl->nray[cur];
   const RayPool A = d.pool[cur];
   const RayPool Bp = d.pool[nxt];
   const int cap = d.ray_cap, F = d.F;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   long long nsplit = 0;
   double inflight = 0.0;
-  for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
-    const int i = i0 + threadIdx.x;
-    bool live = (i < n) && !d.dead[i];
+  for (int i0 = blockIdx.x * 256; i0 < n; i0 += gridDim.x * 256) {
+    const int i = i0 + t;
+    const bool live = (i < n) && !d.dead[i];
+    int cell = 0, pixel = 0;
+    uint16_t bx = 0, ith = 0;
+    int16_t order = 0;
+    float xh = 0.f, yh = 0.f, zh = 0.f, r = 0.f, dr = 0.f, x = 0.f, y = 0.f, z = 0.f, tm = 0.f, sum = 0.f;
+    float nph[FRT_MAX_FREQ];
     bool split = false;
-    float s = 0.f;
     if (live) {
-      const BoxP& B = d.box[A.box[i]];
-      const int l = A.order[i];
-      s = sum_nphot(A, i, F, cap);
-      split = (A.r[i] > B.rmax[l]) && (l < kLmax) && (s > B.split_thr);
+      cell = A.cell[i];
+      bx = A.box[i];
+      order = A.order[i];
+      pixel = A.pixel[i];
+      ith = A.itheta[i];
+      xh = A.xh[i];
+      yh = A.yh[i];
+      zh = A.zh[i];
+      r = A.r[i];
+      dr = A.dr[i];
+      x = A.x[i];
+      y = A.y[i];
+      z = A.z[i];
+      tm = A.time[i];
+#pragma unroll
+      for (int nu = 0; nu < FRT_MAX_FREQ; nu++) {
+        nph[nu] = (nu < F) ? A.nphot[(size_t)nu * cap + i] : 0.f;
+        sum += (nu < F) ? nph[nu] : 0.f;
+      }
+      const BoxP& B = d.box[bx];
+      split = (r > B.rmax[order]) && (order < kLmax) && (sum > B.split_thr);
     }
+    // one block-wide exclusive scan: slots (low 16 bits, at most 1024) and split rank (high bits)
     const int want = live ? (split ? 4 : 1) : 0;
-    const int pos = reserve(&d.ctl->nray[nxt], want);
-    if (!live) continue;
-    if (pos + want > cap) {
-      atomicOr(&d.ctl->err, ERR_RAY_CAP);
-      continue;
+    const int key = want | ((split ? 1 : 0) << 16);
+    int incl = key;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
     }
-    if (!split) {
-      copy_ray(A, i, Bp, pos, F, cap);
-      inflight += (double)s;
-      continue;
+    if (lane == 31) s_wt[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      int v = (lane < 8) ? s_wt[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+      }
+      if (lane < 8) s_wt[lane] = v;   // inclusive prefix over the warps
+      if (lane == 7) {
+        s_tot = v;
+        const int slots = v & 0xffff;
+        s_base = (slots > 0) ? atomicAdd(&d.ctl->nray[nxt], slots) : 0;
+      }
     }
-    nsplit += 1;
-    const int k = atomicAdd(&d.ctl->n_split, 1);
-    d.split_list[k] = make_int2(i, pos);
+    __syncthreads();
+    const int excl = (w > 0 ? s_wt[w - 1] : 0) + incl - key;
+    const int base = s_base;
+    const int nsp = s_tot >> 16;
+    if (t == 0 && (long long)base + (s_tot & 0xffff) > (long long)cap) atomicOr(&d.ctl->err, ERR_RAY_CAP);
+    const int j = base + (excl & 0xffff);
+    if (live && !split) {
+      // a live ray: copied by its own thread
+      if (j < cap) {
+        Bp.cell[j] = cell;
+        Bp.box[j] = bx;
+        Bp.order[j] = order;
+        Bp.pixel[j] = pixel;
+        Bp.itheta[j] = ith;
+        Bp.xh[j] = xh;
+        Bp.yh[j] = yh;
+        Bp.zh[j] = zh;
+#pragma unroll
+        for (int nu = 0; nu < FRT_MAX_FREQ; nu++)
+          if (nu < F) Bp.nphot[(size_t)nu * cap + j] = nph[nu];
+        Bp.r[j] = r;
+        Bp.dr[j] = dr;
+        Bp.x[j] = x;
+        Bp.y[j] = y;
+        Bp.z[j] = z;
+        Bp.time[j] = tm;
+        inflight += (double)sum;
+      }
+    } else if (split) {
+      const int k = excl >> 16;
+      nsplit += 1;
+      s_dst[k] = j;
+      s_cell[k] = cell;
+      s_pixel[k] = pixel;
+      s_box[k] = bx;
+      s_ith[k] = ith;
+      s_order[k] = order;
+      s_xh[k] = xh;
+      s_yh[k] = yh;
+      s_zh[k] = zh;
+      s_r[k] = r;
+      s_x[k] = x;
+      s_y[k] = y;
+      s_z[k] = z;
+      s_time[k] = tm;
+#pragma unroll
+      for (int nu = 0; nu < FRT_MAX_FREQ; nu++)
+        if (nu < F) s_nph[nu][k] = nph[nu];
+    }
+    __syncthreads();
+    // the children, four per split ray of the block, over all threads
+    for (int u = t; u < 4 * nsp; u += 256) {
+      const int k = u >> 2, c = u & 3;
+      const int jc = s_dst[k] + c;
+      if (jc >= cap) continue;
+      const uint16_t cbx = s_box[k];
+      const BoxP& B = d.box[cbx];
+      const int N = B.n;
+      const int l = s_order[k];
+      const int pix = 4 * s_pixel[k] + c;
+      const uint16_t cith = s_ith[k];
+      const float r0 = s_r[k];
+      const float rs = r0 * B.scale;
+      float fx, fy, fz;
+      pix_dir(d, l + 1, pix, &fx, &fy, &fz);
+      float nx, ny, nz;
+      rot_apply(d.rot + (size_t)cith * 18, fx, fy, fz, &nx, &ny, &nz);
+      float x0 = (float)((double)s_x[k] + ((double)nx - (double)s_xh[k]) * (double)rs);
+      float y0 = (float)((double)s_y[k] + ((double)ny - (double)s_yh[k]) * (double)rs);
+      float z0 = (float)((double)s_z[k] + ((double)nz - (double)s_zh[k]) * (double)rs);
+      const int ind = s_cell[k];
+      const int ic = ind / B.nn, jcl = (ind - ic * B.nn) / N, kc = ind - ic * B.nn - jcl * N;
+      int icn = ic, jcn = jcl, kcn = kc;
+      for (int g = 0; g < 64 && x0 > B.dx; g++) { x0 -= B.dx; icn = imod(icn + 1, N); }
+      for (int g = 0; g < 64 && x0 < 0.f; g++) { x0 += B.dx; icn = imod(icn - 1, N); }
+      for (int g = 0; g < 64 && y0 > B.dx; g++) { y0 -= B.dx; jcn = imod(jcn + 1, N); }
+      for (int g = 0; g < 64 && y0 < 0.f; g++) { y0 += B.dx; jcn = imod(jcn - 1, N); }
+      for (int g = 0; g < 64 && z0 > B.dx; g++) { z0 -= B.dx; kcn = imod(kcn + 1, N); }
+      for (int g = 0; g < 64 && z0 < 0.f; g++) { z0 += B.dx; kcn = imod(kcn - 1, N); }
+      Bp.cell[jc] = icn * B.nn + jcn * N + kcn;
+      Bp.box[jc] = cbx;
+      Bp.order[jc] = (int16_t)(l + 1);
+      Bp.pixel[jc] = pix;
+      Bp.itheta[jc] = cith;
+      Bp.xh[jc] = nx;
+      Bp.yh[jc] = ny;
+      Bp.zh[jc] = nz;
+      float cs = 0.f;
+      for (int nu = 0; nu < F; nu++) {
+        const float q = (float)((double)s_nph[nu][k] / 4.);
+        Bp.nphot[(size_t)nu * cap + jc] = q;
+        cs += q;
+      }
+      inflight += (double)cs;
+      Bp.r[jc] = r0;
+      Bp.dr[jc] = B.rmax[l + 1] - r0;
+      Bp.x[jc] = x0;
+      Bp.y[jc] = y0;
+      Bp.z[jc] = z0;
+      Bp.time[jc] = s_time[k];
+    }
+    __syncthreads();   // the shared records take the next 256 rays
   }
   nsplit = block_sum(nsplit);
   inflight = block_sum(inflight);
@@ -523,66 +684,6 @@ __global__ void __launch_bounds__(256) k_compact(Dev d) {
     if (nsplit) atomicAdd((unsigned long long*)&d.ctl->split, (unsigned long long)nsplit);
     if (inflight != 0.0) atomicAdd(&d.ctl->in_flight, inflight * kPhotNorm);
   }
-}
-
-__global__ void __launch_bounds__(256) k_split(Dev d) {
-  const int cur = d.ctl->cur;
-  const RayPool A = d.pool[cur];
-  const RayPool Bp = d.pool[cur ^ 1];
-  const int cap = d.ray_cap, F = d.F;
-  const int nchild = 4 * d.ctl->n_split;
-  double inflight = 0.0;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nchild; t += gridDim.x * blockDim.x) {
-    const int2 e = d.split_list[t >> 2];
-    const int c = t & 3;
-    const int i = e.x, j = e.y + c;
-    const BoxP& B = d.box[A.box[i]];
-    const int N = B.n;
-    const int l = A.order[i];
-    const int pix = 4 * A.pixel[i] + c;
-    const uint16_t ith = A.itheta[i];
-    const float r0 = A.r[i];
-    const float rs = r0 * B.scale;
-    float fx, fy, fz;
-    pix_dir(d, l + 1, pix, &fx, &fy, &fz);
-    float nx, ny, nz;
-    rot_apply(d.rot + (size_t)ith * 18, fx, fy, fz, &nx, &ny, &nz);
-    float x0 = (float)((double)A.x[i] + ((double)nx - (double)A.xh[i]) * (double)rs);
-    float y0 = (float)((double)A.y[i] + ((double)ny - (double)A.yh[i]) * (double)rs);
-    float z0 = (float)((double)A.z[i] + ((double)nz - (double)A.zh[i]) * (double)rs);
-    const int ind = A.cell[i];
-    const int ic = ind / B.nn, jc = (ind - ic * B.nn) / N, kc = ind - ic * B.nn - jc * N;
-    int icn = ic, jcn = jc, kcn = kc;
-    for (int g = 0; g < 64 && x0 > B.dx; g++) { x0 -= B.dx; icn = imod(icn + 1, N); }
-    for (int g = 0; g < 64 && x0 < 0.f; g++) { x0 += B.dx; icn = imod(icn - 1, N); }
-    for (int g = 0; g < 64 && y0 > B.dx; g++) { y0 -= B.dx; jcn = imod(jcn + 1, N); }
-    for (int g = 0; g < 64 && y0 < 0.f; g++) { y0 += B.dx; jcn = imod(jcn - 1, N); }
-    for (int g = 0; g < 64 && z0 > B.dx; g++) { z0 -= B.dx; kcn = imod(kcn + 1, N); }
-    for (int g = 0; g < 64 && z0 < 0.f; g++) { z0 += B.dx; kcn = imod(kcn - 1, N); }
-    Bp.cell[j] = icn * B.nn + jcn * N + kcn;
-    Bp.box[j] = A.box[i];
-    Bp.order[j] = (int16_t)(l + 1);
-    Bp.pixel[j] = pix;
-    Bp.itheta[j] = ith;
-    Bp.xh[j] = nx;
-    Bp.yh[j] = ny;
-    Bp.zh[j] = nz;
-    float s = 0.f;
-    for (int nu = 0; nu < F; nu++) {
-      const float q = (float)((double)A.nphot[(size_t)nu * cap + i] / 4.);
-      Bp.nphot[(size_t)nu * cap + j] = q;
-      s += q;
-    }
-    inflight += (double)s;
-    Bp.r[j] = r0;
-    Bp.dr[j] = B.rmax[l + 1] - r0;
-    Bp.x[j] = x0;
-    Bp.y[j] = y0;
-    Bp.z[j] = z0;
-    Bp.time[j] = A.time[i];
-  }
-  inflight = block_sum(inflight);
-  if (threadIdx.x == 0 && inflight != 0.0) atomicAdd(&d.ctl->in_flight, inflight * kPhotNorm);
 }
 
 __global__ void k_swap(Dev d) {
@@ -736,6 +837,7 @@ void launch_step_begin(const Dev& d, cudaStream_t s) { k_step_begin<<<grid_for(d
 void launch_advance(const Dev& d, int grid, cudaStream_t s) {
   k_advance<<<grid, 256, 0, s>>>(d);
   k_lit_compact<<<grid_for(d.ncell_total >> 4, 256, 148 * 8), 256, 0, s>>>(d);
+  k_moved_pack<<<grid, 256, 0, s>>>(d);
 }
 
 void launch_count(const Dev& d, int grid, cudaStream_t s) {
@@ -756,9 +858,7 @@ void launch_merge(const Dev& d, int grid, cudaStream_t s) {
 }
 
 void launch_split_compact(const Dev& d, int grid, cudaStream_t s) {
-  cudaMemsetAsync(&d.ctl->n_split, 0, sizeof(int), s);
-  k_compact<<<grid, 256, 0, s>>>(d);
-  k_split<<<grid, 256, 0, s>>>(d);
+  k_compact_split<<<grid, 256, 0, s>>>(d);
   k_swap<<<1, 1, 0, s>>>(d);
 }
 

@@ -40,9 +40,9 @@ struct Ctl {
   int n_lit_prev;
   unsigned err;
   int any_merge;           // some box has nphot_merge > 0
-  int n_split;             // entries of the split list this step
-  int n_moved;             // entries of the moved-ray list this step
-  int pad2;
+  // moved rays this step (high 32 bits) and their segments (low 32 bits), counted together so
+  // that one atomicAdd gives a block both bases (k_moved_pack)
+  unsigned long long mv_seg;
   long long rays_moved, crossings, split, merged, killed, cast;
   double emitted, deposited, killed_ph, overlap, in_flight;
 };
@@ -67,6 +67,7 @@ struct Dev {
   float spectrum[FRT_MAX_FREQ];
   double sigH1_d[FRT_MAX_FREQ], sigHe1_d[FRT_MAX_FREQ];
   float sigH1_f[FRT_MAX_FREQ], sigHe1_f[FRT_MAX_FREQ];
+  float sigH1_l2[FRT_MAX_FREQ], sigHe1_l2[FRT_MAX_FREQ];   // the same times log2(e)
   double sigH1_0, sigH1_912;
   // tables
   const float* rot;        // [kNtheta][2][9] forward, inverse
@@ -82,20 +83,24 @@ struct Dev {
   // lit cells
   int* l_cell;
   float *l_nh, *l_nhe, *l_y0h, *l_y0he, *l_crec_h, *l_crec_he, *l_rec_h2, *l_rec_he2;
-  float *l_avg_h, *l_avg_he, *l_nh1_old, *l_acc_g, *l_acc_ghe;
+  float* l_nh1_old;
+  // pairs (H, He) side by side: a crossing gathers both averages in one 8-byte load and adds both
+  // rates in one vector reduction
+  float2* l_avg;           // iteration-averaged (n_HI, n_HeI)
+  float2* l_acc;           // (Gamma_HI, Gamma_HeI) summed over the crossings of this iteration
+  float2* l_heat;          // bin-weighted photo-heating sums (HI, HeI) (mixed, core outputs)
   float *l_acc_nu_h, *l_acc_nu_he, *l_ngam;   // [F][lit_cap]
-  float *l_heat_h, *l_heat_he;              // bin-weighted photo-heating sums (mixed, core outputs)
   int per_bin;                               // keep per-bin rates (diag outputs or strict)
   float cH1_f[FRT_MAX_FREQ], cHe1_f[FRT_MAX_FREQ];  // h (h_eV nu - Eth)/h_eV
   // rays
   RayPool pool[2];
   int2* segs;              // [ray_cap][PL] {cell (then lit slot), dist bits}: a ray's segments contiguous
   uint8_t* nseg;
-  int* moved;              // rays with segments this step (appended by k_advance)
+  int4* mv_hdr;            // [ray_cap] moved ray q: {pool index, first packed segment, segments, box}
+  int2* pk;                // [ray_cap][PL] packed segments {lit slot, dist bits | head bit}, moved-list order
   uint8_t* dead;
   int* ray_bin;            // merge bin of a candidate or -1
   uint8_t* merged_flag;
-  int2* split_list;         // (parent ray, first child slot) of the rays split this step
   int* bin_base;           // [ncell_total * 12*4^lm] or NULL when merging is unreachable
   // sources
   int* src_cell;           // local cell

@@ -35,27 +35,23 @@ __device__ __forceinline__ T block_sum(T v) {
 
 __device__ __forceinline__ int box_of_cell(const Dev& d, long long gc) { return d.tile_box[gc >> kTileShift]; }
 
-// 1 - e^-x and e^-x, both to full relative precision, for one transcendental: for x > 0.5 the
-// transmission is formed directly and the absorbed part as 1 - e (>= 0.39, no cancellation);
-// below, the absorbed part is the Taylor series of 1 - e^-x = x - x^2/2! + x^3/3! - ... to the
-// x^8 term (alternating with decreasing terms for x <= 0.5: truncation below 0.5^8/9! ~ 1e-11
-// relative) and the transmission is 1 - a (>= 0.61).
-__device__ __forceinline__ void absorb_transmit(float x, float* a, float* e) {
-  if (x > 0.5f) {
-    *e = expf(-x);
-    *a = 1.0f - *e;
-  } else {
-    float p = -1.0f / 40320.0f;
-    p = fmaf(p, x, 1.0f / 5040.0f);
-    p = fmaf(p, x, -1.0f / 720.0f);
-    p = fmaf(p, x, 1.0f / 120.0f);
-    p = fmaf(p, x, -1.0f / 24.0f);
-    p = fmaf(p, x, 1.0f / 6.0f);
-    p = fmaf(p, x, -0.5f);
-    p = fmaf(p, x, 1.0f);
-    *a = x * p;
-    *e = 1.0f - *a;
-  }
+// 1 - e^-x and e^-x of one optical depth x >= 0 (xl = x log2(e)). Below x = 1/4 the absorbed
+// part is the Taylor series of 1 - e^-x = x - x^2/2! + x^3/3! - ... to the x^6 term (alternating
+// with decreasing terms: truncation below 0.25^6/7! ~ 5e-8 relative) and the transmission is
+// 1 - a (>= 0.77); above, the transmission is exp2(-xl) and the absorbed part 1 - e (e <= 0.78,
+// so the subtraction costs under 3 bits). Both forms are evaluated and one is selected, so the
+// lanes of a warp never split on the optical depth.
+__device__ __forceinline__ void absorb_transmit(float x, float xl, float* a, float* e) {
+  const float ex = exp2f(-xl);
+  float p = fmaf(x, -1.0f / 720.0f, 1.0f / 120.0f);
+  p = fmaf(p, x, -1.0f / 24.0f);
+  p = fmaf(p, x, 1.0f / 6.0f);
+  p = fmaf(p, x, -0.5f);
+  p = fmaf(p, x, 1.0f);
+  const float at = x * p;
+  const bool small = x <= 0.25f;
+  *a = small ? at : 1.0f - ex;
+  *e = small ? 1.0f - at : ex;
 }
 
 // ---- clear the previous step's lit marks ------------------------------------------------
@@ -88,13 +84,10 @@ __global__ void k_lit_init(Dev d) {
     d.l_crec_h[s] = cl * rh;
     d.l_crec_he[s] = cl * rhe;
     const float nh1 = d.nH1[gc];
-    d.l_avg_h[s] = nh1;
+    d.l_avg[s] = make_float2(nh1, d.nHe1[gc]);
     d.l_nh1_old[s] = nh1;
-    d.l_avg_he[s] = d.nHe1[gc];
-    d.l_acc_g[s] = 0.f;
-    d.l_acc_ghe[s] = 0.f;
-    d.l_heat_h[s] = 0.f;
-    d.l_heat_he[s] = 0.f;
+    d.l_acc[s] = make_float2(0.f, 0.f);
+    d.l_heat[s] = make_float2(0.f, 0.f);
     if (STRICT || d.per_bin)
       for (int nu = 0; nu < F; nu++) {
         d.l_ngam[(size_t)nu * L + s] = 0.f;
@@ -105,37 +98,24 @@ __global__ void k_lit_init(Dev d) {
 }
 
 // ---- ray pass of one C2Ray iteration (ray_tracing.cc:701-938), plain mode ------------------
-// The moved rays (the list k_advance builds) walk their stored segments, attenuate the photon
-// count per bin with the current time-averaged neutral densities of the lit cells, and deposit
-// Gamma_HI / HeI (the segments hold lit slots, k_seg_slots); LAST also writes the per-bin output
-// fields (diag), the new photon counts, and removes rays below nphot_min.
-
-// The segments' cell indices become lit slots once per step, before the first ray pass: one
-// thread per moved ray, whose segments are contiguous.
-__global__ void __launch_bounds__(256) k_seg_slots(Dev d) {
-  const int nmv = min(d.ctl->n_moved, d.ray_cap);
-  const int PL = d.PL;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nmv; q += gridDim.x * blockDim.x) {
-    const int i = d.moved[q];
-    const int ns = d.nseg[i];
-    int2* sp = d.segs + (size_t)i * PL;
-    for (int p = 0; p < ns; p++) sp[p].x = d.lit_slot[sp[p].x];
-  }
-}
+// The moved rays walk their packed segments (k_moved_pack: lit slot + path length, in moved-list
+// order), attenuate the photon count per bin with the current time-averaged neutral densities of
+// the lit cells, and deposit Gamma_HI / HeI; LAST also writes the per-bin output fields (diag),
+// the new photon counts, and removes rays below nphot_min.
 
 // Strict precision: the reference's double expressions, one thread per moved ray.
 template <bool LAST>
 __global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
-  const int nmv = min(d.ctl->n_moved, d.ray_cap);
+  const int nmv = min((int)(d.ctl->mv_seg >> 32), d.ray_cap);
   const RayPool A = d.pool[d.ctl->cur];
-  const int cap = d.ray_cap, F = d.F, L = d.lit_cap, PL = d.PL;
+  const int cap = d.ray_cap, F = d.F, L = d.lit_cap;
   double dep = 0.0, kil = 0.0, ovl = 0.0;
   long long nkill = 0;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nmv; q += gridDim.x * blockDim.x) {
-    const int i = d.moved[q];
-    const int ns = d.nseg[i];
-    const int2* sp = d.segs + (size_t)i * PL;
-    const BoxP& B = d.box[A.box[i]];
+    const int4 hd = d.mv_hdr[q];
+    const int i = hd.x, ns = hd.z;
+    const int2* sp = d.pk + hd.y;
+    const BoxP& B = d.box[hd.w];
     const double nmin = B.nphot_min;
     float nph[FRT_MAX_FREQ];
     for (int nu = 0; nu < F; nu++) nph[nu] = A.nphot[(size_t)nu * cap + i];
@@ -148,8 +128,9 @@ __global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
       const int2 sg = sp[p];
       const int slot = sg.x;
       if (slot < 0) continue;
-      const float dist = __int_as_float(sg.y);
-      const float a = d.l_avg_h[slot], b = d.l_avg_he[slot];
+      const float dist = __int_as_float(sg.y & 0x7fffffff);
+      const float2 av = d.l_avg[slot];
+      const float a = av.x, b = av.y;
       double dth[FRT_MAX_FREQ], dthe[FRT_MAX_FREQ], nin[FRT_MAX_FREQ];
       double total = 0.;
       for (int nu = 0; nu < F; nu++) {
@@ -169,8 +150,7 @@ __global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
         const double absb = dump ? 1.0 : (1. - exp(-dth[nu] - dthe[nu]));
         const float gh = (float)(fh * nin[nu] * absb / dt / vol / a);
         const float ghe = (float)(fhe * nin[nu] * absb / dt / vol / b);
-        atomicAdd(&d.l_acc_g[slot], gh);
-        atomicAdd(&d.l_acc_ghe[slot], ghe);
+        atomicAdd(&d.l_acc[slot], make_float2(gh, ghe));
         if (LAST) {
           atomicAdd(&d.l_ngam[(size_t)nu * L + slot], (float)(nin[nu] / kPhotNorm));
           atomicAdd(&d.l_acc_nu_h[(size_t)nu * L + slot], gh);
@@ -217,20 +197,23 @@ __global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
 // Mixed precision, persistent lanes. Rays have 1..path_length segments, so one ray per thread
 // leaves most lanes of a warp idle behind its longest ray. Here every warp owns a contiguous slice
 // of the moved list and a lane takes the slice's next ray as soon as its own ray ends (a ballot
-// and a warp-uniform cursor, no atomics), so every lane walks a segment in every loop trip; a
-// ray's segments are contiguous, so a lane's walk stays in one or two cache lines. Per bin the
-// photon count is carried from segment to segment by its transmission e^-dtau instead of
-// recomputing e^-tau, and each bin costs one transcendental when HeI does not absorb there
-// (sigma_HeI = 0 below 24.59 eV) and two when it does.
+// and a warp-uniform cursor, no atomics), so every lane walks a segment in every loop trip. A
+// ray's header (pool index, packed segments, count, box) is one 16-byte load and its segments are
+// contiguous; the loads run two segments ahead of the arithmetic (the next segment's cell state,
+// the segment after it), so a lane's gathers are in flight while it works the current segment.
+// Per bin the photon count is carried from segment to segment by its transmission e^-dtau, and
+// each bin costs one exp2 when HeI does not absorb there (sigma_HeI = 0 below 24.59 eV) and two
+// when it does.
 // NF > 0 fixes the number of frequency bins at compile time (the 5-bin spectrum of every
 // configuration here), so the per-bin loops unroll exactly; NF = 0 takes d.F at run time.
 template <bool LAST, int NF>
 __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
   constexpr int MAXF = NF > 0 ? NF : FRT_MAX_FREQ;
+  constexpr unsigned FULL = 0xffffffffu;
   const int Fr = NF > 0 ? NF : d.F;
-  const int nmv = min(d.ctl->n_moved, d.ray_cap);
+  const int nmv = min((int)(d.ctl->mv_seg >> 32), d.ray_cap);
   const RayPool A = d.pool[d.ctl->cur];
-  const int cap = d.ray_cap, L = d.lit_cap, PL = d.PL;
+  const int cap = d.ray_cap, L = d.lit_cap;
   const int lane = threadIdx.x & 31;
   const unsigned lanes_below = (1u << lane) - 1u;
   // this warp's slice [cursor, slice_end) of the moved list
@@ -245,43 +228,61 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
   bool exhausted = false, dumped = false;
   unsigned dump_mask = 0;
   float nin[MAXF];
+#pragma unroll
+  for (int nu = 0; nu < MAXF; nu++) nin[nu] = 0.f;
   float kdep = 0.f;
   double nmin = 0.0;
   const int2* sp = nullptr;
+  int2 sg0 = make_int2(-1, 0), sg1 = make_int2(-1, 0);   // segments p and p + 1
+  float2 av0 = make_float2(0.f, 0.f);                     // cell state of segment p
   while (true) {
     // refill the lanes whose ray ended
     const bool need = (i < 0) && !exhausted;
-    const unsigned m = __ballot_sync(0xffffffffu, need);
+    const unsigned m = __ballot_sync(FULL, need);
     if (m) {
       const long long q = cursor + __popc(m & lanes_below);
       cursor += __popc(m);
       if (need) {
         if (q < slice_end) {
-          i = d.moved[q];
-          ns = d.nseg[i];
+          const int4 hd = d.mv_hdr[q];
+          i = hd.x;
+          sp = d.pk + hd.y;
+          ns = hd.z;
           p = 0;
           dumped = false;
           dump_mask = 0;
-          sp = d.segs + (size_t)i * PL;
-          const BoxP& B = d.box[A.box[i]];
+          const BoxP& B = d.box[hd.w];
           kdep = B.kdep_f;
           nmin = B.nphot_min;
+          sg0 = sp[0];
+          sg1 = (ns > 1) ? sp[1] : make_int2(-1, 0);
 #pragma unroll
           for (int nu = 0; nu < MAXF; nu++) nin[nu] = (nu < Fr) ? A.nphot[(size_t)nu * cap + i] : 0.f;
+          av0 = (sg0.x >= 0 && sg0.x < L) ? d.l_avg[sg0.x] : make_float2(0.f, 0.f);
         } else {
           exhausted = true;
         }
       }
     }
-    if (__all_sync(0xffffffffu, i < 0)) break;
+    if (__all_sync(FULL, i < 0)) break;
     if (i < 0) continue;
-    // one segment of ray i
-    const int2 sg = sp[p];
-    const int slot = sg.x;
+    // one segment of ray i; the loads of the next two are issued first
+    const int2 sg = sg0;
+    const float2 av = av0;
     bool done = (p + 1 >= ns);
-    if (slot >= 0) {
-      const float dist = __int_as_float(sg.y);
-      const float a = d.l_avg_h[slot], b = d.l_avg_he[slot];
+    {
+      float2 av_n = make_float2(0.f, 0.f);
+      if (!done && sg1.x >= 0 && sg1.x < L) av_n = d.l_avg[sg1.x];
+      int2 sg_n = make_int2(-1, 0);
+      if (p + 2 < ns) sg_n = sp[p + 2];
+      sg0 = sg1;
+      av0 = av_n;
+      sg1 = sg_n;
+    }
+    const int slot = sg.x;
+    if (slot >= 0 && slot < L) {
+      const float dist = __int_as_float(sg.y & 0x7fffffff);
+      const float a = av.x, b = av.y;
       float total = 0.f;
 #pragma unroll
       for (int nu = 0; nu < MAXF; nu++) total += (nu < Fr) ? nin[nu] : 0.f;
@@ -293,11 +294,11 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
         const float dth = (a * d.sigH1_f[nu]) * dist;
         const float dthe = (b * d.sigHe1_f[nu]) * dist;
         float ah, eh;
-        absorb_transmit(dth, &ah, &eh);
+        absorb_transmit(dth, (a * d.sigH1_l2[nu]) * dist, &ah, &eh);
         float fh, fhe, absb, e;
         if (dthe > 0.f) {
           float ahe, ehe;
-          absorb_transmit(dthe, &ahe, &ehe);
+          absorb_transmit(dthe, (b * d.sigHe1_l2[nu]) * dist, &ahe, &ehe);
           e = eh * ehe;
           absb = ah + eh * ahe;                   // 1 - e^-(dth+dthe) without cancellation
           // frac_h1 = A e^-b / (A e^-b + B e^-a) (ray_tracing.cc:770-771)
@@ -321,8 +322,8 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
           fh = (dth > 0.f) ? 1.0f : 0.0f;           // frac_h1 = 1, frac_he1 = 0 when dtau_he1 = 0
           fhe = 0.f;
         }
-        const float q = nin[nu] * (dump ? 1.0f : absb);
-        const float gh = fh * q, ghe = fhe * q;
+        const float qv = nin[nu] * (dump ? 1.0f : absb);
+        const float gh = fh * qv, ghe = fhe * qv;
         gsum_h += gh;
         gsum_he += ghe;
         if (LAST) {
@@ -339,12 +340,12 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
         nin[nu] *= e;
       }
       const float wh = __fdividef(kdep, a), whe = __fdividef(kdep, b);
-      if (gsum_h != 0.f) atomicAdd(&d.l_acc_g[slot], gsum_h * wh);
-      if (gsum_he != 0.f) atomicAdd(&d.l_acc_ghe[slot], gsum_he * whe);
+      if (gsum_h != 0.f || gsum_he != 0.f)
+        atomicAdd(&d.l_acc[slot], make_float2(gsum_h != 0.f ? gsum_h * wh : 0.f, gsum_he != 0.f ? gsum_he * whe : 0.f));
       if (LAST) {
         // photo-heating weights sum_nu Gamma_nu h (h_eV nu - Eth)/h_eV (gas_funcs.cc:155-158)
-        if (hh != 0.f) atomicAdd(&d.l_heat_h[slot], hh * wh);
-        if (hhe != 0.f) atomicAdd(&d.l_heat_he[slot], hhe * whe);
+        if (hh != 0.f || hhe != 0.f)
+          atomicAdd(&d.l_heat[slot], make_float2(hh != 0.f ? hh * wh : 0.f, hhe != 0.f ? hhe * whe : 0.f));
         dep += (double)gsum_h + (double)gsum_he;
       }
       if (dump) {
@@ -435,8 +436,9 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d) {
     const int gc = d.l_cell[s];
     const BoxP& B = d.box[box_of_cell(d, gc)];
     const float dt = B.dt;
-    const float g = d.l_acc_g[s], ghe = d.l_acc_ghe[s];
-    const float a_prev = d.l_avg_h[s], b_prev = d.l_avg_he[s];
+    const float2 acc = d.l_acc[s], av = d.l_avg[s];
+    const float g = acc.x, ghe = acc.y;
+    const float a_prev = av.x, b_prev = av.y;
     const float nH = d.l_nh[s], nHe = d.l_nhe[s];
     const float nelec_f = nH - a_prev + nHe - b_prev;
     const double nelec_d = (double)nelec_f;
@@ -446,10 +448,8 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d) {
     const float a_new = c2ray_species<STRICT>(H, g, nelec_d, nelec_f, a_prev, dt, LAST, &nh1_end);
     const float b_new = c2ray_species<STRICT>(He, ghe, nelec_d, nelec_f, b_prev, dt, LAST, &nhe1_end);
     if (!LAST) {
-      d.l_avg_h[s] = a_new;
-      d.l_avg_he[s] = b_new;
-      d.l_acc_g[s] = 0.f;
-      d.l_acc_ghe[s] = 0.f;
+      d.l_avg[s] = make_float2(a_new, b_new);
+      d.l_acc[s] = make_float2(0.f, 0.f);
       continue;
     }
     const bool flag = d.treion_flag[gc] != 0;
@@ -495,8 +495,9 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d) {
       HeatSrc hs{d.l_acc_nu_h + s, d.l_acc_nu_he + s, L, 0.f, 0.f, 1};
       if (!STRICT && !d.per_bin) {
         hs.mode = 2;
-        hs.hh = d.l_heat_h[s];
-        hs.hhe = d.l_heat_he[s];
+        const float2 ht = d.l_heat[s];
+        hs.hh = ht.x;
+        hs.hhe = ht.y;
       }
       thermal_update<STRICT>(c, B.th, hs, d.F, d.nhe_to_nh);
       d.temp[gc] = c.temp;
@@ -643,7 +644,7 @@ __global__ void __launch_bounds__(256) k_thermal_all(Dev d) {
     const int slot = d.lit_slot[gc];
     HeatSrc hs{nullptr, nullptr, 0, 0.f, 0.f, 0};
     if (slot >= 0) {
-      if (!STRICT && !d.per_bin) hs = HeatSrc{nullptr, nullptr, 0, d.l_heat_h[slot], d.l_heat_he[slot], 2};
+      if (!STRICT && !d.per_bin) hs = HeatSrc{nullptr, nullptr, 0, d.l_heat[slot].x, d.l_heat[slot].y, 2};
       else hs = HeatSrc{d.l_acc_nu_h + slot, d.l_acc_nu_he + slot, L, 0.f, 0.f, 1};
     }
     thermal_update<STRICT>(c, B.th, hs, d.F, d.nhe_to_nh);
@@ -665,8 +666,8 @@ __global__ void k_gather_sparse(Dev d, long long cell0, long long ncell, int whi
     const int slot = d.lit_slot[cell0 + c];
     float v = 0.f;
     if (slot >= 0) {
-      if (which == 0) v = d.l_acc_g[slot];
-      else if (which == 1) v = d.l_acc_ghe[slot];
+      if (which == 0) v = d.l_acc[slot].x;
+      else if (which == 1) v = d.l_acc[slot].y;
       else if (which < 2 + F) v = d.l_acc_nu_h[(size_t)(which - 2) * L + slot];
       else if (which < 2 + 2 * F) v = d.l_acc_nu_he[(size_t)(which - 2 - F) * L + slot];
       else v = d.l_ngam[(size_t)(which - 2 - 2 * F) * L + slot];
@@ -687,7 +688,6 @@ void launch_lit_init(const Dev& d, bool strict, int grid, cudaStream_t s) {
 
 void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t s) {
   const bool last = iter == d.itercount - 1;
-  if (iter == 0) k_seg_slots<<<grid, 256, 0, s>>>(d);
   if (strict) {
     if (last) k_raypass_strict<true><<<grid, 256, 0, s>>>(d);
     else k_raypass_strict<false><<<grid, 256, 0, s>>>(d);
