@@ -38,11 +38,17 @@ __device__ __forceinline__ int box_of_cell(const Dev& d, long long gc) { return 
 // 1 - e^-x and e^-x of one optical depth x >= 0 (xl = x log2(e)). Below x = 1/4 the absorbed
 // part is the Taylor series of 1 - e^-x = x - x^2/2! + x^3/3! - ... to the x^6 term (alternating
 // with decreasing terms: truncation below 0.25^6/7! ~ 5e-8 relative) and the transmission is
-// 1 - a (>= 0.77); above, the transmission is exp2(-xl) and the absorbed part 1 - e (e <= 0.78,
+// 1 - a (>= 0.77); above, the transmission is 2^-xl and the absorbed part 1 - e (e <= 0.78,
 // so the subtraction costs under 3 bits). Both forms are evaluated and one is selected, so the
 // lanes of a warp never split on the optical depth.
+__device__ __forceinline__ float ex2_approx(float x) {   // 2^x, hardware approximation (~2 ulp), flushes tiny results to 0
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 __device__ __forceinline__ void absorb_transmit(float x, float xl, float* a, float* e) {
-  const float ex = exp2f(-xl);
+  const float ex = ex2_approx(-xl);
   float p = fmaf(x, -1.0f / 720.0f, 1.0f / 120.0f);
   p = fmaf(p, x, -1.0f / 24.0f);
   p = fmaf(p, x, 1.0f / 6.0f);
@@ -230,8 +236,7 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
   float nin[MAXF];
 #pragma unroll
   for (int nu = 0; nu < MAXF; nu++) nin[nu] = 0.f;
-  float kdep = 0.f;
-  double nmin = 0.0;
+  float kdep = 0.f, nmin_ru = 0.f, nmin_rd = 0.f;
   const int2* sp = nullptr;
   int2 sg0 = make_int2(-1, 0), sg1 = make_int2(-1, 0);   // segments p and p + 1
   float2 av0 = make_float2(0.f, 0.f);                     // cell state of segment p
@@ -253,7 +258,10 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
           dump_mask = 0;
           const BoxP& B = d.box[hd.w];
           kdep = B.kdep_f;
-          nmin = B.nphot_min;
+          // (double)x < nphot_min <=> x < nmin_ru and (double)x > nphot_min <=> x > nmin_rd for a
+          // float x, with nphot_min rounded up / down to float
+          nmin_ru = __double2float_ru(B.nphot_min);
+          nmin_rd = __double2float_rd(B.nphot_min);
           sg0 = sp[0];
           sg1 = (ns > 1) ? sp[1] : make_int2(-1, 0);
 #pragma unroll
@@ -286,19 +294,20 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
       float total = 0.f;
 #pragma unroll
       for (int nu = 0; nu < MAXF; nu++) total += (nu < Fr) ? nin[nu] : 0.f;
-      const bool dump = (double)total < nmin;
+      const bool dump = total < nmin_ru;
+      const float ad = a * dist, bd = b * dist;   // column densities of the segment
       float gsum_h = 0.f, gsum_he = 0.f, hh = 0.f, hhe = 0.f;
 #pragma unroll
       for (int nu = 0; nu < MAXF; nu++) {
         if (nu >= Fr) continue;
-        const float dth = (a * d.sigH1_f[nu]) * dist;
-        const float dthe = (b * d.sigHe1_f[nu]) * dist;
+        const float dth = ad * d.sigH1_f[nu];
+        const float dthe = bd * d.sigHe1_f[nu];
         float ah, eh;
-        absorb_transmit(dth, (a * d.sigH1_l2[nu]) * dist, &ah, &eh);
+        absorb_transmit(dth, ad * d.sigH1_l2[nu], &ah, &eh);
         float fh, fhe, absb, e;
         if (dthe > 0.f) {
           float ahe, ehe;
-          absorb_transmit(dthe, (b * d.sigHe1_l2[nu]) * dist, &ahe, &ehe);
+          absorb_transmit(dthe, bd * d.sigHe1_l2[nu], &ahe, &ehe);
           e = eh * ehe;
           absb = ah + eh * ahe;                   // 1 - e^-(dth+dthe) without cancellation
           // frac_h1 = A e^-b / (A e^-b + B e^-a) (ray_tracing.cc:770-771)
@@ -339,13 +348,11 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
         }
         nin[nu] *= e;
       }
-      const float wh = __fdividef(kdep, a), whe = __fdividef(kdep, b);
-      if (gsum_h != 0.f || gsum_he != 0.f)
-        atomicAdd(&d.l_acc[slot], make_float2(gsum_h != 0.f ? gsum_h * wh : 0.f, gsum_he != 0.f ? gsum_he * whe : 0.f));
+      // absorbed photons of the crossing; k_litpass applies the rate weight kdep / <n> per cell
+      if (gsum_h != 0.f || gsum_he != 0.f) atomicAdd(&d.l_acc[slot], make_float2(gsum_h, gsum_he));
       if (LAST) {
         // photo-heating weights sum_nu Gamma_nu h (h_eV nu - Eth)/h_eV (gas_funcs.cc:155-158)
-        if (hh != 0.f || hhe != 0.f)
-          atomicAdd(&d.l_heat[slot], make_float2(hh != 0.f ? hh * wh : 0.f, hhe != 0.f ? hhe * whe : 0.f));
+        if (hh != 0.f || hhe != 0.f) atomicAdd(&d.l_heat[slot], make_float2(hh, hhe));
         dep += (double)gsum_h + (double)gsum_he;
       }
       if (dump) {
@@ -365,7 +372,7 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
           A.nphot[(size_t)nu * cap + i] = nin[nu];
           s += nin[nu];
         }
-        if (!((double)s > nmin)) {
+        if (!(s > nmin_rd)) {
           d.dead[i] = 1;
           nkill += 1;
           kil += (double)s;
@@ -437,8 +444,18 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d) {
     const BoxP& B = d.box[box_of_cell(d, gc)];
     const float dt = B.dt;
     const float2 acc = d.l_acc[s], av = d.l_avg[s];
-    const float g = acc.x, ghe = acc.y;
     const float a_prev = av.x, b_prev = av.y;
+    // mixed precision: the ray pass sums the absorbed photons of a cell's crossings and the rate
+    // weight kdep / <n> (ray_tracing.cc:787-790), the same for every crossing of the cell in this
+    // iteration, is applied here once (strict: the ray pass deposits the reference's rates)
+    float g = acc.x, ghe = acc.y;
+    float wh = 0.f, whe = 0.f;
+    if (!STRICT) {
+      wh = __fdividef(B.kdep_f, a_prev);
+      whe = __fdividef(B.kdep_f, b_prev);
+      g = (acc.x != 0.f) ? acc.x * wh : 0.f;
+      ghe = (acc.y != 0.f) ? acc.y * whe : 0.f;
+    }
     const float nH = d.l_nh[s], nHe = d.l_nhe[s];
     const float nelec_f = nH - a_prev + nHe - b_prev;
     const double nelec_d = (double)nelec_f;
@@ -451,6 +468,12 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d) {
       d.l_avg[s] = make_float2(a_new, b_new);
       d.l_acc[s] = make_float2(0.f, 0.f);
       continue;
+    }
+    if (!STRICT) {
+      // the step's outputs keep the rates: Gamma and the bin-weighted heating sums, weighted
+      const float2 ht = d.l_heat[s];
+      d.l_acc[s] = make_float2(g, ghe);
+      d.l_heat[s] = make_float2((ht.x != 0.f) ? ht.x * wh : 0.f, (ht.y != 0.f) ? ht.y * whe : 0.f);
     }
     const bool flag = d.treion_flag[gc] != 0;
     const float ne_old = d.ne[gc];
