@@ -47,10 +47,10 @@ DARK_TRAFFIC_BYTES_PER_CELL = 1342312448 / 13264000
 # Ray pass (the dominant kernel): the algorithmic bytes of one crossing in one C2Ray iteration as
 # the hot-path analysis counts them -- 8 B segment read, 8 B of gathered <n_HI>, <n_HeI>, 68 B of
 # deposits (2 + 3 x 5 floats) -- and the ncu DRAM bytes (read + write) per crossing of one launch,
-# the mean over the 5 passes of step 24 of L (17 465 926 crossings per pass; 1160.4 MB per launch).
+# the mean over the 5 passes of step 24 of L (17 465 925 crossings per pass; 676.1 MB per launch).
 ITERCOUNT = 5
 RAYPASS_BYTES_PER_CROSSING = 8 + 8 + 68
-RAYPASS_TRAFFIC_BYTES_PER_CROSSING = 66.4
+RAYPASS_TRAFFIC_BYTES_PER_CROSSING = 38.7
 
 
 def _peaks():
