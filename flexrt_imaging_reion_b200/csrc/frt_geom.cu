@@ -212,6 +212,16 @@ __global__ void __launch_bounds__(256) k_moved_pack(Dev d) {
     const int i = i0 + threadIdx.x;
     const bool take = (i < n) && d.nseg[i] > 0 && !d.dead[i];
     const int ns = take ? (int)d.nseg[i] : 0;
+    // the first kHeld segments and their lit slots, loaded before the scan so that the gathers
+    // are in flight while the block scans
+    constexpr int kHeld = 8;
+    const int2* sp = d.segs + (size_t)(take ? i : 0) * PL;
+    int2 sg[kHeld];
+    int sl[kHeld];
+#pragma unroll
+    for (int p = 0; p < kHeld; p++) sg[p] = (p < ns) ? sp[p] : make_int2(0, 0);
+#pragma unroll
+    for (int p = 0; p < kHeld; p++) sl[p] = (p < ns) ? d.lit_slot[sg[p].x] : -1;
     const unsigned m = __ballot_sync(0xffffffffu, take);
     int x = ns;   // inclusive scan of the segment counts over the warp
 #pragma unroll
@@ -246,12 +256,14 @@ __global__ void __launch_bounds__(256) k_moved_pack(Dev d) {
       const int q = (int)(base_s >> 32) + (w > 0 ? wt[w - 1] : 0) + __popc(m & below);
       const int off = (int)(base_s & 0xffffffffull) + (w > 0 ? ws[w - 1] : 0) + (x - ns);
       d.mv_hdr[q] = make_int4(i, off, ns, (int)rbox[i]);
-      const int2* sp = d.segs + (size_t)i * PL;
       int2* dp = d.pk + off;
-      for (int p = 0; p < ns; p++) {
+      // dist > 0: its sign bit is free for the head mark
+#pragma unroll
+      for (int p = 0; p < kHeld; p++)
+        if (p < ns) dp[p] = make_int2(sl[p], (int)(((unsigned)sg[p].y & 0x7fffffffu) | (p == 0 ? 0x80000000u : 0u)));
+      for (int p = kHeld; p < ns; p++) {
         const int2 c = sp[p];
-        // dist > 0: its sign bit is free for the head mark
-        dp[p] = make_int2(d.lit_slot[c.x], (int)(((unsigned)c.y & 0x7fffffffu) | (p == 0 ? 0x80000000u : 0u)));
+        dp[p] = make_int2(d.lit_slot[c.x], (int)((unsigned)c.y & 0x7fffffffu));
       }
     }
     __syncthreads();

@@ -77,20 +77,22 @@ __global__ void k_lit_init(Dev d) {
   const int F = d.F, L = d.lit_cap;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
     const int gc = d.l_cell[s];
+    // every load of the cell first, then the stores (the loads overlap)
     const float temp = d.temp[gc];
+    const float cl = d.clump ? d.clump[gc] : d.const_clump;
+    const float nh = d.nH[gc], nhe = d.nHe[gc], y0h = d.f_H1[gc], y0he = d.f_He1[gc];
+    const float nh1 = d.nH1[gc], nhe1 = d.nHe1[gc];
     float rh, rhe;
     recomb_coeffs<STRICT>(temp, &rh, &rhe);
-    const float cl = d.clump ? d.clump[gc] : d.const_clump;
-    d.l_nh[s] = d.nH[gc];
-    d.l_nhe[s] = d.nHe[gc];
-    d.l_y0h[s] = d.f_H1[gc];
-    d.l_y0he[s] = d.f_He1[gc];
+    d.l_nh[s] = nh;
+    d.l_nhe[s] = nhe;
+    d.l_y0h[s] = y0h;
+    d.l_y0he[s] = y0he;
     d.l_rec_h2[s] = rh;
     d.l_rec_he2[s] = rhe;
     d.l_crec_h[s] = cl * rh;
     d.l_crec_he[s] = cl * rhe;
-    const float nh1 = d.nH1[gc];
-    d.l_avg[s] = make_float2(nh1, d.nHe1[gc]);
+    d.l_avg[s] = make_float2(nh1, nhe1);
     d.l_nh1_old[s] = nh1;
     d.l_acc[s] = make_float2(0.f, 0.f);
     d.l_heat[s] = make_float2(0.f, 0.f);
@@ -445,6 +447,21 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d) {
     const float dt = B.dt;
     const float2 acc = d.l_acc[s], av = d.l_avg[s];
     const float a_prev = av.x, b_prev = av.y;
+    // the last pass's dense-cell inputs, loaded before any store so that all loads overlap
+    bool flag = false;
+    float ne_old = 0.f, nh1_old = 0.f, t_old = 0.f, heat_old = 0.f, cool_old = 0.f;
+    float2 ht = make_float2(0.f, 0.f);
+    if (LAST) {
+      flag = d.treion_flag[gc] != 0;
+      ne_old = d.ne[gc];
+      nh1_old = d.l_nh1_old[s];
+      if (!STRICT) ht = d.l_heat[s];
+      if (THERMAL) {
+        t_old = d.temp[gc];
+        heat_old = d.heat[gc];
+        cool_old = d.cool[gc];
+      }
+    }
     // mixed precision: the ray pass sums the absorbed photons of a cell's crossings and the rate
     // weight kdep / <n> (ray_tracing.cc:787-790), the same for every crossing of the cell in this
     // iteration, is applied here once (strict: the ray pass deposits the reference's rates)
@@ -471,12 +488,10 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d) {
     }
     if (!STRICT) {
       // the step's outputs keep the rates: Gamma and the bin-weighted heating sums, weighted
-      const float2 ht = d.l_heat[s];
+      ht = make_float2((ht.x != 0.f) ? ht.x * wh : 0.f, (ht.y != 0.f) ? ht.y * whe : 0.f);
       d.l_acc[s] = make_float2(g, ghe);
-      d.l_heat[s] = make_float2((ht.x != 0.f) ? ht.x * wh : 0.f, (ht.y != 0.f) ? ht.y * whe : 0.f);
+      d.l_heat[s] = ht;
     }
-    const bool flag = d.treion_flag[gc] != 0;
-    const float ne_old = d.ne[gc];
     const Final f = finalize<STRICT>(nH, nHe, nh1_end, nhe1_end, a_new, ne_old, dt, flag);
     if (f.set_treion) {
       d.treion[gc] = B.t;
@@ -501,12 +516,12 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d) {
     }
     if (THERMAL) {
       ThermCell c;
-      c.temp = d.temp[gc];
-      c.heat = d.heat[gc];
-      c.cool = d.cool[gc];
+      c.temp = t_old;
+      c.heat = heat_old;
+      c.cool = cool_old;
       c.nH = nH;
       c.nH1 = f.nH1;
-      c.nH1_prev = d.l_nh1_old[s];
+      c.nH1_prev = nh1_old;
       c.nH2 = f.nH2;
       c.nHe2 = f.nHe2;
       c.ne = f.ne;
@@ -518,7 +533,6 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d) {
       HeatSrc hs{d.l_acc_nu_h + s, d.l_acc_nu_he + s, L, 0.f, 0.f, 1};
       if (!STRICT && !d.per_bin) {
         hs.mode = 2;
-        const float2 ht = d.l_heat[s];
         hs.hh = ht.x;
         hs.hhe = ht.y;
       }
@@ -531,7 +545,7 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d) {
         d.inc_flux[gc] = c.inc_flux;
       }
     } else {
-      d.nH1_prev[gc] = d.l_nh1_old[s];
+      d.nH1_prev[gc] = nh1_old;
       d.n_tot[gc] = f.n_tot;
       d.dne_dt[gc] = f.dne_dt;
     }
@@ -558,6 +572,10 @@ __global__ void __launch_bounds__(256, 4) k_dark(Dev d) {
     const float nh1 = d.nH1[gc], nhe1 = d.nHe1[gc];
     const float temp0 = d.temp[gc];
     const float cl = d.clump ? d.clump[gc] : d.const_clump;
+    // the inputs of the bookkeeping and the thermal update, loaded before any store
+    const bool flag = d.treion_flag[gc] != 0;
+    const float ne_old = d.ne[gc];
+    const float heat_old = THERMAL ? d.heat[gc] : 0.f, cool_old = THERMAL ? d.cool[gc] : 0.f;
     float rh, rhe;
     recomb_coeffs<STRICT>(temp0, &rh, &rhe);
     const C2Species H{nH, d.f_H1[gc], cl * rh};
@@ -580,8 +598,6 @@ __global__ void __launch_bounds__(256, 4) k_dark(Dev d) {
       bb = bn;
       nelec_last = nelec_d;
     }
-    const bool flag = d.treion_flag[gc] != 0;
-    const float ne_old = d.ne[gc];
     const Final f = finalize<STRICT>(nH, nHe, nh1_end, nhe1_end, a, ne_old, dt, flag);
     if (f.set_treion) {
       d.treion[gc] = B.t;
@@ -607,8 +623,8 @@ __global__ void __launch_bounds__(256, 4) k_dark(Dev d) {
     if (THERMAL) {
       ThermCell c;
       c.temp = temp0;
-      c.heat = d.heat[gc];
-      c.cool = d.cool[gc];
+      c.heat = heat_old;
+      c.cool = cool_old;
       c.nH = nH;
       c.nH1 = f.nH1;
       c.nH1_prev = nh1;
