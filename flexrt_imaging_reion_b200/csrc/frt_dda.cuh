@@ -19,8 +19,8 @@ __device__ __forceinline__ int dda_imod(int a, int b) {
 __device__ __forceinline__ bool ray_moves(const BoxP& B, float x0, float y0, float z0, float xhat, float yhat,
                                           float zhat, float dist) {
   const float px = x0 + dist * xhat, py = y0 + dist * yhat, pz = z0 + dist * zhat;
-  return (px > B.mv_hi) || (py > B.mv_hi) || (pz > B.mv_hi) || ((double)px < B.mv_lo) || ((double)py < B.mv_lo) ||
-         ((double)pz < B.mv_lo);
+  return (px > B.mv_hi) || (py > B.mv_hi) || (pz > B.mv_hi) || (px < B.mv_lo_f) || (py < B.mv_lo_f) ||
+         (pz < B.mv_lo_f);   // (double)p < mv_lo, compared in float
 }
 
 // Walk c_sim * deltat from (x0, y0, z0) in cell (in, jn, kn): calls seg(p, global cell, dist)
@@ -33,18 +33,20 @@ __device__ __forceinline__ int dda_walk(const BoxP& B, int PL, float xhat, float
   const int N = B.n;
   const float clgt = B.clight;
   const float dxc = B.dx;
+  // the double operands of the -x, -y, -z face times that do not change along the walk
+  const double xhd = (double)xhat, yhd = (double)yhat, zhd = (double)zhat, cld = (double)clgt;
   float tlast = 0.f, tmin = 0.f, dist;
   int p = 0;
   while (tlast < deltat) {
     float tx, ty, tz;
     if (xhat > 0.f) tx = (dxc - x0) / xhat / clgt;
-    else if (xhat < 0.f) tx = (float)(-1. * (double)x0 / (double)xhat / (double)clgt);
+    else if (xhat < 0.f) tx = (float)(-1. * (double)x0 / xhd / cld);
     else tx = INFINITY;
     if (yhat > 0.f) ty = (dxc - y0) / yhat / clgt;
-    else if (yhat < 0.f) ty = (float)(-1. * (double)y0 / (double)yhat / (double)clgt);
+    else if (yhat < 0.f) ty = (float)(-1. * (double)y0 / yhd / cld);
     else ty = INFINITY;
     if (zhat > 0.f) tz = (dxc - z0) / zhat / clgt;
-    else if (zhat < 0.f) tz = (float)(-1. * (double)z0 / (double)zhat / (double)clgt);
+    else if (zhat < 0.f) tz = (float)(-1. * (double)z0 / zhd / cld);
     else tz = INFINITY;
     int tag;
     if ((tx <= ty) && (tx <= tz)) { tmin = tx; tag = 0; }
@@ -69,11 +71,11 @@ __device__ __forceinline__ int dda_walk(const BoxP& B, int PL, float xhat, float
         else { kn = dda_imod(kn - 1, N); z0 = B.hi_edge; }
       }
       if (x0 <= 0.f) x0 = B.lo_edge;
-      if ((double)x0 >= B.hi_thr) x0 = B.hi_edge;
+      if (x0 >= B.hi_thr_f) x0 = B.hi_edge;
       if (y0 <= 0.f) y0 = B.lo_edge;
-      if ((double)y0 >= B.hi_thr) y0 = B.hi_edge;
+      if (y0 >= B.hi_thr_f) y0 = B.hi_edge;
       if (z0 <= 0.f) z0 = B.lo_edge;
-      if ((double)z0 >= B.hi_thr) z0 = B.hi_edge;
+      if (z0 >= B.hi_thr_f) z0 = B.hi_edge;
     }
     tlast += tmin;
   }
@@ -84,11 +86,11 @@ __device__ __forceinline__ int dda_walk(const BoxP& B, int PL, float xhat, float
   y0 += dist * yhat;
   z0 += dist * zhat;
   if (x0 <= 0.f) x0 = B.lo_edge;
-  if ((double)x0 >= B.hi_thr) x0 = B.hi_edge;
+  if (x0 >= B.hi_thr_f) x0 = B.hi_edge;
   if (y0 <= 0.f) y0 = B.lo_edge;
-  if ((double)y0 >= B.hi_thr) y0 = B.hi_edge;
+  if (y0 >= B.hi_thr_f) y0 = B.hi_edge;
   if (z0 <= 0.f) z0 = B.lo_edge;
-  if ((double)z0 >= B.hi_thr) z0 = B.hi_edge;
+  if (z0 >= B.hi_thr_f) z0 = B.hi_edge;
   return p + 1;
 }
 

@@ -825,11 +825,11 @@ __global__ void k_cosmo_rays(Dev d, int box, float ratio) {
     y *= ratio;
     z *= ratio;
     if (x <= 0.f) x = B.lo_edge;
-    if ((double)x >= B.hi_thr) x = B.hi_edge;
+    if (x >= B.hi_thr_f) x = B.hi_edge;
     if (y <= 0.f) y = B.lo_edge;
-    if ((double)y >= B.hi_thr) y = B.hi_edge;
+    if (y >= B.hi_thr_f) y = B.hi_edge;
     if (z <= 0.f) z = B.lo_edge;
-    if ((double)z >= B.hi_thr) z = B.hi_edge;
+    if (z >= B.hi_thr_f) z = B.hi_edge;
     A.x[i] = x;
     A.y[i] = y;
     A.z[i] = z;

@@ -85,6 +85,14 @@ void rotation_table(float* out) {
       }
 }
 
+// The smallest float >= v. For a float x, (double)x >= v <=> x >= float_at_or_above(v) and
+// (double)x < v <=> x < float_at_or_above(v), so the device compares in float.
+static float float_at_or_above(double v) {
+  float f = (float)v;
+  if ((double)f < v) f = std::nextafter(f, INFINITY);
+  return f;
+}
+
 void set_cell_size(BoxP* B, const frt_config* cfg, const frt_box_desc* bd, float dx) {
   B->dx = dx;
   B->scale = dx / B->dx0;                                            // ray_tracing.cc:1262
@@ -92,9 +100,11 @@ void set_cell_size(BoxP* B, const frt_config* cfg, const frt_box_desc* bd, float
   B->lo_edge = kMinDist * dx;                                        // ray_tracing.cc:1366
   B->hi_edge = dx * (1. - kMinDist);                                 // ray_tracing.cc:1370
   B->hi_thr = dx * (1. - kMinDist / 2.);                             // ray_tracing.cc:1403
+  B->hi_thr_f = float_at_or_above(B->hi_thr);
   const float nc = B->nc;
   B->mv_hi = nc * dx;                                                // ray_tracing.cc:1252
   B->mv_lo = (1. - nc) * dx;                                         // ray_tracing.cc:1253
+  B->mv_lo_f = float_at_or_above(B->mv_lo);
   B->dt = cfg->tstep_factor * dx / bd->cl_factor / kCl;              // rt_funcs.cc:11
   B->vol = ((double)dx) * ((double)dx) * ((double)dx);               // ray_tracing.cc:747
   B->kdep = 1e60 / (double)B->dt / B->vol;

@@ -34,8 +34,10 @@ struct BoxP {
   float lo_edge;             // min_dist*dx (float)
   float hi_edge;             // dx*(1.-min_dist) rounded to float
   double hi_thr;             // dx*(1.-min_dist/2.) (compared in double)
+  float hi_thr_f;            // the smallest float >= hi_thr: (double)x >= hi_thr <=> x >= hi_thr_f
   float mv_hi;               // nc*dx (float)
   double mv_lo;              // (1.-nc)*dx (double)
+  float mv_lo_f;             // the smallest float >= mv_lo: (double)x < mv_lo <=> x < mv_lo_f
   float clight, nc;          // cl_factor*cl (float), nl_const
   float dt, t;
   double vol;                // dx*dy*dz in double
