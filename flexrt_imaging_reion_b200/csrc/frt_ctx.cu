@@ -317,8 +317,13 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
   ctx->grid_rays = nsm * 8;
   ctx->grid_cells = nsm * 8;
   ctx->grid_lit = nsm * 8;
-  CK(cudaStreamCreateWithFlags(&ctx->s_main, cudaStreamNonBlocking));
-  CK(cudaStreamCreateWithFlags(&ctx->s_dark, cudaStreamNonBlocking));
+  // The lit-cell chain is the step's critical path; the dark-cell pass on its own stream only
+  // has to end before the join. With the chain's stream at the highest priority the block
+  // scheduler hands freed SM slots to the chain first and the dark pass fills the rest.
+  int prio_least = 0, prio_greatest = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
+  CK(cudaStreamCreateWithPriority(&ctx->s_main, cudaStreamNonBlocking, prio_greatest));
+  CK(cudaStreamCreateWithPriority(&ctx->s_dark, cudaStreamNonBlocking, prio_least));
   CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
   CK(cudaEventCreate(&ctx->ev_t0));
@@ -941,7 +946,7 @@ frt_status frt_step(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t
     CK(cudaStreamBeginCapture(ctx->s_main, cudaStreamCaptureModeThreadLocal));
     enqueue_step(ctx, true);
     CK(cudaStreamEndCapture(ctx->s_main, &g));
-    CK(cudaGraphInstantiate(&ctx->graph, g, 0));
+    CK(cudaGraphInstantiate(&ctx->graph, g, cudaGraphInstantiateFlagUseNodePriority));   // the streams' priorities
     CK(cudaGraphDestroy(g));
     ctx->graph_valid = true;
   }

@@ -102,7 +102,13 @@ __global__ void k_step_begin(Dev d) {
     c->mv_seg = 0ull;
     c->emitted = c->deposited = c->killed_ph = c->overlap = c->in_flight = 0.0;
   }
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < d.nbox; b += gridDim.x * blockDim.x) d.box[b].t += d.box[b].dt;
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < d.nbox; b += gridDim.x * blockDim.x) {
+    BoxP& B = d.box[b];
+    B.t += B.dt;
+    // for a float x: (double)x < nphot_min <=> x < nmin_ru, (double)x > nphot_min <=> x > nmin_rd
+    B.nmin_ru = __double2float_ru(B.nphot_min);
+    B.nmin_rd = __double2float_rd(B.nphot_min);
+  }
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < d.nsrc; s += gridDim.x * blockDim.x)
     d.src_ray_dt[s] += d.box[d.src_box[s]].dt;
 }
@@ -110,7 +116,7 @@ __global__ void k_step_begin(Dev d) {
 // Mark a cell touched by a segment. The lit list is numbered afterwards in cell order
 // (k_lit_compact), so that the lit-cell kernels read the dense fields in address order.
 __device__ __forceinline__ void mark_lit(const Dev& d, long long gc) {
-  if (!d.lit_flag[gc]) d.lit_flag[gc] = 1;
+  d.lit_flag[gc] = 1;   // a plain byte store: no load, so the walk never waits on the flag
 }
 
 // Number the marked cells in cell order (compact_marked, frt_dda.cuh).

@@ -45,6 +45,7 @@ struct BoxP {
   float kdep_f;              // the same in float (mixed-precision deposits)
   double rkill;              // comoving cm; 0 = off
   double nphot_min, nphot_max;
+  float nmin_ru, nmin_rd;    // nphot_min rounded up / down to float (set at the start of each step)
   float nphot_merge, split_thr;
   long long num_thresh;
   int lm;                    // merging HEALPix order (hpx_lvl)

@@ -260,10 +260,8 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
           dump_mask = 0;
           const BoxP& B = d.box[hd.w];
           kdep = B.kdep_f;
-          // (double)x < nphot_min <=> x < nmin_ru and (double)x > nphot_min <=> x > nmin_rd for a
-          // float x, with nphot_min rounded up / down to float
-          nmin_ru = __double2float_ru(B.nphot_min);
-          nmin_rd = __double2float_rd(B.nphot_min);
+          nmin_ru = B.nmin_ru;   // the photon threshold as float bounds (k_step_begin)
+          nmin_rd = B.nmin_rd;
           sg0 = sp[0];
           sg1 = (ns > 1) ? sp[1] : make_int2(-1, 0);
 #pragma unroll
