@@ -354,6 +354,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     d2h = 0
     launches = 0
     lit = 0
+    alive = moved = 0
     per_step = launches_per_step(spec, args.ray_capacity)
     t0 = time.perf_counter()
     for _ in range(args.steps):
@@ -366,6 +367,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dark_bytes += DARK_BYTES_PER_CELL * (ncell - st["lit_cells"])
         launches += per_step
         lit += st["lit_cells"]
+        alive += st["rays_alive"]
+        moved += st["rays_moved"]
     wall = time.perf_counter() - t0
     clk = clocks.stop()
     d2h = 144  # control block (per-step totals) read back each step
@@ -415,6 +418,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "clocks": clk,
         "crossings_per_step": cross / args.steps,
         "lit_cells_per_step": lit / args.steps,
+        "rays_alive_per_step": alive / args.steps,
+        "rays_moved_per_step": moved / args.steps,
     }
     ctx.close()
     return res

@@ -41,6 +41,7 @@ struct frt_ctx {
   bool graph_valid = false;
   bool strict = false;
   int grid_rays = 0, grid_cells = 0, grid_lit = 0;
+  int grid_dark = 0;       // one block per 256 cells: short blocks that yield SM slots to the lit chain
   float last_step_ms = 0.f, last_dark_ms = 0.f;
   bool rays_moved = false;   // an advance, merge or split ran (rays no longer one source's cast)
   bool cast_per_source = false;   // unbatched cast in the direct-launch step (comparison baseline)
@@ -183,7 +184,7 @@ void enqueue_step(frt_ctx* ctx, bool in_graph) {
   cudaStreamWaitEvent(ctx->s_dark, ctx->ev_fork, 0);
   if (in_graph) cudaEventRecordWithFlags(ctx->ev_d0, ctx->s_dark, cudaEventRecordExternal);
   else cudaEventRecord(ctx->ev_d0, ctx->s_dark);
-  launch_dark(d, ctx->strict, true, ctx->grid_cells, ctx->s_dark);
+  launch_dark(d, ctx->strict, true, ctx->grid_dark, ctx->s_dark);
   if (in_graph) cudaEventRecordWithFlags(ctx->ev_d1, ctx->s_dark, cudaEventRecordExternal);
   else cudaEventRecord(ctx->ev_d1, ctx->s_dark);
   cudaEventRecord(ctx->ev_join, ctx->s_dark);
@@ -355,6 +356,7 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
     off += ((ctx->hbox[b].ncell + kTile - 1) / kTile) * kTile;
   }
   d.ncell_total = off;
+  ctx->grid_dark = (int)std::min<long long>((off + 255) / 256, 1LL << 30);
   d.ntile = off / kTile;
   if (off >= (1LL << 31)) {
     ctx->err = "too many cells for 32-bit cell indices";
