@@ -418,7 +418,7 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
   }
   launch_fill_i32(d.lit_slot, -1, (long long)NC, ctx->s_main);
   const size_t L = (size_t)d.lit_cap;
-  AL(d.l_cell, L); AL(d.l_nh, L); AL(d.l_nhe, L); AL(d.l_y0h, L); AL(d.l_y0he, L); AL(d.l_crec_h, L);
+  AL(d.l_cell, L); AL(d.l_box, L); AL(d.l_nh, L); AL(d.l_nhe, L); AL(d.l_y0h, L); AL(d.l_y0he, L); AL(d.l_crec_h, L);
   AL(d.l_crec_he, L); AL(d.l_rec_h2, L); AL(d.l_rec_he2, L); AL(d.l_avg, L);
   AL(d.l_nh1_old, L); AL(d.l_acc, L);
   d.per_bin = (ctx->strict || cfg->outputs == FRT_OUT_DIAG) ? 1 : 0;

@@ -82,6 +82,7 @@ struct Dev {
   float *rec_h2, *rec_he2, *recrate_h2, *recrate_he2, *mfp, *mfp912, *if_speed, *inc_flux;  // diag
   // lit cells
   int* l_cell;
+  uint16_t* l_box;          // box of the lit cell (k_lit_init), so the cell passes reach BoxP in one load
   float *l_nh, *l_nhe, *l_y0h, *l_y0he, *l_crec_h, *l_crec_he, *l_rec_h2, *l_rec_he2;
   float* l_nh1_old;
   // pairs (H, He) side by side: a crossing gathers both averages in one 8-byte load and adds both

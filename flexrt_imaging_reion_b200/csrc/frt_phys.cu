@@ -78,12 +78,14 @@ __global__ void k_lit_init(Dev d) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
     const int gc = d.l_cell[s];
     // every load of the cell first, then the stores (the loads overlap)
+    const int bx = box_of_cell(d, gc);
     const float temp = d.temp[gc];
     const float cl = d.clump ? d.clump[gc] : d.const_clump;
     const float nh = d.nH[gc], nhe = d.nHe[gc], y0h = d.f_H1[gc], y0he = d.f_He1[gc];
     const float nh1 = d.nH1[gc], nhe1 = d.nHe1[gc];
     float rh, rhe;
     recomb_coeffs<STRICT>(temp, &rh, &rhe);
+    d.l_box[s] = (uint16_t)bx;
     d.l_nh[s] = nh;
     d.l_nhe[s] = nhe;
     d.l_y0h[s] = y0h;
@@ -440,8 +442,8 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d) {
   const int L = d.lit_cap;
   const bool diag = d.outputs == FRT_OUT_DIAG;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
-    const int gc = d.l_cell[s];
-    const BoxP& B = d.box[box_of_cell(d, gc)];
+    const BoxP& B = d.box[d.l_box[s]];
+    const int gc = LAST ? d.l_cell[s] : 0;   // the middle passes touch only the lit arrays
     const float dt = B.dt;
     const float2 acc = d.l_acc[s], av = d.l_avg[s];
     const float a_prev = av.x, b_prev = av.y;
