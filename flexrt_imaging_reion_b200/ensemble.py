@@ -59,12 +59,13 @@ def run_batched(inputs: Sequence[W.BoxInputs], seeds: Sequence[int], warmup: int
                 device: int = 0, box_ids: Sequence[int] = ()) -> Dict[str, object]:
     """All boxes in one context, one graph launch per step. Device time from CUDA events around
     each graph launch; wall time around the frt_step calls (H2D of the step's random angles,
-    launch, D2H of the step totals). per_box maps each box id to [t, dt, live rays]."""
+    launch, D2H of the step totals); raypass_ms sums the CUDA-event time of the ray passes. per_box
+    maps each box id to [t, dt, live rays]."""
     ctx = _ctx(inputs, seeds, device)
     ctx.setup()
     for _ in range(warmup):
         ctx.step(graph=True)
-    cross, dev_ms, dark_ms, lit = 0, 0.0, 0.0, 0
+    cross, dev_ms, dark_ms, rp_ms, lit = 0, 0.0, 0.0, 0.0, 0
     t0 = time.perf_counter()
     for _ in range(steps):
         st = ctx.step(graph=True)
@@ -73,6 +74,7 @@ def run_batched(inputs: Sequence[W.BoxInputs], seeds: Sequence[int], warmup: int
         ms, dms = ctx.last_timing()
         dev_ms += ms
         dark_ms += dms
+        rp_ms += ctx.last_raypass_ms()
     wall = time.perf_counter() - t0
     ids = list(box_ids) or list(range(ctx.nbox))
     per_box = {}
@@ -81,8 +83,8 @@ def run_batched(inputs: Sequence[W.BoxInputs], seeds: Sequence[int], warmup: int
         per_box[ids[b]] = [sc["t"], sc["dt"], float(ctx.num_rays(b))]
     rays = ctx.num_rays()
     ctx.close()
-    return {"crossings": cross, "device_ms": dev_ms, "dark_ms": dark_ms, "lit_cells": lit, "wall_s": wall,
-            "rays": rays, "per_box": per_box}
+    return {"crossings": cross, "device_ms": dev_ms, "dark_ms": dark_ms, "raypass_ms": rp_ms, "lit_cells": lit,
+            "wall_s": wall, "rays": rays, "per_box": per_box}
 
 
 def run_per_box_loop(inputs: Sequence[W.BoxInputs], seeds: Sequence[int], warmup: int, steps: int,
