@@ -334,6 +334,63 @@ def launches_per_step(spec, ray_capacity, itercount=5, hpx_lvl=0):
     return n
 
 
+def run_partition(args, rank: int, world: int, local_rank: int):
+    """One box, its sources shared over the ranks (partition.py): every rank holds the whole box,
+    walks its share of the rays and runs the same cell passes; per step one OR all-reduce of the
+    lit flags and per C2Ray iteration one sum all-reduce of the lit cells' rates (NCCL). Timed by
+    CUDA events on the rank's device around each step (collectives included), max over ranks."""
+    import torch
+    from flexrt_imaging_reion_b200 import partition as P, workloads as W
+    spec = _spec(args.workload)
+    inp = W.make_inputs(spec)
+    ctx = P.make_share(inp, args.seed, rank, world, device=local_rank, ray_capacity=args.ray_capacity)
+    comb = P.DistCombiner(ctx, local_rank) if world > 1 else P.LocalCombiner([ctx], local_rank)
+    for _ in range(args.warmup):
+        P.step_shares([ctx], comb)
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+        tdist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    cross, dev_ms = 0, 0.0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        torch.cuda.synchronize(local_rank)
+        e0.record()
+        st = P.step_shares([ctx], comb)[0]
+        e1.record()
+        torch.cuda.synchronize(local_rank)
+        dev_ms += e0.elapsed_time(e1)
+        cross += st["crossings"]
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    if dist:
+        t = torch.tensor([dev_ms, wall, float(cross)], dtype=torch.float64, device=f"cuda:{local_rank}")
+        mx, sm = t.clone(), t.clone()
+        tdist.all_reduce(mx, op=tdist.ReduceOp.MAX)
+        tdist.all_reduce(sm, op=tdist.ReduceOp.SUM)
+        dev_ms, wall, cross_all = float(mx[0]), float(mx[1]), float(sm[2])
+    else:
+        cross_all = float(cross)
+    ctx.close()
+    return {
+        "metric": "ray-cell crossings/s", "value": cross_all / (dev_ms * 1e-3), "unit": "crossings/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded lognormal gas + L^-2 sources; the reference's inputs are not shipped)",
+        "config": {"workload": _describe(spec), "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps}",
+                   "graph": False, "l2": "state (>1 GB) larger than L2, no flush",
+                   "parallelism": f"sources shared over {world} ranks, lit-cell rates all-reduced"},
+        "e2e": {"value": cross_all / wall, "unit": "crossings/s",
+                "h2d_bytes_per_step": 2 + 2 * len(W.grid_sources(inp)[1]), "d2h_bytes_per_step": 144 + 4},
+        "gpu_launches": args.steps * launches_per_step(spec, args.ray_capacity),
+        "clocks": clk,
+        "crossings_per_step": cross_all / args.steps,
+    }
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import numpy as np
     from flexrt_imaging_reion_b200 import workloads as W, rt
@@ -446,6 +503,9 @@ def main():
     ap.add_argument("--cpu-baseline-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-time-cap", type=float, default=150.0)
+    ap.add_argument("--mode", choices=["replicas", "partition"], default="replicas",
+                    help="N>1 on one box: N independent replicas (weak), or the box's sources shared "
+                         "over the N ranks with the lit cells' rates all-reduced (strong)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -512,6 +572,8 @@ def main():
         return
     if args.workload == "E":
         res = run_ensemble(args, rank, world, local_rank)
+    elif args.mode == "partition":
+        res = run_partition(args, rank, world, local_rank)
     else:
         res = run_ours(args, rank, world, local_rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "E":

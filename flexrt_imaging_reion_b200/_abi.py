@@ -33,7 +33,9 @@ EXPORTS = ["frt_create", "frt_destroy", "frt_last_error", "frt_rotation_table", 
            "frt_last_timing", "frt_seed_boxes", "frt_draw_cast", "frt_draw_step", "frt_get_sparse_field_noalloc", "frt_adjoint",
            "frt_last_adjoint_timing", "frt_write_gas", "frt_write_rays", "frt_write_treion", "frt_read_gas",
            "frt_read_treion", "frt_read_rays", "frt_update_cosmo_expansion",
-           "frt_set_cast_per_source", "frt_last_kernel_timing"]
+           "frt_set_cast_per_source", "frt_last_kernel_timing", "frt_set_source_owner", "frt_step_phase",
+           "frt_phase_buffers"]
+PHASE_WALK, PHASE_CELLS, PHASE_RAYPASS, PHASE_CELLPASS, PHASE_END = 0, 1, 2, 3, 4
 NOALLOC_MAX_CELLS = 1 << 20
 
 
@@ -124,6 +126,9 @@ def lib() -> C.CDLL:
         "frt_read_rays": ([P, I, P, C.c_size_t], I),
         "frt_update_cosmo_expansion": ([P, P, P], I),
         "frt_set_cast_per_source": ([P, I], I),
+        "frt_set_source_owner": ([P, P], I),
+        "frt_step_phase": ([P, I, I, P, P, C.POINTER(StepStats)], I),
+        "frt_phase_buffers": ([P, C.POINTER(P), C.POINTER(LL), C.POINTER(P), C.POINTER(P), C.POINTER(LL)], I),
         "frt_last_kernel_timing": ([P, I, P], I),
     }
     for name, (args, res) in sig.items():

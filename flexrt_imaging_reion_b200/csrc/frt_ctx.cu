@@ -39,6 +39,10 @@ struct frt_ctx {
   Ctl* h_ctl = nullptr;
   cudaGraphExec_t graph = nullptr;
   bool graph_valid = false;
+  long long phase_nlit = 0;   // lit cells of the current phased step (frt_step_phase)
+  uint8_t* src_own_buf = nullptr;
+  int* chunk_buf = nullptr;   // per-chunk lit counts of the phased step
+  frt_step_stats stats_scratch{};
   bool strict = false;
   int grid_rays = 0, grid_cells = 0, grid_lit = 0;
   int grid_dark = 0;       // one block per 256 cells: short blocks that yield SM slots to the lit chain
@@ -1050,6 +1054,115 @@ frt_status frt_box_scalars(frt_ctx* ctx, int box, double* out8) {
 frt_status frt_set_cast_per_source(frt_ctx* ctx, int per_source) {
   if (!ctx) return FRT_ERR_INVALID;
   ctx->cast_per_source = per_source != 0;
+  return FRT_OK;
+}
+
+// ---- one box shared by several contexts: the step in phases ------------------------------------
+// Every context holds the whole box and casts only the sources it owns; the caller combines the
+// contexts between phases (OR of the lit flags after the walk, sum of the lit cells' absorbed
+// photons after each ray pass) so that all of them run the same cell passes.
+frt_status frt_set_source_owner(frt_ctx* ctx, const uint8_t* own) {
+  if (!ctx) return FRT_ERR_INVALID;
+  Dev& d = ctx->d;
+  if (!own) {
+    d.src_own = nullptr;
+  } else {
+    if (d.nsrc < 1) return FRT_ERR_INVALID;
+    if (!ctx->src_own_buf) {
+      void* q = nullptr;
+      CK(cudaMalloc(&q, (size_t)d.src_cap));
+      ctx->allocs.push_back(q);
+      ctx->src_own_buf = (uint8_t*)q;
+    }
+    CK(cudaMemcpy(ctx->src_own_buf, own, (size_t)d.nsrc, cudaMemcpyHostToDevice));
+    d.src_own = ctx->src_own_buf;
+  }
+  ctx->graph_valid = false;   // the step graph holds the Dev block by value
+  return FRT_OK;
+}
+
+frt_status frt_phase_buffers(frt_ctx* ctx, void** lit_flag, long long* ncell, void** lit_acc, void** lit_heat,
+                             long long* nlit) {
+  if (!ctx) return FRT_ERR_INVALID;
+  if (lit_flag) *lit_flag = ctx->d.lit_flag;
+  if (ncell) *ncell = ctx->d.ncell_total;
+  if (lit_acc) *lit_acc = ctx->d.l_acc;
+  if (lit_heat) *lit_heat = ctx->d.l_heat;
+  if (nlit) *nlit = ctx->phase_nlit;
+  return FRT_OK;
+}
+
+frt_status frt_step_phase(frt_ctx* ctx, int phase, int iter, const uint16_t* itheta_per_box,
+                          const uint16_t* itheta_per_source, frt_step_stats* stats) {
+  if (!ctx) return FRT_ERR_INVALID;
+  Dev& d = ctx->d;
+  if (d.per_bin || d.bin_base) {
+    ctx->err = "frt_step_phase: needs core outputs, mixed precision and a box whose ray count cannot reach the "
+               "merge threshold (the per-bin rates and the merge are not combined across contexts)";
+    return FRT_ERR_INVALID;
+  }
+  cudaStream_t s = ctx->s_main;
+  switch (phase) {
+    case FRT_PHASE_WALK: {
+      frt_status st = step_inputs(ctx, itheta_per_box, itheta_per_source);
+      if (st) return st;
+      cudaMemcpyAsync(d.itheta_merge, ctx->h_ith_box, sizeof(uint16_t) * d.nbox, cudaMemcpyHostToDevice, s);
+      if (d.nsrc) cudaMemcpyAsync(d.src_itheta, ctx->h_ith_src, sizeof(uint16_t) * d.nsrc, cudaMemcpyHostToDevice, s);
+      CK(cudaEventRecord(ctx->ev_t0, s));
+      ctx->rays_moved = true;
+      launch_clear_lit(d, ctx->grid_lit, s);
+      launch_step_begin(d, s);
+      launch_walk(d, ctx->grid_rays, s);
+      break;
+    }
+    case FRT_PHASE_CELLS: {
+      // strict cell order, so that every context sharing the box numbers its lit cells alike
+      const long long nchunk = (d.ncell_total / 16 + 255) / 256;
+      if (!ctx->chunk_buf) {
+        void* q = nullptr;
+        CK(cudaMalloc(&q, sizeof(int) * (size_t)nchunk));
+        ctx->allocs.push_back(q);
+        ctx->chunk_buf = (int*)q;
+      }
+      launch_lit_number_ordered(d, ctx->chunk_buf, nchunk, ctx->grid_rays, s);
+      CK(cudaEventRecord(ctx->ev_fork, s));
+      CK(cudaStreamWaitEvent(ctx->s_dark, ctx->ev_fork, 0));
+      CK(cudaEventRecord(ctx->ev_d0, ctx->s_dark));
+      launch_dark(d, ctx->strict, true, ctx->grid_dark, ctx->s_dark);
+      CK(cudaEventRecord(ctx->ev_d1, ctx->s_dark));
+      CK(cudaEventRecord(ctx->ev_join, ctx->s_dark));
+      launch_lit_init(d, ctx->strict, ctx->grid_lit, s);
+      int nl = 0;
+      CK(cudaMemcpyAsync(&nl, &d.ctl->n_lit, sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      ctx->phase_nlit = std::min(nl, d.lit_cap);
+      break;
+    }
+    case FRT_PHASE_RAYPASS:
+      if (iter < 0 || iter >= d.itercount) return FRT_ERR_INVALID;
+      if (iter < frt_ctx::kMaxTimedIter) CK(cudaEventRecord(ctx->ev_r[2 * iter], s));
+      launch_raypass(d, iter, ctx->strict, ctx->grid_rays, s);
+      if (iter < frt_ctx::kMaxTimedIter) CK(cudaEventRecord(ctx->ev_r[2 * iter + 1], s));
+      break;
+    case FRT_PHASE_CELLPASS:
+      if (iter < 0 || iter >= d.itercount) return FRT_ERR_INVALID;
+      launch_litpass(d, iter, ctx->strict, true, ctx->grid_lit, s);
+      break;
+    case FRT_PHASE_END:
+      launch_count(d, ctx->grid_rays, s);
+      launch_merge(d, ctx->grid_rays, s);
+      launch_split_compact(d, ctx->grid_rays, s);
+      CK(cudaStreamWaitEvent(s, ctx->ev_join, 0));
+      launch_cast(d, s);
+      CK(cudaMemcpyAsync(ctx->h_ctl, d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+      CK(cudaEventRecord(ctx->ev_t1, s));
+      return finish_step(ctx, stats ? stats : &ctx->stats_scratch);
+    default:
+      return FRT_ERR_INVALID;
+  }
+  // the caller reads or combines device arrays next: the phase's work is complete on return
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
   return FRT_OK;
 }
 

@@ -124,6 +124,117 @@ __global__ void __launch_bounds__(256) k_lit_compact(Dev d) {
   compact_marked(d.lit_flag, d.ncell_total, d.lit_slot, d.l_cell, &d.ctl->n_lit, d.lit_cap, &d.ctl->err, ERR_LIT_CAP);
 }
 
+// The lit numbering in strict cell order, for a box shared by several contexts (the phased step):
+// every context must give a cell the same slot, so the chunks' bases come from a scan over the
+// chunks (k_lit_chunk_scan) instead of one atomicAdd per block. A chunk is 4096 cells: 256
+// threads x 16 flag bytes (one 16-byte load; a flag byte is 0 or 1).
+__device__ __forceinline__ int flags16(const uint8_t* flag, long long nvec, long long v) {
+  if (v >= nvec) return 0;
+  const uint4 f = reinterpret_cast<const uint4*>(flag)[v];
+  return __popc(f.x) + __popc(f.y) + __popc(f.z) + __popc(f.w);
+}
+
+__global__ void __launch_bounds__(256) k_lit_chunk_count(Dev d, int* chunk_cnt, long long nchunk) {
+  __shared__ int red[8];
+  const long long nvec = d.ncell_total >> 4;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (long long c = blockIdx.x; c < nchunk; c += gridDim.x) {
+    int x = flags16(d.lit_flag, nvec, c * 256 + threadIdx.x);
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) red[w] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int t = 0;
+      for (int k = 0; k < 8; k++) t += red[k];
+      chunk_cnt[c] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// one block of 1024 threads: exclusive scan of the chunk counts in place; the total is n_lit
+__global__ void __launch_bounds__(1024) k_lit_chunk_scan(Dev d, int* chunk, long long nchunk) {
+  __shared__ int wt[32];
+  __shared__ long long carry_s;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry_s = 0;
+  __syncthreads();
+  for (long long t0 = 0; t0 < nchunk; t0 += 1024) {
+    const long long i = t0 + threadIdx.x;
+    const int v = (i < nchunk) ? chunk[i] : 0;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) wt[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      int x = wt[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      wt[lane] = x;   // inclusive prefix over the warps
+    }
+    __syncthreads();
+    const long long carry = carry_s;
+    if (i < nchunk) chunk[i] = (int)(carry + (w > 0 ? wt[w - 1] : 0) + incl - v);
+    __syncthreads();
+    if (threadIdx.x == 0) carry_s = carry + wt[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) d.ctl->n_lit = (int)carry_s;
+}
+
+__global__ void __launch_bounds__(256) k_lit_chunk_write(Dev d, const int* chunk_off, long long nchunk) {
+  __shared__ int warp_tot[8];
+  const long long nvec = d.ncell_total >> 4;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (long long c = blockIdx.x; c < nchunk; c += gridDim.x) {
+    const long long v = c * 256 + threadIdx.x;
+    uint4 f = make_uint4(0u, 0u, 0u, 0u);
+    if (v < nvec) f = reinterpret_cast<const uint4*>(d.lit_flag)[v];
+    const int cnt = __popc(f.x) + __popc(f.y) + __popc(f.z) + __popc(f.w);
+    int incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) warp_tot[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      int x = (lane < 8) ? warp_tot[lane] : 0;
+      for (int o = 1; o < 8; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (lane < 8) warp_tot[lane] = x;
+    }
+    __syncthreads();
+    int s = chunk_off[c] + (w > 0 ? warp_tot[w - 1] : 0) + incl - cnt;
+    if (cnt) {
+      const unsigned words[4] = {f.x, f.y, f.z, f.w};
+      for (int q = 0; q < 4; q++) {
+        unsigned m = words[q];
+        while (m) {
+          const int bit = __ffs(m) - 1;   // flag bytes hold 0 or 1: bit 8k is byte k
+          m &= m - 1;
+          const long long gc = v * 16 + q * 4 + (bit >> 3);
+          if (s < d.lit_cap) {
+            d.l_cell[s] = (int)gc;
+            d.lit_slot[gc] = s;
+          } else {
+            atomicOr(&d.ctl->err, ERR_LIT_CAP);
+          }
+          s++;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // advance_ray (ray_tracing.cc:1222-1512) with c2ray_iter = TRUE and fion = 1 (plain mode):
 // cell-boundary walk over c_sim * time, path segments {cell, dist}, periodic wrap, corner nudge.
 __global__ void __launch_bounds__(256, 4) k_advance(Dev d) {
@@ -722,6 +833,7 @@ __global__ void k_cast(Dev d, int s_begin, int s_end) {
   long long ncast = 0;
   double emitted = 0.0;
   for (int s = s_begin + blockIdx.x * blockDim.x + threadIdx.x; s < s_end; s += gridDim.x * blockDim.x) {
+    if (d.src_own && !d.src_own[s]) continue;   // another context casts this source
     const int b = d.src_box[s];
     const BoxP& B = d.box[b];
     const int c = d.src_cell[s];
@@ -855,6 +967,20 @@ void launch_step_begin(const Dev& d, cudaStream_t s) { k_step_begin<<<grid_for(d
 void launch_advance(const Dev& d, int grid, cudaStream_t s) {
   k_advance<<<grid, 256, 0, s>>>(d);
   k_lit_compact<<<grid_for(d.ncell_total >> 4, 256, 148 * 8), 256, 0, s>>>(d);
+  k_moved_pack<<<grid, 256, 0, s>>>(d);
+}
+
+void launch_walk(const Dev& d, int grid, cudaStream_t s) { k_advance<<<grid, 256, 0, s>>>(d); }
+
+void launch_lit_number(const Dev& d, int grid, cudaStream_t s) {
+  k_lit_compact<<<grid_for(d.ncell_total >> 4, 256, 148 * 8), 256, 0, s>>>(d);
+  k_moved_pack<<<grid, 256, 0, s>>>(d);
+}
+
+void launch_lit_number_ordered(const Dev& d, int* chunk, long long nchunk, int grid, cudaStream_t s) {
+  k_lit_chunk_count<<<grid, 256, 0, s>>>(d, chunk, nchunk);
+  k_lit_chunk_scan<<<1, 1024, 0, s>>>(d, chunk, nchunk);
+  k_lit_chunk_write<<<grid, 256, 0, s>>>(d, chunk, nchunk);
   k_moved_pack<<<grid, 256, 0, s>>>(d);
 }
 

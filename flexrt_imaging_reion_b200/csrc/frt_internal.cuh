@@ -109,6 +109,7 @@ struct Dev {
   double* src_lum;
   float* src_ray_dt;
   uint16_t* src_itheta;
+  uint8_t* src_own;          // null, or 1 for the sources this context casts (a share of a box's sources)
   // control
   Ctl* ctl;
 };
@@ -143,6 +144,10 @@ inline __host__ __device__ int grid_for(long long n, int block, int maxblocks) {
 // ---- launchers (frt_geom.cu) ----------------------------------------------------------
 void launch_step_begin(const Dev& d, cudaStream_t s);
 void launch_advance(const Dev& d, int grid, cudaStream_t s);
+void launch_walk(const Dev& d, int grid, cudaStream_t s);         // k_advance alone
+void launch_lit_number(const Dev& d, int grid, cudaStream_t s);   // k_lit_compact + k_moved_pack
+// the same with the lit cells numbered in strict cell order (chunk: ncell/4096 ints of scratch)
+void launch_lit_number_ordered(const Dev& d, int* chunk, long long nchunk, int grid, cudaStream_t s);
 void launch_count(const Dev& d, int grid, cudaStream_t s);
 void launch_merge(const Dev& d, int grid, cudaStream_t s);
 void launch_split_compact(const Dev& d, int grid, cudaStream_t s);

@@ -1,0 +1,163 @@
+"""One box over several contexts: a share of its sources per context (per GPU).
+
+Rays of different sources meet only through the photo-ionisation rates of the cells they cross,
+so a box whose ray count cannot reach the merge threshold (merging is the one step that combines
+rays of different sources) splits exactly by sources. Every context holds the whole box and casts
+only its sources (frt_set_source_owner); the step runs in phases (frt_step_phase) and, between
+them, the contexts combine two things:
+
+* after the walk, the lit-cell flags (OR over the contexts, one byte per cell), so that every
+  context numbers the same lit cells in the same order;
+* after each of the 5 ray passes, the lit cells' absorbed photons (a sum of float2 pairs), and
+  after the last one also the photo-heating pairs.
+
+Every context then runs the same cell passes and holds the same cell state; the ray-side work
+(walk, ray passes, compaction, splitting, cast) is divided by the number of contexts. The sums
+of the float pairs are taken in a different order than one context's atomics take them, so the
+results agree with a one-context run to float rounding (and the ray trees agree up to rays whose
+photon count ties with nphot_min).
+
+`DistCombiner` combines over torch.distributed ranks (NCCL, one GPU per rank); `LocalCombiner`
+combines contexts that live in one process (the emulation the tests use on one GPU).
+"""
+from __future__ import annotations
+
+from typing import Dict, List, Sequence
+
+import numpy as np
+
+from . import _abi, rt, workloads as W
+
+
+def source_owner_masks(lum: Sequence[float], world: int) -> List[np.ndarray]:
+    """Owner masks that deal the sources out by luminosity, brightest first, round robin (bright
+    sources keep their rays longest): mask r has a 1 for every source of rank r."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = np.argsort(-np.asarray(lum, np.float64), kind="stable")
+    masks = [np.zeros(len(lum), np.uint8) for _ in range(world)]
+    for k, s in enumerate(order):
+        masks[k % world][s] = 1
+    return masks
+
+
+class _DevArray:
+    """A device array handed to torch by __cuda_array_interface__ (no copy)."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 2}
+
+
+def _views(ctx: rt.RTContext, device: int):
+    import torch
+    lf, nc, la, lh, nl = ctx.phase_buffers()
+    dev = torch.device("cuda", device)
+    flags = torch.as_tensor(_DevArray(lf, nc, "|u1"), device=dev)
+    acc = torch.as_tensor(_DevArray(la, 2 * nl, "<f4"), device=dev) if nl else None
+    heat = torch.as_tensor(_DevArray(lh, 2 * nl, "<f4"), device=dev) if nl else None
+    return flags, acc, heat
+
+
+class LocalCombiner:
+    """Combines contexts of one process (all on one device)."""
+
+    def __init__(self, ctxs: Sequence[rt.RTContext], device: int = 0):
+        self.ctxs, self.device = list(ctxs), device
+
+    def _apply(self, pick, reduce):
+        import torch
+        views = [pick(_views(c, self.device)) for c in self.ctxs]
+        if views[0] is None:
+            return
+        tot = views[0].clone()
+        for v in views[1:]:
+            tot = reduce(tot, v)
+        for v in views:
+            v.copy_(tot)
+        torch.cuda.synchronize(self.device)
+
+    def flags(self):
+        import torch
+        self._apply(lambda v: v[0], torch.maximum)
+
+    def acc(self):
+        self._apply(lambda v: v[1], lambda a, b: a + b)
+
+    def heat(self):
+        self._apply(lambda v: v[2], lambda a, b: a + b)
+
+
+class DistCombiner:
+    """Combines one context per rank over torch.distributed (NCCL: one GPU per rank)."""
+
+    def __init__(self, ctx: rt.RTContext, device: int):
+        self.ctxs, self.device = [ctx], device
+
+    def _all_reduce(self, t, op):
+        import torch
+        import torch.distributed as dist
+        if t is None:
+            return
+        torch.cuda.synchronize(self.device)
+        dist.all_reduce(t, op=op)
+        torch.cuda.synchronize(self.device)
+
+    def flags(self):
+        import torch.distributed as dist
+        self._all_reduce(_views(self.ctxs[0], self.device)[0], dist.ReduceOp.MAX)
+
+    def acc(self):
+        import torch.distributed as dist
+        self._all_reduce(_views(self.ctxs[0], self.device)[1], dist.ReduceOp.SUM)
+
+    def heat(self):
+        import torch.distributed as dist
+        self._all_reduce(_views(self.ctxs[0], self.device)[2], dist.ReduceOp.SUM)
+
+
+def step_shares(ctxs: Sequence[rt.RTContext], combiner, itercount: int = 5) -> List[Dict[str, float]]:
+    """One step of a box shared by `ctxs` (the contexts of this process: all of them for a
+    LocalCombiner, this rank's one for a DistCombiner). Returns each context's totals."""
+    for c in ctxs:
+        c.step_phase(_abi.PHASE_WALK)
+    combiner.flags()
+    for c in ctxs:
+        c.step_phase(_abi.PHASE_CELLS)
+    for it in range(itercount):
+        for c in ctxs:
+            c.step_phase(_abi.PHASE_RAYPASS, it)
+        combiner.acc()
+        if it == itercount - 1:
+            combiner.heat()
+        for c in ctxs:
+            c.step_phase(_abi.PHASE_CELLPASS, it)
+    return [c.step_phase(_abi.PHASE_END) for c in ctxs]
+
+
+def sum_stats(stats: Sequence[Dict[str, float]]) -> Dict[str, float]:
+    """Whole-box totals of a step from the contexts' totals (t and dt are the box's)."""
+    out = dict(stats[0])
+    for k in out:
+        if k in ("t", "dt"):
+            continue
+        if k == "error_flags":
+            v = 0
+            for st in stats:
+                v |= int(st[k])
+            out[k] = v
+        elif k == "lit_cells":
+            out[k] = stats[0][k]   # the same lit list in every context
+        else:
+            out[k] = sum(st[k] for st in stats)
+    return out
+
+
+def make_share(inp: W.BoxInputs, seed: int, rank: int, world: int, device: int = 0,
+               ray_capacity: int = 16 << 20) -> rt.RTContext:
+    """The context of share `rank` of `world`: the whole box, its own sources cast."""
+    _, lum = W.grid_sources(inp)
+    own = source_owner_masks(lum, world)[rank]
+    ctx = rt.RTContext([inp], [seed], precision="mixed", outputs="core", ray_capacity=ray_capacity, device=device)
+    ctx.setup(owner=own)
+    return ctx

@@ -156,7 +156,10 @@ class RTContext:
         self.close()
 
     # ---- set-up, as main.cc:10-106 -------------------------------------------------------------
-    def setup(self) -> None:
+    def setup(self, owner=None) -> None:
+        """init + init_rt + the set-up cast + get_nphot_min_max. With `owner` (one byte per
+        source, in set-up order), only the sources marked 1 are cast, here and in every step
+        (frt_set_source_owner): the context then holds one share of a box's sources."""
         for b, inp in enumerate(self.inputs):
             d1 = np.ascontiguousarray(inp.delta1, np.float32)
             self._check(self.L.frt_init_gas(self.h, b, d1.ctypes.data), "frt_init_gas")
@@ -168,10 +171,27 @@ class RTContext:
             if inp.clump is not None:
                 cl = np.ascontiguousarray(inp.clump, np.float32)
                 self._check(self.L.frt_set_clump_field(self.h, b, cl.ctypes.data), "frt_set_clump_field")
+        if owner is not None:
+            own = np.ascontiguousarray(owner, np.uint8)
+            self._check(self.L.frt_set_source_owner(self.h, own.ctypes.data), "frt_set_source_owner")
         self.update_dt()
         self.init_rt()
         self.new_rays(self.draw_cast())
         self.get_nphot_min_max()
+
+    def step_phase(self, phase: int, it: int = 0) -> Dict[str, float]:
+        """frt_step_phase: one phase of a step shared with other contexts (partition.py)."""
+        self._check(self.L.frt_step_phase(self.h, phase, it, None, None, C.byref(self.stats)), "frt_step_phase")
+        return self.stats.as_dict()
+
+    def phase_buffers(self):
+        """Device addresses and sizes of the arrays combined between phases:
+        (lit_flag, ncell, lit_acc, lit_heat, nlit)."""
+        lf, la, lh = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        nc, nl = C.c_longlong(), C.c_longlong()
+        self._check(self.L.frt_phase_buffers(self.h, C.byref(lf), C.byref(nc), C.byref(la), C.byref(lh), C.byref(nl)),
+                    "frt_phase_buffers")
+        return lf.value, nc.value, la.value, lh.value, nl.value
 
     def setup_restart(self, files) -> None:
         """Set-up from restart records in the reference's formats, one (gas, treion, rays) bytes

@@ -186,6 +186,33 @@ frt_status frt_step(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t
  * with one kernel launch per source (the way a per-source loop would), not one for all sources.
  * Results are the same; frt_step (the graph) is not affected. */
 frt_status frt_set_cast_per_source(frt_ctx* ctx, int per_source);
+
+/* ---- one box over several contexts (one per GPU): the step in phases ------------------------
+ * Replaces the reference's whole-box OpenMP loops over rays (update_rays, the ray part of
+ * find_avg_unu, split_rays, new_rays; main.cc:127-246) by a share of the sources per context:
+ * every context holds the whole box, frt_set_source_owner marks the sources it casts (own[s] = 1;
+ * NULL = all), and the caller runs the step as frt_step_phase(WALK), combine A, (CELLS), then per
+ * C2Ray iteration it: (RAYPASS, it), combine B, (CELLPASS, it), then (END). Combine A ORs the
+ * lit-flag bytes (frt_phase_buffers: ncell of them) over the contexts; combine B sums the float2
+ * lit-cell pairs lit_acc[nlit] and, after the last iteration's ray pass, lit_heat[nlit]. Every
+ * context then runs the same cell passes, and END returns this context's totals (rays, crossings,
+ * photons: sum them over the contexts). Each phase has finished on the device when it returns.
+ * Needs core outputs, mixed precision and a box whose ray count cannot reach the merge threshold
+ * (FRT_ERR_INVALID otherwise). The draws are the box's own reference-order draws when the
+ * itheta pointers are NULL, so contexts seeded alike cast with the same angles. */
+#define FRT_PHASE_WALK 0
+#define FRT_PHASE_CELLS 1
+#define FRT_PHASE_RAYPASS 2
+#define FRT_PHASE_CELLPASS 3
+#define FRT_PHASE_END 4
+frt_status frt_set_source_owner(frt_ctx* ctx, const uint8_t* own);
+frt_status frt_step_phase(frt_ctx* ctx, int phase, int iter, const uint16_t* itheta_per_box,
+                          const uint16_t* itheta_per_source, frt_step_stats* stats);
+/* Device addresses of the arrays the caller combines between phases: lit_flag (ncell bytes, one
+ * per cell of all boxes), lit_acc and lit_heat (nlit float2 each; nlit is set by the CELLS phase
+ * of the current step). */
+frt_status frt_phase_buffers(frt_ctx* ctx, void** lit_flag, long long* ncell, void** lit_acc, void** lit_heat,
+                             long long* nlit);
 /* Same as frt_step but launching every kernel directly (no graph) */
 frt_status frt_step_plain(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t* itheta_per_source,
                           frt_step_stats* stats);

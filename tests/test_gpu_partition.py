@@ -1,0 +1,59 @@
+"""One box shared by several contexts, each casting a share of the sources (partition.py), run on
+one GPU with the contexts combined in-process between the phases of the step: the shared run must
+match the oracle's one-box run with the contract tolerances of tests/test_gpu_parity.py, every
+share must hold bit-identical cell state, and the shares' ray totals must add up."""
+import numpy as np
+import pytest
+
+import parity_tools as PT
+from flexrt_imaging_reion_b200 import partition as P, rt, workloads as W
+from test_gpu_parity import check
+
+pytestmark = pytest.mark.gpu
+
+
+def _union_state(shares):
+    st = PT.device_state(shares[0], 0, False)
+    parts = [PT.device_state(c, 0, False) for c in shares[1:]]
+    for k in ("ray_order", "ray_pixel", "ray_itheta", "ray_cell", "ray_geom", "ray_nphot"):
+        st[k] = np.concatenate([st[k]] + [p[k] for p in parts])
+    # every share runs the same cell passes on the same combined inputs
+    for p in parts:
+        for k in ("f_H1", "f_He1", "temp", "gamma_H1_tot", "gamma_He1_tot"):
+            np.testing.assert_array_equal(p[k], st[k], err_msg=k)
+    return st
+
+
+@pytest.mark.parametrize("case", ["T16x3", "Sx2"])
+def test_shares_match_oracle(case):
+    if case == "T16x3":
+        # a ray capacity below the merge threshold: merging cannot be reached
+        spec, seed, world, cap = W.config_tiny(steps=6), 11, 3, 40000
+    else:
+        spec, seed, world, cap = W.config_S(), 21, 2, 1 << 20
+        spec = W.BoxSpec(**{**spec.__dict__, "steps": 4})
+    inp = W.make_inputs(spec)
+    ref = PT.oracle_states(inp, seed, spec.steps)
+    shares = [P.make_share(inp, seed, r, world, ray_capacity=cap) for r in range(world)]
+    comb = P.LocalCombiner(shares)
+    states = [_union_state(shares)]
+    in0 = sum(c.in_flight() for c in shares)
+    stats = []
+    for s in range(spec.steps):
+        tot = P.sum_stats(P.step_shares(shares, comb))
+        assert tot["error_flags"] == 0, tot
+        assert tot["crossings"] == int(ref[s + 1]["scalars"][10]), (s, tot["crossings"], ref[s + 1]["scalars"][10])
+        stats.append(tot)
+        states.append(_union_state(shares))
+    for c in shares:
+        c.close()
+    check(states, ref, False)
+    assert PT.photon_budget(stats, in0) < 1e-6
+
+
+def test_phases_refused_when_merging_is_reachable():
+    inp = W.make_inputs(W.config_tiny())
+    ctx = P.make_share(inp, 11, 0, 2, ray_capacity=1 << 20)
+    with pytest.raises(rt.FrtError, match="status 1"):
+        P.step_shares([ctx], P.LocalCombiner([ctx]))
+    ctx.close()
