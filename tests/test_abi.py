@@ -41,3 +41,6 @@ def test_invalid_config_rejected(product_lib):
 def test_null_context_calls_fail_cleanly(product_lib):
     for name in ("frt_update_rays", "frt_find_avg_unu", "frt_split_rays", "frt_update_thermal", "frt_init_rt"):
         assert getattr(product_lib, name)(None) == _abi.FRT_ERR_INVALID
+    assert product_lib.frt_set_source_owner(None, None) == _abi.FRT_ERR_INVALID
+    assert product_lib.frt_step_phase(None, _abi.PHASE_WALK, 0, None, None, None) == _abi.FRT_ERR_INVALID
+    assert product_lib.frt_phase_buffers(None, None, None, None, None, None) == _abi.FRT_ERR_INVALID
