@@ -89,31 +89,38 @@ class LocalCombiner:
 
 
 class DistCombiner:
-    """Combines one context per rank over torch.distributed (NCCL: one GPU per rank)."""
+    """Combines one context per rank over torch.distributed (NCCL: one GPU per rank). `views`
+    and `sync` default to the context's device arrays and a device synchronisation; they are
+    parameters so that the exchange can be exercised with host tensors over gloo."""
 
-    def __init__(self, ctx: rt.RTContext, device: int):
+    def __init__(self, ctx, device: int, views=None, sync=None):
         self.ctxs, self.device = [ctx], device
+        self._views = views or (lambda c: _views(c, self.device))
+        self._sync = sync or self._device_sync
+
+    def _device_sync(self):
+        import torch
+        torch.cuda.synchronize(self.device)
 
     def _all_reduce(self, t, op):
-        import torch
         import torch.distributed as dist
         if t is None:
             return
-        torch.cuda.synchronize(self.device)
+        self._sync()
         dist.all_reduce(t, op=op)
-        torch.cuda.synchronize(self.device)
+        self._sync()
 
     def flags(self):
         import torch.distributed as dist
-        self._all_reduce(_views(self.ctxs[0], self.device)[0], dist.ReduceOp.MAX)
+        self._all_reduce(self._views(self.ctxs[0])[0], dist.ReduceOp.MAX)
 
     def acc(self):
         import torch.distributed as dist
-        self._all_reduce(_views(self.ctxs[0], self.device)[1], dist.ReduceOp.SUM)
+        self._all_reduce(self._views(self.ctxs[0])[1], dist.ReduceOp.SUM)
 
     def heat(self):
         import torch.distributed as dist
-        self._all_reduce(_views(self.ctxs[0], self.device)[2], dist.ReduceOp.SUM)
+        self._all_reduce(self._views(self.ctxs[0])[2], dist.ReduceOp.SUM)
 
 
 def step_shares(ctxs: Sequence[rt.RTContext], combiner, itercount: int = 5) -> List[Dict[str, float]]:
