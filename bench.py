@@ -480,6 +480,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "gpu_launches": launches,
         "clocks": clk,
         "crossings_per_step": cross / args.steps,
+        # each crossing is written once by the walk and read by each of the C2Ray iterations
+        "segment_visits_per_step": cross * (1 + ITERCOUNT) / args.steps,
         "lit_cells_per_step": lit / args.steps,
         "rays_alive_per_step": alive / args.steps,
         "rays_moved_per_step": moved / args.steps,
