@@ -16,7 +16,9 @@ L2 flush is needed between steps.
              pass): algorithmic bytes = cells x 82 B (10 float fields + 2 flag bytes read,
              10 float fields written) / its CUDA-event time, against MEASURED_PEAKS.json hbm_gbs
   cpu_baseline  the reference's own OpenMP code (compiled from its sources, oracle/_ref) on the
-             host cores, on a bounded sample (its first steps) of the same workload
+             host cores, on a bounded steady-state sample of the same workload: the device's state
+             after the last timed step, written in the reference's restart formats, is read by the
+             reference's own restart path (input_grid = TRUE), which then runs two steps
 
 --impl reference runs that compiled reference alone (all host threads) and prints its line.
 Multi-GPU: the single-box workloads do not shard; --gpus N runs N independent replicas (one per
@@ -48,7 +50,7 @@ DARK_TRAFFIC_BYTES_PER_CELL = 1343184384 / 13264001
 # the hot-path analysis counts them -- 8 B segment read, 8 B of gathered <n_HI>, <n_HeI>, 68 B of
 # deposits (2 + 3 x 5 floats) -- and the ncu DRAM bytes (read + write) per crossing of one launch,
 # the mean over the 5 passes of step 24 of L (17 465 923 crossings per pass; 679.6 MB per launch).
-ITERCOUNT = 5
+# The number of ray passes per step is the context's C2Ray iteration count (RTContext.itercount).
 RAYPASS_BYTES_PER_CROSSING = 8 + 8 + 68
 RAYPASS_TRAFFIC_BYTES_PER_CROSSING = 38.9
 
@@ -130,7 +132,7 @@ def _unlimited_stack():
 
 
 # ---- the compiled reference (oracle/_ref) ------------------------------------------------------
-def _ref_exe(name: str, spec, threads: int) -> str:
+def _ref_exe(name: str, spec, threads: int, restart: bool = False) -> str:
     from oracle import build_ref as B
     d = os.path.join(B.OUT, name)
     exe = os.path.join(d, "ref_driver")
@@ -141,7 +143,7 @@ def _ref_exe(name: str, spec, threads: int) -> str:
             ncpu = json.load(f).get("ncpu")
     if not os.path.exists(exe) or ncpu is None or ncpu < threads:
         if os.path.isdir(B.REF_SRC):
-            B.build(name, spec, ncpu=threads)
+            B.build(name, spec, ncpu=threads, restart=restart)
         elif os.path.isdir(os.path.join(d, "src")):
             B.compile_stage(d, ncpu=threads)
         else:
@@ -177,6 +179,42 @@ def run_reference(spec, name: str, steps: int, threads: int, time_cap_s: float, 
                     break
         p.wait()
     return rows, setup
+
+
+def run_reference_restart(spec, name: str, files, steps: int, threads: int, seed: int):
+    """The compiled reference started through its own restart path (input_grid = TRUE: init()
+    reads the gas and treion records, init_rt() the ray records, rt_funcs.cc:95-124) from
+    `files` = (gas, rays, treion) bytes in its formats, then run for `steps` steps; returns
+    per-step (crossings, wall) and the restart set-up time."""
+    from flexrt_imaging_reion_b200 import workloads as W
+    exe = _ref_exe(name, spec, threads, restart=True)
+    d = os.path.dirname(exe)
+    gas, rays, tre = files
+    paths = [os.path.join(d, "input_files", f"restart_{k}.bin") for k in ("gas", "rays", "tre")]
+    try:
+        for pth, data in zip(paths, (gas, rays, tre)):
+            with open(pth, "wb") as f:
+                f.write(data)
+        inp = W.make_inputs(spec)
+        with tempfile.TemporaryDirectory() as td:
+            W.write_reference_inputs(inp, td)
+            args = [exe, td, str(steps), str(seed), "0", repr(spec.rkill_cm())]
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+            r = subprocess.run(args, cwd=d, env=env, capture_output=True, text=True, preexec_fn=_unlimited_stack)
+            if r.returncode != 0:
+                raise RuntimeError(f"ref_driver (restart) failed: {r.stdout[-500:]} {r.stderr[-500:]}")
+        rows, setup = [], None
+        for line in r.stdout.splitlines():
+            if line.startswith("SETUP"):
+                setup = float(line.split()[1])
+            m = re.match(r"STEP (\d+) rays_before=\d+ crossings=(\d+) moved=\d+ wall=([0-9.eE+-]+)", line)
+            if m:
+                rows.append((int(m.group(2)), float(m.group(3))))
+        return rows, setup
+    finally:
+        for pth in paths:
+            if os.path.exists(pth):
+                os.remove(pth)
 
 
 # ---- uneven ensemble (E) --------------------------------------------------------------------
@@ -229,8 +267,9 @@ def run_ensemble(args, rank: int, world: int, local_rank: int):
     else:
         dev_ms, wall, cross = bat["device_ms"], bat["wall_s"], float(bat["crossings"])
     cap = EN.ray_capacity([specs[b] for b in mine])
-    per_step = max(launches_per_step(specs[b], cap) for b in mine) if mine else 0
-    rp_gbs = (RAYPASS_BYTES_PER_CROSSING * float(bat["crossings"]) * ITERCOUNT / (bat["raypass_ms"] * 1e-3) / 1e9
+    itercount = int(bat["itercount"])
+    per_step = max(launches_per_step(specs[b], cap, itercount) for b in mine) if mine else 0
+    rp_gbs = (RAYPASS_BYTES_PER_CROSSING * float(bat["crossings"]) * itercount / (bat["raypass_ms"] * 1e-3) / 1e9
               if bat["raypass_ms"] > 0 else None)
     peak, peak_kind = _peaks()
     res = {
@@ -251,7 +290,7 @@ def run_ensemble(args, rank: int, world: int, local_rank: int):
                      "traffic_note": "bytes per launch: ncu DRAM bytes per crossing of a ray pass (L) x crossings per step",
                      "algorithmic_bytes_per_launch": RAYPASS_BYTES_PER_CROSSING * float(bat["crossings"]) / args.steps,
                      "bytes_per_crossing": RAYPASS_BYTES_PER_CROSSING, "peak_kind": peak_kind,
-                     "launch_ms": bat["raypass_ms"] / args.steps / ITERCOUNT, "launches_per_step": ITERCOUNT},
+                     "launch_ms": bat["raypass_ms"] / args.steps / itercount, "launches_per_step": itercount},
         "dark_pass": {"kernel": "k_dark (cells no ray touched: whole step in one pass)",
                       "span_ms_per_step": bat["dark_ms"] / args.steps, "bytes_per_cell": DARK_BYTES_PER_CELL,
                       "cells_per_step": ncell - bat["lit_cells"] / args.steps,
@@ -267,7 +306,8 @@ def run_ensemble(args, rank: int, world: int, local_rank: int):
         res["per_box_plain_loop"] = {
             "value": loop["crossings"] / loop["wall_s"], "unit": "crossings/s", "ms_per_step": 1e3 * loop["wall_s"] / args.steps,
             "crossings": loop["crossings"],
-            "gpu_launches": args.steps * sum(launches_per_step(specs[b], EN.ray_capacity([specs[b]])) for b in mine),
+            "gpu_launches": args.steps * sum(launches_per_step(specs[b], EN.ray_capacity([specs[b]]), itercount)
+                                             for b in mine),
             "what": "one context per box, every kernel launched directly (no graph), boxes one after another; "
                     "host wall clock"}
         res["batched_vs_loop_wall"] = (cross / wall) / (loop["crossings"] / loop["wall_s"])
@@ -278,7 +318,7 @@ def run_ensemble(args, rank: int, world: int, local_rank: int):
         res["per_box_per_source_loop"] = {
             "value": ps["crossings"] / ps["wall_s"], "unit": "crossings/s", "ms_per_step": 1e3 * ps["wall_s"] / args.steps,
             "crossings": ps["crossings"],
-            "gpu_launches": args.steps * sum(launches_per_step(specs[b], EN.ray_capacity([specs[b]])) - 1 +
+            "gpu_launches": args.steps * sum(launches_per_step(specs[b], EN.ray_capacity([specs[b]]), itercount) - 1 +
                                              len(W.grid_sources(inp)[1]) for b, inp in zip(mine, inputs)),
             "what": "as per_box_plain_loop, and the cast launched once per source; host wall clock"}
         res["batched_vs_per_source_loop_wall"] = (cross / wall) / (ps["crossings"] / ps["wall_s"])
@@ -400,6 +440,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                        ray_capacity=args.ray_capacity, lit_capacity=args.lit_capacity, device=local_rank)
     ctx.setup()
     ncell = spec.n ** 3
+    itercount = ctx.itercount
     for _ in range(args.warmup):
         ctx.step(graph=not args.plain)
     dist = world > 1
@@ -418,7 +459,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     launches = 0
     lit = 0
     alive = moved = 0
-    per_step = launches_per_step(spec, args.ray_capacity)
+    per_step = launches_per_step(spec, args.ray_capacity, itercount)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         st = ctx.step(graph=not args.plain)
@@ -434,6 +475,15 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     wall = time.perf_counter() - t0
     clk = clocks.stop()
     d2h = 144  # control block (per-step totals) read back each step
+    # the state after the last timed step in the reference's restart formats: the CPU baseline
+    # resumes the reference from it (a steady-state sample instead of the set-up-dominated first
+    # steps)
+    restart_files = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            restart_files = ctx.write_restart(0)
+        except Exception:
+            restart_files = None
     if dist:
         import torch
         import torch.distributed as tdist
@@ -446,7 +496,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     else:
         dev_ms_max, wall_max, cross_all = dev_ms, wall, float(cross)
     peak, peak_kind = _peaks()
-    rp_gbs = RAYPASS_BYTES_PER_CROSSING * cross * ITERCOUNT / (rp_ms * 1e-3) / 1e9 if rp_ms > 0 else None
+    rp_gbs = RAYPASS_BYTES_PER_CROSSING * cross * itercount / (rp_ms * 1e-3) / 1e9 if rp_ms > 0 else None
     res = {
         "metric": "ray-cell crossings/s", "value": cross_all / (dev_ms_max * 1e-3), "unit": "crossings/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps,
@@ -466,8 +516,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                      "traffic_note": "bytes per launch: ncu DRAM bytes per crossing of a ray pass x crossings per step",
                      "algorithmic_bytes_per_launch": RAYPASS_BYTES_PER_CROSSING * cross / args.steps,
                      "bytes_per_crossing": RAYPASS_BYTES_PER_CROSSING,
-                     "peak_kind": peak_kind, "launch_ms": rp_ms / args.steps / ITERCOUNT,
-                     "launches_per_step": ITERCOUNT},
+                     "peak_kind": peak_kind, "launch_ms": rp_ms / args.steps / itercount,
+                     "launches_per_step": itercount},
         # the dark-cell pass runs on its own stream in the gaps of the lit-cell chain: its event
         # span is not its busy time, so it gets no roofline here (its serialised ncu time and
         # DRAM traffic are in the profiles)
@@ -481,19 +531,22 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "clocks": clk,
         "crossings_per_step": cross / args.steps,
         # each crossing is written once by the walk and read by each of the C2Ray iterations
-        "segment_visits_per_step": cross * (1 + ITERCOUNT) / args.steps,
+        "segment_visits_per_step": cross * (1 + itercount) / args.steps,
         "lit_cells_per_step": lit / args.steps,
         "rays_alive_per_step": alive / args.steps,
         "rays_moved_per_step": moved / args.steps,
     }
     ctx.close()
+    if restart_files is not None:
+        res["_restart_files"] = restart_files
     return res
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    # L runs 50 steps: 5 warm-up steps, then steps 6..50 timed
+    ap.add_argument("--steps", type=int, default=45)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["L", "M", "S", "E", "A"], default="L")
@@ -504,7 +557,8 @@ def main():
     ap.add_argument("--plain", action="store_true", help="launch kernels directly instead of the CUDA graph")
     ap.add_argument("--cpu-baseline-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-time-cap", type=float, default=150.0)
+    # the reference arm times the same step window as this arm (about 8-10 s per L step on 16 cores)
+    ap.add_argument("--ref-time-cap", type=float, default=900.0)
     ap.add_argument("--mode", choices=["replicas", "partition"], default="replicas",
                     help="N>1 on one box: N independent replicas (weak), or the box's sources shared "
                          "over the N ranks with the lit cells' rates all-reduced (strong)")
@@ -588,16 +642,30 @@ def main():
         except Exception as e:
             res["cpu_baseline"] = {"value": None, "unit": "crossings/s", "cores": threads, "kind": "reference",
                                    "sample": f"unavailable: {e}"}
+    restart_files = res.pop("_restart_files", None)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != "E":
         spec = _spec(args.workload)
+        last = args.warmup + args.steps
         try:
+            if restart_files is None:
+                raise RuntimeError("no restart records of the device state")
+            rows, setup = run_reference_restart(spec, args.workload + "_restart", restart_files,
+                                                args.cpu_baseline_steps, threads, args.seed)
+            sample = (f"steps {last + 1}..{last + len(rows)} of the same workload: the device state after step "
+                      f"{last} written in the reference's restart formats and resumed by the reference's own "
+                      f"restart path (input_grid = TRUE; restart set-up {setup:.1f} s excluded); reference "
+                      f"OpenMP code compiled from its sources, {threads} threads")
+        except Exception as e:
+            # no restart build: the first steps from a fresh start (set-up-dominated, labelled so)
             rows, setup = run_reference(spec, args.workload, args.cpu_baseline_steps, threads, 60.0, args.seed)
+            sample = (f"steps 1..{len(rows)} of the same workload from a fresh start (set-up {setup:.1f} s "
+                      f"excluded; the restart sample was unavailable: {e}), reference OpenMP code compiled "
+                      f"from its sources, {threads} threads")
+        try:
             cr = sum(c for c, _ in rows)
             wt = sum(w for _, w in rows)
             res["cpu_baseline"] = {"value": cr / wt if wt else None, "unit": "crossings/s", "cores": threads,
-                                   "kind": "reference",
-                                   "sample": f"steps 1..{len(rows)} of the same workload (set-up {setup:.1f} s "
-                                             f"excluded), reference OpenMP code compiled from its sources"}
+                                   "kind": "reference", "sample": sample}
         except Exception as e:
             res["cpu_baseline"] = {"value": None, "unit": "crossings/s", "cores": threads, "kind": "reference",
                                    "sample": f"unavailable: {e}"}

@@ -45,6 +45,8 @@ struct frt_ctx {
   frt_step_stats stats_scratch{};
   bool strict = false;
   int grid_rays = 0, grid_cells = 0, grid_lit = 0;
+  int nsm = 148;
+  Tune tune;               // launch shapes of the tunable kernels (frt_autotune / frt_set_tuning)
   int grid_dark = 0;       // one block per 256 cells: short blocks that yield SM slots to the lit chain
   float last_step_ms = 0.f, last_dark_ms = 0.f;
   bool rays_moved = false;   // an advance, merge or split ran (rays no longer one source's cast)
@@ -140,6 +142,10 @@ frt_status upload_sources(frt_ctx* ctx) {
     return FRT_ERR_CAPACITY;
   }
   ctx->d.nsrc = n;
+  // an owner mask (frt_set_source_owner) describes the previous source list: drop it, so that no
+  // kernel reads owner bytes that were never written for the new sources (all sources are cast
+  // until the caller sets a mask for the new list)
+  ctx->d.src_own = nullptr;
   if (n) {
     CK(cudaMemcpy(ctx->d.src_cell, cell.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->d.src_box, box.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice));
@@ -156,7 +162,7 @@ void enqueue_begin_advance(frt_ctx* ctx) {
   const Dev& d = ctx->d;
   launch_clear_lit(d, ctx->grid_lit, ctx->s_main);
   launch_step_begin(d, ctx->s_main);
-  launch_advance(d, ctx->grid_rays, ctx->s_main);
+  launch_advance(d, ctx->nsm * ctx->tune.adv_grid, ctx->s_main, ctx->tune.adv_block, ctx->grid_rays);
 }
 
 void record(cudaEvent_t e, cudaStream_t s, bool in_graph) {
@@ -170,9 +176,10 @@ void enqueue_iterations(frt_ctx* ctx, bool fused_thermal, bool in_graph = false)
   for (int it = 0; it < d.itercount; it++) {
     const bool timed = it < frt_ctx::kMaxTimedIter;
     if (timed) record(ctx->ev_r[2 * it], ctx->s_main, in_graph);
-    launch_raypass(d, it, ctx->strict, ctx->grid_rays, ctx->s_main);
+    launch_raypass(d, it, ctx->strict, ctx->nsm * ctx->tune.rp_grid, ctx->s_main, ctx->tune.rp_block,
+                   ctx->tune.rp_chunk);
     if (timed) record(ctx->ev_r[2 * it + 1], ctx->s_main, in_graph);
-    launch_litpass(d, it, ctx->strict, fused_thermal, ctx->grid_lit, ctx->s_main);
+    launch_litpass(d, it, ctx->strict, fused_thermal, ctx->nsm * ctx->tune.lit_grid, ctx->s_main);
   }
 }
 
@@ -195,7 +202,7 @@ void enqueue_step(frt_ctx* ctx, bool in_graph) {
   enqueue_iterations(ctx, true, in_graph);
   launch_count(d, ctx->grid_rays, s);
   launch_merge(d, ctx->grid_rays, s);
-  launch_split_compact(d, ctx->grid_rays, s);
+  launch_split_compact(d, ctx->nsm * ctx->tune.split_grid, s);
   cudaStreamWaitEvent(s, ctx->ev_join, 0);
   if (!in_graph && ctx->cast_per_source) launch_cast_per_source(d, s);
   else launch_cast(d, s);
@@ -319,6 +326,7 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
   CK(cudaSetDevice(cfg->device));
   int nsm = 148;
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cfg->device));
+  ctx->nsm = nsm;
   ctx->grid_rays = nsm * 8;
   ctx->grid_cells = nsm * 8;
   ctx->grid_lit = nsm * 8;
@@ -463,6 +471,7 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
   AL(d.src_cell, d.src_cap); AL(d.src_box, d.src_cap); AL(d.src_lum, d.src_cap); AL(d.src_ray_dt, d.src_cap);
   AL(d.src_itheta, d.src_cap);
   AL(d.ctl, 1);
+  AL(d.rp_queue, kMaxIterQueue);
   CK(cudaMallocHost(&ctx->h_ith_box, sizeof(uint16_t) * cfg->nbox));
   CK(cudaMallocHost(&ctx->h_ith_src, sizeof(uint16_t) * d.src_cap));
   CK(cudaMallocHost(&ctx->h_ctl, sizeof(Ctl)));
@@ -868,7 +877,7 @@ frt_status frt_merge(frt_ctx* ctx, const uint16_t* itheta_per_box) {
 frt_status frt_split_rays(frt_ctx* ctx) {
   if (!ctx) return FRT_ERR_INVALID;
   ctx->rays_moved = true;
-  launch_split_compact(ctx->d, ctx->grid_rays, ctx->s_main);
+  launch_split_compact(ctx->d, ctx->nsm * ctx->tune.split_grid, ctx->s_main);
   return sync_and_check(ctx);
 }
 
@@ -1106,13 +1115,14 @@ frt_status frt_step_phase(frt_ctx* ctx, int phase, int iter, const uint16_t* ith
     case FRT_PHASE_WALK: {
       frt_status st = step_inputs(ctx, itheta_per_box, itheta_per_source);
       if (st) return st;
-      cudaMemcpyAsync(d.itheta_merge, ctx->h_ith_box, sizeof(uint16_t) * d.nbox, cudaMemcpyHostToDevice, s);
-      if (d.nsrc) cudaMemcpyAsync(d.src_itheta, ctx->h_ith_src, sizeof(uint16_t) * d.nsrc, cudaMemcpyHostToDevice, s);
+      CK(cudaMemcpyAsync(d.itheta_merge, ctx->h_ith_box, sizeof(uint16_t) * d.nbox, cudaMemcpyHostToDevice, s));
+      if (d.nsrc)
+        CK(cudaMemcpyAsync(d.src_itheta, ctx->h_ith_src, sizeof(uint16_t) * d.nsrc, cudaMemcpyHostToDevice, s));
       CK(cudaEventRecord(ctx->ev_t0, s));
       ctx->rays_moved = true;
       launch_clear_lit(d, ctx->grid_lit, s);
       launch_step_begin(d, s);
-      launch_walk(d, ctx->grid_rays, s);
+      launch_walk(d, ctx->nsm * ctx->tune.adv_grid, s, ctx->tune.adv_block);
       break;
     }
     case FRT_PHASE_CELLS: {
@@ -1141,17 +1151,17 @@ frt_status frt_step_phase(frt_ctx* ctx, int phase, int iter, const uint16_t* ith
     case FRT_PHASE_RAYPASS:
       if (iter < 0 || iter >= d.itercount) return FRT_ERR_INVALID;
       if (iter < frt_ctx::kMaxTimedIter) CK(cudaEventRecord(ctx->ev_r[2 * iter], s));
-      launch_raypass(d, iter, ctx->strict, ctx->grid_rays, s);
+      launch_raypass(d, iter, ctx->strict, ctx->nsm * ctx->tune.rp_grid, s, ctx->tune.rp_block, ctx->tune.rp_chunk);
       if (iter < frt_ctx::kMaxTimedIter) CK(cudaEventRecord(ctx->ev_r[2 * iter + 1], s));
       break;
     case FRT_PHASE_CELLPASS:
       if (iter < 0 || iter >= d.itercount) return FRT_ERR_INVALID;
-      launch_litpass(d, iter, ctx->strict, true, ctx->grid_lit, s);
+      launch_litpass(d, iter, ctx->strict, true, ctx->nsm * ctx->tune.lit_grid, s);
       break;
     case FRT_PHASE_END:
       launch_count(d, ctx->grid_rays, s);
       launch_merge(d, ctx->grid_rays, s);
-      launch_split_compact(d, ctx->grid_rays, s);
+      launch_split_compact(d, ctx->nsm * ctx->tune.split_grid, s);
       CK(cudaStreamWaitEvent(s, ctx->ev_join, 0));
       launch_cast(d, s);
       CK(cudaMemcpyAsync(ctx->h_ctl, d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));

@@ -5,6 +5,7 @@
 // merge trees and HEALPix pixels, so every product and sum here is rounded exactly as the
 // reference's g++ build rounds it (no a*b+c contraction). Each kernel cites the reference code
 // whose arithmetic it reproduces.
+#include <limits.h>
 #include <math.h>
 
 #include "frt_internal.cuh"
@@ -237,14 +238,16 @@ __global__ void __launch_bounds__(256) k_lit_chunk_write(Dev d, const int* chunk
 
 // advance_ray (ray_tracing.cc:1222-1512) with c2ray_iter = TRUE and fion = 1 (plain mode):
 // cell-boundary walk over c_sim * time, path segments {cell, dist}, periodic wrap, corner nudge.
-__global__ void __launch_bounds__(256, 4) k_advance(Dev d) {
+// Rays [r_begin, min(r_end, pool size)) of the pool (the autotuner times launch shapes on shares
+// of one step's rays; the step itself launches the whole pool).
+__global__ void __launch_bounds__(256, 4) k_advance(Dev d, int r_begin, int r_end) {
   const int cur = d.ctl->cur;
-  const int n = d.ctl->nray[cur];
+  const int n = min(d.ctl->nray[cur], r_end);
   const RayPool A = d.pool[cur];
   const int cap = d.ray_cap, PL = d.PL;
   long long cross = 0, moved = 0, killed = 0;
   double killed_ph = 0.0;
-  for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+  for (int i0 = r_begin + blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
     const int i = i0 + threadIdx.x;
     if (i < n) do {
       d.dead[i] = 0;
@@ -630,7 +633,7 @@ __global__ void k_merge_final(Dev d, double pi_sf_3, double log4) {
 // live ray is written by its own thread from registers; a split ray parks its record in shared
 // memory and the block's threads then build the children, four per split ray, spread over all
 // threads so that the child arithmetic (pixel table, rotation, wrap) runs at full width.
-__global__ void __launch_bounds__(256) k_compact_split(Dev d) {
+__global__ void __launch_bounds__(256) k_compact_split(Dev d, int r_begin, int r_end) {
   __shared__ int s_cell[256], s_pixel[256], s_dst[256];
   __shared__ float s_xh[256], s_yh[256], s_zh[256], s_r[256], s_x[256], s_y[256], s_z[256], s_time[256];
   __shared__ float s_nph[FRT_MAX_FREQ][256];
@@ -640,14 +643,14 @@ __global__ void __launch_bounds__(256) k_compact_split(Dev d) {
   __shared__ int s_tot, s_base;
   const int cur = d.ctl->cur;
   const int nxt = cur ^ 1;
-  const int n = d.ctl->nray[cur];
+  const int n = min(d.ctl->nray[cur], r_end);   // rays [r_begin, n): see k_advance
   const RayPool A = d.pool[cur];
   const RayPool Bp = d.pool[nxt];
   const int cap = d.ray_cap, F = d.F;
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   long long nsplit = 0;
   double inflight = 0.0;
-  for (int i0 = blockIdx.x * 256; i0 < n; i0 += gridDim.x * 256) {
+  for (int i0 = r_begin + blockIdx.x * 256; i0 < n; i0 += gridDim.x * 256) {
     const int i = i0 + t;
     const bool live = (i < n) && !d.dead[i];
     int cell = 0, pixel = 0;
@@ -964,13 +967,15 @@ __global__ void k_fill_i32(int* p, int v, long long n) {
 // ---- launchers ------------------------------------------------------------------------------
 void launch_step_begin(const Dev& d, cudaStream_t s) { k_step_begin<<<grid_for(d.nsrc + 1, 256, 1184), 256, 0, s>>>(d); }
 
-void launch_advance(const Dev& d, int grid, cudaStream_t s) {
-  k_advance<<<grid, 256, 0, s>>>(d);
+void launch_advance(const Dev& d, int grid, cudaStream_t s, int block, int pack_grid) {
+  k_advance<<<grid, block, 0, s>>>(d, 0, INT_MAX);
   k_lit_compact<<<grid_for(d.ncell_total >> 4, 256, 148 * 8), 256, 0, s>>>(d);
-  k_moved_pack<<<grid, 256, 0, s>>>(d);
+  k_moved_pack<<<pack_grid > 0 ? pack_grid : grid, 256, 0, s>>>(d);
 }
 
-void launch_walk(const Dev& d, int grid, cudaStream_t s) { k_advance<<<grid, 256, 0, s>>>(d); }
+void launch_walk(const Dev& d, int grid, cudaStream_t s, int block, int r_begin, int r_end) {
+  k_advance<<<grid, block, 0, s>>>(d, r_begin, r_end);
+}
 
 void launch_lit_number(const Dev& d, int grid, cudaStream_t s) {
   k_lit_compact<<<grid_for(d.ncell_total >> 4, 256, 148 * 8), 256, 0, s>>>(d);
@@ -1002,9 +1007,15 @@ void launch_merge(const Dev& d, int grid, cudaStream_t s) {
 }
 
 void launch_split_compact(const Dev& d, int grid, cudaStream_t s) {
-  k_compact_split<<<grid, 256, 0, s>>>(d);
+  k_compact_split<<<grid, 256, 0, s>>>(d, 0, INT_MAX);
   k_swap<<<1, 1, 0, s>>>(d);
 }
+
+void launch_split_range(const Dev& d, int grid, int r_begin, int r_end, cudaStream_t s) {
+  k_compact_split<<<grid, 256, 0, s>>>(d, r_begin, r_end);
+}
+
+void launch_swap(const Dev& d, cudaStream_t s) { k_swap<<<1, 1, 0, s>>>(d); }
 
 void launch_cast(const Dev& d, cudaStream_t s) {
   if (d.nsrc > 0) k_cast<<<grid_for(d.nsrc, 128, 4096), 128, 0, s>>>(d, 0, d.nsrc);

@@ -112,6 +112,20 @@ struct Dev {
   uint8_t* src_own;          // null, or 1 for the sources this context casts (a share of a box's sources)
   // control
   Ctl* ctl;
+  int* rp_queue;           // [kMaxIterQueue] ray-pass work counters, one per C2Ray iteration (chunked queue)
+};
+
+constexpr int kMaxIterQueue = 16;
+
+// Launch shapes of the tunable kernels (frt_tune.h picks them; the defaults are the untuned
+// shapes). Grids are in blocks per SM; rp_chunk = 0 gives each warp of the ray pass a static
+// slice of the moved-ray list, rp_chunk > 0 lets warps take chunks of that many rays from a
+// device-side queue (one atomicAdd per chunk).
+struct Tune {
+  int rp_block = 256, rp_grid = 8, rp_chunk = 0;
+  int adv_block = 256, adv_grid = 8;
+  int lit_grid = 8;
+  int split_grid = 8;
 };
 
 // Buffers of the adjoint of one step's Gamma field (frt_adjoint.cu). Cells on the paths of the
@@ -143,14 +157,18 @@ inline __host__ __device__ int grid_for(long long n, int block, int maxblocks) {
 
 // ---- launchers (frt_geom.cu) ----------------------------------------------------------
 void launch_step_begin(const Dev& d, cudaStream_t s);
-void launch_advance(const Dev& d, int grid, cudaStream_t s);
-void launch_walk(const Dev& d, int grid, cudaStream_t s);         // k_advance alone
+void launch_advance(const Dev& d, int grid, cudaStream_t s, int block = 256, int pack_grid = 0);
+// k_advance alone, over pool rays [r_begin, r_end)
+void launch_walk(const Dev& d, int grid, cudaStream_t s, int block = 256, int r_begin = 0, int r_end = 0x7fffffff);
 void launch_lit_number(const Dev& d, int grid, cudaStream_t s);   // k_lit_compact + k_moved_pack
 // the same with the lit cells numbered in strict cell order (chunk: ncell/4096 ints of scratch)
 void launch_lit_number_ordered(const Dev& d, int* chunk, long long nchunk, int grid, cudaStream_t s);
 void launch_count(const Dev& d, int grid, cudaStream_t s);
 void launch_merge(const Dev& d, int grid, cudaStream_t s);
 void launch_split_compact(const Dev& d, int grid, cudaStream_t s);
+// k_compact_split over pool rays [r_begin, r_end) without the pool swap; then launch_swap
+void launch_split_range(const Dev& d, int grid, int r_begin, int r_end, cudaStream_t s);
+void launch_swap(const Dev& d, cudaStream_t s);
 void launch_cast(const Dev& d, cudaStream_t s);
 void launch_cast_per_source(const Dev& d, cudaStream_t s);   // one launch per source
 void launch_fill_i32(int* p, int v, long long n, cudaStream_t s);
@@ -160,8 +178,9 @@ void launch_pix_table(float4* tab, cudaStream_t s);
 void launch_cosmo_expansion(const Dev& d, int box, float ratio, double rho_factor, int grid, cudaStream_t s);
 // ---- launchers (frt_phys.cu) ----------------------------------------------------------
 void launch_lit_init(const Dev& d, bool strict, int grid, cudaStream_t s);
-void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t s);
-void launch_litpass(const Dev& d, int iter, bool strict, bool fused_thermal, int grid, cudaStream_t s);
+void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t s, int block = 256, int chunk = 0);
+void launch_litpass(const Dev& d, int iter, bool strict, bool fused_thermal, int grid, cudaStream_t s,
+                    int s_begin = 0, int s_end = 0x7fffffff);
 void launch_dark(const Dev& d, bool strict, bool fused_thermal, int grid, cudaStream_t s);
 void launch_thermal_all(const Dev& d, bool strict, int grid, cudaStream_t s);
 void launch_clear_lit(const Dev& d, int grid, cudaStream_t s);

@@ -9,6 +9,7 @@
 // through the iteration with the ray passes in between (k_lit_init, k_raypass, k_litpass).
 // Both paths call the same per-cell device functions (frt_physics.cuh), so a cell gets the same
 // arithmetic whichever path handles it.
+#include <limits.h>
 #include <math.h>
 
 #include "frt_internal.cuh"
@@ -75,6 +76,8 @@ template <bool STRICT>
 __global__ void k_lit_init(Dev d) {
   const int n = min(d.ctl->n_lit, d.lit_cap);
   const int F = d.F, L = d.lit_cap;
+  // the ray passes of this step start with empty work queues
+  if (blockIdx.x == 0 && threadIdx.x < kMaxIterQueue) d.rp_queue[threadIdx.x] = 0;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
     const int gc = d.l_cell[s];
     // every load of the cell first, then the stores (the loads overlap)
@@ -205,9 +208,12 @@ __global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
 }
 
 // Mixed precision, persistent lanes. Rays have 1..path_length segments, so one ray per thread
-// leaves most lanes of a warp idle behind its longest ray. Here every warp owns a contiguous slice
-// of the moved list and a lane takes the slice's next ray as soon as its own ray ends (a ballot
-// and a warp-uniform cursor, no atomics), so every lane walks a segment in every loop trip. A
+// leaves most lanes of a warp idle behind its longest ray. Here a lane takes the next ray of its
+// warp's share of the moved list as soon as its own ray ends (a ballot and a warp-uniform
+// cursor), so every lane walks a segment in every loop trip. The warp's share is either a static
+// contiguous slice of the moved list (chunk = 0: no atomics) or a sequence of chunks of `chunk`
+// rays taken from a device-side queue (queue[iter], one atomicAdd per chunk by lane 0), which
+// evens out warps whose rays happen to be long; the autotuner picks between them. A
 // ray's header (pool index, packed segments, count, box) is one 16-byte load and its segments are
 // contiguous; the loads run two segments ahead of the arithmetic (the next segment's cell state,
 // the segment after it), so a lane's gathers are in flight while it works the current segment.
@@ -217,7 +223,7 @@ __global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
 // NF > 0 fixes the number of frequency bins at compile time (the 5-bin spectrum of every
 // configuration here), so the per-bin loops unroll exactly; NF = 0 takes d.F at run time.
 template <bool LAST, int NF>
-__global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
+__global__ void __launch_bounds__(256) k_raypass_mixed(Dev d, int iter, int chunk) {
   constexpr int MAXF = NF > 0 ? NF : FRT_MAX_FREQ;
   constexpr unsigned FULL = 0xffffffffu;
   const int Fr = NF > 0 ? NF : d.F;
@@ -226,12 +232,19 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
   const int cap = d.ray_cap, L = d.lit_cap;
   const int lane = threadIdx.x & 31;
   const unsigned lanes_below = (1u << lane) - 1u;
-  // this warp's slice [cursor, slice_end) of the moved list
-  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
-  const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const long long per = (nmv + nwarps - 1) / nwarps;
-  long long cursor = wid * per;
-  const long long slice_end = min((long long)nmv, cursor + per);
+  // this warp's current share [cursor, slice_end) of the moved list: its static slice, or (chunked
+  // queue) empty until the first chunk is taken
+  long long cursor = 0, slice_end = 0;
+  bool queue_done = false;
+  int* queue = d.rp_queue + (iter < kMaxIterQueue ? iter : kMaxIterQueue - 1);
+  if (chunk <= 0) {
+    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+    const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const long long per = (nmv + nwarps - 1) / nwarps;
+    cursor = wid * per;
+    slice_end = min((long long)nmv, cursor + per);
+    queue_done = true;
+  }
   double dep = 0.0, kil = 0.0, ovl = 0.0;
   long long nkill = 0;
   int i = -1, p = 0, ns = 0;
@@ -248,9 +261,21 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
     // refill the lanes whose ray ended
     const bool need = (i < 0) && !exhausted;
     const unsigned m = __ballot_sync(FULL, need);
+    if (m && cursor >= slice_end && !queue_done) {
+      // the warp's chunk is used up: take the next one from the queue
+      int base = 0;
+      if (lane == 0) base = atomicAdd(queue, chunk);
+      base = __shfl_sync(FULL, base, 0);
+      if (base >= nmv) {
+        queue_done = true;
+      } else {
+        cursor = base;
+        slice_end = min((long long)nmv, (long long)base + chunk);
+      }
+    }
     if (m) {
       const long long q = cursor + __popc(m & lanes_below);
-      cursor += __popc(m);
+      cursor = min(cursor + __popc(m), max(cursor, slice_end));
       if (need) {
         if (q < slice_end) {
           const int4 hd = d.mv_hdr[q];
@@ -269,8 +294,8 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d) {
 #pragma unroll
           for (int nu = 0; nu < MAXF; nu++) nin[nu] = (nu < Fr) ? A.nphot[(size_t)nu * cap + i] : 0.f;
           av0 = (sg0.x >= 0 && sg0.x < L) ? d.l_avg[sg0.x] : make_float2(0.f, 0.f);
-        } else {
-          exhausted = true;
+        } else if (queue_done) {
+          exhausted = true;   // (a lane short of a chunk's remainder asks again next trip)
         }
       }
     }
@@ -436,12 +461,14 @@ __device__ __forceinline__ Final finalize(float nH, float nHe, float nh1_end, fl
 }
 
 // ---- cell pass of one C2Ray iteration over the lit cells ----------------------------------
+// Lit cells [s_begin, min(s_end, n_lit)) (the autotuner times launch shapes on shares of one
+// pass's cells; the step launches them all).
 template <bool STRICT, bool LAST, bool THERMAL>
-__global__ void __launch_bounds__(256) k_litpass(Dev d) {
-  const int n = min(d.ctl->n_lit, d.lit_cap);
+__global__ void __launch_bounds__(256) k_litpass(Dev d, int s_begin, int s_end) {
+  const int n = min(min(d.ctl->n_lit, d.lit_cap), s_end);
   const int L = d.lit_cap;
   const bool diag = d.outputs == FRT_OUT_DIAG;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+  for (int s = s_begin + blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
     const BoxP& B = d.box[d.l_box[s]];
     const int gc = LAST ? d.l_cell[s] : 0;   // the middle passes touch only the lit arrays
     const float dt = B.dt;
@@ -725,7 +752,7 @@ void launch_lit_init(const Dev& d, bool strict, int grid, cudaStream_t s) {
   else k_lit_init<false><<<grid, 256, 0, s>>>(d);
 }
 
-void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t s) {
+void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t s, int block, int chunk) {
   const bool last = iter == d.itercount - 1;
   if (strict) {
     if (last) k_raypass_strict<true><<<grid, 256, 0, s>>>(d);
@@ -733,24 +760,25 @@ void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t 
     return;
   }
   if (d.F == 5) {
-    if (last) k_raypass_mixed<true, 5><<<grid, 256, 0, s>>>(d);
-    else k_raypass_mixed<false, 5><<<grid, 256, 0, s>>>(d);
+    if (last) k_raypass_mixed<true, 5><<<grid, block, 0, s>>>(d, iter, chunk);
+    else k_raypass_mixed<false, 5><<<grid, block, 0, s>>>(d, iter, chunk);
   } else {
-    if (last) k_raypass_mixed<true, 0><<<grid, 256, 0, s>>>(d);
-    else k_raypass_mixed<false, 0><<<grid, 256, 0, s>>>(d);
+    if (last) k_raypass_mixed<true, 0><<<grid, block, 0, s>>>(d, iter, chunk);
+    else k_raypass_mixed<false, 0><<<grid, block, 0, s>>>(d, iter, chunk);
   }
 }
 
-void launch_litpass(const Dev& d, int iter, bool strict, bool fused_thermal, int grid, cudaStream_t s) {
+void launch_litpass(const Dev& d, int iter, bool strict, bool fused_thermal, int grid, cudaStream_t s, int s_begin,
+                    int s_end) {
   const bool last = iter == d.itercount - 1;
   if (strict) {
-    if (!last) k_litpass<true, false, false><<<grid, 256, 0, s>>>(d);
-    else if (fused_thermal) k_litpass<true, true, true><<<grid, 256, 0, s>>>(d);
-    else k_litpass<true, true, false><<<grid, 256, 0, s>>>(d);
+    if (!last) k_litpass<true, false, false><<<grid, 256, 0, s>>>(d, s_begin, s_end);
+    else if (fused_thermal) k_litpass<true, true, true><<<grid, 256, 0, s>>>(d, s_begin, s_end);
+    else k_litpass<true, true, false><<<grid, 256, 0, s>>>(d, s_begin, s_end);
   } else {
-    if (!last) k_litpass<false, false, false><<<grid, 256, 0, s>>>(d);
-    else if (fused_thermal) k_litpass<false, true, true><<<grid, 256, 0, s>>>(d);
-    else k_litpass<false, true, false><<<grid, 256, 0, s>>>(d);
+    if (!last) k_litpass<false, false, false><<<grid, 256, 0, s>>>(d, s_begin, s_end);
+    else if (fused_thermal) k_litpass<false, true, true><<<grid, 256, 0, s>>>(d, s_begin, s_end);
+    else k_litpass<false, true, false><<<grid, 256, 0, s>>>(d, s_begin, s_end);
   }
 }
 

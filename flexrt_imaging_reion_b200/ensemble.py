@@ -82,9 +82,10 @@ def run_batched(inputs: Sequence[W.BoxInputs], seeds: Sequence[int], warmup: int
         sc = ctx.box_scalars(b)
         per_box[ids[b]] = [sc["t"], sc["dt"], float(ctx.num_rays(b))]
     rays = ctx.num_rays()
+    itercount = ctx.itercount
     ctx.close()
     return {"crossings": cross, "device_ms": dev_ms, "dark_ms": dark_ms, "raypass_ms": rp_ms, "lit_cells": lit,
-            "wall_s": wall, "rays": rays, "per_box": per_box}
+            "wall_s": wall, "rays": rays, "per_box": per_box, "itercount": itercount}
 
 
 def run_per_box_loop(inputs: Sequence[W.BoxInputs], seeds: Sequence[int], warmup: int, steps: int,

@@ -99,6 +99,7 @@ class RTContext:
             cfg.nu_phot[nu] = e / W.H_EV
             cfg.spectrum[nu] = float(self.spectrum[nu])
         cfg.itercount = 5
+        self.itercount = cfg.itercount
         cfg.path_length = path_length
         cfg.hpx_lvl = 0
         cfg.safety_factor = 3.0

@@ -192,7 +192,8 @@ frt_status frt_set_cast_per_source(frt_ctx* ctx, int per_source);
  * find_avg_unu, split_rays, new_rays; main.cc:127-246) by a share of the sources per context:
  * every context holds the whole box, frt_set_source_owner marks the sources it casts (own[s] = 1;
  * NULL = all), and the caller runs the step as frt_step_phase(WALK), combine A, (CELLS), then per
- * C2Ray iteration it: (RAYPASS, it), combine B, (CELLPASS, it), then (END). Combine A ORs the
+ * C2Ray iteration it: (RAYPASS, it), combine B, (CELLPASS, it), then (END). A new source list
+ * (frt_set_sources) clears the mask: set it again after the sources. Combine A ORs the
  * lit-flag bytes (frt_phase_buffers: ncell of them) over the contexts; combine B sums the float2
  * lit-cell pairs lit_acc[nlit] and, after the last iteration's ray pass, lit_heat[nlit]. Every
  * context then runs the same cell passes, and END returns this context's totals (rays, crossings,

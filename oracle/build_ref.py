@@ -32,7 +32,9 @@ from typing import Optional
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
-REF_SRC = "/root/reference"
+# the reference checkout: FRT_REFERENCE_DIR, else the development container's checkout; a box
+# without it rebuilds from the staged copies under oracle/_ref (build(..., from_stage=True))
+REF_SRC = os.environ.get("FRT_REFERENCE_DIR", "/root/reference")
 OUT = os.path.join(HERE, "_ref")
 
 sys.path.insert(0, REPO)

@@ -157,6 +157,11 @@ struct Ctx {
   long last_crossings, last_moved;
   int step;
   unsigned seed;
+  // photon ledger of the last step (physical photons, double): the cast, the photons absorbed on
+  // the last C2Ray iteration (dumps included), the photons left in removed rays, and the photons
+  // that a dumping ray both deposited and kept until its removal. Bookkeeping only: no field or
+  // ray of the restatement depends on it.
+  double led_emitted, led_deposited, led_killed, led_overlap;
 };
 
 static inline long cidx(const Ctx& c, int i, int j, int k) { return ((long)i * c.N + j) * c.N + k; }
@@ -303,6 +308,7 @@ static void init_rays(Ctx& c, int i, int j, int k, double lum) {
       R.z = c.dxc / 2.;
       R.time = 0.;
       R.pind[0] = i * c.N * c.N + j * c.N + k;
+      for (int nu = 0; nu < c.F; nu++) c.led_emitted += (double)R.nphot[nu] * kPhotNorm;
       c.rays.push_back(R);
     }
   }
@@ -444,6 +450,7 @@ static void find_avg_unu(Ctx& c) {
         dtau_he1[nu] = 0.;
       }
       short p = 0;
+      unsigned dump_mask = 0;   // ledger: bins that a dump deposited
       while (p < R.ray_end) {
         const int ind = R.pind[p];
         const long q = ind;
@@ -469,8 +476,13 @@ static void find_avg_unu(Ctx& c) {
             frac_he1[nu] = 0.;
           }
         }
+        const bool last_iter = (iter == c.itercount - 1);
         if (nphot_in_total < c.nphot_min) {
           for (int nu = 0; nu < F; nu++) {
+            if (last_iter) {
+              c.led_deposited += (frac_h1[nu] + frac_he1[nu]) * nphot_in[nu];
+              if (frac_h1[nu] + frac_he1[nu] > 0.) dump_mask |= 1u << nu;
+            }
             c.ngam_nu[q * F + nu] += (float)(nphot_in[nu] / kPhotNorm);
             c.avg_gamma_nu[q * F + nu] += (float)(frac_h1[nu] * nphot_in[nu] / c.dt / vol / c.avg_nh1[q]);
             c.avg_gamma[q] += (float)(frac_h1[nu] * nphot_in[nu] / c.dt / vol / c.avg_nh1[q]);
@@ -480,6 +492,8 @@ static void find_avg_unu(Ctx& c) {
           p = 99;
         } else {
           for (int nu = 0; nu < F; nu++) {
+            if (last_iter)
+              c.led_deposited += (frac_h1[nu] + frac_he1[nu]) * nphot_in[nu] * (1. - exp(-dtau_h1[nu] - dtau_he1[nu]));
             c.ngam_nu[q * F + nu] += (float)(nphot_in[nu] / kPhotNorm);
             c.avg_gamma_nu[q * F + nu] +=
                 (float)(frac_h1[nu] * nphot_in[nu] * (1. - exp(-dtau_h1[nu] - dtau_he1[nu])) / c.dt / vol / c.avg_nh1[q]);
@@ -503,6 +517,9 @@ static void find_avg_unu(Ctx& c) {
           R.active = true;
           R.pind[0] = R.pind[R.ray_end - 1];
         } else {
+          c.led_killed += (double)sum_nphot(c, R) * kPhotNorm;
+          for (int nu = 0; nu < F; nu++)
+            if (dump_mask & (1u << nu)) c.led_overlap += (double)R.nphot[nu] * kPhotNorm;
           R.alive = false;
           R.active = false;
         }
@@ -909,6 +926,7 @@ void* orc_create(const Params* p, const float* delta1, int nsrc, const int32_t* 
   c->t = 0.;
   c->nphot_merge = 0.;
   c->step = 0;
+  c->led_emitted = c->led_deposited = c->led_killed = c->led_overlap = 0.;
   new_rays(*c);
   // get_nphot_min_max (ray_tracing.cc:129-154)
   {
@@ -937,6 +955,7 @@ void* orc_create(const Params* p, const float* delta1, int nsrc, const int32_t* 
 void orc_step(void* h) {
   Ctx& c = *(Ctx*)h;
   c.step += 1;
+  c.led_emitted = c.led_deposited = c.led_killed = c.led_overlap = 0.;
   const long n3 = (long)c.N * c.N * c.N;
   for (long q = 0; q < n3; q++) c.clump[q] = c.const_clump;
   if (c.have_clump) c.clump = c.clump_in;
@@ -953,7 +972,11 @@ void orc_step(void* h) {
     }
   if (c.rkill > 0.0)
     for (Ray& R : c.rays)
-      if (R.alive && (double)R.r > c.rkill) { R.alive = false; R.active = false; }
+      if (R.alive && (double)R.r > c.rkill) {
+        c.led_killed += (double)sum_nphot(c, R) * kPhotNorm;
+        R.alive = false;
+        R.active = false;
+      }
   find_avg_unu(c);
   c.num_thresh = 0;
   for (long q = 0; q < n3; q++) c.num_thresh += (long)(c.ray_per_cell_max - 12 * pow(2, 2 * c.hpx_lvl));
@@ -999,6 +1022,15 @@ int orc_dump(void* h, const char* path) {
   double sc[16];
   orc_scalars(h, sc);
   frtd_add1(&w, "scalars", FRTD_F64, 16, sc);
+  {
+    // photon ledger of the last step: emitted, deposited, killed, overlap, in flight
+    double in_flight = 0.;
+    for (const Ray& R : c.rays)
+      if (R.alive)
+        for (int nu = 0; nu < c.F; nu++) in_flight += (double)R.nphot[nu] * kPhotNorm;
+    const double led[5] = {c.led_emitted, c.led_deposited, c.led_killed, c.led_overlap, in_flight};
+    frtd_add1(&w, "ledger", FRTD_F64, 5, led);
+  }
   frtd_add1(&w, "spectrum", FRTD_F32, c.F, c.spectrum);
   std::vector<const Ray*> live;
   for (const Ray& R : c.rays)

@@ -4,12 +4,14 @@ Tolerances (stated per quantity, checked per cell / per ray):
   * ray tree: (cell, order, pixel, itheta) exact; geometry (x, y, z, r, dr, direction) bit-exact
     except for rays that went through a merge (photon-weighted float sums: 1e-5 relative);
   * ray photon counts: 1e-4 relative (mixed precision) / 1e-6 (strict);
-  * Gamma_HI, Gamma_HeI per cell: 1e-4 relative where the oracle value is above 1e-6 of the box
-    maximum (mixed) / 1e-6 (strict), and both zero where the oracle has no deposit;
-  * x_HI (f_H1) and avg x_HI: 1e-4 absolute; T: 1e-4 relative.
-A ray whose photon count sits within 1e-4 of the removal threshold nphot_min (or of a split
-threshold) may legitimately be kept by one side and removed by the other; such near-tie rays are
-reported separately and not counted as mismatches.
+  * Gamma_HI, Gamma_HeI per cell: 1e-4 relative (mixed) / 1e-5 (strict) in every cell where the
+    oracle deposited (no absolute floor), and zero exactly where the oracle has no deposit;
+  * x_HI (f_H1) and avg x_HI: 1e-4 absolute; T: 1e-3 relative (mixed) / 1e-4 (strict);
+  * photon ledger of a step (emitted, deposited, killed, in flight) against the oracle's own
+    ledger: 1e-6 of the photons emitted since the start.
+A ray whose photon count sits within 1e-4 (relative) of the removal threshold nphot_min may
+legitimately be kept by one side and removed by the other (the ray photon counts themselves are
+held to 1e-4); such near-tie rays are reported separately, and the tests bound their number.
 """
 from __future__ import annotations
 
@@ -28,6 +30,9 @@ from oracle import frtd  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 from flexrt_imaging_reion_b200 import workloads as W  # noqa: E402
 
+# relative distance of a ray's photon count from nphot_min within which keep / remove may differ
+NEAR_TIE = 1e-4
+
 
 def oracle_states(inp: W.BoxInputs, seed: int, steps: int) -> List[Dict[str, np.ndarray]]:
     """States of the CPU oracle after the set-up (index 0) and after each step."""
@@ -42,6 +47,22 @@ def oracle_states(inp: W.BoxInputs, seed: int, steps: int) -> List[Dict[str, np.
             out.append(frtd.read(p))
     o.close()
     return out
+
+
+def oracle_iter(inp: W.BoxInputs, seed: int, steps: int):
+    """The same states as oracle_states, one at a time (for boxes whose states are too large to
+    hold all at once)."""
+    o = O.Oracle(inp, seed)
+    try:
+        with tempfile.TemporaryDirectory() as td:
+            p = os.path.join(td, "s.frtd")
+            for s in range(steps + 1):
+                if s > 0:
+                    o.step()
+                o.dump(p)
+                yield frtd.read(p)
+    finally:
+        o.close()
 
 
 DEVICE_FIELDS = {
@@ -80,8 +101,7 @@ def compare_fields(dev: Dict[str, np.ndarray], ref: Dict[str, np.ndarray], rel_g
     out = {}
     for k in ("gamma_H1_tot", "gamma_He1_tot"):
         a, b = dev[k], ref[k]
-        floor = max(float(np.abs(b).max()) * 1e-6, 1e-300)
-        r = _rel(a, b, floor)
+        r = _rel(a, b, 1e-300)   # relative per cell, no floor
         out[k + "_maxrel"] = float(r.max()) if r.size else 0.0
         out[k + "_bad"] = int((r > rel_gamma).sum())
         out[k + "_zero_mismatch"] = int(((a == 0) != (b == 0)).sum())
@@ -221,12 +241,21 @@ def compare_rays(dev: Dict[str, np.ndarray], ref: Dict[str, np.ndarray], nphot_m
 
     def near_tie(st, ids):
         s = st["ray_nphot"][ids].astype(np.float64).sum(axis=1) if len(ids) else np.zeros(0)
-        return int((np.abs(s / nphot_min - 1.0) < 1e-3).sum()) if nphot_min > 0 else 0
+        return int((np.abs(s / nphot_min - 1.0) < NEAR_TIE).sum()) if nphot_min > 0 else 0
 
     out["unmatched_dev"] = len(ud2)
     out["unmatched_ref"] = len(ur2)
     out["unmatched_near_tie"] = near_tie(dev, ud2) + near_tie(ref, ur2)
     return out
+
+
+def compare_ledger(stats: Dict[str, float], ref: Dict[str, np.ndarray], emitted_total: float) -> Dict[str, float]:
+    """Device photon totals of one step against the oracle's ledger of the same step (emitted,
+    deposited on the last C2Ray iteration, killed, dumped-and-killed overlap, in flight after the
+    step), each difference divided by the photons emitted since the start of the run."""
+    led = ref["ledger"]
+    keys = ("photons_emitted", "photons_deposited", "photons_killed", "photons_overlap", "photons_in_flight")
+    return {k: abs(float(stats[k]) - float(led[j])) / emitted_total for j, k in enumerate(keys)}
 
 
 def photon_budget(stats_list, in_flight_0: float) -> float:

@@ -56,3 +56,71 @@ def test_ensemble_photon_budget():
     stats = [ctx.step() for _ in range(4)]
     assert PT.photon_budget(stats, in0) < 1e-6
     ctx.close()
+
+
+def e_subset():
+    """One box of the uneven ensemble per grid size (32, 64, 96, 128 cells per side), each the one
+    with the most sources of its size; the box with the most sources of the whole ensemble (4005)
+    is among them."""
+    from flexrt_imaging_reion_b200 import ensemble as EN  # noqa: F401
+    specs = W.config_E()
+    pick = {}
+    for b, s in enumerate(specs):
+        if s.n not in pick or s.n_src > specs[pick[s.n]].n_src:
+            pick[s.n] = b
+    return [(specs[b], 1234 + b) for _, b in sorted(pick.items())]
+
+
+def test_e_subset_parity():
+    """Four real ensemble boxes (32^3 to 128^3, 3546-4005 sources each), batched in one context
+    as the benchmark runs them, 3 steps, against one oracle run per box; the step's photon ledger
+    of the context against the sum of the boxes' oracle ledgers."""
+    from flexrt_imaging_reion_b200 import ensemble as EN
+    boxes = e_subset()
+    steps = 3
+    refs = [PT.oracle_states(W.make_inputs(spec), seed, steps) for spec, seed in boxes]
+    inputs = [W.make_inputs(spec) for spec, _ in boxes]
+    ctx = rt.RTContext(inputs, [seed for _, seed in boxes], precision="mixed", outputs="core",
+                       ray_capacity=EN.ray_capacity([spec for spec, _ in boxes]))
+    ctx.setup()
+    states = [[PT.device_state(ctx, b, False)] for b in range(len(boxes))]
+    stats = []
+    for s in range(1, steps + 1):
+        st = ctx.step(graph=True)
+        assert st["error_flags"] == 0, st
+        assert st["crossings"] == sum(int(r[s]["scalars"][10]) for r in refs)
+        stats.append(st)
+        for b in range(len(boxes)):
+            states[b].append(PT.device_state(ctx, b, False))
+    ctx.close()
+    for b in range(len(boxes)):
+        check(states[b], refs[b], False)
+    emitted = sum(float(r[0]["ledger"][0]) for r in refs)
+    for s in range(1, steps + 1):
+        emitted += sum(float(r[s]["ledger"][0]) for r in refs)
+        led = {k: 0.0 for k in ("photons_emitted", "photons_deposited", "photons_killed", "photons_overlap",
+                                "photons_in_flight")}
+        for j, k in enumerate(led):
+            led[k] = abs(float(stats[s - 1][k]) - sum(float(r[s]["ledger"][j]) for r in refs)) / emitted
+        assert max(led.values()) < 1e-6, (s, led)
+
+
+def test_e_batched_graph_beats_per_box_loop():
+    """The whole uneven ensemble (96 boxes, 32^3-128^3): the batched form (all boxes in one
+    context, one graph launch per step) against the per-box loop (one context per box, every
+    kernel launched directly, boxes one after another), the same boxes, seeds and steps, both timed
+    by host wall clock around the steps. Target: batched at least 3x the loop's crossings/s, with
+    the same crossings (ray trees identical up to nphot_min ties)."""
+    from flexrt_imaging_reion_b200 import ensemble as EN
+    specs = W.config_E()
+    inputs = [W.make_inputs(s) for s in specs]
+    seeds = [1234 + b for b in range(len(specs))]
+    warmup, steps = 3, 4
+    bat = EN.run_batched(inputs, seeds, warmup, steps)
+    loop = EN.run_per_box_loop(inputs, seeds, warmup, steps)
+    rate_b = bat["crossings"] / bat["wall_s"]
+    rate_l = loop["crossings"] / loop["wall_s"]
+    print(f"E: batched {rate_b:.3e} crossings/s ({1e3 * bat['wall_s'] / steps:.2f} ms/step), per-box loop "
+          f"{rate_l:.3e} ({1e3 * loop['wall_s'] / steps:.2f} ms/step), ratio {rate_b / rate_l:.2f}")
+    assert abs(bat["crossings"] - loop["crossings"]) <= 1e-5 * bat["crossings"]
+    assert rate_b >= 3.0 * rate_l
