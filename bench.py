@@ -52,6 +52,8 @@ DARK_TRAFFIC_BYTES_PER_CELL = 1343184384 / 13264001
 # the mean over the 5 passes of step 24 of L (17 465 923 crossings per pass; 679.6 MB per launch).
 # The number of ray passes per step is the context's C2Ray iteration count (RTContext.itercount).
 RAYPASS_BYTES_PER_CROSSING = 8 + 8 + 68
+# warm-up steps that frt_autotune takes (the last ones of the warm-up)
+AUTOTUNE_STEPS = 3
 RAYPASS_TRAFFIC_BYTES_PER_CROSSING = 38.9
 
 
@@ -251,7 +253,9 @@ def run_ensemble(args, rank: int, world: int, local_rank: int):
         tdist.barrier()
     clocks = ClockSampler(local_rank)
     clocks.start()
-    bat = EN.run_batched(inputs, seeds, args.warmup, args.steps, device=local_rank, box_ids=mine)
+    n_tune = AUTOTUNE_STEPS if (not args.no_autotune and args.warmup >= AUTOTUNE_STEPS + 1) else 0
+    bat = EN.run_batched(inputs, seeds, args.warmup, args.steps, device=local_rank, box_ids=mine,
+                         autotune_steps=n_tune)
     clk = clocks.stop()
     per_box = EN.gather_box_results(bat["per_box"], world)
     ncell = sum(s.n ** 3 for s in (specs[b] for b in mine))
@@ -279,7 +283,8 @@ def run_ensemble(args, rank: int, world: int, local_rank: int):
         "data": "synthetic (seeded lognormal gas + L^-2 sources per box)",
         "config": {"workload": _describe_ensemble(specs), "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps}",
                    "graph": True, "l2": "state larger than L2, no flush",
-                   "parallelism": f"boxes sharded over {world} ranks (LPT)" if dist else "single"},
+                   "parallelism": f"boxes sharded over {world} ranks (LPT)" if dist else "single",
+                   "launch_shapes": _tuning_config(bat.get("tuning"))},
         "e2e": {"value": cross / wall, "unit": "crossings/s", "h2d_bytes_per_step": 2 * len(mine) + 2 * sum(
             len(W.grid_sources(i)[1]) for i in inputs), "d2h_bytes_per_step": 144},
         # the ray pass (five launches per step on the main stream), as for a single box
@@ -431,6 +436,29 @@ def run_partition(args, rank: int, world: int, local_rank: int):
     }
 
 
+def warm_up(ctx, args):
+    """The W warm-up steps: graph steps, the last AUTOTUNE_STEPS of them taken by frt_autotune
+    (real steps that also time candidate launch shapes; the chosen shapes are then captured in
+    the step graph). Returns the chosen shapes, or None without autotuning."""
+    n_tune = AUTOTUNE_STEPS if (not args.no_autotune and args.warmup >= AUTOTUNE_STEPS + 1) else 0
+    for _ in range(args.warmup - n_tune):
+        ctx.step(graph=not args.plain)
+    if not n_tune:
+        return None
+    return ctx.autotune(n_tune)
+
+
+def _tuning_config(t):
+    if t is None:
+        return "default shapes (no autotuning)"
+    keys = ("raypass_block", "raypass_blocks_per_sm", "raypass_chunk", "walk_block", "walk_blocks_per_sm",
+            "cellpass_blocks_per_sm", "split_blocks_per_sm", "steps")
+    out = {k: int(t[k]) for k in keys}
+    out["measured_ns"] = {k: round(float(t[k]), 4) for k in ("raypass_ns_per_crossing", "walk_ns_per_ray",
+                                                              "cellpass_ns_per_cell", "split_ns_per_ray")}
+    return out
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import numpy as np
     from flexrt_imaging_reion_b200 import workloads as W, rt
@@ -441,8 +469,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     ctx.setup()
     ncell = spec.n ** 3
     itercount = ctx.itercount
-    for _ in range(args.warmup):
-        ctx.step(graph=not args.plain)
+    tuning = warm_up(ctx, args)
     dist = world > 1
     if dist:
         import torch
@@ -504,7 +531,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "data": "synthetic (seeded lognormal gas + L^-2 sources; the reference's inputs are not shipped)",
         "config": {"workload": _describe(spec), "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps}",
                    "graph": not args.plain, "l2": "state (>1 GB) larger than L2, no flush",
-                   "parallelism": "replicas" if world > 1 else "single"},
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "launch_shapes": _tuning_config(tuning)},
         "e2e": {"value": cross_all / wall_max, "unit": "crossings/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         # the dominant kernel: the ray pass (five launches per step, one per C2Ray iteration)
@@ -555,6 +583,7 @@ def main():
     ap.add_argument("--ray-capacity", type=int, default=16 << 20)
     ap.add_argument("--lit-capacity", type=int, default=0, help="0 = all cells")
     ap.add_argument("--plain", action="store_true", help="launch kernels directly instead of the CUDA graph")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--cpu-baseline-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # the reference arm times the same step window as this arm (about 8-10 s per L step on 16 cores)

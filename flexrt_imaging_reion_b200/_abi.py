@@ -34,7 +34,7 @@ EXPORTS = ["frt_create", "frt_destroy", "frt_last_error", "frt_rotation_table", 
            "frt_last_adjoint_timing", "frt_write_gas", "frt_write_rays", "frt_write_treion", "frt_read_gas",
            "frt_read_treion", "frt_read_rays", "frt_update_cosmo_expansion",
            "frt_set_cast_per_source", "frt_last_kernel_timing", "frt_set_source_owner", "frt_step_phase",
-           "frt_phase_buffers"]
+           "frt_phase_buffers", "frt_autotune", "frt_get_tuning", "frt_set_tuning", "frt_update_hydro_step"]
 PHASE_WALK, PHASE_CELLS, PHASE_RAYPASS, PHASE_CELLPASS, PHASE_END = 0, 1, 2, 3, 4
 NOALLOC_MAX_CELLS = 1 << 20
 
@@ -56,6 +56,17 @@ class Config(C.Structure):
                 ("temp_0", C.c_float), ("nbox", C.c_int), ("boxes", C.POINTER(BoxDesc)),
                 ("ray_capacity", C.c_longlong), ("lit_capacity", C.c_longlong), ("src_capacity", C.c_longlong),
                 ("precision", C.c_int), ("outputs", C.c_int), ("device", C.c_int)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("raypass_block", C.c_int), ("raypass_blocks_per_sm", C.c_int), ("raypass_chunk", C.c_int),
+                ("walk_block", C.c_int), ("walk_blocks_per_sm", C.c_int), ("cellpass_blocks_per_sm", C.c_int),
+                ("split_blocks_per_sm", C.c_int), ("steps", C.c_int), ("raypass_ns_per_crossing", C.c_double),
+                ("walk_ns_per_ray", C.c_double), ("cellpass_ns_per_cell", C.c_double),
+                ("split_ns_per_ray", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class StepStats(C.Structure):
@@ -130,6 +141,10 @@ def lib() -> C.CDLL:
         "frt_step_phase": ([P, I, I, P, P, C.POINTER(StepStats)], I),
         "frt_phase_buffers": ([P, C.POINTER(P), C.POINTER(LL), C.POINTER(P), C.POINTER(P), C.POINTER(LL)], I),
         "frt_last_kernel_timing": ([P, I, P], I),
+        "frt_autotune": ([P, I, C.POINTER(Tuning)], I),
+        "frt_update_hydro_step": ([P, I, P, C.c_float, C.c_float, C.c_float, I, P, P], I),
+        "frt_get_tuning": ([P, C.POINTER(Tuning)], I),
+        "frt_set_tuning": ([P, C.POINTER(Tuning)], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -28,7 +28,7 @@ SOURCES = [
     ("frt_adjoint.cu", ["-fmad=false"]),
     ("frt_ctx.cu", []),
 ]
-HEADERS = ["frt_internal.cuh", "frt_physics.cuh", "frt_params.h", "hp_nest.h", "frt_hostmath.h", "frt_dda.cuh",
+HEADERS = ["frt_internal.cuh", "frt_physics.cuh", "frt_params.h", "hp_nest.h", "frt_hostmath.h", "frt_dda.cuh", "frt_tune.h",
            os.path.join("..", "..", "include", "flexrt.h")]
 
 
@@ -56,11 +56,12 @@ def build(verbose: bool = False, force: bool = False) -> str:
         if force or _newer(o, [s] + hdrs + [__file__]):
             _run(["nvcc"] + ARCH + NVCC_COMMON + extra + ["-c", s, "-o", o], verbose)
         objs.append(o)
-    s = os.path.join(CSRC, "frt_hostmath.cc")
-    o = os.path.join(OBJ, "frt_hostmath.o")
-    if force or _newer(o, [s] + hdrs + [__file__]):
-        _run(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-c", s, "-o", o], verbose)
-    objs.append(o)
+    for src in ("frt_hostmath.cc", "frt_tune.cc"):
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJ, src.replace(".cc", ".o"))
+        if force or _newer(o, [s] + hdrs + [__file__]):
+            _run(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-c", s, "-o", o], verbose)
+        objs.append(o)
     if force or _newer(LIB, objs):
         _run(["nvcc"] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"], verbose)
     return LIB

@@ -270,6 +270,30 @@ __global__ void k_adj_objective(AdjDev a) {
   if (threadIdx.x == 0 && s != 0.0) atomicAdd(a.J, s);
 }
 
+// The source that cast a ray, from the ray alone. The cast puts a ray at the centre of its
+// source's cell with r = 0 (ray_tracing.cc:300-312); the advance moves it along its direction
+// while r grows by the comoving distance (ray_tracing.cc:1259-1263); a split places each child at
+// the parent's position plus (child direction - parent direction) r dx/dx0 (ray_tracing.cc:540-548).
+// So every ray that no merge has touched sits at source + r (dx/dx0) direction, up to the corner
+// nudges of 1e-4 cells, and in cell units the source cell is floor(i + x/dx - r xhat/dx0)
+// (periodic), the same for y and z. Returns the context-wide source index, or -1.
+__device__ __forceinline__ int ray_source(const Dev& d, const AdjDev& a, const RayPool& A, int i) {
+  const BoxP& B = d.box[A.box[i]];
+  const int N = B.n;
+  const int ind = A.cell[i];
+  const int ii = ind / B.nn, jj = (ind - ii * B.nn) / N, kk = ind - ii * B.nn - jj * N;
+  const double r = (double)A.r[i] / (double)B.dx0;
+  const double gx = ii + (double)A.x[i] / (double)B.dx - r * (double)A.xh[i];
+  const double gy = jj + (double)A.y[i] / (double)B.dx - r * (double)A.yh[i];
+  const double gz = kk + (double)A.z[i] / (double)B.dx - r * (double)A.zh[i];
+  auto wrap = [N](double g) {
+    long long c = (long long)floor(g) % N;
+    return (int)(c < 0 ? c + N : c);
+  };
+  const long long cell = ((long long)wrap(gx) * N + wrap(gy)) * N + wrap(gz);
+  return a.src_of_cell[B.cell0 + cell];
+}
+
 // reverse ray pass k: from the rate weights Gbar^k of the path cells to abar^k, bbar^k and to
 // the sources' photon counts
 __global__ void k_adj_rev_ray(Dev d, AdjDev a, int k) {
@@ -312,7 +336,7 @@ __global__ void k_adj_rev_ray(Dev d, AdjDev a, int k) {
       dl += tot[nu];   // n0 dJ/dn0 (J_ray is linear in n0)
       nin[nu] = n0[nu];
     }
-    const int src = a.src_of_cell[(long long)B.cell0 + A.cell[i]];
+    const int src = ray_source(d, a, A, i);
     if (src >= 0 && dl != 0.0) atomicAdd(&a.dlbar[src], dl);
     // walk 2: derivatives of every segment's g and transmission
     double pre[FRT_MAX_FREQ];

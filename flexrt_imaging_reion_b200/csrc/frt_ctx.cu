@@ -6,11 +6,14 @@
 #include <string.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "frt_hostmath.h"
 #include "frt_internal.cuh"
+#include "frt_tune.h"
 
 using namespace frt;
 
@@ -32,6 +35,9 @@ struct frt_ctx {
   std::vector<char> restarted;           // gas read from a restart file (init_rt's restart branch)
   std::vector<float> restart_t;          // its time
   std::vector<std::vector<float>> rho;  // host copy of the proper density (set-up output)
+  std::vector<std::vector<float>> rho_prev_h;   // the last hydro switch's density (host copy)
+  std::vector<char> frac_kept;   // an expansion just kept the ionised fractions (d.frac_h2, frac_he2)
+  std::vector<float> step_dt;    // the time step the last step ran with, per box
   std::vector<float> rot;
   // pinned staging
   uint16_t* h_ith_box = nullptr;
@@ -46,13 +52,18 @@ struct frt_ctx {
   bool strict = false;
   int grid_rays = 0, grid_cells = 0, grid_lit = 0;
   int nsm = 148;
+  std::string dev_name;
   Tune tune;               // launch shapes of the tunable kernels (frt_autotune / frt_set_tuning)
+  bool tune_auto = false;  // frt_step follows the remembered shapes of the ray-count bucket
+  frt_tuning tune_measured{};
   int grid_dark = 0;       // one block per 256 cells: short blocks that yield SM slots to the lit chain
   float last_step_ms = 0.f, last_dark_ms = 0.f;
-  bool rays_moved = false;   // an advance, merge or split ran (rays no longer one source's cast)
+  bool rays_moved = false;   // an advance, merge or split ran
+  bool merged_any = false;   // a merge combined rays (a merged ray may mix the photons of several sources)
   bool cast_per_source = false;   // unbatched cast in the direct-launch step (comparison baseline)
   AdjDev adj{};
   bool adj_ready = false;
+  bool adj_src_stale = true;   // the source-cell map of the adjoint follows the source list
   float* adj_out = nullptr;   // gather buffer of the adjoint's per-cell output (largest box)
   float last_adjoint_ms = 0.f;
   frt_step_stats last{};
@@ -146,6 +157,7 @@ frt_status upload_sources(frt_ctx* ctx) {
   // kernel reads owner bytes that were never written for the new sources (all sources are cast
   // until the caller sets a mask for the new list)
   ctx->d.src_own = nullptr;
+  ctx->adj_src_stale = true;
   if (n) {
     CK(cudaMemcpy(ctx->d.src_cell, cell.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->d.src_box, box.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice));
@@ -157,6 +169,13 @@ frt_status upload_sources(frt_ctx* ctx) {
 }
 
 // ---- step sequences ---------------------------------------------------------------------------
+// Host bookkeeping of a step about to run: its time step per box (get_nphot_min_max at a hydro
+// switch after it uses it), and the fractions an expansion kept are stale once cells update.
+void note_step(frt_ctx* ctx) {
+  for (size_t b = 0; b < ctx->hbox.size(); b++) ctx->step_dt[b] = ctx->hbox[b].dt;
+  std::fill(ctx->frac_kept.begin(), ctx->frac_kept.end(), 0);
+}
+
 void enqueue_begin_advance(frt_ctx* ctx) {
   ctx->rays_moved = true;
   const Dev& d = ctx->d;
@@ -297,6 +316,7 @@ frt_status finish_step(frt_ctx* ctx, frt_step_stats* stats) {
     rms += x;
   }
   ctx->last_raypass_ms = rms;
+  if (ctx->h_ctl->merged > 0) ctx->merged_any = true;
   fill_stats(ctx, *ctx->h_ctl, stats);
   if (ctx->h_ctl->err) {
     ctx->err = "device error flags " + std::to_string(ctx->h_ctl->err) +
@@ -327,6 +347,11 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
   int nsm = 148;
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cfg->device));
   ctx->nsm = nsm;
+  {
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, cfg->device));
+    ctx->dev_name = prop.name;
+  }
   ctx->grid_rays = nsm * 8;
   ctx->grid_cells = nsm * 8;
   ctx->grid_lit = nsm * 8;
@@ -479,6 +504,9 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
   ctx->src_cell.resize(cfg->nbox);
   ctx->src_lum.resize(cfg->nbox);
   ctx->gas_ready.assign(cfg->nbox, 0);
+  ctx->rho_prev_h.resize(cfg->nbox);
+  ctx->frac_kept.assign(cfg->nbox, 0);
+  ctx->step_dt.assign(cfg->nbox, 0.f);
   ctx->restarted.assign(cfg->nbox, 0);
   ctx->restart_t.assign(cfg->nbox, 0.f);
   ctx->rho.resize(cfg->nbox);
@@ -551,7 +579,13 @@ frt_status frt_init_gas(frt_ctx* ctx, int box, const float* delta1) {
   ctx->rho[box] = rho;
   ctx->gas_ready[box] = 1;
   ctx->restarted[box] = 0;
-  return FRT_OK;
+  {
+    // <rho> of the snapshot (get_ugas, io_funcs.cc:61, then a^-3, gas_funcs.cc:613)
+    std::vector<float> tmp(n);
+    host::snapshot_rho(B.n, delta1, (float)(1. / (1. + ctx->boxes[box].zz)), tmp.data(), &ctx->hbox[box].avg_rho);
+  }
+  ctx->rho_prev_h[box].clear();
+  return upload_boxes(ctx);
 }
 
 frt_status frt_set_sources(frt_ctx* ctx, int box, int nsrc, const int32_t* ijk, const double* lum) {
@@ -767,6 +801,7 @@ frt_status frt_init_rt(frt_ctx* ctx) {
     ctx->hbox[b].nphot_merge = 0.f;
   }
   ctx->rays_moved = false;
+  ctx->merged_any = false;
   return upload_boxes(ctx);
 }
 
@@ -786,6 +821,8 @@ frt_status frt_update_cosmo_expansion(frt_ctx* ctx, const float* a_current, cons
     for (size_t b = 0; b < ctx->hbox.size(); b++)
       CK(cudaMemcpy(d.rho + ctx->hbox[b].cell0, ctx->rho[b].data(), sizeof(float) * ctx->rho[b].size(),
                     cudaMemcpyHostToDevice));
+    if ((st = dalloc(ctx, &d.frac_h2, (size_t)d.ncell_total))) return st;
+    if ((st = dalloc(ctx, &d.frac_he2, (size_t)d.ncell_total))) return st;
     ctx->graph_valid = false;   // the graph keeps a copy of the device pointers
   }
   frt_status st = download_boxes(ctx);
@@ -796,6 +833,8 @@ frt_status frt_update_cosmo_expansion(frt_ctx* ctx, const float* a_current, cons
     // gas_funcs.cc:472-485: dx[i] *= a_current/a_prev; rho *= pow(a_prev/a_current, 3.)
     ratio[b] = a_current[b] / a_prev[b];
     rf[b] = pow(a_prev[b] / a_current[b], 3.);
+    ctx->hbox[b].avg_rho *= pow(a_prev[b] / a_current[b], 3.);   // gas_funcs.cc:520
+    ctx->frac_kept[b] = 1;
     float dx = ctx->hbox[b].dx;
     dx *= ratio[b];
     host::set_cell_size(&ctx->hbox[b], &ctx->cfg, &ctx->boxes[b], dx);
@@ -804,6 +843,88 @@ frt_status frt_update_cosmo_expansion(frt_ctx* ctx, const float* a_current, cons
   for (size_t b = 0; b < ctx->hbox.size(); b++)
     launch_cosmo_expansion(d, (int)b, ratio[b], rf[b], ctx->grid_cells, ctx->s_main);
   return sync_and_check(ctx);
+}
+
+frt_status frt_update_hydro_step(frt_ctx* ctx, int box, const float* delta1, float a_rt, float dt_snap, float zz,
+                                 int nsrc, const int32_t* ijk, const double* lum) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  if (!delta1 || !(a_rt > 0.f) || !(dt_snap > 0.f) || !ctx->gas_ready[box] || nsrc < 0 ||
+      (nsrc > 0 && (!ijk || !lum))) {
+    ctx->err = "frt_update_hydro_step: density, a positive scale factor and snapshot interval, gas set up";
+    return FRT_ERR_INVALID;
+  }
+  Dev& d = ctx->d;
+  CK(cudaStreamSynchronize(ctx->s_main));
+  CK(cudaStreamSynchronize(ctx->s_dark));
+  BoxP& B = ctx->hbox[box];
+  const size_t n = (size_t)B.ncell;
+  // the new proper density and <rho> (get_ugas, then a_rt^-3)
+  std::vector<float> rho(n);
+  float avg = 0.f;
+  host::snapshot_rho(B.n, delta1, a_rt, rho.data(), &avg);
+  // <rho_prev> over the previous snapshot's density (0 before any switch: no d(delta)/dt yet)
+  const float avg_prev = ctx->rho_prev_h[box].empty() ? 0.f : host::vol_avg(ctx->rho_prev_h[box].data(), B.n);
+  if (!d.rho) {
+    if ((st = dalloc(ctx, &d.rho, (size_t)d.ncell_total))) return st;
+    for (size_t b = 0; b < ctx->hbox.size(); b++)
+      if (ctx->rho[b].size() == (size_t)ctx->hbox[b].ncell)
+        CK(cudaMemcpy(d.rho + ctx->hbox[b].cell0, ctx->rho[b].data(), sizeof(float) * ctx->rho[b].size(),
+                      cudaMemcpyHostToDevice));
+    ctx->graph_valid = false;
+  }
+  if (!d.rho_prev) {
+    if ((st = dalloc(ctx, &d.rho_prev, (size_t)d.ncell_total))) return st;
+    ctx->graph_valid = false;
+  }
+  if (avg_prev > 0.f && !d.ddelta) {
+    if ((st = dalloc(ctx, &d.ddelta, (size_t)d.ncell_total))) return st;   // 0 in the other boxes
+    ctx->graph_valid = false;
+  }
+  CK(cudaMemcpy(d.rho + B.cell0, rho.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  // the box at the new snapshot: redshift, cell size Lx0 a_rt / N (gas_funcs.cc:590-592, 689-691)
+  host::set_cell_size(&B, &ctx->cfg, &ctx->boxes[box], host::snapshot_dx(&ctx->boxes[box], a_rt));
+  host::set_redshift(&B, zz);
+  B.avg_rho = avg;
+  if ((st = upload_boxes(ctx))) return st;
+  const bool cached = ctx->frac_kept[box] && d.frac_h2;
+  launch_hydro_switch(d, box, cached, avg_prev, dt_snap, ctx->grid_cells, ctx->s_main);
+  ctx->frac_kept[box] = 0;
+  if ((st = sync_and_check(ctx))) return st;
+  ctx->rho[box] = rho;
+  ctx->rho_prev_h[box] = rho;
+  ctx->boxes[box].zz = zz;
+  // read_source_catalog (io_funcs.cc:157-233): the new sources, every ray_dt back to 0
+  ctx->src_cell[box].clear();
+  ctx->src_lum[box].clear();
+  for (int s = 0; s < nsrc; s++) {
+    const int i = ijk[3 * s], j = ijk[3 * s + 1], k = ijk[3 * s + 2];
+    if (i < 0 || j < 0 || k < 0 || i >= B.n || j >= B.n || k >= B.n) {
+      ctx->err = "source cell out of range";
+      return FRT_ERR_INVALID;
+    }
+    ctx->src_cell[box].push_back((i * B.n + j) * B.n + k);
+    ctx->src_lum[box].push_back(lum[s]);
+  }
+  if ((st = upload_sources(ctx))) return st;   // ray_dt of every source 0
+  // get_nphot_min_max (main.cc:222) with the new sources and the step's time step
+  double mn = 0., mx = 0.;
+  if (!ctx->src_lum[box].empty()) {
+    BoxP tmp = B;
+    tmp.dt = ctx->step_dt[box] > 0.f ? ctx->step_dt[box] : B.dt;
+    host::nphot_min_max(&ctx->cfg, &tmp, (int)ctx->src_lum[box].size(), ctx->src_lum[box].data(), &mn, &mx);
+  }
+  B.nphot_min = mn;
+  B.nphot_max = mx;
+  {
+    std::vector<double> lg(2);   // as frt_get_nphot_min_max: log10 nphot_min and the PDF bin width
+    lg[0] = log10(mn);
+    lg[1] = (log10(mx) - log10(mn)) / (10000 - 1);
+    CK(cudaMemcpy(d.lg + 2 * box, lg.data(), sizeof(double) * 2, cudaMemcpyHostToDevice));
+  }
+  const float a4 = (float)(4. * (double)B.nphot_merge), c4 = (float)(4. * B.nphot_min);
+  B.split_thr = (c4 >= a4) ? c4 : a4;
+  return upload_boxes(ctx);
 }
 
 frt_status frt_update_dt(frt_ctx* ctx, float* dt_out) {
@@ -842,6 +963,7 @@ frt_status frt_set_clight(frt_ctx* ctx) { return ctx ? FRT_OK : FRT_ERR_INVALID;
 
 frt_status frt_update_rays(frt_ctx* ctx) {
   if (!ctx) return FRT_ERR_INVALID;
+  note_step(ctx);
   enqueue_begin_advance(ctx);
   return sync_and_check(ctx);
 }
@@ -871,7 +993,12 @@ frt_status frt_merge(frt_ctx* ctx, const uint16_t* itheta_per_box) {
                      ctx->s_main));
   launch_count(ctx->d, ctx->grid_rays, ctx->s_main);
   launch_merge(ctx->d, ctx->grid_rays, ctx->s_main);
-  return sync_and_check(ctx);
+  frt_status st2 = sync_and_check(ctx);
+  if (st2) return st2;
+  long long merged = 0;
+  CK(cudaMemcpy(&merged, &ctx->d.ctl->merged, sizeof merged, cudaMemcpyDeviceToHost));
+  if (merged > 0) ctx->merged_any = true;
+  return FRT_OK;
 }
 
 frt_status frt_split_rays(frt_ctx* ctx) {
@@ -923,6 +1050,33 @@ frt_status frt_draw_step(frt_ctx* ctx, uint16_t* itheta_per_box, uint16_t* ithet
   return draw(ctx, itheta_per_box, itheta_per_source);
 }
 
+// ---- remembered launch shapes (frt_autotune) ------------------------------------------------
+// One shape set per (device, SM count, cells, precision, power-of-two bucket of the live rays).
+static std::mutex g_tune_mu;
+static std::map<std::string, Tune> g_tune_cache;
+
+static std::string tune_key(const frt_ctx* ctx, long long rays) {
+  int bucket = 0;
+  while (bucket < 62 && (2LL << bucket) <= rays) bucket++;
+  return ctx->dev_name + "|" + std::to_string(ctx->nsm) + "|" + std::to_string(ctx->d.ncell_total) + "|" +
+         (ctx->strict ? "strict" : "mixed") + "|" + std::to_string(bucket);
+}
+
+// frt_step: switch to the remembered shapes of the current ray-count bucket, if any
+static void follow_tune_cache(frt_ctx* ctx) {
+  Tune t;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(tune_key(ctx, ctx->last.rays_alive));
+    if (it == g_tune_cache.end()) return;
+    t = it->second;
+  }
+  if (!(t == ctx->tune)) {
+    ctx->tune = t;
+    ctx->graph_valid = false;
+  }
+}
+
 // Resolve the step's angle indices: caller-provided, or drawn from the context's streams.
 static frt_status step_inputs(frt_ctx* ctx, const uint16_t* ib, const uint16_t* is) {
   if (!ib && !is) {
@@ -940,6 +1094,7 @@ frt_status frt_step_plain(frt_ctx* ctx, const uint16_t* itheta_per_box, const ui
   if (!ctx) return FRT_ERR_INVALID;
   frt_status st = step_inputs(ctx, itheta_per_box, itheta_per_source);
   if (st) return st;
+  note_step(ctx);
   CK(cudaEventRecord(ctx->ev_t0, ctx->s_main));
   enqueue_step(ctx, false);
   CK(cudaEventRecord(ctx->ev_t1, ctx->s_main));
@@ -951,6 +1106,7 @@ frt_status frt_step(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t
   if (!ctx) return FRT_ERR_INVALID;
   frt_status st = step_inputs(ctx, itheta_per_box, itheta_per_source);
   if (st) return st;
+  if (ctx->tune_auto) follow_tune_cache(ctx);
   if (!ctx->graph_valid) {
     if (ctx->graph) {
       cudaGraphExecDestroy(ctx->graph);
@@ -965,6 +1121,7 @@ frt_status frt_step(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t
     CK(cudaGraphDestroy(g));
     ctx->graph_valid = true;
   }
+  note_step(ctx);
   CK(cudaEventRecord(ctx->ev_t0, ctx->s_main));
   CK(cudaGraphLaunch(ctx->graph, ctx->s_main));
   CK(cudaEventRecord(ctx->ev_t1, ctx->s_main));
@@ -1118,6 +1275,7 @@ frt_status frt_step_phase(frt_ctx* ctx, int phase, int iter, const uint16_t* ith
       CK(cudaMemcpyAsync(d.itheta_merge, ctx->h_ith_box, sizeof(uint16_t) * d.nbox, cudaMemcpyHostToDevice, s));
       if (d.nsrc)
         CK(cudaMemcpyAsync(d.src_itheta, ctx->h_ith_src, sizeof(uint16_t) * d.nsrc, cudaMemcpyHostToDevice, s));
+      note_step(ctx);
       CK(cudaEventRecord(ctx->ev_t0, s));
       ctx->rays_moved = true;
       launch_clear_lit(d, ctx->grid_lit, s);
@@ -1493,13 +1651,20 @@ frt_status adj_alloc(frt_ctx* ctx) {
   long long maxcell = 1;
   for (const BoxP& B : ctx->hbox) maxcell = std::max(maxcell, B.ncell);
   AL(ctx->adj_out, (size_t)maxcell);
-  // source cell -> context-wide source index
+  ctx->adj_ready = true;
+  return FRT_OK;
+}
+
+// source cell -> context-wide source index, rebuilt after the source list changed
+frt_status adj_source_map(frt_ctx* ctx) {
+  if (!ctx->adj_src_stale) return FRT_OK;
+  const size_t NC = (size_t)ctx->d.ncell_total;
   std::vector<int> soc(NC, -1);
   int s = 0;
   for (size_t b = 0; b < ctx->src_cell.size(); b++)
     for (size_t q = 0; q < ctx->src_cell[b].size(); q++, s++) soc[(size_t)ctx->hbox[b].cell0 + ctx->src_cell[b][q]] = s;
-  CK(cudaMemcpy(a.src_of_cell, soc.data(), sizeof(int) * NC, cudaMemcpyHostToDevice));
-  ctx->adj_ready = true;
+  CK(cudaMemcpy(ctx->adj.src_of_cell, soc.data(), sizeof(int) * NC, cudaMemcpyHostToDevice));
+  ctx->adj_src_stale = false;
   return FRT_OK;
 }
 
@@ -1517,11 +1682,14 @@ frt_status frt_adjoint(frt_ctx* ctx, const frt_adj_objective* obj, double* J, do
       ctx->err = "frt_adjoint: objective sub-box outside the box";
       return FRT_ERR_INVALID;
     }
-  if (ctx->rays_moved) {
-    ctx->err = "frt_adjoint needs the state right after set-up (no advance, merge or split yet)";
+  if (ctx->merged_any || ctx->restarted[obj->box]) {
+    ctx->err = "frt_adjoint needs every ray to come from one source's cast: a merge has combined rays of "
+               "several sources, or the rays were read from a restart file";
     return FRT_ERR_STATE;
   }
   st = adj_alloc(ctx);
+  if (st) return st;
+  st = adj_source_map(ctx);
   if (st) return st;
   Dev& d = ctx->d;
   AdjDev& a = ctx->adj;
@@ -1668,6 +1836,221 @@ frt_status frt_get_sparse_field_noalloc(frt_ctx* ctx, int box, frt_field f, int 
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(host, scratch, sizeof(float) * (size_t)count, cudaMemcpyDeviceToHost, ctx->s_main));
   CK(cudaStreamSynchronize(ctx->s_main));
+  return FRT_OK;
+}
+
+}  // extern "C"
+
+// ---- launch shapes and the autotuner ----------------------------------------------------------
+namespace {
+
+void tuning_out(const frt_ctx* ctx, frt_tuning* o) {
+  const Tune& t = ctx->tune;
+  *o = ctx->tune_measured;
+  o->raypass_block = t.rp_block;
+  o->raypass_blocks_per_sm = t.rp_grid;
+  o->raypass_chunk = t.rp_chunk;
+  o->walk_block = t.adv_block;
+  o->walk_blocks_per_sm = t.adv_grid;
+  o->cellpass_blocks_per_sm = t.lit_grid;
+  o->split_blocks_per_sm = t.split_grid;
+}
+
+bool block_ok(int b) { return b >= 32 && b <= 256 && b % 32 == 0; }
+bool grid_ok(int g) { return g >= 1 && g <= 32; }
+
+// Equal shares [lo, hi) of n work items for k candidates.
+void share(long long n, int k, int q, int* lo, int* hi) {
+  *lo = (int)(n * q / k);
+  *hi = (int)(n * (q + 1) / k);
+}
+
+}  // namespace
+
+extern "C" {
+
+frt_status frt_get_tuning(frt_ctx* ctx, frt_tuning* out) {
+  if (!ctx || !out) return FRT_ERR_INVALID;
+  tuning_out(ctx, out);
+  return FRT_OK;
+}
+
+frt_status frt_set_tuning(frt_ctx* ctx, const frt_tuning* in) {
+  if (!ctx || !in) return FRT_ERR_INVALID;
+  if (!block_ok(in->raypass_block) || !grid_ok(in->raypass_blocks_per_sm) || in->raypass_chunk < 0 ||
+      in->raypass_chunk > 65536 || !block_ok(in->walk_block) || !grid_ok(in->walk_blocks_per_sm) ||
+      !grid_ok(in->cellpass_blocks_per_sm) || !grid_ok(in->split_blocks_per_sm)) {
+    ctx->err = "frt_set_tuning: blocks 32..256 in multiples of 32, 1..32 blocks per SM, chunk 0..65536";
+    return FRT_ERR_INVALID;
+  }
+  Tune t;
+  t.rp_block = in->raypass_block;
+  t.rp_grid = in->raypass_blocks_per_sm;
+  t.rp_chunk = in->raypass_chunk;
+  t.adv_block = in->walk_block;
+  t.adv_grid = in->walk_blocks_per_sm;
+  t.lit_grid = in->cellpass_blocks_per_sm;
+  t.split_grid = in->split_blocks_per_sm;
+  ctx->tune = t;
+  ctx->tune_auto = false;
+  ctx->tune_measured = frt_tuning{};
+  ctx->graph_valid = false;
+  return FRT_OK;
+}
+
+frt_status frt_autotune(frt_ctx* ctx, int steps, frt_tuning* out) {
+  if (!ctx || steps < 1 || steps > 16) return FRT_ERR_INVALID;
+  Dev& d = ctx->d;
+  const int I = d.itercount;
+  cudaStream_t s = ctx->s_main;
+  const Tune t0 = ctx->tune;
+  // candidate values per family; the ray pass and the cell pass get one candidate per C2Ray
+  // iteration but the last (a different kernel), the walk and the compaction split their rays
+  // into four equal ranges
+  const int per_iter = std::max(1, I - 1);
+  const bool tune_rp = !ctx->strict && I > 1;
+  ShapeSearch rp("raypass", Shape{t0.rp_block, t0.rp_grid, t0.rp_chunk}, {128, 256}, {4, 8, 12, 16},
+                 {0, 32, 128, 512}, per_iter);
+  ShapeSearch adv("walk", Shape{t0.adv_block, t0.adv_grid, 0}, {128, 256}, {4, 8, 16}, {0}, 4);
+  ShapeSearch lit("cellpass", Shape{256, t0.lit_grid, 0}, {256}, {2, 4, 8, 16}, {0}, per_iter);
+  ShapeSearch spl("split", Shape{256, t0.split_grid, 0}, {256}, {2, 4, 8, 16}, {0}, 4);
+  for (ShapeSearch* f : {&rp, &adv, &lit, &spl}) f->set_max_rounds(steps);
+  constexpr int kEv = 2 * (4 + 16 + 16 + 4);
+  std::vector<cudaEvent_t> ev(kEv, nullptr);
+  auto destroy = [&]() {
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
+  };
+  for (cudaEvent_t& e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      destroy();
+      ctx->err = "frt_autotune: cudaEventCreate failed";
+      return FRT_ERR_CUDA;
+    }
+  frt_status st = FRT_OK;
+  double c_rp = 0, c_adv = 0, c_lit = 0, c_spl = 0;
+  for (int round = 0; round < steps && st == FRT_OK; round++) {
+    if ((st = step_inputs(ctx, nullptr, nullptr))) break;
+    if (cudaStreamSynchronize(s) != cudaSuccess || cudaStreamSynchronize(ctx->s_dark) != cudaSuccess) {
+      st = FRT_ERR_CUDA;
+      break;
+    }
+    Ctl c0;
+    if (cudaMemcpy(&c0, d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      st = FRT_ERR_CUDA;
+      break;
+    }
+    const long long nray = std::min(c0.nray[c0.cur], d.ray_cap);
+    const std::vector<Shape> ca = adv.next_round(), cs = spl.next_round();
+    const std::vector<Shape> cr = tune_rp ? rp.next_round() : std::vector<Shape>{rp.best()};
+    const std::vector<Shape> cl = lit.next_round();
+    int e = 0;
+    std::vector<int> e_adv, e_spl, e_rp, e_lit;
+    std::vector<long long> n_adv, n_spl;
+    cudaMemcpyAsync(d.itheta_merge, ctx->h_ith_box, sizeof(uint16_t) * d.nbox, cudaMemcpyHostToDevice, s);
+    if (d.nsrc) cudaMemcpyAsync(d.src_itheta, ctx->h_ith_src, sizeof(uint16_t) * d.nsrc, cudaMemcpyHostToDevice, s);
+    note_step(ctx);
+    cudaEventRecord(ctx->ev_t0, s);
+    ctx->rays_moved = true;
+    launch_clear_lit(d, ctx->grid_lit, s);
+    launch_step_begin(d, s);
+    for (int q = 0; q < (int)ca.size(); q++) {
+      int lo, hi;
+      share(nray, (int)ca.size(), q, &lo, &hi);
+      e_adv.push_back(e);
+      n_adv.push_back(hi - lo);
+      cudaEventRecord(ev[e++], s);
+      launch_walk(d, ctx->nsm * ca[q].grid, s, ca[q].block, lo, hi);
+      cudaEventRecord(ev[e++], s);
+    }
+    launch_lit_number(d, ctx->grid_rays, s);
+    launch_lit_init(d, ctx->strict, ctx->grid_lit, s);
+    for (int it = 0; it < I; it++) {
+      const bool last = it == I - 1;
+      const Shape a = (!last && it < (int)cr.size()) ? cr[it] : rp.best();
+      const Shape b = (!last && it < (int)cl.size()) ? cl[it] : lit.best();
+      const bool ta = !last && it < (int)cr.size() && tune_rp, tb = !last && it < (int)cl.size();
+      if (ta) {
+        e_rp.push_back(e);
+        cudaEventRecord(ev[e++], s);
+      }
+      launch_raypass(d, it, ctx->strict, ctx->nsm * a.grid, s, a.block, a.chunk);
+      if (ta) cudaEventRecord(ev[e++], s);
+      if (tb) {
+        e_lit.push_back(e);
+        cudaEventRecord(ev[e++], s);
+      }
+      launch_litpass(d, it, ctx->strict, true, ctx->nsm * b.grid, s);
+      if (tb) cudaEventRecord(ev[e++], s);
+    }
+    launch_count(d, ctx->grid_rays, s);
+    launch_merge(d, ctx->grid_rays, s);
+    for (int q = 0; q < (int)cs.size(); q++) {
+      int lo, hi;
+      share(nray, (int)cs.size(), q, &lo, &hi);
+      e_spl.push_back(e);
+      n_spl.push_back(hi - lo);
+      cudaEventRecord(ev[e++], s);
+      launch_split_range(d, ctx->nsm * cs[q].grid, lo, hi, s);
+      cudaEventRecord(ev[e++], s);
+    }
+    launch_swap(d, s);
+    // the dark-cell pass after the timed kernels, on the same stream: no concurrent kernel
+    // perturbs the candidates' times
+    launch_dark(d, ctx->strict, true, ctx->grid_dark, s);
+    launch_cast(d, s);
+    cudaMemcpyAsync(ctx->h_ctl, d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+    cudaEventRecord(ctx->ev_t1, s);
+    if ((st = finish_step(ctx, nullptr))) break;
+    const Ctl& c1 = *ctx->h_ctl;
+    auto ms = [&](int k) {
+      float x = 0.f;
+      return cudaEventElapsedTime(&x, ev[k], ev[k + 1]) == cudaSuccess ? (double)x : -1.0;
+    };
+    for (size_t q = 0; q < e_adv.size(); q++)
+      if (n_adv[q] > 0 && ms(e_adv[q]) > 0) adv.record((int)q, 1e6 * ms(e_adv[q]) / (double)n_adv[q]);
+    for (size_t q = 0; q < e_spl.size(); q++)
+      if (n_spl[q] > 0 && ms(e_spl[q]) > 0) spl.record((int)q, 1e6 * ms(e_spl[q]) / (double)n_spl[q]);
+    for (size_t q = 0; q < e_rp.size(); q++)
+      if (c1.crossings > 0 && ms(e_rp[q]) > 0) rp.record((int)q, 1e6 * ms(e_rp[q]) / (double)c1.crossings);
+    for (size_t q = 0; q < e_lit.size(); q++)
+      if (c1.n_lit > 0 && ms(e_lit[q]) > 0) lit.record((int)q, 1e6 * ms(e_lit[q]) / (double)c1.n_lit);
+    adv.end_round();
+    spl.end_round();
+    if (tune_rp) rp.end_round();
+    lit.end_round();
+    c_rp = rp.best_cost();
+    c_adv = adv.best_cost();
+    c_lit = lit.best_cost();
+    c_spl = spl.best_cost();
+  }
+  destroy();
+  if (st) return st;
+  Tune t = t0;
+  if (tune_rp) {
+    t.rp_block = rp.best().block;
+    t.rp_grid = rp.best().grid;
+    t.rp_chunk = rp.best().chunk;
+  }
+  t.adv_block = adv.best().block;
+  t.adv_grid = adv.best().grid;
+  t.lit_grid = lit.best().grid;
+  t.split_grid = spl.best().grid;
+  ctx->tune = t;
+  ctx->tune_auto = true;
+  ctx->graph_valid = false;
+  frt_tuning m{};
+  m.steps = steps;
+  m.raypass_ns_per_crossing = tune_rp && c_rp < 1e299 ? c_rp : 0.0;
+  m.walk_ns_per_ray = c_adv < 1e299 ? c_adv : 0.0;
+  m.cellpass_ns_per_cell = c_lit < 1e299 ? c_lit : 0.0;
+  m.split_ns_per_ray = c_spl < 1e299 ? c_spl : 0.0;
+  ctx->tune_measured = m;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[tune_key(ctx, ctx->last.rays_alive)] = t;
+  }
+  if (out) tuning_out(ctx, out);
   return FRT_OK;
 }
 

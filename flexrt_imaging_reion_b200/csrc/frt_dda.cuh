@@ -10,10 +10,10 @@
 
 namespace frt {
 
-__device__ __forceinline__ int dda_imod(int a, int b) {
-  while (a < 0) a += b;
-  return a % b;
-}
+// The periodic neighbours of a cell index i in [0, N): the reference's mod(i +- 1, N) without an
+// integer division.
+__device__ __forceinline__ int dda_up(int i, int N) { return (i + 1 == N) ? 0 : i + 1; }
+__device__ __forceinline__ int dda_down(int i, int N) { return (i == 0) ? N - 1 : i - 1; }
 
 // Does the ray, moved by dist, leave its cell this step (ray_tracing.cc:1243-1250)?
 __device__ __forceinline__ bool ray_moves(const BoxP& B, float x0, float y0, float z0, float xhat, float yhat,
@@ -61,14 +61,14 @@ __device__ __forceinline__ int dda_walk(const BoxP& B, int PL, float xhat, float
       y0 += dist * yhat;
       z0 += dist * zhat;
       if (tag == 0) {
-        if (xhat > 0.f) { in = dda_imod(in + 1, N); x0 = B.lo_edge; }
-        else { in = dda_imod(in - 1, N); x0 = B.hi_edge; }
+        if (xhat > 0.f) { in = dda_up(in, N); x0 = B.lo_edge; }
+        else { in = dda_down(in, N); x0 = B.hi_edge; }
       } else if (tag == 1) {
-        if (yhat > 0.f) { jn = dda_imod(jn + 1, N); y0 = B.lo_edge; }
-        else { jn = dda_imod(jn - 1, N); y0 = B.hi_edge; }
+        if (yhat > 0.f) { jn = dda_up(jn, N); y0 = B.lo_edge; }
+        else { jn = dda_down(jn, N); y0 = B.hi_edge; }
       } else {
-        if (zhat > 0.f) { kn = dda_imod(kn + 1, N); z0 = B.lo_edge; }
-        else { kn = dda_imod(kn - 1, N); z0 = B.hi_edge; }
+        if (zhat > 0.f) { kn = dda_up(kn, N); z0 = B.lo_edge; }
+        else { kn = dda_down(kn, N); z0 = B.hi_edge; }
       }
       if (x0 <= 0.f) x0 = B.lo_edge;
       if (x0 >= B.hi_thr_f) x0 = B.hi_edge;

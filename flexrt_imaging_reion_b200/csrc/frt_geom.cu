@@ -238,39 +238,102 @@ __global__ void __launch_bounds__(256) k_lit_chunk_write(Dev d, const int* chunk
 
 // advance_ray (ray_tracing.cc:1222-1512) with c2ray_iter = TRUE and fion = 1 (plain mode):
 // cell-boundary walk over c_sim * time, path segments {cell, dist}, periodic wrap, corner nudge.
-// Rays [r_begin, min(r_end, pool size)) of the pool (the autotuner times launch shapes on shares
-// of one step's rays; the step itself launches the whole pool).
-__global__ void __launch_bounds__(256, 4) k_advance(Dev d, int r_begin, int r_end) {
+//
+// Work layout. A tile of T consecutive pool rays is loaded by T threads (coalesced) into shared
+// memory and counting-sorted by a key of the ray's direction octant and its estimated number of
+// segments; thread t then walks the tile's t-th ray in key order. The walk's arithmetic depends on
+// the signs of the direction (a float quotient for a positive component, a double one for a
+// negative, ray_tracing.cc:1273-1296) and its trip count on the number of segments, so after the
+// sort the lanes of a warp take the same branches and end together instead of every warp running
+// both branches of every axis behind its longest ray. The results go back through shared memory
+// and are stored by the thread that loaded the ray (coalesced). Which thread walks which ray does
+// not change any ray's arithmetic. Rays [r_begin, min(r_end, pool size)) of the pool (the
+// autotuner times launch shapes on shares of one step's rays; the step launches the whole pool).
+template <int T>
+__global__ void __launch_bounds__(T) k_advance(Dev d, int r_begin, int r_end) {
+  constexpr int kKeys = 32;   // 8 octants x 4 segment classes
+  __shared__ float s_f[9][T];  // xh yh zh x y z time r dr (results: x y z time r dr)
+  __shared__ int s_cell[T];
+  __shared__ uint16_t s_box[T];
+  __shared__ uint8_t s_nseg[T], s_dead[T];
+  __shared__ uint16_t s_perm[T];
+  __shared__ int s_cnt[kKeys], s_base[kKeys + 1];
   const int cur = d.ctl->cur;
   const int n = min(d.ctl->nray[cur], r_end);
   const RayPool A = d.pool[cur];
   const int cap = d.ray_cap, PL = d.PL;
+  const int t = threadIdx.x;
   long long cross = 0, moved = 0, killed = 0;
   double killed_ph = 0.0;
-  for (int i0 = r_begin + blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
-    const int i = i0 + threadIdx.x;
-    if (i < n) do {
+  for (int i0 = r_begin + blockIdx.x * T; i0 < n; i0 += gridDim.x * T) {
+    const int i = i0 + t;
+    if (t < kKeys) s_cnt[t] = 0;
+    __syncthreads();
+    int key = -1, rank = 0;
+    if (i < n) {
       d.dead[i] = 0;
-      const BoxP& B = d.box[A.box[i]];
-      const int N = B.n;
-      const int ind = A.cell[i];
-      const int ii = ind / B.nn;
-      const int jj = (ind - ii * B.nn) / N;
-      const int kk = ind - ii * B.nn - jj * N;
+      const uint16_t bx = A.box[i];
+      const BoxP& B = d.box[bx];
       const float xhat = A.xh[i], yhat = A.yh[i], zhat = A.zh[i];
-      float x0 = A.x[i], y0 = A.y[i], z0 = A.z[i];
+      const float x0 = A.x[i], y0 = A.y[i], z0 = A.z[i];
       const float deltat = A.time[i] + B.dt;
       const float dist = B.clight * deltat;
       if (!ray_moves(B, x0, y0, z0, xhat, yhat, zhat, dist)) {
         A.time[i] = deltat;
         d.nseg[i] = 0;
-        break;
+      } else {
+        s_f[0][t] = xhat;
+        s_f[1][t] = yhat;
+        s_f[2][t] = zhat;
+        s_f[3][t] = x0;
+        s_f[4][t] = y0;
+        s_f[5][t] = z0;
+        s_f[6][t] = deltat;
+        s_f[7][t] = A.r[i];
+        s_f[8][t] = A.dr[i];
+        s_cell[t] = A.cell[i];
+        s_box[t] = bx;
+        // sort key: octant of the direction, and the cell faces the straight path crosses
+        // (an estimate of the segment count: only the walk order depends on it)
+        const float inv = __fdividef(1.0f, B.dx);
+        const int faces = abs((int)floorf((x0 + dist * xhat) * inv)) + abs((int)floorf((y0 + dist * yhat) * inv)) +
+                          abs((int)floorf((z0 + dist * zhat) * inv));
+        const int oct = (xhat < 0.f ? 1 : 0) | (yhat < 0.f ? 2 : 0) | (zhat < 0.f ? 4 : 0);
+        key = oct * 4 + min(faces, 3);
+        rank = atomicAdd(&s_cnt[key], 1);
       }
-      float r0 = A.r[i], dr = A.dr[i];
+    }
+    __syncthreads();
+    if (t == 0) {
+      int acc = 0;
+      for (int k = 0; k < kKeys; k++) {
+        s_base[k] = acc;
+        acc += s_cnt[k];
+      }
+      s_base[kKeys] = acc;
+    }
+    __syncthreads();
+    if (key >= 0) s_perm[s_base[key] + rank] = (uint16_t)t;
+    __syncthreads();
+    const int nwalk = s_base[kKeys];
+    if (t < nwalk) do {
+      const int j = s_perm[t];    // the tile ray this thread walks
+      const int iw = i0 + j;
+      const BoxP& B = d.box[s_box[j]];
+      const int N = B.n;
+      const int ind = s_cell[j];
+      const int ii = ind / B.nn;
+      const int jj = (ind - ii * B.nn) / N;
+      const int kk = ind - ii * B.nn - jj * N;
+      const float xhat = s_f[0][j], yhat = s_f[1][j], zhat = s_f[2][j];
+      float x0 = s_f[3][j], y0 = s_f[4][j], z0 = s_f[5][j];
+      const float deltat = s_f[6][j];
+      const float dist = B.clight * deltat;
+      float r0 = s_f[7][j], dr = s_f[8][j];
       r0 += dist / B.scale;
       dr -= dist / B.scale;
       int in = ii, jn = jj, kn = kk;
-      int2* sp = d.segs + (size_t)i * PL;
+      int2* sp = d.segs + (size_t)iw * PL;
       const int ns = dda_walk(B, PL, xhat, yhat, zhat, deltat, x0, y0, z0, in, jn, kn,
                               [&](int p, long long gc, float ds) {
                                 sp[p] = make_int2((int)gc, __float_as_int(ds));
@@ -278,28 +341,47 @@ __global__ void __launch_bounds__(256, 4) k_advance(Dev d, int r_begin, int r_en
                               });
       if (ns < 0) {
         atomicOr(&d.ctl->err, ERR_PATH);
-        d.nseg[i] = 0;
-        d.dead[i] = 1;
+        s_nseg[j] = 0;   // the record is left as it was and the ray flagged
+        s_dead[j] = 1;
         break;
       }
-      d.nseg[i] = (uint8_t)ns;
-      A.time[i] = 0.f;
-      A.r[i] = r0;
-      A.dr[i] = dr;
-      A.x[i] = x0;
-      A.y[i] = y0;
-      A.z[i] = z0;
-      A.cell[i] = in * B.nn + jn * N + kn;
+      s_nseg[j] = (uint8_t)ns;
+      s_dead[j] = 0;
+      s_f[3][j] = x0;
+      s_f[4][j] = y0;
+      s_f[5][j] = z0;
+      s_f[6][j] = 0.f;
+      s_f[7][j] = r0;
+      s_f[8][j] = dr;
+      s_cell[j] = in * B.nn + jn * N + kn;
       cross += ns;
       moved += 1;
       // optional removal beyond rkill (comoving), applied after update_rays
       if (B.rkill > 0.0 && (double)r0 > B.rkill) {
-        d.dead[i] = 1;
+        s_dead[j] = 1;
         killed += 1;
-        killed_ph += (double)sum_nphot(A, i, d.F, cap) * kPhotNorm;
-        break;
+        killed_ph += (double)sum_nphot(A, iw, d.F, cap) * kPhotNorm;
       }
     } while (0);
+    __syncthreads();
+    if (key >= 0) {   // this thread loaded a walked ray: store its results
+      if (s_nseg[t] == 0 && s_dead[t]) {
+        // path overflow: keep the record, flag the ray
+        d.nseg[i] = 0;
+        d.dead[i] = 1;
+      } else {
+        d.nseg[i] = s_nseg[t];
+        d.dead[i] = s_dead[t];
+        A.time[i] = 0.f;
+        A.r[i] = s_f[7][t];
+        A.dr[i] = s_f[8][t];
+        A.x[i] = s_f[3][t];
+        A.y[i] = s_f[4][t];
+        A.z[i] = s_f[5][t];
+        A.cell[i] = s_cell[t];
+      }
+    }
+    __syncthreads();   // the shared tile takes the next T rays
   }
   cross = block_sum(cross);
   moved = block_sum(moved);
@@ -910,8 +992,14 @@ __global__ void k_cosmo_cells(Dev d, int box, double rho_factor) {
        c += (long long)gridDim.x * blockDim.x) {
     const long long q = B.cell0 + c;
     const float nH0 = d.nH[q], nHe0 = d.nHe[q];
+    // the ionised fractions of the last cell pass (f_H2 = nH2 / nH with nH2 = nH - nH1,
+    // ray_tracing.cc:1119, 1192); kept for a snapshot switch that follows this expansion
     const float f_H2 = (nH0 - d.nH1[q]) / nH0;
     const float f_He2 = (nHe0 - d.nHe1[q]) / nHe0;
+    if (d.frac_h2) {
+      d.frac_h2[q] = f_H2;
+      d.frac_he2[q] = f_He2;
+    }
     float rho = d.rho[q];
     rho *= rho_factor;
     d.rho[q] = rho;
@@ -931,6 +1019,48 @@ __global__ void k_cosmo_cells(Dev d, int box, double rho_factor) {
     d.ne[q] = ne;
     d.n_tot[q] = nH + nHe + ne;
     d.nH1_prev[q] = nH1;
+  }
+}
+
+// update_hydro_step's cell update for a later snapshot (gas_funcs.cc:686-745, fion = 1 in plain
+// mode): n_H, n_He from the new proper density (already in d.rho), the ionised densities keep the
+// fractions f_HII, f_HeII (of the last cell pass, or the ones an expansion just before this
+// switch kept), n_HI = n_H - n_HII, <n_HI> = n_HI, n_e, n_tot; with a previous snapshot
+// (avg_rho_prev > 0) d(delta)/dt = (rho/<rho> - rho_prev/<rho_prev>) / dt_snap; rho_prev = rho.
+__global__ void k_hydro_cells(Dev d, int box, bool cached, float avg_rho_prev, float dt_snap) {
+  const BoxP& B = d.box[box];
+  const float avg_rho = B.avg_rho;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < B.ncell;
+       c += (long long)gridDim.x * blockDim.x) {
+    const long long q = B.cell0 + c;
+    float f_H2, f_He2;
+    if (cached) {
+      f_H2 = d.frac_h2[q];
+      f_He2 = d.frac_he2[q];
+    } else {
+      const float nH0 = d.nH[q], nHe0 = d.nHe[q];
+      f_H2 = (nH0 - d.nH1[q]) / nH0;
+      f_He2 = (nHe0 - d.nHe1[q]) / nHe0;
+    }
+    const float rho = d.rho[q];
+    const float nH = (1. - kY) * rho / kMH;
+    const float nHe = kY * rho / (4. * kMH);
+    const float nH2 = f_H2 * nH / 1.0f;
+    const float nHe2 = f_He2 * nHe / 1.0f;
+    const float nH1 = nH - nH2;
+    const float nHe1 = nHe - nHe2;
+    const float ne = nH2 + nHe2;
+    d.nH[q] = nH;
+    d.nHe[q] = nHe;
+    d.nH1[q] = nH1;
+    d.nHe1[q] = nHe1;
+    d.avg_nh1[q] = nH1;
+    d.avg_nhe1[q] = nHe1;
+    d.ne[q] = ne;
+    d.n_tot[q] = nH + nHe + ne;
+    d.nH1_prev[q] = nH1;
+    if (avg_rho_prev > 0.f) d.ddelta[q] = (rho / avg_rho - d.rho_prev[q] / avg_rho_prev) / dt_snap;
+    d.rho_prev[q] = rho;
   }
 }
 
@@ -967,14 +1097,19 @@ __global__ void k_fill_i32(int* p, int v, long long n) {
 // ---- launchers ------------------------------------------------------------------------------
 void launch_step_begin(const Dev& d, cudaStream_t s) { k_step_begin<<<grid_for(d.nsrc + 1, 256, 1184), 256, 0, s>>>(d); }
 
+static void launch_k_advance(const Dev& d, int grid, int block, int r_begin, int r_end, cudaStream_t s) {
+  if (block <= 128) k_advance<128><<<grid, 128, 0, s>>>(d, r_begin, r_end);
+  else k_advance<256><<<grid, 256, 0, s>>>(d, r_begin, r_end);
+}
+
 void launch_advance(const Dev& d, int grid, cudaStream_t s, int block, int pack_grid) {
-  k_advance<<<grid, block, 0, s>>>(d, 0, INT_MAX);
+  launch_k_advance(d, grid, block, 0, INT_MAX, s);
   k_lit_compact<<<grid_for(d.ncell_total >> 4, 256, 148 * 8), 256, 0, s>>>(d);
   k_moved_pack<<<pack_grid > 0 ? pack_grid : grid, 256, 0, s>>>(d);
 }
 
 void launch_walk(const Dev& d, int grid, cudaStream_t s, int block, int r_begin, int r_end) {
-  k_advance<<<grid, block, 0, s>>>(d, r_begin, r_end);
+  launch_k_advance(d, grid, block, r_begin, r_end, s);
 }
 
 void launch_lit_number(const Dev& d, int grid, cudaStream_t s) {
@@ -1028,6 +1163,11 @@ void launch_cast_per_source(const Dev& d, cudaStream_t s) {
 void launch_cosmo_expansion(const Dev& d, int box, float ratio, double rho_factor, int grid, cudaStream_t s) {
   k_cosmo_cells<<<grid, 256, 0, s>>>(d, box, rho_factor);
   k_cosmo_rays<<<grid, 256, 0, s>>>(d, box, ratio);
+}
+
+void launch_hydro_switch(const Dev& d, int box, bool cached_fractions, float avg_rho_prev, float dt_snap, int grid,
+                         cudaStream_t s) {
+  k_hydro_cells<<<grid, 256, 0, s>>>(d, box, cached_fractions, avg_rho_prev, dt_snap);
 }
 
 void launch_pix_table(float4* tab, cudaStream_t s) { k_pix_table<<<148 * 8, 256, 0, s>>>(tab); }

@@ -148,13 +148,7 @@ void box_params(BoxP* B, const frt_config* cfg, const frt_box_desc* bd, long lon
   ThermConst& th = B->th;
   th.dt = B->dt;
   th.dx = dx;
-  const float zz = bd->zz;
-  const float Hf = hubble(1. / (1. + zz));                           // gas_funcs.cc:356, 405
-  th.hub2f = 2.0f * Hf;
-  th.hub_d = Hf;
-  th.zz = zz;
-  th.compton_d = 5.6072e-36 * pow(1 + (double)zz, 4.);               // rates.cc:234-238
-  th.compton_f = (float)th.compton_d;
+  set_redshift(B, bd->zz);
   th.nfreq = (float)cfg->nfreq;
   for (int nu = 0; nu < 8; nu++) {
     const double f = nu < cfg->nfreq ? cfg->nu_phot[nu] : 0.0;
@@ -162,6 +156,43 @@ void box_params(BoxP* B, const frt_config* cfg, const frt_box_desc* bd, long lon
     th.cH1[nu] = (float)(kHPlanck * (kHeV * f - 13.6) / kHeV);      // gas_funcs.cc:155-156
     th.cHe1[nu] = (float)(kHPlanck * (kHeV * f - 2.459e+1) / kHeV);
   }
+}
+
+float snapshot_dx(const frt_box_desc* bd, float a) {
+  const float Lx0 = bd->box_hmpc * 1e3 / kHh;                        // user_inputs.h:92
+  const float Lx = Lx0 * a;                                          // gas_funcs.cc:590
+  return Lx / bd->n * kKpcToCm;                                      // gas_funcs.cc:689
+}
+
+void set_redshift(BoxP* B, float zz) {
+  ThermConst& th = B->th;
+  const float Hf = hubble(1. / (1. + zz));                           // gas_funcs.cc:356, 405
+  th.hub2f = 2.0f * Hf;
+  th.hub_d = Hf;
+  th.zz = zz;
+  th.compton_d = 5.6072e-36 * pow(1 + (double)zz, 4.);               // rates.cc:234-238
+  th.compton_f = (float)th.compton_d;
+}
+
+float vol_avg(const float* f, int n) {
+  double tot = 0.;
+  const long long n3 = (long long)n * n * n;
+  for (long long q = 0; q < n3; q++) tot += (double)f[q];
+  return (float)tot / pow((double)n, 3.);
+}
+
+void snapshot_rho(int n, const float* delta1, float a, float* rho, float* avg_rho) {
+  const long long n3 = (long long)n * n * n;
+  const float rho_c_cgs = 1.87890e-29, ob = 0.0482266, h0 = 0.68;
+  const double rho_unit = rho_c_cgs * ob * pow(h0, 2.);
+  for (long long q = 0; q < n3; q++) {
+    rho[q] = delta1[q];
+    rho[q] *= (float)rho_unit;
+  }
+  float avg = vol_avg(rho, n);
+  for (long long q = 0; q < n3; q++) rho[q] *= pow(a, -3.);
+  avg *= pow(a, -3.);
+  *avg_rho = avg;
 }
 
 void init_gas(const frt_config* cfg, const frt_box_desc* bd, const float* delta1, GasInit* g) {

@@ -25,6 +25,15 @@ struct GasRestart {
 void init_gas_restart(const frt_config* cfg, const frt_box_desc* bd, const GasRestart& r, GasInit* g, float* heat,
                       float* cool);
 void nphot_min_max(const frt_config* cfg, const BoxP* B, int nsrc, const double* lum, double* nmin, double* nmax);
+// calc_vol_avg (data_funcs.cc:75-92): double sum in cell order, float result
+float vol_avg(const float* f, int n);
+// A snapshot's proper density as get_ugas reads it (io_funcs.cc:33-62) scaled by a^-3, and its
+// volume average (taken before the scaling and scaled the same way, gas_funcs.cc:606-613, 669-684)
+void snapshot_rho(int n, const float* delta1, float a, float* rho, float* avg_rho);
+// The proper cell size Lx0 a / N kpc_to_cm of a box at scale factor a (init_funcs.cc:23, gas_funcs.cc:689)
+float snapshot_dx(const frt_box_desc* bd, float a);
+// The redshift-dependent constants of the thermal update (Hubble rate, Compton rate)
+void set_redshift(BoxP* B, float zz);
 void derived_constants(const frt_config* cfg, double* sigH1, double* sigHe1, double* sig0, double* sig912,
                        double* pi_sf_3, double* log4);
 

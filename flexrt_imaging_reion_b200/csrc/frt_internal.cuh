@@ -79,6 +79,10 @@ struct Dev {
   int* lit_slot;
   float *nH1_prev, *n_tot, *dne_dt;                              // unfused path
   float* rho;              // proper density, on the device once a cosmological expansion ran
+  // hydro snapshots (update_hydro_step): the previous snapshot's density and d(delta)/dt of the
+  // temperature equation (both from the second switch on), and the ionised fractions an
+  // expansion kept (read by a switch right after it)
+  float *rho_prev, *ddelta, *frac_h2, *frac_he2;
   float *rec_h2, *rec_he2, *recrate_h2, *recrate_he2, *mfp, *mfp912, *if_speed, *inc_flux;  // diag
   // lit cells
   int* l_cell;
@@ -126,6 +130,10 @@ struct Tune {
   int adv_block = 256, adv_grid = 8;
   int lit_grid = 8;
   int split_grid = 8;
+  bool operator==(const Tune& o) const {
+    return rp_block == o.rp_block && rp_grid == o.rp_grid && rp_chunk == o.rp_chunk && adv_block == o.adv_block &&
+           adv_grid == o.adv_grid && lit_grid == o.lit_grid && split_grid == o.split_grid;
+  }
 };
 
 // Buffers of the adjoint of one step's Gamma field (frt_adjoint.cu). Cells on the paths of the
@@ -176,6 +184,9 @@ constexpr int kPixTabMax = 9;
 inline long long pix_tab_offset(int order) { return 4ll * ((1ll << (2 * order)) - 1); }   // sum of 12*4^k, k < order
 void launch_pix_table(float4* tab, cudaStream_t s);
 void launch_cosmo_expansion(const Dev& d, int box, float ratio, double rho_factor, int grid, cudaStream_t s);
+// the cells of update_hydro_step for box `box` (d.rho holds the new snapshot's proper density)
+void launch_hydro_switch(const Dev& d, int box, bool cached_fractions, float avg_rho_prev, float dt_snap, int grid,
+                         cudaStream_t s);
 // ---- launchers (frt_phys.cu) ----------------------------------------------------------
 void launch_lit_init(const Dev& d, bool strict, int grid, cudaStream_t s);
 void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t s, int block = 256, int chunk = 0);

@@ -52,6 +52,7 @@ struct BoxP {
   int lsource;               // casting order for cells below 10% neutral
   ThermConst th;
   float rmax[kLtab], rmin[kLtab];
+  float avg_rho;             // volume-averaged proper density (calc_vol_avg, data_funcs.cc:75-92)
 };
 
 }  // namespace frt

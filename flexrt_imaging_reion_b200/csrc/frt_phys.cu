@@ -36,6 +36,15 @@ __device__ __forceinline__ T block_sum(T v) {
 
 __device__ __forceinline__ int box_of_cell(const Dev& d, long long gc) { return d.tile_box[gc >> kTileShift]; }
 
+// The density-change term of the temperature equation: d(delta)/dt and rho / <rho> of a cell
+// (gas_funcs.cc:399), present once a second hydro snapshot has been read.
+__device__ __forceinline__ void density_change(const Dev& d, const BoxP& B, long long gc, ThermCell* c) {
+  if (d.ddelta) {
+    c->ddelta = d.ddelta[gc];
+    c->rho_rel = d.rho[gc] / B.avg_rho;
+  }
+}
+
 // 1 - e^-x and e^-x of one optical depth x >= 0 (xl = x log2(e)). Below x = 1/4 the absorbed
 // part is the Taylor series of 1 - e^-x = x - x^2/2! + x^3/3! - ... to the x^6 term (alternating
 // with decreasing terms: truncation below 0.25^6/7! ~ 5e-8 relative) and the transmission is
@@ -563,6 +572,7 @@ __global__ void __launch_bounds__(256) k_litpass(Dev d, int s_begin, int s_end) 
         hs.hh = ht.x;
         hs.hhe = ht.y;
       }
+      density_change(d, B, gc, &c);
       thermal_update<STRICT>(c, B.th, hs, d.F, d.nhe_to_nh);
       d.temp[gc] = c.temp;
       d.heat[gc] = c.heat;
@@ -664,6 +674,7 @@ __global__ void __launch_bounds__(256, 4) k_dark(Dev d) {
       c.avg_nh1 = a;
       c.avg_nhe1 = bb;
       const HeatSrc hs{nullptr, nullptr, 0, 0.f, 0.f, 0};
+      density_change(d, B, gc, &c);
       thermal_update<STRICT>(c, B.th, hs, d.F, d.nhe_to_nh);
       d.temp[gc] = c.temp;
       d.heat[gc] = c.heat;
@@ -713,7 +724,8 @@ __global__ void __launch_bounds__(256) k_thermal_all(Dev d) {
       if (!STRICT && !d.per_bin) hs = HeatSrc{nullptr, nullptr, 0, d.l_heat[slot].x, d.l_heat[slot].y, 2};
       else hs = HeatSrc{d.l_acc_nu_h + slot, d.l_acc_nu_he + slot, L, 0.f, 0.f, 1};
     }
-    thermal_update<STRICT>(c, B.th, hs, d.F, d.nhe_to_nh);
+    density_change(d, B, gc, &c);
+      thermal_update<STRICT>(c, B.th, hs, d.F, d.nhe_to_nh);
     d.temp[gc] = c.temp;
     d.heat[gc] = c.heat;
     d.cool[gc] = c.cool;

@@ -175,6 +175,9 @@ struct ThermCell {
   float temp, heat, cool;
   float nH, nH1, nH1_prev, nH2, nHe2, ne, n_tot, dne_dt, f_H2, avg_nh1, avg_nhe1;
   float if_speed, inc_flux;
+  // d(delta)/dt and rho / <rho> of the temperature equation (gas_funcs.cc:399); 0 and 1 until a
+  // second hydro snapshot gives the density a rate of change
+  float ddelta = 0.f, rho_rel = 1.f;
 };
 
 // Photo-ionisation input of the heating term. The reference sums over bins
@@ -314,12 +317,14 @@ __device__ inline void thermal_update(ThermCell& c, const ThermConst& k, const H
     heat_cool<STRICT>(c, k, hs, nfreq);
     if (STRICT) {
       c.temp = (c.temp + 2. / 3. / kKB / c.n_tot * (c.heat - c.cool) * dt_temp) /
-               (1. + 2. * (double)(k.hub2f * 0.5f) * dt_temp + 1. / c.n_tot * c.dne_dt * dt_temp);
+               (1. + 2. * (double)(k.hub2f * 0.5f) * dt_temp + 1. / c.n_tot * c.dne_dt * dt_temp -
+                2. * (double)c.ddelta / 3. / (double)c.rho_rel * dt_temp);
     } else {
       const float c23 = (float)(2. / 3. / kKB);
       const float inv_n = __fdividef(1.0f, c.n_tot);
       c.temp = __fdividef(c.temp + (c23 * inv_n) * (c.heat - c.cool) * dt_temp,
-                          1.0f + k.hub2f * dt_temp + (c.dne_dt * inv_n) * dt_temp);
+                          1.0f + k.hub2f * dt_temp + (c.dne_dt * inv_n) * dt_temp -
+                              __fdividef((2.0f / 3.0f) * c.ddelta, c.rho_rel) * dt_temp);
     }
     t_temp += dt_temp;
     ++guard;

@@ -2,6 +2,7 @@
 #include "frt_tune.h"
 
 #include <algorithm>
+#include <cstdlib>
 
 namespace frt {
 
@@ -30,6 +31,7 @@ std::vector<Shape> ShapeSearch::next_round() {
   cur_.clear();
   cur_.push_back(best_);   // the best so far is re-timed: the round compares like with like
   const std::vector<int>* lists[3] = {&chunks_, &grids_, &blocks_};
+  for (int& a : probe_axis_) a = -1;
   if (round_ == 0) {
     // spread: one change per axis, to the value farthest from the start
     for (int a = 0; a < 3; a++) {
@@ -42,19 +44,25 @@ std::vector<Shape> ShapeSearch::next_round() {
       for (int x : L)
         if (std::abs(x - v0) > std::abs(far - v0)) far = x;
       v = far;
+      const size_t before = cur_.size();
       add_unique(&cur_, s);
+      if (cur_.size() > before && cur_.size() <= 8) probe_axis_[cur_.size() - 1] = a;
     }
   }
-  // coordinate descent around the best: the untried values of one axis, then the others
+  // coordinate descent around the best: the untried values of one axis (nearest the best's value
+  // first), then the next axes
   for (int k = 0; k < 3 && (int)cur_.size() < per_round_; k++) {
-    const int a = (axis_ + k) % 3;
-    for (int x : *lists[a]) {
+    const int a = axis_order_[(axis_ + k) % 3];
+    std::vector<int> vals = *lists[a];
+    const int v0 = axis_value(best_, a);
+    std::stable_sort(vals.begin(), vals.end(), [v0](int x, int y) { return std::abs(x - v0) < std::abs(y - v0); });
+    for (int x : vals) {
       Shape s = best_;
       axis_value(s, a) = x;
       if (!find(s)) add_unique(&cur_, s);
     }
   }
-  axis_ = (axis_ + 1) % 3;
+  if (round_ > 0) axis_ = (axis_ + 1) % 3;
   cur_cost_.assign(cur_.size(), 1e300);
   return cur_;
 }
@@ -77,6 +85,13 @@ void ShapeSearch::end_round() {
       x->n += 1;
       if (w < 0 || cur_cost_[k] < cur_cost_[w]) w = k;
     }
+  }
+  if (round_ == 0 && cur_cost_[0] < 1e299) {
+    // the descent visits first the axes whose probe gained most against the start
+    double gain[3] = {-1e300, -1e300, -1e300};
+    for (int k = 1; k < (int)cur_.size() && k < 8; k++)
+      if (probe_axis_[k] >= 0 && cur_cost_[k] < 1e299) gain[probe_axis_[k]] = cur_cost_[0] - cur_cost_[k];
+    std::stable_sort(axis_order_, axis_order_ + 3, [&gain](int x, int y) { return gain[x] > gain[y]; });
   }
   if (w >= 0) {
     best_ = cur_[w];

@@ -14,7 +14,8 @@
 // its cost is the time per unit of work (crossing, ray, lit cell). The first round spreads over
 // the parameter space, the next rounds vary one parameter at a time around the best so far
 // (coordinate descent); the current best is always re-timed in a round, so a choice never rests
-// on one early sample alone.
+// on one early sample alone. The axes are visited in the order of the gain their round-0 probe
+// showed, and along an axis the untried values nearest the current best come first.
 #pragma once
 #include <string>
 #include <vector>
@@ -61,6 +62,8 @@ class ShapeSearch {
   double best_cost_ = 1e300;
   std::vector<int> blocks_, grids_, chunks_;
   int per_round_ = 4, round_ = 0, max_rounds_ = 2, axis_ = 0;
+  int axis_order_[3] = {0, 1, 2};   // descent order of the axes (chunk, grid, block)
+  int probe_axis_[8] = {-1, -1, -1, -1, -1, -1, -1, -1};   // round 0: the axis each candidate probes
   std::vector<Shape> cur_;
   std::vector<double> cur_cost_;
   std::vector<Seen> seen_;

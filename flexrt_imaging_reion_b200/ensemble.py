@@ -56,15 +56,18 @@ def _ctx(inputs, seeds, device):
 
 
 def run_batched(inputs: Sequence[W.BoxInputs], seeds: Sequence[int], warmup: int, steps: int,
-                device: int = 0, box_ids: Sequence[int] = ()) -> Dict[str, object]:
+                device: int = 0, box_ids: Sequence[int] = (), autotune_steps: int = 0) -> Dict[str, object]:
     """All boxes in one context, one graph launch per step. Device time from CUDA events around
     each graph launch; wall time around the frt_step calls (H2D of the step's random angles,
     launch, D2H of the step totals); raypass_ms sums the CUDA-event time of the ray passes. per_box
-    maps each box id to [t, dt, live rays]."""
+    maps each box id to [t, dt, live rays]. With autotune_steps > 0 the last that many warm-up
+    steps are frt_autotune's (the chosen launch shapes are returned as "tuning")."""
     ctx = _ctx(inputs, seeds, device)
     ctx.setup()
-    for _ in range(warmup):
+    n_tune = min(autotune_steps, warmup)
+    for _ in range(warmup - n_tune):
         ctx.step(graph=True)
+    tuning = ctx.autotune(n_tune) if n_tune else None
     cross, dev_ms, dark_ms, rp_ms, lit = 0, 0.0, 0.0, 0.0, 0
     t0 = time.perf_counter()
     for _ in range(steps):
@@ -85,7 +88,7 @@ def run_batched(inputs: Sequence[W.BoxInputs], seeds: Sequence[int], warmup: int
     itercount = ctx.itercount
     ctx.close()
     return {"crossings": cross, "device_ms": dev_ms, "dark_ms": dark_ms, "raypass_ms": rp_ms, "lit_cells": lit,
-            "wall_s": wall, "rays": rays, "per_box": per_box, "itercount": itercount}
+            "wall_s": wall, "rays": rays, "per_box": per_box, "itercount": itercount, "tuning": tuning}
 
 
 def run_per_box_loop(inputs: Sequence[W.BoxInputs], seeds: Sequence[int], warmup: int, steps: int,

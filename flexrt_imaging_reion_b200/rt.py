@@ -228,6 +228,20 @@ class RTContext:
         self._check(self.L.frt_update_cosmo_expansion(self.h, ac.ctypes.data, ap.ctypes.data),
                     "frt_update_cosmo_expansion")
 
+    def hydro_step(self, box: int, snap: W.BoxInputs, a_rt: float, dt_snap: float, zz: float) -> None:
+        """update_hydro_step of one box to the snapshot `snap` (its density cube and sources), with
+        get_nphot_min_max; call after new_rays and the expansion, as main.cc:219-222 does."""
+        d1 = np.ascontiguousarray(snap.delta1, np.float32)
+        ijk, lum = W.grid_sources(snap)
+        ijk = np.ascontiguousarray(ijk, np.int32)
+        lum = np.ascontiguousarray(lum, np.float64)
+        self._check(self.L.frt_update_hydro_step(self.h, box, d1.ctypes.data, C.c_float(a_rt), C.c_float(dt_snap),
+                                                 C.c_float(zz), len(lum), ijk.ctypes.data, lum.ctypes.data),
+                    "frt_update_hydro_step")
+        self.src[box] = (ijk, lum)
+        self.nsrc_box[box] = len(lum)
+        self.nsrc = sum(self.nsrc_box)
+
     def write_restart(self, box: int = 0):
         """(gas, rays, treion) records of a box in the reference's restart formats."""
         out = []
@@ -325,6 +339,27 @@ class RTContext:
             st = fn(self.h, self._ith_box.ctypes.data, self._ith_src.ctypes.data, C.byref(self.stats))
         self._check(st, "frt_step")
         return self.stats.as_dict()
+
+    # ---- launch shapes -------------------------------------------------------------------------
+    def autotune(self, steps: int = 3) -> Dict[str, float]:
+        """frt_autotune: `steps` RT steps that also time candidate launch shapes; the chosen
+        shapes are set on the context (and remembered for its ray-count bucket)."""
+        t = _abi.Tuning()
+        self._check(self.L.frt_autotune(self.h, int(steps), C.byref(t)), "frt_autotune")
+        return t.as_dict()
+
+    def tuning(self) -> Dict[str, float]:
+        t = _abi.Tuning()
+        self._check(self.L.frt_get_tuning(self.h, C.byref(t)), "frt_get_tuning")
+        return t.as_dict()
+
+    def set_tuning(self, **shape) -> None:
+        """frt_set_tuning with the given fields changed from the current shapes."""
+        t = _abi.Tuning()
+        self._check(self.L.frt_get_tuning(self.h, C.byref(t)), "frt_get_tuning")
+        for k, v in shape.items():
+            setattr(t, k, v)
+        self._check(self.L.frt_set_tuning(self.h, C.byref(t)), "frt_set_tuning")
 
     def last_stats(self) -> Dict[str, float]:
         st = _abi.StepStats()

@@ -144,6 +144,19 @@ frt_status frt_update_dt(frt_ctx* ctx, float* dt_out);
  * and ray positions scale by a_current/a_prev, the proper density by (a_prev/a_current)^3, and the
  * number densities follow from it with the ionised fractions kept. */
 frt_status frt_update_cosmo_expansion(frt_ctx* ctx, const float* a_current, const float* a_prev);
+/* update_hydro_step to a later hydro snapshot of one box (gas_funcs.cc:554-752), with the
+ * get_nphot_min_max that follows it (main.cc:221-222); call it where main.cc does, after new_rays
+ * and frt_update_cosmo_expansion. delta1: the new snapshot's 1+delta cube as get_ugas reads it
+ * (io_funcs.cc:33-62); a_rt: the scale factor at the current time (gas_funcs.cc:566); dt_snap: the
+ * cosmic time from this snapshot to the next (gas_funcs.cc:711); zz: this snapshot's redshift; the
+ * new sources gridded per cell as read_source_catalog leaves them (io_funcs.cc:157-233). The
+ * proper density becomes the new cube's times a_rt^-3, the cell size Lx0 a_rt / N, n_H and n_He
+ * follow from it, the ionised densities keep the box's ionised fractions, and n_HI = n_H - n_HII;
+ * the rays in flight keep their records. From the second switch on, d(delta)/dt between the
+ * last two snapshots enters the temperature equation (gas_funcs.cc:399, 711). The new source
+ * list replaces the old one (an owner mask, frt_set_source_owner, is cleared). */
+frt_status frt_update_hydro_step(frt_ctx* ctx, int box, const float* delta1, float a_rt, float dt_snap, float zz,
+                                 int nsrc, const int32_t* ijk, const double* lum);
 /* get_nphot_min_max (ray_tracing.cc:129-154) */
 frt_status frt_get_nphot_min_max(frt_ctx* ctx, double* nmin_out, double* nmax_out);
 /* set_clump + set_clight (subgrid.cc:799-811, rt_funcs.cc:129-143) */
@@ -219,6 +232,38 @@ frt_status frt_step_plain(frt_ctx* ctx, const uint16_t* itheta_per_box, const ui
                           frt_step_stats* stats);
 frt_status frt_last_stats(frt_ctx* ctx, frt_step_stats* stats);
 
+/* ---- launch shapes and the autotuner ----------------------------------------------------------
+ * The reference divides its ray loops statically over OpenMP threads (size_cpu,
+ * global_variables.cc:44) and rebalances the per-thread ray buffers between steps (balance_cpus,
+ * free_cpu; mem_funcs.cc:186-299). Here the matching choices are the launch shapes of the ray and
+ * cell kernels: block size and blocks per SM of the ray pass, the walk, the cell pass and the
+ * compaction + split, and how the ray pass hands out its moved rays (static per-warp slices, or
+ * chunks of a device-side queue). Shapes change only the work distribution, not the arithmetic of
+ * a ray or a cell. */
+typedef struct {
+  int raypass_block, raypass_blocks_per_sm; /* ray pass of a C2Ray iteration (mixed precision) */
+  int raypass_chunk;                        /* 0: static per-warp slices; > 0: rays per queue chunk */
+  int walk_block, walk_blocks_per_sm;       /* cell-boundary walk (update_rays) */
+  int cellpass_blocks_per_sm;               /* lit-cell pass of a C2Ray iteration */
+  int split_blocks_per_sm;                  /* compaction + split (split_rays) */
+  int steps;                                /* frt_autotune: RT steps it took */
+  /* frt_autotune: measured cost of the chosen shapes, ns per unit of work (crossing, ray, lit cell) */
+  double raypass_ns_per_crossing, walk_ns_per_ray, cellpass_ns_per_cell, split_ns_per_ray;
+} frt_tuning;
+/* Runs `steps` (>= 1; 3 recommended) whole RT steps of the context (they advance the simulation
+ * like frt_step_plain; the draws come from the context's streams) and times candidate shapes on
+ * them: every candidate of a round runs on a comparable share of one step's work (one C2Ray
+ * iteration's ray or cell pass, or one of k equal ray ranges of the walk and the compaction),
+ * costs are time per unit of work, and each round varies one parameter around the best so far.
+ * The chosen shapes are set on the context, reported in *out, and remembered for contexts of the
+ * same device, cell count and live-ray count (power-of-two bucket): frt_step switches to a
+ * remembered shape set when its ray count enters that bucket. */
+frt_status frt_autotune(frt_ctx* ctx, int steps, frt_tuning* out);
+frt_status frt_get_tuning(frt_ctx* ctx, frt_tuning* out);
+/* Sets the shapes (blocks 32..256, multiples of 32; blocks per SM 1..32; chunk 0..65536);
+ * FRT_ERR_INVALID otherwise. Turns off the remembered-shape switching of frt_step. */
+frt_status frt_set_tuning(frt_ctx* ctx, const frt_tuning* in);
+
 /* ---- rays ----------------------------------------------------------------------------------- */
 frt_status frt_num_rays(frt_ctx* ctx, int box, long long* n);
 /* Live rays of a box in pool order, unpacked like write_rays_binary (io_funcs.cc:274-303):
@@ -264,8 +309,11 @@ frt_status frt_read_rays(frt_ctx* ctx, int box, const void* buf, size_t len);
  * frt_set_sources order) and every cell's hydrogen density n_H (cm^-3; the cell's n_He, n_HI and
  * n_HeI scale with it as one density; ionised fractions, temperature, clumping and nphot_min are
  * held fixed). The segments of the step's rays are recomputed from the ray state, nothing is
- * stored between passes, and the context's state is not modified. Needs the state right after
- * set-up (no step taken: every ray still belongs to one source's cast); FRT_ERR_STATE otherwise.
+ * stored between passes, and the context's state is not modified. Any state of the run will do
+ * (after set-up or after any number of steps): a ray's photons are proportional to the luminosity
+ * of the source that cast it, found from the ray itself (an unmerged ray lies on the straight
+ * line from its source's cell centre along its direction). A merge combines rays of different
+ * sources, and rays read from a restart file have no known source: after either, FRT_ERR_STATE.
  * dL (nsrc of the box) and dnH (N^3) may be NULL. No counterpart in the reference. */
 typedef struct {
   int box;

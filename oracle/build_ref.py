@@ -30,6 +30,8 @@ import subprocess
 import sys
 from typing import Optional
 
+import numpy as np
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 # the reference checkout: FRT_REFERENCE_DIR, else the development container's checkout; a box
@@ -116,6 +118,13 @@ def _configure(d: str, spec: W.BoxSpec, ncpu: int, path_length: int, restart: bo
         (r"^double const nu_phot\[Nfreq\]\s*=.*$", f"double const nu_phot[Nfreq] = {{{nu}}};"),
         (r"^float const temp_0\s*=.*$", "float const temp_0 = 1e4;"),
         (r"^int const path_length\s*=.*$", f"int const path_length = {path_length};"),
+        # file names of update_hydro_step (gas_funcs.cc:554-752), relative to the stage directory
+        # (ref_driver's FRT_HYDRO hook)
+        (r"^const int snapinit\s*=.*$", "const int snapinit             = 10;"),
+        (r"^const char output_dir\[\]\s*=.*$", 'const char output_dir[]      = "./hydro_out/";'),
+        (r"^const char hydro_base\[\]\s*=.*$", 'const char hydro_base[]    = "./hydro/";'),
+        (r"^const char density_dir\[\]\s*=.*$", 'const char density_dir[] = "";'),
+        (r"^const char source_dir\[\]\s*=.*$", 'const char source_dir[] = "";'),
     ]
     for pat, rep in reps:
         t = _sub_line(t, pat, rep)
@@ -171,7 +180,7 @@ def _unlimited_stack():
 
 def run(name: str, inp: W.BoxInputs, rundir: str, nsteps: int, seed: int, dump_every: int = 1,
         threads: int = 1, timeout: Optional[float] = None, restart_out: Optional[str] = None,
-        cosmo: bool = False) -> str:
+        cosmo: bool = False, hydro=None) -> str:
     """Run the compiled reference on inputs written to rundir; returns stdout. With restart_out,
     the reference's restart writers store gas.bin / rays.bin / tre.bin there after the last step;
     with cosmo, the cosmological expansion runs after every step (its scale factors are logged as
@@ -187,6 +196,21 @@ def run(name: str, inp: W.BoxInputs, rundir: str, nsteps: int, seed: int, dump_e
         env["FRT_RESTART_OUT"] = os.path.abspath(restart_out)
     if cosmo:
         env["FRT_COSMO"] = "1"
+    if hydro:
+        # snapshot switches: ([step, ...], [z1, z2, z3], [BoxInputs of snapshot 1, 2])
+        at, zs, snaps = hydro
+        os.makedirs(os.path.join(d, "hydro"), exist_ok=True)
+        os.makedirs(os.path.join(d, "hydro_out"), exist_ok=True)
+        for n, snap in enumerate(snaps, 1):
+            tag = f"01{n}"
+            snap.delta1.astype("float32").tofile(os.path.join(d, "hydro", f"density.{tag}.{snap.spec.n}"))
+            cat = np.zeros((snap.src_pos.shape[0], 5), dtype=np.float64)
+            cat[:, 0:3] = snap.src_pos
+            cat[:, 4] = snap.src_lum
+            cat.tofile(os.path.join(d, "hydro", f"ndot_catalog_{tag}"))
+            np.array([snap.src_pos.shape[0]], dtype=np.int64).tofile(os.path.join(d, "hydro", f"numhalos.{tag}"))
+        env["FRT_HYDRO"] = ",".join(str(k) for k in at)
+        env["FRT_HYDRO_Z"] = ",".join(repr(float(z)) for z in zs)
     r = subprocess.run(args, cwd=d, env=env, capture_output=True, text=True, timeout=timeout,
                        preexec_fn=_unlimited_stack)
     if r.returncode != 0:

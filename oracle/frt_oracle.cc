@@ -123,6 +123,7 @@ struct Ray {
   int pind[kMaxPL];
   float pdist[kMaxPL];
   short ray_end;
+  int src;   // casting source (index into Ctx::src); a merge of rays of several sources gives -1
 };
 
 struct Src {
@@ -162,6 +163,11 @@ struct Ctx {
   // that a dumping ray both deposited and kept until its removal. Bookkeeping only: no field or
   // ray of the restatement depends on it.
   double led_emitted, led_deposited, led_killed, led_overlap;
+  // hydro snapshots (update_hydro_step, gas_funcs.cc:554-752): the volume-averaged density, the
+  // previous snapshot's density and d(delta)/dt of the temperature equation (gas_funcs.cc:399)
+  float avg_rho;
+  std::vector<float> rho_prev, ddelta_dt;
+  float step_dt;   // the time step the last step ran with (get_nphot_min_max at a switch uses it)
 };
 
 static inline long cidx(const Ctx& c, int i, int j, int k) { return ((long)i * c.N + j) * c.N + k; }
@@ -249,7 +255,7 @@ static void alloc(Ctx& c) {
                              &c.avg_nhe1, &c.avg_gamma, &c.avg_gamma_he1, &c.recomb_H2, &c.recomb_He2,
                              &c.recomb_He3, &c.recrate_H2, &c.recrate_He2, &c.dne_dt, &c.mfp, &c.mfp_912, &c.treion,
                              &c.treion_out, &c.heat_rate, &c.cool_rate, &c.gamma_H1_tot, &c.gamma_He1_tot,
-                             &c.nH1_prev, &c.IF_speed, &c.Inc_Flux, &c.ray_dt};
+                             &c.nH1_prev, &c.IF_speed, &c.Inc_Flux, &c.ray_dt, &c.rho_prev, &c.ddelta_dt};
   for (auto* v : f) v->assign(n3, 0.f);
   std::vector<float>* g[] = {&c.gamma_H1_nu, &c.gamma_He1_nu, &c.ngam_nu, &c.u_nu, &c.avg_gamma_nu,
                              &c.avg_gamma_nu_he1};
@@ -257,20 +263,20 @@ static void alloc(Ctx& c) {
   c.treion_flag.assign(n3, 0);
 }
 
-static void init_rays(Ctx& c, int i, int j, int k, double lum);
+static void init_rays(Ctx& c, int i, int j, int k, double lum, int src);
 
 static void new_rays(Ctx& c) {
   long created = 0;
   for (size_t s = 0; s < c.src.size(); ++s) {
     const Src& S = c.src[s];
-    init_rays(c, S.i, S.j, S.k, S.lum);
+    init_rays(c, S.i, S.j, S.k, S.lum, (int)s);
     created += 12 * pow(2, 2 * c.hpx_lvl);
     c.ray_dt[cidx(c, S.i, S.j, S.k)] = 0.;
   }
   c.total_rays += created;
 }
 
-static void init_rays(Ctx& c, int i, int j, int k, double lum) {
+static void init_rays(Ctx& c, int i, int j, int k, double lum, int src) {
   const long ci = cidx(c, i, j, k);
   unsigned short itheta = (unsigned short)(rand() % kNtheta);
   float a0 = c.random_angles[itheta][0], b0 = c.random_angles[itheta][1], g0 = c.random_angles[itheta][2];
@@ -308,6 +314,7 @@ static void init_rays(Ctx& c, int i, int j, int k, double lum) {
       R.z = c.dxc / 2.;
       R.time = 0.;
       R.pind[0] = i * c.N * c.N + j * c.N + k;
+      R.src = src;
       for (int nu = 0; nu < c.F; nu++) c.led_emitted += (double)R.nphot[nu] * kPhotNorm;
       c.rays.push_back(R);
     }
@@ -640,6 +647,7 @@ static void merge(Ctx& c) {
     } else {
       Ray& M = c.rays[base[b]];
       float nt = sum_nphot(c, R);
+      if (M.src != R.src) M.src = -1;
       for (int nu = 0; nu < c.F; nu++) M.nphot[nu] += R.nphot[nu];
       R.r /= c.dx0;
       M.r += pow(R.r, 2.) * nt;
@@ -743,6 +751,7 @@ static void split_rays(Ctx& c) {
       Ch.z = z0;
       Ch.time = time;
       Ch.pind[0] = icn * c.N * c.N + jcn * c.N + kcn;
+      Ch.src = P.src;
       c.rays.push_back(Ch);
     }
   }
@@ -801,12 +810,21 @@ static void update_thermal(Ctx& c) {
       float dt_temp = mind(get_thermal_tstep(c, q), c.dt - t_temp);
       update_heat_cool(c, q);
       c.temp[q] = (c.temp[q] + 2. / 3. / O_KB / c.n_tot[q] * (c.heat_rate[q] - c.cool_rate[q]) * dt_temp) /
-                  (1. + 2. * hubble(1. / (1. + c.zz)) * dt_temp + 1. / c.n_tot[q] * c.dne_dt[q] * dt_temp);
+                  (1. + 2. * hubble(1. / (1. + c.zz)) * dt_temp + 1. / c.n_tot[q] * c.dne_dt[q] * dt_temp -
+                   2. * c.ddelta_dt[q] / 3. / (c.rho[q] / c.avg_rho) * dt_temp);
       t_temp += dt_temp;
     }
     c.temp[q] = maxd(c.temp[q], kTempMin);
     c.nH1_prev[q] = c.nH1[q];
   }
+}
+
+// calc_vol_avg (data_funcs.cc:75-92): double sum in (i, j, k) order, float result
+static float vol_avg(const Ctx& c, const std::vector<float>& f) {
+  double tot = 0.;
+  const long n3 = (long)c.N * c.N * c.N;
+  for (long q = 0; q < n3; q++) tot += (double)f[q];
+  return (float)tot / pow((double)c.N, 3.);
 }
 
 static void compact(Ctx& c) {
@@ -866,7 +884,9 @@ void* orc_create(const Params* p, const float* delta1, int nsrc, const int32_t* 
       c->rho[q] = delta1[q];
       c->rho[q] *= (float)rho_unit;
     }
+    c->avg_rho = vol_avg(*c, c->rho);
     for (long q = 0; q < n3; q++) c->rho[q] *= pow(a_snap, -3.);
+    c->avg_rho *= pow(a_snap, -3.);
   }
   for (int s = 0; s < nsrc; s++) c->src.push_back({src_ijk[3 * s], src_ijk[3 * s + 1], src_ijk[3 * s + 2], src_lum[s]});
   for (int i = 0; i < kNalpha; i++)
@@ -956,6 +976,7 @@ void orc_step(void* h) {
   Ctx& c = *(Ctx*)h;
   c.step += 1;
   c.led_emitted = c.led_deposited = c.led_killed = c.led_overlap = 0.;
+  c.step_dt = c.dt;
   const long n3 = (long)c.N * c.N * c.N;
   for (long q = 0; q < n3; q++) c.clump[q] = c.const_clump;
   if (c.have_clump) c.clump = c.clump_in;
@@ -1096,6 +1117,7 @@ extern "C" void orc_cosmo_expansion(void* h, float a_current, float a_prev) {
     c.n_tot[q] = c.nH[q] + c.nHe[q] + c.ne[q];
     c.nH1_prev[q] = c.nH1[q];
   }
+  c.avg_rho *= pow(a_prev / a_current, 3.);
   const float dxc = c.dxc;
   for (Ray& R : c.rays) {
     if (!R.alive) continue;
@@ -1108,6 +1130,74 @@ extern "C" void orc_cosmo_expansion(void* h, float a_current, float a_prev) {
     if (R.y >= dxc * (1. - kMinDist / 2.)) R.y = dxc * (1. - kMinDist);
     if (R.z <= 0.) R.z = kMinDist * dxc;
     if (R.z >= dxc * (1. - kMinDist / 2.)) R.z = dxc * (1. - kMinDist);
+  }
+  c.dt = c.tstep_factor * c.dxc / c.cl_factor / O_CL;   // update_dt (main.cc:237)
+}
+
+// update_hydro_step for a later snapshot (gas_funcs.cc:554-752; the branch zz != zinit with a
+// next snapshot to come), then get_nphot_min_max and update_dt (main.cc:221-237): delta1 is the
+// new 1+delta cube as get_ugas reads it, the sources are gridded (i, j, k, lum) as
+// read_source_catalog leaves them (io_funcs.cc:157-233), a_rt the scale factor at the current
+// time, dt_snap = cosmic_time(a_next) - cosmic_time(a) of the snapshots, zz the new redshift.
+extern "C" void orc_hydro_step(void* h, const float* delta1, int nsrc, const int32_t* src_ijk, const double* src_lum,
+                               float a_rt, float dt_snap, float zz_new) {
+  Ctx& c = *(Ctx*)h;
+  const long n3 = (long)c.N * c.N * c.N;
+  c.zz = zz_new;
+  c.Lx = c.Lx0 * a_rt;
+  // get_ugas (io_funcs.cc:33-62) and the a^-3 of update_hydro_step (gas_funcs.cc:669-684)
+  {
+    float rho_c_cgs = 1.87890e-29, ob = 0.0482266, h0 = 0.68;
+    double rho_unit = rho_c_cgs * ob * pow(h0, 2.);
+    for (long q = 0; q < n3; q++) {
+      c.rho[q] = delta1[q];
+      c.rho[q] *= (float)rho_unit;
+    }
+    c.avg_rho = vol_avg(c, c.rho);
+    for (long q = 0; q < n3; q++) c.rho[q] *= pow(a_rt, -3.);
+    c.avg_rho *= pow(a_rt, -3.);
+  }
+  // read_source_catalog: the new sources; every ray_dt back to 0
+  c.src.clear();
+  for (int s = 0; s < nsrc; s++) c.src.push_back({src_ijk[3 * s], src_ijk[3 * s + 1], src_ijk[3 * s + 2], src_lum[s]});
+  for (long q = 0; q < n3; q++) c.ray_dt[q] = 0.;
+  const float avg_rho_prev = vol_avg(c, c.rho_prev);
+  c.dxc = c.Lx / c.N * O_KPC_TO_CM;
+  const float fion = 1.f;   // plain mode (rt_funcs.cc:55)
+  for (long q = 0; q < n3; q++) {
+    c.nH[q] = (1. - O_Y) * c.rho[q] / O_MH;
+    c.nHe[q] = O_Y * c.rho[q] / (4. * O_MH);
+    c.nH2[q] = c.f_H2[q] * c.nH[q] / fion;
+    c.nHe2[q] = c.f_He2[q] * c.nHe[q] / fion;
+    c.nHe3[q] = c.f_He3[q] * c.nHe[q] / fion;
+    c.nH1[q] = c.nH[q] - c.nH2[q];
+    c.avg_nh1[q] = c.nH1[q];
+    c.nHe1[q] = c.nHe[q] - c.nHe2[q] - c.nHe3[q];
+    c.avg_nhe1[q] = c.nHe1[q];
+    c.ne[q] = c.nH2[q] + c.nHe2[q] + 2. * c.nHe3[q];
+    c.n_tot[q] = c.nH[q] + c.nHe[q] + c.ne[q];
+    if (avg_rho_prev > 0.) c.ddelta_dt[q] = (c.rho[q] / c.avg_rho - c.rho_prev[q] / avg_rho_prev) / dt_snap;
+    c.rho_prev[q] = c.rho[q];
+    c.nH1_prev[q] = c.nH1[q];
+  }
+  // get_nphot_min_max (ray_tracing.cc:129-154) with the new sources and the time step of the
+  // step just taken (update_dt follows it, main.cc:237)
+  {
+    int counter = 0;
+    c.nphot_base_avg = 0.;
+    for (const Src& S : c.src) {
+      if (S.lum > 0.) {
+        double tmp = 0.;
+        for (int nu = 0; nu < c.F; nu++)
+          tmp += c.spectrum[nu] * S.lum * c.step_dt / 12. / pow(2., 2. * c.hpx_lvl) / kPhotNorm;
+        c.nphot_base_avg += (double)log10(tmp);
+        counter += 1;
+      }
+    }
+    c.nphot_base_avg /= counter;
+    c.nphot_base_avg = pow(10., c.nphot_base_avg);
+    c.nphot_max = 1e3 * c.nphot_base_avg;
+    c.nphot_min = 1e-10 * c.nphot_base_avg;
   }
   c.dt = c.tstep_factor * c.dxc / c.cl_factor / O_CL;   // update_dt (main.cc:237)
 }
@@ -1284,6 +1374,7 @@ int orc_read_restart(void* h, const void* gas, size_t gas_size, const void* tre,
       R.r = in.get<float>(); R.dr = in.get<float>(); R.x = in.get<float>(); R.y = in.get<float>();
       R.z = in.get<float>(); R.time = in.get<float>();
       R.pind[0] = in.get<int>();
+      R.src = -1;   // the restart records do not say which source cast a ray
       if (in.ok && !(x == 0 && R.nphot[0] == 0.)) c.rays.push_back(R);
       x = in.get<long>();
     }
@@ -1344,8 +1435,6 @@ struct AdjProblem {
 
 AdjProblem adj_setup(Ctx& c, const int* lo, const int* hi) {
   AdjProblem P;
-  std::unordered_map<long, int> src_of;
-  for (size_t s = 0; s < c.src.size(); ++s) src_of[cidx(c, c.src[s].i, c.src[s].j, c.src[s].k)] = (int)s;
   c.clight = c.cl_factor * O_CL;
   c.nc = c.nl_const;
   for (const Ray& R0 : c.rays) {
@@ -1356,8 +1445,8 @@ AdjProblem adj_setup(Ctx& c, const int* lo, const int* hi) {
     if (R.active) continue;   // did not leave its cell: no segments this step
     if (c.rkill > 0.0 && (double)R.r > c.rkill) continue;
     AdjRay A;
-    auto it = src_of.find(cell0);
-    A.src = it == src_of.end() ? -1 : it->second;
+    A.src = R0.src;   // the source that cast the ray (a ray merged from several sources: -1)
+    (void)cell0;
     A.nseg = R.ray_end;
     for (int p = 0; p < R.ray_end; ++p) {
       A.cell[p] = R.pind[p];

@@ -77,6 +77,8 @@ def lib():
         _lib.orc_read_restart.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                                           C.c_size_t]
         _lib.orc_cosmo_expansion.argtypes = [C.c_void_p, C.c_float, C.c_float]
+        _lib.orc_hydro_step.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
+                                        C.c_float]
         _lib.orc_adj_objective.restype = C.c_double
         _lib.orc_adj_objective.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_long)]
@@ -154,6 +156,15 @@ class Oracle:
     def cosmo_expansion(self, a_current: float, a_prev: float) -> None:
         """update_cosmo_expansion with the given scale factors, then update_dt."""
         self._lib.orc_cosmo_expansion(self.h, C.c_float(a_current), C.c_float(a_prev))
+
+    def hydro_step(self, snap: W.BoxInputs, a_rt: float, dt_snap: float, zz: float) -> None:
+        """update_hydro_step to the snapshot `snap` (its density and sources), then
+        get_nphot_min_max and update_dt (frt_oracle.cc, orc_hydro_step)."""
+        ijk, lum = W.grid_sources(snap)
+        keep = [np.ascontiguousarray(snap.delta1, np.float32), np.ascontiguousarray(ijk, np.int32),
+                np.ascontiguousarray(lum, np.float64)]
+        self._lib.orc_hydro_step(self.h, keep[0].ctypes.data, len(lum), keep[1].ctypes.data, keep[2].ctypes.data,
+                                 C.c_float(a_rt), C.c_float(dt_snap), C.c_float(zz))
 
     def _write(self, fn) -> bytes:
         f = getattr(self._lib, fn)

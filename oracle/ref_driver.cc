@@ -15,6 +15,13 @@
 //     (write_gas_binary, write_rays_binary, write_treion) run after the last step;
 //   * with FRT_COSMO in the environment, update_cosmo_expansion (gas_funcs.cc:460-548) runs after
 //     new_rays as in main.cc:219-220, and the two scale factors it uses are logged (hex floats);
+//   * with FRT_HYDRO=<k1>[,<k2>] and FRT_HYDRO_Z=<z1>,<z2>,<z3> in the environment, the
+//     reference's own update_hydro_step (gas_funcs.cc:554-752) and get_nphot_min_max run after
+//     steps k1 (and k2), after new_rays and the optional expansion (main.cc:219-224): the
+//     snapshot list is {zinit, z1, z2, z3}, the n-th switch reads hydro/density.01<n>.<N>,
+//     hydro/ndot_catalog_01<n> and hydro/numhalos.01<n> under the stage directory (snapinit =
+//     10) and writes its outputs under hydro_out/; the scale factor, the snapshot interval and the
+//     redshift it uses are logged as 'HYDRO step a_rt dt_snap zz' (hex floats);
 //   * in a stage built with input_grid = TRUE the set-up is the reference's restart path: the
 //     grid is sized as init() would (init_funcs.cc:22-30), the catalogue is read, init() reads the
 //     gas and treion restart files, init_rt() reads the ray file, and no rays are cast.
@@ -115,7 +122,17 @@ int main(int argc, char** argv) {
   init_lock();
   import_cosmic_time();
   const bool cosmo = getenv("FRT_COSMO") != nullptr;
-  if (cosmo) make_scale_factor_table();
+  int hydro_at[2] = {-1, -1}, n_hydro = 0;
+  float hydro_z[3] = {0.f, 0.f, 0.f};
+  if (const char* hy = getenv("FRT_HYDRO")) {
+    n_hydro = sscanf(hy, "%d,%d", &hydro_at[0], &hydro_at[1]);
+    const char* hz = getenv("FRT_HYDRO_Z");
+    if (n_hydro < 1 || !hz || sscanf(hz, "%f,%f,%f", &hydro_z[0], &hydro_z[1], &hydro_z[2]) != 3) {
+      printf("FRT_HYDRO needs FRT_HYDRO_Z=z1,z2,z3\n");
+      return 2;
+    }
+  }
+  if (cosmo || n_hydro > 0) make_scale_factor_table();
 
   // first-snapshot set-up (gas_funcs.cc:595-613) at a = 1/(1+zinit)
   zz = zinit;
@@ -199,6 +216,18 @@ int main(int argc, char** argv) {
       printf("COSMO %d %a %a\n", s, a_current, a_prev);
       update_cosmo_expansion();
     }
+    for (int hsw = 0; hsw < n_hydro; hsw++)
+      if (s == hydro_at[hsw]) {
+        hydro_steps.assign({zinit, hydro_z[0], hydro_z[1], hydro_z[2]});
+        num_hydro_steps = 4;
+        ihydro = hsw + 1;
+        const float a_rt = scale_factor(t + cosmic_time(1. / (1. + zinit)));
+        const float aa = 1. / (1. + hydro_steps[ihydro]), aa_next = 1. / (1. + hydro_steps[ihydro + 1]);
+        const float dt_snap = cosmic_time(aa_next) - cosmic_time(aa);
+        printf("HYDRO %d %a %a %a\n", s, a_rt, dt_snap, hydro_steps[ihydro]);
+        update_hydro_step();
+        get_nphot_min_max();
+      }
     update_dt();
     balance_cpus();
     const double w6 = omp_get_wtime();

@@ -8,7 +8,7 @@ files pin the CPU restatement in oracle/frt_oracle.cc and, through it, the CUDA 
     python tests/golden/make_golden.py [names]
 
 T16C holds a run with the reference's cosmological expansion after every step and the scale
-factors it used. T16R holds the reference's restart files (write_gas_binary / write_rays_binary / write_treion
+factors it used. T16H adds two hydro snapshot switches (update_hydro_step) with rays in flight. T16R holds the reference's restart files (write_gas_binary / write_rays_binary / write_treion
 after 3 steps of T16) and the states of the reference's own restart path run from them.
 """
 from __future__ import annotations
@@ -127,6 +127,49 @@ def make_cosmo(name="T16C", base=("T16", W.config_tiny(), 11), steps=4):
                         a_current=np.array(ac, np.float32), a_prev=np.array(ap, np.float32), **out)
 
 
+HYDRO_Z = (7.9, 7.8, 7.7)   # the redshifts of snapshots 1, 2 and the one after them
+HYDRO_AT = (2, 4)           # switches after these steps
+
+
+def hydro_snapshots(spec):
+    """The later snapshots of the snapshot-switch case: the same box, its own seeded density and
+    sources per snapshot (seeds 101, 102)."""
+    import dataclasses
+    return [W.make_inputs(dataclasses.replace(spec, seed=100 + n, sigma_ln=0.5 + 0.05 * n)) for n in (1, 2)]
+
+
+def make_hydro(name="T16H", base=("T16", W.config_tiny(), 11), steps=6):
+    """A run with the cosmological expansion after every step and two hydro snapshot switches
+    (the reference's own update_hydro_step and get_nphot_min_max) after steps 2 and 4, with rays
+    in flight: its states, the scale factors of every expansion and the (a_rt, dt_snap, zz) of
+    every switch. The second switch is the first with a previous snapshot, so d(delta)/dt enters
+    the temperature equation from then on."""
+    bname, spec, seed = base
+    B.build(bname, spec, ncpu=1)
+    inp = W.make_inputs(spec)
+    snaps = hydro_snapshots(spec)
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        log = B.run(bname, inp, td, steps, seed, dump_every=1, cosmo=True, hydro=(HYDRO_AT, HYDRO_Z, snaps))
+        ac, ap, hy = [], [], []
+        for line in log.splitlines():
+            if line.startswith("COSMO"):
+                _, s_, a, b = line.split()
+                ac.append(float.fromhex(a))
+                ap.append(float.fromhex(b))
+            if line.startswith("HYDRO"):
+                _, s_, a, dts, z = line.split()
+                hy.append([float(int(s_)), float.fromhex(a), float.fromhex(dts), float.fromhex(z)])
+        assert len(ac) == steps and len(hy) == len(HYDRO_AT), log[-2000:]
+        for s in range(1, steps + 1):
+            dd = frtd.read(os.path.join(td, f"dump_{s:04d}.frtd"))
+            for k in FIELDS + RAYS + ["scalars"]:
+                out[f"s{s}_{k}"] = dd[k]
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), seed=seed, steps=np.arange(1, steps + 1),
+                        a_current=np.array(ac, np.float32), a_prev=np.array(ap, np.float32),
+                        hydro=np.array(hy, np.float64), **out)
+
+
 if __name__ == "__main__":
     only = sys.argv[1:]
     for case in CASES:
@@ -139,3 +182,6 @@ if __name__ == "__main__":
     if not only or "T16C" in only:
         make_cosmo()
         print("wrote T16C")
+    if not only or "T16H" in only:
+        make_hydro()
+        print("wrote T16H")
