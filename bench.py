@@ -389,7 +389,12 @@ def run_partition(args, rank: int, world: int, local_rank: int):
     spec = _spec(args.workload)
     inp = W.make_inputs(spec)
     ctx = P.make_share(inp, args.seed, rank, world, device=local_rank, ray_capacity=args.ray_capacity)
-    comb = P.DistCombiner(ctx, local_rank) if world > 1 else P.LocalCombiner([ctx], local_rank)
+    if world > 1:
+        comb = P.DistCombiner(ctx, local_rank)   # all-reduces ordered on the context's stream
+    else:
+        ctx.set_phase_async(True)                # one share: nothing to combine, phases only enqueue
+        comb = P.LocalCombiner([ctx], local_rank)
+    stream = torch.cuda.ExternalStream(ctx.phase_stream(), device=torch.device("cuda", local_rank))
     for _ in range(args.warmup):
         P.step_shares([ctx], comb)
     dist = world > 1
@@ -403,9 +408,9 @@ def run_partition(args, rank: int, world: int, local_rank: int):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         torch.cuda.synchronize(local_rank)
-        e0.record()
+        e0.record(stream)   # the phases run on the context's stream
         st = P.step_shares([ctx], comb)[0]
-        e1.record()
+        e1.record(stream)
         torch.cuda.synchronize(local_rank)
         dev_ms += e0.elapsed_time(e1)
         cross += st["crossings"]

@@ -34,7 +34,8 @@ EXPORTS = ["frt_create", "frt_destroy", "frt_last_error", "frt_rotation_table", 
            "frt_last_adjoint_timing", "frt_write_gas", "frt_write_rays", "frt_write_treion", "frt_read_gas",
            "frt_read_treion", "frt_read_rays", "frt_update_cosmo_expansion",
            "frt_set_cast_per_source", "frt_last_kernel_timing", "frt_set_source_owner", "frt_step_phase",
-           "frt_phase_buffers", "frt_autotune", "frt_get_tuning", "frt_set_tuning", "frt_update_hydro_step"]
+           "frt_phase_buffers", "frt_autotune", "frt_get_tuning", "frt_set_tuning", "frt_update_hydro_step", "frt_set_phase_async",
+           "frt_phase_stream"]
 PHASE_WALK, PHASE_CELLS, PHASE_RAYPASS, PHASE_CELLPASS, PHASE_END = 0, 1, 2, 3, 4
 NOALLOC_MAX_CELLS = 1 << 20
 
@@ -143,6 +144,8 @@ def lib() -> C.CDLL:
         "frt_last_kernel_timing": ([P, I, P], I),
         "frt_autotune": ([P, I, C.POINTER(Tuning)], I),
         "frt_update_hydro_step": ([P, I, P, C.c_float, C.c_float, C.c_float, I, P, P], I),
+        "frt_set_phase_async": ([P, I], I),
+        "frt_phase_stream": ([P, C.POINTER(P)], I),
         "frt_get_tuning": ([P, C.POINTER(Tuning)], I),
         "frt_set_tuning": ([P, C.POINTER(Tuning)], I),
     }

@@ -46,6 +46,7 @@ struct frt_ctx {
   cudaGraphExec_t graph = nullptr;
   bool graph_valid = false;
   long long phase_nlit = 0;   // lit cells of the current phased step (frt_step_phase)
+  bool phase_async = false;   // phases only enqueue (frt_set_phase_async)
   uint8_t* src_own_buf = nullptr;
   int* chunk_buf = nullptr;   // per-chunk lit counts of the phased step
   frt_step_stats stats_scratch{};
@@ -1328,9 +1329,22 @@ frt_status frt_step_phase(frt_ctx* ctx, int phase, int iter, const uint16_t* ith
     default:
       return FRT_ERR_INVALID;
   }
-  // the caller reads or combines device arrays next: the phase's work is complete on return
-  CK(cudaStreamSynchronize(s));
+  // the caller reads or combines device arrays next: unless it orders its combines on the
+  // context's stream (frt_set_phase_async), the phase's work is complete on return
+  if (!ctx->phase_async) CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
+  return FRT_OK;
+}
+
+frt_status frt_set_phase_async(frt_ctx* ctx, int async) {
+  if (!ctx) return FRT_ERR_INVALID;
+  ctx->phase_async = async != 0;
+  return FRT_OK;
+}
+
+frt_status frt_phase_stream(frt_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return FRT_ERR_INVALID;
+  *stream = (void*)ctx->s_main;
   return FRT_OK;
 }
 

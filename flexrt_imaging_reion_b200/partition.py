@@ -60,13 +60,16 @@ def _views(ctx: rt.RTContext, device: int):
 
 
 class LocalCombiner:
-    """Combines contexts of one process (all on one device)."""
+    """Combines contexts of one process (all on one device). With one context there is nothing to
+    combine, so no work and no synchronisation (the one-GPU run of the phased step)."""
 
     def __init__(self, ctxs: Sequence[rt.RTContext], device: int = 0):
         self.ctxs, self.device = list(ctxs), device
 
     def _apply(self, pick, reduce):
         import torch
+        if len(self.ctxs) == 1:
+            return
         views = [pick(_views(c, self.device)) for c in self.ctxs]
         if views[0] is None:
             return
@@ -91,12 +94,21 @@ class LocalCombiner:
 class DistCombiner:
     """Combines one context per rank over torch.distributed (NCCL: one GPU per rank). `views`
     and `sync` default to the context's device arrays and a device synchronisation; they are
-    parameters so that the exchange can be exercised with host tensors over gloo."""
+    parameters so that the exchange can be exercised with host tensors over gloo. With
+    `on_stream` (the default on a GPU), the context's phases only enqueue and every all-reduce is
+    ordered on the context's own stream (torch waits for the phases queued before it and the
+    phases queued after it wait for the collective): no host synchronisation between phases."""
 
-    def __init__(self, ctx, device: int, views=None, sync=None):
+    def __init__(self, ctx, device: int, views=None, sync=None, on_stream: bool = None):
         self.ctxs, self.device = [ctx], device
         self._views = views or (lambda c: _views(c, self.device))
+        self.on_stream = (views is None and sync is None) if on_stream is None else on_stream
         self._sync = sync or self._device_sync
+        self._stream = None
+        if self.on_stream:
+            import torch
+            ctx.set_phase_async(True)
+            self._stream = torch.cuda.ExternalStream(ctx.phase_stream(), device=torch.device("cuda", device))
 
     def _device_sync(self):
         import torch
@@ -105,6 +117,11 @@ class DistCombiner:
     def _all_reduce(self, t, op):
         import torch.distributed as dist
         if t is None:
+            return
+        if self._stream is not None:
+            import torch
+            with torch.cuda.stream(self._stream):
+                dist.all_reduce(t, op=op)
             return
         self._sync()
         dist.all_reduce(t, op=op)

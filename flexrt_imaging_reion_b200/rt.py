@@ -185,6 +185,16 @@ class RTContext:
         self._check(self.L.frt_step_phase(self.h, phase, it, None, None, C.byref(self.stats)), "frt_step_phase")
         return self.stats.as_dict()
 
+    def set_phase_async(self, on: bool) -> None:
+        """frt_set_phase_async: phases only enqueue on the context's stream (phase_stream())."""
+        self._check(self.L.frt_set_phase_async(self.h, int(bool(on))), "frt_set_phase_async")
+
+    def phase_stream(self) -> int:
+        """The context's stream (cudaStream_t as an integer), for work ordered with the phases."""
+        v = C.c_void_p()
+        self._check(self.L.frt_phase_stream(self.h, C.byref(v)), "frt_phase_stream")
+        return int(v.value or 0)
+
     def phase_buffers(self):
         """Device addresses and sizes of the arrays combined between phases:
         (lit_flag, ncell, lit_acc, lit_heat, nlit)."""

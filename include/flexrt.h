@@ -227,6 +227,13 @@ frt_status frt_step_phase(frt_ctx* ctx, int phase, int iter, const uint16_t* ith
  * of the current step). */
 frt_status frt_phase_buffers(frt_ctx* ctx, void** lit_flag, long long* ncell, void** lit_acc, void** lit_heat,
                              long long* nlit);
+/* Phases that only enqueue (async != 0): each phase returns once its kernels are queued on the
+ * context's stream (frt_phase_stream returns it as a cudaStream_t), except CELLS, which waits for
+ * the lit-cell count (the length of the combined arrays), and END, which waits for the step's
+ * totals. The caller then orders its combines on that stream (e.g. NCCL collectives enqueued on
+ * it). Default (async = 0): every phase has finished on the device when it returns. */
+frt_status frt_set_phase_async(frt_ctx* ctx, int async);
+frt_status frt_phase_stream(frt_ctx* ctx, void** stream);
 /* Same as frt_step but launching every kernel directly (no graph) */
 frt_status frt_step_plain(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t* itheta_per_source,
                           frt_step_stats* stats);

@@ -62,9 +62,12 @@ def user_inputs_values(spec: W.BoxSpec, ncpu: int, path_length: int = 8) -> dict
     }
 
 
-def stage(name: str, spec: W.BoxSpec, ncpu: int, path_length: int = 8, restart: bool = False) -> str:
+def stage(name: str, spec: W.BoxSpec, ncpu: int, path_length: int = 8, restart: bool = False,
+          subgrid: bool = False) -> str:
     """Copy + configure the reference sources into oracle/_ref/<name>. A restart stage is built
-    with input_grid = TRUE and reads input_files/restart_{gas,rays,tre}.bin."""
+    with input_grid = TRUE and reads input_files/restart_{gas,rays,tre}.bin. A sub-grid stage is
+    built with subgrid = TRUE, equilibrium = TRUE, ifront = FALSE and reads its tables from
+    subgrid_files/ under the stage directory."""
     d = os.path.join(OUT, name)
     src = os.path.join(d, "src")
     os.makedirs(src, exist_ok=True)
@@ -73,11 +76,12 @@ def stage(name: str, spec: W.BoxSpec, ncpu: int, path_length: int = 8, restart: 
         shutil.copyfile(os.path.join(REF_SRC, f), os.path.join(src, f))
     for f in REF_DATA:
         shutil.copyfile(os.path.join(REF_SRC, f), os.path.join(d, f))
-    _configure(d, spec, ncpu, path_length, restart)
+    _configure(d, spec, ncpu, path_length, restart, subgrid)
     return d
 
 
-def _configure(d: str, spec: W.BoxSpec, ncpu: int, path_length: int, restart: bool = False) -> None:
+def _configure(d: str, spec: W.BoxSpec, ncpu: int, path_length: int, restart: bool = False,
+               subgrid: bool = False) -> None:
     src = os.path.join(d, "src")
     # HEALPix includes -> project shim
     for f in ("ray_tracing.cc", "mem_funcs.cc"):
@@ -96,7 +100,10 @@ def _configure(d: str, spec: W.BoxSpec, ncpu: int, path_length: int, restart: bo
         (r"^bool const c2ray_iter\s*=.*$", "bool const c2ray_iter    = TRUE;"),
         (r"^bool const ifront\s*=.*$", "bool const ifront        = FALSE;"),
         (r"^bool const he2_tr_h2\s*=.*$", "bool const he2_tr_h2     = FALSE;"),
-        (r"^bool const subgrid\s*=.*$", "bool const subgrid       = FALSE;"),
+        (r"^bool const subgrid\s*=.*$", f"bool const subgrid       = {'TRUE' if subgrid else 'FALSE'};"),
+        (r"^bool const equilibrium\s*=.*$", "bool const equilibrium   = TRUE;"),
+        (r"^bool const relaxed\s*=.*$", "bool const relaxed       = FALSE;"),
+        (r"^const char subgrid_dir\[\]\s*=.*$", 'const char subgrid_dir[]  = "./subgrid_files/";'),
         (r"^bool const multi_freq\s*=.*$", "bool const multi_freq = TRUE;"),
         (r"^bool const MP_GADGET_HEAT\s*=.*$", "bool const MP_GADGET_HEAT = FALSE;"),
         (r"^int const Ncpu\s*=.*$", f"int const Ncpu    = {ncpu};"),
@@ -134,7 +141,7 @@ def _configure(d: str, spec: W.BoxSpec, ncpu: int, path_length: int, restart: bo
     t = _sub_line(t, r"^short int const ray_per_cell_max\s*=.*$",
                   f"short int const ray_per_cell_max = {spec.ray_per_cell_max};")
     open(p, "w").write(t)
-    json.dump({"name": os.path.basename(d), "ncpu": ncpu, "path_length": path_length,
+    json.dump({"name": os.path.basename(d), "ncpu": ncpu, "path_length": path_length, "subgrid": subgrid,
                "spec": __import__("dataclasses").asdict(spec)},
               open(os.path.join(d, "stage.json"), "w"), indent=1)
 
@@ -159,12 +166,12 @@ def compile_stage(d: str, ncpu: Optional[int] = None) -> str:
 
 
 def build(name: str, spec: W.BoxSpec, ncpu: int = 1, path_length: int = 8, from_stage: bool = False,
-          restart: bool = False) -> str:
+          restart: bool = False, subgrid: bool = False) -> str:
     d = os.path.join(OUT, name)
     if not from_stage:
         if not os.path.isdir(REF_SRC):
             raise RuntimeError("reference checkout not available; use from_stage=True")
-        stage(name, spec, ncpu, path_length, restart)
+        stage(name, spec, ncpu, path_length, restart, subgrid)
         return compile_stage(d)
     return compile_stage(d, ncpu)
 

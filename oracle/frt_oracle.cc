@@ -62,6 +62,7 @@ static inline float absd(float x) { return (x >= 0.) ? x : -1. * x; }
 static inline int mins(short a, short b) { return (a >= b) ? b : a; }
 static inline int maxs(short a, short b) { return (b >= a) ? b : a; }
 static inline int imin(int a, int b) { return (a >= b) ? b : a; }
+static inline int imax(int a, int b) { return (a >= b) ? a : b; }
 static inline int imod(int a, int b) {
   while (a < 0) a += b;
   return a % b;
@@ -110,6 +111,36 @@ static double rcrB_He2(double T) { return O_KB * T * alphaB_He2(T); }
 static double free_free_rate(double T) { return 1.42e-27 * pow(T, 0.5) * 1.30; }
 static double compton_rate(double z) { return 5.6072e-36 * pow(1 + z, 4.); }
 static float hubble(float a) { return O_HH * 100. / O_MPC_TO_KM * pow(O_OMEGA_M / pow(a, 3.) + O_OMEGA_L, 0.5); }
+
+// sub-grid model rates (rates.cc:128-145, 240-254) and constants (global_variables.cc:241-304)
+static double alphaA_H2(double T) {
+  double x = lambda_x(T, 13.6);
+  return 1.269e-13 * pow(x, 1.503) / pow((1.0 + pow((x / 0.522), 0.470)), 1.923);
+}
+static double alphaA_He2(double T) {
+  double x = lambda_x(T, 2.459e+1);
+  return 3.0e-14 * pow(x, 0.654);
+}
+static double phothtHI(double alpha, double T, double ne) {
+  return 1.360e+1 / O_H_EV * O_H *
+         ((alpha + 2.8) / (1.8 + alpha) * (1. - pow(4., -1.8 - alpha)) / (1. - pow(4., -2.8 - alpha)) - 1.) *
+         alphaA_H2(T) * ne;
+}
+static double phothtHeI(double alpha, double T, double ne) {
+  return 2.459e+1 / O_H_EV * O_H *
+         ((alpha + 1.7) / (0.7 + alpha) * (1. - pow(2.2, -0.7 - alpha)) / (1. - pow(2.2, -1.7 - alpha)) - 1.) *
+         alphaA_He2(T) * ne;
+}
+static double photoheat_HIHeI(double alpha, double T, double ne, double nH, double nHe) {
+  return phothtHI(alpha, T, ne) * nH + phothtHeI(alpha, T, ne) * nHe;
+}
+static const float kSigmaEffRH = 2.517139346618065e-18;
+static const float kGammaMin = 1e-16;
+static const float kMaxSubgridFrac = 0.49;
+static const int kNt = 5000;
+static const int kNdlin = 500;
+// the parameter domain of the RadHydro runs (init_radhydro_data, subgrid.cc:114-128)
+static const float kGammaDom[5] = {3e-15f, 3e-14f, 3e-13f, 3e-12f, 3e-11f};
 
 // ---- state -----------------------------------------------------------------------------
 struct Ray {
@@ -168,6 +199,15 @@ struct Ctx {
   float avg_rho;
   std::vector<float> rho_prev, ddelta_dt;
   float step_dt;   // the time step the last step ran with (get_nphot_min_max at a switch uses it)
+  // sub-grid model (subgrid = TRUE, equilibrium = TRUE, ifront = FALSE): the RadHydro time and
+  // HI-fraction tables in the reference's memory layout (see orc_set_subgrid), the linear ->
+  // non-linear overdensity table, the cosmic times the model uses, the overdensity domain of the
+  // current step and the per-cell HI-fraction interpolants of the current step
+  bool subgrid = false;
+  std::vector<float> sg_time, sg_fh1, sg_t_dnl, sg_ds, sg_dnl;
+  float sg_tinit, sg_t12, sg_t8, sg_tcap, sg_tre_dom[3];
+  float sg_dnl_dom[3];
+  std::vector<float> sg_fh1_interp;
 };
 
 static inline long cidx(const Ctx& c, int i, int j, int k) { return ((long)i * c.N + j) * c.N + k; }
@@ -183,6 +223,153 @@ static float sum_nphot(const Ctx& c, const Ray& R) {
   float s = 0.;
   for (int nu = 0; nu < c.F; nu++) s += R.nphot[nu];
   return s;
+}
+
+// ---- sub-grid model (subgrid.cc), equilibrium = TRUE, ifront = FALSE ----------------------
+// interpolate (general_funcs.cc:275-315): linear interpolation with linear extrapolation
+static float sg_interpolate(const float* x, const float* y, float x0, int n) {
+  float y0 = 0.;
+  bool itp = false;
+  for (int i = 0; i < n - 1; i++) {
+    if (((x[i] <= x0) && (x[i + 1] >= x0)) || ((x[i] >= x0) && (x[i + 1] <= x0))) {
+      y0 = y[i] + (y[i + 1] - y[i]) / (x[i + 1] - x[i]) * (x0 - x[i]);
+      itp = true;
+      break;
+    }
+  }
+  if (!itp) {
+    if (x[0] < x[n - 1]) {
+      if (x0 > x[n - 1]) {
+        float slope = (y[n - 1] - y[n - 2]) / (x[n - 1] - x[n - 2]);
+        y0 = y[n - 1] + slope * (x0 - x[n - 1]);
+      } else {
+        float slope = (y[1] - y[0]) / (x[1] - x[0]);
+        y0 = y[0] + slope * (x0 - x[0]);
+      }
+    } else {
+      if (x0 < x[n - 1]) {
+        float slope = (y[n - 1] - y[n - 2]) / (x[n - 1] - x[n - 2]);
+        y0 = y[n - 1] + slope * (x0 - x[n - 1]);
+      } else {
+        float slope = (y[1] - y[0]) / (x[1] - x[0]);
+        y0 = y[0] + slope * (x0 - x[0]);
+      }
+    }
+  }
+  return y0;
+}
+
+// delta_dom_to_deltaNL_dom (subgrid.cc:97-132): the non-linear overdensities of the RadHydro
+// domain's linear ones (-sqrt(3), 0, sqrt(3)) at cosmic time `time`, the upper one capped at its
+// value at z = 5.5
+static void sg_delta_dom(Ctx& c, float time) {
+  const float delta_dom[3] = {(float)-pow(3., 0.5), 0.f, (float)pow(3., 0.5)};
+  c.sg_dnl_dom[1] = 0.;
+  const float tcap = c.sg_tcap;
+  int ti_m = 0, ti_p = 1, tcap_m = 0, tcap_p = 1;
+  const float* t = c.sg_t_dnl.data();
+  for (int i = 0; i < kNdlin - 1; i++) {
+    if ((t[i] <= time) && (t[i + 1] >= time)) {
+      ti_m = i;
+      ti_p = i + 1;
+    }
+    if ((t[i] <= tcap) && (t[i + 1] >= tcap)) {
+      tcap_m = i;
+      tcap_p = i + 1;
+    }
+  }
+  const float* ds = c.sg_ds.data();
+  auto row = [&](int i) { return c.sg_dnl.data() + (size_t)i * kNdlin; };
+  float d0m = sg_interpolate(ds, row(ti_m), delta_dom[0], kNdlin);
+  float d0p = sg_interpolate(ds, row(ti_p), delta_dom[0], kNdlin);
+  float d2m = sg_interpolate(ds, row(ti_m), delta_dom[2], kNdlin);
+  float d2p = sg_interpolate(ds, row(ti_p), delta_dom[2], kNdlin);
+  float capm = sg_interpolate(ds, row(tcap_m), delta_dom[2], kNdlin);
+  float capp = sg_interpolate(ds, row(tcap_p), delta_dom[2], kNdlin);
+  float cap = capm + (capp - capm) / (t[tcap_p] - t[tcap_m]) * (tcap - t[tcap_m]);
+  c.sg_dnl_dom[0] = d0m + (d0p - d0m) / (t[ti_p] - t[ti_m]) * (time - t[ti_m]);
+  c.sg_dnl_dom[2] = d2m + (d2p - d2m) / (t[ti_p] - t[ti_m]) * (time - t[ti_m]);
+  c.sg_dnl_dom[2] = mind(c.sg_dnl_dom[2], cap);
+}
+
+// deltaNL_to_deltasig (subgrid.cc:196-205): Mo & White (1996) linear overdensity over sigma
+static float sg_deltasig(float deltaNL, float redshift) {
+  float dcmode = 5.10655;
+  float sigma0 = dcmode / pow(3., 0.5);
+  float d_of_z = 1. / (1 + redshift) / 0.78205;
+  float delta = -1.35 * pow(1. + deltaNL, -2. / 3.) + 0.78785 * pow(1. + deltaNL, -0.58661) -
+                1.12431 * pow(1. + deltaNL, -0.5) + 1.68647;
+  return delta / d_of_z / sigma0;
+}
+
+// The reference's RadHydro arrays are [Nt][Nzre][Ndelta][Ngamma] with Ngamma = 3, filled and read
+// at the gamma index q + 1 (gam_offset, subgrid.cc:24-36; ind_gamma, subgrid.cc:329-331), so every
+// access runs one slot past its row into the next: the flat offset below is the reference's own
+// address arithmetic, and the arrays here carry one slot more for the last row's spill.
+static inline size_t sg_at(int t, int m, int p, int iq) { return (((size_t)t * 3 + m) * 3 + p) * 3 + iq; }
+
+// get_tradhydro_index (subgrid.cc:189-193)
+static int sg_tindex(const Ctx& c, float tsince) {
+  int i = (int)floor(tsince / c.sg_time[sg_at(kNt - 1, 0, 0, 0)] * (kNt - 1));
+  return imax(0, imin(i, kNt - 2));
+}
+
+// get_gamma_interp (subgrid.cc:257-486) for the HI fraction, the one interpolant the equilibrium
+// model reads (interp_nh1): tcross_flag stays FALSE without I-front tracking
+static void sg_gamma_interp(Ctx& c, long q, float tre, float deltaNL, float tsince) {
+  int ind_tre[2], ind_delta[2];
+  const int ind_gamma[3] = {1, 2, 3};
+  tre = maxd(c.sg_t12, tre);
+  if (tre > c.sg_t8) { ind_tre[1] = 2; ind_tre[0] = 1; }
+  else { ind_tre[1] = 1; ind_tre[0] = 0; }
+  if (sg_deltasig(deltaNL, c.zz) < 0.) { ind_delta[1] = 1; ind_delta[0] = 0; }
+  else { ind_delta[1] = 2; ind_delta[0] = 1; }
+  const int itf = sg_tindex(c, tsince);
+  float f[2][2][3];
+  const float* T = c.sg_time.data();
+  const float* H = c.sg_fh1.data();
+  for (int m = 0; m < 2; m++)
+    for (int p = 0; p < 2; p++)
+      for (int g = 0; g < 3; g++) {
+        const int im = ind_tre[m], ip = ind_delta[p], iq = ind_gamma[g];
+        float v = H[sg_at(itf, im, ip, iq)] + (H[sg_at(itf + 1, im, ip, iq)] - H[sg_at(itf, im, ip, iq)]) /
+                                                  (T[sg_at(itf + 1, im, ip, iq)] - T[sg_at(itf, im, ip, iq)]) *
+                                                  (tsince - T[sg_at(itf, im, ip, iq)]);
+        f[m][p][g] = mind(maxd(v, 0.), 1.);
+      }
+  // get_interpolate_gamma_f (subgrid.cc:211-250), fractype = TRUE
+  float out[5];
+  const float* tre_dom = c.sg_tre_dom;
+  for (int g = 0; g < 3; g++) {
+    float f_d0 = log10(f[0][0][g]) + (log10(f[1][0][g]) - log10(f[0][0][g])) *
+                                         (log10(tre + tsince) - log10(tre_dom[ind_tre[0]] + tsince)) /
+                                         (log10(tre_dom[ind_tre[1]] + tsince) - log10(tre_dom[ind_tre[0]] + tsince));
+    float f_d1 = log10(f[0][1][g]) + (log10(f[1][1][g]) - log10(f[0][1][g])) *
+                                         (log10(tre + tsince) - log10(tre_dom[ind_tre[0]] + tsince)) /
+                                         (log10(tre_dom[ind_tre[1]] + tsince) - log10(tre_dom[ind_tre[0]] + tsince));
+    float f_dg = f_d0 + (f_d1 - f_d0) * (log10(1. + deltaNL) - log10(1. + c.sg_dnl_dom[ind_delta[0]])) /
+                            (log10(1. + c.sg_dnl_dom[ind_delta[1]]) - log10(1. + c.sg_dnl_dom[ind_delta[0]]));
+    out[g + 1] = pow(10., f_dg);
+    out[g + 1] = mind(out[g + 1], kMaxSubgridFrac);
+  }
+  out[0] = pow(kGammaDom[0] / kGammaDom[1], 0.) * out[1];
+  out[4] = pow(kGammaDom[4] / kGammaDom[3], -1.) * out[3];
+  for (int g = 0; g < 5; g++) c.sg_fh1_interp[(size_t)q * 5 + g] = out[g];
+}
+
+// interp_nh1 (subgrid.cc:629-641), interp_nhe1 (644-647)
+static void sg_interp_nh1(Ctx& c, long q, float gammaH1) {
+  float gamma = maxd(gammaH1, kGammaMin);
+  int g = (int)floor(((float)3 + 2 - 1.) * (log10(gamma) - log10(kGammaDom[0])) /
+                     (log10(kGammaDom[3 + 2 - 1]) - log10(kGammaDom[0])));
+  g = imax(0, imin(g, 3 + 2 - 2));
+  const float* fh = &c.sg_fh1_interp[(size_t)q * 5];
+  c.nH1[q] = log10(fh[g]) + (log10(fh[g + 1]) - log10(fh[g])) / (log10(kGammaDom[g + 1]) - log10(kGammaDom[g])) *
+                                (log10(gamma) - log10(kGammaDom[g]));
+  c.nH1[q] = maxd(mind(pow(10., c.nH1[q]), c.fH1_0), 0.);
+  c.nH1[q] *= c.nH[q];
+  c.nHe1[q] = c.nH1[q] * c.nHe[q] / c.nH[q];
+  c.avg_nhe1[q] = c.nHe1[q];
 }
 
 static float rmin_from_l(const Ctx& c, short l) {
@@ -441,8 +628,18 @@ static void find_avg_unu(Ctx& c) {
         c.recomb_He2[q] = (float)alphaB_He2(maxd(kTempMin, c.temp[q]));
         c.recomb_He3[q] = (float)alphaB_He3(maxd(kTempMin, c.temp[q]));
         if ((c.temp[q] >= 3e4) && (c.temp[q] <= 1e6)) c.recomb_He2[q] += (float)Dalpha_He2(maxd(kTempMin, c.temp[q]));
-        c.dne_dt[q] = -c.ne[q];
-        c.mfp[q] = 1. / c.nH1[q] / c.sigH1[0];
+        if (!c.subgrid) {
+          c.dne_dt[q] = -c.ne[q];
+          c.mfp[q] = 1. / c.nH1[q] / c.sigH1[0];
+        } else {
+          // the gas is taken as fully ionised (ray_tracing.cc:679-682); ionised cells get their
+          // HI-fraction interpolants, the others the mfp of their neutral gas (687-693)
+          c.dne_dt[q] = -(c.nH[q] + c.nHe[q]);
+          if (c.treion_flag[q])
+            sg_gamma_interp(c, q, c.treion[q] + c.sg_tinit, c.rho[q] / c.avg_rho - 1., c.t - c.treion[q]);
+          else
+            c.mfp[q] = 1. / c.nH1[q] / c.sigH1[0];
+        }
       }
     }
     // ray pass
@@ -458,7 +655,45 @@ static void find_avg_unu(Ctx& c) {
       }
       short p = 0;
       unsigned dump_mask = 0;   // ledger: bins that a dump deposited
-      while (p < R.ray_end) {
+      if (c.subgrid) {
+        // sub-grid ray pass (ray_tracing.cc:701-938 with subgrid = TRUE, fion = 1): fixed H/He
+        // split, Gamma from the sub-grid effective cross section over the effective path, the
+        // segment's optical depth from the cell's mean free path after its deposit
+        const double frac_h1 = 1. - (O_Y / 4.) / (1. - O_Y + O_Y / 4.);
+        const double frac_he1 = (O_Y / 4.) / (1. - O_Y + O_Y / 4.);
+        const float fion = 1.f;
+        while (p < R.ray_end) {
+          const long q = R.pind[p];
+          const float dist = R.pdist[p];
+          double nphot_in[kMaxF];
+          double nphot_in_total = 0.;
+          for (int nu = 0; nu < F; nu++) {
+            nphot_in[nu] = nphot[nu] * exp(-tau_h1[nu] - tau_he1[nu]);
+            nphot_in_total += nphot_in[nu] / kPhotNorm;
+          }
+          const bool dump = nphot_in_total < c.nphot_min;
+          for (int nu = 0; nu < F; nu++) {
+            c.ngam_nu[q * F + nu] += (float)(nphot_in[nu] / kPhotNorm);
+            float delta_s_eff;
+            if (iter == 0) delta_s_eff = fion * dist / frac_h1;
+            else delta_s_eff = c.mfp[q] * (1. - exp(-fion * dist / c.mfp[q] / frac_h1));
+            c.avg_gamma_nu[q * F + nu] += (float)(frac_h1 * nphot_in[nu] * kSigmaEffRH * delta_s_eff / c.dt / vol / fion);
+            c.avg_gamma[q] += (float)(frac_h1 * nphot_in[nu] * kSigmaEffRH * delta_s_eff / c.dt / vol / fion);
+            c.avg_gamma_nu_he1[q * F + nu] += (float)(frac_he1 * nphot_in[nu] * kSigmaEffRH * delta_s_eff / c.dt / vol / fion);
+            c.avg_gamma_he1[q] += (float)(frac_he1 * nphot_in[nu] * kSigmaEffRH * delta_s_eff / c.dt / vol / fion);
+          }
+          p = dump ? 99 : p + 1;
+          for (int nu = 0; nu < F; nu++) {
+            dtau_h1[nu] = fion * dist / c.mfp[q];
+            dtau_he1[nu] = kNheToNh * dtau_h1[nu];
+            tau_h1[nu] += dtau_h1[nu];
+            tau_he1[nu] += dtau_he1[nu];
+            // ledger: the photons the segment takes out of the ray
+            if (iter == c.itercount - 1) c.led_deposited += nphot_in[nu] * (1. - exp(-(dtau_h1[nu] + dtau_he1[nu])));
+          }
+        }
+      }
+      while (!c.subgrid && p < R.ray_end) {
         const int ind = R.pind[p];
         const long q = ind;
         for (int nu = 0; nu < F; nu++) {
@@ -533,7 +768,53 @@ static void find_avg_unu(Ctx& c) {
       }
     }
     // cell pass B
-    for (long q = 0; q < n3; q++) {
+    for (long q = 0; q < n3 && c.subgrid; q++) {
+      // the sub-grid branch (ray_tracing.cc:956-1071, equilibrium = TRUE, ifront = FALSE) and the
+      // last-iteration bookkeeping (1138-1209)
+      double nelec = (double)(c.nH[q] - c.avg_nh1[q] + c.nHe[q] - c.avg_nhe1[q]);
+      const float fion = 1.f;
+      if ((iter == c.itercount - 1) && !c.treion_flag[q] && (c.avg_gamma[q] > 0.)) {
+        c.treion[q] = c.t - c.dt;
+        c.treion_flag[q] = 1;
+        sg_gamma_interp(c, q, c.treion[q] + c.sg_tinit, c.rho[q] / c.avg_rho - 1., c.t - c.treion[q]);
+      }
+      if (c.treion_flag[q] && fion > 0.) {
+        c.mfp[q] = maxd(kGammaMin, c.avg_gamma[q]) / c.clump[q] / kSigmaEffRH / alphaB_H2(maxd(kTempMin, c.temp[q])) /
+                   pow(c.nH[q], 2.) / 1.082;
+        c.mfp_912[q] = maxd(kGammaMin, c.avg_gamma[q]) / c.clump[q] / sig_H1(13.6 / O_H_EV) /
+                       alphaB_H2(maxd(kTempMin, c.temp[q])) / pow(c.nH[q], 2.) / 1.082;
+        c.mfp[q] = maxd(0.f, c.mfp[q]);   // mfp_min = 1e-2*dx[0] taken while dx is still 0 (global_variables.cc:301)
+        c.mfp_912[q] = maxd(0.f, c.mfp_912[q]);
+      }
+      if (iter != c.itercount - 1) continue;
+      if (c.treion_flag[q]) {
+        sg_interp_nh1(c, q, c.avg_gamma[q]);
+        c.nH2[q] = c.nH[q] * fion;
+        c.nHe2[q] = c.nHe[q] * fion;
+        c.nHe3[q] = 0.;
+      }
+      for (int nu = 0; nu < F; nu++)
+        c.u_nu[q * F + nu] = (float)(c.spectrum[nu] * c.avg_gamma[q] / c.sigH1[nu]) * O_H * (c.nu[nu]) / c.clight;
+      for (int nu = 0; nu < F; nu++) {
+        c.gamma_H1_nu[q * F + nu] = c.avg_gamma_nu[q * F + nu];
+        c.gamma_He1_nu[q * F + nu] = c.avg_gamma_nu_he1[q * F + nu];
+      }
+      c.gamma_H1_tot[q] = c.avg_gamma[q];
+      c.gamma_He1_tot[q] = c.avg_gamma_he1[q];
+      c.recrate_H2[q] = c.clump[q] * c.recomb_H2[q] * nelec * c.nH2[q];
+      c.recrate_He2[q] = c.clump[q] * c.recomb_He2[q] * nelec * c.nHe2[q];
+      c.ne[q] = c.nH2[q] + c.nHe2[q] + 2. * c.nHe3[q];
+      c.dne_dt[q] += c.nH[q] + c.nHe[q];
+      c.n_tot[q] = 2. * (c.nH[q] + c.nHe[q]);
+      c.dne_dt[q] /= c.dt;
+      c.nH1_prev[q] = c.nH1[q];
+      c.f_H2[q] = c.nH2[q] / c.nH[q];
+      c.f_He2[q] = c.nHe2[q] / c.nHe[q];
+      c.f_He3[q] = c.nHe3[q] / c.nHe[q];
+      c.f_H1[q] = c.nH1[q] / c.nH[q];
+      c.f_He1[q] = c.nHe1[q] / c.nHe[q];
+    }
+    for (long q = 0; q < n3 && !c.subgrid; q++) {
       double nelec = (double)(c.nH[q] - c.avg_nh1[q] + c.nHe[q] - c.avg_nhe1[q]);
       c.mfp[q] = 1. / c.sigH1[0] / c.avg_nh1[q];
       c.mfp_912[q] = 1. / sig_H1(13.6 / O_H_EV) / c.avg_nh1[q];
@@ -779,6 +1060,22 @@ static void update_heat_cool(Ctx& c, long q) {
   const int F = c.F;
   c.heat_rate[q] = 0;
   c.cool_rate[q] = 0;
+  if (c.subgrid) {
+    // the sub-grid model's terms (gas_funcs.cc:165-172, 192-200, 221-227, 236-238): analytic
+    // photo-heating above Gamma = 3e-14, the gas taken as fully ionised
+    const float tm = maxd(kTempMin, c.temp[q]);
+    if (c.gamma_H1_tot[q] > 3e-14)
+      c.heat_rate[q] = (float)photoheat_HIHeI(1.5, (double)tm, (double)(c.nH[q] + c.nHe[q]), (double)c.nH[q],
+                                              (double)c.nHe[q]);
+    else
+      c.heat_rate[q] = 0.;
+    c.cool_rate[q] += rcrB_H2(maxd(kTempMin, c.temp[q])) * (c.nH[q] + c.nHe[q]) * c.nH[q];
+    c.cool_rate[q] += rcrB_He2(maxd(kTempMin, c.temp[q])) * (c.nH[q] + c.nHe[q]) * c.nHe[q];
+    float nff = 1.f * (c.nH[q] + c.nHe[q]);   // fion (c.nH + c.nHe), fion = 1
+    c.cool_rate[q] += free_free_rate(maxd(kTempMin, c.temp[q])) * pow(nff, 2.);
+    c.cool_rate[q] -= compton_rate(c.zz) * (c.nH[q] + c.nHe[q]) * (2.726 * (1 + c.zz) - maxd(kTempMin, c.temp[q]));
+    return;
+  }
   if (c.f_H2[q] > 0.98) {
     for (int nu = 0; nu < F; nu++) {
       c.heat_rate[q] += c.avg_nh1[q] * c.gamma_H1_nu[q * F + nu] * O_H * (O_H_EV * c.nu[nu] - 13.6) / O_H_EV;
@@ -805,7 +1102,11 @@ static void update_thermal(Ctx& c) {
   const long n3 = (long)c.N * c.N * c.N;
   for (long q = 0; q < n3; q++) {
     float t_temp = 0.;
-    set_Treion_default(c, q);
+    if (c.subgrid && !c.treion_flag[q]) {   // neutral until ionised (gas_funcs.cc:380-382)
+      c.temp[q] = c.temp_0;
+      continue;
+    }
+    if (!c.subgrid) set_Treion_default(c, q);
     while (t_temp < c.dt) {
       float dt_temp = mind(get_thermal_tstep(c, q), c.dt - t_temp);
       update_heat_cool(c, q);
@@ -815,7 +1116,7 @@ static void update_thermal(Ctx& c) {
       t_temp += dt_temp;
     }
     c.temp[q] = maxd(c.temp[q], kTempMin);
-    c.nH1_prev[q] = c.nH1[q];
+    if (!c.subgrid) c.nH1_prev[q] = c.nH1[q];
   }
 }
 
@@ -983,6 +1284,7 @@ void orc_step(void* h) {
   c.clight = c.cl_factor * O_CL;
   c.nc = c.nl_const;
   c.t += c.dt;
+  if (c.subgrid) sg_delta_dom(c, maxd(c.sg_t12, c.t + c.sg_tinit));   // main.cc:126-128
   update_rays(c);
   c.last_crossings = 0;
   c.last_moved = 0;
@@ -1200,6 +1502,30 @@ extern "C" void orc_hydro_step(void* h, const float* delta1, int nsrc, const int
     c.nphot_min = 1e-10 * c.nphot_base_avg;
   }
   c.dt = c.tstep_factor * c.dxc / c.cl_factor / O_CL;   // update_dt (main.cc:237)
+}
+
+// The sub-grid model (subgrid = TRUE, equilibrium = TRUE, ifront = FALSE), set up after the cast
+// as main.cc:86-90 does: time_tab and fh1_tab are the reference's time_RH and fh1_RH arrays
+// ([Nt][3][3][3] floats, filled at the gamma index q + 1, Nt*27 + 1 floats with the last row's
+// spill; times in s), t_dnl / ds / dnl the linear -> non-linear overdensity table (500, 500,
+// 500 x 500 floats), consts = {tinit, cosmic_time(z=12), cosmic_time(z=8), cosmic_time(z=5.5),
+// tre_dom[0..2]} as the reference's cosmic_time gives them.
+extern "C" void orc_set_subgrid(void* h, const float* time_tab, const float* fh1_tab, const float* t_dnl, const float* ds,
+                                const float* dnl, const float* consts) {
+  Ctx& c = *(Ctx*)h;
+  const size_t nrh = (size_t)kNt * 27 + 1;
+  c.subgrid = true;
+  c.sg_time.assign(time_tab, time_tab + nrh);
+  c.sg_fh1.assign(fh1_tab, fh1_tab + nrh);
+  c.sg_t_dnl.assign(t_dnl, t_dnl + kNdlin);
+  c.sg_ds.assign(ds, ds + kNdlin);
+  c.sg_dnl.assign(dnl, dnl + (size_t)kNdlin * kNdlin);
+  c.sg_tinit = consts[0];
+  c.sg_t12 = consts[1];
+  c.sg_t8 = consts[2];
+  c.sg_tcap = consts[3];
+  for (int i = 0; i < 3; i++) c.sg_tre_dom[i] = consts[4 + i];
+  c.sg_fh1_interp.assign((size_t)c.N * c.N * c.N * 5, 0.f);
 }
 
 // ---- restart files in the reference's formats -------------------------------------------------

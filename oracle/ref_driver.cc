@@ -22,6 +22,10 @@
 //     hydro/ndot_catalog_01<n> and hydro/numhalos.01<n> under the stage directory (snapinit =
 //     10) and writes its outputs under hydro_out/; the scale factor, the snapshot interval and the
 //     redshift it uses are logged as 'HYDRO step a_rt dt_snap zz' (hex floats);
+//   * in a stage built with subgrid = TRUE the set-up imports the sub-grid tables after the cast
+//     (main.cc:86-90) and every step updates the non-linear overdensity domain after t += dt
+//     (main.cc:126-128); the cosmic times the model uses are logged once as 'SUBGRID tinit t12 t8
+//     tcap tre0 tre1 tre2' (hex floats);
 //   * in a stage built with input_grid = TRUE the set-up is the reference's restart path: the
 //     grid is sized as init() would (init_funcs.cc:22-30), the catalogue is read, init() reads the
 //     gas and treion restart files, init_rt() reads the ray file, and no rays are cast.
@@ -161,6 +165,13 @@ int main(int argc, char** argv) {
   set_ray_per_cell();
   set_lsource();
   if (input_grid == FALSE) new_rays();
+  if (subgrid == TRUE) {
+    calc_mfp_boost();
+    import_delta_over_sigma_table();
+    init_radhydro_data();
+    printf("SUBGRID %a %a %a %a %a %a %a\n", tinit, cosmic_time(1. / (1. + 12)), cosmic_time(1. / (1. + 8.)),
+           cosmic_time(1. / (1. + 5.5)), tre_dom[0], tre_dom[1], tre_dom[2]);
+  }
   if (have_clump) memcpy(&clump[0][0][0], &clump_in[0][0][0], sizeof(clump));
   get_nphot_min_max();
   const double t_setup = omp_get_wtime() - t_setup0;
@@ -176,6 +187,7 @@ int main(int argc, char** argv) {
     if (have_clump) memcpy(&clump[0][0][0], &clump_in[0][0][0], sizeof(clump));
     set_clight();
     t += dt;
+    if (subgrid == TRUE) delta_dom_to_deltaNL_dom(maxd(cosmic_time(1. / (1. + 12)), t + tinit));
     update_rays();
     long crossings = 0, moved = 0;
 #pragma omp parallel for reduction(+ : crossings, moved)

@@ -22,6 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
+sys.path.insert(0, HERE)
 
 from oracle import build_ref as B, frtd  # noqa: E402
 from flexrt_imaging_reion_b200 import workloads as W  # noqa: E402
@@ -170,6 +171,35 @@ def make_hydro(name="T16H", base=("T16", W.config_tiny(), 11), steps=6):
                         hydro=np.array(hy, np.float64), **out)
 
 
+def make_subgrid(name="T16G", base=("T16", W.config_tiny(steps=6), 11), steps=6):
+    """A run of the reference's sub-grid model (subgrid = TRUE, equilibrium = TRUE, ifront = FALSE)
+    on synthetic tables in its own file formats (tests/golden/subgrid_tables.py): its states, the
+    cosmic times the model used (logged by the reference) and the span of the overdensity table,
+    so that the tables can be rebuilt without the reference's cosmology table."""
+    import subgrid_tables as ST
+    _, spec, seed = base
+    B.build(name, spec, ncpu=1, subgrid=True)
+    d = os.path.join(B.OUT, name)
+    ct = ST.cosmic_time_from_table(os.path.join(d, "input_files", "cosmo_table"))
+    t0, t1 = ST.table_span(ct)
+    ST.write_reference_files(os.path.join(d, "subgrid_files"), ct)
+    inp = W.make_inputs(spec)
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        log = B.run(name, inp, td, steps, seed, dump_every=1)
+        consts = None
+        for line in log.splitlines():
+            if line.startswith("SUBGRID"):
+                consts = [float.fromhex(x) for x in line.split()[1:]]
+        assert consts is not None and len(consts) == 7, log[-2000:]
+        for s in range(1, steps + 1):
+            dd = frtd.read(os.path.join(td, f"dump_{s:04d}.frtd"))
+            for k in FIELDS + RAYS + ["scalars", "mfp", "f_H2"]:
+                out[f"s{s}_{k}"] = dd[k]
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), seed=seed, steps=np.arange(1, steps + 1),
+                        consts=np.array(consts, np.float32), span=np.array([t0, t1], np.float64), **out)
+
+
 if __name__ == "__main__":
     only = sys.argv[1:]
     for case in CASES:
@@ -185,3 +215,6 @@ if __name__ == "__main__":
     if not only or "T16H" in only:
         make_hydro()
         print("wrote T16H")
+    if not only or "T16G" in only:
+        make_subgrid()
+        print("wrote T16G")

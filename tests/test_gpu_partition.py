@@ -57,3 +57,27 @@ def test_phases_refused_when_merging_is_reachable():
     with pytest.raises(rt.FrtError, match="status 1"):
         P.step_shares([ctx], P.LocalCombiner([ctx]))
     ctx.close()
+
+
+def test_one_share_async_phases_match_oracle():
+    """The phased step with one share and phases that only enqueue (frt_set_phase_async: no host
+    synchronisation between phases, the one-GPU run of bench.py --mode partition) against the
+    oracle."""
+    spec, seed, cap = W.config_S(), 21, 1 << 20
+    spec = W.BoxSpec(**{**spec.__dict__, "steps": 4})
+    inp = W.make_inputs(spec)
+    ref = PT.oracle_states(inp, seed, spec.steps)
+    # a ray capacity below S's merge threshold (2.6e6 rays): the phased step needs it
+    ctx = P.make_share(inp, seed, 0, 1, ray_capacity=cap)
+    ctx.set_phase_async(True)
+    assert ctx.phase_stream() != 0
+    comb = P.LocalCombiner([ctx])
+    states, stats = [PT.device_state(ctx, 0, False)], []
+    for s in range(spec.steps):
+        tot = P.step_shares([ctx], comb)[0]
+        assert tot["error_flags"] == 0, tot
+        assert tot["crossings"] == int(ref[s + 1]["scalars"][10])
+        stats.append(tot)
+        states.append(PT.device_state(ctx, 0, False))
+    ctx.close()
+    check(states, ref, False, stats=stats)
