@@ -35,7 +35,7 @@ EXPORTS = ["frt_create", "frt_destroy", "frt_last_error", "frt_rotation_table", 
            "frt_read_treion", "frt_read_rays", "frt_update_cosmo_expansion",
            "frt_set_cast_per_source", "frt_last_kernel_timing", "frt_set_source_owner", "frt_step_phase",
            "frt_phase_buffers", "frt_autotune", "frt_get_tuning", "frt_set_tuning", "frt_update_hydro_step", "frt_set_phase_async",
-           "frt_phase_stream"]
+           "frt_phase_stream", "frt_set_subgrid"]
 PHASE_WALK, PHASE_CELLS, PHASE_RAYPASS, PHASE_CELLPASS, PHASE_END = 0, 1, 2, 3, 4
 NOALLOC_MAX_CELLS = 1 << 20
 
@@ -68,6 +68,12 @@ class Tuning(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class SubgridTables(C.Structure):
+    _fields_ = [("time_RH", C.c_void_p), ("fh1_RH", C.c_void_p), ("t_deltaNL", C.c_void_p),
+                ("delta_over_sigma", C.c_void_p), ("deltaNL", C.c_void_p), ("tinit", C.c_float),
+                ("t_z12", C.c_float), ("t_z8", C.c_float), ("t_z55", C.c_float), ("tre_dom", C.c_float * 3)]
 
 
 class StepStats(C.Structure):
@@ -145,6 +151,7 @@ def lib() -> C.CDLL:
         "frt_autotune": ([P, I, C.POINTER(Tuning)], I),
         "frt_update_hydro_step": ([P, I, P, C.c_float, C.c_float, C.c_float, I, P, P], I),
         "frt_set_phase_async": ([P, I], I),
+        "frt_set_subgrid": ([P, C.POINTER(SubgridTables)], I),
         "frt_phase_stream": ([P, C.POINTER(P)], I),
         "frt_get_tuning": ([P, C.POINTER(Tuning)], I),
         "frt_set_tuning": ([P, C.POINTER(Tuning)], I),

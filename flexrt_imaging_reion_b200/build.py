@@ -26,6 +26,7 @@ SOURCES = [
     ("frt_geom.cu", ["-fmad=false"]),
     ("frt_phys.cu", []),
     ("frt_adjoint.cu", ["-fmad=false"]),
+    ("frt_subgrid.cu", ["-fmad=false"]),
     ("frt_ctx.cu", []),
 ]
 HEADERS = ["frt_internal.cuh", "frt_physics.cuh", "frt_params.h", "hp_nest.h", "frt_hostmath.h", "frt_dda.cuh", "frt_tune.h",

@@ -182,6 +182,7 @@ void enqueue_begin_advance(frt_ctx* ctx) {
   const Dev& d = ctx->d;
   launch_clear_lit(d, ctx->grid_lit, ctx->s_main);
   launch_step_begin(d, ctx->s_main);
+  if (d.subgrid) launch_sg_step(d, ctx->s_main);
   launch_advance(d, ctx->nsm * ctx->tune.adv_grid, ctx->s_main, ctx->tune.adv_block, ctx->grid_rays);
 }
 
@@ -192,6 +193,17 @@ void record(cudaEvent_t e, cudaStream_t s, bool in_graph) {
 
 void enqueue_iterations(frt_ctx* ctx, bool fused_thermal, bool in_graph = false) {
   const Dev& d = ctx->d;
+  if (d.subgrid) {   // the sub-grid model's passes (frt_subgrid.cu)
+    launch_sg_lit_init(d, ctx->grid_lit, ctx->s_main);
+    for (int it = 0; it < d.itercount; it++) {
+      const bool timed = it < frt_ctx::kMaxTimedIter;
+      if (timed) record(ctx->ev_r[2 * it], ctx->s_main, in_graph);
+      launch_sg_raypass(d, it, ctx->grid_rays, ctx->s_main);
+      if (timed) record(ctx->ev_r[2 * it + 1], ctx->s_main, in_graph);
+      launch_sg_litpass(d, it, fused_thermal, ctx->nsm * ctx->tune.lit_grid, ctx->s_main);
+    }
+    return;
+  }
   launch_lit_init(d, ctx->strict, ctx->grid_lit, ctx->s_main);
   for (int it = 0; it < d.itercount; it++) {
     const bool timed = it < frt_ctx::kMaxTimedIter;
@@ -215,7 +227,8 @@ void enqueue_step(frt_ctx* ctx, bool in_graph) {
   cudaStreamWaitEvent(ctx->s_dark, ctx->ev_fork, 0);
   if (in_graph) cudaEventRecordWithFlags(ctx->ev_d0, ctx->s_dark, cudaEventRecordExternal);
   else cudaEventRecord(ctx->ev_d0, ctx->s_dark);
-  launch_dark(d, ctx->strict, true, ctx->grid_dark, ctx->s_dark);
+  if (d.subgrid) launch_sg_dark(d, true, ctx->grid_dark, ctx->s_dark);
+  else launch_dark(d, ctx->strict, true, ctx->grid_dark, ctx->s_dark);
   if (in_graph) cudaEventRecordWithFlags(ctx->ev_d1, ctx->s_dark, cudaEventRecordExternal);
   else cudaEventRecord(ctx->ev_d1, ctx->s_dark);
   cudaEventRecord(ctx->ev_join, ctx->s_dark);
@@ -928,6 +941,53 @@ frt_status frt_update_hydro_step(frt_ctx* ctx, int box, const float* delta1, flo
   return upload_boxes(ctx);
 }
 
+frt_status frt_set_subgrid(frt_ctx* ctx, const frt_subgrid_tables* t) {
+  if (!ctx || !t || !t->time_RH || !t->fh1_RH || !t->t_deltaNL || !t->delta_over_sigma || !t->deltaNL)
+    return FRT_ERR_INVALID;
+  for (size_t b = 0; b < ctx->boxes.size(); b++)
+    if (!ctx->gas_ready[b]) {
+      ctx->err = "frt_set_subgrid: set up the gas of every box first (the model reads the densities)";
+      return FRT_ERR_STATE;
+    }
+  Dev& d = ctx->d;
+  CK(cudaStreamSynchronize(ctx->s_main));
+  CK(cudaStreamSynchronize(ctx->s_dark));
+  const size_t nrh = (size_t)FRT_SUBGRID_NT * 27 + 1, nd = FRT_SUBGRID_NDLIN;
+  auto copy = [&](const float* src, size_t n, const float** dst) -> frt_status {
+    float* p = nullptr;
+    frt_status st = dalloc(ctx, &p, n);
+    if (st) return st;
+    CK(cudaMemcpy(p, src, sizeof(float) * n, cudaMemcpyHostToDevice));
+    *dst = p;
+    return FRT_OK;
+  };
+  frt_status st;
+  if ((st = copy(t->time_RH, nrh, &d.sg_time)) || (st = copy(t->fh1_RH, nrh, &d.sg_fh1)) ||
+      (st = copy(t->t_deltaNL, nd, &d.sg_tdnl)) || (st = copy(t->delta_over_sigma, nd, &d.sg_ds)) ||
+      (st = copy(t->deltaNL, nd * nd, &d.sg_dnl)))
+    return st;
+  d.sg_tinit = t->tinit;
+  d.sg_t12 = t->t_z12;
+  d.sg_t8 = t->t_z8;
+  d.sg_tcap = t->t_z55;
+  for (int k = 0; k < 3; k++) d.sg_tre_dom[k] = t->tre_dom[k];
+  d.sg_fH1_0 = ctx->cfg.fH1_0;
+  d.sg_temp0 = ctx->cfg.temp_0;
+  if (!d.mfp && (st = dalloc(ctx, &d.mfp, (size_t)d.ncell_total))) return st;
+  if (!d.l_mfp && (st = dalloc(ctx, &d.l_mfp, (size_t)d.lit_cap))) return st;
+  if (!d.rho) {   // the model reads rho / <rho> of every ionised cell
+    if ((st = dalloc(ctx, &d.rho, (size_t)d.ncell_total))) return st;
+    for (size_t b = 0; b < ctx->hbox.size(); b++)
+      if (ctx->rho[b].size() == (size_t)ctx->hbox[b].ncell)
+        CK(cudaMemcpy(d.rho + ctx->hbox[b].cell0, ctx->rho[b].data(), sizeof(float) * ctx->rho[b].size(),
+                      cudaMemcpyHostToDevice));
+  }
+  d.subgrid = 1;
+  launch_sg_mfp_init(d, ctx->s_main);
+  ctx->graph_valid = false;
+  return sync_and_check(ctx);
+}
+
 frt_status frt_update_dt(frt_ctx* ctx, float* dt_out) {
   if (!ctx) return FRT_ERR_INVALID;
   if (dt_out)
@@ -972,7 +1032,8 @@ frt_status frt_update_rays(frt_ctx* ctx) {
 frt_status frt_find_avg_unu(frt_ctx* ctx) {
   if (!ctx) return FRT_ERR_INVALID;
   enqueue_iterations(ctx, false);
-  launch_dark(ctx->d, ctx->strict, false, ctx->grid_cells, ctx->s_main);
+  if (ctx->d.subgrid) launch_sg_dark(ctx->d, false, ctx->grid_cells, ctx->s_main);
+  else launch_dark(ctx->d, ctx->strict, false, ctx->grid_cells, ctx->s_main);
   return sync_and_check(ctx);
 }
 
@@ -1011,7 +1072,8 @@ frt_status frt_split_rays(frt_ctx* ctx) {
 
 frt_status frt_update_thermal(frt_ctx* ctx) {
   if (!ctx) return FRT_ERR_INVALID;
-  launch_thermal_all(ctx->d, ctx->strict, ctx->grid_cells, ctx->s_main);
+  if (ctx->d.subgrid) launch_sg_thermal_all(ctx->d, ctx->grid_cells, ctx->s_main);
+  else launch_thermal_all(ctx->d, ctx->strict, ctx->grid_cells, ctx->s_main);
   return sync_and_check(ctx);
 }
 
@@ -1263,9 +1325,9 @@ frt_status frt_step_phase(frt_ctx* ctx, int phase, int iter, const uint16_t* ith
                           const uint16_t* itheta_per_source, frt_step_stats* stats) {
   if (!ctx) return FRT_ERR_INVALID;
   Dev& d = ctx->d;
-  if (d.per_bin || d.bin_base) {
-    ctx->err = "frt_step_phase: needs core outputs, mixed precision and a box whose ray count cannot reach the "
-               "merge threshold (the per-bin rates and the merge are not combined across contexts)";
+  if (d.per_bin || d.bin_base || d.subgrid) {
+    ctx->err = "frt_step_phase: needs core outputs, mixed precision, the plain model and a box whose ray count "
+               "cannot reach the merge threshold (the per-bin rates and the merge are not combined across contexts)";
     return FRT_ERR_INVALID;
   }
   cudaStream_t s = ctx->s_main;
@@ -1696,6 +1758,10 @@ frt_status frt_adjoint(frt_ctx* ctx, const frt_adj_objective* obj, double* J, do
       ctx->err = "frt_adjoint: objective sub-box outside the box";
       return FRT_ERR_INVALID;
     }
+  if (ctx->d.subgrid) {
+    ctx->err = "frt_adjoint differentiates the plain C2Ray model, not the sub-grid model";
+    return FRT_ERR_STATE;
+  }
   if (ctx->merged_any || ctx->restarted[obj->box]) {
     ctx->err = "frt_adjoint needs every ray to come from one source's cast: a merge has combined rays of "
                "several sources, or the rays were read from a restart file";
@@ -1915,6 +1981,10 @@ frt_status frt_set_tuning(frt_ctx* ctx, const frt_tuning* in) {
 frt_status frt_autotune(frt_ctx* ctx, int steps, frt_tuning* out) {
   if (!ctx || steps < 1 || steps > 16) return FRT_ERR_INVALID;
   Dev& d = ctx->d;
+  if (d.subgrid) {
+    ctx->err = "frt_autotune times the plain model's kernels";
+    return FRT_ERR_INVALID;
+  }
   const int I = d.itercount;
   cudaStream_t s = ctx->s_main;
   const Tune t0 = ctx->tune;

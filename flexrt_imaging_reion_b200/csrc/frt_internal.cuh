@@ -117,6 +117,14 @@ struct Dev {
   // control
   Ctl* ctl;
   int* rp_queue;           // [kMaxIterQueue] ray-pass work counters, one per C2Ray iteration (chunked queue)
+  // sub-grid model (frt_set_subgrid; frt_subgrid.cu): the RadHydro time and HI-fraction tables in
+  // the reference's layout, the linear -> non-linear overdensity table, the cosmic times the model
+  // uses, and the cells' mean free paths (per cell, and per lit cell during the iteration)
+  int subgrid;
+  const float *sg_time, *sg_fh1, *sg_tdnl, *sg_ds, *sg_dnl;
+  float sg_tinit, sg_t12, sg_t8, sg_tcap, sg_tre_dom[3];
+  float sg_fH1_0, sg_temp0;   // the HI-fraction cap of interp_nh1 and the neutral gas temperature
+  float* l_mfp;
 };
 
 constexpr int kMaxIterQueue = 16;
@@ -196,6 +204,14 @@ void launch_dark(const Dev& d, bool strict, bool fused_thermal, int grid, cudaSt
 void launch_thermal_all(const Dev& d, bool strict, int grid, cudaStream_t s);
 void launch_clear_lit(const Dev& d, int grid, cudaStream_t s);
 void launch_gather_sparse(const Dev& d, long long cell0, long long ncell, int which, float* out, cudaStream_t s);
+// ---- sub-grid model (frt_subgrid.cu) ---------------------------------------------------
+void launch_sg_step(const Dev& d, cudaStream_t s);                         // the step's overdensity domain
+void launch_sg_mfp_init(const Dev& d, cudaStream_t s);                     // init()'s mean free paths
+void launch_sg_lit_init(const Dev& d, int grid, cudaStream_t s);
+void launch_sg_raypass(const Dev& d, int iter, int grid, cudaStream_t s);
+void launch_sg_litpass(const Dev& d, int iter, bool fused_thermal, int grid, cudaStream_t s);
+void launch_sg_dark(const Dev& d, bool fused_thermal, int grid, cudaStream_t s);
+void launch_sg_thermal_all(const Dev& d, int grid, cudaStream_t s);
 // ---- adjoint (frt_adjoint.cu) --------------------------------------------------------
 void launch_adjoint(const Dev& d, const AdjDev& a, int grid, cudaStream_t s);
 void launch_adjoint_gather(const Dev& d, const AdjDev& a, long long cell0, long long ncell, float* out,

@@ -53,6 +53,7 @@ struct BoxP {
   ThermConst th;
   float rmax[kLtab], rmin[kLtab];
   float avg_rho;             // volume-averaged proper density (calc_vol_avg, data_funcs.cc:75-92)
+  float sg_dnl_dom[3];       // sub-grid model: the non-linear overdensities of the RadHydro domain this step
 };
 
 }  // namespace frt

@@ -238,6 +238,20 @@ class RTContext:
         self._check(self.L.frt_update_cosmo_expansion(self.h, ac.ctypes.data, ap.ctypes.data),
                     "frt_update_cosmo_expansion")
 
+    def set_subgrid(self, tables, consts) -> None:
+        """frt_set_subgrid: the sub-grid RadHydro model from here on. `tables` holds the reference's
+        in-memory arrays ("time", "fh1": Nt*27+1 floats; "t_dnl", "ds": 500; "dnl": 500*500),
+        `consts` the cosmic times (tinit, t(z=12), t(z=8), t(z=5.5), tre_dom[0..2])."""
+        keep = {k: np.ascontiguousarray(tables[k], np.float32) for k in ("time", "fh1", "t_dnl", "ds", "dnl")}
+        t = _abi.SubgridTables()
+        t.time_RH, t.fh1_RH = keep["time"].ctypes.data, keep["fh1"].ctypes.data
+        t.t_deltaNL, t.delta_over_sigma, t.deltaNL = keep["t_dnl"].ctypes.data, keep["ds"].ctypes.data, keep["dnl"].ctypes.data
+        c = [float(x) for x in consts]
+        t.tinit, t.t_z12, t.t_z8, t.t_z55 = c[0], c[1], c[2], c[3]
+        for k in range(3):
+            t.tre_dom[k] = c[4 + k]
+        self._check(self.L.frt_set_subgrid(self.h, C.byref(t)), "frt_set_subgrid")
+
     def hydro_step(self, box: int, snap: W.BoxInputs, a_rt: float, dt_snap: float, zz: float) -> None:
         """update_hydro_step of one box to the snapshot `snap` (its density cube and sources), with
         get_nphot_min_max; call after new_rays and the expansion, as main.cc:219-222 does."""

@@ -157,6 +157,31 @@ frt_status frt_update_cosmo_expansion(frt_ctx* ctx, const float* a_current, cons
  * list replaces the old one (an owner mask, frt_set_source_owner, is cleared). */
 frt_status frt_update_hydro_step(frt_ctx* ctx, int box, const float* delta1, float a_rt, float dt_snap, float zz,
                                  int nsrc, const int32_t* ijk, const double* lum);
+/* The sub-grid RadHydro model of the reference (subgrid = TRUE with equilibrium = TRUE and
+ * ifront = FALSE, user_inputs.h:11-15): photo-ionisation equilibrium mean free paths in ionised
+ * cells, HI fractions interpolated in the RadHydro tables (get_gamma_interp / interp_nh1,
+ * subgrid.cc:257-647), the sub-grid ray deposition (ray_tracing.cc:764-856) and heating / cooling
+ * (gas_funcs.cc:134-242, 362-418). Call after the gas set-up and the set-up cast, as main.cc:86-90
+ * imports the tables; every later step runs the sub-grid model. The tables are the reference's
+ * arrays after import_subgrid_file / import_delta_over_sigma_table (subgrid.cc:20-95): time_RH and
+ * fh1_RH in its [Nt][3][3][3] layout, filled at the gamma index q + 1 (Nt * 27 + 1 floats with the
+ * last row's spill), times in s; the cosmic times are the reference's cosmic_time() at zinit,
+ * z = 12, 8, 5.5 and at the three RadHydro reionisation redshifts. Without I-front tracking the
+ * result of a ray pass does not depend on the order of the rays (no per-cell photon budget, the
+ * neutral-absorption block ray_tracing.cc:867-919 never runs). The phased step, the autotuner and
+ * the adjoint stay with the plain model (FRT_ERR_INVALID / FRT_ERR_STATE). */
+#define FRT_SUBGRID_NT 5000
+#define FRT_SUBGRID_NDLIN 500
+typedef struct {
+  const float* time_RH;            /* FRT_SUBGRID_NT * 27 + 1 */
+  const float* fh1_RH;             /* FRT_SUBGRID_NT * 27 + 1 */
+  const float* t_deltaNL;          /* FRT_SUBGRID_NDLIN cosmic times, s */
+  const float* delta_over_sigma;   /* FRT_SUBGRID_NDLIN */
+  const float* deltaNL;            /* FRT_SUBGRID_NDLIN x FRT_SUBGRID_NDLIN, one row per time */
+  float tinit, t_z12, t_z8, t_z55; /* cosmic_time at zinit, z = 12, 8, 5.5 */
+  float tre_dom[3];                /* cosmic_time at z = 12, 8, 6 (init_radhydro_data, subgrid.cc:176-178) */
+} frt_subgrid_tables;
+frt_status frt_set_subgrid(frt_ctx* ctx, const frt_subgrid_tables* tables);
 /* get_nphot_min_max (ray_tracing.cc:129-154) */
 frt_status frt_get_nphot_min_max(frt_ctx* ctx, double* nmin_out, double* nmax_out);
 /* set_clump + set_clight (subgrid.cc:799-811, rt_funcs.cc:129-143) */
