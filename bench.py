@@ -55,6 +55,11 @@ RAYPASS_BYTES_PER_CROSSING = 8 + 8 + 68
 # warm-up steps that frt_autotune takes (the last ones of the warm-up)
 AUTOTUNE_STEPS = 3
 RAYPASS_TRAFFIC_BYTES_PER_CROSSING = 38.9
+# Walk (k_advance): per live ray its record read (cell, geometry, order/pixel/itheta, time: 44 B)
+# and written back (30 B); per crossing its segment {cell, dist} written (8 B) and the cell's
+# lit mark (1 B).
+WALK_BYTES_PER_RAY = 44 + 30
+WALK_BYTES_PER_CROSSING = 8 + 1
 
 
 def _peaks():
@@ -183,6 +188,19 @@ def run_reference(spec, name: str, steps: int, threads: int, time_cap_s: float, 
     return rows, setup
 
 
+def _step_phases(line: str) -> dict:
+    """The key=value fields of one STEP line of the reference driver (step wall time and its parts:
+    adv, iter, merge, split, thermal, cast, in s; rays_before, crossings, moved)."""
+    out = {}
+    for tok in line.split()[2:]:
+        k, _, v = tok.partition("=")
+        try:
+            out[k] = float(v)
+        except ValueError:
+            pass
+    return out
+
+
 def run_reference_restart(spec, name: str, files, steps: int, threads: int, seed: int):
     """The compiled reference started through its own restart path (input_grid = TRUE: init()
     reads the gas and treion records, init_rt() the ray records, rt_funcs.cc:95-124) from
@@ -211,7 +229,7 @@ def run_reference_restart(spec, name: str, files, steps: int, threads: int, seed
                 setup = float(line.split()[1])
             m = re.match(r"STEP (\d+) rays_before=\d+ crossings=(\d+) moved=\d+ wall=([0-9.eE+-]+)", line)
             if m:
-                rows.append((int(m.group(2)), float(m.group(3))))
+                rows.append((int(m.group(2)), float(m.group(3)), _step_phases(line)))
         return rows, setup
     finally:
         for pth in paths:
@@ -492,6 +510,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     lit = 0
     alive = moved = 0
     per_step = launches_per_step(spec, args.ray_capacity, itercount)
+    walk_ms, walked = 0.0, 0
+    prev_alive = ctx.num_rays()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         st = ctx.step(graph=not args.plain)
@@ -500,6 +520,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dev_ms += ms
         dark_ms += dms
         rp_ms += ctx.last_raypass_ms()
+        walk_ms += ctx.last_walk_ms()
+        walked += prev_alive
+        prev_alive = st["rays_alive"]
         launches += per_step
         lit += st["lit_cells"]
         alive += st["rays_alive"]
@@ -560,6 +583,17 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                       "traffic_per_step": DARK_TRAFFIC_BYTES_PER_CELL * (ncell - lit / args.steps),
                       "note": "CUDA-event span on its own stream, overlapped with the higher-priority "
                               "lit-cell chain; not its busy time"},
+        # the walk: every live ray advanced, its segments and lit-cell marks written
+        "walk": {"kernel": "k_advance (update_rays: every live ray walked one step)",
+                 "launch_ms": walk_ms / args.steps,
+                 "algorithmic_bytes_per_launch": (WALK_BYTES_PER_RAY * walked + WALK_BYTES_PER_CROSSING * cross) / args.steps,
+                 "achieved": ((WALK_BYTES_PER_RAY * walked + WALK_BYTES_PER_CROSSING * cross) / (walk_ms * 1e-3) / 1e9
+                              if walk_ms > 0 else None),
+                 "unit": "GB/s", "peak": peak,
+                 "frac": ((WALK_BYTES_PER_RAY * walked + WALK_BYTES_PER_CROSSING * cross) / (walk_ms * 1e-3) / 1e9 / peak
+                          if walk_ms > 0 and peak else None),
+                 "rays_per_launch": walked / args.steps,
+                 "bytes_per_ray": WALK_BYTES_PER_RAY, "bytes_per_crossing": WALK_BYTES_PER_CROSSING},
         "gpu_launches": launches,
         "clocks": clk,
         "crossings_per_step": cross / args.steps,
@@ -589,7 +623,7 @@ def main():
     ap.add_argument("--lit-capacity", type=int, default=0, help="0 = all cells")
     ap.add_argument("--plain", action="store_true", help="launch kernels directly instead of the CUDA graph")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
-    ap.add_argument("--cpu-baseline-steps", type=int, default=2)
+    ap.add_argument("--cpu-baseline-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # the reference arm times the same step window as this arm (about 8-10 s per L step on 16 cores)
     ap.add_argument("--ref-time-cap", type=float, default=900.0)
@@ -696,10 +730,12 @@ def main():
                       f"excluded; the restart sample was unavailable: {e}), reference OpenMP code compiled "
                       f"from its sources, {threads} threads")
         try:
-            cr = sum(c for c, _ in rows)
-            wt = sum(w for _, w in rows)
+            cr = sum(r[0] for r in rows)
+            wt = sum(r[1] for r in rows)
             res["cpu_baseline"] = {"value": cr / wt if wt else None, "unit": "crossings/s", "cores": threads,
                                    "kind": "reference", "sample": sample}
+            if rows and len(rows[0]) > 2:
+                res["cpu_baseline"]["per_step"] = [r[2] for r in rows]
         except Exception as e:
             res["cpu_baseline"] = {"value": None, "unit": "crossings/s", "cores": threads, "kind": "reference",
                                    "sample": f"unavailable: {e}"}

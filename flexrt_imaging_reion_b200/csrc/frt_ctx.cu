@@ -25,9 +25,10 @@ struct frt_ctx {
   std::vector<void*> allocs;
   cudaStream_t s_main = nullptr, s_dark = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_t0 = nullptr, ev_t1 = nullptr, ev_d0 = nullptr, ev_d1 = nullptr;
+  cudaEvent_t ev_a0 = nullptr, ev_a1 = nullptr;   // around the walk (k_advance)
   static constexpr int kMaxTimedIter = 16;
   cudaEvent_t ev_r[2 * kMaxTimedIter] = {};   // around each ray pass of the step
-  float last_raypass_ms = 0.f;
+  float last_raypass_ms = 0.f, last_walk_ms = 0.f;
   // sources per box (host copy)
   std::vector<std::vector<int>> src_cell;
   std::vector<std::vector<double>> src_lum;
@@ -177,18 +178,20 @@ void note_step(frt_ctx* ctx) {
   std::fill(ctx->frac_kept.begin(), ctx->frac_kept.end(), 0);
 }
 
-void enqueue_begin_advance(frt_ctx* ctx) {
+void record(cudaEvent_t e, cudaStream_t s, bool in_graph) {
+  if (in_graph) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+  else cudaEventRecord(e, s);
+}
+
+void enqueue_begin_advance(frt_ctx* ctx, bool in_graph = false) {
   ctx->rays_moved = true;
   const Dev& d = ctx->d;
   launch_clear_lit(d, ctx->grid_lit, ctx->s_main);
   launch_step_begin(d, ctx->s_main);
   if (d.subgrid) launch_sg_step(d, ctx->s_main);
+  record(ctx->ev_a0, ctx->s_main, in_graph);
   launch_advance(d, ctx->nsm * ctx->tune.adv_grid, ctx->s_main, ctx->tune.adv_block, ctx->grid_rays);
-}
-
-void record(cudaEvent_t e, cudaStream_t s, bool in_graph) {
-  if (in_graph) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
-  else cudaEventRecord(e, s);
+  record(ctx->ev_a1, ctx->s_main, in_graph);
 }
 
 void enqueue_iterations(frt_ctx* ctx, bool fused_thermal, bool in_graph = false) {
@@ -222,7 +225,7 @@ void enqueue_step(frt_ctx* ctx, bool in_graph) {
   cudaStream_t s = ctx->s_main;
   cudaMemcpyAsync(d.itheta_merge, ctx->h_ith_box, sizeof(uint16_t) * d.nbox, cudaMemcpyHostToDevice, s);
   if (d.nsrc) cudaMemcpyAsync(d.src_itheta, ctx->h_ith_src, sizeof(uint16_t) * d.nsrc, cudaMemcpyHostToDevice, s);
-  enqueue_begin_advance(ctx);
+  enqueue_begin_advance(ctx, in_graph);
   cudaEventRecord(ctx->ev_fork, s);
   cudaStreamWaitEvent(ctx->s_dark, ctx->ev_fork, 0);
   if (in_graph) cudaEventRecordWithFlags(ctx->ev_d0, ctx->s_dark, cudaEventRecordExternal);
@@ -330,6 +333,12 @@ frt_status finish_step(frt_ctx* ctx, frt_step_stats* stats) {
     rms += x;
   }
   ctx->last_raypass_ms = rms;
+  float ams = 0.f;
+  if (cudaEventElapsedTime(&ams, ctx->ev_a0, ctx->ev_a1) != cudaSuccess) {
+    cudaGetLastError();
+    ams = -1.f;
+  }
+  ctx->last_walk_ms = ams;
   if (ctx->h_ctl->merged > 0) ctx->merged_any = true;
   fill_stats(ctx, *ctx->h_ctl, stats);
   if (ctx->h_ctl->err) {
@@ -382,6 +391,8 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
   CK(cudaEventCreate(&ctx->ev_t1));
   CK(cudaEventCreate(&ctx->ev_d0));
   CK(cudaEventCreate(&ctx->ev_d1));
+  CK(cudaEventCreate(&ctx->ev_a0));
+  CK(cudaEventCreate(&ctx->ev_a1));
   for (cudaEvent_t& e : ctx->ev_r) CK(cudaEventCreate(&e));
 
   Dev& d = ctx->d;
@@ -541,7 +552,7 @@ frt_status frt_destroy(frt_ctx* ctx) {
   if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
   for (cudaEvent_t e : ctx->ev_r)
     if (e) cudaEventDestroy(e);
-  cudaEvent_t evs[] = {ctx->ev_fork, ctx->ev_join, ctx->ev_t0, ctx->ev_t1, ctx->ev_d0, ctx->ev_d1};
+  cudaEvent_t evs[] = {ctx->ev_fork, ctx->ev_join, ctx->ev_t0, ctx->ev_t1, ctx->ev_d0, ctx->ev_d1, ctx->ev_a0, ctx->ev_a1};
   for (cudaEvent_t e : evs)
     if (e) cudaEventDestroy(e);
   if (ctx->s_main) cudaStreamDestroy(ctx->s_main);
@@ -1417,8 +1428,8 @@ frt_status frt_last_adjoint_timing(frt_ctx* ctx, float* ms) {
 }
 
 frt_status frt_last_kernel_timing(frt_ctx* ctx, int which, float* ms) {
-  if (!ctx || !ms || which < 0 || which > 1) return FRT_ERR_INVALID;
-  *ms = which == 0 ? ctx->last_dark_ms : ctx->last_raypass_ms;
+  if (!ctx || !ms || which < 0 || which > 2) return FRT_ERR_INVALID;
+  *ms = which == 0 ? ctx->last_dark_ms : (which == 1 ? ctx->last_raypass_ms : ctx->last_walk_ms);
   return FRT_OK;
 }
 

@@ -113,10 +113,10 @@ def run_per_box_loop(inputs: Sequence[W.BoxInputs], seeds: Sequence[int], warmup
         for c in ctxs:
             cross += c.step(graph=False)["crossings"]
     wall = time.perf_counter() - t0
-    rays = sum(c.num_rays() for c in ctxs)
+    per_box_rays = [float(c.num_rays()) for c in ctxs]
     for c in ctxs:
         c.close()
-    return {"crossings": cross, "wall_s": wall, "rays": rays}
+    return {"crossings": cross, "wall_s": wall, "rays": sum(per_box_rays), "per_box_rays": per_box_rays}
 
 
 def gather_box_results(local: Dict[int, List[float]], world: int) -> Dict[int, List[float]]:

@@ -452,6 +452,12 @@ class RTContext:
         self._check(self.L.frt_last_kernel_timing(self.h, 1, C.byref(v)), "frt_last_kernel_timing")
         return float(v.value)
 
+    def last_walk_ms(self) -> float:
+        """Device time of the walk (k_advance over every live ray) of the last step."""
+        v = C.c_float(0.0)
+        self._check(self.L.frt_last_kernel_timing(self.h, 2, C.byref(v)), "frt_last_kernel_timing")
+        return float(v.value)
+
     def last_adjoint_ms(self) -> float:
         v = C.c_float(0.0)
         self._check(self.L.frt_last_adjoint_timing(self.h, C.byref(v)), "frt_last_adjoint_timing")

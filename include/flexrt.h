@@ -310,7 +310,8 @@ frt_status frt_box_scalars(frt_ctx* ctx, int box, double* out8);
  * and the time of its dominant cell kernel. */
 frt_status frt_last_timing(frt_ctx* ctx, float* step_ms, float* cell_kernel_ms);
 /* Device time in ms of one kernel family in the last frt_step / frt_step_plain (CUDA events on its
- * stream): which = 0 the dark-cell kernel, 1 the ray passes of the C2Ray iteration (summed). */
+ * stream): which = 0 the dark-cell kernel, 1 the ray passes of the C2Ray iteration (summed),
+ * 2 the walk (update_rays' advance of every ray). */
 frt_status frt_last_kernel_timing(frt_ctx* ctx, int which, float* ms);
 
 /* ---- restart files (the reference's own formats) ------------------------------------------------

@@ -63,11 +63,11 @@ def user_inputs_values(spec: W.BoxSpec, ncpu: int, path_length: int = 8) -> dict
 
 
 def stage(name: str, spec: W.BoxSpec, ncpu: int, path_length: int = 8, restart: bool = False,
-          subgrid: bool = False) -> str:
+          subgrid: bool = False, ifront: bool = False) -> str:
     """Copy + configure the reference sources into oracle/_ref/<name>. A restart stage is built
     with input_grid = TRUE and reads input_files/restart_{gas,rays,tre}.bin. A sub-grid stage is
-    built with subgrid = TRUE, equilibrium = TRUE, ifront = FALSE and reads its tables from
-    subgrid_files/ under the stage directory."""
+    built with subgrid = TRUE, equilibrium = TRUE, ifront = `ifront` (I-front tracking) and reads
+    its tables from subgrid_files/ under the stage directory."""
     d = os.path.join(OUT, name)
     src = os.path.join(d, "src")
     os.makedirs(src, exist_ok=True)
@@ -76,12 +76,12 @@ def stage(name: str, spec: W.BoxSpec, ncpu: int, path_length: int = 8, restart: 
         shutil.copyfile(os.path.join(REF_SRC, f), os.path.join(src, f))
     for f in REF_DATA:
         shutil.copyfile(os.path.join(REF_SRC, f), os.path.join(d, f))
-    _configure(d, spec, ncpu, path_length, restart, subgrid)
+    _configure(d, spec, ncpu, path_length, restart, subgrid, ifront)
     return d
 
 
 def _configure(d: str, spec: W.BoxSpec, ncpu: int, path_length: int, restart: bool = False,
-               subgrid: bool = False) -> None:
+               subgrid: bool = False, ifront: bool = False) -> None:
     src = os.path.join(d, "src")
     # HEALPix includes -> project shim
     for f in ("ray_tracing.cc", "mem_funcs.cc"):
@@ -98,7 +98,7 @@ def _configure(d: str, spec: W.BoxSpec, ncpu: int, path_length: int, restart: bo
         (r"^const char ray_file_init\[\]\s*=.*$", 'const char ray_file_init[]     = "./input_files/restart_rays.bin";'),
         (r"^const char treion_file_init\[\]\s*=.*$", 'const char treion_file_init[]  = "./input_files/restart_tre.bin";'),
         (r"^bool const c2ray_iter\s*=.*$", "bool const c2ray_iter    = TRUE;"),
-        (r"^bool const ifront\s*=.*$", "bool const ifront        = FALSE;"),
+        (r"^bool const ifront\s*=.*$", f"bool const ifront        = {'TRUE' if ifront else 'FALSE'};"),
         (r"^bool const he2_tr_h2\s*=.*$", "bool const he2_tr_h2     = FALSE;"),
         (r"^bool const subgrid\s*=.*$", f"bool const subgrid       = {'TRUE' if subgrid else 'FALSE'};"),
         (r"^bool const equilibrium\s*=.*$", "bool const equilibrium   = TRUE;"),
@@ -142,6 +142,7 @@ def _configure(d: str, spec: W.BoxSpec, ncpu: int, path_length: int, restart: bo
                   f"short int const ray_per_cell_max = {spec.ray_per_cell_max};")
     open(p, "w").write(t)
     json.dump({"name": os.path.basename(d), "ncpu": ncpu, "path_length": path_length, "subgrid": subgrid,
+               "ifront": ifront,
                "spec": __import__("dataclasses").asdict(spec)},
               open(os.path.join(d, "stage.json"), "w"), indent=1)
 
@@ -166,12 +167,12 @@ def compile_stage(d: str, ncpu: Optional[int] = None) -> str:
 
 
 def build(name: str, spec: W.BoxSpec, ncpu: int = 1, path_length: int = 8, from_stage: bool = False,
-          restart: bool = False, subgrid: bool = False) -> str:
+          restart: bool = False, subgrid: bool = False, ifront: bool = False) -> str:
     d = os.path.join(OUT, name)
     if not from_stage:
         if not os.path.isdir(REF_SRC):
             raise RuntimeError("reference checkout not available; use from_stage=True")
-        stage(name, spec, ncpu, path_length, restart, subgrid)
+        stage(name, spec, ncpu, path_length, restart, subgrid, ifront)
         return compile_stage(d)
     return compile_stage(d, ncpu)
 

@@ -208,7 +208,22 @@ struct Ctx {
   float sg_tinit, sg_t12, sg_t8, sg_tcap, sg_tre_dom[3];
   float sg_dnl_dom[3];
   std::vector<float> sg_fh1_interp;
+  // I-front tracking (ifront = TRUE, subgrid.cc:660-751, ray_tracing.cc:863-919, 1003-1053): the
+  // fraction of each cell the fronts have passed and its maximum, the crossing time in total and
+  // per tenth of the cell (with the tenths already passed), the flags, and the photon counts of
+  // one C2Ray iteration per cell: [0] absorbed by the neutral part, [1] the same weighted by
+  // sigma_eff_rh times path length, [2] entering the neutral part
+  bool ifront = false;
+  std::vector<float> fion, fion_max, tcross, tcross_new, Delta_fion;
+  std::vector<unsigned char> tcross_check, tcross_flag, neutral_flag;
+  std::vector<double> ngam3;
 };
+
+static const int kNtcross = 10;   // global_variables.cc:224
+
+// the ionised fraction the sub-grid branch uses for a cell: 1 without I-front tracking
+// (rt_funcs.cc:55)
+static inline float fion_of(const Ctx& c, long q) { return c.ifront ? c.fion[q] : 1.f; }
 
 static inline long cidx(const Ctx& c, int i, int j, int k) { return ((long)i * c.N + j) * c.N + k; }
 static inline void split_ind(const Ctx& c, int ind, int* i, int* j, int* k) {
@@ -314,31 +329,11 @@ static int sg_tindex(const Ctx& c, float tsince) {
   return imax(0, imin(i, kNt - 2));
 }
 
-// get_gamma_interp (subgrid.cc:257-486) for the HI fraction, the one interpolant the equilibrium
-// model reads (interp_nh1): tcross_flag stays FALSE without I-front tracking
-static void sg_gamma_interp(Ctx& c, long q, float tre, float deltaNL, float tsince) {
-  int ind_tre[2], ind_delta[2];
-  const int ind_gamma[3] = {1, 2, 3};
-  tre = maxd(c.sg_t12, tre);
-  if (tre > c.sg_t8) { ind_tre[1] = 2; ind_tre[0] = 1; }
-  else { ind_tre[1] = 1; ind_tre[0] = 0; }
-  if (sg_deltasig(deltaNL, c.zz) < 0.) { ind_delta[1] = 1; ind_delta[0] = 0; }
-  else { ind_delta[1] = 2; ind_delta[0] = 1; }
-  const int itf = sg_tindex(c, tsince);
-  float f[2][2][3];
-  const float* T = c.sg_time.data();
-  const float* H = c.sg_fh1.data();
-  for (int m = 0; m < 2; m++)
-    for (int p = 0; p < 2; p++)
-      for (int g = 0; g < 3; g++) {
-        const int im = ind_tre[m], ip = ind_delta[p], iq = ind_gamma[g];
-        float v = H[sg_at(itf, im, ip, iq)] + (H[sg_at(itf + 1, im, ip, iq)] - H[sg_at(itf, im, ip, iq)]) /
-                                                  (T[sg_at(itf + 1, im, ip, iq)] - T[sg_at(itf, im, ip, iq)]) *
-                                                  (tsince - T[sg_at(itf, im, ip, iq)]);
-        f[m][p][g] = mind(maxd(v, 0.), 1.);
-      }
-  // get_interpolate_gamma_f (subgrid.cc:211-250), fractype = TRUE
-  float out[5];
+// get_interpolate_gamma_f (subgrid.cc:211-250) with fractype = TRUE, and the extension to the
+// outer rates of get_gamma_interp (subgrid.cc:451-452): out[5] over kGammaDom from the time-
+// interpolated HI fractions f[tre][delta][gamma]
+static void sg_gamma_f(const Ctx& c, float tsince, float tre, float deltaNL, const int ind_tre[2],
+                       const int ind_delta[2], float f[2][2][3], float out[5]) {
   const float* tre_dom = c.sg_tre_dom;
   for (int g = 0; g < 3; g++) {
     float f_d0 = log10(f[0][0][g]) + (log10(f[1][0][g]) - log10(f[0][0][g])) *
@@ -354,6 +349,77 @@ static void sg_gamma_interp(Ctx& c, long q, float tre, float deltaNL, float tsin
   }
   out[0] = pow(kGammaDom[0] / kGammaDom[1], 0.) * out[1];
   out[4] = pow(kGammaDom[4] / kGammaDom[3], -1.) * out[3];
+}
+
+// the HI fractions of the RadHydro runs at time x since ionisation, linear in time between the
+// table rows itf and itf + 1, for the tre indices ind_tre and the density indices ind_delta
+static void sg_fh1_at(const Ctx& c, int itf, float x, const int ind_tre[2], const int ind_delta[2], float f[2][2][3]) {
+  const int ind_gamma[3] = {1, 2, 3};
+  const float* T = c.sg_time.data();
+  const float* H = c.sg_fh1.data();
+  for (int m = 0; m < 2; m++)
+    for (int p = 0; p < 2; p++)
+      for (int g = 0; g < 3; g++) {
+        const int im = ind_tre[m], ip = ind_delta[p], iq = ind_gamma[g];
+        float v = H[sg_at(itf, im, ip, iq)] + (H[sg_at(itf + 1, im, ip, iq)] - H[sg_at(itf, im, ip, iq)]) /
+                                                  (T[sg_at(itf + 1, im, ip, iq)] - T[sg_at(itf, im, ip, iq)]) *
+                                                  (x - T[sg_at(itf, im, ip, iq)]);
+        f[m][p][g] = mind(maxd(v, 0.), 1.);
+      }
+}
+
+// get_gamma_interp (subgrid.cc:257-545) for the HI fraction, the one interpolant the equilibrium
+// model reads (interp_nh1). Once an I-front has started to cross the cell (tcross_flag), the
+// interpolant is the average over the tenths of the cell the fronts have passed, each tenth
+// evaluated at its own crossing time, weighted up to fion_max.
+static void sg_gamma_interp(Ctx& c, long q, float tre, float deltaNL, float tsince) {
+  int ind_tre[2], ind_delta[2];
+  tre = maxd(c.sg_t12, tre);
+  if (tre > c.sg_t8) { ind_tre[1] = 2; ind_tre[0] = 1; }
+  else { ind_tre[1] = 1; ind_tre[0] = 0; }
+  if (sg_deltasig(deltaNL, c.zz) < 0.) { ind_delta[1] = 1; ind_delta[0] = 0; }
+  else { ind_delta[1] = 2; ind_delta[0] = 1; }
+  float out[5];
+  {
+    float f[2][2][3];
+    sg_fh1_at(c, sg_tindex(c, tsince), tsince, ind_tre, ind_delta, f);
+    sg_gamma_f(c, tsince, tre, deltaNL, ind_tre, ind_delta, f, out);
+  }
+  if (c.ifront && c.tcross_flag[q]) {
+    const float* tcn = &c.tcross_new[(size_t)q * kNtcross];
+    float ftt[kNtcross][5];
+    for (int tt = 0; tt < kNtcross; tt++) {
+      int ind_tre_tc[2];
+      if (tre + tcn[tt] > c.sg_t8) { ind_tre_tc[1] = 2; ind_tre_tc[0] = 1; }
+      else { ind_tre_tc[1] = 1; ind_tre_tc[0] = 0; }
+      float tc = 0.;
+      if (tt == 0) tc = tcn[0] / 2.;
+      else tc = tcn[tt - 1] + (tcn[tt] - tcn[tt - 1]) / 2.;
+      float f[2][2][3];
+      sg_fh1_at(c, sg_tindex(c, tsince - tc), tsince - tc, ind_tre_tc, ind_delta, f);
+      sg_gamma_f(c, tsince - tc, tre + tc, deltaNL, ind_tre_tc, ind_delta, f, ftt[tt]);
+    }
+    const float fmax = c.fion_max[q];
+    for (int g = 0; g < 5; g++) {
+      float acc = 0.;
+      if (fmax == 1.) {
+        for (int tt = 0; tt < kNtcross; tt++) {
+          float tc_frac = 1. / ((float)kNtcross);
+          acc += tc_frac * ftt[tt][g];
+        }
+      } else {
+        for (int tt = 0; tt < kNtcross; tt++) {
+          float tc_frac = 1. / ((float)kNtcross);
+          if ((fmax >= tt * tc_frac) && (fmax < (tt + 1.) * tc_frac)) {
+            for (int ttt = 0; ttt < tt; ttt++) acc += tc_frac * ftt[ttt][g];
+            acc += (maxd(0.01, fmax) - tt * tc_frac) * ftt[tt][g];
+          }
+        }
+      }
+      acc = acc / maxd(0.01, fmax);
+      out[g] = mind(acc, kMaxSubgridFrac);
+    }
+  }
   for (int g = 0; g < 5; g++) c.sg_fh1_interp[(size_t)q * 5 + g] = out[g];
 }
 
@@ -508,7 +574,7 @@ static void init_rays(Ctx& c, int i, int j, int k, double lum, int src) {
   }
 }
 
-// ---- advance (ray_tracing.cc:1222-1512), plain mode: fion = 1 everywhere ---------------------
+// ---- advance (ray_tracing.cc:1222-1512) ------------------------------------------------------
 static void advance_ray(Ctx& c, Ray& R) {
   float tx, ty, tz, tmin = 0;
   int tag;
@@ -574,7 +640,10 @@ static void advance_ray(Ctx& c, Ray& R) {
       }
       tlast += tmin;
     }
-    dist = (deltat - tlast + tmin) * c.clight;
+    // in a cell a front has not fully passed, the last segment is the whole crossing of the cell
+    // (ray_tracing.cc:1425-1437)
+    if (fion_of(c, in * c.N * c.N + jn * c.N + kn) < 1.) dist = tmin * c.clight;
+    else dist = (deltat - tlast + tmin) * c.clight;
     dist = maxd(dist, kMinDist * dxc);
     if (p >= c.PL) { fprintf(stderr, "oracle: path overflow\n"); abort(); }
     R.pind[p] = in * c.N * c.N + jn * c.N + kn;
@@ -604,6 +673,58 @@ static void update_rays(Ctx& c) {
     if (R.alive) advance_ray(c, R);
 }
 
+// the equilibrium mean free paths of an ionised cell (ray_tracing.cc:989-994, 1031-1036)
+static void sg_eq_mfp(Ctx& c, long q) {
+  c.mfp[q] = maxd(kGammaMin, c.avg_gamma[q]) / c.clump[q] / kSigmaEffRH / alphaB_H2(maxd(kTempMin, c.temp[q])) /
+             pow(c.nH[q], 2.) / 1.082;
+  c.mfp_912[q] = maxd(kGammaMin, c.avg_gamma[q]) / c.clump[q] / sig_H1(13.6 / O_H_EV) /
+                 alphaB_H2(maxd(kTempMin, c.temp[q])) / pow(c.nH[q], 2.) / 1.082;
+  c.mfp[q] = maxd(0.f, c.mfp[q]);   // mfp_min = 1e-2*dx[0] taken while dx is still 0 (global_variables.cc:301)
+  c.mfp_912[q] = maxd(0.f, c.mfp_912[q]);
+}
+
+// set_Treion (subgrid.cc:660-670): the temperature of the newly ionised part of a cell from the
+// I-front speed (D'Aloisio et al. 2019 fit), averaged into the cell's temperature
+static void set_Treion(Ctx& c, long q, float vIF, float fi_old, float fi_new) {
+  float Cn[5] = {9.5432, -1.6441e-2, -9.8010e-3, 4.1664e-3, -2.2710e-4};
+  float lnTreion = 0.;
+  for (int t = 0; t < 5; t++) lnTreion += Cn[t] * pow(log(vIF / 1e5), t);
+  if (fi_new > 0.) c.temp[q] = (fi_old * c.temp[q] + (fi_new - fi_old) * exp(lnTreion)) / fi_new;
+}
+
+// update_fion (subgrid.cc:694-751): the front advances by vIF dt / dx with vIF from the photons
+// entering the neutral part, and the crossing times are booked per tenth of the cell
+static void update_fion(Ctx& c, long q) {
+  float tdiff;
+  float vIF_min = 5e1 * 1e5;
+  double Fl = c.ngam3[(size_t)q * 3 + 2] / pow(c.dxc, 2.) / c.dt;
+  float vIF = (float)(Fl / c.nH[q] / (1. + kNheToNh));
+  float fion_old = c.fion[q];
+  float fion_max_old = c.fion_max[q];
+  c.fion[q] = mind(c.fion[q] + vIF * c.dt / c.dxc, 1.);
+  if (c.fion[q] > c.fion_max[q]) c.fion_max[q] = c.fion[q];
+  if ((vIF > vIF_min) || (fion_old == 0.)) set_Treion(c, q, maxd(vIF, vIF_min), fion_old, c.fion[q]);
+  if ((fion_old < 0.5) && (c.fion[q] >= 0.5)) c.treion_out[q] = c.t - c.dt;
+  if (c.fion[q] >= 1.) tdiff = 0.5 * c.dt;
+  else tdiff = 0.;
+  c.IF_speed[q] = vIF;
+  c.Inc_Flux[q] = Fl;
+  c.Delta_fion[q] = c.fion[q] - fion_old;
+  c.tcross[q] += c.dt - tdiff;
+  for (int tt = 0; tt < kNtcross; tt++) {
+    float tc_frac = 1. / ((float)kNtcross);
+    float& tn = c.tcross_new[(size_t)q * kNtcross + tt];
+    unsigned char& ck = c.tcross_check[(size_t)q * kNtcross + tt];
+    if ((c.fion_max[q] < tc_frac * (tt + 1.)) && !ck) {
+      tn += c.dt;
+    } else if ((c.fion_max[q] >= tc_frac * (tt + 1.)) && (fion_max_old < tc_frac * (tt + 1.)) && !ck) {
+      tn += c.dt * (tc_frac * (tt + 1.) - fion_max_old) / (c.fion_max[q] - fion_max_old);
+      ck = 1;
+    }
+  }
+  if (!c.tcross_flag[q]) c.tcross_flag[q] = 1;
+}
+
 // ---- C2Ray iteration (ray_tracing.cc:623-1216), plain mode -------------------------------
 static void find_avg_unu(Ctx& c) {
   const long n3 = (long)c.N * c.N * c.N;
@@ -615,6 +736,10 @@ static void find_avg_unu(Ctx& c) {
       c.avg_gamma_he1[q] = 0.;
       c.IF_speed[q] = 0.;
       c.Inc_Flux[q] = 0.;
+      if (c.ifront) {
+        c.ngam3[(size_t)q * 3] = c.ngam3[(size_t)q * 3 + 1] = c.ngam3[(size_t)q * 3 + 2] = 0.;
+        c.Delta_fion[q] = 0.;
+      }
       for (int nu = 0; nu < F; nu++) {
         c.ngam_nu[q * F + nu] = 0.;
         c.avg_gamma_nu[q * F + nu] = 0.;
@@ -656,15 +781,18 @@ static void find_avg_unu(Ctx& c) {
       short p = 0;
       unsigned dump_mask = 0;   // ledger: bins that a dump deposited
       if (c.subgrid) {
-        // sub-grid ray pass (ray_tracing.cc:701-938 with subgrid = TRUE, fion = 1): fixed H/He
-        // split, Gamma from the sub-grid effective cross section over the effective path, the
-        // segment's optical depth from the cell's mean free path after its deposit
+        // sub-grid ray pass (ray_tracing.cc:701-938 with subgrid = TRUE): fixed H/He split, Gamma
+        // from the sub-grid effective cross section over the effective path in the part of the
+        // cell the fronts have passed, the segment's optical depth from the cell's mean free path
+        // there (a cell no front has reached keeps the previous segment's dtau); with I-front
+        // tracking, the neutral part of a cell absorbs the photons of the rays in ray order up to
+        // its hydrogen and helium atoms (ray_tracing.cc:863-919)
         const double frac_h1 = 1. - (O_Y / 4.) / (1. - O_Y + O_Y / 4.);
         const double frac_he1 = (O_Y / 4.) / (1. - O_Y + O_Y / 4.);
-        const float fion = 1.f;
+        short p_prev = 0;
         while (p < R.ray_end) {
           const long q = R.pind[p];
-          const float dist = R.pdist[p];
+          const float fion = fion_of(c, q);
           double nphot_in[kMaxF];
           double nphot_in_total = 0.;
           for (int nu = 0; nu < F; nu++) {
@@ -674,23 +802,59 @@ static void find_avg_unu(Ctx& c) {
           const bool dump = nphot_in_total < c.nphot_min;
           for (int nu = 0; nu < F; nu++) {
             c.ngam_nu[q * F + nu] += (float)(nphot_in[nu] / kPhotNorm);
-            float delta_s_eff;
-            if (iter == 0) delta_s_eff = fion * dist / frac_h1;
-            else delta_s_eff = c.mfp[q] * (1. - exp(-fion * dist / c.mfp[q] / frac_h1));
-            c.avg_gamma_nu[q * F + nu] += (float)(frac_h1 * nphot_in[nu] * kSigmaEffRH * delta_s_eff / c.dt / vol / fion);
-            c.avg_gamma[q] += (float)(frac_h1 * nphot_in[nu] * kSigmaEffRH * delta_s_eff / c.dt / vol / fion);
-            c.avg_gamma_nu_he1[q * F + nu] += (float)(frac_he1 * nphot_in[nu] * kSigmaEffRH * delta_s_eff / c.dt / vol / fion);
-            c.avg_gamma_he1[q] += (float)(frac_he1 * nphot_in[nu] * kSigmaEffRH * delta_s_eff / c.dt / vol / fion);
+            if (fion > 0.) {
+              float delta_s_eff;
+              if (iter == 0) delta_s_eff = fion * R.pdist[p] / frac_h1;
+              else delta_s_eff = c.mfp[q] * (1. - exp(-fion * R.pdist[p] / c.mfp[q] / frac_h1));
+              c.avg_gamma_nu[q * F + nu] += (float)(frac_h1 * nphot_in[nu] * kSigmaEffRH * delta_s_eff / c.dt / vol / fion);
+              c.avg_gamma[q] += (float)(frac_h1 * nphot_in[nu] * kSigmaEffRH * delta_s_eff / c.dt / vol / fion);
+              c.avg_gamma_nu_he1[q * F + nu] += (float)(frac_he1 * nphot_in[nu] * kSigmaEffRH * delta_s_eff / c.dt / vol / fion);
+              c.avg_gamma_he1[q] += (float)(frac_he1 * nphot_in[nu] * kSigmaEffRH * delta_s_eff / c.dt / vol / fion);
+            }
           }
           p = dump ? 99 : p + 1;
+          if (fion > 0.)
+            for (int nu = 0; nu < F; nu++) {
+              dtau_h1[nu] = fion * R.pdist[p_prev] / c.mfp[q];
+              dtau_he1[nu] = kNheToNh * dtau_h1[nu];
+            }
+          double before = 0.;   // ledger: the photons entering the segment
           for (int nu = 0; nu < F; nu++) {
-            dtau_h1[nu] = fion * dist / c.mfp[q];
-            dtau_he1[nu] = kNheToNh * dtau_h1[nu];
+            before += nphot_in[nu];
             tau_h1[nu] += dtau_h1[nu];
             tau_he1[nu] += dtau_he1[nu];
-            // ledger: the photons the segment takes out of the ray
-            if (iter == c.itercount - 1) c.led_deposited += nphot_in[nu] * (1. - exp(-(dtau_h1[nu] + dtau_he1[nu])));
           }
+          if (fion < 1.) {
+            double* ng = &c.ngam3[(size_t)q * 3];
+            const double sum_ngam = ng[0];
+            const double chi = kNheToNh;
+            const double free_ngam = vol * c.nH[q] * (1. + chi) * (1. - fion);
+            double nphot_left = 0.;
+            for (int nu = 0; nu < F; nu++) ng[2] += nphot_in[nu] * exp(-(dtau_h1[nu] + dtau_he1[nu]));
+            if (sum_ngam < free_ngam) {
+              for (int nu = 0; nu < F; nu++) {
+                const double ngam_abs = mindd(nphot_in[nu] * exp(-(dtau_h1[nu] + dtau_he1[nu])), free_ngam - sum_ngam);
+                ng[0] += ngam_abs;
+                ng[1] += ngam_abs * kSigmaEffRH * R.pdist[p_prev];
+                nphot_in[nu] = nphot_in[nu] * exp(-(dtau_h1[nu] + dtau_he1[nu])) - ngam_abs;
+                nphot_left += nphot_in[nu];
+              }
+              if (nphot_left == 0.) {
+                p = 99;
+                for (int nu = 0; nu < F; nu++) tau_h1[nu] = 999.;
+              } else {
+                for (int nu = 0; nu < F; nu++)
+                  tau_h1[nu] += -log(nphot_in[nu] / nphot[nu] / exp(-(tau_h1[nu] + tau_he1[nu])));
+              }
+            }
+          }
+          if (iter == c.itercount - 1) {
+            // ledger: what the segment took out of the ray
+            double after = 0.;
+            for (int nu = 0; nu < F; nu++) after += nphot[nu] * exp(-tau_h1[nu] - tau_he1[nu]);
+            c.led_deposited += before - after;
+          }
+          p_prev = p;
         }
       }
       while (!c.subgrid && p < R.ray_end) {
@@ -769,25 +933,41 @@ static void find_avg_unu(Ctx& c) {
     }
     // cell pass B
     for (long q = 0; q < n3 && c.subgrid; q++) {
-      // the sub-grid branch (ray_tracing.cc:956-1071, equilibrium = TRUE, ifront = FALSE) and the
-      // last-iteration bookkeeping (1138-1209)
+      // the sub-grid branch (ray_tracing.cc:956-1071, equilibrium = TRUE) and the last-iteration
+      // bookkeeping (1138-1209)
       double nelec = (double)(c.nH[q] - c.avg_nh1[q] + c.nHe[q] - c.avg_nhe1[q]);
-      const float fion = 1.f;
-      if ((iter == c.itercount - 1) && !c.treion_flag[q] && (c.avg_gamma[q] > 0.)) {
+      const bool last = iter == c.itercount - 1;
+      const double* ng = c.ifront ? &c.ngam3[(size_t)q * 3] : nullptr;
+      bool first = false;
+      if (last && !c.treion_flag[q] && ((c.ifront && ng[1] > 0.) || (c.avg_gamma[q] > 0.))) {
         c.treion[q] = c.t - c.dt;
         c.treion_flag[q] = 1;
         sg_gamma_interp(c, q, c.treion[q] + c.sg_tinit, c.rho[q] / c.avg_rho - 1., c.t - c.treion[q]);
+        first = true;
       }
-      if (c.treion_flag[q] && fion > 0.) {
-        c.mfp[q] = maxd(kGammaMin, c.avg_gamma[q]) / c.clump[q] / kSigmaEffRH / alphaB_H2(maxd(kTempMin, c.temp[q])) /
-                   pow(c.nH[q], 2.) / 1.082;
-        c.mfp_912[q] = maxd(kGammaMin, c.avg_gamma[q]) / c.clump[q] / sig_H1(13.6 / O_H_EV) /
-                       alphaB_H2(maxd(kTempMin, c.temp[q])) / pow(c.nH[q], 2.) / 1.082;
-        c.mfp[q] = maxd(0.f, c.mfp[q]);   // mfp_min = 1e-2*dx[0] taken while dx is still 0 (global_variables.cc:301)
-        c.mfp_912[q] = maxd(0.f, c.mfp_912[q]);
+      if (c.treion_flag[q] && fion_of(c, q) > 0.) sg_eq_mfp(c, q);
+      if (c.ifront && c.treion_flag[q] && last && (c.fion[q] < 1.)) {
+        // I-front correction (ray_tracing.cc:1003-1047)
+        const double gamma_fion = ng[1] / c.dt / vol;
+        update_fion(c, q);
+        if (c.fion[q] >= 1.) c.neutral_flag[q] = 0;
+        float clump_fion = c.clump[q];   // equilibrium: C_HII
+        if ((c.fion[q] < 1.) && (c.avg_gamma[q] == 0.) && !first)
+          c.fion[q] = maxd(0., c.fion[q] - clump_fion * alphaB_H2(maxd(kTempMin, c.temp[q])) * (1. + kNheToNh) *
+                                               c.nH[q] * c.fion[q] * c.dt);
+        if (first) {   // a newly ionised cell: its rate and mean free path from the front's photons
+          c.avg_gamma[q] = gamma_fion;
+          sg_eq_mfp(c, q);
+        }
       }
-      if (iter != c.itercount - 1) continue;
+      if (c.ifront && (c.fion[q] == 1.) && (c.avg_gamma[q] == 0.) && last) {   // ray_tracing.cc:1051-1054
+        float clump_fion_2 = c.clump[q];
+        c.fion[q] = maxd(0., c.fion[q] - clump_fion_2 * alphaB_H2(maxd(kTempMin, c.temp[q])) * (1. + kNheToNh) *
+                                             c.nH[q] * c.fion[q] * c.dt);
+      }
+      if (!last) continue;
       if (c.treion_flag[q]) {
+        const float fion = fion_of(c, q);
         sg_interp_nh1(c, q, c.avg_gamma[q]);
         c.nH2[q] = c.nH[q] * fion;
         c.nHe2[q] = c.nHe[q] * fion;
@@ -811,8 +991,18 @@ static void find_avg_unu(Ctx& c) {
       c.f_H2[q] = c.nH2[q] / c.nH[q];
       c.f_He2[q] = c.nHe2[q] / c.nHe[q];
       c.f_He3[q] = c.nHe3[q] / c.nHe[q];
-      c.f_H1[q] = c.nH1[q] / c.nH[q];
-      c.f_He1[q] = c.nHe1[q] / c.nHe[q];
+      if (!c.ifront) {
+        c.f_H1[q] = c.nH1[q] / c.nH[q];
+        c.f_He1[q] = c.nHe1[q] / c.nHe[q];
+      } else {
+        if (c.fion[q] > 0.) {
+          c.f_H2[q] *= c.fion[q];
+          c.f_He2[q] *= c.fion[q];
+          c.f_He3[q] *= c.fion[q];
+        }
+        c.f_H1[q] = (float)((double)1. - c.f_H2[q]);
+        c.f_He1[q] = (float)((double)1. - c.f_He2[q] - c.f_He3[q]);
+      }
     }
     for (long q = 0; q < n3 && !c.subgrid; q++) {
       double nelec = (double)(c.nH[q] - c.avg_nh1[q] + c.nHe[q] - c.avg_nhe1[q]);
@@ -1071,7 +1261,7 @@ static void update_heat_cool(Ctx& c, long q) {
       c.heat_rate[q] = 0.;
     c.cool_rate[q] += rcrB_H2(maxd(kTempMin, c.temp[q])) * (c.nH[q] + c.nHe[q]) * c.nH[q];
     c.cool_rate[q] += rcrB_He2(maxd(kTempMin, c.temp[q])) * (c.nH[q] + c.nHe[q]) * c.nHe[q];
-    float nff = 1.f * (c.nH[q] + c.nHe[q]);   // fion (c.nH + c.nHe), fion = 1
+    float nff = fion_of(c, q) * (c.nH[q] + c.nHe[q]);
     c.cool_rate[q] += free_free_rate(maxd(kTempMin, c.temp[q])) * pow(nff, 2.);
     c.cool_rate[q] -= compton_rate(c.zz) * (c.nH[q] + c.nHe[q]) * (2.726 * (1 + c.zz) - maxd(kTempMin, c.temp[q]));
     return;
@@ -1342,6 +1532,16 @@ int orc_dump(void* h, const char* path) {
 #undef DF
 #undef DFN
   frtd_add1(&w, "treion_flag", FRTD_U8, n3, c.treion_flag.data());
+  if (c.ifront) {
+    frtd_add1(&w, "fion", FRTD_F32, n3, c.fion.data());
+    frtd_add1(&w, "fion_max", FRTD_F32, n3, c.fion_max.data());
+    frtd_add1(&w, "tcross", FRTD_F32, n3, c.tcross.data());
+    frtd_add1(&w, "Delta_fion", FRTD_F32, n3, c.Delta_fion.data());
+    const int64_t nt[2] = {n3, kNtcross};
+    frtd_add(&w, "tcross_new", FRTD_F32, 2, nt, c.tcross_new.data());
+    frtd_add1(&w, "tcross_flag", FRTD_U8, n3, c.tcross_flag.data());
+    frtd_add1(&w, "neutral_flag", FRTD_U8, n3, c.neutral_flag.data());
+  }
   double sc[16];
   orc_scalars(h, sc);
   frtd_add1(&w, "scalars", FRTD_F64, 16, sc);
@@ -1511,8 +1711,21 @@ extern "C" void orc_hydro_step(void* h, const float* delta1, int nsrc, const int
 // 500 x 500 floats), consts = {tinit, cosmic_time(z=12), cosmic_time(z=8), cosmic_time(z=5.5),
 // tre_dom[0..2]} as the reference's cosmic_time gives them.
 extern "C" void orc_set_subgrid(void* h, const float* time_tab, const float* fh1_tab, const float* t_dnl, const float* ds,
-                                const float* dnl, const float* consts) {
+                                const float* dnl, const float* consts, int ifront) {
   Ctx& c = *(Ctx*)h;
+  const size_t n3 = (size_t)c.N * c.N * c.N;
+  c.ifront = ifront != 0;
+  if (c.ifront) {   // init_rt with ifront = TRUE (rt_funcs.cc:49-69)
+    c.fion.assign(n3, 0.f);
+    c.fion_max.assign(n3, 0.f);
+    c.tcross.assign(n3, 0.f);
+    c.Delta_fion.assign(n3, 0.f);
+    c.tcross_new.assign(n3 * kNtcross, 0.f);
+    c.tcross_check.assign(n3 * kNtcross, 0);
+    c.tcross_flag.assign(n3, 0);
+    c.neutral_flag.assign(n3, 1);
+    c.ngam3.assign(n3 * 3, 0.);
+  }
   const size_t nrh = (size_t)kNt * 27 + 1;
   c.subgrid = true;
   c.sg_time.assign(time_tab, time_tab + nrh);

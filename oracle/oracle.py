@@ -77,7 +77,7 @@ def lib():
         _lib.orc_read_restart.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                                           C.c_size_t]
         _lib.orc_cosmo_expansion.argtypes = [C.c_void_p, C.c_float, C.c_float]
-        _lib.orc_set_subgrid.argtypes = [C.c_void_p] * 7
+        _lib.orc_set_subgrid.argtypes = [C.c_void_p] * 7 + [C.c_int]
         _lib.orc_hydro_step.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
                                         C.c_float]
         _lib.orc_adj_objective.restype = C.c_double
@@ -158,14 +158,14 @@ class Oracle:
         """update_cosmo_expansion with the given scale factors, then update_dt."""
         self._lib.orc_cosmo_expansion(self.h, C.c_float(a_current), C.c_float(a_prev))
 
-    def set_subgrid(self, tables, consts) -> None:
-        """The sub-grid model (equilibrium, no I-front tracking) with the reference's in-memory
-        tables (tests/golden/subgrid_tables.reference_arrays) and cosmic-time constants
-        {tinit, t(z=12), t(z=8), t(z=5.5), tre_dom[0..2]}."""
+    def set_subgrid(self, tables, consts, ifront: bool = False) -> None:
+        """The sub-grid model (equilibrium; with I-front tracking when ifront) with the
+        reference's in-memory tables (tests/golden/subgrid_tables.reference_arrays) and
+        cosmic-time constants {tinit, t(z=12), t(z=8), t(z=5.5), tre_dom[0..2]}."""
         keep = [np.ascontiguousarray(tables[k], np.float32) for k in ("time", "fh1", "t_dnl", "ds", "dnl")]
         c = np.ascontiguousarray(consts, np.float32)
         self._sg_keep = keep + [c]
-        self._lib.orc_set_subgrid(self.h, *[a.ctypes.data for a in keep], c.ctypes.data)
+        self._lib.orc_set_subgrid(self.h, *[a.ctypes.data for a in keep], c.ctypes.data, 1 if ifront else 0)
 
     def hydro_step(self, snap: W.BoxInputs, a_rt: float, dt_snap: float, zz: float) -> None:
         """update_hydro_step to the snapshot `snap` (its density and sources), then

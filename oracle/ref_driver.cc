@@ -59,6 +59,20 @@ static void drv_dump_state(const std::string& path, long step_no, long crossings
     for (int64_t c = 0; c < n3; ++c) fl[c] = (&treion_flag[0][0][0])[c] ? 1 : 0;
     frtd_add1(&w, "treion_flag", FRTD_U8, n3, fl.data());
   }
+  if (ifront == TRUE) {
+    frtd_add1(&w, "fion_max", FRTD_F32, n3, &fion_max[0][0][0]);
+    frtd_add1(&w, "tcross", FRTD_F32, n3, &tcross[0][0][0]);
+    frtd_add1(&w, "Delta_fion", FRTD_F32, n3, &Delta_fion[0][0][0]);
+    const int64_t nt[2] = {n3, Ntcross};
+    frtd_add(&w, "tcross_new", FRTD_F32, 2, nt, &tcross_new[0][0][0][0]);
+    std::vector<uint8_t> tf(n3), nf3(n3);
+    for (int64_t c = 0; c < n3; ++c) {
+      tf[c] = (&tcross_flag[0][0][0])[c] ? 1 : 0;
+      nf3[c] = (&neutral_flag[0][0][0])[c] ? 1 : 0;
+    }
+    frtd_add1(&w, "tcross_flag", FRTD_U8, n3, tf.data());
+    frtd_add1(&w, "neutral_flag", FRTD_U8, n3, nf3.data());
+  }
   // scalars
   double sc[16] = {(double)t, (double)dt, nphot_min, nphot_max, (double)nphot_merge, (double)num_thresh,
                    (double)total_rays, (double)dx0, (double)dx[0], (double)step_no, (double)crossings,

@@ -8,7 +8,8 @@ files pin the CPU restatement in oracle/frt_oracle.cc and, through it, the CUDA 
     python tests/golden/make_golden.py [names]
 
 T16C holds a run with the reference's cosmological expansion after every step and the scale
-factors it used. T16H adds two hydro snapshot switches (update_hydro_step) with rays in flight. T16R holds the reference's restart files (write_gas_binary / write_rays_binary / write_treion
+factors it used. T16G and T16F run the sub-grid model on synthetic RadHydro tables, without and with
+I-front tracking. T16H adds two hydro snapshot switches (update_hydro_step) with rays in flight. T16R holds the reference's restart files (write_gas_binary / write_rays_binary / write_treion
 after 3 steps of T16) and the states of the reference's own restart path run from them.
 """
 from __future__ import annotations
@@ -171,14 +172,19 @@ def make_hydro(name="T16H", base=("T16", W.config_tiny(), 11), steps=6):
                         hydro=np.array(hy, np.float64), **out)
 
 
-def make_subgrid(name="T16G", base=("T16", W.config_tiny(steps=6), 11), steps=6):
-    """A run of the reference's sub-grid model (subgrid = TRUE, equilibrium = TRUE, ifront = FALSE)
-    on synthetic tables in its own file formats (tests/golden/subgrid_tables.py): its states, the
-    cosmic times the model used (logged by the reference) and the span of the overdensity table,
-    so that the tables can be rebuilt without the reference's cosmology table."""
+IFRONT_FIELDS = ["fion", "fion_max", "tcross", "tcross_new", "tcross_flag", "neutral_flag", "Delta_fion", "IF_speed",
+                 "Inc_Flux", "treion_out"]
+
+
+def make_subgrid(name="T16G", base=("T16", W.config_tiny(steps=6), 11), steps=6, ifront=False):
+    """A run of the reference's sub-grid model (subgrid = TRUE, equilibrium = TRUE, ifront as
+    given) on synthetic tables in its own file formats (tests/golden/subgrid_tables.py): its
+    states, the cosmic times the model used (logged by the reference) and the span of the
+    overdensity table, so that the tables can be rebuilt without the reference's cosmology
+    table. With I-front tracking the states also hold the front fractions and crossing times."""
     import subgrid_tables as ST
     _, spec, seed = base
-    B.build(name, spec, ncpu=1, subgrid=True)
+    B.build(name, spec, ncpu=1, subgrid=True, ifront=ifront)
     d = os.path.join(B.OUT, name)
     ct = ST.cosmic_time_from_table(os.path.join(d, "input_files", "cosmo_table"))
     t0, t1 = ST.table_span(ct)
@@ -194,7 +200,7 @@ def make_subgrid(name="T16G", base=("T16", W.config_tiny(steps=6), 11), steps=6)
         assert consts is not None and len(consts) == 7, log[-2000:]
         for s in range(1, steps + 1):
             dd = frtd.read(os.path.join(td, f"dump_{s:04d}.frtd"))
-            for k in FIELDS + RAYS + ["scalars", "mfp", "f_H2"]:
+            for k in FIELDS + RAYS + ["scalars", "mfp", "f_H2"] + (IFRONT_FIELDS if ifront else []):
                 out[f"s{s}_{k}"] = dd[k]
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), seed=seed, steps=np.arange(1, steps + 1),
                         consts=np.array(consts, np.float32), span=np.array([t0, t1], np.float64), **out)
@@ -218,3 +224,6 @@ if __name__ == "__main__":
     if not only or "T16G" in only:
         make_subgrid()
         print("wrote T16G")
+    if not only or "T16F" in only:
+        make_subgrid(name="T16F", steps=8, ifront=True)
+        print("wrote T16F")
