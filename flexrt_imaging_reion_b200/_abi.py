@@ -21,7 +21,8 @@ FRT_OUT_CORE, FRT_OUT_DIAG = 0, 1
 FIELDS = ["RHO", "NH", "NHE", "NH1", "NHE1", "NH2", "NHE2", "NE", "N_TOT", "F_H1", "F_HE1", "F_H2", "F_HE2", "TEMP",
           "CLUMP", "AVG_NH1", "AVG_NHE1", "GAMMA_H1_TOT", "GAMMA_HE1_TOT", "HEAT_RATE", "COOL_RATE", "TREION",
           "TREION_FLAG", "DNE_DT", "RECOMB_H2", "RECOMB_HE2", "RECRATE_H2", "RECRATE_HE2", "MFP", "MFP_912",
-          "IF_SPEED", "INC_FLUX", "GAMMA_H1_NU", "GAMMA_HE1_NU", "NGAM_NU", "U_NU"]
+          "IF_SPEED", "INC_FLUX", "GAMMA_H1_NU", "GAMMA_HE1_NU", "NGAM_NU", "U_NU", "FION", "FION_MAX", "TCROSS",
+          "DELTA_FION", "TREION_OUT", "TCROSS_FLAG", "NEUTRAL_FLAG", "TCROSS_NEW"]
 FIELD_ID = {name: i for i, name in enumerate(FIELDS)}
 PER_BIN_FIELDS = {"GAMMA_H1_NU", "GAMMA_HE1_NU", "NGAM_NU", "U_NU"}
 
@@ -73,7 +74,8 @@ class Tuning(C.Structure):
 class SubgridTables(C.Structure):
     _fields_ = [("time_RH", C.c_void_p), ("fh1_RH", C.c_void_p), ("t_deltaNL", C.c_void_p),
                 ("delta_over_sigma", C.c_void_p), ("deltaNL", C.c_void_p), ("tinit", C.c_float),
-                ("t_z12", C.c_float), ("t_z8", C.c_float), ("t_z55", C.c_float), ("tre_dom", C.c_float * 3)]
+                ("t_z12", C.c_float), ("t_z8", C.c_float), ("t_z55", C.c_float), ("tre_dom", C.c_float * 3),
+                ("ifront", C.c_int)]
 
 
 class StepStats(C.Structure):

@@ -29,6 +29,12 @@ struct frt_ctx {
   static constexpr int kMaxTimedIter = 16;
   cudaEvent_t ev_r[2 * kMaxTimedIter] = {};   // around each ray pass of the step
   float last_raypass_ms = 0.f, last_walk_ms = 0.f;
+  // I-front tracking: rounds of the last step (summed over its iterations), a budget that did not
+  // settle, and the pinned word the round flag is read into
+  static constexpr int kMaxFrontRounds = 4096;
+  int if_rounds_last = 0;
+  bool if_unsettled = false;
+  int* h_flag = nullptr;
   // sources per box (host copy)
   std::vector<std::vector<int>> src_cell;
   std::vector<std::vector<double>> src_lum;
@@ -194,8 +200,42 @@ void enqueue_begin_advance(frt_ctx* ctx, bool in_graph = false) {
   record(ctx->ev_a1, ctx->s_main, in_graph);
 }
 
+// The C2Ray iterations with I-front tracking: per iteration, rounds of (ray pass, budget pass)
+// until no front cell's sums change (the host reads the flag after each round), then for the
+// last iteration the pass that updates the rays, and the cell pass. Launched directly (the number
+// of rounds is known only on the host), never inside a graph.
+void enqueue_iterations_ifront(frt_ctx* ctx, bool fused_thermal) {
+  Dev& d = ctx->d;
+  cudaStream_t s = ctx->s_main;
+  const int grid = ctx->grid_lit;
+  launch_sg_lit_init(d, grid, s);
+  launch_if_lists(d, grid, s);
+  ctx->if_rounds_last = 0;
+  for (int it = 0; it < d.itercount; it++) {
+    bool settled = false;
+    for (int round = 0; round < frt_ctx::kMaxFrontRounds; round++) {
+      cudaMemsetAsync(&d.ctl->if_changed, 0, sizeof(int), s);
+      launch_if_round(d, it, grid, s);
+      cudaMemcpyAsync(ctx->h_flag, &d.ctl->if_changed, sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (cudaStreamSynchronize(s) != cudaSuccess) return;   // (the step's status check reports it)
+      ctx->if_rounds_last += 1;
+      if (*ctx->h_flag == 0) {
+        settled = true;
+        break;
+      }
+    }
+    if (!settled) ctx->if_unsettled = true;
+    if (it == d.itercount - 1) launch_if_final(d, it, grid, s);
+    launch_sg_litpass(d, it, fused_thermal, ctx->nsm * ctx->tune.lit_grid, s);
+  }
+}
+
 void enqueue_iterations(frt_ctx* ctx, bool fused_thermal, bool in_graph = false) {
   const Dev& d = ctx->d;
+  if (d.subgrid && d.ifront) {   // I-front tracking: the budget rounds of every C2Ray iteration
+    enqueue_iterations_ifront(ctx, fused_thermal);
+    return;
+  }
   if (d.subgrid) {   // the sub-grid model's passes (frt_subgrid.cu)
     launch_sg_lit_init(d, ctx->grid_lit, ctx->s_main);
     for (int it = 0; it < d.itercount; it++) {
@@ -341,6 +381,12 @@ frt_status finish_step(frt_ctx* ctx, frt_step_stats* stats) {
   ctx->last_walk_ms = ams;
   if (ctx->h_ctl->merged > 0) ctx->merged_any = true;
   fill_stats(ctx, *ctx->h_ctl, stats);
+  if (ctx->if_unsettled) {
+    ctx->if_unsettled = false;
+    ctx->err = "I-front photon budgets did not settle within " + std::to_string(frt_ctx::kMaxFrontRounds) +
+               " rounds in a C2Ray iteration";
+    return FRT_ERR_STATE;
+  }
   if (ctx->h_ctl->err) {
     ctx->err = "device error flags " + std::to_string(ctx->h_ctl->err) +
                " (1 ray pool full, 2 path_length exceeded, 4 lit-cell list full)";
@@ -518,7 +564,7 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
     launch_fill_i32(d.ray_bin, -1, (long long)R, ctx->s_main);
     AL(d.merged_flag, R);
   }
-  AL(d.src_cell, d.src_cap); AL(d.src_box, d.src_cap); AL(d.src_lum, d.src_cap); AL(d.src_ray_dt, d.src_cap);
+  AL(d.src_cell, d.src_cap); AL(d.src_box, d.src_cap); AL(d.src_lum, d.src_cap); AL(d.src_ray_dt, d.src_cap); AL(d.src_pos, d.src_cap);
   AL(d.src_itheta, d.src_cap);
   AL(d.ctl, 1);
   AL(d.rp_queue, kMaxIterQueue);
@@ -550,6 +596,7 @@ frt_status frt_destroy(frt_ctx* ctx) {
   if (ctx->h_ith_box) cudaFreeHost(ctx->h_ith_box);
   if (ctx->h_ith_src) cudaFreeHost(ctx->h_ith_src);
   if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
+  if (ctx->h_flag) cudaFreeHost(ctx->h_flag);
   for (cudaEvent_t e : ctx->ev_r)
     if (e) cudaEventDestroy(e);
   cudaEvent_t evs[] = {ctx->ev_fork, ctx->ev_join, ctx->ev_t0, ctx->ev_t1, ctx->ev_d0, ctx->ev_d1, ctx->ev_a0, ctx->ev_a1};
@@ -757,6 +804,34 @@ frt_status frt_get_field(frt_ctx* ctx, int box, frt_field f, float* host) {
       std::vector<uint8_t> a(n);
       CK(cudaMemcpy(a.data(), d.treion_flag + B.cell0, n, cudaMemcpyDeviceToHost));
       for (size_t i = 0; i < n; i++) host[i] = a[i] ? 1.f : 0.f;
+      return FRT_OK;
+    }
+    case FRT_F_FION:
+    case FRT_F_FION_MAX:
+    case FRT_F_TCROSS:
+    case FRT_F_DELTA_FION:
+    case FRT_F_TREION_OUT:
+    case FRT_F_TCROSS_FLAG:
+    case FRT_F_NEUTRAL_FLAG:
+    case FRT_F_TCROSS_NEW: {
+      if (!d.ifront) {
+        ctx->err = "the I-front fields exist with I-front tracking only (frt_set_subgrid)";
+        return FRT_ERR_STATE;
+      }
+      if (f == FRT_F_TCROSS_FLAG || f == FRT_F_NEUTRAL_FLAG) {
+        std::vector<uint8_t> a(n);
+        CK(cudaMemcpy(a.data(), d.if_flags + B.cell0, n, cudaMemcpyDeviceToHost));
+        const uint8_t bit = (f == FRT_F_TCROSS_FLAG) ? 1 : 2;
+        for (size_t i = 0; i < n; i++) host[i] = (a[i] & bit) ? 1.f : 0.f;
+        return FRT_OK;
+      }
+      if (f == FRT_F_TCROSS_NEW) {
+        CK(cudaMemcpy(host, d.tcross_new + (size_t)B.cell0 * 10, sizeof(float) * n * 10, cudaMemcpyDeviceToHost));
+        return FRT_OK;
+      }
+      const float* src = f == FRT_F_FION ? d.fion : f == FRT_F_FION_MAX ? d.fion_max : f == FRT_F_TCROSS ? d.tcross
+                         : f == FRT_F_DELTA_FION ? d.delta_fion : d.treion_out;
+      CK(get(src, host));
       return FRT_OK;
     }
     case FRT_F_GAMMA_H1_TOT: return sparse(0, host);
@@ -983,7 +1058,36 @@ frt_status frt_set_subgrid(frt_ctx* ctx, const frt_subgrid_tables* t) {
   d.sg_tcap = t->t_z55;
   for (int k = 0; k < 3; k++) d.sg_tre_dom[k] = t->tre_dom[k];
   d.sg_fH1_0 = ctx->cfg.fH1_0;
+  d.sg_fHe1_0 = ctx->cfg.fHe1_0;
   d.sg_temp0 = ctx->cfg.temp_0;
+  if (t->ifront && !d.ifront) {
+    // init_rt with ifront = TRUE (rt_funcs.cc:49-69): no cell passed by a front, neutral_flag set
+    const size_t NC = (size_t)d.ncell_total, L = (size_t)d.lit_cap;
+    const long long XC = (long long)d.ray_cap * d.PL;
+    if ((st = dalloc(ctx, &d.fion, NC)) || (st = dalloc(ctx, &d.fion_max, NC)) || (st = dalloc(ctx, &d.tcross, NC)) ||
+        (st = dalloc(ctx, &d.tcross_new, NC * 10)) || (st = dalloc(ctx, &d.delta_fion, NC)) ||
+        (st = dalloc(ctx, &d.treion_out, NC)) || (st = dalloc(ctx, &d.tcross_bits, NC)) ||
+        (st = dalloc(ctx, &d.if_flags, NC)) || (st = dalloc(ctx, &d.l_fion, L)) || (st = dalloc(ctx, &d.l_free, L)) ||
+        (st = dalloc(ctx, &d.l_ng3, 3 * L)) || (st = dalloc(ctx, &d.if_cnt, L)) || (st = dalloc(ctx, &d.if_off, L)) ||
+        (st = dalloc(ctx, &d.if_fill, L)) || (st = dalloc(ctx, &d.if_list, (size_t)XC)) ||
+        (st = dalloc(ctx, &d.xs_q, (size_t)XC)) || (st = dalloc(ctx, &d.xs_S, (size_t)XC)) ||
+        (st = dalloc(ctx, &d.xs_E, (size_t)XC * d.F)) || (st = dalloc(ctx, &d.xs_reach, (size_t)XC)) ||
+        (st = dalloc(ctx, &d.ord_cnt, (size_t)d.ray_cap / 256 + 1)) ||
+        (st = dalloc(ctx, &d.ord_off, (size_t)d.ray_cap / 256 + 1)))
+      return st;
+    CK(cudaMemset(d.fion, 0, sizeof(float) * NC));
+    CK(cudaMemset(d.fion_max, 0, sizeof(float) * NC));
+    CK(cudaMemset(d.tcross, 0, sizeof(float) * NC));
+    CK(cudaMemset(d.tcross_new, 0, sizeof(float) * NC * 10));
+    CK(cudaMemset(d.delta_fion, 0, sizeof(float) * NC));
+    CK(cudaMemset(d.treion_out, 0, sizeof(float) * NC));
+    CK(cudaMemset(d.tcross_bits, 0, sizeof(uint16_t) * NC));
+    CK(cudaMemset(d.if_flags, 2, NC));   // neutral_flag
+    if (!ctx->h_flag) CK(cudaMallocHost(&ctx->h_flag, sizeof(int)));
+    d.xs_cap = XC;
+    d.ifront = 1;
+    d.ordered = 1;
+  }
   if (!d.mfp && (st = dalloc(ctx, &d.mfp, (size_t)d.ncell_total))) return st;
   if (!d.l_mfp && (st = dalloc(ctx, &d.l_mfp, (size_t)d.lit_cap))) return st;
   if (!d.rho) {   // the model reads rho / <rho> of every ionised cell
@@ -1178,6 +1282,7 @@ frt_status frt_step_plain(frt_ctx* ctx, const uint16_t* itheta_per_box, const ui
 frt_status frt_step(frt_ctx* ctx, const uint16_t* itheta_per_box, const uint16_t* itheta_per_source,
                     frt_step_stats* stats) {
   if (!ctx) return FRT_ERR_INVALID;
+  if (ctx->d.ifront) return frt_step_plain(ctx, itheta_per_box, itheta_per_source, stats);   // host-driven rounds
   frt_status st = step_inputs(ctx, itheta_per_box, itheta_per_source);
   if (st) return st;
   if (ctx->tune_auto) follow_tune_cache(ctx);

@@ -26,10 +26,12 @@ __device__ __forceinline__ bool ray_moves(const BoxP& B, float x0, float y0, flo
 // Walk c_sim * deltat from (x0, y0, z0) in cell (in, jn, kn): calls seg(p, global cell, dist)
 // for each path segment in order and returns their number, or -1 when more than PL segments
 // would be needed. On return x0..z0 and in..kn hold the end position and cell, with the
-// reference's corner nudges applied.
+// reference's corner nudges applied. With I-front tracking (fion not null) the last segment in a
+// cell the fronts have not fully passed is the whole crossing of the cell (ray_tracing.cc:1425-1437).
 template <typename SegFn>
 __device__ __forceinline__ int dda_walk(const BoxP& B, int PL, float xhat, float yhat, float zhat, float deltat,
-                                        float& x0, float& y0, float& z0, int& in, int& jn, int& kn, SegFn seg) {
+                                        float& x0, float& y0, float& z0, int& in, int& jn, int& kn, SegFn seg,
+                                        const float* fion = nullptr) {
   const int N = B.n;
   const float clgt = B.clight;
   const float dxc = B.dx;
@@ -79,9 +81,11 @@ __device__ __forceinline__ int dda_walk(const BoxP& B, int PL, float xhat, float
     }
     tlast += tmin;
   }
-  dist = (deltat - tlast + tmin) * clgt;
+  const long long gc_last = B.cell0 + (long long)in * B.nn + jn * N + kn;
+  if (fion && fion[gc_last] < 1.f) dist = tmin * clgt;
+  else dist = (deltat - tlast + tmin) * clgt;
   dist = (B.lo_edge >= dist) ? B.lo_edge : dist;   // maxd(dist, min_dist*dx)
-  seg(p, B.cell0 + (long long)in * B.nn + jn * N + kn, dist);
+  seg(p, gc_last, dist);
   x0 += dist * xhat;
   y0 += dist * yhat;
   z0 += dist * zhat;

@@ -338,7 +338,8 @@ __global__ void __launch_bounds__(T) k_advance(Dev d, int r_begin, int r_end) {
                               [&](int p, long long gc, float ds) {
                                 sp[p] = make_int2((int)gc, __float_as_int(ds));
                                 mark_lit(d, gc);
-                              });
+                              },
+                              d.ifront ? d.fion : nullptr);
       if (ns < 0) {
         atomicOr(&d.ctl->err, ERR_PATH);
         s_nseg[j] = 0;   // the record is left as it was and the ray flagged
@@ -715,6 +716,13 @@ __global__ void k_merge_final(Dev d, double pi_sf_3, double log4) {
 // live ray is written by its own thread from registers; a split ray parks its record in shared
 // memory and the block's threads then build the children, four per split ray, spread over all
 // threads so that the child arithmetic (pixel table, rotation, wrap) runs at full width.
+// MODE 0: each block of 256 rays places its outputs at a base taken with one atomicAdd (live rays
+// and the children of split rays interleaved in ray order inside the block). MODE 1 only counts
+// each block's live and split rays (ord_cnt); k_order_scan turns the counts into offsets; MODE 2
+// then writes the live rays in pool order followed by the children in the order of their parents
+// (the order the reference's slots take them in: split_rays appends children after the rays it
+// keeps, rt_funcs.cc:211-237), which the I-front photon budget needs.
+template <int MODE>
 __global__ void __launch_bounds__(256) k_compact_split(Dev d, int r_begin, int r_end) {
   __shared__ int s_cell[256], s_pixel[256], s_dst[256];
   __shared__ float s_xh[256], s_yh[256], s_zh[256], s_r[256], s_x[256], s_y[256], s_z[256], s_time[256];
@@ -764,9 +772,10 @@ __global__ void __launch_bounds__(256) k_compact_split(Dev d, int r_begin, int r
       const BoxP& B = d.box[bx];
       split = (r > B.rmax[order]) && (order < kLmax) && (sum > B.split_thr);
     }
-    // one block-wide exclusive scan: slots (low 16 bits, at most 1024) and split rank (high bits)
+    // one block-wide exclusive scan: slots (low 16 bits, at most 1024) and split rank (high bits);
+    // in the ordered modes the low bits count the live rays that are not split
     const int want = live ? (split ? 4 : 1) : 0;
-    const int key = want | ((split ? 1 : 0) << 16);
+    const int key = (MODE == 0 ? want : ((live && !split) ? 1 : 0)) | ((split ? 1 : 0) << 16);
     int incl = key;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -785,16 +794,27 @@ __global__ void __launch_bounds__(256) k_compact_split(Dev d, int r_begin, int r
       if (lane < 8) s_wt[lane] = v;   // inclusive prefix over the warps
       if (lane == 7) {
         s_tot = v;
-        const int slots = v & 0xffff;
-        s_base = (slots > 0) ? atomicAdd(&d.ctl->nray[nxt], slots) : 0;
+        if (MODE == 0) {
+          const int slots = v & 0xffff;
+          s_base = (slots > 0) ? atomicAdd(&d.ctl->nray[nxt], slots) : 0;
+        } else if (MODE == 1) {
+          d.ord_cnt[(i0 - r_begin) >> 8] = make_int2(v & 0xffff, v >> 16);
+        }
       }
     }
     __syncthreads();
+    if (MODE == 1) continue;   // (uniform over the block)
     const int excl = (w > 0 ? s_wt[w - 1] : 0) + incl - key;
-    const int base = s_base;
     const int nsp = s_tot >> 16;
-    if (t == 0 && (long long)base + (s_tot & 0xffff) > (long long)cap) atomicOr(&d.ctl->err, ERR_RAY_CAP);
-    const int j = base + (excl & 0xffff);
+    int j;
+    if (MODE == 0) {
+      const int base = s_base;
+      if (t == 0 && (long long)base + (s_tot & 0xffff) > (long long)cap) atomicOr(&d.ctl->err, ERR_RAY_CAP);
+      j = base + (excl & 0xffff);
+    } else {
+      const int2 off = d.ord_off[(i0 - r_begin) >> 8];
+      j = split ? d.ctl->ord_surv + 4 * (off.y + (excl >> 16)) : off.x + (excl & 0xffff);
+    }
     if (live && !split) {
       // a live ray: copied by its own thread
       if (j < cap) {
@@ -900,6 +920,58 @@ __global__ void __launch_bounds__(256) k_compact_split(Dev d, int r_begin, int r
   }
 }
 
+// Offsets of the ordered compaction (k_compact_split<1> counts per block of 256 rays): exclusive
+// prefixes of the live and of the split rays over the blocks in pool order; the live rays fill
+// the front of the next pool and the children follow them.
+__global__ void __launch_bounds__(1024) k_order_scan(Dev d) {
+  __shared__ int2 wsum[32];
+  __shared__ int2 base_s;
+  const int cur = d.ctl->cur, nxt = cur ^ 1;
+  const long long nchunk = ((long long)d.ctl->nray[cur] + 255) >> 8;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) base_s = make_int2(0, 0);
+  __syncthreads();
+  for (long long c0 = 0; c0 < nchunk; c0 += blockDim.x) {
+    const long long c = c0 + threadIdx.x;
+    const int2 v = (c < nchunk) ? d.ord_cnt[c] : make_int2(0, 0);
+    int2 incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int ax = __shfl_up_sync(0xffffffffu, incl.x, o), ay = __shfl_up_sync(0xffffffffu, incl.y, o);
+      if (lane >= o) {
+        incl.x += ax;
+        incl.y += ay;
+      }
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      int2 u = wsum[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const int ax = __shfl_up_sync(0xffffffffu, u.x, o), ay = __shfl_up_sync(0xffffffffu, u.y, o);
+        if (lane >= o) {
+          u.x += ax;
+          u.y += ay;
+        }
+      }
+      wsum[lane] = u;   // inclusive prefix over the warps
+    }
+    __syncthreads();
+    if (c < nchunk) {
+      const int2 pre = (w > 0) ? wsum[w - 1] : make_int2(0, 0);
+      d.ord_off[c] = make_int2(base_s.x + pre.x + incl.x - v.x, base_s.y + pre.y + incl.y - v.y);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) base_s = make_int2(base_s.x + wsum[31].x, base_s.y + wsum[31].y);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const long long tot = (long long)base_s.x + 4ll * base_s.y;
+    if (tot > d.ray_cap) atomicOr(&d.ctl->err, ERR_RAY_CAP);
+    d.ctl->ord_surv = base_s.x;
+    d.ctl->nray[nxt] = (int)min(tot, (long long)d.ray_cap);
+  }
+}
+
 __global__ void k_swap(Dev d) {
   Ctl* c = d.ctl;
   const int nxt = c->cur ^ 1;
@@ -911,6 +983,63 @@ __global__ void k_swap(Dev d) {
 
 // new_rays -> init_rays (rt_funcs.cc:240-261, ray_tracing.cc:230-321): 12 Nside^2 rays per source
 // at the cell centre, directions of the NEST pixels rotated by the source's random angles.
+// The ray count of a source's cast (init_rays, ray_tracing.cc:230-245): 12 rays at the base order,
+// or 12 nside^2 at the source level lsource when the source cell is no longer neutral.
+__device__ __forceinline__ int cast_count(const Dev& d, int s, int* nside_out, int* lpix_out) {
+  if (d.src_own && !d.src_own[s]) return 0;   // another context casts this source
+  const BoxP& B = d.box[d.src_box[s]];
+  const long long gc = B.cell0 + d.src_cell[s];
+  int nside = 1, lpix = 0;
+  if (!(d.nH1[gc] / d.nH[gc] > 0.1)) {
+    nside = 1 << B.lsource;
+    lpix = B.lsource;
+  }
+  *nside_out = nside;
+  *lpix_out = lpix;
+  return 12 * nside * nside;
+}
+
+// The pool positions of the step's new rays: sources in order, each source's rays together in
+// pixel order after the live rays (the order new_rays appends them in, rt_funcs.cc:240-261). One
+// block scans the sources' ray counts.
+__global__ void __launch_bounds__(1024) k_cast_offsets(Dev d) {
+  __shared__ int wsum[32];
+  __shared__ int base_s;
+  const int cur = d.ctl->cur;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) base_s = d.ctl->nray[cur];
+  __syncthreads();
+  for (int s0 = 0; s0 < d.nsrc; s0 += blockDim.x) {
+    const int s = s0 + threadIdx.x;
+    int nside = 1, lpix = 0;
+    const int cnt = (s < d.nsrc) ? cast_count(d, s, &nside, &lpix) : 0;
+    int incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      int v = (lane < (int)(blockDim.x >> 5)) ? wsum[lane] : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+      }
+      wsum[lane] = v;   // inclusive prefix over the warps
+    }
+    __syncthreads();
+    if (s < d.nsrc) d.src_pos[s] = base_s + (w > 0 ? wsum[w - 1] : 0) + incl - cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) base_s += wsum[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (base_s > d.ray_cap) atomicOr(&d.ctl->err, ERR_RAY_CAP);
+    d.ctl->nray[cur] = min(base_s, d.ray_cap);
+  }
+}
+
 __global__ void k_cast(Dev d, int s_begin, int s_end) {
   const int cur = d.ctl->cur;
   const RayPool A = d.pool[cur];
@@ -918,22 +1047,14 @@ __global__ void k_cast(Dev d, int s_begin, int s_end) {
   long long ncast = 0;
   double emitted = 0.0;
   for (int s = s_begin + blockIdx.x * blockDim.x + threadIdx.x; s < s_end; s += gridDim.x * blockDim.x) {
-    if (d.src_own && !d.src_own[s]) continue;   // another context casts this source
+    int nside = 1, lpix = 0;
+    const int count = cast_count(d, s, &nside, &lpix);
+    if (count == 0) continue;
     const int b = d.src_box[s];
     const BoxP& B = d.box[b];
     const int c = d.src_cell[s];
-    const long long gc = B.cell0 + c;
-    int nside = 1, lpix = 0;
-    if (!(d.nH1[gc] / d.nH[gc] > 0.1)) {
-      nside = 1 << B.lsource;
-      lpix = B.lsource;
-    }
-    const int count = 12 * nside * nside;
-    const int pos = atomicAdd(&d.ctl->nray[cur], count);
-    if (pos + count > cap) {
-      atomicOr(&d.ctl->err, ERR_RAY_CAP);
-      continue;
-    }
+    const int pos = d.src_pos[s];   // k_cast_offsets
+    if (pos + count > cap) continue;   // (k_cast_offsets flagged the overflow)
     const uint16_t ith = d.src_itheta[s];
     const float* m = d.rot + (size_t)ith * 18;
     const double lum = d.src_lum[s];
@@ -1142,21 +1263,31 @@ void launch_merge(const Dev& d, int grid, cudaStream_t s) {
 }
 
 void launch_split_compact(const Dev& d, int grid, cudaStream_t s) {
-  k_compact_split<<<grid, 256, 0, s>>>(d, 0, INT_MAX);
+  if (d.ordered) {
+    k_compact_split<1><<<grid, 256, 0, s>>>(d, 0, INT_MAX);
+    k_order_scan<<<1, 1024, 0, s>>>(d);
+    k_compact_split<2><<<grid, 256, 0, s>>>(d, 0, INT_MAX);
+  } else {
+    k_compact_split<0><<<grid, 256, 0, s>>>(d, 0, INT_MAX);
+  }
   k_swap<<<1, 1, 0, s>>>(d);
 }
 
 void launch_split_range(const Dev& d, int grid, int r_begin, int r_end, cudaStream_t s) {
-  k_compact_split<<<grid, 256, 0, s>>>(d, r_begin, r_end);
+  k_compact_split<0><<<grid, 256, 0, s>>>(d, r_begin, r_end);
 }
 
 void launch_swap(const Dev& d, cudaStream_t s) { k_swap<<<1, 1, 0, s>>>(d); }
 
 void launch_cast(const Dev& d, cudaStream_t s) {
-  if (d.nsrc > 0) k_cast<<<grid_for(d.nsrc, 128, 4096), 128, 0, s>>>(d, 0, d.nsrc);
+  if (d.nsrc > 0) {
+    k_cast_offsets<<<1, 1024, 0, s>>>(d);
+    k_cast<<<grid_for(d.nsrc, 128, 4096), 128, 0, s>>>(d, 0, d.nsrc);
+  }
 }
 
 void launch_cast_per_source(const Dev& d, cudaStream_t s) {
+  if (d.nsrc > 0) k_cast_offsets<<<1, 1024, 0, s>>>(d);
   for (int src = 0; src < d.nsrc; src++) k_cast<<<1, 32, 0, s>>>(d, src, src + 1);
 }
 

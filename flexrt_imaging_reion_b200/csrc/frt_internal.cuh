@@ -43,6 +43,8 @@ struct Ctl {
   // moved rays this step (high 32 bits) and their segments (low 32 bits), counted together so
   // that one atomicAdd gives a block both bases (k_moved_pack)
   unsigned long long mv_seg;
+  int ord_surv;            // live rays kept by the ordered compaction (k_order_scan)
+  int if_changed;          // I-front budget: some crossing's entry sum changed in the last round
   long long rays_moved, crossings, split, merged, killed, cast;
   double emitted, deposited, killed_ph, overlap, in_flight;
 };
@@ -114,6 +116,7 @@ struct Dev {
   float* src_ray_dt;
   uint16_t* src_itheta;
   uint8_t* src_own;          // null, or 1 for the sources this context casts (a share of a box's sources)
+  int* src_pos;              // pool position of a source's first new ray this step (k_cast_offsets)
   // control
   Ctl* ctl;
   int* rp_queue;           // [kMaxIterQueue] ray-pass work counters, one per C2Ray iteration (chunked queue)
@@ -123,8 +126,32 @@ struct Dev {
   int subgrid;
   const float *sg_time, *sg_fh1, *sg_tdnl, *sg_ds, *sg_dnl;
   float sg_tinit, sg_t12, sg_t8, sg_tcap, sg_tre_dom[3];
-  float sg_fH1_0, sg_temp0;   // the HI-fraction cap of interp_nh1 and the neutral gas temperature
+  float sg_fH1_0, sg_fHe1_0, sg_temp0;   // initial neutral fractions (interp_nh1's cap) and the neutral gas temperature
   float* l_mfp;
+  // pool order: with `ordered` the compaction keeps the reference's slot order (live rays in
+  // order, then the children in the order of their parents; k_compact_split<1,2>)
+  int ordered;
+  int2 *ord_cnt, *ord_off;   // per block of 256 pool rays: (live, split) counts and offsets
+  // I-front tracking (ifront = TRUE; frt_ifront.cu): the fraction of each cell the fronts have
+  // passed and its maximum, the crossing times (total, per tenth of the cell, with the tenths
+  // passed as bits), the tcross / neutral flags (bits 0 / 1), the last step's change of fion,
+  // the time the cell passed half-ionised; per lit cell fion at the step's start, the atoms of
+  // its neutral part and the photon counts of the iteration ([3][lit_cap]: absorbed by the
+  // neutral part, the same times sigma_eff_rh times path, entering the neutral part); the
+  // budget cells' crossings in ray order (CSR over lit slots); per packed segment its moved ray,
+  // the absorbed sum it found on entry, the photons entering the neutral part per bin
+  // ([F][ray_cap * PL]) and whether the ray reached it
+  int ifront;
+  float *fion, *fion_max, *tcross, *tcross_new, *delta_fion, *treion_out;
+  uint16_t* tcross_bits;
+  uint8_t* if_flags;
+  float* l_fion;
+  double *l_free, *l_ng3;
+  int *if_cnt, *if_off, *if_fill, *if_list;
+  int* xs_q;
+  double *xs_S, *xs_E;
+  uint8_t* xs_reach;
+  long long xs_cap;
 };
 
 constexpr int kMaxIterQueue = 16;
@@ -212,6 +239,9 @@ void launch_sg_raypass(const Dev& d, int iter, int grid, cudaStream_t s);
 void launch_sg_litpass(const Dev& d, int iter, bool fused_thermal, int grid, cudaStream_t s);
 void launch_sg_dark(const Dev& d, bool fused_thermal, int grid, cudaStream_t s);
 void launch_sg_thermal_all(const Dev& d, int grid, cudaStream_t s);
+void launch_if_lists(const Dev& d, int grid, cudaStream_t s);              // front cells' crossings in ray order
+void launch_if_round(const Dev& d, int iter, int grid, cudaStream_t s);    // ray pass + budget pass
+void launch_if_final(const Dev& d, int iter, int grid, cudaStream_t s);    // the last iteration's ray updates
 // ---- adjoint (frt_adjoint.cu) --------------------------------------------------------
 void launch_adjoint(const Dev& d, const AdjDev& a, int grid, cudaStream_t s);
 void launch_adjoint_gather(const Dev& d, const AdjDev& a, long long cell0, long long ncell, float* out,

@@ -238,10 +238,11 @@ class RTContext:
         self._check(self.L.frt_update_cosmo_expansion(self.h, ac.ctypes.data, ap.ctypes.data),
                     "frt_update_cosmo_expansion")
 
-    def set_subgrid(self, tables, consts) -> None:
-        """frt_set_subgrid: the sub-grid RadHydro model from here on. `tables` holds the reference's
-        in-memory arrays ("time", "fh1": Nt*27+1 floats; "t_dnl", "ds": 500; "dnl": 500*500),
-        `consts` the cosmic times (tinit, t(z=12), t(z=8), t(z=5.5), tre_dom[0..2])."""
+    def set_subgrid(self, tables, consts, ifront: bool = False) -> None:
+        """frt_set_subgrid: the sub-grid RadHydro model from here on, with I-front tracking when
+        `ifront`. `tables` holds the reference's in-memory arrays ("time", "fh1": Nt*27+1 floats;
+        "t_dnl", "ds": 500; "dnl": 500*500), `consts` the cosmic times (tinit, t(z=12), t(z=8),
+        t(z=5.5), tre_dom[0..2])."""
         keep = {k: np.ascontiguousarray(tables[k], np.float32) for k in ("time", "fh1", "t_dnl", "ds", "dnl")}
         t = _abi.SubgridTables()
         t.time_RH, t.fh1_RH = keep["time"].ctypes.data, keep["fh1"].ctypes.data
@@ -250,6 +251,7 @@ class RTContext:
         t.tinit, t.t_z12, t.t_z8, t.t_z55 = c[0], c[1], c[2], c[3]
         for k in range(3):
             t.tre_dom[k] = c[4 + k]
+        t.ifront = 1 if ifront else 0
         self._check(self.L.frt_set_subgrid(self.h, C.byref(t)), "frt_set_subgrid")
 
     def hydro_step(self, box: int, snap: W.BoxInputs, a_rt: float, dt_snap: float, zz: float) -> None:
@@ -403,7 +405,7 @@ class RTContext:
     # ---- state access --------------------------------------------------------------------------------
     def get_field(self, box: int, name: str) -> np.ndarray:
         n = self.specs[box].n
-        shape = (n ** 3, self.F) if name in _abi.PER_BIN_FIELDS else (n ** 3,)
+        shape = (n ** 3, self.F) if name in _abi.PER_BIN_FIELDS else ((n ** 3, 10) if name == "TCROSS_NEW" else (n ** 3,))
         out = np.zeros(shape, np.float32)
         self._check(self.L.frt_get_field(self.h, box, _abi.FIELD_ID[name], out.ctypes.data), f"get_field {name}")
         return out

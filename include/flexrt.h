@@ -87,6 +87,12 @@ typedef enum {
   FRT_F_TREION_FLAG /* as float 0/1 */, FRT_F_DNE_DT, FRT_F_RECOMB_H2, FRT_F_RECOMB_HE2, FRT_F_RECRATE_H2,
   FRT_F_RECRATE_HE2, FRT_F_MFP, FRT_F_MFP_912, FRT_F_IF_SPEED, FRT_F_INC_FLUX,
   FRT_F_GAMMA_H1_NU, FRT_F_GAMMA_HE1_NU, FRT_F_NGAM_NU, FRT_F_U_NU,
+  /* I-front tracking (frt_set_subgrid with ifront): the fraction of the cell the fronts passed, its
+   * maximum, the crossing time, the last step's change of fion, the time the cell passed
+   * half-ionised, tcross_flag and neutral_flag (as float 0/1), and the crossing times of the
+   * tenths of the cell ([ncell][10]) */
+  FRT_F_FION, FRT_F_FION_MAX, FRT_F_TCROSS, FRT_F_DELTA_FION, FRT_F_TREION_OUT, FRT_F_TCROSS_FLAG,
+  FRT_F_NEUTRAL_FLAG, FRT_F_TCROSS_NEW,
   FRT_F_COUNT
 } frt_field;
 
@@ -157,8 +163,8 @@ frt_status frt_update_cosmo_expansion(frt_ctx* ctx, const float* a_current, cons
  * list replaces the old one (an owner mask, frt_set_source_owner, is cleared). */
 frt_status frt_update_hydro_step(frt_ctx* ctx, int box, const float* delta1, float a_rt, float dt_snap, float zz,
                                  int nsrc, const int32_t* ijk, const double* lum);
-/* The sub-grid RadHydro model of the reference (subgrid = TRUE with equilibrium = TRUE and
- * ifront = FALSE, user_inputs.h:11-15): photo-ionisation equilibrium mean free paths in ionised
+/* The sub-grid RadHydro model of the reference (subgrid = TRUE with equilibrium = TRUE,
+ * user_inputs.h:11-15), with or without I-front tracking: photo-ionisation equilibrium mean free paths in ionised
  * cells, HI fractions interpolated in the RadHydro tables (get_gamma_interp / interp_nh1,
  * subgrid.cc:257-647), the sub-grid ray deposition (ray_tracing.cc:764-856) and heating / cooling
  * (gas_funcs.cc:134-242, 362-418). Call after the gas set-up and the set-up cast, as main.cc:86-90
@@ -166,10 +172,15 @@ frt_status frt_update_hydro_step(frt_ctx* ctx, int box, const float* delta1, flo
  * arrays after import_subgrid_file / import_delta_over_sigma_table (subgrid.cc:20-95): time_RH and
  * fh1_RH in its [Nt][3][3][3] layout, filled at the gamma index q + 1 (Nt * 27 + 1 floats with the
  * last row's spill), times in s; the cosmic times are the reference's cosmic_time() at zinit,
- * z = 12, 8, 5.5 and at the three RadHydro reionisation redshifts. Without I-front tracking the
- * result of a ray pass does not depend on the order of the rays (no per-cell photon budget, the
- * neutral-absorption block ray_tracing.cc:867-919 never runs). The phased step, the autotuner and
- * the adjoint stay with the plain model (FRT_ERR_INVALID / FRT_ERR_STATE). */
+ * z = 12, 8, 5.5 and at the three RadHydro reionisation redshifts. With ifront != 0 (the
+ * reference's default, user_inputs.h:11) every cell starts with no front passed (fion = 0,
+ * rt_funcs.cc:49-69) and the neutral part of a cell absorbs the photons of the rays that reach it
+ * in the order of the reference's ray slots, up to its atoms (ray_tracing.cc:863-919); the fronts
+ * then advance by update_fion (subgrid.cc:694-751). The context then keeps its rays in that order
+ * and resolves the order-dependent absorption by rounds that run to a fixed point; frt_step runs
+ * its kernels without a graph. A step whose budgets do not settle returns FRT_ERR_STATE. The
+ * phased step, the autotuner and the adjoint stay with the plain model (FRT_ERR_INVALID /
+ * FRT_ERR_STATE). */
 #define FRT_SUBGRID_NT 5000
 #define FRT_SUBGRID_NDLIN 500
 typedef struct {
@@ -180,6 +191,7 @@ typedef struct {
   const float* deltaNL;            /* FRT_SUBGRID_NDLIN x FRT_SUBGRID_NDLIN, one row per time */
   float tinit, t_z12, t_z8, t_z55; /* cosmic_time at zinit, z = 12, 8, 5.5 */
   float tre_dom[3];                /* cosmic_time at z = 12, 8, 6 (init_radhydro_data, subgrid.cc:176-178) */
+  int ifront;                      /* I-front tracking (ifront = TRUE) */
 } frt_subgrid_tables;
 frt_status frt_set_subgrid(frt_ctx* ctx, const frt_subgrid_tables* tables);
 /* get_nphot_min_max (ray_tracing.cc:129-154) */

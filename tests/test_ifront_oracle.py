@@ -64,6 +64,10 @@ def test_ifront_matches_reference():
             b = _sorted_rays(G, pre)
             for k in a:
                 np.testing.assert_array_equal(a[k], b[k], err_msg=f"step {s} rays {k}")
+            # the order itself: the oracle's rays in creation order are the reference's slots in
+            # order (the order the photon budgets are drawn in)
+            for k in ("ray_cell", "ray_pixel", "ray_order", "ray_itheta"):
+                np.testing.assert_array_equal(d[k], G[pre + k], err_msg=f"step {s} ray order {k}")
     o.close()
     # the fronts were tracked: cells part-way ionised, crossing times booked, rays absorbed
     f = G["s8_fion"]
