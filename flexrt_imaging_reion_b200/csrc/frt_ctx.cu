@@ -93,13 +93,28 @@ namespace {
     }                                                                                  \
   } while (0)
 
+// Copies and fills on the step stream. The library's streams are non-blocking, so they do not
+// wait for the legacy default stream: a plain cudaMemcpy from pageable memory or a cudaMemset
+// may still be in flight when a kernel on s_main reads the buffer. Each helper returns once the
+// operation has completed, in order with the work already queued on s_main.
+cudaError_t copy_sync(frt_ctx* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, ctx->s_main);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(ctx->s_main);
+}
+cudaError_t fill_sync(frt_ctx* ctx, void* dst, int value, size_t bytes) {
+  cudaError_t e = cudaMemsetAsync(dst, value, bytes, ctx->s_main);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(ctx->s_main);
+}
+
 template <typename T>
 frt_status dalloc(frt_ctx* ctx, T** p, size_t n) {
   *p = nullptr;
   if (n == 0) return FRT_OK;
   void* q = nullptr;
   CK(cudaMalloc(&q, n * sizeof(T)));
-  CK(cudaMemset(q, 0, n * sizeof(T)));
+  CK(fill_sync(ctx, q, 0, n * sizeof(T)));
   ctx->allocs.push_back(q);
   *p = (T*)q;
   return FRT_OK;
@@ -112,11 +127,11 @@ frt_status dalloc(frt_ctx* ctx, T** p, size_t n) {
   } while (0)
 
 frt_status upload_boxes(frt_ctx* ctx) {
-  CK(cudaMemcpy(ctx->d.box, ctx->hbox.data(), sizeof(BoxP) * ctx->hbox.size(), cudaMemcpyHostToDevice));
+  CK(copy_sync(ctx, ctx->d.box, ctx->hbox.data(), sizeof(BoxP) * ctx->hbox.size(), cudaMemcpyHostToDevice));
   return FRT_OK;
 }
 frt_status download_boxes(frt_ctx* ctx) {
-  CK(cudaMemcpy(ctx->hbox.data(), ctx->d.box, sizeof(BoxP) * ctx->hbox.size(), cudaMemcpyDeviceToHost));
+  CK(copy_sync(ctx, ctx->hbox.data(), ctx->d.box, sizeof(BoxP) * ctx->hbox.size(), cudaMemcpyDeviceToHost));
   return FRT_OK;
 }
 
@@ -133,7 +148,7 @@ frt_status sync_and_check(frt_ctx* ctx) {
   CK(cudaStreamSynchronize(ctx->s_dark));
   CK(cudaGetLastError());
   Ctl c;
-  CK(cudaMemcpy(&c, ctx->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+  CK(copy_sync(ctx, &c, ctx->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
   if (c.err) {
     ctx->err = "device error flags " + std::to_string(c.err) +
                " (1 ray pool full, 2 path_length exceeded, 4 lit-cell list full)";
@@ -167,10 +182,10 @@ frt_status upload_sources(frt_ctx* ctx) {
   ctx->d.src_own = nullptr;
   ctx->adj_src_stale = true;
   if (n) {
-    CK(cudaMemcpy(ctx->d.src_cell, cell.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d.src_box, box.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d.src_lum, lum.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d.src_ray_dt, rdt.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, ctx->d.src_cell, cell.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, ctx->d.src_box, box.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, ctx->d.src_lum, lum.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, ctx->d.src_ray_dt, rdt.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
   }
   ctx->graph_valid = false;
   return FRT_OK;
@@ -497,7 +512,7 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
     host::rotation_table(ctx->rot.data());
     float* r = nullptr;
     AL(r, ctx->rot.size());
-    CK(cudaMemcpy(r, ctx->rot.data(), sizeof(float) * ctx->rot.size(), cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, r, ctx->rot.data(), sizeof(float) * ctx->rot.size(), cudaMemcpyHostToDevice));
     d.rot = r;
     float4* pt = nullptr;
     AL(pt, (size_t)pix_tab_offset(kPixTabMax + 1));
@@ -512,7 +527,7 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
       for (long long t = t0; t < t0 + nt; t++) tb[t] = (int16_t)b;
     }
     AL(d.tile_box, d.ntile);
-    CK(cudaMemcpy(d.tile_box, tb.data(), sizeof(int16_t) * d.ntile, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, d.tile_box, tb.data(), sizeof(int16_t) * d.ntile, cudaMemcpyHostToDevice));
   }
   const size_t NC = (size_t)off;
   AL(d.nH, NC); AL(d.nHe, NC); AL(d.nH1, NC); AL(d.nHe1, NC); AL(d.f_H1, NC); AL(d.f_He1, NC);
@@ -634,15 +649,15 @@ frt_status frt_init_gas(frt_ctx* ctx, int box, const float* delta1) {
   Dev& d = ctx->d;
   const size_t o = (size_t)B.cell0;
   auto up = [&](float* dst, const std::vector<float>& src) {
-    return cudaMemcpy(dst + o, src.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+    return copy_sync(ctx, dst + o, src.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
   };
   CK(up(d.nH, nH)); CK(up(d.nHe, nHe)); CK(up(d.nH1, nH1)); CK(up(d.nHe1, nHe1)); CK(up(d.f_H1, fH1));
   CK(up(d.f_He1, fHe1)); CK(up(d.temp, temp)); CK(up(d.ne, ne)); CK(up(d.avg_nh1, nH1)); CK(up(d.avg_nhe1, nHe1));
   CK(up(d.n_tot, ntot)); CK(up(d.dne_dt, dne)); CK(up(d.nH1_prev, nH1));
-  CK(cudaMemset(d.heat + o, 0, sizeof(float) * n));
-  CK(cudaMemset(d.cool + o, 0, sizeof(float) * n));
-  CK(cudaMemset(d.treion + o, 0, sizeof(float) * n));
-  CK(cudaMemset(d.treion_flag + o, 0, n));
+  CK(fill_sync(ctx, d.heat + o, 0, sizeof(float) * n));
+  CK(fill_sync(ctx, d.cool + o, 0, sizeof(float) * n));
+  CK(fill_sync(ctx, d.treion + o, 0, sizeof(float) * n));
+  CK(fill_sync(ctx, d.treion_flag + o, 0, n));
   if (d.rec_h2) {
     CK(up(d.rec_h2, rh));
     CK(up(d.rec_he2, rhe));
@@ -688,15 +703,15 @@ frt_status frt_set_clump_field(frt_ctx* ctx, int box, const float* clump) {
     AL(d.clump, (size_t)d.ncell_total);
     // cells of other boxes keep the constant
     std::vector<float> c(d.ncell_total, ctx->cfg.const_clump);
-    CK(cudaMemcpy(d.clump, c.data(), sizeof(float) * c.size(), cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, d.clump, c.data(), sizeof(float) * c.size(), cudaMemcpyHostToDevice));
     ctx->graph_valid = false;
   }
   const BoxP& B = ctx->hbox[box];
   if (clump) {
-    CK(cudaMemcpy(d.clump + B.cell0, clump, sizeof(float) * B.ncell, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, d.clump + B.cell0, clump, sizeof(float) * B.ncell, cudaMemcpyHostToDevice));
   } else {
     std::vector<float> c(B.ncell, ctx->cfg.const_clump);
-    CK(cudaMemcpy(d.clump + B.cell0, c.data(), sizeof(float) * B.ncell, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, d.clump + B.cell0, c.data(), sizeof(float) * B.ncell, cudaMemcpyHostToDevice));
   }
   return FRT_OK;
 }
@@ -743,7 +758,7 @@ frt_status frt_set_field(frt_ctx* ctx, int box, frt_field f, const float* host) 
     return FRT_ERR_INVALID;
   }
   const BoxP& B = ctx->hbox[box];
-  CK(cudaMemcpy(p + B.cell0, host, sizeof(float) * B.ncell, cudaMemcpyHostToDevice));
+  CK(copy_sync(ctx, p + B.cell0, host, sizeof(float) * B.ncell, cudaMemcpyHostToDevice));
   return FRT_OK;
 }
 
@@ -756,14 +771,14 @@ frt_status frt_get_field(frt_ctx* ctx, int box, frt_field f, float* host) {
   const size_t n = (size_t)B.ncell;
   const int F = d.F;
   auto get = [&](const float* src, float* dst) {
-    return cudaMemcpy(dst, src + B.cell0, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    return copy_sync(ctx, dst, src + B.cell0, sizeof(float) * n, cudaMemcpyDeviceToHost);
   };
   auto sparse = [&](int which, float* dst) -> frt_status {
     float* tmp = nullptr;
     CK(cudaMalloc(&tmp, sizeof(float) * n));
     launch_gather_sparse(d, B.cell0, (long long)n, which, tmp, ctx->s_main);
     CK(cudaStreamSynchronize(ctx->s_main));
-    CK(cudaMemcpy(dst, tmp, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    CK(copy_sync(ctx, dst, tmp, sizeof(float) * n, cudaMemcpyDeviceToHost));
     CK(cudaFree(tmp));
     return FRT_OK;
   };
@@ -802,7 +817,7 @@ frt_status frt_get_field(frt_ctx* ctx, int box, frt_field f, float* host) {
     }
     case FRT_F_TREION_FLAG: {
       std::vector<uint8_t> a(n);
-      CK(cudaMemcpy(a.data(), d.treion_flag + B.cell0, n, cudaMemcpyDeviceToHost));
+      CK(copy_sync(ctx, a.data(), d.treion_flag + B.cell0, n, cudaMemcpyDeviceToHost));
       for (size_t i = 0; i < n; i++) host[i] = a[i] ? 1.f : 0.f;
       return FRT_OK;
     }
@@ -820,13 +835,13 @@ frt_status frt_get_field(frt_ctx* ctx, int box, frt_field f, float* host) {
       }
       if (f == FRT_F_TCROSS_FLAG || f == FRT_F_NEUTRAL_FLAG) {
         std::vector<uint8_t> a(n);
-        CK(cudaMemcpy(a.data(), d.if_flags + B.cell0, n, cudaMemcpyDeviceToHost));
+        CK(copy_sync(ctx, a.data(), d.if_flags + B.cell0, n, cudaMemcpyDeviceToHost));
         const uint8_t bit = (f == FRT_F_TCROSS_FLAG) ? 1 : 2;
         for (size_t i = 0; i < n; i++) host[i] = (a[i] & bit) ? 1.f : 0.f;
         return FRT_OK;
       }
       if (f == FRT_F_TCROSS_NEW) {
-        CK(cudaMemcpy(host, d.tcross_new + (size_t)B.cell0 * 10, sizeof(float) * n * 10, cudaMemcpyDeviceToHost));
+        CK(copy_sync(ctx, host, d.tcross_new + (size_t)B.cell0 * 10, sizeof(float) * n * 10, cudaMemcpyDeviceToHost));
         return FRT_OK;
       }
       const float* src = f == FRT_F_FION ? d.fion : f == FRT_F_FION_MAX ? d.fion_max : f == FRT_F_TCROSS ? d.tcross
@@ -889,11 +904,11 @@ frt_status frt_init_rt(frt_ctx* ctx) {
   for (size_t b = 0; b < ctx->boxes.size(); b++)
     for (size_t s = 0; s < ctx->src_cell[b].size(); s++)
       rdt.push_back(ctx->src_lum[b][s] != 0 && !ctx->restarted[b] ? ctx->hbox[b].dt : 0.f);
-  if (!rdt.empty()) CK(cudaMemcpy(d.src_ray_dt, rdt.data(), sizeof(float) * rdt.size(), cudaMemcpyHostToDevice));
+  if (!rdt.empty()) CK(copy_sync(ctx, d.src_ray_dt, rdt.data(), sizeof(float) * rdt.size(), cudaMemcpyHostToDevice));
   Ctl c;
   memset(&c, 0, sizeof(c));
-  CK(cudaMemcpy(d.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice));
-  CK(cudaMemset(d.lit_flag, 0, (size_t)d.ncell_total));
+  CK(copy_sync(ctx, d.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice));
+  CK(fill_sync(ctx, d.lit_flag, 0, (size_t)d.ncell_total));
   launch_fill_i32(d.lit_slot, -1, d.ncell_total, ctx->s_main);
   CK(cudaStreamSynchronize(ctx->s_main));
   for (size_t b = 0; b < ctx->hbox.size(); b++) {
@@ -919,7 +934,7 @@ frt_status frt_update_cosmo_expansion(frt_ctx* ctx, const float* a_current, cons
     frt_status st = dalloc(ctx, &d.rho, (size_t)d.ncell_total);
     if (st) return st;
     for (size_t b = 0; b < ctx->hbox.size(); b++)
-      CK(cudaMemcpy(d.rho + ctx->hbox[b].cell0, ctx->rho[b].data(), sizeof(float) * ctx->rho[b].size(),
+      CK(copy_sync(ctx, d.rho + ctx->hbox[b].cell0, ctx->rho[b].data(), sizeof(float) * ctx->rho[b].size(),
                     cudaMemcpyHostToDevice));
     if ((st = dalloc(ctx, &d.frac_h2, (size_t)d.ncell_total))) return st;
     if ((st = dalloc(ctx, &d.frac_he2, (size_t)d.ncell_total))) return st;
@@ -969,7 +984,7 @@ frt_status frt_update_hydro_step(frt_ctx* ctx, int box, const float* delta1, flo
     if ((st = dalloc(ctx, &d.rho, (size_t)d.ncell_total))) return st;
     for (size_t b = 0; b < ctx->hbox.size(); b++)
       if (ctx->rho[b].size() == (size_t)ctx->hbox[b].ncell)
-        CK(cudaMemcpy(d.rho + ctx->hbox[b].cell0, ctx->rho[b].data(), sizeof(float) * ctx->rho[b].size(),
+        CK(copy_sync(ctx, d.rho + ctx->hbox[b].cell0, ctx->rho[b].data(), sizeof(float) * ctx->rho[b].size(),
                       cudaMemcpyHostToDevice));
     ctx->graph_valid = false;
   }
@@ -981,7 +996,7 @@ frt_status frt_update_hydro_step(frt_ctx* ctx, int box, const float* delta1, flo
     if ((st = dalloc(ctx, &d.ddelta, (size_t)d.ncell_total))) return st;   // 0 in the other boxes
     ctx->graph_valid = false;
   }
-  CK(cudaMemcpy(d.rho + B.cell0, rho.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  CK(copy_sync(ctx, d.rho + B.cell0, rho.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
   // the box at the new snapshot: redshift, cell size Lx0 a_rt / N (gas_funcs.cc:590-592, 689-691)
   host::set_cell_size(&B, &ctx->cfg, &ctx->boxes[box], host::snapshot_dx(&ctx->boxes[box], a_rt));
   host::set_redshift(&B, zz);
@@ -1020,7 +1035,7 @@ frt_status frt_update_hydro_step(frt_ctx* ctx, int box, const float* delta1, flo
     std::vector<double> lg(2);   // as frt_get_nphot_min_max: log10 nphot_min and the PDF bin width
     lg[0] = log10(mn);
     lg[1] = (log10(mx) - log10(mn)) / (10000 - 1);
-    CK(cudaMemcpy(d.lg + 2 * box, lg.data(), sizeof(double) * 2, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, d.lg + 2 * box, lg.data(), sizeof(double) * 2, cudaMemcpyHostToDevice));
   }
   const float a4 = (float)(4. * (double)B.nphot_merge), c4 = (float)(4. * B.nphot_min);
   B.split_thr = (c4 >= a4) ? c4 : a4;
@@ -1043,7 +1058,7 @@ frt_status frt_set_subgrid(frt_ctx* ctx, const frt_subgrid_tables* t) {
     float* p = nullptr;
     frt_status st = dalloc(ctx, &p, n);
     if (st) return st;
-    CK(cudaMemcpy(p, src, sizeof(float) * n, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, p, src, sizeof(float) * n, cudaMemcpyHostToDevice));
     *dst = p;
     return FRT_OK;
   };
@@ -1075,14 +1090,14 @@ frt_status frt_set_subgrid(frt_ctx* ctx, const frt_subgrid_tables* t) {
         (st = dalloc(ctx, &d.ord_cnt, (size_t)d.ray_cap / 256 + 1)) ||
         (st = dalloc(ctx, &d.ord_off, (size_t)d.ray_cap / 256 + 1)))
       return st;
-    CK(cudaMemset(d.fion, 0, sizeof(float) * NC));
-    CK(cudaMemset(d.fion_max, 0, sizeof(float) * NC));
-    CK(cudaMemset(d.tcross, 0, sizeof(float) * NC));
-    CK(cudaMemset(d.tcross_new, 0, sizeof(float) * NC * 10));
-    CK(cudaMemset(d.delta_fion, 0, sizeof(float) * NC));
-    CK(cudaMemset(d.treion_out, 0, sizeof(float) * NC));
-    CK(cudaMemset(d.tcross_bits, 0, sizeof(uint16_t) * NC));
-    CK(cudaMemset(d.if_flags, 2, NC));   // neutral_flag
+    CK(fill_sync(ctx, d.fion, 0, sizeof(float) * NC));
+    CK(fill_sync(ctx, d.fion_max, 0, sizeof(float) * NC));
+    CK(fill_sync(ctx, d.tcross, 0, sizeof(float) * NC));
+    CK(fill_sync(ctx, d.tcross_new, 0, sizeof(float) * NC * 10));
+    CK(fill_sync(ctx, d.delta_fion, 0, sizeof(float) * NC));
+    CK(fill_sync(ctx, d.treion_out, 0, sizeof(float) * NC));
+    CK(fill_sync(ctx, d.tcross_bits, 0, sizeof(uint16_t) * NC));
+    CK(fill_sync(ctx, d.if_flags, 2, NC));   // neutral_flag
     if (!ctx->h_flag) CK(cudaMallocHost(&ctx->h_flag, sizeof(int)));
     d.xs_cap = XC;
     d.ifront = 1;
@@ -1094,7 +1109,7 @@ frt_status frt_set_subgrid(frt_ctx* ctx, const frt_subgrid_tables* t) {
     if ((st = dalloc(ctx, &d.rho, (size_t)d.ncell_total))) return st;
     for (size_t b = 0; b < ctx->hbox.size(); b++)
       if (ctx->rho[b].size() == (size_t)ctx->hbox[b].ncell)
-        CK(cudaMemcpy(d.rho + ctx->hbox[b].cell0, ctx->rho[b].data(), sizeof(float) * ctx->rho[b].size(),
+        CK(copy_sync(ctx, d.rho + ctx->hbox[b].cell0, ctx->rho[b].data(), sizeof(float) * ctx->rho[b].size(),
                       cudaMemcpyHostToDevice));
   }
   d.subgrid = 1;
@@ -1130,7 +1145,7 @@ frt_status frt_get_nphot_min_max(frt_ctx* ctx, double* nmin_out, double* nmax_ou
     if (nmin_out) nmin_out[b] = mn;
     if (nmax_out) nmax_out[b] = mx;
   }
-  CK(cudaMemcpy(ctx->d.lg, lg.data(), sizeof(double) * lg.size(), cudaMemcpyHostToDevice));
+  CK(copy_sync(ctx, ctx->d.lg, lg.data(), sizeof(double) * lg.size(), cudaMemcpyHostToDevice));
   return upload_boxes(ctx);
 }
 
@@ -1157,7 +1172,7 @@ frt_status frt_count_rays(frt_ctx* ctx, long long* count_per_box) {
   launch_count(ctx->d, ctx->grid_rays, ctx->s_main);
   frt_status st = sync_and_check(ctx);
   if (st) return st;
-  if (count_per_box) CK(cudaMemcpy(count_per_box, ctx->d.count, sizeof(long long) * ctx->d.nbox, cudaMemcpyDeviceToHost));
+  if (count_per_box) CK(copy_sync(ctx, count_per_box, ctx->d.count, sizeof(long long) * ctx->d.nbox, cudaMemcpyDeviceToHost));
   return FRT_OK;
 }
 
@@ -1173,7 +1188,7 @@ frt_status frt_merge(frt_ctx* ctx, const uint16_t* itheta_per_box) {
   frt_status st2 = sync_and_check(ctx);
   if (st2) return st2;
   long long merged = 0;
-  CK(cudaMemcpy(&merged, &ctx->d.ctl->merged, sizeof merged, cudaMemcpyDeviceToHost));
+  CK(copy_sync(ctx, &merged, &ctx->d.ctl->merged, sizeof merged, cudaMemcpyDeviceToHost));
   if (merged > 0) ctx->merged_any = true;
   return FRT_OK;
 }
@@ -1311,7 +1326,7 @@ frt_status frt_last_stats(frt_ctx* ctx, frt_step_stats* stats) {
   if (!ctx || !stats) return FRT_ERR_INVALID;
   Ctl c;
   CK(cudaStreamSynchronize(ctx->s_main));
-  CK(cudaMemcpy(&c, ctx->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+  CK(copy_sync(ctx, &c, ctx->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
   fill_stats(ctx, c, stats);
   return FRT_OK;
 }
@@ -1320,7 +1335,7 @@ frt_status frt_num_rays(frt_ctx* ctx, int box, long long* n) {
   if (!ctx || !n) return FRT_ERR_INVALID;
   Ctl c;
   CK(cudaStreamSynchronize(ctx->s_main));
-  CK(cudaMemcpy(&c, ctx->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+  CK(copy_sync(ctx, &c, ctx->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
   const int nr = std::min(c.nray[c.cur], ctx->d.ray_cap);
   if (box < 0) {
     *n = nr;
@@ -1329,7 +1344,7 @@ frt_status frt_num_rays(frt_ctx* ctx, int box, long long* n) {
   std::vector<uint16_t> bx(nr);
   std::vector<uint8_t> dead(nr);
   if (nr) {
-    CK(cudaMemcpy(bx.data(), ctx->d.pool[c.cur].box, sizeof(uint16_t) * nr, cudaMemcpyDeviceToHost));
+    CK(copy_sync(ctx, bx.data(), ctx->d.pool[c.cur].box, sizeof(uint16_t) * nr, cudaMemcpyDeviceToHost));
   }
   long long k = 0;
   for (int i = 0; i < nr; i++) k += (bx[i] == box);
@@ -1343,7 +1358,7 @@ frt_status frt_download_rays(frt_ctx* ctx, int box, int16_t* order, int32_t* pix
   if (st) return st;
   Ctl c;
   CK(cudaStreamSynchronize(ctx->s_main));
-  CK(cudaMemcpy(&c, ctx->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+  CK(copy_sync(ctx, &c, ctx->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
   const int nr = std::min(c.nray[c.cur], ctx->d.ray_cap);
   const RayPool& P = ctx->d.pool[c.cur];
   const int F = ctx->d.F;
@@ -1354,17 +1369,17 @@ frt_status frt_download_rays(frt_ctx* ctx, int box, int16_t* order, int32_t* pix
   std::vector<float> g[9], np((size_t)F * nr);
   float* gp[9] = {P.xh, P.yh, P.zh, P.r, P.dr, P.x, P.y, P.z, P.time};
   if (nr) {
-    CK(cudaMemcpy(bx.data(), P.box, sizeof(uint16_t) * nr, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(ith.data(), P.itheta, sizeof(uint16_t) * nr, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(ord.data(), P.order, sizeof(int16_t) * nr, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(pix.data(), P.pixel, sizeof(int32_t) * nr, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(cl.data(), P.cell, sizeof(int32_t) * nr, cudaMemcpyDeviceToHost));
+    CK(copy_sync(ctx, bx.data(), P.box, sizeof(uint16_t) * nr, cudaMemcpyDeviceToHost));
+    CK(copy_sync(ctx, ith.data(), P.itheta, sizeof(uint16_t) * nr, cudaMemcpyDeviceToHost));
+    CK(copy_sync(ctx, ord.data(), P.order, sizeof(int16_t) * nr, cudaMemcpyDeviceToHost));
+    CK(copy_sync(ctx, pix.data(), P.pixel, sizeof(int32_t) * nr, cudaMemcpyDeviceToHost));
+    CK(copy_sync(ctx, cl.data(), P.cell, sizeof(int32_t) * nr, cudaMemcpyDeviceToHost));
     for (int k = 0; k < 9; k++) {
       g[k].resize(nr);
-      CK(cudaMemcpy(g[k].data(), gp[k], sizeof(float) * nr, cudaMemcpyDeviceToHost));
+      CK(copy_sync(ctx, g[k].data(), gp[k], sizeof(float) * nr, cudaMemcpyDeviceToHost));
     }
     for (int nu = 0; nu < F; nu++)
-      CK(cudaMemcpy(np.data() + (size_t)nu * nr, P.nphot + nu * cap, sizeof(float) * nr, cudaMemcpyDeviceToHost));
+      CK(copy_sync(ctx, np.data() + (size_t)nu * nr, P.nphot + nu * cap, sizeof(float) * nr, cudaMemcpyDeviceToHost));
   }
   size_t w = 0;
   for (int i = 0; i < nr; i++) {
@@ -1419,7 +1434,7 @@ frt_status frt_set_source_owner(frt_ctx* ctx, const uint8_t* own) {
       ctx->allocs.push_back(q);
       ctx->src_own_buf = (uint8_t*)q;
     }
-    CK(cudaMemcpy(ctx->src_own_buf, own, (size_t)d.nsrc, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, ctx->src_own_buf, own, (size_t)d.nsrc, cudaMemcpyHostToDevice));
     d.src_own = ctx->src_own_buf;
   }
   ctx->graph_valid = false;   // the step graph holds the Dev block by value
@@ -1707,7 +1722,7 @@ frt_status frt_read_gas(frt_ctx* ctx, int box, const void* buf, size_t len) {
   Dev& d = ctx->d;
   const size_t o = (size_t)B.cell0;
   auto up = [&](float* dst, const std::vector<float>& src) {
-    return cudaMemcpy(dst + o, src.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+    return copy_sync(ctx, dst + o, src.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
   };
   CK(up(d.nH, nH)); CK(up(d.nHe, nHe)); CK(up(d.nH1, nH1)); CK(up(d.nHe1, nHe1)); CK(up(d.f_H1, fH1));
   CK(up(d.f_He1, fHe1)); CK(up(d.temp, temp)); CK(up(d.ne, ne)); CK(up(d.avg_nh1, nH1)); CK(up(d.avg_nhe1, nHe1));
@@ -1741,8 +1756,8 @@ frt_status frt_read_treion(frt_ctx* ctx, int box, const void* buf, size_t len) {
     fl[q] = p[q * 7 + 4] ? 1 : 0;
   }
   Dev& d = ctx->d;
-  CK(cudaMemcpy(d.treion + B.cell0, tre.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(d.treion_flag + B.cell0, fl.data(), n, cudaMemcpyHostToDevice));
+  CK(copy_sync(ctx, d.treion + B.cell0, tre.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  CK(copy_sync(ctx, d.treion_flag + B.cell0, fl.data(), n, cudaMemcpyHostToDevice));
   return FRT_OK;
 }
 
@@ -1796,7 +1811,7 @@ frt_status frt_read_rays(frt_ctx* ctx, int box, const void* buf, size_t len) {
   }
   Ctl c;
   CK(cudaStreamSynchronize(ctx->s_main));
-  CK(cudaMemcpy(&c, d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+  CK(copy_sync(ctx, &c, d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
   const size_t base = (size_t)c.nray[c.cur], m = cell.size();
   if (base + m > (size_t)d.ray_cap) {
     ctx->err = "frt_read_rays: ray pool capacity exceeded";
@@ -1805,21 +1820,21 @@ frt_status frt_read_rays(frt_ctx* ctx, int box, const void* buf, size_t len) {
   double inflight = 0.0;
   if (m) {
     const RayPool& P = d.pool[c.cur];
-    CK(cudaMemcpy(P.cell + base, cell.data(), 4 * m, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(P.pixel + base, pix.data(), 4 * m, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(P.order + base, ord.data(), 2 * m, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(P.itheta + base, ith.data(), 2 * m, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(P.box + base, bx.data(), 2 * m, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, P.cell + base, cell.data(), 4 * m, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, P.pixel + base, pix.data(), 4 * m, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, P.order + base, ord.data(), 2 * m, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, P.itheta + base, ith.data(), 2 * m, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx, P.box + base, bx.data(), 2 * m, cudaMemcpyHostToDevice));
     float* gp[9] = {P.xh, P.yh, P.zh, P.r, P.dr, P.x, P.y, P.z, P.time};
-    for (int k = 0; k < 9; k++) CK(cudaMemcpy(gp[k] + base, g[k].data(), 4 * m, cudaMemcpyHostToDevice));
+    for (int k = 0; k < 9; k++) CK(copy_sync(ctx, gp[k] + base, g[k].data(), 4 * m, cudaMemcpyHostToDevice));
     for (int nu = 0; nu < F; nu++) {
-      CK(cudaMemcpy(P.nphot + (size_t)nu * d.ray_cap + base, np[nu].data(), 4 * m, cudaMemcpyHostToDevice));
+      CK(copy_sync(ctx, P.nphot + (size_t)nu * d.ray_cap + base, np[nu].data(), 4 * m, cudaMemcpyHostToDevice));
       for (float x : np[nu]) inflight += (double)x;
     }
   }
   c.nray[c.cur] = (int)(base + m);
   c.in_flight += inflight * 1e60;   // photon ledger: physical photons of the loaded rays
-  CK(cudaMemcpy(d.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice));
+  CK(copy_sync(ctx, d.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice));
   return FRT_OK;
 }
 
@@ -1855,7 +1870,7 @@ frt_status adj_source_map(frt_ctx* ctx) {
   int s = 0;
   for (size_t b = 0; b < ctx->src_cell.size(); b++)
     for (size_t q = 0; q < ctx->src_cell[b].size(); q++, s++) soc[(size_t)ctx->hbox[b].cell0 + ctx->src_cell[b][q]] = s;
-  CK(cudaMemcpy(ctx->adj.src_of_cell, soc.data(), sizeof(int) * NC, cudaMemcpyHostToDevice));
+  CK(copy_sync(ctx, ctx->adj.src_of_cell, soc.data(), sizeof(int) * NC, cudaMemcpyHostToDevice));
   ctx->adj_src_stale = false;
   return FRT_OK;
 }
@@ -1910,8 +1925,8 @@ frt_status frt_adjoint(frt_ctx* ctx, const frt_adj_objective* obj, double* J, do
   CK(cudaEventElapsedTime(&ctx->last_adjoint_ms, ctx->ev_t0, ctx->ev_t1));
   unsigned err = 0;
   double Jv = 0.0;
-  CK(cudaMemcpy(&err, a.err, sizeof err, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(&Jv, a.J, sizeof Jv, cudaMemcpyDeviceToHost));
+  CK(copy_sync(ctx, &err, a.err, sizeof err, cudaMemcpyDeviceToHost));
+  CK(copy_sync(ctx, &Jv, a.J, sizeof Jv, cudaMemcpyDeviceToHost));
   if (err) {
     ctx->err = "frt_adjoint: " + std::string((err & 1u) ? "path_length exceeded " : "") +
                std::string((err & 2u) ? "path cells above the lit-cell capacity" : "");
@@ -1923,7 +1938,7 @@ frt_status frt_adjoint(frt_ctx* ctx, const frt_adj_objective* obj, double* J, do
     for (int b = 0; b < obj->box; b++) s0 += (int)ctx->src_cell[b].size();
     const size_t ns = ctx->src_cell[obj->box].size();
     std::vector<double> v(ns);
-    if (ns) CK(cudaMemcpy(v.data(), a.dlbar + s0, sizeof(double) * ns, cudaMemcpyDeviceToHost));
+    if (ns) CK(copy_sync(ctx, v.data(), a.dlbar + s0, sizeof(double) * ns, cudaMemcpyDeviceToHost));
     for (size_t q = 0; q < ns; q++) {
       const double lum = ctx->src_lum[obj->box][q];
       dL[q] = lum != 0.0 ? v[q] / lum : 0.0;
@@ -1931,7 +1946,7 @@ frt_status frt_adjoint(frt_ctx* ctx, const frt_adj_objective* obj, double* J, do
   }
   if (dnH) {
     launch_adjoint_gather(d, a, B.cell0, B.ncell, ctx->adj_out, s);
-    CK(cudaMemcpy(dnH, ctx->adj_out, sizeof(float) * (size_t)B.ncell, cudaMemcpyDeviceToHost));
+    CK(copy_sync(ctx, dnH, ctx->adj_out, sizeof(float) * (size_t)B.ncell, cudaMemcpyDeviceToHost));
   }
   return FRT_OK;
 }
@@ -2136,7 +2151,7 @@ frt_status frt_autotune(frt_ctx* ctx, int steps, frt_tuning* out) {
       break;
     }
     Ctl c0;
-    if (cudaMemcpy(&c0, d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    if (copy_sync(ctx, &c0, d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost) != cudaSuccess) {
       st = FRT_ERR_CUDA;
       break;
     }
