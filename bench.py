@@ -12,13 +12,14 @@ L2 flush is needed between steps.
              graph launch on the step stream), summed over ranks / max over ranks
   e2e        same crossings / host wall time of the frt_step calls (per step: H2D of the step's
              random-angle indices from pinned memory, graph launch, D2H of the step totals)
-  roofline   the dark-cell kernel (the whole step of every cell no ray touched, one streaming
-             pass): algorithmic bytes = cells x 82 B (10 float fields + 2 flag bytes read,
-             10 float fields written) / its CUDA-event time, against MEASURED_PEAKS.json hbm_gbs
+  roofline   the ray pass (k_raypass_mixed, five launches per step): algorithmic bytes = crossings
+             x 84 B / its CUDA-event time, against MEASURED_PEAKS.json hbm_gbs; "walk" gives the
+             same for the walk (k_advance) and "dark_pass" the dark-cell pass's span
   cpu_baseline  the reference's own OpenMP code (compiled from its sources, oracle/_ref) on the
              host cores, on a bounded steady-state sample of the same workload: the device's state
              after the last timed step, written in the reference's restart formats, is read by the
-             reference's own restart path (input_grid = TRUE), which then runs two steps
+             reference's own restart path (input_grid = TRUE), its balance_cpus spreads the rays
+             over the threads, and it then runs three timed steps
 
 --impl reference runs that compiled reference alone (all host threads) and prints its line.
 Multi-GPU: the single-box workloads do not shard; --gpus N runs N independent replicas (one per
@@ -148,7 +149,9 @@ def _ref_exe(name: str, spec, threads: int, restart: bool = False) -> str:
     if os.path.exists(meta_p):
         with open(meta_p) as f:
             ncpu = json.load(f).get("ncpu")
-    if not os.path.exists(exe) or ncpu is None or ncpu < threads:
+    drv = os.path.join(HERE, "oracle", "ref_driver.cc")
+    stale = os.path.exists(exe) and os.path.getmtime(exe) < os.path.getmtime(drv)
+    if not os.path.exists(exe) or ncpu is None or ncpu < threads or stale:
         if os.path.isdir(B.REF_SRC):
             B.build(name, spec, ncpu=threads, restart=restart)
         elif os.path.isdir(os.path.join(d, "src")):
@@ -219,7 +222,9 @@ def run_reference_restart(spec, name: str, files, steps: int, threads: int, seed
         with tempfile.TemporaryDirectory() as td:
             W.write_reference_inputs(inp, td)
             args = [exe, td, str(steps), str(seed), "0", repr(spec.rkill_cm())]
-            env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+            # the rays read from the restart file are spread over the threads by the reference's
+            # balance_cpus before the first timed step (its step loop does that after every step)
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads), FRT_RESTART_BALANCE="1")
             r = subprocess.run(args, cwd=d, env=env, capture_output=True, text=True, preexec_fn=_unlimited_stack)
             if r.returncode != 0:
                 raise RuntimeError(f"ref_driver (restart) failed: {r.stdout[-500:]} {r.stderr[-500:]}")
@@ -721,7 +726,8 @@ def main():
                                                 args.cpu_baseline_steps, threads, args.seed)
             sample = (f"steps {last + 1}..{last + len(rows)} of the same workload: the device state after step "
                       f"{last} written in the reference's restart formats and resumed by the reference's own "
-                      f"restart path (input_grid = TRUE; restart set-up {setup:.1f} s excluded); reference "
+                      f"restart path (input_grid = TRUE; restart set-up and the reference's balance_cpus over the restored "
+                      f"rays, {setup:.1f} s, excluded); reference "
                       f"OpenMP code compiled from its sources, {threads} threads")
         except Exception as e:
             # no restart build: the first steps from a fresh start (set-up-dominated, labelled so)

@@ -211,8 +211,9 @@ void enqueue_begin_advance(frt_ctx* ctx, bool in_graph = false) {
   launch_step_begin(d, ctx->s_main);
   if (d.subgrid) launch_sg_step(d, ctx->s_main);
   record(ctx->ev_a0, ctx->s_main, in_graph);
-  launch_advance(d, ctx->nsm * ctx->tune.adv_grid, ctx->s_main, ctx->tune.adv_block, ctx->grid_rays);
+  launch_walk(d, ctx->nsm * ctx->tune.adv_grid, ctx->s_main, ctx->tune.adv_block, 0, INT_MAX);
   record(ctx->ev_a1, ctx->s_main, in_graph);
+  launch_lit_number(d, ctx->grid_rays, ctx->s_main);   // lit cells numbered, moved rays packed
 }
 
 // The C2Ray iterations with I-front tracking: per iteration, rounds of (ray pass, budget pass)

@@ -188,6 +188,11 @@ int main(int argc, char** argv) {
   }
   if (have_clump) memcpy(&clump[0][0][0], &clump_in[0][0][0], sizeof(clump));
   get_nphot_min_max();
+  // FRT_RESTART_BALANCE: after the restart set-up, spread the rays read from the file over the
+  // threads' buffer regions with the reference's own balance_cpus (mem_funcs.cc:186-236), which
+  // its step loop runs at the end of every step (main.cc:258) but the restart set-up does not:
+  // without it the first restarted step runs with every ray in the first threads' regions
+  if (input_grid == TRUE && getenv("FRT_RESTART_BALANCE")) balance_cpus();
   const double t_setup = omp_get_wtime() - t_setup0;
   printf("SETUP %.6f s num_src=%d dt=%.9e dx=%.9e nphot_min=%.9e\n", t_setup, num_src, (double)dt, (double)dx[0],
          nphot_min);
