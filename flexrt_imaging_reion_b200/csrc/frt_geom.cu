@@ -1000,9 +1000,18 @@ __device__ __forceinline__ int cast_count(const Dev& d, int s, int* nside_out, i
 }
 
 // The pool positions of the step's new rays: sources in order, each source's rays together in
-// pixel order after the live rays (the order new_rays appends them in, rt_funcs.cc:240-261). One
-// block scans the sources' ray counts.
-__global__ void __launch_bounds__(1024) k_cast_offsets(Dev d) {
+// pixel order after the live rays (the order new_rays appends them in, rt_funcs.cc:240-261).
+// k_cast_count writes each source's ray count into src_pos (many blocks: the counts read the
+// source cells' neutral fractions); k_cast_scan then turns the counts into positions in place
+// (one block over the sources, coalesced) and moves the pool count past the new rays.
+__global__ void k_cast_count(Dev d) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < d.nsrc; s += gridDim.x * blockDim.x) {
+    int nside = 1, lpix = 0;
+    d.src_pos[s] = cast_count(d, s, &nside, &lpix);
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_cast_scan(Dev d) {
   __shared__ int wsum[32];
   __shared__ int base_s;
   const int cur = d.ctl->cur;
@@ -1011,8 +1020,7 @@ __global__ void __launch_bounds__(1024) k_cast_offsets(Dev d) {
   __syncthreads();
   for (int s0 = 0; s0 < d.nsrc; s0 += blockDim.x) {
     const int s = s0 + threadIdx.x;
-    int nside = 1, lpix = 0;
-    const int cnt = (s < d.nsrc) ? cast_count(d, s, &nside, &lpix) : 0;
+    const int cnt = (s < d.nsrc) ? d.src_pos[s] : 0;
     int incl = cnt;
     for (int o = 1; o < 32; o <<= 1) {
       const int v = __shfl_up_sync(0xffffffffu, incl, o);
@@ -1053,8 +1061,8 @@ __global__ void k_cast(Dev d, int s_begin, int s_end) {
     const int b = d.src_box[s];
     const BoxP& B = d.box[b];
     const int c = d.src_cell[s];
-    const int pos = d.src_pos[s];   // k_cast_offsets
-    if (pos + count > cap) continue;   // (k_cast_offsets flagged the overflow)
+    const int pos = d.src_pos[s];   // k_cast_scan
+    if (pos + count > cap) continue;   // (k_cast_scan flagged the overflow)
     const uint16_t ith = d.src_itheta[s];
     const float* m = d.rot + (size_t)ith * 18;
     const double lum = d.src_lum[s];
@@ -1279,15 +1287,20 @@ void launch_split_range(const Dev& d, int grid, int r_begin, int r_end, cudaStre
 
 void launch_swap(const Dev& d, cudaStream_t s) { k_swap<<<1, 1, 0, s>>>(d); }
 
+void launch_cast_positions(const Dev& d, cudaStream_t s) {
+  k_cast_count<<<grid_for(d.nsrc, 256, 4096), 256, 0, s>>>(d);
+  k_cast_scan<<<1, 1024, 0, s>>>(d);
+}
+
 void launch_cast(const Dev& d, cudaStream_t s) {
   if (d.nsrc > 0) {
-    k_cast_offsets<<<1, 1024, 0, s>>>(d);
+    launch_cast_positions(d, s);
     k_cast<<<grid_for(d.nsrc, 128, 4096), 128, 0, s>>>(d, 0, d.nsrc);
   }
 }
 
 void launch_cast_per_source(const Dev& d, cudaStream_t s) {
-  if (d.nsrc > 0) k_cast_offsets<<<1, 1024, 0, s>>>(d);
+  if (d.nsrc > 0) launch_cast_positions(d, s);
   for (int src = 0; src < d.nsrc; src++) k_cast<<<1, 32, 0, s>>>(d, src, src + 1);
 }
 
