@@ -276,7 +276,8 @@ def run_ensemble(args, rank: int, world: int, local_rank: int):
         tdist.barrier()
     clocks = ClockSampler(local_rank)
     clocks.start()
-    n_tune = AUTOTUNE_STEPS if (not args.no_autotune and args.warmup >= AUTOTUNE_STEPS + 1) else 0
+    n_tune = AUTOTUNE_STEPS if (not args.no_autotune and args.subgrid == "off"
+                                and args.warmup >= AUTOTUNE_STEPS + 1) else 0
     bat = EN.run_batched(inputs, seeds, args.warmup, args.steps, device=local_rank, box_ids=mine,
                          autotune_steps=n_tune)
     clk = clocks.stop()
@@ -496,6 +497,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     ctx = rt.RTContext([inp], [args.seed + rank], precision="mixed", outputs="core",
                        ray_capacity=args.ray_capacity, lit_capacity=args.lit_capacity, device=local_rank)
     ctx.setup()
+    if args.subgrid != "off":   # the sub-grid model on the synthetic RadHydro tables
+        tables, consts = W.subgrid_inputs(spec.z)
+        ctx.set_subgrid(tables, consts, ifront=(args.subgrid == "ifront"))
     ncell = spec.n ** 3
     itercount = ctx.itercount
     tuning = warm_up(ctx, args)
@@ -564,7 +568,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded lognormal gas + L^-2 sources; the reference's inputs are not shipped)",
         "config": {"workload": _describe(spec), "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps}",
-                   "graph": not args.plain, "l2": "state (>1 GB) larger than L2, no flush",
+                   "graph": not args.plain and args.subgrid != "ifront",
+                   "subgrid": {"off": "none", "eq": "equilibrium sub-grid model (synthetic RadHydro tables)",
+                               "ifront": "equilibrium sub-grid model with I-front tracking (synthetic RadHydro "
+                                         "tables)"}[args.subgrid], "l2": "state (>1 GB) larger than L2, no flush",
                    "parallelism": "replicas" if world > 1 else "single",
                    "launch_shapes": _tuning_config(tuning)},
         "e2e": {"value": cross_all / wall_max, "unit": "crossings/s", "h2d_bytes_per_step": h2d,
@@ -633,10 +640,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # the reference arm times the same step window as this arm (about 8-10 s per L step on 16 cores)
     ap.add_argument("--ref-time-cap", type=float, default=900.0)
+    ap.add_argument("--subgrid", choices=["off", "eq", "ifront"], default="off",
+                    help="single boxes: run the sub-grid model (eq) or the sub-grid model with I-front tracking "
+                         "(ifront) on synthetic RadHydro tables; no CPU baseline or reference arm for these")
     ap.add_argument("--mode", choices=["replicas", "partition"], default="replicas",
                     help="N>1 on one box: N independent replicas (weak), or the box's sources shared "
                          "over the N ranks with the lit cells' rates all-reduced (strong)")
     args = ap.parse_args()
+    if args.subgrid != "off":
+        args.no_cpu_baseline = True   # the reference arm and the CPU baseline time the plain model
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

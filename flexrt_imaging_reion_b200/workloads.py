@@ -209,3 +209,83 @@ def config_tiny(n: int = 16, n_src: int = 6, steps: int = 6, seed: int = 7, name
 
 
 CONFIGS = {"S": config_S, "M": config_M, "L": config_L, "A": config_A}
+
+
+# ---- synthetic sub-grid tables ------------------------------------------------------------
+# The reference's sub-grid model reads RadHydro tables (27 runs: 3 photo-ionisation rates x 3
+# reionisation redshifts x 3 overdensities, Nt = 5000 rows of time since ionisation, two mean free
+# paths, HI fraction, temperature; subgrid.cc:20-47) and a linear -> non-linear overdensity table
+# (500 cosmic times x 500 delta/sigma; subgrid.cc:49-95), neither of which is shipped. These are
+# smooth closed-form stand-ins with the tables' shapes; the same arrays feed the device, the
+# oracle and (written in the reference's file formats) the compiled reference.
+SG_NT = 5000
+SG_NDLIN = 500
+
+
+def subgrid_radhydro():
+    """Per run (q rate, m reionisation redshift, p density, the reference's loop order) the 4
+    table columns after the time: mfp (frequency-averaged, 912 A), HI fraction, temperature."""
+    t_yr = np.arange(SG_NT, dtype=np.float64) * 2.0e5           # 0 .. 1 Gyr since ionisation
+    cols = np.zeros((3, 3, 3, 4, SG_NT))
+    for q in range(3):
+        for m in range(3):
+            for p in range(3):
+                g = 10.0 ** (q - 1)                              # Gamma / 3e-13
+                d = 2.0 ** (p - 1)                               # 1 + delta ~ 0.5, 1, 2
+                z = 1.0 + 0.1 * m
+                relax = 1.0 + 4.0 * np.exp(-t_yr / 3.0e7)
+                mfp0 = 8.0 * g ** (2.0 / 3.0) / d / z / relax
+                mfp1 = 0.6 * mfp0
+                fh1 = 2.0e-4 / g ** 0.7 * d ** 0.8 * z * (1.0 + 3.0 * np.exp(-t_yr / 1.0e7))
+                temp = 1.2e4 * d ** 0.3 / z * (1.0 + 1.5 * np.exp(-t_yr / 5.0e7))
+                cols[q, m, p] = np.stack([mfp0, mfp1, np.minimum(fh1, 0.9), temp])
+    return {"time_yr": t_yr, "cols": cols}
+
+
+def subgrid_delta_over_sigma(t0: float, t1: float):
+    """The linear -> non-linear overdensity table: times from t0 to t1 [s], delta/sigma in
+    [-4, 4], and a lognormal-like growth of the non-linear overdensity with time."""
+    t = np.linspace(t0, t1, SG_NDLIN)
+    ds = np.linspace(-4.0, 4.0, SG_NDLIN)
+    grow = 0.2 + 0.5 * (t - t0) / (t1 - t0)
+    dnl = np.exp(grow[:, None] * ds[None, :]) - 1.0
+    return {"t": t, "ds": ds, "dnl": dnl}
+
+
+def subgrid_arrays(t0: float, t1: float):
+    """The tables as the reference holds them in memory after reading the files (the layout
+    frt_set_subgrid takes): time_RH and fh1_RH as flat [Nt][3][3][3] floats written at the gamma
+    index q + 1 (subgrid.cc:24-36), with one slot more for the last row's spill; times in s; the
+    overdensity table as floats."""
+    rh = subgrid_radhydro()
+    n = SG_NT * 27 + 1
+    time = np.zeros(n, np.float32)
+    fh1 = np.zeros(n, np.float32)
+    t_s = (rh["time_yr"].astype(np.float32).astype(np.float64) * YR_TO_S).astype(np.float32)
+    for q in range(3):
+        for m in range(3):
+            for p in range(3):
+                off = ((np.arange(SG_NT) * 3 + m) * 3 + p) * 3 + (q + 1)
+                time[off] = t_s
+                fh1[off] = rh["cols"][q, m, p, 2].astype(np.float32)
+    ds = subgrid_delta_over_sigma(t0, t1)
+    return {"time": time, "fh1": fh1, "t_dnl": ds["t"].astype(np.float32), "ds": ds["ds"].astype(np.float32),
+            "dnl": ds["dnl"].astype(np.float32).ravel()}
+
+
+def cosmic_time_lcdm(a: float, h: float = HH, omega_m: float = 0.305) -> float:
+    """Age of a flat LambdaCDM universe at scale factor a [s] (closed form,
+    t = 2 / (3 H0 sqrt(OL)) asinh(sqrt(OL / Om) a^1.5)); the cosmic times the sub-grid model
+    reads (tinit and the RadHydro reionisation redshifts) for a synthetic run."""
+    h0 = 100.0 * h * 1e5 / MPC_TO_CM
+    ol = 1.0 - omega_m
+    return float(2.0 / (3.0 * h0 * np.sqrt(ol)) * np.arcsinh(np.sqrt(ol / omega_m) * a ** 1.5))
+
+
+def subgrid_inputs(z: float):
+    """Tables and cosmic-time constants for frt_set_subgrid on a box starting at redshift z:
+    {tinit, t(z=12), t(z=8), t(z=5.5), tre_dom = t(z=12, 8, 6)}, the overdensity table spanning
+    z = 16 to 4.5."""
+    ct = lambda zz: cosmic_time_lcdm(1.0 / (1.0 + zz))   # noqa: E731
+    consts = [ct(z), ct(12.0), ct(8.0), ct(5.5), ct(12.0), ct(8.0), ct(6.0)]
+    return subgrid_arrays(ct(16.0), ct(4.5)), np.asarray(consts, np.float32)

@@ -10,10 +10,11 @@ The reference's sub-grid model reads RadHydro tables that are not shipped with i
   linear overdensity / sigma, then 500 lines of 500 non-linear overdensities, one line per time
   (import_delta_over_sigma_table, subgrid.cc:49-95).
 
-Here they are smooth, seeded-free closed-form functions of their indices, written with 17
-significant digits so that the reference's fscanf("%le") and this module give the same doubles
-(and the same floats after the reference's (float) casts). The same arrays feed the oracle and
-the device; nothing here is taken from the RadHydro simulations, which are not available.
+Here they are the smooth closed-form functions of flexrt_imaging_reion_b200.workloads (the
+package's synthetic inputs), written with 17 significant digits so that the reference's
+fscanf("%le") and the in-memory arrays give the same doubles (and the same floats after the
+reference's (float) casts). The same arrays feed the oracle and the device; nothing here is
+taken from the RadHydro simulations, which are not available.
 """
 from __future__ import annotations
 
@@ -22,33 +23,18 @@ from typing import Dict
 
 import numpy as np
 
-NT = 5000
-N_DLIN = 500
+from flexrt_imaging_reion_b200 import workloads as W
+
+NT = W.SG_NT
+N_DLIN = W.SG_NDLIN
 GAMMA_TAGS = ["G14", "G13", "G12"]
 ZRE_TAGS = ["zre12", "zre8", "zre6"]
 DENSITY_TAGS = ["dm3", "d0", "dp3"]
-YR_TO_S = 3.154e7
 
 
 def radhydro() -> Dict[str, np.ndarray]:
     """Per file (q gamma, m zre, p density, in the reference's loop order) the 5 columns."""
-    t_yr = np.arange(NT, dtype=np.float64) * 2.0e5           # 0 .. 1 Gyr since ionisation
-    out = {"time_yr": t_yr}
-    cols = np.zeros((3, 3, 3, 4, NT))
-    for q in range(3):
-        for m in range(3):
-            for p in range(3):
-                g = 10.0 ** (q - 1)                              # Gamma / 3e-13
-                d = 2.0 ** (p - 1)                               # 1 + delta ~ 0.5, 1, 2
-                z = 1.0 + 0.1 * m
-                relax = 1.0 + 4.0 * np.exp(-t_yr / 3.0e7)
-                mfp0 = 8.0 * g ** (2.0 / 3.0) / d / z / relax
-                mfp1 = 0.6 * mfp0
-                fh1 = 2.0e-4 / g ** 0.7 * d ** 0.8 * z * (1.0 + 3.0 * np.exp(-t_yr / 1.0e7))
-                temp = 1.2e4 * d ** 0.3 / z * (1.0 + 1.5 * np.exp(-t_yr / 5.0e7))
-                cols[q, m, p] = np.stack([mfp0, mfp1, np.minimum(fh1, 0.9), temp])
-    out["cols"] = cols
-    return out
+    return W.subgrid_radhydro()
 
 
 def table_span(cosmic_time_s):
@@ -57,13 +43,8 @@ def table_span(cosmic_time_s):
 
 
 def delta_over_sigma(t0: float, t1: float) -> Dict[str, np.ndarray]:
-    """The linear -> non-linear overdensity table: times from t0 to t1, delta/sigma in [-4, 4], and
-    a lognormal-like growth of the non-linear overdensity with time."""
-    t = np.linspace(t0, t1, N_DLIN)
-    ds = np.linspace(-4.0, 4.0, N_DLIN)
-    grow = 0.2 + 0.5 * (t - t0) / (t1 - t0)
-    dnl = np.exp(grow[:, None] * ds[None, :]) - 1.0
-    return {"t": t, "ds": ds, "dnl": dnl}
+    """The linear -> non-linear overdensity table (flexrt_imaging_reion_b200.workloads)."""
+    return W.subgrid_delta_over_sigma(t0, t1)
 
 
 def write_reference_files(directory: str, cosmic_time_s) -> None:
@@ -108,17 +89,4 @@ def reference_arrays(t0: float, t1: float) -> Dict[str, np.ndarray]:
     fh1_RH as flat [Nt][3][3][3] floats written at the gamma index q + 1 (gam_offset,
     subgrid.cc:24-36), with one slot more for the last row's spill; times in s (time_RH *= yr_to_s,
     float); the overdensity table as floats."""
-    rh = radhydro()
-    n = NT * 27 + 1
-    time = np.zeros(n, np.float32)
-    fh1 = np.zeros(n, np.float32)
-    t_s = (rh["time_yr"].astype(np.float32).astype(np.float64) * YR_TO_S).astype(np.float32)
-    for q in range(3):
-        for m in range(3):
-            for p in range(3):
-                off = ((np.arange(NT) * 3 + m) * 3 + p) * 3 + (q + 1)
-                time[off] = t_s
-                fh1[off] = rh["cols"][q, m, p, 2].astype(np.float32)
-    ds = delta_over_sigma(t0, t1)
-    return {"time": time, "fh1": fh1, "t_dnl": ds["t"].astype(np.float32), "ds": ds["ds"].astype(np.float32),
-            "dnl": ds["dnl"].astype(np.float32).ravel()}
+    return W.subgrid_arrays(t0, t1)
