@@ -54,7 +54,7 @@ DARK_TRAFFIC_BYTES_PER_CELL = 1343184384 / 13264001
 # The number of ray passes per step is the context's C2Ray iteration count (RTContext.itercount).
 RAYPASS_BYTES_PER_CROSSING = 8 + 8 + 68
 # warm-up steps that frt_autotune takes (the last ones of the warm-up)
-AUTOTUNE_STEPS = 3
+AUTOTUNE_STEPS = 4
 RAYPASS_TRAFFIC_BYTES_PER_CROSSING = 38.9
 # Walk (k_advance): per live ray its record read (cell, geometry, order/pixel/itheta, time: 44 B)
 # and written back (30 B); per crossing its segment {cell, dist} written (8 B) and the cell's
@@ -470,7 +470,8 @@ def warm_up(ctx, args):
     """The W warm-up steps: graph steps, the last AUTOTUNE_STEPS of them taken by frt_autotune
     (real steps that also time candidate launch shapes; the chosen shapes are then captured in
     the step graph). Returns the chosen shapes, or None without autotuning."""
-    n_tune = AUTOTUNE_STEPS if (not args.no_autotune and args.warmup >= AUTOTUNE_STEPS + 1) else 0
+    n_tune = AUTOTUNE_STEPS if (not args.no_autotune and args.subgrid == "off"
+                                and args.warmup >= AUTOTUNE_STEPS + 1) else 0
     for _ in range(args.warmup - n_tune):
         ctx.step(graph=not args.plain)
     if not n_tune:

@@ -2130,7 +2130,9 @@ frt_status frt_autotune(frt_ctx* ctx, int steps, frt_tuning* out) {
   ShapeSearch adv("walk", Shape{t0.adv_block, t0.adv_grid, 0}, {128, 256}, {4, 8, 16}, {0}, 4);
   ShapeSearch lit("cellpass", Shape{256, t0.lit_grid, 0}, {256}, {2, 4, 8, 16}, {0}, per_iter);
   ShapeSearch spl("split", Shape{256, t0.split_grid, 0}, {256}, {2, 4, 8, 16}, {0}, 4);
-  for (ShapeSearch* f : {&rp, &adv, &lit, &spl}) f->set_max_rounds(steps);
+  // with three steps or more, the last two validate the search on whole graph steps (below)
+  const int search_steps = steps >= 3 ? steps - 2 : steps;
+  for (ShapeSearch* f : {&rp, &adv, &lit, &spl}) f->set_max_rounds(search_steps);
   constexpr int kEv = 2 * (4 + 16 + 16 + 4);
   std::vector<cudaEvent_t> ev(kEv, nullptr);
   auto destroy = [&]() {
@@ -2145,7 +2147,7 @@ frt_status frt_autotune(frt_ctx* ctx, int steps, frt_tuning* out) {
     }
   frt_status st = FRT_OK;
   double c_rp = 0, c_adv = 0, c_lit = 0, c_spl = 0;
-  for (int round = 0; round < steps && st == FRT_OK; round++) {
+  for (int round = 0; round < search_steps && st == FRT_OK; round++) {
     if ((st = step_inputs(ctx, nullptr, nullptr))) break;
     if (cudaStreamSynchronize(s) != cudaSuccess || cudaStreamSynchronize(ctx->s_dark) != cudaSuccess) {
       st = FRT_ERR_CUDA;
@@ -2252,6 +2254,23 @@ frt_status frt_autotune(frt_ctx* ctx, int steps, frt_tuning* out) {
   t.adv_grid = adv.best().grid;
   t.lit_grid = lit.best().grid;
   t.split_grid = spl.best().grid;
+  if (steps >= 3) {
+    // The search times each kernel family alone, with no dark pass beside it; in the step graph
+    // the dark pass shares the SMs with the lit-cell chain. So the search's shapes and the
+    // starting ones each run one whole graph step, and the faster per crossing is kept.
+    double per_cross[2] = {0.0, 0.0};
+    const Tune cand[2] = {t, t0};
+    ctx->tune_auto = false;
+    for (int k = 0; k < 2 && st == FRT_OK; k++) {
+      ctx->tune = cand[k];
+      ctx->graph_valid = false;
+      frt_step_stats ss{};
+      st = frt_step(ctx, nullptr, nullptr, &ss);
+      if (st == FRT_OK && ss.crossings > 0) per_cross[k] = (double)ctx->last_step_ms / (double)ss.crossings;
+    }
+    if (st) return st;
+    if (per_cross[1] > 0.0 && per_cross[0] > per_cross[1]) t = t0;
+  }
   ctx->tune = t;
   ctx->tune_auto = true;
   ctx->graph_valid = false;

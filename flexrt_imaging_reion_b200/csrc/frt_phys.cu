@@ -231,8 +231,11 @@ __global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
 // when it does.
 // NF > 0 fixes the number of frequency bins at compile time (the 5-bin spectrum of every
 // configuration here), so the per-bin loops unroll exactly; NF = 0 takes d.F at run time.
-template <bool LAST, int NF>
-__global__ void __launch_bounds__(256) k_raypass_mixed(Dev d, int iter, int chunk) {
+// CHUNKED compiles the queue form; the static-slice form carries none of its bookkeeping. The
+// minimum resident blocks keep the last pass (which also writes the rays' photon counts and
+// the heating pairs) at 64 registers, four 256-thread blocks per SM.
+template <bool LAST, int NF, bool CHUNKED>
+__global__ void __launch_bounds__(256, LAST ? 4 : 5) k_raypass_mixed(Dev d, int iter, int chunk) {
   constexpr int MAXF = NF > 0 ? NF : FRT_MAX_FREQ;
   constexpr unsigned FULL = 0xffffffffu;
   const int Fr = NF > 0 ? NF : d.F;
@@ -246,7 +249,7 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d, int iter, int chun
   long long cursor = 0, slice_end = 0;
   bool queue_done = false;
   int* queue = d.rp_queue + (iter < kMaxIterQueue ? iter : kMaxIterQueue - 1);
-  if (chunk <= 0) {
+  if (!CHUNKED) {
     const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
     const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const long long per = (nmv + nwarps - 1) / nwarps;
@@ -270,7 +273,7 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d, int iter, int chun
     // refill the lanes whose ray ended
     const bool need = (i < 0) && !exhausted;
     const unsigned m = __ballot_sync(FULL, need);
-    if (m && cursor >= slice_end && !queue_done) {
+    if (CHUNKED && m && cursor >= slice_end && !queue_done) {
       // the warp's chunk is used up: take the next one from the queue
       int base = 0;
       if (lane == 0) base = atomicAdd(queue, chunk);
@@ -284,7 +287,7 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d, int iter, int chun
     }
     if (m) {
       const long long q = cursor + __popc(m & lanes_below);
-      cursor = min(cursor + __popc(m), max(cursor, slice_end));
+      cursor = CHUNKED ? min(cursor + __popc(m), max(cursor, slice_end)) : cursor + __popc(m);
       if (need) {
         if (q < slice_end) {
           const int4 hd = d.mv_hdr[q];
@@ -303,7 +306,7 @@ __global__ void __launch_bounds__(256) k_raypass_mixed(Dev d, int iter, int chun
 #pragma unroll
           for (int nu = 0; nu < MAXF; nu++) nin[nu] = (nu < Fr) ? A.nphot[(size_t)nu * cap + i] : 0.f;
           av0 = (sg0.x >= 0 && sg0.x < L) ? d.l_avg[sg0.x] : make_float2(0.f, 0.f);
-        } else if (queue_done) {
+        } else if (!CHUNKED || queue_done) {
           exhausted = true;   // (a lane short of a chunk's remainder asks again next trip)
         }
       }
@@ -771,12 +774,23 @@ void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t 
     else k_raypass_strict<false><<<grid, 256, 0, s>>>(d);
     return;
   }
+  const bool q = chunk > 0;
   if (d.F == 5) {
-    if (last) k_raypass_mixed<true, 5><<<grid, block, 0, s>>>(d, iter, chunk);
-    else k_raypass_mixed<false, 5><<<grid, block, 0, s>>>(d, iter, chunk);
+    if (last) {
+      if (q) k_raypass_mixed<true, 5, true><<<grid, block, 0, s>>>(d, iter, chunk);
+      else k_raypass_mixed<true, 5, false><<<grid, block, 0, s>>>(d, iter, chunk);
+    } else {
+      if (q) k_raypass_mixed<false, 5, true><<<grid, block, 0, s>>>(d, iter, chunk);
+      else k_raypass_mixed<false, 5, false><<<grid, block, 0, s>>>(d, iter, chunk);
+    }
   } else {
-    if (last) k_raypass_mixed<true, 0><<<grid, block, 0, s>>>(d, iter, chunk);
-    else k_raypass_mixed<false, 0><<<grid, block, 0, s>>>(d, iter, chunk);
+    if (last) {
+      if (q) k_raypass_mixed<true, 0, true><<<grid, block, 0, s>>>(d, iter, chunk);
+      else k_raypass_mixed<true, 0, false><<<grid, block, 0, s>>>(d, iter, chunk);
+    } else {
+      if (q) k_raypass_mixed<false, 0, true><<<grid, block, 0, s>>>(d, iter, chunk);
+      else k_raypass_mixed<false, 0, false><<<grid, block, 0, s>>>(d, iter, chunk);
+    }
   }
 }
 

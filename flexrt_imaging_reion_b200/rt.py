@@ -367,7 +367,7 @@ class RTContext:
         return self.stats.as_dict()
 
     # ---- launch shapes -------------------------------------------------------------------------
-    def autotune(self, steps: int = 3) -> Dict[str, float]:
+    def autotune(self, steps: int = 4) -> Dict[str, float]:
         """frt_autotune: `steps` RT steps that also time candidate launch shapes; the chosen
         shapes are set on the context (and remembered for its ray-count bucket)."""
         t = _abi.Tuning()

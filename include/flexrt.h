@@ -294,11 +294,14 @@ typedef struct {
   /* frt_autotune: measured cost of the chosen shapes, ns per unit of work (crossing, ray, lit cell) */
   double raypass_ns_per_crossing, walk_ns_per_ray, cellpass_ns_per_cell, split_ns_per_ray;
 } frt_tuning;
-/* Runs `steps` (>= 1; 3 recommended) whole RT steps of the context (they advance the simulation
+/* Runs `steps` (>= 1; 4 recommended) whole RT steps of the context (they advance the simulation
  * like frt_step_plain; the draws come from the context's streams) and times candidate shapes on
  * them: every candidate of a round runs on a comparable share of one step's work (one C2Ray
  * iteration's ray or cell pass, or one of k equal ray ranges of the walk and the compaction),
  * costs are time per unit of work, and each round varies one parameter around the best so far.
+ * With steps >= 3 the last two steps validate the result on whole graph steps (where the dark
+ * pass shares the SMs): one runs the search's shapes, one the starting shapes, and the faster
+ * per crossing is kept.
  * The chosen shapes are set on the context, reported in *out, and remembered for contexts of the
  * same device, cell count and live-ray count (power-of-two bucket): frt_step switches to a
  * remembered shape set when its ray count enters that bucket. */
