@@ -73,29 +73,74 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons of this rank's GPU, sampled during the timed
+    region. NVML is polled every 10 ms on the device's UUID (the timed region of the default run
+    is a fraction of a second, shorter than one nvidia-smi call); nvidia-smi on the same UUID
+    every 200 ms is the fallback. Only reads: no setting of the GPU is changed."""
+
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
     def __init__(self, index: int):
         self.index = index
-        self.rows = []
+        self.rows = []          # (sm_mhz, sm_max_mhz, reason bits)
+        self.source = None
         self._stop = threading.Event()
         self._t = None
 
-    def start(self):
-        def run():
-            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_power_cap")
+    def _uuid(self):
+        try:
+            import torch
+            u = str(torch.cuda.get_device_properties(self.index).uuid)
+            return u if u.startswith("GPU-") else "GPU-" + u
+        except Exception:
+            return None
+
+    def _run_nvml(self, uuid):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            h = (pynvml.nvmlDeviceGetHandleByUUID(uuid.encode()) if uuid
+                 else pynvml.nvmlDeviceGetHandleByIndex(self.index))
+            get_reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons",
+                                  getattr(pynvml, "nvmlDeviceGetCurrentClocksThrottleReasons", None))
+            mx = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.source = "nvml, 10 ms"
             while not self._stop.is_set():
-                try:
-                    out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                         timeout=5).stdout.strip()
-                    if out:
-                        self.rows.append([x.strip() for x in out.split(",")])
-                except Exception:
-                    pass
-                self._stop.wait(0.2)
+                sm = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                bits = int(get_reasons(h)) if get_reasons else 0
+                self.rows.append((sm, mx, bits))
+                self._stop.wait(0.01)
+        finally:
+            pynvml.nvmlShutdown()
+
+    def _run_smi(self, uuid):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        self.source = "nvidia-smi, 200 ms"
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={uuid or self.index}", f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                r = [x.strip() for x in out.split(",")]
+                if len(r) == 6 and r[0].replace(".", "").isdigit():
+                    bits = sum(b for (_, b), v in zip(self.REASONS, r[2:]) if v == "Active")
+                    self.rows.append((float(r[0]), float(r[1]), bits))
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def start(self):
+        uuid = self._uuid()
+
+        def run():
+            try:
+                self._run_nvml(uuid)
+            except Exception:
+                if not self._stop.is_set():
+                    self._run_smi(uuid)
         self._t = threading.Thread(target=run, daemon=True)
         self._t.start()
 
@@ -103,12 +148,11 @@ class ClockSampler:
         self._stop.set()
         if self._t:
             self._t.join(timeout=10)
-        sm = [float(r[0]) for r in self.rows if r and r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if len(r) > 1 and r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 3 + k and r[3 + k] == "Active"})
+        sm = [r[0] for r in self.rows]
+        mx = [r[1] for r in self.rows]
+        reasons = sorted({n for r in self.rows for n, b in self.REASONS if r[2] & b})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(self.rows), "source": self.source}
 
 
 def _spec(name):

@@ -97,8 +97,9 @@ def test_other_shapes_same_results(chunk):
 
 @pytest.mark.gpu
 def test_autotune_steps_match_oracle():
-    """The tuning steps are real steps: T16 tuned over its first 3 steps, then stepped on, matches
-    the oracle at every step."""
+    """The tuning steps are real steps: T16 tuned over its first 4 steps (two searched, two
+    validating the choice on whole graph steps), then stepped on, matches the oracle at every
+    step."""
     from test_gpu_parity import check
     spec, seed = W.config_tiny(), 11
     ref = PT.oracle_states(W.make_inputs(spec), seed, spec.steps)
@@ -106,11 +107,11 @@ def test_autotune_steps_match_oracle():
     ctx.setup()
     states = [PT.device_state(ctx, 0, False)]
     t = ctx.autotune(4)
-    assert t["steps"] == 3
-    states += [None, None, None]
-    states[3] = PT.device_state(ctx, 0, False)
-    for _ in range(spec.steps - 3):
+    assert t["steps"] == 4
+    states += [None] * 4
+    states[4] = PT.device_state(ctx, 0, False)
+    for _ in range(spec.steps - 4):
         ctx.step()
         states.append(PT.device_state(ctx, 0, False))
     ctx.close()
-    check([states[0]] + states[3:], [ref[0]] + ref[3:], False)
+    check([states[0]] + states[4:], [ref[0]] + ref[4:], False)
