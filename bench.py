@@ -437,14 +437,15 @@ def run_adjoint(args):
 
 # ---- our arm ---------------------------------------------------------------------------------
 def launches_per_step(spec, ray_capacity, itercount=5, hpx_lvl=0):
-    """Kernels one fused step launches: clear_lit, step_begin, advance, lit_compact, moved_pack,
-    dark, lit_init, itercount x (ray pass + lit pass), count, 3 merge set-up kernels (+4 binning
-    kernels when the pool can reach the merge threshold), compact_split, swap, the cast's count
-    and scan of the new rays' positions, cast."""
-    n = 1 + 1 + 1 + 1 + 1 + 1 + 1 + 2 * itercount + 1 + 3 + 2 + 3
+    """Kernels one fused step launches: clear_lit, step_begin, advance, lit_compact, pk_slots,
+    dark, lit_init, itercount x (ray pass + lit pass), the split thresholds (when the pool can
+    reach the merge threshold also count and 2 merge set-up kernels before them and 4 binning
+    kernels after them), compact_split, swap, the cast's count and scan of the new rays'
+    positions, cast."""
+    n = 1 + 1 + 1 + 1 + 1 + 1 + 1 + 2 * itercount + 1 + 2 + 3
     num_thresh = (spec.ray_per_cell_max - 12 * 4 ** hpx_lvl) * spec.n ** 3
     if num_thresh < ray_capacity:
-        n += 4
+        n += 3 + 4
     return n
 
 

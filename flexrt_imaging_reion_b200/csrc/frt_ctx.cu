@@ -292,8 +292,7 @@ void enqueue_step(frt_ctx* ctx, bool in_graph) {
   else cudaEventRecord(ctx->ev_d1, ctx->s_dark);
   cudaEventRecord(ctx->ev_join, ctx->s_dark);
   enqueue_iterations(ctx, true, in_graph);
-  launch_count(d, ctx->grid_rays, s);
-  launch_merge(d, ctx->grid_rays, s);
+  launch_count_merge(d, ctx->grid_rays, s);
   launch_split_compact(d, ctx->nsm * ctx->tune.split_grid, s);
   cudaStreamWaitEvent(s, ctx->ev_join, 0);
   if (!in_graph && ctx->cast_per_source) launch_cast_per_source(d, s);
@@ -563,7 +562,7 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
     AL(P.xh, R); AL(P.yh, R); AL(P.zh, R); AL(P.nphot, R * d.F);
     AL(P.r, R); AL(P.dr, R); AL(P.x, R); AL(P.y, R); AL(P.z, R); AL(P.time, R);
   }
-  AL(d.segs, R * d.PL); AL(d.nseg, R); AL(d.dead, R);
+  AL(d.dead, R);
   AL(d.pk, R * d.PL); AL(d.mv_hdr, R);
   // merge bins only when some box can reach its merge threshold with this pool size
   bool merge_reachable = false;
@@ -1512,8 +1511,7 @@ frt_status frt_step_phase(frt_ctx* ctx, int phase, int iter, const uint16_t* ith
       launch_litpass(d, iter, ctx->strict, true, ctx->nsm * ctx->tune.lit_grid, s);
       break;
     case FRT_PHASE_END:
-      launch_count(d, ctx->grid_rays, s);
-      launch_merge(d, ctx->grid_rays, s);
+      launch_count_merge(d, ctx->grid_rays, s);
       launch_split_compact(d, ctx->nsm * ctx->tune.split_grid, s);
       CK(cudaStreamWaitEvent(s, ctx->ev_join, 0));
       launch_cast(d, s);
@@ -2201,8 +2199,7 @@ frt_status frt_autotune(frt_ctx* ctx, int steps, frt_tuning* out) {
       launch_litpass(d, it, ctx->strict, true, ctx->nsm * b.grid, s);
       if (tb) cudaEventRecord(ev[e++], s);
     }
-    launch_count(d, ctx->grid_rays, s);
-    launch_merge(d, ctx->grid_rays, s);
+    launch_count_merge(d, ctx->grid_rays, s);
     for (int q = 0; q < (int)cs.size(); q++) {
       int lo, hi;
       share(nray, (int)cs.size(), q, &lo, &hi);

@@ -239,237 +239,170 @@ __global__ void __launch_bounds__(256) k_lit_chunk_write(Dev d, const int* chunk
 // advance_ray (ray_tracing.cc:1222-1512) with c2ray_iter = TRUE and fion = 1 (plain mode):
 // cell-boundary walk over c_sim * time, path segments {cell, dist}, periodic wrap, corner nudge.
 //
-// Work layout. A tile of T consecutive pool rays is loaded by T threads (coalesced) into shared
-// memory and counting-sorted by a key of the ray's direction octant and its estimated number of
-// segments; thread t then walks the tile's t-th ray in key order. The walk's arithmetic depends on
-// the signs of the direction (a float quotient for a positive component, a double one for a
-// negative, ray_tracing.cc:1273-1296) and its trip count on the number of segments, so after the
-// sort the lanes of a warp take the same branches and end together instead of every warp running
-// both branches of every axis behind its longest ray. The results go back through shared memory
-// and are stored by the thread that loaded the ray (coalesced). Which thread walks which ray does
-// not change any ray's arithmetic. Rays [r_begin, min(r_end, pool size)) of the pool (the
-// autotuner times launch shapes on shares of one step's rays; the step launches the whole pool).
+// One thread per pool ray: the thread loads its ray (consecutive threads, consecutive rays:
+// coalesced), walks it (dda_walk: the exact face time of the reference only for the axes that can
+// be the next face) and stores the updated record. The walk also builds the ray passes' input:
+// the segments go to the thread's column of a shared-memory tile ([PL][T], dynamic), then the
+// block scans its moved rays (moved and not removed) and their segment counts in pool order,
+// takes the bases of both with one 64-bit atomicAdd per tile of T rays, and every thread with a
+// moved ray writes its 16-byte header {pool index, first packed segment, segment count, box} and
+// copies its segments to the packed array (the first segment of a ray carries the head bit in
+// the sign of its positive distance). A tile costs two block barriers; the scan's per-warp
+// totals are double-buffered by tile parity, so a warp that runs ahead into the next tile never
+// overwrites totals another warp still reads. The packed segments hold cells; k_pk_slots turns
+// them into lit slots once the lit cells are numbered. Rays [r_begin, min(r_end, pool size)) of
+// the pool (the autotuner times launch shapes on shares of one step's rays; the step launches
+// the whole pool).
 template <int T>
-__global__ void __launch_bounds__(T) k_advance(Dev d, int r_begin, int r_end) {
-  constexpr int kKeys = 32;   // 8 octants x 4 segment classes
-  __shared__ float s_f[9][T];  // xh yh zh x y z time r dr (results: x y z time r dr)
-  __shared__ int s_cell[T];
-  __shared__ uint16_t s_box[T];
-  __shared__ uint8_t s_nseg[T], s_dead[T];
-  __shared__ uint16_t s_perm[T];
-  __shared__ int s_cnt[kKeys], s_base[kKeys + 1];
+__global__ void __launch_bounds__(T, 1024 / T) k_advance(Dev d, int r_begin, int r_end) {
+  constexpr int W = T / 32;
+  extern __shared__ int2 s_seg[];      // [PL][T]: segment p of thread t's ray at s_seg[p * T + t]
+  __shared__ int s_wq[2][W], s_ws[2][W];   // per-warp inclusive prefixes (moved rays, segments), by tile parity
+  __shared__ unsigned long long s_tile[2];
   const int cur = d.ctl->cur;
   const int n = min(d.ctl->nray[cur], r_end);
   const RayPool A = d.pool[cur];
   const int cap = d.ray_cap, PL = d.PL;
-  const int t = threadIdx.x;
-  long long cross = 0, moved = 0, killed = 0;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  int cross = 0, moved = 0, killed = 0;   // this thread's walks (a few thousand at most)
   double killed_ph = 0.0;
-  for (int i0 = r_begin + blockIdx.x * T; i0 < n; i0 += gridDim.x * T) {
+  int par = 0;
+  for (int i0 = r_begin + blockIdx.x * T; i0 < n; i0 += gridDim.x * T, par ^= 1) {
     const int i = i0 + t;
-    if (t < kKeys) s_cnt[t] = 0;
-    __syncthreads();
-    int key = -1, rank = 0;
+    int ns_t = 0;   // segments this thread's ray contributes to the packed list
+    uint16_t bx = 0;
     if (i < n) {
-      d.dead[i] = 0;
-      const uint16_t bx = A.box[i];
+      bx = A.box[i];
       const BoxP& B = d.box[bx];
       const float xhat = A.xh[i], yhat = A.yh[i], zhat = A.zh[i];
-      const float x0 = A.x[i], y0 = A.y[i], z0 = A.z[i];
+      float x0 = A.x[i], y0 = A.y[i], z0 = A.z[i];
       const float deltat = A.time[i] + B.dt;
       const float dist = B.clight * deltat;
       if (!ray_moves(B, x0, y0, z0, xhat, yhat, zhat, dist)) {
         A.time[i] = deltat;
-        d.nseg[i] = 0;
+        d.dead[i] = 0;
       } else {
-        s_f[0][t] = xhat;
-        s_f[1][t] = yhat;
-        s_f[2][t] = zhat;
-        s_f[3][t] = x0;
-        s_f[4][t] = y0;
-        s_f[5][t] = z0;
-        s_f[6][t] = deltat;
-        s_f[7][t] = A.r[i];
-        s_f[8][t] = A.dr[i];
-        s_cell[t] = A.cell[i];
-        s_box[t] = bx;
-        // sort key: octant of the direction, and the cell faces the straight path crosses
-        // (an estimate of the segment count: only the walk order depends on it)
-        const float inv = __fdividef(1.0f, B.dx);
-        const int faces = abs((int)floorf((x0 + dist * xhat) * inv)) + abs((int)floorf((y0 + dist * yhat) * inv)) +
-                          abs((int)floorf((z0 + dist * zhat) * inv));
-        const int oct = (xhat < 0.f ? 1 : 0) | (yhat < 0.f ? 2 : 0) | (zhat < 0.f ? 4 : 0);
-        key = oct * 4 + min(faces, 3);
-        rank = atomicAdd(&s_cnt[key], 1);
+        const int N = B.n, NN = B.nn;
+        const int ind = A.cell[i];
+        float r0 = A.r[i], dr = A.dr[i];
+        int in, jn, kn;
+        cell_ijk(ind, N, NN, B.inv_n, B.inv_nn, &in, &jn, &kn);
+        r0 += dist / B.scale;
+        dr -= dist / B.scale;
+        int2* sp = s_seg + t;
+        const int ns = dda_walk(B, PL, xhat, yhat, zhat, deltat, x0, y0, z0, in, jn, kn,
+                                [&](int p, long long gc, float ds) {
+                                  sp[p * T] = make_int2((int)gc, __float_as_int(ds));
+                                  mark_lit(d, gc);
+                                },
+                                d.ifront ? d.fion : nullptr);
+        if (ns < 0) {
+          // path overflow: the record is left as it was and the ray flagged
+          atomicOr(&d.ctl->err, ERR_PATH);
+          d.dead[i] = 1;
+        } else {
+          cross += ns;
+          moved += 1;
+          // optional removal beyond rkill (comoving), applied after update_rays
+          bool dead = false;
+          if (B.rkill > 0.0 && (double)r0 > B.rkill) {
+            dead = true;
+            killed += 1;
+            killed_ph += (double)sum_nphot(A, i, d.F, cap) * kPhotNorm;
+          }
+          d.dead[i] = dead ? 1 : 0;
+          A.time[i] = 0.f;
+          A.r[i] = r0;
+          A.dr[i] = dr;
+          A.x[i] = x0;
+          A.y[i] = y0;
+          A.z[i] = z0;
+          A.cell[i] = in * NN + jn * N + kn;
+          if (!dead) ns_t = ns;
+        }
       }
     }
-    __syncthreads();
-    if (t == 0) {
-      int acc = 0;
-      for (int k = 0; k < kKeys; k++) {
-        s_base[k] = acc;
-        acc += s_cnt[k];
-      }
-      s_base[kKeys] = acc;
+    // the tile's moved rays and their segments, in pool order: warp scans, then the warps'
+    // prefixes and one atomicAdd per tile for the bases of both
+    const unsigned mq = __ballot_sync(0xffffffffu, ns_t > 0);
+    int xs = ns_t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, xs, o);
+      if (lane >= o) xs += y;
+    }
+    if (lane == 31) {
+      s_wq[par][w] = __popc(mq);
+      s_ws[par][w] = xs;
     }
     __syncthreads();
-    if (key >= 0) s_perm[s_base[key] + rank] = (uint16_t)t;
-    __syncthreads();
-    const int nwalk = s_base[kKeys];
-    if (t < nwalk) do {
-      const int j = s_perm[t];    // the tile ray this thread walks
-      const int iw = i0 + j;
-      const BoxP& B = d.box[s_box[j]];
-      const int N = B.n;
-      const int ind = s_cell[j];
-      const int ii = ind / B.nn;
-      const int jj = (ind - ii * B.nn) / N;
-      const int kk = ind - ii * B.nn - jj * N;
-      const float xhat = s_f[0][j], yhat = s_f[1][j], zhat = s_f[2][j];
-      float x0 = s_f[3][j], y0 = s_f[4][j], z0 = s_f[5][j];
-      const float deltat = s_f[6][j];
-      const float dist = B.clight * deltat;
-      float r0 = s_f[7][j], dr = s_f[8][j];
-      r0 += dist / B.scale;
-      dr -= dist / B.scale;
-      int in = ii, jn = jj, kn = kk;
-      int2* sp = d.segs + (size_t)iw * PL;
-      const int ns = dda_walk(B, PL, xhat, yhat, zhat, deltat, x0, y0, z0, in, jn, kn,
-                              [&](int p, long long gc, float ds) {
-                                sp[p] = make_int2((int)gc, __float_as_int(ds));
-                                mark_lit(d, gc);
-                              },
-                              d.ifront ? d.fion : nullptr);
-      if (ns < 0) {
-        atomicOr(&d.ctl->err, ERR_PATH);
-        s_nseg[j] = 0;   // the record is left as it was and the ray flagged
-        s_dead[j] = 1;
-        break;
+    if (w == 0) {
+      int qa = (lane < W) ? s_wq[par][lane] : 0, sa = (lane < W) ? s_ws[par][lane] : 0;
+#pragma unroll
+      for (int o = 1; o < W; o <<= 1) {
+        const int yq = __shfl_up_sync(0xffffffffu, qa, o), ys = __shfl_up_sync(0xffffffffu, sa, o);
+        if (lane >= o) {
+          qa += yq;
+          sa += ys;
+        }
       }
-      s_nseg[j] = (uint8_t)ns;
-      s_dead[j] = 0;
-      s_f[3][j] = x0;
-      s_f[4][j] = y0;
-      s_f[5][j] = z0;
-      s_f[6][j] = 0.f;
-      s_f[7][j] = r0;
-      s_f[8][j] = dr;
-      s_cell[j] = in * B.nn + jn * N + kn;
-      cross += ns;
-      moved += 1;
-      // optional removal beyond rkill (comoving), applied after update_rays
-      if (B.rkill > 0.0 && (double)r0 > B.rkill) {
-        s_dead[j] = 1;
-        killed += 1;
-        killed_ph += (double)sum_nphot(A, iw, d.F, cap) * kPhotNorm;
+      if (lane < W) {
+        s_wq[par][lane] = qa;
+        s_ws[par][lane] = sa;
       }
-    } while (0);
+      if (lane == W - 1)
+        s_tile[par] = (qa > 0) ? atomicAdd(&d.ctl->mv_seg, ((unsigned long long)qa << 32) | (unsigned long long)sa)
+                               : 0ull;
+    }
     __syncthreads();
-    if (key >= 0) {   // this thread loaded a walked ray: store its results
-      if (s_nseg[t] == 0 && s_dead[t]) {
-        // path overflow: keep the record, flag the ray
-        d.nseg[i] = 0;
-        d.dead[i] = 1;
-      } else {
-        d.nseg[i] = s_nseg[t];
-        d.dead[i] = s_dead[t];
-        A.time[i] = 0.f;
-        A.r[i] = s_f[7][t];
-        A.dr[i] = s_f[8][t];
-        A.x[i] = s_f[3][t];
-        A.y[i] = s_f[4][t];
-        A.z[i] = s_f[5][t];
-        A.cell[i] = s_cell[t];
+    if (ns_t > 0) {
+      // the header and the segments of this thread's ray (consecutive threads' rays are
+      // consecutive in the packed list, so a warp's stores cover a few contiguous sectors)
+      const unsigned long long tb = s_tile[par];
+      const int off = (int)(tb & 0xffffffffull) + (w > 0 ? s_ws[par][w - 1] : 0) + xs - ns_t;
+      const int q = (int)(tb >> 32) + (w > 0 ? s_wq[par][w - 1] : 0) + __popc(mq & ((1u << lane) - 1u));
+      d.mv_hdr[q] = make_int4(i, off, ns_t, (int)bx);
+      int2* dp = d.pk + off;
+      for (int p = 0; p < ns_t; p++) {
+        const int2 sg = s_seg[p * T + t];
+        // dist > 0: its sign bit is free for the head mark
+        dp[p] = make_int2(sg.x, (int)(((unsigned)sg.y & 0x7fffffffu) | (p == 0 ? 0x80000000u : 0u)));
       }
     }
-    __syncthreads();   // the shared tile takes the next T rays
   }
-  cross = block_sum(cross);
-  moved = block_sum(moved);
-  killed = block_sum(killed);
+  const long long cross_b = block_sum((long long)cross);
+  const long long moved_b = block_sum((long long)moved);
+  const long long killed_b = block_sum((long long)killed);
   killed_ph = block_sum(killed_ph);
   if (threadIdx.x == 0) {
-    if (cross) atomicAdd((unsigned long long*)&d.ctl->crossings, (unsigned long long)cross);
-    if (moved) atomicAdd((unsigned long long*)&d.ctl->rays_moved, (unsigned long long)moved);
-    if (killed) atomicAdd((unsigned long long*)&d.ctl->killed, (unsigned long long)killed);
+    if (cross_b) atomicAdd((unsigned long long*)&d.ctl->crossings, (unsigned long long)cross_b);
+    if (moved_b) atomicAdd((unsigned long long*)&d.ctl->rays_moved, (unsigned long long)moved_b);
+    if (killed_b) atomicAdd((unsigned long long*)&d.ctl->killed, (unsigned long long)killed_b);
     if (killed_ph != 0.0) atomicAdd(&d.ctl->killed_ph, killed_ph);
   }
 }
 
-// The rays with segments this step (moved and not removed) and their segments, packed in
-// moved-list order for the ray passes: thread per pool ray, block-wide scans of the predicate and
-// of the segment counts, one 64-bit atomicAdd per block for both bases (so that the moved list
-// and the packed segments are allocated in the same block order). Moved ray q gets a 16-byte
-// header {pool index, first packed segment, segment count, box} that a ray pass reads at once. The
-// segment cells become lit slots here (after k_lit_compact); the first segment of each ray
-// carries the head bit (the sign of its dist, which is positive).
-__global__ void __launch_bounds__(256) k_moved_pack(Dev d) {
-  __shared__ int wt[8], ws[8];
-  __shared__ unsigned long long base_s;
-  const int n = d.ctl->nray[d.ctl->cur];
-  const uint16_t* rbox = d.pool[d.ctl->cur].box;
-  const int PL = d.PL;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const unsigned below = (1u << lane) - 1u;
-  for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
-    const int i = i0 + threadIdx.x;
-    const bool take = (i < n) && d.nseg[i] > 0 && !d.dead[i];
-    const int ns = take ? (int)d.nseg[i] : 0;
-    // the first kHeld segments and their lit slots, loaded before the scan so that the gathers
-    // are in flight while the block scans
-    constexpr int kHeld = 8;
-    const int2* sp = d.segs + (size_t)(take ? i : 0) * PL;
-    int2 sg[kHeld];
-    int sl[kHeld];
+// The packed segments' cells become lit slots once the lit cells are numbered (k_lit_compact or
+// the strict-order numbering): a coalesced pass over the packed list with one lit-slot gather per
+// segment, four segments per thread in flight.
+__global__ void __launch_bounds__(256) k_pk_slots(Dev d) {
+  const long long nseg = (long long)(d.ctl->mv_seg & 0xffffffffull);
+  int* pkx = reinterpret_cast<int*>(d.pk);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long x0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; x0 < nseg; x0 += 4 * stride) {
+    int c[4];
 #pragma unroll
-    for (int p = 0; p < kHeld; p++) sg[p] = (p < ns) ? sp[p] : make_int2(0, 0);
-#pragma unroll
-    for (int p = 0; p < kHeld; p++) sl[p] = (p < ns) ? d.lit_slot[sg[p].x] : -1;
-    const unsigned m = __ballot_sync(0xffffffffu, take);
-    int x = ns;   // inclusive scan of the segment counts over the warp
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
+    for (int u = 0; u < 4; u++) {
+      const long long x = x0 + u * stride;
+      c[u] = (x < nseg) ? pkx[2 * x] : -1;
     }
-    if (lane == 31) {
-      wt[w] = __popc(m);
-      ws[w] = x;
-    }
-    __syncthreads();
-    if (w == 0) {
-      int a = (lane < 8) ? wt[lane] : 0, b = (lane < 8) ? ws[lane] : 0;
 #pragma unroll
-      for (int o = 1; o < 8; o <<= 1) {
-        const int ya = __shfl_up_sync(0xffffffffu, a, o), yb = __shfl_up_sync(0xffffffffu, b, o);
-        if (lane >= o) {
-          a += ya;
-          b += yb;
-        }
-      }
-      if (lane < 8) {   // inclusive prefixes over the warps
-        wt[lane] = a;
-        ws[lane] = b;
-      }
-      if (lane == 7)
-        base_s = (a > 0) ? atomicAdd(&d.ctl->mv_seg, ((unsigned long long)a << 32) | (unsigned long long)b) : 0ull;
-    }
-    __syncthreads();
-    if (take) {
-      const int q = (int)(base_s >> 32) + (w > 0 ? wt[w - 1] : 0) + __popc(m & below);
-      const int off = (int)(base_s & 0xffffffffull) + (w > 0 ? ws[w - 1] : 0) + (x - ns);
-      d.mv_hdr[q] = make_int4(i, off, ns, (int)rbox[i]);
-      int2* dp = d.pk + off;
-      // dist > 0: its sign bit is free for the head mark
+    for (int u = 0; u < 4; u++) c[u] = (c[u] >= 0) ? d.lit_slot[c[u]] : -1;
 #pragma unroll
-      for (int p = 0; p < kHeld; p++)
-        if (p < ns) dp[p] = make_int2(sl[p], (int)(((unsigned)sg[p].y & 0x7fffffffu) | (p == 0 ? 0x80000000u : 0u)));
-      for (int p = kHeld; p < ns; p++) {
-        const int2 c = sp[p];
-        dp[p] = make_int2(d.lit_slot[c.x], (int)((unsigned)c.y & 0x7fffffffu));
-      }
+    for (int u = 0; u < 4; u++) {
+      const long long x = x0 + u * stride;
+      if (x < nseg) pkx[2 * x] = c[u];
     }
-    __syncthreads();
   }
 }
 
@@ -723,7 +656,7 @@ __global__ void k_merge_final(Dev d, double pi_sf_3, double log4) {
 // (the order the reference's slots take them in: split_rays appends children after the rays it
 // keeps, rt_funcs.cc:211-237), which the I-front photon budget needs.
 template <int MODE>
-__global__ void __launch_bounds__(256) k_compact_split(Dev d, int r_begin, int r_end) {
+__global__ void __launch_bounds__(256, 4) k_compact_split(Dev d, int r_begin, int r_end) {
   __shared__ int s_cell[256], s_pixel[256], s_dst[256];
   __shared__ float s_xh[256], s_yh[256], s_zh[256], s_r[256], s_x[256], s_y[256], s_z[256], s_time[256];
   __shared__ float s_nph[FRT_MAX_FREQ][256];
@@ -742,14 +675,16 @@ __global__ void __launch_bounds__(256) k_compact_split(Dev d, int r_begin, int r
   double inflight = 0.0;
   for (int i0 = r_begin + blockIdx.x * 256; i0 < n; i0 += gridDim.x * 256) {
     const int i = i0 + t;
-    const bool live = (i < n) && !d.dead[i];
     int cell = 0, pixel = 0;
     uint16_t bx = 0, ith = 0;
     int16_t order = 0;
     float xh = 0.f, yh = 0.f, zh = 0.f, r = 0.f, dr = 0.f, x = 0.f, y = 0.f, z = 0.f, tm = 0.f, sum = 0.f;
     float nph[FRT_MAX_FREQ];
-    bool split = false;
-    if (live) {
+    bool split = false, live = false;
+    if (i < n) {
+      // the record is loaded with the dead flag, not after it (every slot below n holds a written
+      // record), so that the tile waits for one round trip to memory instead of two
+      live = !d.dead[i];
       cell = A.cell[i];
       bx = A.box[i];
       order = A.order[i];
@@ -770,7 +705,7 @@ __global__ void __launch_bounds__(256) k_compact_split(Dev d, int r_begin, int r
         sum += (nu < F) ? nph[nu] : 0.f;
       }
       const BoxP& B = d.box[bx];
-      split = (r > B.rmax[order]) && (order < kLmax) && (sum > B.split_thr);
+      split = live && (r > B.rmax[order]) && (order < kLmax) && (sum > B.split_thr);
     }
     // one block-wide exclusive scan: slots (low 16 bits, at most 1024) and split rank (high bits);
     // in the ordered modes the low bits count the live rays that are not split
@@ -880,7 +815,8 @@ __global__ void __launch_bounds__(256) k_compact_split(Dev d, int r_begin, int r
       float y0 = (float)((double)s_y[k] + ((double)ny - (double)s_yh[k]) * (double)rs);
       float z0 = (float)((double)s_z[k] + ((double)nz - (double)s_zh[k]) * (double)rs);
       const int ind = s_cell[k];
-      const int ic = ind / B.nn, jcl = (ind - ic * B.nn) / N, kc = ind - ic * B.nn - jcl * N;
+      int ic, jcl, kc;
+      cell_ijk(ind, N, B.nn, B.inv_n, B.inv_nn, &ic, &jcl, &kc);
       int icn = ic, jcn = jcl, kcn = kc;
       for (int g = 0; g < 64 && x0 > B.dx; g++) { x0 -= B.dx; icn = imod(icn + 1, N); }
       for (int g = 0; g < 64 && x0 < 0.f; g++) { x0 += B.dx; icn = imod(icn - 1, N); }
@@ -1226,15 +1162,17 @@ __global__ void k_fill_i32(int* p, int v, long long n) {
 // ---- launchers ------------------------------------------------------------------------------
 void launch_step_begin(const Dev& d, cudaStream_t s) { k_step_begin<<<grid_for(d.nsrc + 1, 256, 1184), 256, 0, s>>>(d); }
 
+// k_advance's dynamic shared memory holds a tile's segments: block * path_length * 8 bytes
+// (32 KB at most: 256 threads, FRT_MAX_PATH = 16)
 static void launch_k_advance(const Dev& d, int grid, int block, int r_begin, int r_end, cudaStream_t s) {
-  if (block <= 128) k_advance<128><<<grid, 128, 0, s>>>(d, r_begin, r_end);
-  else k_advance<256><<<grid, 256, 0, s>>>(d, r_begin, r_end);
+  if (block <= 128) k_advance<128><<<grid, 128, sizeof(int2) * 128 * d.PL, s>>>(d, r_begin, r_end);
+  else k_advance<256><<<grid, 256, sizeof(int2) * 256 * d.PL, s>>>(d, r_begin, r_end);
 }
 
 void launch_advance(const Dev& d, int grid, cudaStream_t s, int block, int pack_grid) {
   launch_k_advance(d, grid, block, 0, INT_MAX, s);
   k_lit_compact<<<grid_for(d.ncell_total >> 4, 256, 148 * 8), 256, 0, s>>>(d);
-  k_moved_pack<<<pack_grid > 0 ? pack_grid : grid, 256, 0, s>>>(d);
+  k_pk_slots<<<pack_grid > 0 ? pack_grid : grid, 256, 0, s>>>(d);
 }
 
 void launch_walk(const Dev& d, int grid, cudaStream_t s, int block, int r_begin, int r_end) {
@@ -1243,19 +1181,31 @@ void launch_walk(const Dev& d, int grid, cudaStream_t s, int block, int r_begin,
 
 void launch_lit_number(const Dev& d, int grid, cudaStream_t s) {
   k_lit_compact<<<grid_for(d.ncell_total >> 4, 256, 148 * 8), 256, 0, s>>>(d);
-  k_moved_pack<<<grid, 256, 0, s>>>(d);
+  k_pk_slots<<<grid, 256, 0, s>>>(d);
 }
 
 void launch_lit_number_ordered(const Dev& d, int* chunk, long long nchunk, int grid, cudaStream_t s) {
   k_lit_chunk_count<<<grid, 256, 0, s>>>(d, chunk, nchunk);
   k_lit_chunk_scan<<<1, 1024, 0, s>>>(d, chunk, nchunk);
   k_lit_chunk_write<<<grid, 256, 0, s>>>(d, chunk, nchunk);
-  k_moved_pack<<<grid, 256, 0, s>>>(d);
+  k_pk_slots<<<grid, 256, 0, s>>>(d);
 }
 
 void launch_count(const Dev& d, int grid, cudaStream_t s) {
   cudaMemsetAsync(d.count, 0, sizeof(long long) * d.nbox, s);
   k_count<<<grid, 256, 0, s>>>(d);
+}
+
+// The step's count_rays + merge: when no box can reach its merge threshold with this pool size
+// (no merge bins), the per-box counts cannot exceed a threshold, so only the split thresholds are
+// refreshed (k_merge_thresh, with every need_hist at its initial 0).
+void launch_count_merge(const Dev& d, int grid, cudaStream_t s) {
+  if (d.bin_base) {
+    launch_count(d, grid, s);
+    launch_merge(d, grid, s);
+  } else {
+    k_merge_thresh<<<grid_for(d.nbox, 128, 1024), 128, 0, s>>>(d, d.lg);
+  }
 }
 
 void launch_merge(const Dev& d, int grid, cudaStream_t s) {

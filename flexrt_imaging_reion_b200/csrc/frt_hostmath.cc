@@ -117,6 +117,8 @@ void box_params(BoxP* B, const frt_config* cfg, const frt_box_desc* bd, long lon
   const int n = bd->n;
   B->n = n;
   B->nn = n * n;
+  B->inv_n = 1.0 / n;
+  B->inv_nn = 1.0 / ((double)n * n);
   B->cell0 = cell0;
   B->ncell = (long long)n * n * n;
   const float Lx0 = bd->box_hmpc * 1e3 / kHh;                        // user_inputs.h:92

@@ -8,7 +8,7 @@
 //    with the per-iteration C2Ray state of just those cells, so that the 5 C2Ray iterations
 //    only revisit lit cells while all other cells do their whole step in one streaming pass;
 //  * two ray pools (the current one and the one the next step compacts into) indexed by ray,
-//    plus the per-step path segments [path_length][capacity];
+//    plus the step's path segments of the moved rays, packed in moved-list order;
 //  * a control block with the pool counts, lit count, error word and per-step totals.
 #pragma once
 #include <cuda_runtime.h>
@@ -41,7 +41,7 @@ struct Ctl {
   unsigned err;
   int any_merge;           // some box has nphot_merge > 0
   // moved rays this step (high 32 bits) and their segments (low 32 bits), counted together so
-  // that one atomicAdd gives a block both bases (k_moved_pack)
+  // that one atomicAdd gives a tile of the walk both bases (k_advance)
   unsigned long long mv_seg;
   int ord_surv;            // live rays kept by the ordered compaction (k_order_scan)
   int if_changed;          // I-front budget: some crossing's entry sum changed in the last round
@@ -101,10 +101,8 @@ struct Dev {
   float cH1_f[FRT_MAX_FREQ], cHe1_f[FRT_MAX_FREQ];  // h (h_eV nu - Eth)/h_eV
   // rays
   RayPool pool[2];
-  int2* segs;              // [ray_cap][PL] {cell (then lit slot), dist bits}: a ray's segments contiguous
-  uint8_t* nseg;
   int4* mv_hdr;            // [ray_cap] moved ray q: {pool index, first packed segment, segments, box}
-  int2* pk;                // [ray_cap][PL] packed segments {lit slot, dist bits | head bit}, moved-list order
+  int2* pk;                // [ray_cap * PL] packed segments {cell, then lit slot; dist bits | head bit}, moved-list order
   uint8_t* dead;
   int* ray_bin;            // merge bin of a candidate or -1
   uint8_t* merged_flag;
@@ -203,11 +201,12 @@ void launch_step_begin(const Dev& d, cudaStream_t s);
 void launch_advance(const Dev& d, int grid, cudaStream_t s, int block = 256, int pack_grid = 0);
 // k_advance alone, over pool rays [r_begin, r_end)
 void launch_walk(const Dev& d, int grid, cudaStream_t s, int block = 256, int r_begin = 0, int r_end = 0x7fffffff);
-void launch_lit_number(const Dev& d, int grid, cudaStream_t s);   // k_lit_compact + k_moved_pack
+void launch_lit_number(const Dev& d, int grid, cudaStream_t s);   // k_lit_compact + k_pk_slots
 // the same with the lit cells numbered in strict cell order (chunk: ncell/4096 ints of scratch)
 void launch_lit_number_ordered(const Dev& d, int* chunk, long long nchunk, int grid, cudaStream_t s);
 void launch_count(const Dev& d, int grid, cudaStream_t s);
 void launch_merge(const Dev& d, int grid, cudaStream_t s);
+void launch_count_merge(const Dev& d, int grid, cudaStream_t s);   // the step's count + merge
 void launch_split_compact(const Dev& d, int grid, cudaStream_t s);
 // k_compact_split over pool rays [r_begin, r_end) without the pool swap; then launch_swap
 void launch_split_range(const Dev& d, int grid, int r_begin, int r_end, cudaStream_t s);

@@ -28,6 +28,7 @@ struct ThermConst {
 
 struct BoxP {
   int n, nn;                 // cells per side, n*n
+  double inv_n, inv_nn;      // 1/n, 1/(n*n) (cell_ijk)
   long long cell0, ncell;    // first global cell, n^3
   float dx, dx0, scale;      // proper cell, comoving cell, dx/dx0 (float, ray_tracing.cc:1262)
   float dx_half;             // dx/2. (ray_tracing.cc:308)

@@ -120,8 +120,8 @@ __global__ void k_lit_init(Dev d) {
 }
 
 // ---- ray pass of one C2Ray iteration (ray_tracing.cc:701-938), plain mode ------------------
-// The moved rays walk their packed segments (k_moved_pack: lit slot + path length, in moved-list
-// order), attenuate the photon count per bin with the current time-averaged neutral densities of
+// The moved rays walk their packed segments (k_advance and k_pk_slots: lit slot + path length,
+// in moved-list order), attenuate the photon count per bin with the current time-averaged neutral densities of
 // the lit cells, and deposit Gamma_HI / HeI; LAST also writes the per-bin output fields (diag),
 // the new photon counts, and removes rays below nphot_min.
 
@@ -604,22 +604,26 @@ __global__ void __launch_bounds__(256, 4) k_dark(Dev d) {
        gc += (long long)gridDim.x * blockDim.x) {
     const int b = box_of_cell(d, gc);
     if (b < 0) continue;   // padding between boxes
-    if (d.lit_flag[gc]) continue;
-    const BoxP& B = d.box[b];
-    if (gc - B.cell0 >= B.ncell) continue;
-    const float dt = B.dt;
+    // every input of the cell is requested together with its lit flag (one round trip to memory
+    // instead of two; a lit cell's sectors are read for the dark cells beside it anyway), and
+    // all before any store
+    const uint8_t lit = d.lit_flag[gc];
     const float nH = d.nH[gc], nHe = d.nHe[gc];
     const float nh1 = d.nH1[gc], nhe1 = d.nHe1[gc];
     const float temp0 = d.temp[gc];
     const float cl = d.clump ? d.clump[gc] : d.const_clump;
-    // the inputs of the bookkeeping and the thermal update, loaded before any store
     const bool flag = d.treion_flag[gc] != 0;
     const float ne_old = d.ne[gc];
     const float heat_old = THERMAL ? d.heat[gc] : 0.f, cool_old = THERMAL ? d.cool[gc] : 0.f;
+    const float y0h = d.f_H1[gc], y0he = d.f_He1[gc];
+    if (lit) continue;
+    const BoxP& B = d.box[b];
+    if (gc - B.cell0 >= B.ncell) continue;
+    const float dt = B.dt;
     float rh, rhe;
     recomb_coeffs<STRICT>(temp0, &rh, &rhe);
-    const C2Species H{nH, d.f_H1[gc], cl * rh};
-    const C2Species He{nHe, d.f_He1[gc], cl * rhe};
+    const C2Species H{nH, y0h, cl * rh};
+    const C2Species He{nHe, y0he, cl * rhe};
     float a = nh1, bb = nhe1, a_prev = nh1;
     float nh1_end = 0.f, nhe1_end = 0.f;
     double nelec_last = 0.0;
