@@ -56,10 +56,11 @@ RAYPASS_BYTES_PER_CROSSING = 8 + 8 + 68
 # warm-up steps that frt_autotune takes (the last ones of the warm-up)
 AUTOTUNE_STEPS = 4
 RAYPASS_TRAFFIC_BYTES_PER_CROSSING = 38.9
-# Walk (k_advance): per live ray its record read (cell, geometry, order/pixel/itheta, time: 44 B)
-# and written back (30 B); per crossing its segment {cell, dist} written (8 B) and the cell's
-# lit mark (1 B).
-WALK_BYTES_PER_RAY = 44 + 30
+# Walk (k_advance): per live ray its record read (cell, geometry, box, time: 44 B) and written
+# back with its removal flag (29 B); per moved ray the 16-byte header of the ray passes; per
+# crossing its packed segment {cell, dist} written (8 B) and the cell's lit mark (1 B).
+WALK_BYTES_PER_RAY = 44 + 29
+WALK_BYTES_PER_MOVED = 16
 WALK_BYTES_PER_CROSSING = 8 + 1
 
 
@@ -564,7 +565,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     d2h = 0
     launches = 0
     lit = 0
-    alive = moved = 0
+    alive = moved = split = killed = 0
     per_step = launches_per_step(spec, args.ray_capacity, itercount)
     walk_ms, walked = 0.0, 0
     prev_alive = ctx.num_rays()
@@ -583,8 +584,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         lit += st["lit_cells"]
         alive += st["rays_alive"]
         moved += st["rays_moved"]
+        split += st["rays_split"]
+        killed += st["rays_killed"]
     wall = time.perf_counter() - t0
     clk = clocks.stop()
+    walk_bytes = WALK_BYTES_PER_RAY * walked + WALK_BYTES_PER_MOVED * moved + WALK_BYTES_PER_CROSSING * cross
     d2h = 144  # control block (per-step totals) read back each step
     # the state after the last timed step in the reference's restart formats: the CPU baseline
     # resumes the reference from it (a steady-state sample instead of the set-up-dominated first
@@ -642,17 +646,18 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                       "traffic_per_step": DARK_TRAFFIC_BYTES_PER_CELL * (ncell - lit / args.steps),
                       "note": "CUDA-event span on its own stream, overlapped with the higher-priority "
                               "lit-cell chain; not its busy time"},
-        # the walk: every live ray advanced, its segments and lit-cell marks written
-        "walk": {"kernel": "k_advance (update_rays: every live ray walked one step)",
+        # the walk: every live ray advanced, the moved rays' headers, segments and lit-cell marks
+        # written
+        "walk": {"kernel": "k_advance (update_rays: every live ray walked one step, the ray passes' "
+                           "headers and packed segments written)",
                  "launch_ms": walk_ms / args.steps,
-                 "algorithmic_bytes_per_launch": (WALK_BYTES_PER_RAY * walked + WALK_BYTES_PER_CROSSING * cross) / args.steps,
-                 "achieved": ((WALK_BYTES_PER_RAY * walked + WALK_BYTES_PER_CROSSING * cross) / (walk_ms * 1e-3) / 1e9
-                              if walk_ms > 0 else None),
+                 "algorithmic_bytes_per_launch": walk_bytes / args.steps,
+                 "achieved": (walk_bytes / (walk_ms * 1e-3) / 1e9 if walk_ms > 0 else None),
                  "unit": "GB/s", "peak": peak,
-                 "frac": ((WALK_BYTES_PER_RAY * walked + WALK_BYTES_PER_CROSSING * cross) / (walk_ms * 1e-3) / 1e9 / peak
-                          if walk_ms > 0 and peak else None),
+                 "frac": (walk_bytes / (walk_ms * 1e-3) / 1e9 / peak if walk_ms > 0 and peak else None),
                  "rays_per_launch": walked / args.steps,
-                 "bytes_per_ray": WALK_BYTES_PER_RAY, "bytes_per_crossing": WALK_BYTES_PER_CROSSING},
+                 "bytes_per_ray": WALK_BYTES_PER_RAY, "bytes_per_moved_ray": WALK_BYTES_PER_MOVED,
+                 "bytes_per_crossing": WALK_BYTES_PER_CROSSING},
         "gpu_launches": launches,
         "clocks": clk,
         "crossings_per_step": cross / args.steps,
@@ -661,6 +666,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "lit_cells_per_step": lit / args.steps,
         "rays_alive_per_step": alive / args.steps,
         "rays_moved_per_step": moved / args.steps,
+        "rays_split_per_step": split / args.steps,
+        "rays_killed_per_step": killed / args.steps,
     }
     ctx.close()
     if restart_files is not None:
