@@ -500,6 +500,8 @@ frt_status frt_create(const frt_config* cfg, frt_ctx** out) {
     d.sigH1_l2[nu] = (float)(d.sigH1_d[nu] * 1.4426950408889634);
     d.sigHe1_l2[nu] = (float)(d.sigHe1_d[nu] * 1.4426950408889634);
   }
+  d.nho = 0;
+  while (d.nho < d.F && d.sigHe1_f[d.nho] == 0.f) d.nho++;
   // device memory
   AL(d.box, cfg->nbox);
   AL(d.count, cfg->nbox);

@@ -16,11 +16,6 @@ namespace frt {
 
 namespace {
 
-__device__ __forceinline__ int imod(int a, int b) {
-  while (a < 0) a += b;
-  return a % b;
-}
-
 // Rotation of a unit vector by the precomputed coefficient table: the reference evaluates
 // (c00)*xhat + (c01)*yhat + (c02)*zhat with each coefficient a float product of cosf/sinf
 // values (healpix_funcs.cc:102-143); the host builds those coefficients with the same
@@ -657,8 +652,12 @@ __global__ void k_merge_final(Dev d, double pi_sf_3, double log4) {
 // keeps, rt_funcs.cc:211-237), which the I-front photon budget needs.
 template <int MODE>
 __global__ void __launch_bounds__(256, 4) k_compact_split(Dev d, int r_begin, int r_end) {
-  __shared__ int s_cell[256], s_pixel[256], s_dst[256];
-  __shared__ float s_xh[256], s_yh[256], s_zh[256], s_r[256], s_x[256], s_y[256], s_z[256], s_time[256];
+  // a split ray's record for its children: position, direction and r * scale as the doubles the
+  // children's positions are formed in (ray_tracing.cc:586-588), its cell as (i, j, k)
+  __shared__ int s_pixel[256], s_dst[256];
+  __shared__ int3 s_ijk[256];
+  __shared__ double s_pd[3][256], s_hd[3][256], s_rsd[256];
+  __shared__ float s_r[256], s_time[256];
   __shared__ float s_nph[FRT_MAX_FREQ][256];
   __shared__ uint16_t s_box[256], s_ith[256];
   __shared__ int16_t s_order[256];
@@ -776,18 +775,22 @@ __global__ void __launch_bounds__(256, 4) k_compact_split(Dev d, int r_begin, in
       const int k = excl >> 16;
       nsplit += 1;
       s_dst[k] = j;
-      s_cell[k] = cell;
       s_pixel[k] = pixel;
       s_box[k] = bx;
       s_ith[k] = ith;
       s_order[k] = order;
-      s_xh[k] = xh;
-      s_yh[k] = yh;
-      s_zh[k] = zh;
+      s_hd[0][k] = (double)xh;
+      s_hd[1][k] = (double)yh;
+      s_hd[2][k] = (double)zh;
       s_r[k] = r;
-      s_x[k] = x;
-      s_y[k] = y;
-      s_z[k] = z;
+      const BoxP& B = d.box[bx];
+      s_rsd[k] = (double)(r * B.scale);
+      s_pd[0][k] = (double)x;
+      s_pd[1][k] = (double)y;
+      s_pd[2][k] = (double)z;
+      int ic, jcl, kc;
+      cell_ijk(cell, B.n, B.nn, B.inv_n, B.inv_nn, &ic, &jcl, &kc);
+      s_ijk[k] = make_int3(ic, jcl, kc);
       s_time[k] = tm;
 #pragma unroll
       for (int nu = 0; nu < FRT_MAX_FREQ; nu++)
@@ -806,24 +809,24 @@ __global__ void __launch_bounds__(256, 4) k_compact_split(Dev d, int r_begin, in
       const int pix = 4 * s_pixel[k] + c;
       const uint16_t cith = s_ith[k];
       const float r0 = s_r[k];
-      const float rs = r0 * B.scale;
+      const double rsd = s_rsd[k];   // (double)(r0 * scale)
       float fx, fy, fz;
       pix_dir(d, l + 1, pix, &fx, &fy, &fz);
       float nx, ny, nz;
       rot_apply(d.rot + (size_t)cith * 18, fx, fy, fz, &nx, &ny, &nz);
-      float x0 = (float)((double)s_x[k] + ((double)nx - (double)s_xh[k]) * (double)rs);
-      float y0 = (float)((double)s_y[k] + ((double)ny - (double)s_yh[k]) * (double)rs);
-      float z0 = (float)((double)s_z[k] + ((double)nz - (double)s_zh[k]) * (double)rs);
-      const int ind = s_cell[k];
-      int ic, jcl, kc;
-      cell_ijk(ind, N, B.nn, B.inv_n, B.inv_nn, &ic, &jcl, &kc);
-      int icn = ic, jcn = jcl, kcn = kc;
-      for (int g = 0; g < 64 && x0 > B.dx; g++) { x0 -= B.dx; icn = imod(icn + 1, N); }
-      for (int g = 0; g < 64 && x0 < 0.f; g++) { x0 += B.dx; icn = imod(icn - 1, N); }
-      for (int g = 0; g < 64 && y0 > B.dx; g++) { y0 -= B.dx; jcn = imod(jcn + 1, N); }
-      for (int g = 0; g < 64 && y0 < 0.f; g++) { y0 += B.dx; jcn = imod(jcn - 1, N); }
-      for (int g = 0; g < 64 && z0 > B.dx; g++) { z0 -= B.dx; kcn = imod(kcn + 1, N); }
-      for (int g = 0; g < 64 && z0 < 0.f; g++) { z0 += B.dx; kcn = imod(kcn - 1, N); }
+      float x0 = (float)(s_pd[0][k] + ((double)nx - s_hd[0][k]) * rsd);
+      float y0 = (float)(s_pd[1][k] + ((double)ny - s_hd[1][k]) * rsd);
+      float z0 = (float)(s_pd[2][k] + ((double)nz - s_hd[2][k]) * rsd);
+      const int3 ijk = s_ijk[k];
+      int icn = ijk.x, jcn = ijk.y, kcn = ijk.z;
+      // the reference's mod(i +- 1, N) (imod) of an index in [0, N)
+      const float dxb = B.dx;
+      for (int g = 0; g < 64 && x0 > dxb; g++) { x0 -= dxb; icn = dda_up(icn, N); }
+      for (int g = 0; g < 64 && x0 < 0.f; g++) { x0 += dxb; icn = dda_down(icn, N); }
+      for (int g = 0; g < 64 && y0 > dxb; g++) { y0 -= dxb; jcn = dda_up(jcn, N); }
+      for (int g = 0; g < 64 && y0 < 0.f; g++) { y0 += dxb; jcn = dda_down(jcn, N); }
+      for (int g = 0; g < 64 && z0 > dxb; g++) { z0 -= dxb; kcn = dda_up(kcn, N); }
+      for (int g = 0; g < 64 && z0 < 0.f; g++) { z0 += dxb; kcn = dda_down(kcn, N); }
       Bp.cell[jc] = icn * B.nn + jcn * N + kcn;
       Bp.box[jc] = cbx;
       Bp.order[jc] = (int16_t)(l + 1);
@@ -834,7 +837,9 @@ __global__ void __launch_bounds__(256, 4) k_compact_split(Dev d, int r_begin, in
       Bp.zh[jc] = nz;
       float cs = 0.f;
       for (int nu = 0; nu < F; nu++) {
-        const float q = (float)((double)s_nph[nu][k] / 4.);
+        // (float)((double)n / 4.) of split_ray: a division by 4 is exact in double, and the float
+        // product n * 0.25f rounds the same exact value (also in the subnormal range)
+        const float q = s_nph[nu][k] * 0.25f;
         Bp.nphot[(size_t)nu * cap + jc] = q;
         cs += q;
       }

@@ -70,6 +70,7 @@ struct Dev {
   double sigH1_d[FRT_MAX_FREQ], sigHe1_d[FRT_MAX_FREQ];
   float sigH1_f[FRT_MAX_FREQ], sigHe1_f[FRT_MAX_FREQ];
   float sigH1_l2[FRT_MAX_FREQ], sigHe1_l2[FRT_MAX_FREQ];   // the same times log2(e)
+  int nho;                 // leading bins with sigma_HeI = 0 (HI alone absorbs)
   double sigH1_0, sigH1_912;
   // tables
   const float* rot;        // [kNtheta][2][9] forward, inverse

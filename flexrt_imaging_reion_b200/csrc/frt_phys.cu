@@ -234,7 +234,10 @@ __global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
 // CHUNKED compiles the queue form; the static-slice form carries none of its bookkeeping. The
 // minimum resident blocks keep the last pass (which also writes the rays' photon counts and
 // the heating pairs) at 64 registers, four 256-thread blocks per SM.
-template <bool LAST, int NF, bool CHUNKED>
+// NHO > 0 declares the first NHO bins below the HeI edge (sigma_HeI = 0 there, as in the 5-bin
+// spectrum, whose lowest three bins lie below 24.59 eV): those bins skip the HeI optical depth and
+// the H/He split, which give frac_h1 = 1 (or 0 where dtau_HI = 0) and frac_he1 = 0 for them.
+template <bool LAST, int NF, bool CHUNKED, int NHO = 0>
 __global__ void __launch_bounds__(256, LAST ? 4 : 5) k_raypass_mixed(Dev d, int iter, int chunk) {
   constexpr int MAXF = NF > 0 ? NF : FRT_MAX_FREQ;
   constexpr unsigned FULL = 0xffffffffu;
@@ -340,9 +343,23 @@ __global__ void __launch_bounds__(256, LAST ? 4 : 5) k_raypass_mixed(Dev d, int 
       for (int nu = 0; nu < MAXF; nu++) {
         if (nu >= Fr) continue;
         const float dth = ad * d.sigH1_f[nu];
-        const float dthe = bd * d.sigHe1_f[nu];
         float ah, eh;
         absorb_transmit(dth, ad * d.sigH1_l2[nu], &ah, &eh);
+        if (nu < NHO) {   // HI alone absorbs in this bin
+          const float gh = (dth > 0.f) ? nin[nu] * (dump ? 1.0f : ah) : 0.f;
+          gsum_h += gh;
+          if (LAST) {
+            hh += gh * d.cH1_f[nu];
+            if (d.per_bin) {
+              atomicAdd(&d.l_ngam[(size_t)nu * L + slot], nin[nu]);
+              if (gh != 0.f) atomicAdd(&d.l_acc_nu_h[(size_t)nu * L + slot], gh * __fdividef(kdep, a));
+            }
+            if (dump && dth > 0.f) dump_mask |= 1u << nu;
+          }
+          nin[nu] *= eh;
+          continue;
+        }
+        const float dthe = bd * d.sigHe1_f[nu];
         float fh, fhe, absb, e;
         if (dthe > 0.f) {
           float ahe, ehe;
@@ -779,7 +796,15 @@ void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t 
     return;
   }
   const bool q = chunk > 0;
-  if (d.F == 5) {
+  if (d.F == 5 && d.nho >= 3) {
+    if (last) {
+      if (q) k_raypass_mixed<true, 5, true, 3><<<grid, block, 0, s>>>(d, iter, chunk);
+      else k_raypass_mixed<true, 5, false, 3><<<grid, block, 0, s>>>(d, iter, chunk);
+    } else {
+      if (q) k_raypass_mixed<false, 5, true, 3><<<grid, block, 0, s>>>(d, iter, chunk);
+      else k_raypass_mixed<false, 5, false, 3><<<grid, block, 0, s>>>(d, iter, chunk);
+    }
+  } else if (d.F == 5) {
     if (last) {
       if (q) k_raypass_mixed<true, 5, true><<<grid, block, 0, s>>>(d, iter, chunk);
       else k_raypass_mixed<true, 5, false><<<grid, block, 0, s>>>(d, iter, chunk);
