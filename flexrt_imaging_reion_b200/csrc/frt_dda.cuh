@@ -52,12 +52,28 @@ __device__ __forceinline__ bool ray_moves(const BoxP& B, float x0, float y0, flo
 }
 
 // The reference's time to the next cell face along one axis (ray_tracing.cc:1273-1296): a float
-// quotient for a positive direction component, a double one rounded to float for a negative
-// component, infinity for a zero component.
+// quotient for a positive direction component, ((dx - x0) / xhat) / clight in float, a double one
+// rounded to float for a negative component, (float)((-x0 / xhat) / clight) in double, infinity
+// for a zero component.
 __host__ __device__ __forceinline__ float face_time(float pos, float hat, float dxc, float clgt, double cld) {
   if (hat > 0.f) return (dxc - pos) / hat / clgt;
   if (hat < 0.f) return (float)(-1. * (double)pos / (double)hat / cld);
   return INFINITY;
+}
+
+// The same time for a nonzero component as one instruction sequence for both signs, so that the
+// lanes of a warp never split between a float and a double path. The float quotients of the
+// positive case are formed as double quotients rounded to float: for binary32 operands a binary64
+// quotient rounded to binary32 is the correctly rounded binary32 quotient, because 53 >= 2*24 + 2
+// (double rounding is innocuous for the basic operations under that condition; Figueroa, "When is
+// double rounding innocuous?", SIGNUM Newsletter 30(3), 1995), so each of the two roundings
+// equals the float division's.
+__host__ __device__ __forceinline__ float face_time_nz(float pos, float hat, float dxc, double cld) {
+  const bool pos_dir = hat > 0.f;
+  const double num = pos_dir ? (double)(dxc - pos) : -1. * (double)pos;
+  double q = num / (double)hat;
+  if (pos_dir) q = (double)(float)q;   // the float quotient (dx - x0) / xhat
+  return (float)(q / cld);
 }
 
 // Approximate face times rank the axes; the exact expression is evaluated only for the axes that
@@ -112,7 +128,7 @@ __host__ __device__ __forceinline__ int dda_walk(const BoxP& B, int PL, float xh
       tag = (cand == 1u) ? 0 : ((cand == 2u) ? 1 : 2);
       const float pos = (tag == 0) ? x0 : ((tag == 1) ? y0 : z0);
       const float hat = (tag == 0) ? xhat : ((tag == 1) ? yhat : zhat);
-      tmin = face_time(pos, hat, dxc, clgt, cld);
+      tmin = face_time_nz(pos, hat, dxc, cld);   // (an axis with a finite approximation: hat != 0)
     } else {
       // near-ties (or no usable approximation): the exact times of the candidate axes, the
       // others slower than the minimum, and the reference's tie rule
