@@ -2089,7 +2089,8 @@ frt_status frt_get_tuning(frt_ctx* ctx, frt_tuning* out) {
 
 frt_status frt_set_tuning(frt_ctx* ctx, const frt_tuning* in) {
   if (!ctx || !in) return FRT_ERR_INVALID;
-  if (!block_ok(in->raypass_block) || !grid_ok(in->raypass_blocks_per_sm) || in->raypass_chunk < 0 ||
+  if (!block_ok(in->raypass_block) || !(in->raypass_blocks_per_sm == 0 || grid_ok(in->raypass_blocks_per_sm)) ||
+      in->raypass_chunk < 0 ||
       in->raypass_chunk > 65536 || !block_ok(in->walk_block) || !grid_ok(in->walk_blocks_per_sm) ||
       !grid_ok(in->cellpass_blocks_per_sm) || !grid_ok(in->split_blocks_per_sm)) {
     ctx->err = "frt_set_tuning: blocks 32..256 in multiples of 32, 1..32 blocks per SM, chunk 0..65536";
@@ -2125,7 +2126,8 @@ frt_status frt_autotune(frt_ctx* ctx, int steps, frt_tuning* out) {
   // into four equal ranges
   const int per_iter = std::max(1, I - 1);
   const bool tune_rp = !ctx->strict && I > 1;
-  ShapeSearch rp("raypass", Shape{t0.rp_block, t0.rp_grid, t0.rp_chunk}, {128, 256}, {4, 8, 12, 16},
+  // (ray-pass grid 0: exactly the blocks resident on the SMs, one wave of the persistent kernel)
+  ShapeSearch rp("raypass", Shape{t0.rp_block, t0.rp_grid, t0.rp_chunk}, {128, 256}, {0, 4, 8, 12, 16},
                  {0, 32, 128, 512}, per_iter);
   ShapeSearch adv("walk", Shape{t0.adv_block, t0.adv_grid, 0}, {128, 256}, {4, 8, 16}, {0}, 4);
   ShapeSearch lit("cellpass", Shape{256, t0.lit_grid, 0}, {256}, {2, 4, 8, 16}, {0}, per_iter);

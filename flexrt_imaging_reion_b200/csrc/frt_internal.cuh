@@ -156,11 +156,13 @@ struct Dev {
 constexpr int kMaxIterQueue = 16;
 
 // Launch shapes of the tunable kernels (frt_tune.h picks them; the defaults are the untuned
-// shapes). Grids are in blocks per SM; rp_chunk = 0 gives each warp of the ray pass a static
-// slice of the moved-ray list, rp_chunk > 0 lets warps take chunks of that many rays from a
-// device-side queue (one atomicAdd per chunk).
+// shapes). Grids are in blocks per SM; rp_grid = 0 launches the persistent ray pass with exactly
+// the blocks resident at once (one wave), the default: with 8 blocks per SM requested and 5
+// resident, the second wave of blocks left 40 % of the slots idle while it ran. rp_chunk = 0 gives
+// each warp of the ray pass a static slice of the moved-ray list, rp_chunk > 0 lets warps take
+// chunks of that many rays from a device-side queue (one atomicAdd per chunk).
 struct Tune {
-  int rp_block = 256, rp_grid = 8, rp_chunk = 0;
+  int rp_block = 256, rp_grid = 0, rp_chunk = 0;
   int adv_block = 256, adv_grid = 8;
   int lit_grid = 8;
   int split_grid = 8;

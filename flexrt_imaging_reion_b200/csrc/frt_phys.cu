@@ -12,6 +12,8 @@
 #include <limits.h>
 #include <math.h>
 
+#include <mutex>
+
 #include "frt_internal.cuh"
 
 namespace frt {
@@ -788,39 +790,53 @@ void launch_lit_init(const Dev& d, bool strict, int grid, cudaStream_t s) {
   else k_lit_init<false><<<grid, 256, 0, s>>>(d);
 }
 
+// The blocks of `kernel` at `block` threads that fit on all SMs at once (its occupancy times the SM
+// count), remembered per kernel and block size (a host-side query: no work is enqueued, so it may
+// run while a stream is being captured).
+template <typename K>
+static int resident_grid(K kernel, int block) {
+  struct Entry {
+    const void* k;
+    int block, grid;
+  };
+  static Entry cache[64];
+  static int n = 0;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  for (int i = 0; i < n; i++)
+    if (cache[i].k == (const void*)kernel && cache[i].block == block) return cache[i].grid;
+  int dev = 0, nsm = 148, nb = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, block, 0) != cudaSuccess || nb < 1) nb = 1;
+  const int g = nb * nsm;
+  if (n < 64) cache[n++] = Entry{(const void*)kernel, block, g};
+  return g;
+}
+
+// grid <= 0: the persistent ray pass with exactly its resident blocks (one wave: every warp's
+// static slice starts at once, none waits for a second wave)
 void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t s, int block, int chunk) {
   const bool last = iter == d.itercount - 1;
   if (strict) {
-    if (last) k_raypass_strict<true><<<grid, 256, 0, s>>>(d);
-    else k_raypass_strict<false><<<grid, 256, 0, s>>>(d);
+    if (last) k_raypass_strict<true><<<grid > 0 ? grid : 148 * 8, 256, 0, s>>>(d);
+    else k_raypass_strict<false><<<grid > 0 ? grid : 148 * 8, 256, 0, s>>>(d);
     return;
   }
   const bool q = chunk > 0;
+  void (*k)(Dev, int, int);
   if (d.F == 5 && d.nho >= 3) {
-    if (last) {
-      if (q) k_raypass_mixed<true, 5, true, 3><<<grid, block, 0, s>>>(d, iter, chunk);
-      else k_raypass_mixed<true, 5, false, 3><<<grid, block, 0, s>>>(d, iter, chunk);
-    } else {
-      if (q) k_raypass_mixed<false, 5, true, 3><<<grid, block, 0, s>>>(d, iter, chunk);
-      else k_raypass_mixed<false, 5, false, 3><<<grid, block, 0, s>>>(d, iter, chunk);
-    }
+    if (last) k = q ? k_raypass_mixed<true, 5, true, 3> : k_raypass_mixed<true, 5, false, 3>;
+    else k = q ? k_raypass_mixed<false, 5, true, 3> : k_raypass_mixed<false, 5, false, 3>;
   } else if (d.F == 5) {
-    if (last) {
-      if (q) k_raypass_mixed<true, 5, true><<<grid, block, 0, s>>>(d, iter, chunk);
-      else k_raypass_mixed<true, 5, false><<<grid, block, 0, s>>>(d, iter, chunk);
-    } else {
-      if (q) k_raypass_mixed<false, 5, true><<<grid, block, 0, s>>>(d, iter, chunk);
-      else k_raypass_mixed<false, 5, false><<<grid, block, 0, s>>>(d, iter, chunk);
-    }
+    if (last) k = q ? k_raypass_mixed<true, 5, true> : k_raypass_mixed<true, 5, false>;
+    else k = q ? k_raypass_mixed<false, 5, true> : k_raypass_mixed<false, 5, false>;
   } else {
-    if (last) {
-      if (q) k_raypass_mixed<true, 0, true><<<grid, block, 0, s>>>(d, iter, chunk);
-      else k_raypass_mixed<true, 0, false><<<grid, block, 0, s>>>(d, iter, chunk);
-    } else {
-      if (q) k_raypass_mixed<false, 0, true><<<grid, block, 0, s>>>(d, iter, chunk);
-      else k_raypass_mixed<false, 0, false><<<grid, block, 0, s>>>(d, iter, chunk);
-    }
+    if (last) k = q ? k_raypass_mixed<true, 0, true> : k_raypass_mixed<true, 0, false>;
+    else k = q ? k_raypass_mixed<false, 0, true> : k_raypass_mixed<false, 0, false>;
   }
+  const int g = grid > 0 ? grid : resident_grid(k, block);
+  k<<<g, block, 0, s>>>(d, iter, chunk);
 }
 
 void launch_litpass(const Dev& d, int iter, bool strict, bool fused_thermal, int grid, cudaStream_t s, int s_begin,

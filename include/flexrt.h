@@ -285,7 +285,8 @@ frt_status frt_last_stats(frt_ctx* ctx, frt_step_stats* stats);
  * chunks of a device-side queue). Shapes change only the work distribution, not the arithmetic of
  * a ray or a cell. */
 typedef struct {
-  int raypass_block, raypass_blocks_per_sm; /* ray pass of a C2Ray iteration (mixed precision) */
+  int raypass_block, raypass_blocks_per_sm; /* ray pass of a C2Ray iteration (mixed precision);
+                                               blocks_per_sm 0: the blocks resident at once */
   int raypass_chunk;                        /* 0: static per-warp slices; > 0: rays per queue chunk */
   int walk_block, walk_blocks_per_sm;       /* cell-boundary walk (update_rays) */
   int cellpass_blocks_per_sm;               /* lit-cell pass of a C2Ray iteration */
