@@ -531,8 +531,9 @@ def _tuning_config(t):
     keys = ("raypass_block", "raypass_blocks_per_sm", "raypass_chunk", "walk_block", "walk_blocks_per_sm",
             "cellpass_blocks_per_sm", "split_blocks_per_sm", "steps")
     out = {k: int(t[k]) for k in keys}
-    if out["raypass_blocks_per_sm"] == 0:
-        out["raypass_blocks_per_sm"] = "resident (one wave of the persistent kernel)"
+    for k in ("raypass_blocks_per_sm", "cellpass_blocks_per_sm"):
+        if out[k] == 0:
+            out[k] = "resident (one wave)"
     out["measured_ns"] = {k: round(float(t[k]), 4) for k in ("raypass_ns_per_crossing", "walk_ns_per_ray",
                                                               "cellpass_ns_per_cell", "split_ns_per_ray")}
     return out

@@ -199,6 +199,10 @@ void note_step(frt_ctx* ctx) {
   std::fill(ctx->frac_kept.begin(), ctx->frac_kept.end(), 0);
 }
 
+// The sub-grid model's cell passes take the tuned cell-pass grid, or 8 blocks per SM where that
+// grid is the resident count (which only the plain cell passes resolve)
+int sg_cell_grid(const frt_ctx* ctx) { return ctx->nsm * (ctx->tune.lit_grid > 0 ? ctx->tune.lit_grid : 8); }
+
 void record(cudaEvent_t e, cudaStream_t s, bool in_graph) {
   if (in_graph) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
   else cudaEventRecord(e, s);
@@ -242,7 +246,7 @@ void enqueue_iterations_ifront(frt_ctx* ctx, bool fused_thermal) {
     }
     if (!settled) ctx->if_unsettled = true;
     if (it == d.itercount - 1) launch_if_final(d, it, grid, s);
-    launch_sg_litpass(d, it, fused_thermal, ctx->nsm * ctx->tune.lit_grid, s);
+    launch_sg_litpass(d, it, fused_thermal, sg_cell_grid(ctx), s);
   }
 }
 
@@ -259,7 +263,7 @@ void enqueue_iterations(frt_ctx* ctx, bool fused_thermal, bool in_graph = false)
       if (timed) record(ctx->ev_r[2 * it], ctx->s_main, in_graph);
       launch_sg_raypass(d, it, ctx->grid_rays, ctx->s_main);
       if (timed) record(ctx->ev_r[2 * it + 1], ctx->s_main, in_graph);
-      launch_sg_litpass(d, it, fused_thermal, ctx->nsm * ctx->tune.lit_grid, ctx->s_main);
+      launch_sg_litpass(d, it, fused_thermal, sg_cell_grid(ctx), ctx->s_main);
     }
     return;
   }
@@ -1399,6 +1403,54 @@ frt_status frt_download_rays(frt_ctx* ctx, int box, int16_t* order, int32_t* pix
   return FRT_OK;
 }
 
+frt_status frt_set_tau_limit(frt_ctx* ctx, double tau_max) {
+  if (!ctx) return FRT_ERR_INVALID;
+  if (!(tau_max >= 0.0) || tau_max > 1e30) {
+    ctx->err = "frt_set_tau_limit: tau_max must be >= 0 (0 turns the limit off)";
+    return FRT_ERR_INVALID;
+  }
+  Dev& d = ctx->d;
+  if (tau_max > 0.0 && d.subgrid) {
+    ctx->err = "frt_set_tau_limit: not available with the sub-grid model";
+    return FRT_ERR_INVALID;
+  }
+  if (tau_max > 0.0 && !d.pool[0].col) {
+    CK(cudaStreamSynchronize(ctx->s_main));
+    for (int p = 0; p < 2; p++) AL(d.pool[p].col, 2 * (size_t)d.ray_cap);   // zero-filled
+  }
+  d.tau_max = tau_max;
+  ctx->graph_valid = false;
+  return FRT_OK;
+}
+
+frt_status frt_download_ray_columns(frt_ctx* ctx, int box, double* col2) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  if (!col2) return FRT_ERR_INVALID;
+  Ctl c;
+  CK(cudaStreamSynchronize(ctx->s_main));
+  CK(copy_sync(ctx, &c, ctx->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+  const int nr = std::min(c.nray[c.cur], ctx->d.ray_cap);
+  const RayPool& P = ctx->d.pool[c.cur];
+  std::vector<uint16_t> bx(nr);
+  std::vector<double> ch(nr, 0.0), che(nr, 0.0);
+  if (nr) {
+    CK(copy_sync(ctx, bx.data(), P.box, sizeof(uint16_t) * nr, cudaMemcpyDeviceToHost));
+    if (P.col) {
+      CK(copy_sync(ctx, ch.data(), P.col, sizeof(double) * nr, cudaMemcpyDeviceToHost));
+      CK(copy_sync(ctx, che.data(), P.col + ctx->d.ray_cap, sizeof(double) * nr, cudaMemcpyDeviceToHost));
+    }
+  }
+  size_t w = 0;
+  for (int i = 0; i < nr; i++) {
+    if (bx[i] != box) continue;
+    col2[2 * w] = ch[i];
+    col2[2 * w + 1] = che[i];
+    w++;
+  }
+  return FRT_OK;
+}
+
 frt_status frt_box_scalars(frt_ctx* ctx, int box, double* out8) {
   frt_status st = check_box(ctx, box);
   if (st) return st;
@@ -1833,6 +1885,11 @@ frt_status frt_read_rays(frt_ctx* ctx, int box, const void* buf, size_t len) {
       for (float x : np[nu]) inflight += (double)x;
     }
   }
+  if (m && d.pool[c.cur].col) {   // the restart records carry no columns: loaded rays start at 0
+    double* col = d.pool[c.cur].col;
+    CK(fill_sync(ctx, col + base, 0, sizeof(double) * m));
+    CK(fill_sync(ctx, col + d.ray_cap + base, 0, sizeof(double) * m));
+  }
   c.nray[c.cur] = (int)(base + m);
   c.in_flight += inflight * 1e60;   // photon ledger: physical photons of the loaded rays
   CK(copy_sync(ctx, d.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice));
@@ -2092,7 +2149,7 @@ frt_status frt_set_tuning(frt_ctx* ctx, const frt_tuning* in) {
   if (!block_ok(in->raypass_block) || !(in->raypass_blocks_per_sm == 0 || grid_ok(in->raypass_blocks_per_sm)) ||
       in->raypass_chunk < 0 ||
       in->raypass_chunk > 65536 || !block_ok(in->walk_block) || !grid_ok(in->walk_blocks_per_sm) ||
-      !grid_ok(in->cellpass_blocks_per_sm) || !grid_ok(in->split_blocks_per_sm)) {
+      !(in->cellpass_blocks_per_sm == 0 || grid_ok(in->cellpass_blocks_per_sm)) || !grid_ok(in->split_blocks_per_sm)) {
     ctx->err = "frt_set_tuning: blocks 32..256 in multiples of 32, 1..32 blocks per SM, chunk 0..65536";
     return FRT_ERR_INVALID;
   }
@@ -2130,7 +2187,7 @@ frt_status frt_autotune(frt_ctx* ctx, int steps, frt_tuning* out) {
   ShapeSearch rp("raypass", Shape{t0.rp_block, t0.rp_grid, t0.rp_chunk}, {128, 256}, {0, 4, 8, 12, 16},
                  {0, 32, 128, 512}, per_iter);
   ShapeSearch adv("walk", Shape{t0.adv_block, t0.adv_grid, 0}, {128, 256}, {4, 8, 16}, {0}, 4);
-  ShapeSearch lit("cellpass", Shape{256, t0.lit_grid, 0}, {256}, {2, 4, 8, 16}, {0}, per_iter);
+  ShapeSearch lit("cellpass", Shape{256, t0.lit_grid, 0}, {256}, {0, 2, 4, 8, 16}, {0}, per_iter);
   ShapeSearch spl("split", Shape{256, t0.split_grid, 0}, {256}, {2, 4, 8, 16}, {0}, 4);
   // with three steps or more, the last two validate the search on whole graph steps (below)
   const int search_steps = steps >= 3 ? steps - 2 : steps;

@@ -657,6 +657,7 @@ __global__ void __launch_bounds__(256, 4) k_compact_split(Dev d, int r_begin, in
   __shared__ int s_pixel[256], s_dst[256];
   __shared__ int3 s_ijk[256];
   __shared__ double s_pd[3][256], s_hd[3][256], s_rsd[256];
+  __shared__ double s_col[2][256];   // the split ray's columns (optical-depth limit on)
   __shared__ float s_r[256], s_time[256];
   __shared__ float s_nph[FRT_MAX_FREQ][256];
   __shared__ uint16_t s_box[256], s_ith[256];
@@ -769,6 +770,10 @@ __global__ void __launch_bounds__(256, 4) k_compact_split(Dev d, int r_begin, in
         Bp.y[j] = y;
         Bp.z[j] = z;
         Bp.time[j] = tm;
+        if (A.col) {
+          Bp.col[j] = A.col[i];
+          Bp.col[(size_t)cap + j] = A.col[(size_t)cap + i];
+        }
         inflight += (double)sum;
       }
     } else if (split) {
@@ -792,6 +797,10 @@ __global__ void __launch_bounds__(256, 4) k_compact_split(Dev d, int r_begin, in
       cell_ijk(cell, B.n, B.nn, B.inv_n, B.inv_nn, &ic, &jcl, &kc);
       s_ijk[k] = make_int3(ic, jcl, kc);
       s_time[k] = tm;
+      if (A.col) {
+        s_col[0][k] = A.col[i];
+        s_col[1][k] = A.col[(size_t)cap + i];
+      }
 #pragma unroll
       for (int nu = 0; nu < FRT_MAX_FREQ; nu++)
         if (nu < F) s_nph[nu][k] = nph[nu];
@@ -850,6 +859,10 @@ __global__ void __launch_bounds__(256, 4) k_compact_split(Dev d, int r_begin, in
       Bp.y[jc] = y0;
       Bp.z[jc] = z0;
       Bp.time[jc] = s_time[k];
+      if (A.col) {   // children inherit the columns their parent crossed
+        Bp.col[jc] = s_col[0][k];
+        Bp.col[(size_t)cap + jc] = s_col[1][k];
+      }
     }
     __syncthreads();   // the shared records take the next 256 rays
   }
@@ -1035,6 +1048,10 @@ __global__ void k_cast(Dev d, int s_begin, int s_end) {
       A.y[j] = B.dx_half;
       A.z[j] = B.dx_half;
       A.time[j] = 0.f;
+      if (A.col) {   // optical-depth limit on: no column crossed yet
+        A.col[j] = 0.0;
+        A.col[(size_t)cap + j] = 0.0;
+      }
     }
     d.src_ray_dt[s] = 0.f;
     ncast += count;
@@ -1177,7 +1194,7 @@ static void launch_k_advance(const Dev& d, int grid, int block, int r_begin, int
 void launch_advance(const Dev& d, int grid, cudaStream_t s, int block, int pack_grid) {
   launch_k_advance(d, grid, block, 0, INT_MAX, s);
   k_lit_compact<<<grid_for(d.ncell_total >> 4, 256, 148 * 8), 256, 0, s>>>(d);
-  k_pk_slots<<<pack_grid > 0 ? pack_grid : grid, 256, 0, s>>>(d);
+  k_pk_slots<<<pack_grid > 0 ? pack_grid : resident_grid(k_pk_slots, 256), 256, 0, s>>>(d);
 }
 
 void launch_walk(const Dev& d, int grid, cudaStream_t s, int block, int r_begin, int r_end) {
@@ -1186,14 +1203,14 @@ void launch_walk(const Dev& d, int grid, cudaStream_t s, int block, int r_begin,
 
 void launch_lit_number(const Dev& d, int grid, cudaStream_t s) {
   k_lit_compact<<<grid_for(d.ncell_total >> 4, 256, 148 * 8), 256, 0, s>>>(d);
-  k_pk_slots<<<grid, 256, 0, s>>>(d);
+  k_pk_slots<<<resident_grid(k_pk_slots, 256), 256, 0, s>>>(d);
 }
 
 void launch_lit_number_ordered(const Dev& d, int* chunk, long long nchunk, int grid, cudaStream_t s) {
   k_lit_chunk_count<<<grid, 256, 0, s>>>(d, chunk, nchunk);
   k_lit_chunk_scan<<<1, 1024, 0, s>>>(d, chunk, nchunk);
   k_lit_chunk_write<<<grid, 256, 0, s>>>(d, chunk, nchunk);
-  k_pk_slots<<<grid, 256, 0, s>>>(d);
+  k_pk_slots<<<resident_grid(k_pk_slots, 256), 256, 0, s>>>(d);
 }
 
 void launch_count(const Dev& d, int grid, cudaStream_t s) {

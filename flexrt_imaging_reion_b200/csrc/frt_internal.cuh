@@ -14,6 +14,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "../../include/flexrt.h"
 #include "frt_physics.cuh"
 
@@ -31,6 +33,9 @@ struct RayPool {
   float *xh, *yh, *zh;
   float* nphot;       // [F][cap]
   float *r, *dr, *x, *y, *z, *time;
+  // opt-in optical-depth limit (frt_set_tau_limit; null when off): the HI and HeI column
+  // densities ([2][cap], cm^-2 proper, FP64) each ray crossed since its cast
+  double* col;
 };
 
 struct Ctl {
@@ -57,6 +62,7 @@ struct Dev {
   int outputs;             // FRT_OUT_*
   float nhe_to_nh;
   float const_clump;
+  double tau_max;          // opt-in: remove rays whose optical depth exceeds it in every bin (0: off)
   // per-box
   BoxP* box;
   long long* count;        // live rays per box (count_rays)
@@ -155,6 +161,31 @@ struct Dev {
 
 constexpr int kMaxIterQueue = 16;
 
+// The blocks of `kernel` at `block` threads that fit on all SMs at once (its occupancy times the SM
+// count), remembered per kernel and block size (a host-side query: no work is enqueued, so it may
+// run while a stream is being captured).
+template <typename K>
+inline int resident_grid(K kernel, int block) {
+  struct Entry {
+    const void* k;
+    int block, grid;
+  };
+  static Entry cache[64];
+  static int n = 0;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  for (int i = 0; i < n; i++)
+    if (cache[i].k == (const void*)kernel && cache[i].block == block) return cache[i].grid;
+  int dev = 0, nsm = 148, nb = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, block, 0) != cudaSuccess || nb < 1) nb = 1;
+  const int g = nb * nsm;
+  if (n < 64) cache[n++] = Entry{(const void*)kernel, block, g};
+  return g;
+}
+
+
 // Launch shapes of the tunable kernels (frt_tune.h picks them; the defaults are the untuned
 // shapes). Grids are in blocks per SM; rp_grid = 0 launches the persistent ray pass with exactly
 // the blocks resident at once (one wave), the default: with 8 blocks per SM requested and 5
@@ -164,7 +195,7 @@ constexpr int kMaxIterQueue = 16;
 struct Tune {
   int rp_block = 256, rp_grid = 0, rp_chunk = 0;
   int adv_block = 256, adv_grid = 8;
-  int lit_grid = 8;
+  int lit_grid = 0;
   int split_grid = 8;
   bool operator==(const Tune& o) const {
     return rp_block == o.rp_block && rp_grid == o.rp_grid && rp_chunk == o.rp_chunk && adv_block == o.adv_block &&

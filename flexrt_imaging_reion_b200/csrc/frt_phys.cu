@@ -12,8 +12,6 @@
 #include <limits.h>
 #include <math.h>
 
-#include <mutex>
-
 #include "frt_internal.cuh"
 
 namespace frt {
@@ -148,6 +146,7 @@ __global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
     double tau_h1[FRT_MAX_FREQ], tau_he1[FRT_MAX_FREQ];
     for (int nu = 0; nu < F; nu++) { tau_h1[nu] = 0.; tau_he1[nu] = 0.; }
     const double dt = B.dt, vol = B.vol;
+    double colh = 0.0, colhe = 0.0;   // optical-depth limit: this pass's columns
     for (int p = 0; p < ns; p++) {
       const int2 sg = sp[p];
       const int slot = sg.x;
@@ -155,6 +154,8 @@ __global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
       const float dist = __int_as_float(sg.y & 0x7fffffff);
       const float2 av = d.l_avg[slot];
       const float a = av.x, b = av.y;
+      colh += (double)a * (double)dist;
+      colhe += (double)b * (double)dist;
       double dth[FRT_MAX_FREQ], dthe[FRT_MAX_FREQ], nin[FRT_MAX_FREQ];
       double total = 0.;
       for (int nu = 0; nu < F; nu++) {
@@ -194,7 +195,16 @@ __global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
         A.nphot[(size_t)nu * cap + i] = nph[nu];
         s += nph[nu];
       }
-      if (!(s > nmin)) {
+      bool tau_over = false;
+      if (A.col) {   // the optical-depth limit (opt-in)
+        const double nh = A.col[i] + colh, nhe = A.col[(size_t)cap + i] + colhe;
+        A.col[i] = nh;
+        A.col[(size_t)cap + i] = nhe;
+        double tmin = 1e300;
+        for (int nu = 0; nu < F; nu++) tmin = fmin(tmin, d.sigH1_d[nu] * nh + d.sigHe1_d[nu] * nhe);
+        tau_over = d.tau_max > 0.0 && tmin > d.tau_max;
+      }
+      if (!(s > nmin) || tau_over) {
         d.dead[i] = 1;
         nkill += 1;
         kil += (double)s;
@@ -239,7 +249,10 @@ __global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
 // NHO > 0 declares the first NHO bins below the HeI edge (sigma_HeI = 0 there, as in the 5-bin
 // spectrum, whose lowest three bins lie below 24.59 eV): those bins skip the HeI optical depth and
 // the H/He split, which give frac_h1 = 1 (or 0 where dtau_HI = 0) and frac_he1 = 0 for them.
-template <bool LAST, int NF, bool CHUNKED, int NHO = 0>
+// TAU (last pass, optical-depth limit on) sums each ray's HI and HeI columns over its segments in
+// FP64 (exact products of the float density and path), adds them to the ray's columns and removes
+// the ray once its optical depth exceeds d.tau_max in every bin.
+template <bool LAST, int NF, bool CHUNKED, int NHO = 0, bool TAU = false>
 __global__ void __launch_bounds__(256, LAST ? 4 : 5) k_raypass_mixed(Dev d, int iter, int chunk) {
   constexpr int MAXF = NF > 0 ? NF : FRT_MAX_FREQ;
   constexpr unsigned FULL = 0xffffffffu;
@@ -271,6 +284,7 @@ __global__ void __launch_bounds__(256, LAST ? 4 : 5) k_raypass_mixed(Dev d, int 
 #pragma unroll
   for (int nu = 0; nu < MAXF; nu++) nin[nu] = 0.f;
   float kdep = 0.f, nmin_ru = 0.f, nmin_rd = 0.f;
+  double colh = 0.0, colhe = 0.0;   // TAU: this pass's columns of the current ray
   const int2* sp = nullptr;
   int2 sg0 = make_int2(-1, 0), sg1 = make_int2(-1, 0);   // segments p and p + 1
   float2 av0 = make_float2(0.f, 0.f);                     // cell state of segment p
@@ -301,6 +315,7 @@ __global__ void __launch_bounds__(256, LAST ? 4 : 5) k_raypass_mixed(Dev d, int 
           ns = hd.z;
           p = 0;
           dumped = false;
+          colh = colhe = 0.0;
           dump_mask = 0;
           const BoxP& B = d.box[hd.w];
           kdep = B.kdep_f;
@@ -335,6 +350,10 @@ __global__ void __launch_bounds__(256, LAST ? 4 : 5) k_raypass_mixed(Dev d, int 
     if (slot >= 0 && slot < L) {
       const float dist = __int_as_float(sg.y & 0x7fffffff);
       const float a = av.x, b = av.y;
+      if (TAU) {
+        colh += (double)a * (double)dist;
+        colhe += (double)b * (double)dist;
+      }
       float total = 0.f;
 #pragma unroll
       for (int nu = 0; nu < MAXF; nu++) total += (nu < Fr) ? nin[nu] : 0.f;
@@ -430,7 +449,16 @@ __global__ void __launch_bounds__(256, LAST ? 4 : 5) k_raypass_mixed(Dev d, int 
           A.nphot[(size_t)nu * cap + i] = nin[nu];
           s += nin[nu];
         }
-        if (!(s > nmin_rd)) {
+        bool tau_over = false;
+        if (TAU) {
+          const double nh = A.col[i] + colh, nhe = A.col[(size_t)cap + i] + colhe;
+          A.col[i] = nh;
+          A.col[(size_t)cap + i] = nhe;
+          double tmin = 1e300;
+          for (int nu = 0; nu < Fr; nu++) tmin = fmin(tmin, d.sigH1_d[nu] * nh + d.sigHe1_d[nu] * nhe);
+          tau_over = tmin > d.tau_max;
+        }
+        if (!(s > nmin_rd) || tau_over) {
           d.dead[i] = 1;
           nkill += 1;
           kil += (double)s;
@@ -790,30 +818,6 @@ void launch_lit_init(const Dev& d, bool strict, int grid, cudaStream_t s) {
   else k_lit_init<false><<<grid, 256, 0, s>>>(d);
 }
 
-// The blocks of `kernel` at `block` threads that fit on all SMs at once (its occupancy times the SM
-// count), remembered per kernel and block size (a host-side query: no work is enqueued, so it may
-// run while a stream is being captured).
-template <typename K>
-static int resident_grid(K kernel, int block) {
-  struct Entry {
-    const void* k;
-    int block, grid;
-  };
-  static Entry cache[64];
-  static int n = 0;
-  static std::mutex mu;
-  std::lock_guard<std::mutex> lock(mu);
-  for (int i = 0; i < n; i++)
-    if (cache[i].k == (const void*)kernel && cache[i].block == block) return cache[i].grid;
-  int dev = 0, nsm = 148, nb = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, block, 0) != cudaSuccess || nb < 1) nb = 1;
-  const int g = nb * nsm;
-  if (n < 64) cache[n++] = Entry{(const void*)kernel, block, g};
-  return g;
-}
-
 // grid <= 0: the persistent ray pass with exactly its resident blocks (one wave: every warp's
 // static slice starts at once, none waits for a second wave)
 void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t s, int block, int chunk) {
@@ -825,7 +829,9 @@ void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t 
   }
   const bool q = chunk > 0;
   void (*k)(Dev, int, int);
-  if (d.F == 5 && d.nho >= 3) {
+  if (last && d.tau_max > 0.0) {   // the optical-depth limit (opt-in): the generic last pass with the columns
+    k = q ? k_raypass_mixed<true, 0, true, 0, true> : k_raypass_mixed<true, 0, false, 0, true>;
+  } else if (d.F == 5 && d.nho >= 3) {
     if (last) k = q ? k_raypass_mixed<true, 5, true, 3> : k_raypass_mixed<true, 5, false, 3>;
     else k = q ? k_raypass_mixed<false, 5, true, 3> : k_raypass_mixed<false, 5, false, 3>;
   } else if (d.F == 5) {
@@ -839,18 +845,23 @@ void launch_raypass(const Dev& d, int iter, bool strict, int grid, cudaStream_t 
   k<<<g, block, 0, s>>>(d, iter, chunk);
 }
 
+// grid <= 0: exactly the resident blocks of the chosen pass (its grid-stride loop then runs in one
+// wave; 8 blocks per SM against 5 resident for the middle passes ran 1.6 waves)
 void launch_litpass(const Dev& d, int iter, bool strict, bool fused_thermal, int grid, cudaStream_t s, int s_begin,
                     int s_end) {
   const bool last = iter == d.itercount - 1;
+  void (*k)(Dev, int, int);
   if (strict) {
-    if (!last) k_litpass<true, false, false><<<grid, 256, 0, s>>>(d, s_begin, s_end);
-    else if (fused_thermal) k_litpass<true, true, true><<<grid, 256, 0, s>>>(d, s_begin, s_end);
-    else k_litpass<true, true, false><<<grid, 256, 0, s>>>(d, s_begin, s_end);
+    if (!last) k = k_litpass<true, false, false>;
+    else if (fused_thermal) k = k_litpass<true, true, true>;
+    else k = k_litpass<true, true, false>;
   } else {
-    if (!last) k_litpass<false, false, false><<<grid, 256, 0, s>>>(d, s_begin, s_end);
-    else if (fused_thermal) k_litpass<false, true, true><<<grid, 256, 0, s>>>(d, s_begin, s_end);
-    else k_litpass<false, true, false><<<grid, 256, 0, s>>>(d, s_begin, s_end);
+    if (!last) k = k_litpass<false, false, false>;
+    else if (fused_thermal) k = k_litpass<false, true, true>;
+    else k = k_litpass<false, true, false>;
   }
+  const int g = grid > 0 ? grid : resident_grid(k, 256);
+  k<<<g, 256, 0, s>>>(d, s_begin, s_end);
 }
 
 void launch_dark(const Dev& d, bool strict, bool fused_thermal, int grid, cudaStream_t s) {

@@ -430,6 +430,19 @@ class RTContext:
                     "frt_download_rays")
         return out
 
+    def set_tau_limit(self, tau_max: float) -> None:
+        """frt_set_tau_limit: remove rays whose optical depth since their cast exceeds tau_max in
+        every frequency bin (an opt-in rule the reference does not have; 0 turns it off)."""
+        self._check(self.L.frt_set_tau_limit(self.h, C.c_double(tau_max)), "frt_set_tau_limit")
+
+    def ray_columns(self, box: int = 0) -> np.ndarray:
+        """The HI and HeI column densities (cm^-2) of the live rays, [n, 2] float64, in the order
+        of rays()."""
+        n = self.num_rays(box)
+        out = np.zeros((n, 2), np.float64)
+        self._check(self.L.frt_download_ray_columns(self.h, box, out.ctypes.data), "frt_download_ray_columns")
+        return out
+
     def adjoint(self, lo, hi, box: int = 0, want_dl: bool = True, want_dnh: bool = True):
         """frt_adjoint: J = sum of Gamma_HI over cells [lo, hi) of `box` after the next step's
         C2Ray iteration, with dJ/dL per source (photons/s) and dJ/dn_H per cell (cm^-3, N^3).

@@ -289,7 +289,7 @@ typedef struct {
                                                blocks_per_sm 0: the blocks resident at once */
   int raypass_chunk;                        /* 0: static per-warp slices; > 0: rays per queue chunk */
   int walk_block, walk_blocks_per_sm;       /* cell-boundary walk (update_rays) */
-  int cellpass_blocks_per_sm;               /* lit-cell pass of a C2Ray iteration */
+  int cellpass_blocks_per_sm;               /* lit-cell pass of a C2Ray iteration (0: resident) */
   int split_blocks_per_sm;                  /* compaction + split (split_rays) */
   int steps;                                /* frt_autotune: RT steps it took */
   /* frt_autotune: measured cost of the chosen shapes, ns per unit of work (crossing, ray, lit cell) */
@@ -319,6 +319,19 @@ frt_status frt_num_rays(frt_ctx* ctx, int box, long long* n);
  * x, y, z, time; nphot[nfreq]. Arrays must hold frt_num_rays() entries. */
 frt_status frt_download_rays(frt_ctx* ctx, int box, int16_t* order, int32_t* pixel, uint16_t* itheta,
                              int32_t* cell, float* geom9, float* nphot);
+
+/* Opt-in optical-depth limit; no counterpart in the reference, whose rays end only below
+ * nphot_min (ray_tracing.cc:782, 927-933). With tau_max > 0 every ray carries the HI and HeI
+ * column densities it crossed since its cast, summed in FP64 over the segments of each step's
+ * last C2Ray iteration (split children inherit them, a merged ray keeps its base ray's, rays read
+ * by frt_read_rays start at 0), and after the step's last ray pass a ray whose optical depth
+ * sigma_HI(nu) N_HI + sigma_HeI(nu) N_HeI exceeds tau_max in every frequency bin is removed like
+ * a ray below nphot_min (its photons counted as killed). 0 turns the limit off (the default);
+ * refused with the sub-grid model. Takes effect from the next step. */
+frt_status frt_set_tau_limit(frt_ctx* ctx, double tau_max);
+/* The HI and HeI column densities (cm^-2, 2 doubles per ray) of a box's live rays in the order of
+ * frt_download_rays; zeros while the optical-depth limit was never set. */
+frt_status frt_download_ray_columns(frt_ctx* ctx, int box, double* col2);
 
 /* Scalars of one box: t, dt, nphot_min, nphot_max, nphot_merge, num_thresh, dx, dx0 */
 frt_status frt_box_scalars(frt_ctx* ctx, int box, double* out8);

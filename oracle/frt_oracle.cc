@@ -155,6 +155,10 @@ struct Ray {
   float pdist[kMaxPL];
   short ray_end;
   int src;   // casting source (index into Ctx::src); a merge of rays of several sources gives -1
+  // opt-in optical-depth limit (not in the reference): the HI and HeI column densities the ray
+  // crossed since its cast (cm^-2 proper, FP64; split children inherit them, a merged ray keeps
+  // its base ray's)
+  double colH, colHe;
 };
 
 struct Src {
@@ -172,6 +176,7 @@ struct Ctx {
   float dx0, Lx, dxc, dt, t, clight, nc;
   float spectrum[kMaxF];
   double nphot_min, nphot_max, nphot_base_avg;
+  double tau_max;   // opt-in: remove a ray once its optical depth exceeds this in every bin (0: off)
   float nphot_merge;
   long num_thresh, total_rays;
   float random_angles[kNtheta][3];
@@ -857,9 +862,12 @@ static void find_avg_unu(Ctx& c) {
           p_prev = p;
         }
       }
+      double colH = 0., colHe = 0.;   // the columns of this pass's segments (tau limit)
       while (!c.subgrid && p < R.ray_end) {
         const int ind = R.pind[p];
         const long q = ind;
+        colH += (double)c.avg_nh1[q] * (double)R.pdist[p];
+        colHe += (double)c.avg_nhe1[q] * (double)R.pdist[p];
         for (int nu = 0; nu < F; nu++) {
           dtau_h1[nu] = c.avg_nh1[q] * c.sigH1[nu] * R.pdist[p];
           dtau_he1[nu] = c.avg_nhe1[q] * c.sigHe1[nu] * R.pdist[p];
@@ -919,7 +927,16 @@ static void find_avg_unu(Ctx& c) {
       }
       if (iter == c.itercount - 1) {
         for (int nu = 0; nu < F; nu++) R.nphot[nu] = (float)(nphot[nu] * exp(-tau_h1[nu] - tau_he1[nu]) / kPhotNorm);
-        if (sum_nphot(c, R) > c.nphot_min) {
+        bool tau_over = false;
+        if (c.tau_max > 0. && !c.subgrid) {
+          // opt-in limit: the ray's optical depth since its cast in its most transparent bin
+          R.colH += colH;
+          R.colHe += colHe;
+          double tau_min = 1e300;
+          for (int nu = 0; nu < F; nu++) tau_min = mindd(tau_min, c.sigH1[nu] * R.colH + c.sigHe1[nu] * R.colHe);
+          tau_over = tau_min > c.tau_max;
+        }
+        if (sum_nphot(c, R) > c.nphot_min && !tau_over) {
           R.active = true;
           R.pind[0] = R.pind[R.ray_end - 1];
         } else {
@@ -1223,6 +1240,8 @@ static void split_rays(Ctx& c) {
       Ch.time = time;
       Ch.pind[0] = icn * c.N * c.N + jcn * c.N + kcn;
       Ch.src = P.src;
+      Ch.colH = P.colH;
+      Ch.colHe = P.colHe;
       c.rays.push_back(Ch);
     }
   }
@@ -1589,11 +1608,33 @@ int orc_dump(void* h, const char* path) {
   frtd_add(&w, "ray_geom", FRTD_F32, 2, d9, g9.data());
   const int64_t dnf[2] = {nr, c.F};
   frtd_add(&w, "ray_nphot", FRTD_F32, 2, dnf, np.data());
+  if (c.tau_max > 0.) {
+    std::vector<double> col(nr * 2);
+    for (int64_t q = 0; q < nr; ++q) {
+      col[q * 2] = live[q]->colH;
+      col[q * 2 + 1] = live[q]->colHe;
+    }
+    const int64_t d2[2] = {nr, 2};
+    frtd_add(&w, "ray_col", FRTD_F64, 2, d2, col.data());
+    std::vector<double> sig(2 * c.F);
+    for (int nu = 0; nu < c.F; nu++) {
+      sig[nu] = c.sigH1[nu];
+      sig[c.F + nu] = c.sigHe1[nu];
+    }
+    const int64_t ds[2] = {2, c.F};
+    frtd_add(&w, "tau_sigma", FRTD_F64, 2, ds, sig.data());
+    frtd_add1(&w, "tau_max", FRTD_F64, 1, &c.tau_max);
+  }
   frtd_close(&w);
   return 0;
 }
 
 void orc_destroy(void* h) { delete (Ctx*)h; }
+
+// The opt-in optical-depth limit (no counterpart in the reference): from the next step on, a ray
+// whose optical depth since its cast exceeds tau_max in every frequency bin is removed like a ray
+// below nphot_min; 0 turns it off.
+void orc_set_tau_limit(void* h, double tau_max) { ((Ctx*)h)->tau_max = tau_max; }
 
 }  // extern "C"
 

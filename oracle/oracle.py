@@ -80,6 +80,7 @@ def lib():
         _lib.orc_set_subgrid.argtypes = [C.c_void_p] * 7 + [C.c_int]
         _lib.orc_hydro_step.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
                                         C.c_float]
+        _lib.orc_set_tau_limit.argtypes = [C.c_void_p, C.c_double]
         _lib.orc_adj_objective.restype = C.c_double
         _lib.orc_adj_objective.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_long)]
@@ -157,6 +158,12 @@ class Oracle:
     def cosmo_expansion(self, a_current: float, a_prev: float) -> None:
         """update_cosmo_expansion with the given scale factors, then update_dt."""
         self._lib.orc_cosmo_expansion(self.h, C.c_float(a_current), C.c_float(a_prev))
+
+    def set_tau_limit(self, tau_max: float) -> None:
+        """The opt-in optical-depth limit (not in the reference): a ray whose optical depth since
+        its cast exceeds tau_max in every bin is removed after the step's last ray pass; the dump
+        then carries each ray's HI and HeI columns ("ray_col"). 0 turns it off."""
+        self._lib.orc_set_tau_limit(self.h, C.c_double(tau_max))
 
     def set_subgrid(self, tables, consts, ifront: bool = False) -> None:
         """The sub-grid model (equilibrium; with I-front tracking when ifront) with the

@@ -51,9 +51,12 @@ def threshold_cells_bound(ncell: int) -> int:
     return 2 + ncell // 10000
 
 
-def oracle_states(inp: W.BoxInputs, seed: int, steps: int) -> List[Dict[str, np.ndarray]]:
-    """States of the CPU oracle after the set-up (index 0) and after each step."""
+def oracle_states(inp: W.BoxInputs, seed: int, steps: int, tau_max: float = 0.0) -> List[Dict[str, np.ndarray]]:
+    """States of the CPU oracle after the set-up (index 0) and after each step (with the opt-in
+    optical-depth limit tau_max when it is > 0)."""
     o = O.Oracle(inp, seed)
+    if tau_max > 0:
+        o.set_tau_limit(tau_max)
     out = []
     with tempfile.TemporaryDirectory() as td:
         for s in range(steps + 1):
@@ -269,9 +272,26 @@ def compare_rays(dev: Dict[str, np.ndarray], ref: Dict[str, np.ndarray], nphot_m
         hd, hr = dev["ray_geom"][ma, 0:3], ref["ray_geom"][mb, 0:3]
         out["dir_maxabs"] = float(np.abs(hd.astype(np.float64) - hr).max())
 
+    # the optical-depth limit (opt-in, oracle dumps with "ray_col"): the columns of the matched
+    # rays, and rays whose optical depth ties with the limit count as near ties
+    tau = None
+    if "ray_col" in ref and "ray_col" in dev and "tau_sigma" in ref:
+        tau = (float(ref["tau_max"][0]), ref["tau_sigma"].astype(np.float64))
+        out["col_maxrel"] = 0.0
+        if len(ma):
+            cd, cr = dev["ray_col"][ma].astype(np.float64), ref["ray_col"][mb].astype(np.float64)
+            den = np.maximum(np.abs(cr), 1.0)
+            out["col_maxrel"] = float((np.abs(cd - cr) / den).max())
+
     def near_tie(st, ids):
         s = st["ray_nphot"][ids].astype(np.float64).sum(axis=1) if len(ids) else np.zeros(0)
-        return int((np.abs(s / nphot_min - 1.0) < NEAR_TIE).sum()) if nphot_min > 0 else 0
+        tie = (np.abs(s / nphot_min - 1.0) < NEAR_TIE) if nphot_min > 0 else np.zeros(len(s), bool)
+        if tau is not None and len(ids):
+            tmax, sig = tau
+            col = st["ray_col"][ids].astype(np.float64)
+            tmin = (col[:, :1] * sig[0][None, :] + col[:, 1:2] * sig[1][None, :]).min(axis=1)
+            tie |= np.abs(tmin / tmax - 1.0) < NEAR_TIE
+        return int(tie.sum())
 
     out["unmatched_dev"] = len(ud2)
     out["unmatched_ref"] = len(ur2)
