@@ -972,10 +972,19 @@ __global__ void __launch_bounds__(1024) k_cast_scan(Dev d) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (threadIdx.x == 0) base_s = d.ctl->nray[cur];
   __syncthreads();
-  for (int s0 = 0; s0 < d.nsrc; s0 += blockDim.x) {
-    const int s = s0 + threadIdx.x;
-    const int cnt = (s < d.nsrc) ? d.src_pos[s] : 0;
-    int incl = cnt;
+  // each thread takes K consecutive sources per round (one round for up to 16 384 sources): its
+  // own sum, one block-wide scan of the sums, then the K positions in order
+  constexpr int K = 16;
+  for (int s0 = 0; s0 < d.nsrc; s0 += (int)blockDim.x * K) {
+    const int sb = s0 + (int)threadIdx.x * K;
+    int cnt[K];
+    int tot = 0;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      cnt[k] = (sb + k < d.nsrc) ? d.src_pos[sb + k] : 0;
+      tot += cnt[k];
+    }
+    int incl = tot;
     for (int o = 1; o < 32; o <<= 1) {
       const int v = __shfl_up_sync(0xffffffffu, incl, o);
       if (lane >= o) incl += v;
@@ -991,7 +1000,13 @@ __global__ void __launch_bounds__(1024) k_cast_scan(Dev d) {
       wsum[lane] = v;   // inclusive prefix over the warps
     }
     __syncthreads();
-    if (s < d.nsrc) d.src_pos[s] = base_s + (w > 0 ? wsum[w - 1] : 0) + incl - cnt;
+    int off = base_s + (w > 0 ? wsum[w - 1] : 0) + incl - tot;
+#pragma unroll
+    for (int k = 0; k < K; k++)
+      if (sb + k < d.nsrc) {
+        d.src_pos[sb + k] = off;
+        off += cnt[k];
+      }
     __syncthreads();
     if (threadIdx.x == 0) base_s += wsum[31];
     __syncthreads();

@@ -4,9 +4,9 @@ frt_set_tau_limit(5): each ray carries its HI and HeI columns in FP64 and is rem
 optical depth exceeds 5 in every bin (a rule of the hot-path specification that the reference does
 not have, so parity is pinned on the oracle only). The 16^3 box over 8 steps in both precisions:
 the contract tolerances of tests/test_gpu_parity.py on every field, the ray tree and the photon
-ledger, each matched ray's columns (1e-4 relative in mixed precision, whose time-averaged densities
-carry float rounding, 1e-6 in strict), and a ray kept on one side only must tie with nphot_min or
-with the limit. The limit must remove rays the reference rule keeps.
+ledger, each matched ray's columns (sums of the cells' time-averaged densities, which the device
+forms from float-atomic rate sums: 1e-4 relative in mixed precision, 1e-5 in strict, the rates'
+tolerances), and a ray kept on one side only must tie with nphot_min or with the limit. The limit must remove rays the reference rule keeps.
 """
 import numpy as np
 import pytest
@@ -49,7 +49,7 @@ def test_tau_limit_matches_oracle(precision):
     for s in range(1, SPEC.steps + 1):
         r = PT.compare_rays(states[s], ref[s], ref[s]["scalars"][2], 1e-5 if strict else 1e-4,
                             dx=float(ref[s]["scalars"][8]), dx0=float(ref[s]["scalars"][7]))
-        assert r["col_maxrel"] < (1e-6 if strict else 1e-4), (s, r["col_maxrel"])
+        assert r["col_maxrel"] < (1e-5 if strict else 1e-4), (s, r["col_maxrel"])
     # the limit removed rays that the nphot_min rule alone keeps
     off, _ = _device(precision, 0.0)
     assert len(states[-1]["ray_order"]) < len(off[-1]["ray_order"])
