@@ -50,12 +50,12 @@ DARK_TRAFFIC_BYTES_PER_CELL = 1343184384 / 13264001
 # Ray pass (the dominant kernel): the algorithmic bytes of one crossing in one C2Ray iteration as
 # the hot-path analysis counts them -- 8 B segment read, 8 B of gathered <n_HI>, <n_HeI>, 68 B of
 # deposits (2 + 3 x 5 floats) -- and the ncu DRAM bytes (read + write) per crossing of one launch,
-# the mean over the 5 passes of step 24 of L (17 465 923 crossings per pass; 679.6 MB per launch).
+# the mean over the 5 passes of step 24 of L (17 465 922 crossings per pass; 675.7 MB per launch).
 # The number of ray passes per step is the context's C2Ray iteration count (RTContext.itercount).
 RAYPASS_BYTES_PER_CROSSING = 8 + 8 + 68
 # warm-up steps that frt_autotune takes (the last ones of the warm-up)
 AUTOTUNE_STEPS = 4
-RAYPASS_TRAFFIC_BYTES_PER_CROSSING = 38.9
+RAYPASS_TRAFFIC_BYTES_PER_CROSSING = 38.7
 # Walk (k_advance): per live ray its record read (cell, geometry, box, time: 44 B) and written
 # back with its removal flag (29 B); per moved ray the 16-byte header of the ray passes; per
 # crossing its packed segment {cell, dist} written (8 B) and the cell's lit mark (1 B).
