@@ -44,9 +44,9 @@ sys.path.insert(0, HERE)
 
 DARK_BYTES_PER_CELL = 82  # 10 float fields + treion_flag + lit_flag read, 10 float fields written
 # DRAM bytes per dark cell of one k_dark launch, from ncu (dram__bytes_read.sum + write.sum) at
-# step 24 of the L workload: 1343.2 MB for 13 264 001 dark cells. The
+# step 24 of the L workload: 1344.7 MB for 13 264 001 dark cells. The
 # bench scales it by the dark cells of its own steps (traffic grows with the cells processed).
-DARK_TRAFFIC_BYTES_PER_CELL = 1343184384 / 13264001
+DARK_TRAFFIC_BYTES_PER_CELL = 1344697856 / 13264001
 # Ray pass (the dominant kernel): the algorithmic bytes of one crossing in one C2Ray iteration as
 # the hot-path analysis counts them -- 8 B segment read, 8 B of gathered <n_HI>, <n_HeI>, 68 B of
 # deposits (2 + 3 x 5 floats) -- and the ncu DRAM bytes (read + write) per crossing of one launch,
