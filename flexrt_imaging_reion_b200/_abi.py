@@ -36,7 +36,7 @@ EXPORTS = ["frt_create", "frt_destroy", "frt_last_error", "frt_rotation_table", 
            "frt_read_treion", "frt_read_rays", "frt_update_cosmo_expansion",
            "frt_set_cast_per_source", "frt_last_kernel_timing", "frt_set_source_owner", "frt_step_phase",
            "frt_phase_buffers", "frt_autotune", "frt_get_tuning", "frt_set_tuning", "frt_update_hydro_step", "frt_set_phase_async",
-           "frt_phase_stream", "frt_set_subgrid", "frt_set_tau_limit", "frt_download_ray_columns"]
+           "frt_phase_stream", "frt_set_subgrid", "frt_set_tau_limit", "frt_download_ray_columns", "frt_take_rays", "frt_put_rays", "frt_set_nphot_merge"]
 PHASE_WALK, PHASE_CELLS, PHASE_RAYPASS, PHASE_CELLPASS, PHASE_END = 0, 1, 2, 3, 4
 NOALLOC_MAX_CELLS = 1 << 20
 
@@ -131,6 +131,9 @@ def lib() -> C.CDLL:
         "frt_num_rays": ([P, I, C.POINTER(LL)], I),
         "frt_download_rays": ([P, I, P, P, P, P, P, P], I),
         "frt_set_tau_limit": ([P, C.c_double], I),
+        "frt_take_rays": ([P, I, I, P, C.c_size_t, C.POINTER(C.c_size_t)], I),
+        "frt_put_rays": ([P, I, P, C.c_size_t], I),
+        "frt_set_nphot_merge": ([P, I, C.c_double], I),
         "frt_download_ray_columns": ([P, I, P], I),
         "frt_box_scalars": ([P, I, P], I),
         "frt_last_timing": ([P, P, P], I),

@@ -1451,6 +1451,17 @@ frt_status frt_download_ray_columns(frt_ctx* ctx, int box, double* col2) {
   return FRT_OK;
 }
 
+frt_status frt_set_nphot_merge(frt_ctx* ctx, int box, double nphot_merge) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  if (!(nphot_merge >= 0.0)) return FRT_ERR_INVALID;
+  CK(cudaStreamSynchronize(ctx->s_main));
+  if ((st = download_boxes(ctx))) return st;
+  ctx->hbox[box].nphot_merge = (float)nphot_merge;
+  CK(copy_sync(ctx, &ctx->d.box[box].nphot_merge, &ctx->hbox[box].nphot_merge, sizeof(float), cudaMemcpyHostToDevice));
+  return FRT_OK;
+}
+
 frt_status frt_box_scalars(frt_ctx* ctx, int box, double* out8) {
   frt_status st = check_box(ctx, box);
   if (st) return st;
@@ -1510,9 +1521,9 @@ frt_status frt_step_phase(frt_ctx* ctx, int phase, int iter, const uint16_t* ith
                           const uint16_t* itheta_per_source, frt_step_stats* stats) {
   if (!ctx) return FRT_ERR_INVALID;
   Dev& d = ctx->d;
-  if (d.per_bin || d.bin_base || d.subgrid) {
-    ctx->err = "frt_step_phase: needs core outputs, mixed precision, the plain model and a box whose ray count "
-               "cannot reach the merge threshold (the per-bin rates and the merge are not combined across contexts)";
+  if (d.per_bin || d.subgrid) {
+    ctx->err = "frt_step_phase: needs core outputs, mixed precision and the plain model (the per-bin rates are "
+               "not combined across contexts)";
     return FRT_ERR_INVALID;
   }
   cudaStream_t s = ctx->s_main;
@@ -1814,7 +1825,16 @@ frt_status frt_read_treion(frt_ctx* ctx, int box, const void* buf, size_t len) {
   return FRT_OK;
 }
 
-frt_status frt_read_rays(frt_ctx* ctx, int box, const void* buf, size_t len) {
+}  // extern "C"
+
+namespace {
+// Appends ray records of the reference's ray-file format (write_rays_binary) to the current pool
+// of a box. restart: the restart path of init_rt (the free-slot probe drops a record at slot 0 with
+// no first-bin photons, and the loaded photons enter the ledger's in-flight count); otherwise the
+// records are rays moved between contexts during or between steps (every record kept, the ledger
+// untouched, the new slots' removal flags cleared).
+static frt_status append_ray_records(frt_ctx* ctx, int box, const void* buf, size_t len, bool restart,
+                                     const char* what) {
   frt_status st = check_box(ctx, box);
   if (st) return st;
   if (!buf) return FRT_ERR_INVALID;
@@ -1829,14 +1849,14 @@ frt_status frt_read_rays(frt_ctx* ctx, int box, const void* buf, size_t len) {
   size_t pos = 0;
   while (true) {
     if (pos + 8 > len) {
-      ctx->err = "frt_read_rays: record set not ended by slot -1";
+      ctx->err = std::string(what) + ": record set not ended by slot -1";
       return FRT_ERR_INVALID;
     }
     int64_t slot;
     memcpy(&slot, p + pos, 8);
     if (slot == -1) break;
     if (pos + rs > len) {
-      ctx->err = "frt_read_rays: truncated record";
+      ctx->err = std::string(what) + ": truncated record";
       return FRT_ERR_INVALID;
     }
     const unsigned char* r = p + pos + 8;
@@ -1852,9 +1872,9 @@ frt_status frt_read_rays(frt_ctx* ctx, int box, const void* buf, size_t len) {
     pos += rs;
     // init_rt's free-slot probe (rt_funcs.cc:117-124): select_index(0) hands out slot 0, and a ray
     // there whose first-bin photon count is 0 is removed
-    if (slot == 0 && v[3] == 0.f) continue;
+    if (restart && slot == 0 && v[3] == 0.f) continue;
     if (c < 0 || c >= ctx->hbox[box].ncell || px < 0 || o < 0 || o > kLmax || it >= kNtheta) {
-      ctx->err = "frt_read_rays: ray outside the box or with an invalid order / pixel / angle index";
+      ctx->err = std::string(what) + ": ray outside the box or with an invalid order / pixel / angle index";
       return FRT_ERR_INVALID;
     }
     cell.push_back(c); pix.push_back(px); ord.push_back(o); ith.push_back(it); bx.push_back((uint16_t)box);
@@ -1867,7 +1887,7 @@ frt_status frt_read_rays(frt_ctx* ctx, int box, const void* buf, size_t len) {
   CK(copy_sync(ctx, &c, d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
   const size_t base = (size_t)c.nray[c.cur], m = cell.size();
   if (base + m > (size_t)d.ray_cap) {
-    ctx->err = "frt_read_rays: ray pool capacity exceeded";
+    ctx->err = std::string(what) + ": ray pool capacity exceeded";
     return FRT_ERR_CAPACITY;
   }
   double inflight = 0.0;
@@ -1890,9 +1910,77 @@ frt_status frt_read_rays(frt_ctx* ctx, int box, const void* buf, size_t len) {
     CK(fill_sync(ctx, col + base, 0, sizeof(double) * m));
     CK(fill_sync(ctx, col + d.ray_cap + base, 0, sizeof(double) * m));
   }
+  if (m && !restart) CK(fill_sync(ctx, d.dead + base, 0, m));
   c.nray[c.cur] = (int)(base + m);
-  c.in_flight += inflight * 1e60;   // photon ledger: physical photons of the loaded rays
+  if (restart) c.in_flight += inflight * 1e60;   // photon ledger: physical photons of the loaded rays
   CK(copy_sync(ctx, d.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice));
+  return FRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+frt_status frt_read_rays(frt_ctx* ctx, int box, const void* buf, size_t len) {
+  return append_ray_records(ctx, box, buf, len, true, "frt_read_rays");
+}
+
+frt_status frt_put_rays(frt_ctx* ctx, int box, const void* buf, size_t len) {
+  return append_ray_records(ctx, box, buf, len, false, "frt_put_rays");
+}
+
+frt_status frt_take_rays(frt_ctx* ctx, int box, int in_step, void* buf, size_t cap, size_t* len) {
+  frt_status st = check_box(ctx, box);
+  if (st) return st;
+  if (ctx->d.nbox != 1) {
+    ctx->err = "frt_take_rays: a context of one box";
+    return FRT_ERR_INVALID;
+  }
+  Dev& d = ctx->d;
+  Ctl c;
+  CK(cudaStreamSynchronize(ctx->s_main));
+  CK(cudaStreamSynchronize(ctx->s_dark));
+  CK(copy_sync(ctx, &c, d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+  const int nr = std::min(c.nray[c.cur], d.ray_cap);
+  // within a step (after its last C2Ray pass) the removal flags of the pool are the step's; between
+  // steps they belong to the previous pool and every ray of the current one is live
+  std::vector<uint8_t> dead(nr, 0);
+  if (nr && in_step) CK(copy_sync(ctx, dead.data(), d.dead, (size_t)nr, cudaMemcpyDeviceToHost));
+  long long live = 0;
+  for (int i = 0; i < nr; i++) live += dead[i] ? 0 : 1;
+  const int F = d.F;
+  const size_t need = (size_t)live * ray_record_size(F) + 8;
+  if (len) *len = need;
+  if (!buf) return FRT_OK;
+  if (cap < need) {
+    ctx->err = "frt_take_rays: buffer too small";
+    return FRT_ERR_INVALID;
+  }
+  std::vector<int16_t> ord(nr);
+  std::vector<int32_t> pix(nr), cell(nr);
+  std::vector<uint16_t> ith(nr);
+  std::vector<float> g((size_t)nr * 9), np((size_t)nr * F);
+  if ((st = frt_download_rays(ctx, box, ord.data(), pix.data(), ith.data(), cell.data(), g.data(), np.data())))
+    return st;
+  Bytes o{(unsigned char*)buf, 0, cap};
+  long long x = 0;
+  for (int i = 0; i < nr; i++) {
+    if (dead[i]) continue;
+    const float* v = &g[(size_t)i * 9];
+    o.put<int64_t>(x++);
+    o.put<bool>(true);
+    o.put<int16_t>(ord[i]);
+    o.put<int32_t>(pix[i]);
+    o.put<uint16_t>(ith[i]);
+    o.put<float>(v[0]); o.put<float>(v[1]); o.put<float>(v[2]);
+    for (int nu = 0; nu < F; nu++) o.put<float>(np[(size_t)i * F + nu]);
+    for (int k = 3; k < 9; k++) o.put<float>(v[k]);   // r dr x y z time
+    o.put<int32_t>(cell[i]);
+  }
+  o.put<int64_t>(-1);
+  // the context keeps none of its rays
+  c.nray[c.cur] = 0;
+  CK(copy_sync(ctx, &d.ctl->nray[c.cur], &c.nray[c.cur], sizeof(int), cudaMemcpyHostToDevice));
   return FRT_OK;
 }
 

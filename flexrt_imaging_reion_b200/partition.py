@@ -17,6 +17,16 @@ of the float pairs are taken in a different order than one context's atomics tak
 results agree with a one-context run to float rounding (and the ray trees agree up to rays whose
 photon count ties with nphot_min).
 
+A box whose ray count reaches its merge threshold merges rays of different sources, so in a step
+where the contexts' live rays together exceed the threshold (their counts summed after the last
+ray pass) the rays are brought together first: every other context hands its live rays to context
+0 (frt_take_rays / frt_put_rays, ray records in the reference's ray-file format), context 0 runs
+the end of the step (count, merge, split, compaction) on all of them, the others end the step
+without rays, context 0's merge threshold nphot_merge goes to the others, and after the step the
+rays are dealt out again in equal shares (a ray's context does not matter: every context adds the
+deposits of all of them). The records pass through the host: a correct first form whose cost
+grows with the ray count of the merging steps.
+
 `DistCombiner` combines over torch.distributed ranks (NCCL, one GPU per rank); `LocalCombiner`
 combines contexts that live in one process (the emulation the tests use on one GPU).
 """
@@ -39,6 +49,31 @@ def source_owner_masks(lum: Sequence[float], world: int) -> List[np.ndarray]:
     for k, s in enumerate(order):
         masks[k % world][s] = 1
     return masks
+
+
+# bytes of a ray record besides its photon counts (frt_write_rays: slot, active flag, order, pixel,
+# angle index, direction, r, dr, x, y, z, time, cell); a record set ends with the slot -1
+RAY_RECORD_HEAD = 8 + 1 + 2 + 4 + 2 + 12 + 24 + 4
+_RECORDS_END = (-1).to_bytes(8, "little", signed=True)
+
+
+def split_records(data: bytes, nfreq: int, parts: int) -> List[bytes]:
+    """A record set cut into `parts` record sets of (nearly) equal ray counts, in order."""
+    rec = RAY_RECORD_HEAD + 4 * nfreq
+    n = (len(data) - 8) // rec
+    if n * rec + 8 != len(data) or data[-8:] != _RECORDS_END:
+        raise ValueError("not a ray record set of this frequency count")
+    return [data[(n * k // parts) * rec:(n * (k + 1) // parts) * rec] + _RECORDS_END for k in range(parts)]
+
+
+def merge_reachable(ctx: rt.RTContext) -> bool:
+    """Whether the box's ray count can reach its merge threshold with this ray capacity (fixed for
+    the context: asked once)."""
+    v = getattr(ctx, "_merge_reachable", None)
+    if v is None:
+        v = ctx.box_scalars()["num_thresh"] < ctx._cfg.ray_capacity
+        ctx._merge_reachable = v
+    return v
 
 
 class _DevArray:
@@ -90,6 +125,24 @@ class LocalCombiner:
     def heat(self):
         self._apply(lambda v: v[2], lambda a, b: a + b)
 
+    # the merge of a shared box (see the module docstring)
+    def live_rays(self) -> int:
+        return sum(int(c.count_rays()[0]) for c in self.ctxs)
+
+    def gather_rays(self):
+        for c in self.ctxs[1:]:
+            self.ctxs[0].put_rays(c.take_rays(0, in_step=True))
+
+    def share_merge_threshold(self):
+        v = self.ctxs[0].box_scalars()["nphot_merge"]
+        for c in self.ctxs[1:]:
+            c.set_nphot_merge(v)
+
+    def deal_rays(self):
+        parts = split_records(self.ctxs[0].take_rays(0, in_step=False), self.ctxs[0].F, len(self.ctxs))
+        for c, p in zip(self.ctxs, parts):
+            c.put_rays(p)
+
 
 class DistCombiner:
     """Combines one context per rank over torch.distributed (NCCL: one GPU per rank). `views`
@@ -139,6 +192,41 @@ class DistCombiner:
         import torch.distributed as dist
         self._all_reduce(self._views(self.ctxs[0])[2], dist.ReduceOp.SUM)
 
+    # the merge of a shared box: host records through object collectives (every rank takes the
+    # same steps in the same order)
+    def live_rays(self) -> int:
+        import torch.distributed as dist
+        out = [None] * dist.get_world_size()
+        dist.all_gather_object(out, int(self.ctxs[0].count_rays()[0]))
+        return sum(out)
+
+    def gather_rays(self):
+        import torch.distributed as dist
+        rank, world = dist.get_rank(), dist.get_world_size()
+        mine = self.ctxs[0].take_rays(0, in_step=True) if rank != 0 else b""
+        got = [None] * world if rank == 0 else None
+        dist.gather_object(mine, got, dst=0)
+        if rank == 0:
+            for data in got[1:]:
+                self.ctxs[0].put_rays(data)
+
+    def share_merge_threshold(self):
+        import torch.distributed as dist
+        v = [self.ctxs[0].box_scalars()["nphot_merge"] if dist.get_rank() == 0 else None]
+        dist.broadcast_object_list(v, src=0)
+        if dist.get_rank() != 0:
+            self.ctxs[0].set_nphot_merge(v[0])
+
+    def deal_rays(self):
+        import torch.distributed as dist
+        rank, world = dist.get_rank(), dist.get_world_size()
+        parts = None
+        if rank == 0:
+            parts = split_records(self.ctxs[0].take_rays(0, in_step=False), self.ctxs[0].F, world)
+        out = [None]
+        dist.scatter_object_list(out, parts, src=0)
+        self.ctxs[0].put_rays(out[0])
+
 
 def step_shares(ctxs: Sequence[rt.RTContext], combiner, itercount: int = 5) -> List[Dict[str, float]]:
     """One step of a box shared by `ctxs` (the contexts of this process: all of them for a
@@ -156,7 +244,16 @@ def step_shares(ctxs: Sequence[rt.RTContext], combiner, itercount: int = 5) -> L
             combiner.heat()
         for c in ctxs:
             c.step_phase(_abi.PHASE_CELLPASS, it)
-    return [c.step_phase(_abi.PHASE_END) for c in ctxs]
+    # a box that can reach its merge threshold: the contexts' live rays counted together, and
+    # merged on context 0 when they exceed it
+    merge = merge_reachable(ctxs[0]) and combiner.live_rays() > ctxs[0].box_scalars()["num_thresh"]
+    if merge:
+        combiner.gather_rays()
+    stats = [c.step_phase(_abi.PHASE_END) for c in ctxs]
+    if merge:
+        combiner.share_merge_threshold()
+        combiner.deal_rays()
+    return stats
 
 
 def sum_stats(stats: Sequence[Dict[str, float]]) -> Dict[str, float]:

@@ -478,6 +478,24 @@ class RTContext:
         self._check(self.L.frt_last_adjoint_timing(self.h, C.byref(v)), "frt_last_adjoint_timing")
         return float(v.value)
 
+    def take_rays(self, box: int = 0, in_step: bool = False) -> bytes:
+        """frt_take_rays: the live rays of the box as ray records (bytes); the context keeps none.
+        in_step: between the step's last C2Ray pass and its end phase (the pass's removals are
+        skipped); otherwise between steps."""
+        n = C.c_size_t(0)
+        self._check(self.L.frt_take_rays(self.h, box, 1 if in_step else 0, None, 0, C.byref(n)), "frt_take_rays")
+        buf = C.create_string_buffer(n.value)
+        self._check(self.L.frt_take_rays(self.h, box, 1 if in_step else 0, buf, n.value, C.byref(n)),
+                    "frt_take_rays")
+        return buf.raw[: n.value]
+
+    def put_rays(self, data: bytes, box: int = 0) -> None:
+        """frt_put_rays: appends ray records taken from another context of the same box."""
+        self._check(self.L.frt_put_rays(self.h, box, data, len(data)), "frt_put_rays")
+
+    def set_nphot_merge(self, value: float, box: int = 0) -> None:
+        self._check(self.L.frt_set_nphot_merge(self.h, box, C.c_double(value)), "frt_set_nphot_merge")
+
     def box_scalars(self, box: int = 0) -> Dict[str, float]:
         v = np.zeros(8)
         self._check(self.L.frt_box_scalars(self.h, box, v.ctypes.data), "frt_box_scalars")

@@ -364,6 +364,23 @@ frt_status frt_read_gas(frt_ctx* ctx, int box, const void* buf, size_t len);
 frt_status frt_read_treion(frt_ctx* ctx, int box, const void* buf, size_t len);
 frt_status frt_read_rays(frt_ctx* ctx, int box, const void* buf, size_t len);
 
+/* Rays moved between the contexts that share one box (the source-shared form over several GPUs,
+ * no counterpart in the reference). frt_take_rays writes the live rays of a one-box context in
+ * the ray-record format of frt_write_rays and leaves the context without rays: with in_step = 1
+ * between the step's last C2Ray pass (FRT_PHASE_CELLPASS of the last iteration) and
+ * FRT_PHASE_END, skipping the rays that pass removed; with in_step = 0 between steps. buf = NULL
+ * returns the size in *len. frt_put_rays appends such records to a context's rays at the same
+ * points (no free-slot probe, no change to the photon ledger). Used to merge the rays of all
+ * contexts on one of them when the box's ray count reaches the merge threshold, and to deal them
+ * out again after the step. */
+frt_status frt_take_rays(frt_ctx* ctx, int box, int in_step, void* buf, size_t cap, size_t* len);
+frt_status frt_put_rays(frt_ctx* ctx, int box, const void* buf, size_t len);
+/* Sets a box's merge threshold nphot_merge (calc_nphot_merge, ray_tracing.cc:176-227; it persists
+ * between the steps that merge and sets the split threshold max(4 nphot_merge, 4 nphot_min)):
+ * after the contexts of a shared box merged their rays on one of them, the others take that
+ * context's value (frt_box_scalars, index 4) so that every context splits alike. */
+frt_status frt_set_nphot_merge(frt_ctx* ctx, int box, double nphot_merge);
+
 /* ---- adjoint of the next step's Gamma field --------------------------------------------------
  * Objective: J = sum of Gamma_HI (gamma_H1_tot, ray_tracing.cc:1152) over the cells
  * [lo, hi) (i, j, k) of one box after the C2Ray iteration of the next step. frt_adjoint returns J

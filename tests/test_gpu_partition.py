@@ -51,12 +51,39 @@ def test_shares_match_oracle(case):
     assert PT.photon_budget(stats, in0) < 1e-6
 
 
-def test_phases_refused_when_merging_is_reachable():
-    inp = W.make_inputs(W.config_tiny())
-    ctx = P.make_share(inp, 11, 0, 2, ray_capacity=1 << 20)
-    with pytest.raises(rt.FrtError, match="status 1"):
-        P.step_shares([ctx], P.LocalCombiner([ctx]))
-    ctx.close()
+@pytest.mark.parametrize("case,world", [("T16M", 2), ("T16N", 3)])
+def test_shares_merge_like_one_box(case, world):
+    """Boxes whose ray count reaches the merge threshold: in the steps that merge, the shares hand
+    their rays to share 0, which merges, splits and compacts them all; the rays are dealt out
+    again after the step. Against the oracle's one-box run with the merged-ray tolerances of
+    tests/test_gpu_parity.py (merged rays carry float sums in another order), and merging must
+    really happen."""
+    from test_gpu_parity import T16M, T16N
+    spec, seed = {"T16M": T16M, "T16N": T16N}[case]
+    inp = W.make_inputs(spec)
+    ref = PT.oracle_states(inp, seed, spec.steps)
+    shares = [P.make_share(inp, seed, r, world, ray_capacity=1 << 20) for r in range(world)]
+    assert P.merge_reachable(shares[0])
+    comb = P.LocalCombiner(shares)
+    states = [_union_state(shares)]
+    in0 = sum(c.in_flight() for c in shares)
+    stats = []
+    merged = 0
+    for s in range(spec.steps):
+        tot = P.sum_stats(P.step_shares(shares, comb))
+        assert tot["error_flags"] == 0, tot
+        assert tot["crossings"] == int(ref[s + 1]["scalars"][10]), (s, tot["crossings"], ref[s + 1]["scalars"][10])
+        merged += tot["rays_merged"]
+        stats.append(tot)
+        states.append(_union_state(shares))
+        # every share splits with the same merge threshold, and no share is left without rays
+        nm = {c.box_scalars()["nphot_merge"] for c in shares}
+        assert len(nm) == 1, nm
+    for c in shares:
+        c.close()
+    check(states, ref, False, merged=True)
+    assert merged > 0 and any(float(r["scalars"][4]) > 0 for r in ref)
+    assert PT.photon_budget(stats, in0) < 1e-6
 
 
 def test_one_share_async_phases_match_oracle():
