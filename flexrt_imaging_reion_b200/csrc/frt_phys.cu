@@ -245,7 +245,9 @@ __global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
 // configuration here), so the per-bin loops unroll exactly; NF = 0 takes d.F at run time.
 // CHUNKED compiles the queue form; the static-slice form carries none of its bookkeeping. The
 // minimum resident blocks keep the last pass (which also writes the rays' photon counts and
-// the heating pairs) at 64 registers, four 256-thread blocks per SM.
+// the heating pairs) at 64 registers, four 256-thread blocks per SM, and the middle passes at
+// 40 registers, six blocks per SM (48 warps to cover the lit-cell gathers; 0.246 against 0.255 ms
+// per pass at L with five).
 // NHO > 0 declares the first NHO bins below the HeI edge (sigma_HeI = 0 there, as in the 5-bin
 // spectrum, whose lowest three bins lie below 24.59 eV): those bins skip the HeI optical depth and
 // the H/He split, which give frac_h1 = 1 (or 0 where dtau_HI = 0) and frac_he1 = 0 for them.
@@ -253,7 +255,7 @@ __global__ void __launch_bounds__(256) k_raypass_strict(Dev d) {
 // FP64 (exact products of the float density and path), adds them to the ray's columns and removes
 // the ray once its optical depth exceeds d.tau_max in every bin.
 template <bool LAST, int NF, bool CHUNKED, int NHO = 0, bool TAU = false>
-__global__ void __launch_bounds__(256, LAST ? 4 : 5) k_raypass_mixed(Dev d, int iter, int chunk) {
+__global__ void __launch_bounds__(256, LAST ? 4 : 6) k_raypass_mixed(Dev d, int iter, int chunk) {
   constexpr int MAXF = NF > 0 ? NF : FRT_MAX_FREQ;
   constexpr unsigned FULL = 0xffffffffu;
   const int Fr = NF > 0 ? NF : d.F;
